@@ -1,0 +1,427 @@
+#!/usr/bin/env python
+"""Throughput of the batched B+tree on B200: Mops/s at 2^26 uint64 keys with a
+95% search / 5% insert mix, batches of 2^22 requests through the sort-based
+batch merge (the reference's v38 meaning), plain and learned descent, p50/p99
+batch latency.
+
+One step = one bt_execute_batch over a fresh, device-resident batch of 2^22
+seeded synthetic requests (the reference's dataset files are not shipped; the
+generator reproduces their shape: 95% reads, half of them existing keys).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank owns an independent tree (key-range shard stand-in,
+weak scaling, no data-path collective); rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import datetime
+import json
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mops/s at 2^26 keys, 95% search; learned vs plain descent; p99 batch latency"
+BYTES_SEARCH = 288  # leaf keys (256 B) + one 32 B value sector
+BYTES_INSERT = 864  # search bytes + leaf rewrite (512 B) + version acquire/release (64 B)
+BYTES_SORT = 192  # 8 radix passes x (8 B key + 4 B index) x (read + write)
+FALLBACK_HBM_GBS = 6650.0
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"bt_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------
+def cpu_baseline(args, n_sample: int, threads: int):
+    """The oracle (CPU restatement of the reference path; the reference has no
+    CPU implementation) on a bounded sample of the same workload."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    t0 = time.time()
+    keys = O.gen_keys(args.dist, 1, 1 << args.tree_log2)
+    tree = O.OracleTree(24, 24)
+    tree.bulk_build(keys, O.value_of(keys))
+    build_s = time.time() - t0
+    rk, rv, ro = O.gen_requests(args.dist, 999, keys, n_sample, args.search_pct)
+    t1 = time.perf_counter()
+    tree.execute_merged(rk, rv, ro, O.ENGINE_STM, threads)
+    dt = time.perf_counter() - t1
+    del tree
+    return {"value": n_sample / dt / 1e6, "unit": "Mops/s", "cores": threads, "kind": "port",
+            "sample": f"{n_sample} requests ({args.search_pct}% search) of the bench workload against a "
+                      f"2^{args.tree_log2}-key tree, sort-merged batch semantics; tree build ({build_s:.1f} s) untimed"}
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU implementation of the path does not
+    exist (it is GPU-only), so the oracle port stands in for it, timed on the
+    host cores with all threads."""
+    rank = env_int("RANK", 0)
+    if rank != 0:
+        return 0
+    import numpy as np
+
+    from oracle import oracle as O
+
+    threads = os.cpu_count() or 1
+    keys = O.gen_keys(args.dist, 1, 1 << args.tree_log2)
+    tree = O.OracleTree(24, 24)
+    tree.bulk_build(keys, O.value_of(keys))
+    n_step = 1 << 18
+    batches = [O.gen_requests(args.dist, 5000 + i, keys, n_step, args.search_pct)
+               for i in range(args.warmup + args.steps)]
+    for i in range(args.warmup):
+        tree.execute_merged(*batches[i], O.ENGINE_STM, threads)
+    t0 = time.perf_counter()
+    for i in range(args.warmup, args.warmup + args.steps):
+        tree.execute_merged(*batches[i], O.ENGINE_STM, threads)
+    dt = time.perf_counter() - t0
+    val = n_step * args.steps / dt / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": "Mops/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": f"2^{args.tree_log2}-key tree, {args.search_pct}/{100 - args.search_pct} "
+                               f"search/insert, {args.dist} keys, sort-merged batches",
+                   "step_sample": n_step},
+        "cpu_baseline": {"value": val, "unit": "Mops/s", "cores": threads, "kind": "port",
+                         "sample": f"each step {n_step} requests of the bench workload (the reference has no "
+                                   "CPU path; the oracle restatement runs in its place)"},
+        "e2e": {"value": val, "unit": "Mops/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------
+def unique_op_counts(torch, k, o):
+    """(unique GET keys, unique INSERT keys) of a batch under the merged meaning."""
+    u, inv = torch.unique(k, return_inverse=True)
+    has_ins = torch.zeros(u.numel(), dtype=torch.int32, device=k.device)
+    has_ins.scatter_reduce_(0, inv, (o == 0).to(torch.int32), reduce="amax")
+    n_ins = int(has_ins.sum().item())
+    return u.numel() - n_ins, n_ins
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--tree-log2", type=int, default=26)
+    ap.add_argument("--batch-log2", type=int, default=22)
+    ap.add_argument("--search-pct", type=int, default=95)
+    ap.add_argument("--dist", default="uniform", choices=["uniform", "zipf", "normal", "gamma"])
+    ap.add_argument("--descent", default="both", choices=["plain", "learned", "both"])
+    ap.add_argument("--search-group", type=int, default=8)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-log2", type=int, default=20)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import numpy as np
+    import torch
+
+    import eirene_b200 as E
+
+    rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def allmax(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def allsum(x: int) -> int:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.int64, device="cuda")
+        dist.all_reduce(t)
+        return int(t.item())
+
+    n_tree = 1 << args.tree_log2
+    n_b = 1 << args.batch_log2
+    n_steps_total = args.warmup + args.steps
+    stream = torch.cuda.current_stream()
+    # ---- tree
+    tree = E.BTree(max_keys=2 * n_tree + 32 * n_b, max_batch=n_b, device=local, search_group=args.search_group)
+    tk = torch.empty(n_tree, dtype=torch.int64, device="cuda")
+    tv = torch.empty(n_tree, dtype=torch.int64, device="cuda")
+    E.gen_keys(args.dist, 1 + rank, n_tree, tk, tv, stream)
+    t0 = time.time()
+    tree.bulk_build(tk, tv, stream)
+    torch.cuda.synchronize()
+    build_s = time.time() - t0
+    del tv
+
+    # ---- batches: distinct, device resident (each step reads its own 2^22-request batch)
+    def make_batches(seed0):
+        out = []
+        for i in range(n_steps_total):
+            k = torch.empty(n_b, dtype=torch.int64, device="cuda")
+            v = torch.empty(n_b, dtype=torch.int64, device="cuda")
+            o = torch.empty(n_b, dtype=torch.uint8, device="cuda")
+            E.gen_requests(args.dist, seed0 + 1000 * rank + i, tk, n_b, args.search_pct, k, v, o, stream)
+            out.append((k, v, o))
+        torch.cuda.synchronize()
+        return out
+
+    ov = torch.empty(n_b, dtype=torch.int64, device="cuda")
+    ost = torch.empty(n_b, dtype=torch.uint8, device="cuda")
+
+    def run_form(learned: bool, seed0: int):
+        batches = make_batches(seed0)
+        counts = [unique_op_counts(torch, k, o) for (k, v, o) in batches[args.warmup:]]
+        if learned:
+            tree.retrain(stream)
+            tree.set_descent(True)
+        else:
+            tree.set_descent(False)
+        for i in range(args.warmup):
+            tree.execute(*batches[i], ov, ost, mode=E.MODE_SORTED, stream=stream)
+        tree.reset_stats()
+        tree.profile(True)
+        tree.profile_read(reset=True)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+        barrier()
+        sampler = ClockSampler(local)
+        sampler.start()
+        l0 = E.launch_count()
+        ev[0].record(stream)
+        for s in range(args.steps):
+            tree.execute(*batches[args.warmup + s], ov, ost, mode=E.MODE_SORTED, stream=stream)
+            ev[s + 1].record(stream)
+        torch.cuda.synchronize()
+        launches = E.launch_count() - l0
+        clocks = sampler.stop()
+        barrier()
+        step_ms = [ev[s].elapsed_time(ev[s + 1]) for s in range(args.steps)]
+        total_ms = ev[0].elapsed_time(ev[-1])
+        phases = tree.profile_read(reset=True)
+        tree.profile(False)
+        st = tree.stats()
+        del batches
+        return {"total_ms": total_ms, "step_ms": step_ms, "phases": phases, "counts": counts,
+                "launches": launches, "clocks": clocks, "stats": st}
+
+    forms = {}
+    if args.descent in ("plain", "both"):
+        forms["plain"] = run_form(False, 10_000)
+    if args.descent in ("learned", "both"):
+        try:
+            forms["learned"] = run_form(True, 20_000)
+        except E.BTError as e:
+            forms["learned_error"] = str(e)
+    head = "learned" if "learned" in forms else "plain"
+    R = forms[head]
+    total_ms = allmax(R["total_ms"])
+    value = world * n_b * args.steps / (total_ms / 1e3) / 1e6
+
+    # ---- roofline of the dominant phase
+    hbm, peak_kind = peaks()
+    steps = args.steps
+    ph = R["phases"]
+    n_get = sum(c[0] for c in R["counts"]) / steps
+    n_ins = sum(c[1] for c in R["counts"]) / steps
+    alg = {"sort": BYTES_SORT * n_b, "search": BYTES_SEARCH * n_get, "insert": BYTES_INSERT * n_ins}
+    dom = max(("sort", "merge", "search", "insert", "writeback"), key=lambda p: ph[p])
+    dom_ms = ph[dom] / max(1, ph["batches"])
+    dom_bytes = alg.get(dom)
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", f"traffic_{dom}.json")
+    if os.path.exists(tpath):
+        try:
+            t = json.load(open(tpath))
+            traffic = t.get("bytes_per_unit", 0) * (n_get if dom == "search" else n_ins if dom == "insert" else n_b)
+        except Exception:
+            traffic = None
+    roof = None
+    if dom_bytes:
+        ach = dom_bytes / (dom_ms / 1e3) / 1e9
+        roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                "peak_source": peak_kind, "traffic": traffic, "alg_bytes_per_launch": dom_bytes,
+                "launch_ms": dom_ms}
+
+    # ---- e2e through the host entry point (pinned host buffers, copies timed)
+    e2e = None
+    if True:
+        hb = []
+        for i in range(4):
+            k = torch.empty(n_b, dtype=torch.int64, device="cuda")
+            v = torch.empty(n_b, dtype=torch.int64, device="cuda")
+            o = torch.empty(n_b, dtype=torch.uint8, device="cuda")
+            E.gen_requests(args.dist, 30_000 + 1000 * rank + i, tk, n_b, args.search_pct, k, v, o, stream)
+            hb.append((k.cpu().pin_memory(), v.cpu().pin_memory(), o.cpu().pin_memory()))
+        hov = torch.empty(n_b, dtype=torch.int64).pin_memory()
+        hos = torch.empty(n_b, dtype=torch.uint8).pin_memory()
+        L = E.lib()
+        sp = stream.cuda_stream
+
+        def host_step(b):
+            k, v, o = b
+            rc = L.bt_execute_batch_host(tree._h, k.data_ptr(), v.data_ptr(), o.data_ptr(), hov.data_ptr(),
+                                         hos.data_ptr(), n_b, E.MODE_SORTED, sp)
+            if rc != 0:
+                raise E.BTError(rc, "bt_execute_batch_host")
+
+        host_step(hb[0])
+        e2e_steps = 3
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for s in range(e2e_steps):
+            host_step(hb[1 + s])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        e2e_ms = allmax(e0.elapsed_time(e1))
+        e2e = {"value": world * n_b * e2e_steps / (e2e_ms / 1e3) / 1e6, "unit": "Mops/s",
+               "h2d_bytes_per_step": n_b * 17, "d2h_bytes_per_step": n_b * 9,
+               "steps": e2e_steps, "descent": head}
+
+    launches = allsum(R["launches"])
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline(args, 1 << args.cpu_sample_log2, os.cpu_count() or 1)
+        except Exception as ex:  # reported, not fatal
+            cpu = {"error": str(ex)}
+
+    if rank == 0:
+        def form_summary(F):
+            ms = sorted(F["step_ms"])
+            tot = F["total_ms"]
+            s = F["stats"]
+            return {
+                "value": n_b * steps / (tot / 1e3) / 1e6, "ms_per_step": tot / steps,
+                "p50_batch_ms": ms[len(ms) // 2], "p99_batch_ms": ms[min(len(ms) - 1, int(0.99 * len(ms)))],
+                "phases_ms_per_step": {p: F["phases"][p] / max(1, F["phases"]["batches"])
+                                       for p in ("sort", "merge", "search", "insert", "writeback")},
+                "stm_aborts": s["aborts"], "stm_commits": s["commits"],
+                "learned_hits": s["learned_hits"], "learned_fallbacks": s["learned_fallbacks"],
+                "mean_probe": s["learned_probe_sum"] / max(1, s["learned_hits"]),
+            }
+
+        line = {
+            "metric": METRIC, "value": value, "unit": "Mops/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {
+                "workload": f"2^{args.tree_log2} {args.dist} uint64 keys per GPU, batches of 2^{args.batch_log2} "
+                            f"requests, {args.search_pct}% search / {100 - args.search_pct}% insert, "
+                            "sort-merged (v38 meaning)",
+                "descent": head, "tree_keys": n_tree, "batch": n_b, "search_group": args.search_group,
+                "l2": "inputs larger than L2: tree ~1.5 GB; every step reads its own 71 MB batch",
+                "parallelism": f"{world} independent tree(s), one per GPU",
+                "tree_build_s": build_s,
+            },
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "clocks": R["clocks"],
+            "gpu_launches": launches,
+            "p50_batch_ms": form_summary(R)["p50_batch_ms"],
+            "p99_batch_ms": form_summary(R)["p99_batch_ms"],
+            "forms": {k: form_summary(v) for k, v in forms.items() if isinstance(v, dict)},
+        }
+        if "learned_error" in forms:
+            line["learned_error"] = forms["learned_error"]
+        print(json.dumps(line), flush=True)
+    tree.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

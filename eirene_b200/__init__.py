@@ -1,0 +1,307 @@
+"""eirene_b200: B200 batched B+tree (Python front end over the C ABI).
+
+The compute path is libeirene_b200.so (hand-written sm_100a kernels behind the
+C ABI in include/eirene_b200.h).  This module only loads the library and
+passes device pointers (torch CUDA tensors) or host arrays through ctypes; it
+has no fallback: if the library or a GPU is missing, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libeirene_b200.so")
+
+BT_OK = 0
+ERRORS = {
+    -1: "invalid argument",
+    -2: "CUDA error",
+    -3: "out of memory",
+    -4: "node pool exhausted",
+    -5: "reserved key UINT64_MAX",
+    -6: "batch larger than max_batch",
+    -7: "learned predictor not trained",
+}
+OP_INSERT, OP_GET = 0, 1
+ST_ABSENT, ST_FOUND, ST_REJECTED, ST_RETRY_EXHAUSTED, ST_NO_CAPACITY = 0, 1, 2, 3, 4
+MODE_SORTED, MODE_STM, MODE_MERGE_ENGINE = 0, 1, 0x10
+DESCENT_PLAIN, DESCENT_LEARNED = 0, 1
+DIST = {"uniform": 0, "zipf": 1, "normal": 2, "gamma": 3}
+KEY_MAX = (1 << 64) - 1
+
+
+class BTError(RuntimeError):
+    def __init__(self, code: int, what: str = ""):
+        super().__init__(f"{what}: {ERRORS.get(code, code)} ({code})")
+        self.code = code
+
+
+class Config(ctypes.Structure):
+    _fields_ = [
+        ("max_keys", ctypes.c_uint64),
+        ("max_batch", ctypes.c_uint64),
+        ("leaf_fill", ctypes.c_uint32),
+        ("inner_fill", ctypes.c_uint32),
+        ("retry_limit", ctypes.c_uint32),
+        ("device", ctypes.c_int32),
+        ("search_group", ctypes.c_uint32),
+        ("n_segments", ctypes.c_uint32),
+        ("window", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 7),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("n_keys", ctypes.c_uint64),
+        ("n_nodes", ctypes.c_uint64),
+        ("n_leaves", ctypes.c_uint64),
+        ("height", ctypes.c_uint32),
+        ("error", ctypes.c_uint32),
+        ("commits", ctypes.c_uint64),
+        ("aborts", ctypes.c_uint64),
+        ("leaf_splits", ctypes.c_uint64),
+        ("inner_splits", ctypes.c_uint64),
+        ("new_roots", ctypes.c_uint64),
+        ("retry_exhausted", ctypes.c_uint64),
+        ("learned_hits", ctypes.c_uint64),
+        ("learned_fallbacks", ctypes.c_uint64),
+        ("learned_probe_sum", ctypes.c_uint64),
+        ("capacity_nodes", ctypes.c_uint64),
+    ]
+
+
+# every symbol the C header declares (checked by the CPU tests)
+EXPORTS = [
+    "bt_config_init", "bt_create", "bt_destroy", "bt_bulk_build", "bt_execute_batch", "bt_execute_batch_host",
+    "bt_search_batch", "bt_insert_batch", "bt_size", "bt_dump_sorted", "bt_leaf_sizes", "bt_level_counts",
+    "bt_stats_get", "bt_stats_reset", "bt_retrain", "bt_set_descent", "bt_set_root_model", "bt_set_search_group",
+    "bt_host_alloc", "bt_host_free", "bt_gen_keys", "bt_gen_requests", "bt_status_string",
+    "bt_profile", "bt_profile_read", "bt_launch_count",
+]
+PHASES = ["sort", "merge", "search", "insert", "writeback"]
+
+_lib = None
+_P = ctypes.c_void_p
+_SZ = ctypes.c_size_t
+
+
+def build(force: bool = False) -> str:
+    """Compile libeirene_b200.so in place (nvcc, sm_100a)."""
+    import importlib
+
+    return importlib.import_module(__name__ + ".build").build(force=force)
+
+
+def lib():
+    """Load libeirene_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run `python -m eirene_b200.build` (needs nvcc)")
+        L = ctypes.CDLL(LIB_PATH)
+        sig = {
+            "bt_config_init": [ctypes.POINTER(Config)],
+            "bt_create": [ctypes.POINTER(Config), ctypes.POINTER(_P)],
+            "bt_destroy": [_P],
+            "bt_bulk_build": [_P, _P, _P, _SZ, _P],
+            "bt_execute_batch": [_P, _P, _P, _P, _P, _P, _SZ, ctypes.c_int, _P],
+            "bt_execute_batch_host": [_P, _P, _P, _P, _P, _P, _SZ, ctypes.c_int, _P],
+            "bt_search_batch": [_P, _P, _P, _P, _SZ, _P],
+            "bt_insert_batch": [_P, _P, _P, _P, _P, _SZ, _P],
+            "bt_size": [_P, ctypes.POINTER(ctypes.c_uint64)],
+            "bt_dump_sorted": [_P, _P, _P, _SZ, ctypes.POINTER(_SZ), _P],
+            "bt_leaf_sizes": [_P, _P, _SZ, ctypes.POINTER(_SZ)],
+            "bt_level_counts": [_P, _P, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)],
+            "bt_stats_get": [_P, ctypes.POINTER(Stats), ctypes.c_int],
+            "bt_stats_reset": [_P],
+            "bt_retrain": [_P, _P],
+            "bt_set_descent": [_P, ctypes.c_int],
+            "bt_set_root_model": [_P, ctypes.c_int],
+            "bt_set_search_group": [_P, ctypes.c_uint32],
+            "bt_host_alloc": [ctypes.POINTER(_P), _SZ],
+            "bt_host_free": [_P],
+            "bt_gen_keys": [ctypes.c_int, ctypes.c_uint64, _SZ, _P, _P, _P],
+            "bt_gen_requests": [ctypes.c_int, ctypes.c_uint64, _P, _SZ, _SZ, ctypes.c_uint32, _P, _P, _P, _P],
+            "bt_status_string": [ctypes.c_int],
+            "bt_profile": [_P, ctypes.c_int],
+            "bt_profile_read": [_P, _P, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int],
+            "bt_launch_count": [],
+        }
+        for name, args in sig.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = ctypes.c_int
+        L.bt_status_string.restype = ctypes.c_char_p
+        L.bt_launch_count.restype = ctypes.c_uint64
+        _lib = L
+    return _lib
+
+
+def _check(rc: int, what: str):
+    if rc != BT_OK:
+        raise BTError(rc, what)
+
+
+def _ptr(t) -> int:
+    """Device pointer of a torch tensor (or an int already)."""
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return t
+    return t.data_ptr()
+
+
+def _stream_ptr(stream) -> int | None:
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+class BTree:
+    """One device-resident B+tree (one bt_handle)."""
+
+    def __init__(self, max_keys: int = 1 << 20, max_batch: int = 1 << 22, leaf_fill: int = 24,
+                 inner_fill: int = 24, device: int = 0, search_group: int = 8, retry_limit: int = 0,
+                 n_segments: int = 4096, window: int = 64):
+        L = lib()
+        cfg = Config()
+        _check(L.bt_config_init(ctypes.byref(cfg)), "bt_config_init")
+        cfg.max_keys = max_keys
+        cfg.max_batch = max_batch
+        cfg.leaf_fill = leaf_fill
+        cfg.inner_fill = inner_fill
+        cfg.device = device
+        cfg.search_group = search_group
+        if retry_limit:
+            cfg.retry_limit = retry_limit
+        cfg.n_segments = n_segments
+        cfg.window = window
+        h = _P()
+        _check(L.bt_create(ctypes.byref(cfg), ctypes.byref(h)), "bt_create")
+        self._h = h
+        self.device = device
+        self.max_batch = max_batch
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().bt_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --- device-pointer API (torch CUDA tensors of dtype uint64 / uint8) ---
+    def bulk_build(self, keys, vals, stream=None):
+        n = keys.numel()
+        _check(lib().bt_bulk_build(self._h, _ptr(keys), _ptr(vals), n, _stream_ptr(stream)), "bt_bulk_build")
+
+    def execute(self, keys, vals, ops, out_vals, out_status, mode=MODE_SORTED, stream=None):
+        n = keys.numel()
+        _check(lib().bt_execute_batch(self._h, _ptr(keys), _ptr(vals), _ptr(ops), _ptr(out_vals), _ptr(out_status),
+                                      n, mode, _stream_ptr(stream)), "bt_execute_batch")
+
+    def search(self, keys, out_vals, out_status, stream=None):
+        _check(lib().bt_search_batch(self._h, _ptr(keys), _ptr(out_vals), _ptr(out_status), keys.numel(),
+                                     _stream_ptr(stream)), "bt_search_batch")
+
+    def insert(self, keys, vals, out_vals, out_status, stream=None):
+        _check(lib().bt_insert_batch(self._h, _ptr(keys), _ptr(vals), _ptr(out_vals), _ptr(out_status),
+                                     keys.numel(), _stream_ptr(stream)), "bt_insert_batch")
+
+    # --- host-buffer API (numpy arrays) ---
+    def execute_host(self, keys: np.ndarray, vals: np.ndarray, ops: np.ndarray, mode=MODE_SORTED, stream=None,
+                     out_vals: np.ndarray | None = None, out_status: np.ndarray | None = None):
+        keys = np.ascontiguousarray(keys, dtype=np.uint64)
+        vals = np.ascontiguousarray(vals, dtype=np.uint64)
+        ops = np.ascontiguousarray(ops, dtype=np.uint8)
+        n = keys.size
+        if out_vals is None:
+            out_vals = np.zeros(n, np.uint64)
+        if out_status is None:
+            out_status = np.zeros(n, np.uint8)
+        _check(lib().bt_execute_batch_host(self._h, keys.ctypes.data, vals.ctypes.data, ops.ctypes.data,
+                                           out_vals.ctypes.data, out_status.ctypes.data, n, mode,
+                                           _stream_ptr(stream)), "bt_execute_batch_host")
+        return out_vals, out_status
+
+    def size(self) -> int:
+        v = ctypes.c_uint64(0)
+        _check(lib().bt_size(self._h, ctypes.byref(v)), "bt_size")
+        return v.value
+
+    def dump(self):
+        """Sorted (keys, vals) as int64 torch CUDA tensors holding the uint64 bit patterns."""
+        import torch
+
+        n = self.size()
+        k = torch.empty(max(n, 1), dtype=torch.int64, device=f"cuda:{self.device}")
+        v = torch.empty(max(n, 1), dtype=torch.int64, device=f"cuda:{self.device}")
+        got = _SZ(0)
+        _check(lib().bt_dump_sorted(self._h, _ptr(k), _ptr(v), k.numel(), ctypes.byref(got), None), "bt_dump_sorted")
+        return k[: got.value], v[: got.value]
+
+    def leaf_sizes(self) -> np.ndarray:
+        n = _SZ(0)
+        _check(lib().bt_leaf_sizes(self._h, None, 0, ctypes.byref(n)), "bt_leaf_sizes")
+        out = np.zeros(n.value, np.uint32)
+        if n.value:
+            _check(lib().bt_leaf_sizes(self._h, out.ctypes.data, n.value, ctypes.byref(n)), "bt_leaf_sizes")
+        return out
+
+    def level_counts(self) -> np.ndarray:
+        c = np.zeros(48, np.uint64)
+        h = ctypes.c_uint32(0)
+        _check(lib().bt_level_counts(self._h, c.ctypes.data, 48, ctypes.byref(h)), "bt_level_counts")
+        return c[: h.value]
+
+    def stats(self, with_leaves: bool = False) -> dict:
+        s = Stats()
+        _check(lib().bt_stats_get(self._h, ctypes.byref(s), 1 if with_leaves else 0), "bt_stats_get")
+        return {f: getattr(s, f) for f, _ in Stats._fields_}
+
+    def reset_stats(self):
+        _check(lib().bt_stats_reset(self._h), "bt_stats_reset")
+
+    def retrain(self, stream=None):
+        _check(lib().bt_retrain(self._h, _stream_ptr(stream)), "bt_retrain")
+
+    def set_descent(self, learned: bool):
+        _check(lib().bt_set_descent(self._h, DESCENT_LEARNED if learned else DESCENT_PLAIN), "bt_set_descent")
+
+    def set_root_model(self, mlp: bool):
+        _check(lib().bt_set_root_model(self._h, 1 if mlp else 0), "bt_set_root_model")
+
+    def profile(self, enable: bool = True):
+        _check(lib().bt_profile(self._h, 1 if enable else 0), "bt_profile")
+
+    def profile_read(self, reset: bool = True) -> dict:
+        ms = (ctypes.c_double * 5)()
+        b = ctypes.c_uint64(0)
+        _check(lib().bt_profile_read(self._h, ms, ctypes.byref(b), 1 if reset else 0), "bt_profile_read")
+        return {"batches": b.value, **{p: ms[i] for i, p in enumerate(PHASES)}}
+
+    def set_search_group(self, lanes: int):
+        _check(lib().bt_set_search_group(self._h, lanes), "bt_set_search_group")
+
+
+def launch_count() -> int:
+    return lib().bt_launch_count()
+
+
+def gen_keys(dist: str, seed: int, n: int, keys, vals=None, stream=None):
+    _check(lib().bt_gen_keys(DIST[dist], seed, n, _ptr(keys), _ptr(vals), _stream_ptr(stream)), "bt_gen_keys")
+
+
+def gen_requests(dist: str, seed: int, tree_keys, n: int, search_pct: int, keys, vals, ops, stream=None):
+    nt = 0 if tree_keys is None else tree_keys.numel()
+    _check(lib().bt_gen_requests(DIST[dist], seed, _ptr(tree_keys), nt, n, search_pct, _ptr(keys), _ptr(vals),
+                                 _ptr(ops), _stream_ptr(stream)), "bt_gen_requests")

@@ -1,0 +1,419 @@
+// C ABI of libeirene_b200 (declared in include/eirene_b200.h).
+#include <cstdlib>
+#include <cstring>
+#include <new>
+
+#include <cuda_runtime.h>
+
+#include "../../include/eirene_b200.h"
+#include "bt_common.cuh"
+#include "bt_internal.h"
+
+struct bt_handle {
+  bt::Handle h;
+};
+
+namespace {
+
+// Make h's device current for the duration of a call; restore on exit.
+struct DeviceGuard {
+  int prev = -1;
+  bool ok = true;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) ok = cudaSetDevice(dev) == cudaSuccess;
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+int map_internal(int rc) {
+  switch (rc) {
+    case 0: return BT_OK;
+    case -1: return BT_ERR_INVALID_ARG;
+    case -2: return BT_ERR_CUDA;
+    case -3: return BT_ERR_NO_MEMORY;
+    case -4: return BT_ERR_CAPACITY;
+    case -5: return BT_ERR_RESERVED_KEY;
+    case -6: return BT_ERR_BATCH_TOO_LARGE;
+    case -7: return BT_ERR_NOT_TRAINED;
+    default: return BT_ERR_CUDA;
+  }
+}
+
+// node pool size for max_keys: every node holds at least 15 keys except the
+// few rightmost/root nodes, so 2*max_keys/15 + slack bounds the count for
+// any insert order; the bulk layout needs far fewer.
+uint64_t pool_nodes(uint64_t max_keys) { return max_keys / 7 + 4096; }
+
+}  // namespace
+
+namespace bt {
+cudaError_t sort_prepare();
+std::atomic<unsigned long long> g_launches{0};
+
+void prof_mark(Handle* h, int which, cudaStream_t s) {
+  if (!h->prof) return;
+  const size_t base = h->prof_batches * (kNumPhases + 1);
+  if (which == 0) {
+    // grow the event pool by one batch
+    while (h->prof_ev.size() < base + kNumPhases + 1) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) return;
+      h->prof_ev.push_back(e);
+    }
+  }
+  if (base + which < h->prof_ev.size()) cudaEventRecord(h->prof_ev[base + which], s);
+  if (which == kNumPhases) h->prof_batches++;
+}
+}  // namespace bt
+
+namespace {
+// fold recorded batches into phase_ms (synchronises on the events)
+int prof_resolve(bt::Handle& h) {
+  for (size_t b = 0; b < h.prof_batches; b++) {
+    cudaEvent_t* e = &h.prof_ev[b * (bt::kNumPhases + 1)];
+    if (cudaEventSynchronize(e[bt::kNumPhases]) != cudaSuccess) return BT_ERR_CUDA;
+    for (int p = 0; p < bt::kNumPhases; p++) {
+      float ms = 0;
+      if (cudaEventElapsedTime(&ms, e[p], e[p + 1]) != cudaSuccess) return BT_ERR_CUDA;
+      h.phase_ms[p] += ms;
+    }
+    h.phase_batches++;
+  }
+  h.prof_batches = 0;
+  return BT_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int bt_config_init(bt_config* c) {
+  if (!c) return BT_ERR_INVALID_ARG;
+  std::memset(c, 0, sizeof(*c));
+  c->max_keys = 1ull << 20;
+  c->max_batch = 1ull << 22;
+  c->leaf_fill = 24;
+  c->inner_fill = 24;
+  c->retry_limit = 1u << 16;
+  c->device = 0;
+  c->search_group = 8;
+  c->n_segments = 4096;
+  c->window = 64;
+  return BT_OK;
+}
+
+int bt_create(const bt_config* cfg_in, bt_handle** out) {
+  if (!out) return BT_ERR_INVALID_ARG;
+  *out = nullptr;
+  bt_config cfg;
+  if (cfg_in) cfg = *cfg_in;
+  else bt_config_init(&cfg);
+  if (cfg.leaf_fill < 2 || cfg.leaf_fill > 31 || cfg.inner_fill < 1 || cfg.inner_fill > 31) return BT_ERR_INVALID_ARG;
+  if (cfg.search_group != 4 && cfg.search_group != 8 && cfg.search_group != 16 && cfg.search_group != 32)
+    return BT_ERR_INVALID_ARG;
+  if (cfg.max_batch == 0 || cfg.max_batch > (1ull << 30)) return BT_ERR_INVALID_ARG;
+  const uint64_t nodes = pool_nodes(cfg.max_keys);
+  if (nodes >= 0xFFFFFFF0ull) return BT_ERR_INVALID_ARG;
+  int n_dev = 0;
+  if (cudaGetDeviceCount(&n_dev) != cudaSuccess || cfg.device < 0 || cfg.device >= n_dev) return BT_ERR_CUDA;
+  DeviceGuard g(cfg.device);
+  if (!g.ok) return BT_ERR_CUDA;
+  bt_handle* H = new (std::nothrow) bt_handle();
+  if (!H) return BT_ERR_NO_MEMORY;
+  bt::Handle& h = H->h;
+  h.device = cfg.device;
+  h.leaf_fill = cfg.leaf_fill;
+  h.inner_fill = cfg.inner_fill;
+  h.retry_limit = cfg.retry_limit ? cfg.retry_limit : (1u << 16);
+  h.search_group = (int)cfg.search_group;
+  h.L.n_segments = cfg.n_segments ? cfg.n_segments : 4096;
+  h.L.window = cfg.window ? cfg.window : 64;
+  cudaDeviceGetAttribute(&h.sm_count, cudaDevAttrMultiProcessorCount, cfg.device);
+  bool ok = bt::sort_prepare() == cudaSuccess;
+  h.tree.cap = (uint32_t)nodes;
+  ok = ok && cudaMalloc(&h.tree.keys, nodes * 256) == cudaSuccess;
+  ok = ok && cudaMalloc(&h.tree.vals, nodes * 256) == cudaSuccess;
+  ok = ok && cudaMalloc(&h.tree.low, nodes * 8) == cudaSuccess;
+  ok = ok && cudaMalloc(&h.tree.ctrl, sizeof(bt::Ctrl)) == cudaSuccess;
+  ok = ok && bt::work_alloc(&h.w, cfg.max_batch) == 0;
+  ok = ok && cudaStreamCreateWithFlags(&h.internal_stream, cudaStreamNonBlocking) == cudaSuccess;
+  ok = ok && bt::tree_reset(&h, h.internal_stream) == cudaSuccess;
+  ok = ok && cudaStreamSynchronize(h.internal_stream) == cudaSuccess;
+  if (!ok) {
+    bt_destroy(H);
+    return BT_ERR_NO_MEMORY;
+  }
+  *out = H;
+  return BT_OK;
+}
+
+int bt_destroy(bt_handle* H) {
+  if (!H) return BT_ERR_INVALID_ARG;
+  DeviceGuard g(H->h.device);
+  bt::Handle& h = H->h;
+  cudaDeviceSynchronize();
+  cudaFree(h.tree.keys);
+  cudaFree(h.tree.vals);
+  cudaFree(h.tree.low);
+  cudaFree(h.tree.ctrl);
+  bt::work_free(&h.w);
+  bt::learned_free(&h.L);
+  cudaFree(h.enum_a);
+  cudaFree(h.enum_b);
+  cudaFree(h.enum_cnt);
+  cudaFree(h.enum_scan_scratch);
+  if (h.internal_stream) cudaStreamDestroy(h.internal_stream);
+  for (cudaEvent_t e : h.prof_ev) cudaEventDestroy(e);
+  delete H;
+  return BT_OK;
+}
+
+int bt_bulk_build(bt_handle* H, const uint64_t* keys, const uint64_t* vals, size_t n, void* stream) {
+  if (!H || (n && (!keys || !vals))) return BT_ERR_INVALID_ARG;
+  DeviceGuard g(H->h.device);
+  H->h.L.valid = false;
+  return map_internal(bt::tree_bulk_build(&H->h, keys, vals, n, S(stream)));
+}
+
+int bt_execute_batch(bt_handle* H, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops,
+                     uint64_t* out_vals, uint8_t* out_status, size_t n, int mode, void* stream) {
+  if (!H) return BT_ERR_INVALID_ARG;
+  if (n == 0) return BT_OK;
+  if (!keys || !ops || !out_vals || !out_status || !vals) return BT_ERR_INVALID_ARG;
+  bt::Handle& h = H->h;
+  if (n > h.w.cap) return BT_ERR_BATCH_TOO_LARGE;
+  DeviceGuard g(h.device);
+  const int base = mode & 0xF;
+  if (base == BT_MODE_STM) {
+    cudaError_t e = bt::launch_stm(&h, keys, vals, ops, 0xFF, nullptr, nullptr, n, out_vals, out_status, S(stream));
+    return e == cudaSuccess ? BT_OK : BT_ERR_CUDA;
+  }
+  if (base != BT_MODE_SORTED) return BT_ERR_INVALID_ARG;
+  const int engine = (mode & BT_MODE_MERGE_ENGINE) ? 1 : 0;
+  return map_internal(bt::batch_sorted(&h, keys, vals, ops, out_vals, out_status, n, engine, S(stream)));
+}
+
+int bt_execute_batch_host(bt_handle* H, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops,
+                          uint64_t* out_vals, uint8_t* out_status, size_t n, int mode, void* stream) {
+  if (!H) return BT_ERR_INVALID_ARG;
+  if (n == 0) return BT_OK;
+  if (!keys || !ops || !out_vals || !out_status || !vals) return BT_ERR_INVALID_ARG;
+  bt::Handle& h = H->h;
+  if (n > h.w.cap) return BT_ERR_BATCH_TOO_LARGE;
+  DeviceGuard g(h.device);
+  cudaStream_t s = S(stream);
+  bt::Work& w = h.w;
+  if (cudaMemcpyAsync(w.d_in_keys, keys, n * 8, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(w.d_in_vals, vals, n * 8, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(w.d_in_ops, ops, n, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return BT_ERR_CUDA;
+  int rc = bt_execute_batch(H, w.d_in_keys, w.d_in_vals, w.d_in_ops, w.d_out_vals, w.d_out_st, n, mode, stream);
+  if (rc != BT_OK) return rc;
+  if (cudaMemcpyAsync(out_vals, w.d_out_vals, n * 8, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaMemcpyAsync(out_status, w.d_out_st, n, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    return BT_ERR_CUDA;
+  return cudaStreamSynchronize(s) == cudaSuccess ? BT_OK : BT_ERR_CUDA;
+}
+
+int bt_search_batch(bt_handle* H, const uint64_t* keys, uint64_t* out_vals, uint8_t* out_status, size_t n,
+                    void* stream) {
+  if (!H) return BT_ERR_INVALID_ARG;
+  if (n == 0) return BT_OK;
+  if (!keys || !out_vals || !out_status) return BT_ERR_INVALID_ARG;
+  bt::Handle& h = H->h;
+  DeviceGuard g(h.device);
+  // searches alone never conflict: run the search kernel directly on the batch
+  cudaError_t e;
+  if (h.descent == BT_DESCENT_LEARNED && h.L.valid)
+    e = bt::launch_learned_search(&h, keys, nullptr, nullptr, n, out_vals, out_status, S(stream));
+  else
+    e = bt::launch_search(&h, keys, nullptr, nullptr, n, out_vals, out_status, S(stream));
+  return e == cudaSuccess ? BT_OK : BT_ERR_CUDA;
+}
+
+int bt_insert_batch(bt_handle* H, const uint64_t* keys, const uint64_t* vals, uint64_t* out_vals,
+                    uint8_t* out_status, size_t n, void* stream) {
+  if (!H) return BT_ERR_INVALID_ARG;
+  if (n == 0) return BT_OK;
+  if (!keys || !vals || !out_vals || !out_status) return BT_ERR_INVALID_ARG;
+  bt::Handle& h = H->h;
+  if (n > h.w.cap) return BT_ERR_BATCH_TOO_LARGE;
+  DeviceGuard g(h.device);
+  // an all-insert op array in the staging buffer
+  if (cudaMemsetAsync(h.w.d_in_ops, BT_OP_INSERT, n, S(stream)) != cudaSuccess) return BT_ERR_CUDA;
+  return map_internal(bt::batch_sorted(&h, keys, vals, h.w.d_in_ops, out_vals, out_status, n, 0, S(stream)));
+}
+
+int bt_size(bt_handle* H, uint64_t* n_keys) {
+  if (!H || !n_keys) return BT_ERR_INVALID_ARG;
+  DeviceGuard g(H->h.device);
+  bt::Ctrl c;
+  if (cudaMemcpy(&c, H->h.tree.ctrl, sizeof(c), cudaMemcpyDeviceToHost) != cudaSuccess) return BT_ERR_CUDA;
+  *n_keys = c.n_keys;
+  return BT_OK;
+}
+
+int bt_dump_sorted(bt_handle* H, uint64_t* keys, uint64_t* vals, size_t cap, size_t* n_out, void* stream) {
+  if (!H || !n_out) return BT_ERR_INVALID_ARG;
+  DeviceGuard g(H->h.device);
+  cudaStream_t s = stream ? S(stream) : H->h.internal_stream;
+  if (stream == nullptr) cudaDeviceSynchronize();
+  return map_internal(bt::tree_dump(&H->h, keys, vals, cap, n_out, s));
+}
+
+int bt_leaf_sizes(bt_handle* H, uint32_t* sizes_host, size_t cap, size_t* n_leaves) {
+  if (!H || !n_leaves) return BT_ERR_INVALID_ARG;
+  DeviceGuard g(H->h.device);
+  cudaDeviceSynchronize();
+  bt::Handle& h = H->h;
+  uint32_t* leaves = nullptr;
+  size_t nl = 0;
+  int rc = bt::enumerate_leaves(&h, h.internal_stream, &leaves, &nl);
+  if (rc) return map_internal(rc);
+  *n_leaves = nl;
+  if (!sizes_host || nl == 0) return BT_OK;
+  uint32_t* sizes = (leaves == h.enum_a) ? h.enum_b : h.enum_a;
+  if (bt::leaf_sizes_device(&h, leaves, nl, sizes, h.internal_stream) != cudaSuccess) return BT_ERR_CUDA;
+  const size_t m = nl < cap ? nl : cap;
+  if (cudaMemcpyAsync(sizes_host, sizes, m * 4, cudaMemcpyDeviceToHost, h.internal_stream) != cudaSuccess)
+    return BT_ERR_CUDA;
+  return cudaStreamSynchronize(h.internal_stream) == cudaSuccess ? BT_OK : BT_ERR_CUDA;
+}
+
+int bt_level_counts(bt_handle* H, uint64_t* counts_host, uint32_t cap, uint32_t* height) {
+  if (!H || !height) return BT_ERR_INVALID_ARG;
+  DeviceGuard g(H->h.device);
+  cudaDeviceSynchronize();
+  uint32_t* leaves = nullptr;
+  size_t nl = 0;
+  int rc = bt::enumerate_leaves(&H->h, H->h.internal_stream, &leaves, &nl);
+  if (rc) return map_internal(rc);
+  *height = H->h.n_levels;
+  if (counts_host)
+    for (uint32_t i = 0; i < cap; i++) counts_host[i] = (i < H->h.n_levels && i < 48) ? H->h.level_counts[i] : 0;
+  return BT_OK;
+}
+
+int bt_stats_get(bt_handle* H, bt_stats* st, int with_leaves) {
+  if (!H || !st) return BT_ERR_INVALID_ARG;
+  DeviceGuard g(H->h.device);
+  cudaDeviceSynchronize();
+  bt::Ctrl c;
+  if (cudaMemcpy(&c, H->h.tree.ctrl, sizeof(c), cudaMemcpyDeviceToHost) != cudaSuccess) return BT_ERR_CUDA;
+  std::memset(st, 0, sizeof(*st));
+  st->n_keys = c.n_keys;
+  st->n_nodes = c.n_nodes < H->h.tree.cap ? c.n_nodes : H->h.tree.cap;
+  st->height = c.root == bt::kNil ? 0 : c.root_level + 1;
+  st->error = c.error;
+  st->commits = c.commits;
+  st->aborts = c.aborts;
+  st->leaf_splits = c.leaf_splits;
+  st->inner_splits = c.inner_splits;
+  st->new_roots = c.new_roots;
+  st->retry_exhausted = c.retry_exhausted;
+  st->learned_hits = c.learned_hits;
+  st->learned_fallbacks = c.learned_fallbacks;
+  st->learned_probe_sum = c.learned_probe_sum;
+  st->capacity_nodes = H->h.tree.cap;
+  if (with_leaves) {
+    uint32_t* leaves = nullptr;
+    size_t nl = 0;
+    int rc = bt::enumerate_leaves(&H->h, H->h.internal_stream, &leaves, &nl);
+    if (rc) return map_internal(rc);
+    st->n_leaves = nl;
+  }
+  return BT_OK;
+}
+
+int bt_stats_reset(bt_handle* H) {
+  if (!H) return BT_ERR_INVALID_ARG;
+  DeviceGuard g(H->h.device);
+  cudaDeviceSynchronize();
+  bt::Ctrl c;
+  if (cudaMemcpy(&c, H->h.tree.ctrl, sizeof(c), cudaMemcpyDeviceToHost) != cudaSuccess) return BT_ERR_CUDA;
+  c.commits = c.aborts = c.leaf_splits = c.inner_splits = c.new_roots = c.retry_exhausted = 0;
+  c.learned_hits = c.learned_fallbacks = c.learned_probe_sum = 0;
+  c.error = 0;
+  return cudaMemcpy(H->h.tree.ctrl, &c, sizeof(c), cudaMemcpyHostToDevice) == cudaSuccess ? BT_OK : BT_ERR_CUDA;
+}
+
+int bt_retrain(bt_handle* H, void* stream) {
+  if (!H) return BT_ERR_INVALID_ARG;
+  DeviceGuard g(H->h.device);
+  cudaStream_t s = stream ? S(stream) : H->h.internal_stream;
+  if (stream == nullptr) cudaDeviceSynchronize();
+  return map_internal(bt::learned_retrain(&H->h, s));
+}
+
+int bt_set_descent(bt_handle* H, int descent) {
+  if (!H || (descent != BT_DESCENT_PLAIN && descent != BT_DESCENT_LEARNED)) return BT_ERR_INVALID_ARG;
+  if (descent == BT_DESCENT_LEARNED && !H->h.L.valid) return BT_ERR_NOT_TRAINED;
+  H->h.descent = descent;
+  return BT_OK;
+}
+
+int bt_set_root_model(bt_handle* H, int mlp) {
+  if (!H) return BT_ERR_INVALID_ARG;
+  H->h.L.stage1 = mlp ? 1 : 0;
+  return BT_OK;
+}
+
+int bt_set_search_group(bt_handle* H, uint32_t lanes) {
+  if (!H) return BT_ERR_INVALID_ARG;
+  if (lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32) return BT_ERR_INVALID_ARG;
+  H->h.search_group = (int)lanes;
+  return BT_OK;
+}
+
+int bt_profile(bt_handle* H, int enable) {
+  if (!H) return BT_ERR_INVALID_ARG;
+  DeviceGuard g(H->h.device);
+  int rc = prof_resolve(H->h);
+  H->h.prof = enable != 0;
+  return rc;
+}
+
+int bt_profile_read(bt_handle* H, double* phase_ms, uint64_t* batches, int reset) {
+  if (!H) return BT_ERR_INVALID_ARG;
+  DeviceGuard g(H->h.device);
+  int rc = prof_resolve(H->h);
+  if (rc != BT_OK) return rc;
+  if (phase_ms)
+    for (int p = 0; p < bt::kNumPhases; p++) phase_ms[p] = H->h.phase_ms[p];
+  if (batches) *batches = H->h.phase_batches;
+  if (reset) {
+    for (int p = 0; p < bt::kNumPhases; p++) H->h.phase_ms[p] = 0;
+    H->h.phase_batches = 0;
+  }
+  return BT_OK;
+}
+
+uint64_t bt_launch_count(void) { return bt::g_launches.load(); }
+
+int bt_host_alloc(void** p, size_t bytes) {
+  if (!p) return BT_ERR_INVALID_ARG;
+  return cudaMallocHost(p, bytes ? bytes : 1) == cudaSuccess ? BT_OK : BT_ERR_NO_MEMORY;
+}
+
+int bt_host_free(void* p) { return cudaFreeHost(p) == cudaSuccess ? BT_OK : BT_ERR_CUDA; }
+
+const char* bt_status_string(int code) {
+  switch (code) {
+    case BT_OK: return "ok";
+    case BT_ERR_INVALID_ARG: return "invalid argument";
+    case BT_ERR_CUDA: return "CUDA error";
+    case BT_ERR_NO_MEMORY: return "out of memory";
+    case BT_ERR_CAPACITY: return "node pool exhausted";
+    case BT_ERR_RESERVED_KEY: return "reserved key UINT64_MAX";
+    case BT_ERR_BATCH_TOO_LARGE: return "batch larger than max_batch";
+    case BT_ERR_NOT_TRAINED: return "learned predictor not trained";
+    default: return "unknown status";
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,395 @@
+// Sort-based batch merge (the reference's v38 front end and back end,
+// src/gpu-stm-tree-v38/bpt-gpustm-kernel.cu:289-332 and
+// src/gpu-stm-tree-v38/bpt-gpustm-kernel-aux.cuh:16-56), restated for B200:
+//
+//   sort (key, idx|op)        hand-written radix sort (bt_sort.cu)
+//   tile pass 1 / 2 / 3       one segmented scan over the sorted requests
+//                             replaces RunLengthEncode + ExclusiveSum +
+//                             mergeMission; it is parallel per request, so a
+//                             Zipf-hot key with 10^5 repeats costs no more than
+//                             10^5 distinct keys (mergeMission walks each run
+//                             with one thread).
+//   search phase              lock-free grouped search over the unique GETs
+//   insert phase              STM kernel over the unique INSERTs
+//   writeback                 scatter answers to request order
+//
+// Meaning (identical to v38): within a run of equal keys in input order a
+// request sees the pre-batch value until the first INSERT, then the value of
+// the latest INSERT before it; the run reaches the tree as one INSERT (last
+// value) or one GET.  The unique count never leaves the device (the reference
+// copies it to the host and synchronises, v38 bpt-gpustm-kernel.cu:303-306).
+#include <cuda_runtime.h>
+
+#include "bt_block.cuh"
+#include "bt_common.cuh"
+#include "bt_internal.h"
+
+namespace bt {
+
+struct TileSummary {
+  uint64_t agg_v;
+  uint64_t pre_v;
+  uint64_t carry_v;
+  uint32_t agg_f;
+  uint32_t pre_f;
+  uint32_t carry_f;
+  uint32_t heads;
+  uint32_t cont;  // bit0: tile holds the tail of a run begun in an earlier tile; bit1: that key is reserved
+  uint32_t ins_local;
+  uint32_t get_local;
+  uint32_t heads_before;
+  uint32_t ins_before;
+  uint32_t get_before;
+};
+
+namespace {
+
+constexpr int kThreads = 512;
+constexpr int kItems = 8;
+constexpr int kTile = kThreads * kItems;  // matches the sort tile
+constexpr uint32_t kIdxMask = 0x3FFFFFFFu;
+constexpr uint32_t kResolved = 0xFFFFFFFFu;
+
+struct Item {
+  uint64_t k;
+  uint32_t r;
+  uint32_t op;
+  bool head, tail, valid, ins;
+};
+
+__device__ __forceinline__ void load_items(const uint64_t* __restrict__ sk, const uint32_t* __restrict__ sv,
+                                           size_t n, size_t i0, Item (&it)[kItems]) {
+  uint64_t prev = (i0 > 0 && i0 - 1 < n) ? sk[i0 - 1] : 0;
+#pragma unroll
+  for (int j = 0; j < kItems; j++) {
+    const size_t i = i0 + j;
+    it[j].valid = i < n;
+    if (i < n) {
+      it[j].k = sk[i];
+      const uint32_t p = sv[i];
+      it[j].r = p & kIdxMask;
+      it[j].op = p >> 30;
+      it[j].head = (i == 0) || (prev != it[j].k);
+      prev = it[j].k;
+    } else {
+      it[j].k = 0;
+      it[j].r = 0;
+      it[j].op = 3;
+      it[j].head = false;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < kItems; j++) {
+    const size_t i = i0 + j;
+    if (i < n) {
+      const uint64_t nx = (j + 1 < kItems) ? it[j + 1].k : (i + 1 < n ? sk[i + 1] : 0);
+      it[j].tail = (i + 1 == n) || (nx != it[j].k) || (j + 1 < kItems && !it[j + 1].valid);
+      it[j].ins = (it[j].op == kOpInsert) && it[j].k != kKeyMax;
+    } else {
+      it[j].tail = false;
+      it[j].ins = false;
+    }
+  }
+}
+
+__device__ __forceinline__ Seg item_seg(const Item& x, const uint64_t* __restrict__ vals) {
+  Seg s;
+  s.f = x.head ? 1u : 0u;
+  s.v = 0;
+  if (x.valid && x.ins) {
+    s.f |= 2u;
+    s.v = vals[x.r];
+  }
+  return s;
+}
+
+// pass 1: per tile aggregate, head count, locally determined tail counts and
+// the state at the tail of the run continued from the previous tile
+__global__ void __launch_bounds__(kThreads) merge_pass1(const uint64_t* __restrict__ sk,
+                                                        const uint32_t* __restrict__ sv,
+                                                        const uint64_t* __restrict__ vals, size_t n,
+                                                        TileSummary* __restrict__ tiles) {
+  __shared__ uint32_t wsf[32];
+  __shared__ uint64_t wsv[32];
+  __shared__ uint32_t ws[32];
+  __shared__ uint64_t s_pre_v;
+  __shared__ uint32_t s_pre_f, s_cont;
+  if (threadIdx.x == 0) {
+    s_cont = 0;
+    s_pre_f = 0;
+    s_pre_v = 0;
+  }
+  const size_t i0 = (size_t)blockIdx.x * kTile + (size_t)threadIdx.x * kItems;
+  Item it[kItems];
+  load_items(sk, sv, n, i0, it);
+  Seg seg[kItems];
+  Seg tagg{0, 0};
+  uint32_t heads = 0;
+#pragma unroll
+  for (int j = 0; j < kItems; j++) {
+    seg[j] = item_seg(it[j], vals);
+    tagg = seg_combine(tagg, seg[j]);
+    heads += it[j].head ? 1u : 0u;
+  }
+  Seg agg;
+  Seg st = blk_exclusive_seg(tagg, Seg{0, 0}, wsf, wsv, &agg);
+  uint32_t ins_l = 0, get_l = 0;
+#pragma unroll
+  for (int j = 0; j < kItems; j++) {
+    st = seg_combine(st, seg[j]);
+    if (it[j].valid && it[j].tail) {
+      if (st.f & 1u) {  // run began inside this tile
+        if (it[j].k != kKeyMax) {
+          if (st.f & 2u) ins_l++;
+          else get_l++;
+        }
+      } else {  // tail of the run continued from the previous tile
+        s_cont = 1u | (it[j].k == kKeyMax ? 2u : 0u);
+        s_pre_f = st.f;
+        s_pre_v = st.v;
+      }
+    }
+  }
+  uint32_t th, ti, tg;
+  blk_exclusive_sum(heads, ws, &th);
+  blk_exclusive_sum(ins_l, ws, &ti);
+  blk_exclusive_sum(get_l, ws, &tg);
+  if (threadIdx.x == 0) {
+    TileSummary& T = tiles[blockIdx.x];
+    T.agg_f = agg.f;
+    T.agg_v = agg.v;
+    T.heads = th;
+    T.ins_local = ti;
+    T.get_local = tg;
+    T.cont = s_cont;
+    T.pre_f = s_pre_f;
+    T.pre_v = s_pre_v;
+  }
+}
+
+// pass 2 (one block): carries and prefix counts across tiles; writes totals
+__global__ void __launch_bounds__(1024) merge_pass2(TileSummary* __restrict__ tiles, uint32_t n_tiles,
+                                                    BatchCounts* __restrict__ counts) {
+  __shared__ uint32_t wsf[32];
+  __shared__ uint64_t wsv[32];
+  __shared__ uint32_t ws[32];
+  const uint32_t per = (n_tiles + blockDim.x - 1) / blockDim.x;
+  const uint32_t t0 = threadIdx.x * per;
+  const uint32_t t1 = min(n_tiles, t0 + per);
+  Seg a{0, 0};
+  uint32_t hsum = 0;
+  for (uint32_t t = t0; t < t1; t++) {
+    a = seg_combine(a, Seg{tiles[t].agg_f, tiles[t].agg_v});
+    hsum += tiles[t].heads;
+  }
+  Seg carry = blk_exclusive_seg(a, Seg{0, 0}, wsf, wsv, nullptr);
+  uint32_t htot;
+  uint32_t hb = blk_exclusive_sum(hsum, ws, &htot);
+  uint32_t isum = 0, gsum = 0;
+  for (uint32_t t = t0; t < t1; t++) {
+    TileSummary& T = tiles[t];
+    T.carry_f = carry.f;
+    T.carry_v = carry.v;
+    T.heads_before = hb;
+    hb += T.heads;
+    uint32_t ic = T.ins_local, gc = T.get_local;
+    if ((T.cont & 1u) && !(T.cont & 2u)) {
+      const Seg s = seg_combine(carry, Seg{T.pre_f, T.pre_v});
+      if (s.f & 2u) ic++;
+      else gc++;
+    }
+    T.ins_before = ic;  // per-tile counts for now
+    T.get_before = gc;
+    isum += ic;
+    gsum += gc;
+    carry = seg_combine(carry, Seg{T.agg_f, T.agg_v});
+  }
+  uint32_t itot, gtot;
+  uint32_t ib = blk_exclusive_sum(isum, ws, &itot);
+  uint32_t gb = blk_exclusive_sum(gsum, ws, &gtot);
+  for (uint32_t t = t0; t < t1; t++) {
+    TileSummary& T = tiles[t];
+    const uint32_t ic = T.ins_before, gc = T.get_before;
+    T.ins_before = ib;
+    T.get_before = gb;
+    ib += ic;
+    gb += gc;
+  }
+  if (threadIdx.x == 0) {
+    counts->n_unique = htot;
+    counts->n_ins = itot;
+    counts->n_get = gtot;
+  }
+}
+
+// pass 3: per request resolution, unique ops and the two work lists
+__global__ void __launch_bounds__(kThreads) merge_pass3(
+    const uint64_t* __restrict__ sk, const uint32_t* __restrict__ sv, const uint64_t* __restrict__ vals, size_t n,
+    const TileSummary* __restrict__ tiles, uint64_t* __restrict__ ukeys, uint64_t* __restrict__ uvals,
+    uint32_t* __restrict__ ins_list, uint32_t* __restrict__ get_list, uint32_t* __restrict__ pend,
+    uint64_t* __restrict__ out_vals, uint8_t* __restrict__ out_st) {
+  __shared__ uint32_t wsf[32];
+  __shared__ uint64_t wsv[32];
+  __shared__ uint32_t ws[32];
+  const TileSummary& T = tiles[blockIdx.x];
+  const size_t i0 = (size_t)blockIdx.x * kTile + (size_t)threadIdx.x * kItems;
+  Item it[kItems];
+  load_items(sk, sv, n, i0, it);
+  Seg seg[kItems];
+  Seg tagg{0, 0};
+  uint32_t heads = 0;
+#pragma unroll
+  for (int j = 0; j < kItems; j++) {
+    seg[j] = item_seg(it[j], vals);
+    tagg = seg_combine(tagg, seg[j]);
+    heads += it[j].head ? 1u : 0u;
+  }
+  Seg st = blk_exclusive_seg(tagg, Seg{T.carry_f, T.carry_v}, wsf, wsv, nullptr);
+  // tail kinds with the true carry
+  uint32_t n_ins = 0, n_get = 0;
+  {
+    Seg s = st;
+#pragma unroll
+    for (int j = 0; j < kItems; j++) {
+      s = seg_combine(s, seg[j]);
+      if (it[j].valid && it[j].tail && it[j].k != kKeyMax) {
+        if (s.f & 2u) n_ins++;
+        else n_get++;
+      }
+    }
+  }
+  uint32_t hpos = blk_exclusive_sum(heads, ws, nullptr) + T.heads_before;
+  uint32_t ipos = blk_exclusive_sum(n_ins, ws, nullptr) + T.ins_before;
+  uint32_t gpos = blk_exclusive_sum(n_get, ws, nullptr) + T.get_before;
+  // hpos counts heads strictly before this thread's first item
+#pragma unroll
+  for (int j = 0; j < kItems; j++) {
+    if (!it[j].valid) break;
+    const size_t i = i0 + j;
+    if (it[j].head) hpos++;
+    const uint32_t u = hpos - 1;  // unique id of this item's run
+    const bool ok = it[j].k != kKeyMax && it[j].op <= 1u;
+    if (!ok) {
+      out_vals[it[j].r] = 0;
+      out_st[it[j].r] = kRejected;
+      pend[i] = kResolved;
+    } else if (!it[j].head && (st.f & 2u)) {  // an earlier INSERT of this same run
+      out_vals[it[j].r] = st.v;
+      out_st[it[j].r] = kFound;
+      pend[i] = kResolved;
+    } else {
+      pend[i] = u;
+    }
+    st = seg_combine(st, seg[j]);
+    if (it[j].tail && it[j].k != kKeyMax) {
+      ukeys[u] = it[j].k;
+      uvals[u] = st.v;
+      if (st.f & 2u) ins_list[ipos++] = u;
+      else get_list[gpos++] = u;
+    }
+  }
+}
+
+__global__ void writeback_kernel(const uint32_t* __restrict__ sv, const uint32_t* __restrict__ pend, size_t n,
+                                 const uint64_t* __restrict__ uans, const uint8_t* __restrict__ uans_st,
+                                 uint64_t* __restrict__ out_vals, uint8_t* __restrict__ out_st) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint32_t u = pend[i];
+    if (u != kResolved) {
+      const uint32_t r = sv[i] & kIdxMask;
+      out_vals[r] = uans[u];
+      out_st[r] = uans_st[u];
+    }
+  }
+}
+
+}  // namespace
+
+int work_alloc(Work* w, size_t cap) {
+  work_free(w);
+  if (cap == 0) cap = 1;
+  const size_t tiles = sort_tiles(cap);
+  bool ok = true;
+  auto A = [&](void** p, size_t bytes) {
+    if (ok && cudaMalloc(p, bytes) != cudaSuccess) ok = false;
+  };
+  A((void**)&w->k_a, cap * 8);
+  A((void**)&w->k_b, cap * 8);
+  A((void**)&w->v_a, cap * 4);
+  A((void**)&w->v_b, cap * 4);
+  A((void**)&w->sort_scratch, sort_scratch_words(cap) * 4);
+  A((void**)&w->ukeys, cap * 8);
+  A((void**)&w->uvals, cap * 8);
+  A((void**)&w->uans, cap * 8);
+  A((void**)&w->uans_st, cap);
+  A((void**)&w->ins_list, cap * 4);
+  A((void**)&w->get_list, cap * 4);
+  A((void**)&w->pend, cap * 4);
+  A((void**)&w->tiles, tiles * sizeof(TileSummary));
+  A((void**)&w->counts, sizeof(BatchCounts));
+  A((void**)&w->d_in_keys, cap * 8);
+  A((void**)&w->d_in_vals, cap * 8);
+  A((void**)&w->d_in_ops, cap);
+  A((void**)&w->d_out_vals, cap * 8);
+  A((void**)&w->d_out_st, cap);
+  if (!ok) {
+    work_free(w);
+    return -3;
+  }
+  w->cap = cap;
+  return 0;
+}
+
+void work_free(Work* w) {
+  void* ps[] = {w->k_a,     w->k_b,      w->v_a,       w->v_b,      w->sort_scratch, w->ukeys,     w->uvals,
+                w->uans,    w->uans_st,  w->ins_list,  w->get_list, w->pend,         w->tiles,     w->counts,
+                w->d_in_keys, w->d_in_vals, w->d_in_ops, w->d_out_vals, w->d_out_st};
+  for (void* p : ps)
+    if (p) cudaFree(p);
+  *w = Work{};
+}
+
+int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, uint64_t* out_vals,
+                 uint8_t* out_st, size_t n, int engine, cudaStream_t s) {
+  if (n == 0) return 0;
+  Work& w = h->w;
+  if (n > w.cap || n > kIdxMask) return -6;
+  uint64_t* sk = nullptr;
+  uint32_t* sv = nullptr;
+  prof_mark(h, 0, s);
+  if (radix_sort_pairs(keys, nullptr, ops, w.k_a, w.v_a, w.k_b, w.v_b, n, 0, 64, w.sort_scratch, s, &sk, &sv) !=
+      cudaSuccess)
+    return -2;
+  const uint32_t n_tiles = (uint32_t)sort_tiles(n);
+  prof_mark(h, 1, s);
+  merge_pass1<<<n_tiles, kThreads, 0, s>>>(sk, sv, vals, n, w.tiles);
+  count_launch();
+  merge_pass2<<<1, 1024, 0, s>>>(w.tiles, n_tiles, w.counts);
+  count_launch();
+  merge_pass3<<<n_tiles, kThreads, 0, s>>>(sk, sv, vals, n, w.tiles, w.ukeys, w.uvals, w.ins_list, w.get_list,
+                                           w.pend, out_vals, out_st);
+  count_launch();
+  if (cudaGetLastError() != cudaSuccess) return -2;
+  // search phase on the pre-batch tree, then the insert phase
+  prof_mark(h, 2, s);
+  cudaError_t e;
+  if (h->descent == 1 && h->L.valid)
+    e = launch_learned_search(h, w.ukeys, w.get_list, &w.counts->n_get, n, w.uans, w.uans_st, s);
+  else
+    e = launch_search(h, w.ukeys, w.get_list, &w.counts->n_get, n, w.uans, w.uans_st, s);
+  if (e != cudaSuccess) return -2;
+  (void)engine;
+  prof_mark(h, 3, s);
+  e = launch_stm(h, w.ukeys, w.uvals, nullptr, kOpInsert, w.ins_list, &w.counts->n_ins, n, w.uans, w.uans_st, s);
+  if (e != cudaSuccess) return -2;
+  prof_mark(h, 4, s);
+  const unsigned wb_blocks = (unsigned)min((size_t)h->sm_count * 8, (n + 255) / 256);
+  writeback_kernel<<<wb_blocks, 256, 0, s>>>(sv, w.pend, n, w.uans, w.uans_st, out_vals, out_st);
+  count_launch();
+  prof_mark(h, 5, s);
+  if (cudaGetLastError() != cudaSuccess) return -2;
+  return 0;
+}
+
+}  // namespace bt

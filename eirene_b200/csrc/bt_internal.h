@@ -1,0 +1,150 @@
+// Host-side internals shared by the CUDA translation units of libeirene_b200.
+#pragma once
+#include <atomic>
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "bt_common.cuh"
+
+namespace bt {
+
+// process-wide count of kernels launched by this library (reported by the bench)
+extern std::atomic<unsigned long long> g_launches;
+inline void count_launch(unsigned n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+// phases timed with CUDA events when profiling is on (the reference's
+// Time_Measure phases, src/gpu-stm-tree-v38/bpt-gpustm-kernel.cu:289-324)
+enum Phase { kPhSort = 0, kPhMerge, kPhSearch, kPhInsert, kPhWriteback, kNumPhases };
+
+// ---- scan / sort (bt_sort.cu) ----
+size_t scan_scratch_words(size_t n);
+cudaError_t scan_exclusive_u32(const uint32_t* in, uint32_t* out, size_t n, uint32_t* total_dev, uint32_t* scratch,
+                               cudaStream_t s);
+size_t sort_tiles(size_t n);
+cudaError_t sort_prepare();
+size_t sort_scratch_words(size_t n);
+cudaError_t radix_sort_pairs(const uint64_t* keys_in, const uint32_t* vals_in, const uint8_t* ops, uint64_t* k_a,
+                             uint32_t* v_a, uint64_t* k_b, uint32_t* v_b, size_t n, int begin_bit, int end_bit,
+                             uint32_t* scratch, cudaStream_t s, uint64_t** k_out, uint32_t** v_out);
+
+// ---- per-batch work buffers, sized for max_batch requests ----
+struct BatchCounts {
+  uint32_t n_unique;
+  uint32_t n_ins;
+  uint32_t n_get;
+  uint32_t pad;
+};
+
+struct TileSummary;  // bt_batch.cu
+
+struct Work {
+  size_t cap = 0;  // requests
+  uint64_t* k_a = nullptr;
+  uint64_t* k_b = nullptr;
+  uint32_t* v_a = nullptr;
+  uint32_t* v_b = nullptr;
+  uint32_t* sort_scratch = nullptr;
+  uint64_t* ukeys = nullptr;
+  uint64_t* uvals = nullptr;
+  uint64_t* uans = nullptr;
+  uint8_t* uans_st = nullptr;
+  uint32_t* ins_list = nullptr;
+  uint32_t* get_list = nullptr;
+  uint32_t* pend = nullptr;
+  TileSummary* tiles = nullptr;
+  uint64_t* tile_carry = nullptr;  // scratch for the tile pass
+  BatchCounts* counts = nullptr;
+  // host staging for the host-buffer entry point
+  uint64_t* d_in_keys = nullptr;
+  uint64_t* d_in_vals = nullptr;
+  uint8_t* d_in_ops = nullptr;
+  uint64_t* d_out_vals = nullptr;
+  uint8_t* d_out_st = nullptr;
+};
+
+// ---- learned leaf predictor state (bt_learned.cu) ----
+struct Learned {
+  bool valid = false;
+  uint32_t n_leaves = 0;
+  uint32_t n_segments = 0;
+  uint32_t window = 64;
+  uint64_t* leaf_low = nullptr;  // [n_leaves + 1] (sentinel at the end)
+  uint32_t* leaf_id = nullptr;   // [n_leaves]
+  size_t leaf_cap = 0;
+  float* mlp = nullptr;          // 97 params
+  float* mlp_grad = nullptr;     // 97 floats (device gradient buffer)
+  double* seg = nullptr;         // per segment: base(key as double bits), slope, intercept, err (4 doubles)
+  uint32_t* seg_scratch = nullptr;
+  size_t seg_cap = 0;
+  uint64_t kmin = 0, kmax = 0;
+  int stage1 = 1;  // 1 = MLP root model, 0 = linear root model
+  uint32_t train_steps = 300;
+  uint32_t train_batch = 16384;
+  float lr = 0.05f;
+  double last_loss = 0;
+  uint64_t seg_fallback = 0;  // segments whose error exceeds the window
+};
+
+struct Handle {
+  int device = 0;
+  DevTree tree{};
+  uint32_t leaf_fill = 24;
+  uint32_t inner_fill = 24;
+  uint32_t retry_limit = 1u << 16;
+  int descent = 0;     // 0 plain, 1 learned
+  int search_group = 8;  // lanes per request in the lock-free search
+  int sm_count = 148;
+  Work w;
+  Learned L;
+  uint32_t* enum_a = nullptr;  // leaf enumeration buffers (node ids)
+  uint32_t* enum_b = nullptr;
+  uint32_t* enum_cnt = nullptr;
+  uint32_t* enum_scan_scratch = nullptr;
+  size_t enum_cap = 0;
+  uint64_t level_counts[48] = {};  // filled by enumerate_leaves, leaf level first
+  uint32_t n_levels = 0;
+  cudaStream_t internal_stream = nullptr;
+  // profiling: one event per phase boundary per batch, resolved on read
+  bool prof = false;
+  std::vector<cudaEvent_t> prof_ev;  // kNumPhases + 1 events per recorded batch
+  size_t prof_batches = 0;
+  double phase_ms[kNumPhases] = {};
+  unsigned long long phase_batches = 0;
+  unsigned long long phase_items[kNumPhases] = {};
+};
+
+// record the boundary event `which` (0..kNumPhases) of the current batch
+void prof_mark(Handle* h, int which, cudaStream_t s);
+
+// ---- tree kernels (bt_tree.cu) ----
+cudaError_t tree_reset(Handle* h, cudaStream_t s);
+int tree_bulk_build(Handle* h, const uint64_t* keys, const uint64_t* vals, size_t n, cudaStream_t s);
+cudaError_t launch_search(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev, size_t n,
+                          uint64_t* out_vals, uint8_t* out_st, cudaStream_t s);
+// ids of the leaves in key order; returns count (synchronises the stream)
+int enumerate_leaves(Handle* h, cudaStream_t s, uint32_t** leaf_ids, size_t* n_leaves);
+// leaf sizes in key order into a device buffer (after enumerate_leaves)
+cudaError_t leaf_sizes_device(Handle* h, const uint32_t* leaves, size_t n, uint32_t* out, cudaStream_t s);
+int tree_dump(Handle* h, uint64_t* out_keys, uint64_t* out_vals, size_t cap, size_t* n_out, cudaStream_t s);
+
+// ---- STM kernels (bt_stm.cu) ----
+cudaError_t launch_stm(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, uint8_t op_override,
+                       const uint32_t* list, const uint32_t* n_dev, size_t n, uint64_t* out_vals, uint8_t* out_st,
+                       cudaStream_t s);
+
+// ---- sorted-merge batch (bt_batch.cu) ----
+int work_alloc(Work* w, size_t cap);
+void work_free(Work* w);
+int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, uint64_t* out_vals,
+                 uint8_t* out_st, size_t n, int engine, cudaStream_t s);
+
+// ---- learned predictor (bt_learned.cu) ----
+int learned_retrain(Handle* h, cudaStream_t s);
+void learned_free(Learned* L);
+cudaError_t launch_learned_search(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev,
+                                  size_t n, uint64_t* out_vals, uint8_t* out_st, cudaStream_t s);
+
+}  // namespace bt

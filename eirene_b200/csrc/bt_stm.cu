@@ -1,0 +1,383 @@
+// Warp-level software transactional memory over the B+tree: one warp per
+// request, lane i owns slot i of the node it is looking at.  Restates the
+// reference's tx_insert_kernel (src/gpu-stm-tree-v39/bpt-gpustm-kernel.cu:14-256)
+// with three design changes:
+//   * the version/lock word is the node header (keys[31]) rather than a side
+//     table, so the seqlock read of a node needs no extra sector;
+//   * ordering is explicit: ld.acquire of the header, fence.acq_rel before
+//     the validating re-read, release stores of the header on commit (the
+//     reference relies on volatile loads, src/.../bpt-gpustm-kernel-tx.cuh:46-66);
+//   * the parent is re-validated against its full header word (lock bit
+//     included) after the child is read, and retries are bounded: a request
+//     that cannot commit within the limit reports kRetryExhausted.
+// Structure rules (early split of full inner nodes, 16|16 leaf split, new
+// root) follow src/gpu-stm-tree-v39/bpt-gpustm-kernel-tree.cuh:150-467.
+#include <cuda_runtime.h>
+
+#include "bt_common.cuh"
+#include "bt_internal.h"
+
+namespace bt {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+enum : int { TX_DONE = 0, TX_ABORT = 1, TX_AGAIN = 2, TX_NOCAP = 3 };
+
+__device__ __forceinline__ uint64_t* hdr_ptr(const DevTree& t, uint32_t n) { return t.keys + (size_t)n * 32 + 31; }
+
+// Lock node n1 (expected header h1), node n2 (h2) and/or the root lock (rl).
+// Lanes 0, 1, 2 each take one; on any failure the taken ones are restored.
+__device__ bool acquire_locks(const DevTree& t, uint32_t n1, uint64_t h1, uint32_t n2, uint64_t h2, bool lock_root,
+                              uint32_t rl) {
+  const uint32_t lane = lane_id();
+  bool ok = true, got = false;
+  if (lane == 0 && n1 != kNil) {
+    got = atomicCAS((unsigned long long*)hdr_ptr(t, n1), h1, hdr_lock(h1)) == h1;
+    ok = got;
+  } else if (lane == 1 && n2 != kNil) {
+    got = atomicCAS((unsigned long long*)hdr_ptr(t, n2), h2, hdr_lock(h2)) == h2;
+    ok = got;
+  } else if (lane == 2 && lock_root) {
+    got = atomicCAS(&t.ctrl->root_lock, rl, rl | 1u) == rl;
+    ok = got;
+  }
+  if (!__all_sync(kFull, ok)) {
+    if (got) {  // nothing was written: put the same version back
+      if (lane == 0) st_release(hdr_ptr(t, n1), h1);
+      else if (lane == 1) st_release(hdr_ptr(t, n2), h2);
+      else st_release32(&t.ctrl->root_lock, rl);
+    }
+    __syncwarp();
+    return false;
+  }
+  __threadfence();
+  return true;
+}
+
+__device__ void unlock_unchanged(const DevTree& t, uint32_t n1, uint64_t h1, uint32_t n2, uint64_t h2, bool root,
+                                 uint32_t rl) {
+  const uint32_t lane = lane_id();
+  if (lane == 0 && n1 != kNil) st_release(hdr_ptr(t, n1), h1);
+  if (lane == 1 && n2 != kNil) st_release(hdr_ptr(t, n2), h2);
+  if (lane == 2 && root) st_release32(&t.ctrl->root_lock, rl);
+  __syncwarp();
+}
+
+__device__ uint32_t alloc_nodes(const DevTree& t, uint32_t cnt) {
+  uint32_t base = 0;
+  if (lane_id() == 0) {
+    base = atomicAdd(&t.ctrl->n_nodes, cnt);
+    if (base >= t.cap || base + cnt > t.cap) {
+      atomicOr(&t.ctrl->error, kErrCapacity);
+      base = kNil;
+    }
+  }
+  return __shfl_sync(kFull, base, 0);
+}
+
+// lane-parallel row write; the header slot (keys[31]) is written only for new
+// nodes (write_hdr), existing nodes publish their header with a release store.
+__device__ __forceinline__ void write_row(const DevTree& t, uint32_t n, uint64_t k, uint64_t v, bool write_hdr,
+                                          uint64_t hdr) {
+  const uint32_t lane = lane_id();
+  uint64_t* kr = t.keys + (size_t)n * 32;
+  uint64_t* vr = t.vals + (size_t)n * 32;
+  if (lane < 31) kr[lane] = k;
+  else if (write_hdr) kr[31] = hdr;
+  vr[lane] = v;
+}
+
+// Split commit shared by the leaf split and the early inner split.
+// left image (lk, lv, lhdr) replaces node `node` (read at header h);
+// right image (rk, rv, rhdr) becomes a new node with low fence `up`; the
+// parent (read at ph with lanes' slots pk/pv) gets separator `up` at pslot,
+// or a new root is created above `node`.
+__device__ int commit_split(const DevTree& t, uint32_t node, uint64_t h, uint64_t lk, uint64_t lv, uint64_t lhdr,
+                            uint64_t rk, uint64_t rv, uint32_t rsize, uint32_t level, uint64_t up, uint32_t parent,
+                            uint64_t ph, uint32_t pslot, uint64_t pk, uint64_t pv, uint32_t rl) {
+  const uint32_t lane = lane_id();
+  Ctrl* C = t.ctrl;
+  // parent image shift (computed by all lanes before branching)
+  const uint64_t upk = __shfl_up_sync(kFull, pk, 1);
+  const uint64_t upv = __shfl_up_sync(kFull, pv, 1);
+  const bool new_root = (parent == kNil);
+  if (!acquire_locks(t, node, h, parent, ph, new_root, rl)) return TX_ABORT;
+  const uint32_t base = alloc_nodes(t, new_root ? 2u : 1u);
+  if (base == kNil) {
+    unlock_unchanged(t, node, h, parent, ph, new_root, rl);
+    return TX_NOCAP;
+  }
+  const uint32_t right = base;
+  // new right node (unreachable until the parent / root is published)
+  write_row(t, right, rk, rv, true, make_hdr(rsize, level, 0));
+  if (lane == 0) t.low[right] = up;
+  write_row(t, node, lk, lv, false, 0);
+  uint32_t psize = 0;
+  if (!new_root) {
+    psize = hdr_size(ph);
+    const uint64_t npk = lane < pslot ? pk : (lane == pslot ? up : upk);
+    const uint64_t npv = lane <= pslot ? pv : (lane == pslot + 1 ? (uint64_t)right : upv);
+    write_row(t, parent, npk, npv, false, 0);
+  } else {
+    const uint32_t nr = base + 1;
+    const uint64_t nk = lane == 0 ? up : kKeyMax;
+    const uint64_t nv = lane == 0 ? (uint64_t)node : (lane == 1 ? (uint64_t)right : 0);
+    write_row(t, nr, nk, nv, true, make_hdr(1, level + 1, 0));
+    if (lane == 0) t.low[nr] = t.low[node];
+  }
+  __threadfence();
+  __syncwarp();
+  if (lane == 0) st_release(hdr_ptr(t, node), lhdr);
+  if (!new_root) {
+    if (lane == 1) st_release(hdr_ptr(t, parent), make_hdr(psize + 1, hdr_level(ph), hdr_version(ph) + 1));
+  } else if (lane == 0) {
+    C->root_level = level + 1;
+    C->root = base + 1;
+    __threadfence();
+    st_release32(&C->root_lock, rl + 2u);
+  }
+  __syncwarp();
+  if (lane == 0) {
+    if (level == 0) atomicAdd(&C->leaf_splits, 1ull);
+    else atomicAdd(&C->inner_splits, 1ull);
+    if (new_root) {
+      atomicAdd(&C->new_roots, 1ull);
+      atomicAdd(&C->inner_splits, 1ull);
+    }
+  }
+  return TX_DONE;
+}
+
+// One transaction attempt for one request (all 32 lanes).
+__device__ int tx_attempt(const DevTree& t, const uint64_t key, const uint64_t val, const bool is_insert,
+                          uint64_t& ans, uint8_t& st) {
+  const uint32_t lane = lane_id();
+  Ctrl* C = t.ctrl;
+  // ---- root (reference TX_READ_ROOT, bpt-gpustm-kernel-tx.cuh:92-119)
+  uint32_t rl = 0, root = 0;
+  int bad0 = 0;
+  if (lane == 0) {
+    rl = ld_acquire32(&C->root_lock);
+    root = ld_relaxed32(&C->root);
+    fence_acq_rel();
+    bad0 = (rl & 1u) || ld_relaxed32(&C->root_lock) != rl;
+  }
+  if (__shfl_sync(kFull, bad0, 0)) return TX_ABORT;
+  rl = __shfl_sync(kFull, rl, 0);
+  root = __shfl_sync(kFull, root, 0);
+  if (root == kNil) {
+    if (!is_insert) {
+      ans = 0;
+      st = kAbsent;
+      return TX_DONE;
+    }
+    // CREATE_NEW_TREE (bpt-gpustm-kernel-tree.cuh:122-147): an empty leaf root
+    if (!acquire_locks(t, kNil, 0, kNil, 0, true, rl)) return TX_ABORT;
+    const uint32_t id = alloc_nodes(t, 1);
+    if (id == kNil) {
+      unlock_unchanged(t, kNil, 0, kNil, 0, true, rl);
+      return TX_NOCAP;
+    }
+    write_row(t, id, kKeyMax, lane == 31 ? kKeyMax : 0, true, make_hdr(0, 0, 0));
+    if (lane == 0) t.low[id] = 0;
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) {
+      C->root_level = 0;
+      C->root = id;
+      __threadfence();
+      st_release32(&C->root_lock, rl + 2u);
+    }
+    __syncwarp();
+    return TX_AGAIN;
+  }
+  // ---- descent with per-level validation (TX_READ, bpt-gpustm-kernel-tx.cuh:25-88)
+  uint32_t node = root, parent = kNil, pslot = 0;
+  uint64_t h = 0, ph = 0, k = 0, v = 0, pk = kKeyMax, pv = 0;
+  for (int depth = 0;; depth++) {
+    if (depth > 40) return TX_ABORT;  // defensive: no valid tree is this tall
+    const uint64_t* krow = t.keys + (size_t)node * 32;
+    const uint64_t* vrow = t.vals + (size_t)node * 32;
+    h = ld_acquire(krow + 31);
+    k = ld_relaxed(krow + lane);
+    v = ld_relaxed(vrow + lane);
+    fence_acq_rel();
+    const uint64_t h2 = ld_relaxed(krow + 31);
+    const uint64_t h_lane0 = __shfl_sync(kFull, h, 0);  // every lane must see one version
+    const bool up_ok = (parent != kNil) ? (ld_relaxed(hdr_ptr(t, parent)) == ph)
+                                        : (ld_relaxed32(&C->root_lock) == rl);
+    const bool bad = hdr_locked(h) || h2 != h || h != h_lane0 || !up_ok;
+    if (__any_sync(kFull, bad)) return TX_ABORT;
+    if (lane == 31) k = kKeyMax;  // slot 31 is the header
+    const uint32_t level = hdr_level(h), size = hdr_size(h);
+    if (level > 0 && size >= (uint32_t)kMaxKeys && is_insert) {
+      // early split of a full inner node (bpt-gpustm-kernel.cu:160-179,
+      // NODE_SPLITTING bpt-gpustm-kernel-tree.cuh:150-224): up = key[15]
+      const uint32_t mid = 15;
+      const uint64_t up = __shfl_sync(kFull, k, mid);
+      const uint64_t rk0 = __shfl_down_sync(kFull, k, mid + 1);
+      const uint64_t rv0 = __shfl_down_sync(kFull, v, mid + 1);
+      const uint64_t lk = lane < mid ? k : kKeyMax;
+      const uint64_t lv = lane <= mid ? v : 0;
+      const uint64_t rk = lane < mid ? rk0 : kKeyMax;
+      const uint64_t rv = lane <= mid ? rv0 : 0;
+      const int r = commit_split(t, node, h, lk, lv, make_hdr(mid, level, hdr_version(h) + 1), rk, rv, mid, level, up,
+                                 parent, ph, pslot, pk, pv, rl);
+      return r == TX_DONE ? TX_AGAIN : r;
+    }
+    if (level == 0) break;
+    const uint32_t c = __popc(__ballot_sync(kFull, lane < 31 && k <= key));
+    const uint32_t child = (uint32_t)__shfl_sync(kFull, v, c);
+    parent = node;
+    ph = h;
+    pslot = c;
+    pk = k;
+    pv = v;
+    node = child;
+  }
+  // ---- leaf (answer rule bpt-gpustm-kernel.cu:197-213)
+  const uint32_t size = hdr_size(h);
+  const uint32_t mm = __ballot_sync(kFull, lane < size && k == key);
+  if (!is_insert) {
+    if (mm) {
+      ans = __shfl_sync(kFull, v, __ffs(mm) - 1);
+      st = kFound;
+    } else {
+      ans = 0;
+      st = kAbsent;
+    }
+    return TX_DONE;
+  }
+  if (mm) {
+    // key present: update in place, answer the previous value (INSERT_LEAF :373-384)
+    const uint32_t at = __ffs(mm) - 1;
+    const uint64_t old = __shfl_sync(kFull, v, at);
+    if (!acquire_locks(t, node, h, kNil, 0, false, 0)) return TX_ABORT;
+    if (lane == at) t.vals[(size_t)node * 32 + at] = val;
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) st_release(hdr_ptr(t, node), make_hdr(size, 0, hdr_version(h) + 1));
+    __syncwarp();
+    ans = old;
+    st = kFound;
+    return TX_DONE;
+  }
+  // shift-insert at p = number of keys < key
+  const uint32_t p = __popc(__ballot_sync(kFull, lane < size && k < key));
+  const uint64_t uk = __shfl_up_sync(kFull, k, 1);
+  const uint64_t uv = __shfl_up_sync(kFull, v, 1);
+  const uint64_t nk = lane < p ? k : (lane == p ? key : uk);
+  const uint64_t nv = lane < p ? v : (lane == p ? val : uv);
+  if (size < (uint32_t)kMaxKeys) {
+    if (!acquire_locks(t, node, h, kNil, 0, false, 0)) return TX_ABORT;
+    if (lane <= size && lane < 31) {
+      t.keys[(size_t)node * 32 + lane] = nk;
+      t.vals[(size_t)node * 32 + lane] = nv;
+    }
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) {
+      st_release(hdr_ptr(t, node), make_hdr(size + 1, 0, hdr_version(h) + 1));
+      atomicAdd(&C->n_keys, 1ull);
+    }
+    __syncwarp();
+    ans = 0;
+    st = kAbsent;
+    return TX_DONE;
+  }
+  // full leaf: 32 entries split 16 | 16, up = first key of the right half;
+  // left fence = up, right keeps the old fence (INSERT_LEAF :413-452)
+  const uint64_t old_fence = __shfl_sync(kFull, v, 31);
+  const uint64_t up = __shfl_sync(kFull, nk, 16);
+  const uint64_t rk0 = __shfl_down_sync(kFull, nk, 16);
+  const uint64_t rv0 = __shfl_down_sync(kFull, nv, 16);
+  const uint64_t lk = lane < 16 ? nk : kKeyMax;
+  const uint64_t lv = lane < 16 ? nv : (lane == 31 ? up : 0);
+  const uint64_t rk = lane < 16 ? rk0 : kKeyMax;
+  const uint64_t rv = lane < 16 ? rv0 : (lane == 31 ? old_fence : 0);
+  const int r = commit_split(t, node, h, lk, lv, make_hdr(16, 0, hdr_version(h) + 1), rk, rv, 16, 0, up, parent, ph,
+                             pslot, pk, pv, rl);
+  if (r != TX_DONE) return r;
+  if (lane == 0) atomicAdd(&C->n_keys, 1ull);
+  ans = 0;
+  st = kAbsent;
+  return TX_DONE;
+}
+
+__global__ void __launch_bounds__(256) stm_kernel(DevTree t, const uint64_t* __restrict__ keys,
+                                                  const uint64_t* __restrict__ vals, const uint8_t* __restrict__ ops,
+                                                  uint32_t op_override, const uint32_t* __restrict__ list,
+                                                  const uint32_t* __restrict__ n_dev, size_t n_host,
+                                                  uint64_t* __restrict__ out_vals, uint8_t* __restrict__ out_st,
+                                                  uint32_t retry_limit) {
+  const uint32_t lane = lane_id();
+  const size_t n = n_dev ? (size_t)*n_dev : n_host;
+  const size_t n_warps = ((size_t)gridDim.x * blockDim.x) >> 5;
+  unsigned long long commits = 0, aborts = 0, exhausted = 0;
+  for (size_t q = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < n; q += n_warps) {
+    const uint32_t r = list ? list[q] : (uint32_t)q;
+    const uint64_t key = keys[r];
+    const uint32_t op = op_override <= 1 ? op_override : (uint32_t)ops[r];
+    uint64_t ans = 0;
+    uint8_t st = kRejected;
+    if (key != kKeyMax && op <= 1) {
+      const bool ins = (op == kOpInsert);
+      const uint64_t val = ins ? vals[r] : 0;
+      uint32_t attempts = 0, fails = 0;
+      for (;;) {
+        if (attempts++ >= retry_limit) {
+          st = kRetryExhausted;
+          exhausted++;
+          if (lane == 0) atomicOr(&t.ctrl->error, kErrRetry);
+          break;
+        }
+        const int res = tx_attempt(t, key, val, ins, ans, st);
+        if (res == TX_DONE) {
+          if (ins) commits++;
+          break;
+        }
+        if (res == TX_AGAIN) {
+          commits++;
+          fails = 0;
+          continue;
+        }
+        if (res == TX_NOCAP) {
+          st = kNoCapacity;
+          ans = 0;
+          break;
+        }
+        aborts++;
+        fails++;
+        if (fails > 2) __nanosleep(32u << (fails < 8 ? fails : 8));
+      }
+    }
+    if (lane == 0) {
+      out_vals[r] = ans;
+      out_st[r] = st;
+    }
+  }
+  if (lane == 0) {
+    if (commits) atomicAdd(&t.ctrl->commits, commits);
+    if (aborts) atomicAdd(&t.ctrl->aborts, aborts);
+    if (exhausted) atomicAdd(&t.ctrl->retry_exhausted, exhausted);
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_stm(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, uint8_t op_override,
+                       const uint32_t* list, const uint32_t* n_dev, size_t n, uint64_t* out_vals, uint8_t* out_st,
+                       cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  const int threads = 256;  // 8 warps
+  size_t blocks = (n * 32 + threads - 1) / threads;
+  const size_t cap = (size_t)h->sm_count * 8;  // 64 resident warps per SM
+  if (blocks > cap) blocks = cap;
+  stm_kernel<<<(unsigned)blocks, threads, 0, s>>>(h->tree, keys, vals, ops, op_override, list, n_dev, n, out_vals,
+                                                   out_st, h->retry_limit);
+  count_launch();
+  return cudaGetLastError();
+}
+
+}  // namespace bt

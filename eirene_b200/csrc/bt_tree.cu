@@ -1,0 +1,421 @@
+// Tree construction and the lock-free batched point search.
+//
+// Search: a group of G lanes serves one request (G = 4, 8, 16 or 32; the
+// reference uses a whole warp, one key per lane, src/gpu-stm-tree-v39/
+// bpt-gpustm-kernel-tree.cuh:61-118).  Each lane loads 32/G consecutive keys
+// of the node with 16-byte vector loads, counts keys <= target, and the group
+// sums the counts with xor-shuffles: that sum is the child slot (child i covers
+// [key[i-1], key[i]), src/tree.h:7-19).  With G = 8 a warp carries four
+// independent descents, four times the memory-level parallelism of the
+// reference's warp-per-request layout.  This kernel runs only when no writer
+// is active (the batch executor orders it before/after the insert phase), so
+// it needs no version checks and may use the read-only cache path.
+#include <cstdio>
+#include <cuda_runtime.h>
+
+#include "bt_common.cuh"
+#include "bt_internal.h"
+
+namespace bt {
+
+namespace {
+
+__global__ void reset_kernel(Ctrl* c) {
+  c->root = kNil;
+  c->root_lock = 0;
+  c->n_nodes = 0;
+  c->error = 0;
+  c->root_level = 0;
+  c->n_keys = 0;
+  c->commits = c->aborts = c->leaf_splits = c->inner_splits = c->new_roots = 0;
+  c->retry_exhausted = c->learned_hits = c->learned_fallbacks = c->learned_probe_sum = 0;
+}
+
+// ---------------------------------------------------------------- build ----
+__global__ void tail_flags_kernel(const uint64_t* __restrict__ sk, size_t n, uint32_t* __restrict__ flags) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) flags[i] = (i + 1 == n || sk[i + 1] != sk[i]) ? 1u : 0u;
+}
+
+__global__ void dedupe_kernel(const uint64_t* __restrict__ sk, const uint32_t* __restrict__ sidx,
+                              const uint64_t* __restrict__ vals, const uint32_t* __restrict__ flags,
+                              const uint32_t* __restrict__ pos, size_t n, uint64_t* __restrict__ uk,
+                              uint64_t* __restrict__ uv) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && flags[i]) {
+    uint32_t p = pos[i];
+    uk[p] = sk[i];
+    uv[p] = vals[sidx[i]];
+  }
+}
+
+// one warp per leaf; leaves get base or base+1 keys (the first `rem` get one more)
+__global__ void build_leaves_kernel(DevTree t, const uint64_t* __restrict__ uk, const uint64_t* __restrict__ uv,
+                                    size_t m, uint32_t nl) {
+  const uint32_t lane = threadIdx.x & 31;
+  const size_t j = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (j >= nl) return;
+  const size_t base = m / nl, rem = m % nl;
+  const size_t k = base + (j < rem ? 1 : 0);
+  const size_t start = j * base + (j < rem ? j : rem);
+  uint64_t* kr = t.keys + j * 32;
+  uint64_t* vr = t.vals + j * 32;
+  if (lane < 31) {
+    kr[lane] = lane < k ? uk[start + lane] : kKeyMax;
+    vr[lane] = lane < k ? uv[start + lane] : 0;
+  } else {
+    kr[31] = make_hdr((uint32_t)k, 0, 0);
+    vr[31] = (j + 1 < nl) ? uk[start + k] : kKeyMax;
+  }
+  if (lane == 0) t.low[j] = j == 0 ? 0 : uk[start];
+}
+
+// one warp per inner node of a level: node p groups children [c, c + k)
+__global__ void build_inner_kernel(DevTree t, uint32_t first_child, uint32_t n_children, uint32_t first_node,
+                                   uint32_t n_nodes_level, uint32_t level) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t p = (uint32_t)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (p >= n_nodes_level) return;
+  const uint32_t base = n_children / n_nodes_level, rem = n_children % n_nodes_level;
+  const uint32_t k = base + (p < rem ? 1 : 0);
+  const uint32_t c = first_child + p * base + (p < rem ? p : rem);
+  const uint32_t id = first_node + p;
+  uint64_t* kr = t.keys + (size_t)id * 32;
+  uint64_t* vr = t.vals + (size_t)id * 32;
+  // key slot i (i < k-1) = low fence of child i+1
+  if (lane < 31) kr[lane] = (lane + 1 < k) ? t.low[c + lane + 1] : kKeyMax;
+  else kr[31] = make_hdr(k - 1, level, 0);
+  vr[lane] = lane < k ? (uint64_t)(c + lane) : 0;
+  if (lane == 0) t.low[id] = t.low[c];
+}
+
+__global__ void set_root_kernel(Ctrl* c, uint32_t root, uint32_t root_level, uint32_t n_nodes, uint64_t n_keys) {
+  c->root = root;
+  c->root_level = root_level;
+  c->n_nodes = n_nodes;
+  c->n_keys = n_keys;
+}
+
+// --------------------------------------------------------------- search ----
+template <int S>
+__device__ __forceinline__ void load_slots(const uint64_t* p, uint64_t (&x)[S]) {
+  if constexpr (S == 1) {
+    x[0] = __ldg(p);
+  } else {
+#pragma unroll
+    for (int i = 0; i < S; i += 2) {
+      ulonglong2 w = __ldg(reinterpret_cast<const ulonglong2*>(p + i));
+      x[i] = w.x;
+      x[i + 1] = w.y;
+    }
+  }
+}
+
+template <int S>
+__device__ __forceinline__ uint64_t pick(const uint64_t (&x)[S], uint32_t e) {
+  uint64_t r = x[0];
+#pragma unroll
+  for (int i = 1; i < S; i++)
+    if (e == (uint32_t)i) r = x[i];
+  return r;
+}
+
+template <int G, bool kLeafVals>
+__global__ void __launch_bounds__(256) search_kernel(DevTree t, const uint64_t* __restrict__ qkeys,
+                                                     const uint32_t* __restrict__ list,
+                                                     const uint32_t* __restrict__ n_dev, size_t n_host,
+                                                     uint64_t* __restrict__ out_vals, uint8_t* __restrict__ out_st) {
+  constexpr int S = 32 / G;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t g = lane % G;
+  const uint32_t gbase = lane - g;
+  const uint32_t gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << gbase);
+  const size_t n = n_dev ? (size_t)*n_dev : n_host;
+  const uint32_t root = t.ctrl->root;
+  const uint32_t root_level = t.ctrl->root_level;
+  const size_t stride = ((size_t)gridDim.x * blockDim.x) / G;
+  for (size_t q = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) / G; q < n; q += stride) {
+    const uint32_t r = list ? __ldg(list + q) : (uint32_t)q;
+    const uint64_t key = __ldg(qkeys + r);
+    uint8_t st = kAbsent;
+    uint64_t ans = 0;
+    if (key == kKeyMax) {
+      st = kRejected;
+    } else if (root != kNil) {
+      uint32_t node = root;
+      uint32_t level = root_level;
+      uint64_t k[S];
+      uint64_t v[S];
+      uint32_t cnt;
+      for (;;) {
+        const size_t row = (size_t)node * 32 + g * S;
+        load_slots<S>(t.keys + row, k);
+        if (level > 0 || kLeafVals) load_slots<S>(t.vals + row, v);
+        if (g == G - 1) k[S - 1] = kKeyMax;  // slot 31 holds the header
+        uint32_t c = 0;
+#pragma unroll
+        for (int i = 0; i < S; i++) c += (k[i] <= key) ? 1u : 0u;
+#pragma unroll
+        for (int o = G / 2; o >= 1; o >>= 1) c += __shfl_xor_sync(gmask, c, o, G);
+        cnt = c;
+        if (level == 0) break;
+        const uint64_t mine = pick<S>(v, cnt % S);
+        node = (uint32_t)__shfl_sync(gmask, mine, cnt / S, G);
+        level--;
+      }
+      // leaf: the key, if present, sits at slot cnt-1
+      if (cnt > 0) {
+        const uint32_t slot = cnt - 1;
+        const uint32_t owner = slot / S, e = slot % S;
+        const uint64_t kk = __shfl_sync(gmask, pick<S>(k, e), owner, G);
+        if (kk == key) {
+          st = kFound;
+          if (kLeafVals) ans = __shfl_sync(gmask, pick<S>(v, e), owner, G);
+          else ans = (g == 0) ? __ldg(t.vals + (size_t)node * 32 + slot) : 0;
+        }
+      }
+    }
+    if (g == 0) {
+      out_vals[r] = ans;
+      out_st[r] = st;
+    }
+  }
+}
+
+// ---------------------------------------------------------- enumeration ----
+__global__ void child_count_kernel(DevTree t, const uint32_t* __restrict__ nodes, size_t n, uint32_t* cnt,
+                                   int leaf_sizes) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    uint64_t h = t.keys[(size_t)nodes[i] * 32 + 31];
+    cnt[i] = leaf_sizes ? hdr_size(h) : hdr_size(h) + 1;
+  }
+}
+
+__global__ void child_write_kernel(DevTree t, const uint32_t* __restrict__ nodes, size_t n,
+                                   const uint32_t* __restrict__ off, uint32_t* __restrict__ out) {
+  const uint32_t lane = threadIdx.x & 31;
+  const size_t i = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (i >= n) return;
+  const uint32_t node = nodes[i];
+  const uint32_t sz = hdr_size(t.keys[(size_t)node * 32 + 31]);
+  if (lane <= sz) out[off[i] + lane] = (uint32_t)t.vals[(size_t)node * 32 + lane];
+}
+
+__global__ void leaf_dump_kernel(DevTree t, const uint32_t* __restrict__ leaves, size_t n,
+                                 const uint32_t* __restrict__ off, uint64_t* __restrict__ ok,
+                                 uint64_t* __restrict__ ov) {
+  const uint32_t lane = threadIdx.x & 31;
+  const size_t i = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (i >= n) return;
+  const uint32_t node = leaves[i];
+  const uint32_t sz = hdr_size(t.keys[(size_t)node * 32 + 31]);
+  if (lane < sz) {
+    size_t o = (size_t)off[i] + lane;
+    if (ok) ok[o] = t.keys[(size_t)node * 32 + lane];
+    if (ov) ov[o] = t.vals[(size_t)node * 32 + lane];
+  }
+}
+
+inline unsigned blocks_for(size_t n, int per) { return (unsigned)((n + per - 1) / per); }
+
+}  // namespace
+
+cudaError_t tree_reset(Handle* h, cudaStream_t s) {
+  reset_kernel<<<1, 1, 0, s>>>(h->tree.ctrl);
+  count_launch();
+  return cudaGetLastError();
+}
+
+// Bulk loader: replaces the contents.  Same packing rule as the oracle
+// (bto_bulk_build): ceil(m/leaf_fill) leaves of even size, inner levels of
+// inner_fill+1 children per node, leaves first in id order.
+int tree_bulk_build(Handle* h, const uint64_t* keys, const uint64_t* vals, size_t n, cudaStream_t s) {
+  cudaError_t e = tree_reset(h, s);
+  if (e != cudaSuccess) return -2;
+  if (n == 0) return 0;
+  if (n > 0xFFFFFFFFull / 2) return -1;
+  // temporaries (stream ordered)
+  uint64_t *ka = nullptr, *kb = nullptr, *uk = nullptr, *uv = nullptr;
+  uint32_t *va = nullptr, *vb = nullptr, *flags = nullptr, *pos = nullptr, *scratch = nullptr, *tot = nullptr;
+  size_t scw = sort_scratch_words(n);
+  if (scan_scratch_words(n) > scw) scw = scan_scratch_words(n);
+  bool ok = cudaMallocAsync(&ka, n * 8, s) == cudaSuccess && cudaMallocAsync(&kb, n * 8, s) == cudaSuccess &&
+            cudaMallocAsync(&va, n * 4, s) == cudaSuccess && cudaMallocAsync(&vb, n * 4, s) == cudaSuccess &&
+            cudaMallocAsync(&scratch, scw * 4, s) == cudaSuccess && cudaMallocAsync(&tot, 64, s) == cudaSuccess;
+  int rc = 0;
+  uint64_t* sk = nullptr;
+  uint32_t* si = nullptr;
+  uint64_t last_key = 0;
+  uint32_t m32 = 0;
+  if (!ok) { rc = -3; goto done; }
+  if (radix_sort_pairs(keys, nullptr, nullptr, ka, va, kb, vb, n, 0, 64, scratch, s, &sk, &si) != cudaSuccess) {
+    rc = -2;
+    goto done;
+  }
+  // reuse the other ping-pong buffers for flags / positions / unique pairs
+  flags = (si == va) ? vb : va;
+  uk = (sk == ka) ? kb : ka;
+  if (cudaMallocAsync(&pos, n * 4, s) != cudaSuccess || cudaMallocAsync(&uv, n * 8, s) != cudaSuccess) {
+    rc = -3;
+    goto done;
+  }
+  tail_flags_kernel<<<blocks_for(n, 256), 256, 0, s>>>(sk, n, flags);
+  count_launch();
+  if (scan_exclusive_u32(flags, pos, n, tot, scratch, s) != cudaSuccess) { rc = -2; goto done; }
+  dedupe_kernel<<<blocks_for(n, 256), 256, 0, s>>>(sk, si, vals, flags, pos, n, uk, uv);
+  count_launch();
+  cudaMemcpyAsync(&m32, tot, 4, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(&last_key, sk + (n - 1), 8, cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) { rc = -2; goto done; }
+  if (last_key == kKeyMax) { rc = -5; goto done; }
+  {
+    const size_t m = m32;
+    const uint32_t lf = h->leaf_fill, per = h->inner_fill + 1;
+    const uint32_t nl = (uint32_t)((m + lf - 1) / lf);
+    // count nodes first (capacity check)
+    uint64_t total = nl;
+    uint32_t cnt = nl, height = 1;
+    while (cnt > 1) {
+      cnt = (cnt + per - 1) / per;
+      total += cnt;
+      height++;
+    }
+    if (total > h->tree.cap) { rc = -4; goto done; }
+    build_leaves_kernel<<<blocks_for((size_t)nl * 32, 256), 256, 0, s>>>(h->tree, uk, uv, m, nl);
+    count_launch();
+    uint32_t first_child = 0, n_children = nl, next = nl, level = 1;
+    while (n_children > 1) {
+      uint32_t nn = (n_children + per - 1) / per;
+      build_inner_kernel<<<blocks_for((size_t)nn * 32, 256), 256, 0, s>>>(h->tree, first_child, n_children, next,
+                                                                          nn, level);
+      count_launch();
+      first_child = next;
+      next += nn;
+      n_children = nn;
+      level++;
+    }
+    set_root_kernel<<<1, 1, 0, s>>>(h->tree.ctrl, first_child, height - 1, (uint32_t)total, (uint64_t)m);
+    count_launch();
+    if (cudaGetLastError() != cudaSuccess) rc = -2;
+  }
+done:
+  cudaFreeAsync(ka, s);
+  cudaFreeAsync(kb, s);
+  cudaFreeAsync(va, s);
+  cudaFreeAsync(vb, s);
+  cudaFreeAsync(scratch, s);
+  cudaFreeAsync(tot, s);
+  if (pos) cudaFreeAsync(pos, s);
+  if (uv) cudaFreeAsync(uv, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess && rc == 0) rc = -2;
+  return rc;
+}
+
+cudaError_t launch_search(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev, size_t n,
+                          uint64_t* out_vals, uint8_t* out_st, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  const int threads = 256;
+  const int G = h->search_group;
+  // enough groups to cover the requests, capped at a few waves of resident blocks
+  size_t groups_needed = n;
+  size_t blocks = (groups_needed * G + threads - 1) / threads;
+  size_t cap = (size_t)h->sm_count * 8 * 4;
+  if (blocks > cap) blocks = cap;
+  if (blocks == 0) blocks = 1;
+  switch (G) {
+    case 4: search_kernel<4, false><<<(unsigned)blocks, threads, 0, s>>>(h->tree, qkeys, list, n_dev, n, out_vals, out_st); break;
+    case 16: search_kernel<16, false><<<(unsigned)blocks, threads, 0, s>>>(h->tree, qkeys, list, n_dev, n, out_vals, out_st); break;
+    case 32: search_kernel<32, false><<<(unsigned)blocks, threads, 0, s>>>(h->tree, qkeys, list, n_dev, n, out_vals, out_st); break;
+    case -8: search_kernel<8, true><<<(unsigned)blocks, threads, 0, s>>>(h->tree, qkeys, list, n_dev, n, out_vals, out_st); break;
+    default: search_kernel<8, false><<<(unsigned)blocks, threads, 0, s>>>(h->tree, qkeys, list, n_dev, n, out_vals, out_st); break;
+  }
+  count_launch();
+  return cudaGetLastError();
+}
+
+static int ensure_enum(Handle* h, size_t n) {
+  if (n <= h->enum_cap) return 0;
+  cudaFree(h->enum_a);
+  cudaFree(h->enum_b);
+  cudaFree(h->enum_cnt);
+  cudaFree(h->enum_scan_scratch);
+  h->enum_a = h->enum_b = h->enum_cnt = h->enum_scan_scratch = nullptr;
+  h->enum_cap = 0;
+  size_t c = n + 64;
+  if (cudaMalloc(&h->enum_a, c * 4) != cudaSuccess || cudaMalloc(&h->enum_b, c * 4) != cudaSuccess ||
+      cudaMalloc(&h->enum_cnt, (c + 1) * 4) != cudaSuccess ||
+      cudaMalloc(&h->enum_scan_scratch, (scan_scratch_words(c) + 1) * 4) != cudaSuccess)
+    return -3;
+  h->enum_cap = c;
+  return 0;
+}
+
+int enumerate_leaves(Handle* h, cudaStream_t s, uint32_t** leaf_ids, size_t* n_leaves) {
+  Ctrl c;
+  if (cudaMemcpyAsync(&c, h->tree.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s) != cudaSuccess) return -2;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return -2;
+  *n_leaves = 0;
+  *leaf_ids = nullptr;
+  h->n_levels = 0;
+  if (c.root == kNil) return 0;
+  h->n_levels = c.root_level + 1;
+  if (h->n_levels <= 48) h->level_counts[c.root_level] = 1;
+  if (ensure_enum(h, c.n_nodes + 1) != 0) return -3;
+  uint32_t* cur = h->enum_a;
+  uint32_t* nxt = h->enum_b;
+  cudaMemcpyAsync(cur, &c.root, 4, cudaMemcpyHostToDevice, s);
+  size_t n = 1;
+  uint32_t* tot = h->enum_cnt + h->enum_cap;  // last word
+  for (uint32_t l = c.root_level; l > 0; l--) {
+    child_count_kernel<<<blocks_for(n, 256), 256, 0, s>>>(h->tree, cur, n, h->enum_cnt, 0);
+    count_launch();
+    if (scan_exclusive_u32(h->enum_cnt, h->enum_cnt, n, tot, h->enum_scan_scratch, s) != cudaSuccess) return -2;
+    child_write_kernel<<<blocks_for(n * 32, 256), 256, 0, s>>>(h->tree, cur, n, h->enum_cnt, nxt);
+    count_launch();
+    uint32_t m = 0;
+    cudaMemcpyAsync(&m, tot, 4, cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return -2;
+    n = m;
+    if (l - 1 < 48) h->level_counts[l - 1] = m;
+    uint32_t* t = cur;
+    cur = nxt;
+    nxt = t;
+  }
+  *leaf_ids = cur;
+  *n_leaves = n;
+  return 0;
+}
+
+cudaError_t leaf_sizes_device(Handle* h, const uint32_t* leaves, size_t n, uint32_t* out, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  child_count_kernel<<<blocks_for(n, 256), 256, 0, s>>>(h->tree, leaves, n, out, 1);
+  count_launch();
+  return cudaGetLastError();
+}
+
+int tree_dump(Handle* h, uint64_t* out_keys, uint64_t* out_vals, size_t cap, size_t* n_out, cudaStream_t s) {
+  uint32_t* leaves = nullptr;
+  size_t nl = 0;
+  int rc = enumerate_leaves(h, s, &leaves, &nl);
+  if (rc) return rc;
+  *n_out = 0;
+  if (nl == 0) return 0;
+  // leaves live in one enum buffer; use the other for sizes
+  uint32_t* sizes = (leaves == h->enum_a) ? h->enum_b : h->enum_a;
+  uint32_t* tot = h->enum_cnt + h->enum_cap;
+  child_count_kernel<<<blocks_for(nl, 256), 256, 0, s>>>(h->tree, leaves, nl, sizes, 1);
+  count_launch();
+  if (scan_exclusive_u32(sizes, sizes, nl, tot, h->enum_scan_scratch, s) != cudaSuccess) return -2;
+  uint32_t total = 0;
+  cudaMemcpyAsync(&total, tot, 4, cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return -2;
+  *n_out = total;
+  if (total > cap) return -4;
+  leaf_dump_kernel<<<blocks_for(nl * 32, 256), 256, 0, s>>>(h->tree, leaves, nl, sizes, out_keys, out_vals);
+  count_launch();
+  if (cudaStreamSynchronize(s) != cudaSuccess) return -2;
+  return 0;
+}
+
+}  // namespace bt

@@ -1,0 +1,193 @@
+/*
+ * eirene_b200 -- C ABI of the B200 batched B+tree (bulk build, batched point
+ * search, batched insert under warp-level STM, sort-based batch merge,
+ * learned leaf predictor).
+ *
+ * The reference exposes this path as the C++ virtual class GPU_BTree
+ * (src/tree.h:28-43) implemented by gpu_stm_nsp_39::GPU_STM_Tree and
+ * gpu_stm_nsp_38::GPU_STM_Tree; there is no C ABI in the reference.  Each entry
+ * point below names the reference member it replaces (paths are relative to
+ * the reference project root).
+ *
+ * Conventions
+ *   - Keys and values are uint64.  Key UINT64_MAX is reserved (the reference
+ *     reserves INT_MAX as MAX_KEY, src/gpu-stm-tree-v39/bpt-gpustm.h:20).
+ *   - Unless an entry point says "host", every pointer is a device pointer and
+ *     the caller owns the buffer.  `stream` is a cudaStream_t (NULL = legacy
+ *     default stream); calls are stream ordered and return before the work
+ *     finishes unless documented as synchronous.
+ *   - Every entry point returns BT_OK (0) or a negative BT_ERR_* code and
+ *     never exits the process (the reference prints and calls exit(1),
+ *     src/cuda_utils.h:3-12).  No C++ exception crosses this boundary.
+ *   - A handle is not thread-safe; use one handle per host thread or lock.
+ */
+#ifndef EIRENE_B200_H
+#define EIRENE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define BT_OK 0
+#define BT_ERR_INVALID_ARG -1
+#define BT_ERR_CUDA -2
+#define BT_ERR_NO_MEMORY -3
+#define BT_ERR_CAPACITY -4        /* node pool exhausted */
+#define BT_ERR_RESERVED_KEY -5    /* UINT64_MAX given as a key to bt_bulk_build */
+#define BT_ERR_BATCH_TOO_LARGE -6 /* n > bt_config.max_batch */
+#define BT_ERR_NOT_TRAINED -7     /* learned descent requested before bt_retrain */
+
+/* ---- request op codes (same numbering as src/input-helper.h:14-17) ---- */
+#define BT_OP_INSERT 0
+#define BT_OP_GET 1
+
+/* ---- per-request status byte written to out_status ---- */
+#define BT_ST_ABSENT 0          /* key was not present (out_vals = 0) */
+#define BT_ST_FOUND 1           /* key was present; out_vals = its (previous) value */
+#define BT_ST_REJECTED 2        /* reserved key or unknown op; no effect */
+#define BT_ST_RETRY_EXHAUSTED 3 /* STM insert could not commit within retry_limit; no effect */
+#define BT_ST_NO_CAPACITY 4     /* node pool exhausted; no effect */
+
+/* ---- batch modes (bt_execute_batch `mode`) ---- */
+#define BT_MODE_SORTED 0      /* sort-based batch merge, deterministic (reference v38 meaning) */
+#define BT_MODE_STM 1         /* unsorted warp-per-request STM (reference v39 meaning) */
+#define BT_MODE_MERGE_ENGINE 0x10 /* with BT_MODE_SORTED: apply new keys by segmented leaf merge */
+
+/* ---- descent (bt_set_descent) ---- */
+#define BT_DESCENT_PLAIN 0
+#define BT_DESCENT_LEARNED 1
+
+typedef struct bt_config {
+    uint64_t max_keys;     /* node pool sized for this many keys (default 1<<20) */
+    uint64_t max_batch;    /* largest batch accepted (default 1<<22) */
+    uint32_t leaf_fill;    /* keys per leaf for bulk build and merge splits (default 24) */
+    uint32_t inner_fill;   /* keys per inner node for bulk build and merge splits (default 24) */
+    uint32_t retry_limit;  /* STM attempts per request before BT_ST_RETRY_EXHAUSTED (default 65536) */
+    int32_t device;        /* CUDA device ordinal (default 0) */
+    uint32_t search_group; /* lanes per request in the search kernel: 4, 8, 16 or 32 (default 8) */
+    uint32_t n_segments;   /* learned predictor: leaf segments (default 4096) */
+    uint32_t window;       /* learned predictor: max error window in leaf slots (default 64) */
+    uint32_t reserved[7];
+} bt_config;
+
+typedef struct bt_stats {
+    uint64_t n_keys;
+    uint64_t n_nodes;
+    uint64_t n_leaves;        /* filled by bt_stats_get when with_leaves != 0 */
+    uint32_t height;          /* levels including the leaf level, 0 when empty */
+    uint32_t error;           /* sticky device error bits: 1 capacity, 2 retry limit */
+    uint64_t commits;         /* STM commits */
+    uint64_t aborts;          /* STM aborts (reference ABORT_COUNT roll_back_times) */
+    uint64_t leaf_splits;
+    uint64_t inner_splits;
+    uint64_t new_roots;
+    uint64_t retry_exhausted;
+    uint64_t learned_hits;       /* learned descents that answered from the predicted leaf */
+    uint64_t learned_fallbacks;  /* learned descents that fell back to the root descent */
+    uint64_t learned_probe_sum;  /* sum of |predicted slot - true slot| over hits */
+    uint64_t capacity_nodes;
+} bt_stats;
+
+typedef struct bt_handle bt_handle;
+
+/* Fill `cfg` with defaults.  No reference counterpart (compile-time constants
+ * in src/gpu-stm-tree-v39/bpt-gpustm.h:20-38). */
+int bt_config_init(bt_config *cfg);
+
+/* Allocate the node pool and batch work buffers on cfg->device.
+ * Replaces GPU_STM_Tree::prepareGPU (src/gpu-stm-tree-v39/bpt-gpustm.cpp:14-28). */
+int bt_create(const bt_config *cfg, bt_handle **out);
+
+/* Free everything.  The reference never frees (~GPU_STM_Tree(){} ,
+ * src/gpu-stm-tree-v39/bpt-gpustm.h:145). */
+int bt_destroy(bt_handle *h);
+
+/* Replace the tree contents with the n pairs (the last value wins for a repeated
+ * key).  Synchronous.  The reference builds by running gpu_work() over a file of
+ * P lines (src/main.cpp:21-25, src/gpu-stm-tree-v39/bpt-gpustm.cpp:67-132). */
+int bt_bulk_build(bt_handle *h, const uint64_t *keys, const uint64_t *vals, size_t n, void *stream);
+
+/* Run one batch of n requests.  out_vals[i]/out_status[i] answer request i:
+ * GET -> value or absent; INSERT -> previous value or absent, then insert or
+ * update (src/input-helper.h:27-38).  Replaces gpu_work_main's per-batch
+ * transferData/launchKernel/transferAns (src/gpu-stm-tree-v39/bpt-gpustm.cpp:78-105;
+ * v38: src/gpu-stm-tree-v38/bpt-gpustm.cpp:88-112). */
+int bt_execute_batch(bt_handle *h, const uint64_t *keys, const uint64_t *vals, const uint8_t *ops,
+                     uint64_t *out_vals, uint8_t *out_status, size_t n, int mode, void *stream);
+
+/* Same as bt_execute_batch with HOST buffers: copies in, runs, copies out and
+ * synchronises `stream`.  Pinned buffers (bt_host_alloc) give full PCIe speed.
+ * Mirrors the reference's transferData -> kernel -> transferAns loop body. */
+int bt_execute_batch_host(bt_handle *h, const uint64_t *keys, const uint64_t *vals, const uint8_t *ops,
+                          uint64_t *out_vals, uint8_t *out_status, size_t n, int mode, void *stream);
+
+/* Convenience wrappers: all-GET and all-INSERT batches in BT_MODE_SORTED. */
+int bt_search_batch(bt_handle *h, const uint64_t *keys, uint64_t *out_vals, uint8_t *out_status, size_t n,
+                    void *stream);
+int bt_insert_batch(bt_handle *h, const uint64_t *keys, const uint64_t *vals, uint64_t *out_vals,
+                    uint8_t *out_status, size_t n, void *stream);
+
+/* Number of keys (synchronous). */
+int bt_size(bt_handle *h, uint64_t *n_keys);
+
+/* All pairs in ascending key order into device buffers of `cap` entries;
+ * *n_out = number of pairs.  Synchronous.  Replaces the reference's -t answer
+ * print (src/input-helper.h:205-218) as the parity format. */
+int bt_dump_sorted(bt_handle *h, uint64_t *keys, uint64_t *vals, size_t cap, size_t *n_out, void *stream);
+
+/* Host arrays: leaf sizes in key order (cap entries) and node counts per level
+ * (leaf level first).  Synchronous.  Used to check split counts. */
+int bt_leaf_sizes(bt_handle *h, uint32_t *sizes_host, size_t cap, size_t *n_leaves);
+int bt_level_counts(bt_handle *h, uint64_t *counts_host, uint32_t cap, uint32_t *height);
+
+/* Counters (synchronous).  with_leaves != 0 also enumerates the leaves.
+ * Reference: ABORT_COUNT counters (src/gpu-stm-tree-v39/bpt-gpustm.cpp:111-129). */
+int bt_stats_get(bt_handle *h, bt_stats *st, int with_leaves);
+int bt_stats_reset(bt_handle *h);
+
+/* Learned leaf predictor (no reference counterpart: the reference's closest
+ * structure is v35's leaf array, src/gpu-stm-tree-v35/bpt-gpustm-kernel.cu:135-152).
+ * bt_retrain rebuilds the leaf array and trains the model on the GPU
+ * (synchronous); bt_set_descent picks plain or learned search. */
+int bt_retrain(bt_handle *h, void *stream);
+int bt_set_descent(bt_handle *h, int descent);
+/* stage 1 root model: 1 = 1->32->1 MLP (default), 0 = linear */
+int bt_set_root_model(bt_handle *h, int mlp);
+int bt_set_search_group(bt_handle *h, uint32_t lanes);
+
+/* Phase timing with CUDA events recorded on the batch's stream between the
+ * phases of BT_MODE_SORTED (0 sort, 1 merge, 2 search, 3 insert, 4 writeback),
+ * like the reference's Time_Measure (src/time_measure.cuh:14-42,
+ * src/gpu-stm-tree-v38/bpt-gpustm-kernel.cu:289-324).  bt_profile_read
+ * synchronises on the recorded events and returns summed milliseconds. */
+int bt_profile(bt_handle *h, int enable);
+int bt_profile_read(bt_handle *h, double *phase_ms /* [5] */, uint64_t *batches, int reset);
+/* Kernels launched by this library in this process so far. */
+uint64_t bt_launch_count(void);
+
+/* Pinned host memory helpers for bt_execute_batch_host callers. */
+int bt_host_alloc(void **p, size_t bytes);
+int bt_host_free(void *p);
+
+/* ---- benchmark input generators (seeded, counter based; device output) ----
+ * dist: 0 uniform keys in [0, 2^63), 1 Zipf(0.99) ranks over 2^32 hashed to
+ * uint64 (bt_gen_keys returns the n most popular ranks), 2 Normal(2^62, 2^58),
+ * 3 Gamma(2, 2^56).  vals (nullable) receives key ^ 0x9E3779B97F4A7C15.
+ * bt_gen_requests: search_pct % GETs, half of them keys of tree_keys; the rest
+ * INSERTs of fresh keys.  These stand in for the reference's dataset files,
+ * which are not shipped (evalutaion/random_testall_v39.sh:9-28). */
+int bt_gen_keys(int dist, uint64_t seed, size_t n, uint64_t *keys, uint64_t *vals, void *stream);
+int bt_gen_requests(int dist, uint64_t seed, const uint64_t *tree_keys, size_t n_tree, size_t n,
+                    uint32_t search_pct, uint64_t *keys, uint64_t *vals, uint8_t *ops, void *stream);
+
+/* Static text for a status code. */
+const char *bt_status_string(int code);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EIRENE_B200_H */
