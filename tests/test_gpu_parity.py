@@ -186,8 +186,8 @@ def test_batch_too_large_rejected(gpu):
 
 def test_pool_exhaustion_reports_status(gpu):
     # a pool too small for the inserts: requests report NO_CAPACITY, nothing corrupts
-    t = E.BTree(max_keys=0, max_batch=1 << 16)  # pool = 4096 nodes
-    rk = np.arange(1, 200_001, dtype=np.uint64)[:65536] * np.uint64(7)
+    t = E.BTree(max_keys=0, max_batch=1 << 16)  # pool = 4096 nodes, at most 4096 * 31 keys
+    rk = np.arange(1, 4 * 65536 + 1, dtype=np.uint64) * np.uint64(7)
     st_all = []
     for c in range(0, rk.size, 16384):
         k = rk[c:c + 16384]
