@@ -24,7 +24,9 @@ ERRORS = {
     -5: "reserved key UINT64_MAX",
     -6: "batch larger than max_batch",
     -7: "learned predictor not trained",
+    -8: "more keys than BT_STATIC_BUILD_MAX_KEYS",
 }
+STATIC_BUILD_MAX_KEYS = 65536
 OP_INSERT, OP_GET = 0, 1
 ST_ABSENT, ST_FOUND, ST_REJECTED, ST_RETRY_EXHAUSTED, ST_NO_CAPACITY = 0, 1, 2, 3, 4
 MODE_SORTED, MODE_STM, MODE_MERGE_ENGINE = 0, 1, 0x10
@@ -80,7 +82,7 @@ EXPORTS = [
     "bt_search_batch", "bt_insert_batch", "bt_size", "bt_dump_sorted", "bt_leaf_sizes", "bt_level_counts",
     "bt_stats_get", "bt_stats_reset", "bt_retrain", "bt_set_descent", "bt_set_root_model", "bt_set_search_group",
     "bt_host_alloc", "bt_host_free", "bt_gen_keys", "bt_gen_requests", "bt_status_string",
-    "bt_profile", "bt_profile_read", "bt_launch_count",
+    "bt_profile", "bt_profile_read", "bt_launch_count", "bt_bulk_build_static",
 ]
 PHASES = ["sort", "merge", "search", "insert", "writeback"]
 
@@ -130,6 +132,7 @@ def lib():
             "bt_profile": [_P, ctypes.c_int],
             "bt_profile_read": [_P, _P, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int],
             "bt_launch_count": [],
+            "bt_bulk_build_static": [_P, _P, _P, _SZ, _P],
         }
         for name, args in sig.items():
             f = getattr(L, name)

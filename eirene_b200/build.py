@@ -23,6 +23,7 @@ SOURCES = [
     "bt_learned.cu",
     "bt_api.cu",
     "bt_workload.cu",
+    "bt_static.cu",
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -9,9 +9,6 @@
 #include "bt_common.cuh"
 #include "bt_internal.h"
 
-struct bt_handle {
-  bt::Handle h;
-};
 
 namespace {
 
@@ -412,6 +409,7 @@ const char* bt_status_string(int code) {
     case BT_ERR_RESERVED_KEY: return "reserved key UINT64_MAX";
     case BT_ERR_BATCH_TOO_LARGE: return "batch larger than max_batch";
     case BT_ERR_NOT_TRAINED: return "learned predictor not trained";
+    case BT_ERR_STATIC_LIMIT: return "more keys than BT_STATIC_BUILD_MAX_KEYS";
     default: return "unknown status";
   }
 }

@@ -122,6 +122,20 @@ void prof_mark(Handle* h, int which, cudaStream_t s);
 // ---- tree kernels (bt_tree.cu) ----
 cudaError_t tree_reset(Handle* h, cudaStream_t s);
 int tree_bulk_build(Handle* h, const uint64_t* keys, const uint64_t* vals, size_t n, cudaStream_t s);
+// caller-provided scratch for the bulk build (used by the no-allocation entry point)
+struct BuildScratch {
+  uint64_t* ka;
+  uint64_t* kb;
+  uint32_t* va;
+  uint32_t* vb;
+  uint32_t* sort_scratch;  // sort_scratch_words(cap) words (>= scan_scratch_words(cap))
+  uint32_t* pos;
+  uint64_t* uv;
+  uint32_t* tot;  // one word
+  size_t cap;     // keys
+};
+int tree_bulk_build_scratch(Handle* h, const uint64_t* keys, const uint64_t* vals, size_t n, cudaStream_t s,
+                            const BuildScratch& sc);
 cudaError_t launch_search(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev, size_t n,
                           uint64_t* out_vals, uint8_t* out_st, cudaStream_t s);
 // ids of the leaves in key order; returns count (synchronises the stream)
@@ -148,3 +162,8 @@ cudaError_t launch_learned_search(Handle* h, const uint64_t* qkeys, const uint32
                                   size_t n, uint64_t* out_vals, uint8_t* out_st, cudaStream_t s);
 
 }  // namespace bt
+
+// the opaque handle of the C ABI
+struct bt_handle {
+  bt::Handle h;
+};

@@ -312,6 +312,63 @@ done:
   return rc;
 }
 
+// Same bulk build with the scratch supplied by the caller (nothing allocated
+// here); used by bt_bulk_build_static.  Packing rule identical to
+// tree_bulk_build above.
+int tree_bulk_build_scratch(Handle* h, const uint64_t* keys, const uint64_t* vals, size_t n, cudaStream_t s,
+                            const BuildScratch& sc) {
+  if (n > sc.cap) return -6;
+  if (tree_reset(h, s) != cudaSuccess) return -2;
+  if (n == 0) return cudaStreamSynchronize(s) == cudaSuccess ? 0 : -2;
+  uint64_t* sk = nullptr;
+  uint32_t* si = nullptr;
+  if (radix_sort_pairs(keys, nullptr, nullptr, sc.ka, sc.va, sc.kb, sc.vb, n, 0, 64, sc.sort_scratch, s, &sk, &si) !=
+      cudaSuccess)
+    return -2;
+  uint32_t* flags = (si == sc.va) ? sc.vb : sc.va;
+  uint64_t* uk = (sk == sc.ka) ? sc.kb : sc.ka;
+  tail_flags_kernel<<<blocks_for(n, 256), 256, 0, s>>>(sk, n, flags);
+  count_launch();
+  if (scan_exclusive_u32(flags, sc.pos, n, sc.tot, sc.sort_scratch, s) != cudaSuccess) return -2;
+  dedupe_kernel<<<blocks_for(n, 256), 256, 0, s>>>(sk, si, vals, flags, sc.pos, n, uk, sc.uv);
+  count_launch();
+  uint32_t m32 = 0;
+  uint64_t last_key = 0;
+  if (cudaMemcpyAsync(&m32, sc.tot, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaMemcpyAsync(&last_key, sk + (n - 1), 8, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return -2;
+  if (last_key == kKeyMax) return -5;
+  const size_t m = m32;
+  const uint32_t lf = h->leaf_fill, per = h->inner_fill + 1;
+  const uint32_t nl = (uint32_t)((m + lf - 1) / lf);
+  uint64_t total = nl;
+  uint32_t cnt = nl, height = 1;
+  while (cnt > 1) {
+    cnt = (cnt + per - 1) / per;
+    total += cnt;
+    height++;
+  }
+  if (total > h->tree.cap) return -4;
+  build_leaves_kernel<<<blocks_for((size_t)nl * 32, 256), 256, 0, s>>>(h->tree, uk, sc.uv, m, nl);
+  count_launch();
+  uint32_t first_child = 0, n_children = nl, next = nl, level = 1;
+  while (n_children > 1) {
+    const uint32_t nn = (n_children + per - 1) / per;
+    build_inner_kernel<<<blocks_for((size_t)nn * 32, 256), 256, 0, s>>>(h->tree, first_child, n_children, next, nn,
+                                                                        level);
+    count_launch();
+    first_child = next;
+    next += nn;
+    n_children = nn;
+    level++;
+  }
+  set_root_kernel<<<1, 1, 0, s>>>(h->tree.ctrl, first_child, height - 1, (uint32_t)total, (uint64_t)m);
+  count_launch();
+  if (cudaGetLastError() != cudaSuccess) return -2;
+  return cudaStreamSynchronize(s) == cudaSuccess ? 0 : -2;
+}
+
 cudaError_t launch_search(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev, size_t n,
                           uint64_t* out_vals, uint8_t* out_st, cudaStream_t s) {
   if (n == 0) return cudaSuccess;

@@ -40,6 +40,7 @@ extern "C" {
 #define BT_ERR_RESERVED_KEY -5    /* UINT64_MAX given as a key to bt_bulk_build */
 #define BT_ERR_BATCH_TOO_LARGE -6 /* n > bt_config.max_batch */
 #define BT_ERR_NOT_TRAINED -7     /* learned descent requested before bt_retrain */
+#define BT_ERR_STATIC_LIMIT -8    /* n > BT_STATIC_BUILD_MAX_KEYS in bt_bulk_build_static */
 
 /* ---- request op codes (same numbering as src/input-helper.h:14-17) ---- */
 #define BT_OP_INSERT 0
@@ -110,6 +111,22 @@ int bt_destroy(bt_handle *h);
  * key).  Synchronous.  The reference builds by running gpu_work() over a file of
  * P lines (src/main.cpp:21-25, src/gpu-stm-tree-v39/bpt-gpustm.cpp:67-132). */
 int bt_bulk_build(bt_handle *h, const uint64_t *keys, const uint64_t *vals, size_t n, void *stream);
+
+/* bt_bulk_build without any allocation, for callers that must not allocate GPU
+ * memory while they load a tree: services whose device memory is reserved up
+ * front by another allocator (a caching allocator or a start-up pool), where a
+ * cudaMalloc at request time fails or fragments that pool, and latency-critical
+ * threads, since cudaFree synchronises the whole device.  Same result as
+ * bt_bulk_build.  Its scratch is a fixed device array inside the library
+ * (about 2.3 MB, held on every GPU that loads the library until the process
+ * exits), so n may be at most BT_STATIC_BUILD_MAX_KEYS, else
+ * BT_ERR_STATIC_LIMIT.  All calls on a device share that array: calls that
+ * overlap on the GPU race, so serialise them.  The first call on a device
+ * looks up the array's device address; make that first call before any stream
+ * capture on the device.  Synchronous.  This entry point has no counterpart in
+ * the reference. */
+#define BT_STATIC_BUILD_MAX_KEYS 65536
+int bt_bulk_build_static(bt_handle *h, const uint64_t *keys, const uint64_t *vals, size_t n, void *stream);
 
 /* Run one batch of n requests.  out_vals[i]/out_status[i] answer request i:
  * GET -> value or absent; INSERT -> previous value or absent, then insert or
