@@ -261,8 +261,12 @@ def main():
     def run_form(learned: bool, seed0: int):
         batches = make_batches(seed0)
         counts = [unique_op_counts(torch, k, o) for (k, v, o) in batches[args.warmup:]]
+        info = None
         if learned:
+            t_r = time.time()
             tree.retrain(stream)
+            info = tree.learned_info()
+            info["retrain_s"] = time.time() - t_r
             tree.set_descent(True)
         else:
             tree.set_descent(False)
@@ -291,7 +295,7 @@ def main():
         st = tree.stats()
         del batches
         return {"total_ms": total_ms, "step_ms": step_ms, "phases": phases, "counts": counts,
-                "launches": launches, "clocks": clocks, "stats": st}
+                "launches": launches, "clocks": clocks, "stats": st, "learned_info": info}
 
     forms = {}
     if args.descent in ("plain", "both"):
@@ -389,6 +393,7 @@ def main():
                 "stm_aborts": s["aborts"], "stm_commits": s["commits"],
                 "learned_hits": s["learned_hits"], "learned_fallbacks": s["learned_fallbacks"],
                 "mean_probe": s["learned_probe_sum"] / max(1, s["learned_hits"]),
+                "model": F.get("learned_info"),
             }
 
         line = {

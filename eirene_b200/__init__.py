@@ -83,6 +83,7 @@ EXPORTS = [
     "bt_stats_get", "bt_stats_reset", "bt_retrain", "bt_set_descent", "bt_set_root_model", "bt_set_search_group",
     "bt_host_alloc", "bt_host_free", "bt_gen_keys", "bt_gen_requests", "bt_status_string",
     "bt_profile", "bt_profile_read", "bt_launch_count", "bt_bulk_build_static",
+    "bt_set_learned_group", "bt_learned_info", "bt_mlp_grad",
 ]
 PHASES = ["sort", "merge", "search", "insert", "writeback"]
 
@@ -133,6 +134,9 @@ def lib():
             "bt_profile_read": [_P, _P, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int],
             "bt_launch_count": [],
             "bt_bulk_build_static": [_P, _P, _P, _SZ, _P],
+            "bt_set_learned_group": [_P, ctypes.c_uint32],
+            "bt_learned_info": [_P, _P],
+            "bt_mlp_grad": [_P, _P, _P, _P, _SZ, _P, _P, _P],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -291,6 +295,19 @@ class BTree:
         b = ctypes.c_uint64(0)
         _check(lib().bt_profile_read(self._h, ms, ctypes.byref(b), 1 if reset else 0), "bt_profile_read")
         return {"batches": b.value, **{p: ms[i] for i, p in enumerate(PHASES)}}
+
+    def set_learned_group(self, lanes: int):
+        _check(lib().bt_set_learned_group(self._h, lanes), "bt_set_learned_group")
+
+    def learned_info(self) -> dict:
+        a = (ctypes.c_double * 8)()
+        _check(lib().bt_learned_info(self._h, a), "bt_learned_info")
+        keys = ["valid", "n_leaves", "n_segments", "segments_over_window", "window", "loss", "root_mlp", "steps"]
+        return {k: a[i] for i, k in enumerate(keys)}
+
+    def mlp_grad(self, params, x, y, grad_out, loss_out, stream=None):
+        _check(lib().bt_mlp_grad(self._h, _ptr(params), _ptr(x), _ptr(y), x.numel(), _ptr(grad_out),
+                                 _ptr(loss_out), _stream_ptr(stream)), "bt_mlp_grad")
 
     def set_search_group(self, lanes: int):
         _check(lib().bt_set_search_group(self._h, lanes), "bt_set_search_group")

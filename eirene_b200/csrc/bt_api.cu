@@ -392,6 +392,34 @@ int bt_profile_read(bt_handle* H, double* phase_ms, uint64_t* batches, int reset
 
 uint64_t bt_launch_count(void) { return bt::g_launches.load(); }
 
+int bt_set_learned_group(bt_handle* H, uint32_t lanes) {
+  if (!H) return BT_ERR_INVALID_ARG;
+  if (lanes != 8 && lanes != 16 && lanes != 32) return BT_ERR_INVALID_ARG;
+  H->h.learned_group = (int)lanes;
+  return BT_OK;
+}
+
+int bt_learned_info(bt_handle* H, double* info) {
+  if (!H || !info) return BT_ERR_INVALID_ARG;
+  const bt::Learned& L = H->h.L;
+  info[0] = L.valid ? 1.0 : 0.0;
+  info[1] = (double)L.n_leaves;
+  info[2] = (double)L.n_segments;
+  info[3] = (double)L.seg_fallback;
+  info[4] = (double)L.window;
+  info[5] = L.last_loss;
+  info[6] = (double)L.stage1;
+  info[7] = (double)L.train_steps;
+  return BT_OK;
+}
+
+int bt_mlp_grad(bt_handle* H, const float* params, const float* x, const float* y, size_t n, float* grad_out,
+                float* loss_out, void* stream) {
+  if (!H || !params || !x || !y || !grad_out || !loss_out || n == 0) return BT_ERR_INVALID_ARG;
+  DeviceGuard g(H->h.device);
+  return map_internal(bt::learned_mlp_grad(&H->h, params, x, y, n, grad_out, loss_out, S(stream)));
+}
+
 int bt_host_alloc(void** p, size_t bytes) {
   if (!p) return BT_ERR_INVALID_ARG;
   return cudaMallocHost(p, bytes ? bytes : 1) == cudaSuccess ? BT_OK : BT_ERR_NO_MEMORY;

@@ -96,6 +96,7 @@ struct Handle {
   uint32_t retry_limit = 1u << 16;
   int descent = 0;     // 0 plain, 1 learned
   int search_group = 8;  // lanes per request in the lock-free search
+  int learned_group = 32;  // lanes per request in the learned search
   int sm_count = 148;
   Work w;
   Learned L;
@@ -160,6 +161,8 @@ int learned_retrain(Handle* h, cudaStream_t s);
 void learned_free(Learned* L);
 cudaError_t launch_learned_search(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev,
                                   size_t n, uint64_t* out_vals, uint8_t* out_st, cudaStream_t s);
+int learned_mlp_grad(Handle* h, const float* params, const float* x, const float* y, size_t n, float* grad_out,
+                     float* loss_out, cudaStream_t s);
 
 }  // namespace bt
 

@@ -1,0 +1,91 @@
+// Grouped lock-free descent shared by the plain search kernel and the learned
+// search's fallback.  A group of G lanes serves one request; each lane owns
+// S = 32/G consecutive slots of a node row and loads them with 16-byte loads
+// through the read-only path (valid only while no writer runs: the batch
+// executor never overlaps this with the STM insert phase).
+#pragma once
+#include "bt_common.cuh"
+
+namespace bt {
+
+template <int G>
+__device__ __forceinline__ uint32_t group_mask(uint32_t lane) {
+  if constexpr (G == 32) return 0xffffffffu;
+  else return ((1u << G) - 1u) << (lane - lane % G);
+}
+
+template <int S>
+__device__ __forceinline__ void load_slots(const uint64_t* p, uint64_t (&x)[S]) {
+  if constexpr (S == 1) {
+    x[0] = __ldg(p);
+  } else {
+#pragma unroll
+    for (int i = 0; i < S; i += 2) {
+      ulonglong2 w = __ldg(reinterpret_cast<const ulonglong2*>(p + i));
+      x[i] = w.x;
+      x[i + 1] = w.y;
+    }
+  }
+}
+
+template <int S>
+__device__ __forceinline__ uint64_t pick(const uint64_t (&x)[S], uint32_t e) {
+  uint64_t r = x[0];
+#pragma unroll
+  for (int i = 1; i < S; i++)
+    if (e == (uint32_t)i) r = x[i];
+  return r;
+}
+
+template <int G>
+__device__ __forceinline__ uint32_t group_sum(uint32_t c, uint32_t gmask) {
+#pragma unroll
+  for (int o = G / 2; o >= 1; o >>= 1) c += __shfl_xor_sync(gmask, c, o, G);
+  return c;
+}
+
+// Look `key` up in leaf `node` (slots loaded by the group); returns the status
+// and the value (deferred 32 B load of the one matching slot).
+template <int G, bool kLeafVals>
+__device__ __forceinline__ uint8_t group_leaf_lookup(const DevTree& t, uint32_t node, uint64_t key, uint32_t g,
+                                                     uint32_t gmask, const uint64_t (&k)[32 / G],
+                                                     const uint64_t (&v)[32 / G], uint32_t cnt, uint64_t& ans) {
+  constexpr int S = 32 / G;
+  ans = 0;
+  if (cnt == 0) return kAbsent;
+  const uint32_t slot = cnt - 1;
+  const uint32_t owner = slot / S, e = slot % S;
+  const uint64_t kk = __shfl_sync(gmask, pick<S>(k, e), owner, G);
+  if (kk != key) return kAbsent;
+  if (kLeafVals) ans = __shfl_sync(gmask, pick<S>(v, e), owner, G);
+  else ans = (g == 0) ? __ldg(t.vals + (size_t)node * 32 + slot) : 0;
+  return kFound;
+}
+
+// Root-to-leaf descent: child slot = number of keys <= target (child i covers
+// [key[i-1], key[i]), src/tree.h:7-19).
+template <int G, bool kLeafVals>
+__device__ __forceinline__ uint8_t group_descend(const DevTree& t, uint32_t node, uint32_t level, uint64_t key,
+                                                 uint32_t g, uint32_t gmask, uint64_t& ans) {
+  constexpr int S = 32 / G;
+  uint64_t k[S];
+  uint64_t v[S];
+  uint32_t cnt;
+  for (;;) {
+    const size_t row = (size_t)node * 32 + g * S;
+    load_slots<S>(t.keys + row, k);
+    if (level > 0 || kLeafVals) load_slots<S>(t.vals + row, v);
+    if (g == G - 1) k[S - 1] = kKeyMax;  // slot 31 holds the header
+    uint32_t c = 0;
+#pragma unroll
+    for (int i = 0; i < S; i++) c += (k[i] <= key) ? 1u : 0u;
+    cnt = group_sum<G>(c, gmask);
+    if (level == 0) break;
+    const uint64_t mine = pick<S>(v, cnt % S);
+    node = (uint32_t)__shfl_sync(gmask, mine, cnt / S, G);
+    level--;
+  }
+  return group_leaf_lookup<G, kLeafVals>(t, node, key, g, gmask, k, v, cnt, ans);
+}
+
+}  // namespace bt

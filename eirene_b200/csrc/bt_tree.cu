@@ -15,6 +15,7 @@
 
 #include "bt_common.cuh"
 #include "bt_internal.h"
+#include "bt_search.cuh"
 
 namespace bt {
 
@@ -97,39 +98,14 @@ __global__ void set_root_kernel(Ctrl* c, uint32_t root, uint32_t root_level, uin
 }
 
 // --------------------------------------------------------------- search ----
-template <int S>
-__device__ __forceinline__ void load_slots(const uint64_t* p, uint64_t (&x)[S]) {
-  if constexpr (S == 1) {
-    x[0] = __ldg(p);
-  } else {
-#pragma unroll
-    for (int i = 0; i < S; i += 2) {
-      ulonglong2 w = __ldg(reinterpret_cast<const ulonglong2*>(p + i));
-      x[i] = w.x;
-      x[i + 1] = w.y;
-    }
-  }
-}
-
-template <int S>
-__device__ __forceinline__ uint64_t pick(const uint64_t (&x)[S], uint32_t e) {
-  uint64_t r = x[0];
-#pragma unroll
-  for (int i = 1; i < S; i++)
-    if (e == (uint32_t)i) r = x[i];
-  return r;
-}
-
 template <int G, bool kLeafVals>
 __global__ void __launch_bounds__(256) search_kernel(DevTree t, const uint64_t* __restrict__ qkeys,
                                                      const uint32_t* __restrict__ list,
                                                      const uint32_t* __restrict__ n_dev, size_t n_host,
                                                      uint64_t* __restrict__ out_vals, uint8_t* __restrict__ out_st) {
-  constexpr int S = 32 / G;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t g = lane % G;
-  const uint32_t gbase = lane - g;
-  const uint32_t gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << gbase);
+  const uint32_t gmask = group_mask<G>(lane);
   const size_t n = n_dev ? (size_t)*n_dev : n_host;
   const uint32_t root = t.ctrl->root;
   const uint32_t root_level = t.ctrl->root_level;
@@ -139,42 +115,8 @@ __global__ void __launch_bounds__(256) search_kernel(DevTree t, const uint64_t* 
     const uint64_t key = __ldg(qkeys + r);
     uint8_t st = kAbsent;
     uint64_t ans = 0;
-    if (key == kKeyMax) {
-      st = kRejected;
-    } else if (root != kNil) {
-      uint32_t node = root;
-      uint32_t level = root_level;
-      uint64_t k[S];
-      uint64_t v[S];
-      uint32_t cnt;
-      for (;;) {
-        const size_t row = (size_t)node * 32 + g * S;
-        load_slots<S>(t.keys + row, k);
-        if (level > 0 || kLeafVals) load_slots<S>(t.vals + row, v);
-        if (g == G - 1) k[S - 1] = kKeyMax;  // slot 31 holds the header
-        uint32_t c = 0;
-#pragma unroll
-        for (int i = 0; i < S; i++) c += (k[i] <= key) ? 1u : 0u;
-#pragma unroll
-        for (int o = G / 2; o >= 1; o >>= 1) c += __shfl_xor_sync(gmask, c, o, G);
-        cnt = c;
-        if (level == 0) break;
-        const uint64_t mine = pick<S>(v, cnt % S);
-        node = (uint32_t)__shfl_sync(gmask, mine, cnt / S, G);
-        level--;
-      }
-      // leaf: the key, if present, sits at slot cnt-1
-      if (cnt > 0) {
-        const uint32_t slot = cnt - 1;
-        const uint32_t owner = slot / S, e = slot % S;
-        const uint64_t kk = __shfl_sync(gmask, pick<S>(k, e), owner, G);
-        if (kk == key) {
-          st = kFound;
-          if (kLeafVals) ans = __shfl_sync(gmask, pick<S>(v, e), owner, G);
-          else ans = (g == 0) ? __ldg(t.vals + (size_t)node * 32 + slot) : 0;
-        }
-      }
-    }
+    if (key == kKeyMax) st = kRejected;
+    else if (root != kNil) st = group_descend<G, kLeafVals>(t, root, root_level, key, g, gmask, ans);
     if (g == 0) {
       out_vals[r] = ans;
       out_st[r] = st;

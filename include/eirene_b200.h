@@ -175,6 +175,17 @@ int bt_set_descent(bt_handle *h, int descent);
 /* stage 1 root model: 1 = 1->32->1 MLP (default), 0 = linear */
 int bt_set_root_model(bt_handle *h, int mlp);
 int bt_set_search_group(bt_handle *h, uint32_t lanes);
+/* lanes per request in the learned search kernel: 8, 16 or 32 (default 32) */
+int bt_set_learned_group(bt_handle *h, uint32_t lanes);
+/* info[8]: valid, n_leaves, n_segments, segments over the window, window,
+ * final training loss, root model (1 MLP, 0 linear), training steps */
+int bt_learned_info(bt_handle *h, double *info);
+/* Gradient of the mean-squared error of the 1->32->1 MLP (params packed
+ * w1[32] b1[32] w2[32] b2) over n device pairs (x, y), computed by the same
+ * kernels that train the model; grad_out[97] and *loss_out are device
+ * pointers.  Used to check the training kernels against the CPU oracle. */
+int bt_mlp_grad(bt_handle *h, const float *params, const float *x, const float *y, size_t n, float *grad_out,
+                float *loss_out, void *stream);
 
 /* Phase timing with CUDA events recorded on the batch's stream between the
  * phases of BT_MODE_SORTED (0 sort, 1 merge, 2 search, 3 insert, 4 writeback),

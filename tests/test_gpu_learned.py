@@ -1,0 +1,126 @@
+"""Learned leaf predictor on the GPU: gradient check of the training kernels
+against the CPU oracle, bit-exact lookups versus plain descent (and the
+oracle), behaviour after splits, and what the trained MLP root gains over a
+linear root."""
+import numpy as np
+import pytest
+
+import eirene_b200 as E
+from oracle import oracle as O
+from tests.helpers import dev, empty_u64, empty_u8, host_u64, host_u8, run_batch
+
+pytestmark = pytest.mark.gpu
+
+# float32 accumulation over n samples vs a double CPU reference
+GRAD_RTOL = 2e-3
+GRAD_ATOL = 1e-6
+
+
+def test_mlp_gradient_matches_oracle(gpu):
+    import torch
+
+    t = E.BTree(max_keys=1 << 14, max_batch=1 << 12)
+    rng = np.random.default_rng(1)
+    for n in [1, 97, 5000, 65536]:
+        p = rng.normal(0, 0.7, 97).astype(np.float32)
+        x = rng.random(n).astype(np.float32)
+        y = rng.random(n).astype(np.float32)
+        g = torch.zeros(97, dtype=torch.float32, device="cuda")
+        loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+        t.mlp_grad(torch.from_numpy(p).cuda(), torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda(), g, loss)
+        torch.cuda.synchronize()
+        ref_loss, ref_g = O.mlp_grad(p, x, y)
+        gg = g.cpu().numpy().astype(np.float64)
+        scale = np.abs(ref_g).max()
+        assert np.allclose(gg, ref_g, rtol=GRAD_RTOL, atol=GRAD_ATOL + GRAD_RTOL * scale), (n, np.abs(gg - ref_g).max())
+        assert abs(float(loss.item()) - ref_loss) <= GRAD_RTOL * max(1.0, ref_loss)
+
+
+def lookups(t, keys):
+    v, s = empty_u64(keys.size), empty_u8(keys.size)
+    t.search(dev(keys), v, s)
+    return host_u64(v), host_u8(s)
+
+
+@pytest.mark.parametrize("dist", ["uniform", "normal", "gamma", "zipf"])
+def test_learned_lookup_bit_exact(gpu, dist):
+    keys = O.gen_keys(dist, 3, 300_000)
+    vals = O.value_of(keys)
+    t = E.BTree(max_keys=1 << 20, max_batch=1 << 18)
+    t.bulk_build(dev(keys), dev(vals))
+    o = O.OracleTree()
+    o.bulk_build(keys, vals)
+    qk, _, _ = O.gen_requests(dist, 4, keys, 200_000, 100)
+    qk[5] = np.uint64(2**64 - 1)
+    qk[6] = np.uint64(0)
+    ov, os_ = o.execute_merged(qk, np.zeros_like(qk), np.ones(qk.size, np.uint8))
+    t.set_descent(False)
+    pv, ps = lookups(t, qk)
+    t.retrain()
+    info = t.learned_info()
+    assert info["valid"] == 1
+    t.set_descent(True)
+    t.reset_stats()
+    lv, ls = lookups(t, qk)
+    assert (ps == os_).all() and (pv == ov).all()
+    assert (ls == ps).all() and (lv == pv).all()
+    st = t.stats()
+    assert st["learned_hits"] > 0.5 * qk.size, (st, info)
+
+
+def test_learned_after_splits_and_sorted_batches(gpu):
+    keys = O.gen_keys("uniform", 8, 200_000)
+    vals = O.value_of(keys)
+    t = E.BTree(max_keys=1 << 21, max_batch=1 << 18)
+    t.bulk_build(dev(keys), dev(vals))
+    o = O.OracleTree()
+    o.bulk_build(keys, vals)
+    t.retrain()
+    t.set_descent(True)
+    # insert-heavy batches split many leaves after training: lookups must stay exact
+    for b in range(4):
+        rk, rv, ro = O.gen_requests("uniform", 50 + b, keys, 100_000, 50)
+        ov, os_ = o.execute_merged(rk, rv, ro)
+        gv, gs = run_batch(t, rk, rv, ro, E.MODE_SORTED)
+        assert (gs == os_).all() and (gv == ov).all()
+    st = t.stats()
+    assert st["leaf_splits"] > 0 and st["learned_fallbacks"] > 0 and st["learned_hits"] > 0
+    qk, _, _ = O.gen_requests("uniform", 99, o.dump()[0], 100_000, 100)
+    ov, os_ = o.execute_merged(qk, np.zeros_like(qk), np.ones(qk.size, np.uint8))
+    lv, ls = lookups(t, qk)
+    assert (ls == os_).all() and (lv == ov).all()
+    # retraining restores the hit rate
+    t.reset_stats()
+    t.retrain()
+    lookups(t, qk)
+    st2 = t.stats()
+    assert st2["learned_fallbacks"] < st["learned_fallbacks"]
+
+
+def test_trained_mlp_root_beats_linear_root(gpu):
+    # skewed keys: a linear root model piles most leaves into few segments, so
+    # their errors exceed the window and lookups fall back; the trained MLP
+    # spreads leaves evenly over the segments
+    keys = O.gen_keys("gamma", 11, 400_000)
+    vals = O.value_of(keys)
+    qk, _, _ = O.gen_requests("gamma", 12, keys, 200_000, 100)
+    res = {}
+    for mlp in (False, True):
+        t = E.BTree(max_keys=1 << 21, max_batch=1 << 18, n_segments=1024, window=16)
+        t.bulk_build(dev(keys), dev(vals))
+        t.set_root_model(mlp)
+        t.retrain()
+        t.set_descent(True)
+        t.reset_stats()
+        lv, ls = lookups(t, qk)
+        st = t.stats()
+        info = t.learned_info()
+        res[mlp] = (st["learned_fallbacks"] / qk.size, st["learned_probe_sum"] / max(1, st["learned_hits"]),
+                    info["segments_over_window"], info["loss"])
+        t.set_descent(False)
+        pv, ps = lookups(t, qk)
+        assert (lv == pv).all() and (ls == ps).all()
+        t.close()
+    lin, mlp = res[False], res[True]
+    assert mlp[0] < lin[0], res
+    assert mlp[2] <= lin[2], res
