@@ -40,13 +40,23 @@ constexpr uint32_t kErrRetry = 2u;
 constexpr uint32_t kErrSpin = 4u;
 
 // ---- header word ----------------------------------------------------------
-// bits 0..7 level (0 = leaf), 8..15 size, 16 lock, 32..63 version
+// bits 0..7 level (0 = leaf), 8..15 size, 16 lock, 17..31 tree epoch,
+// 32..63 version.  The epoch changes with every bulk build; a reader that
+// reaches a node without validating the path rejects a header from another
+// epoch (a node row left over from an earlier tree, or never written: the pool
+// is zeroed at creation and epochs start at 1).
 __host__ __device__ __forceinline__ uint32_t hdr_level(uint64_t h) { return (uint32_t)(h & 0xff); }
 __host__ __device__ __forceinline__ uint32_t hdr_size(uint64_t h) { return (uint32_t)((h >> 8) & 0xff); }
 __host__ __device__ __forceinline__ bool hdr_locked(uint64_t h) { return (h >> 16) & 1; }
+__host__ __device__ __forceinline__ uint32_t hdr_epoch(uint64_t h) { return (uint32_t)((h >> 17) & 0x7fff); }
 __host__ __device__ __forceinline__ uint32_t hdr_version(uint64_t h) { return (uint32_t)(h >> 32); }
-__host__ __device__ __forceinline__ uint64_t make_hdr(uint32_t size, uint32_t level, uint32_t version) {
-  return ((uint64_t)version << 32) | ((uint64_t)size << 8) | (uint64_t)level;
+__host__ __device__ __forceinline__ uint64_t make_hdr(uint32_t size, uint32_t level, uint32_t version,
+                                                      uint32_t epoch) {
+  return ((uint64_t)version << 32) | ((uint64_t)(epoch & 0x7fff) << 17) | ((uint64_t)size << 8) | (uint64_t)level;
+}
+// next version of an unlocked header with a new size (level and epoch kept)
+__host__ __device__ __forceinline__ uint64_t hdr_next(uint64_t h, uint32_t size) {
+  return make_hdr(size, hdr_level(h), hdr_version(h) + 1, hdr_epoch(h));
 }
 __host__ __device__ __forceinline__ uint64_t hdr_lock(uint64_t h) { return h | (1ull << 16); }
 
@@ -57,7 +67,7 @@ struct Ctrl {
   uint32_t n_nodes;    // bump allocator
   uint32_t error;      // sticky kErr* bits
   uint32_t root_level; // level of the root node (0 = the root is a leaf)
-  uint32_t pad32;
+  uint32_t epoch;      // current tree epoch (header bits 17..31)
   unsigned long long n_keys;
   unsigned long long commits;
   unsigned long long aborts;

@@ -95,8 +95,9 @@ struct Handle {
   uint32_t inner_fill = 24;
   uint32_t retry_limit = 1u << 16;
   int descent = 0;     // 0 plain, 1 learned
+  uint32_t epoch = 0;  // tree epoch, bumped by every reset / bulk build
   int search_group = 8;  // lanes per request in the lock-free search
-  int learned_group = 32;  // lanes per request in the learned search
+  int learned_group = 8;  // lanes per request in the learned search
   int sm_count = 148;
   Work w;
   Learned L;

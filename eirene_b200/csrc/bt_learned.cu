@@ -391,41 +391,73 @@ __global__ void __launch_bounds__(256) learned_search_kernel(DevTree t, LearnedD
         sp.b = __uint_as_float((uint32_t)w2);
         sp.err = (uint32_t)(w2 >> 32);
       }
-      bool ok = sp.err <= M.window;
-      long long lo = 0, hi = -1;
+      // first probe: the G table entries around the prediction in one load
+      // (entries are {low, id}; the sentinel at n_leaves has low = UINT64_MAX)
+      const long long L = (long long)M.n_leaves;
+      bool ok = sp.err != kErrNone;
       float pred = 0.f;
+      long long pc = 0;
       if (ok) {
         pred = seg_predict(sp, key);
         if (!(pred > -1.0e9f && pred < 1.0e10f)) ok = false;
         else {
-          lo = (long long)floorf(pred) - (long long)sp.err - 1;
-          hi = (long long)ceilf(pred) + (long long)sp.err + 1;
-          if (lo < 0) lo = 0;
-          if (hi > (long long)M.n_leaves - 1) hi = (long long)M.n_leaves - 1;
-          ok = lo <= hi;
+          pc = (long long)floorf(pred + 0.5f);
+          if (pc < 0) pc = 0;
+          if (pc > L - 1) pc = L - 1;
         }
       }
-      uint32_t slot = 0;
+      uint32_t slot = 0, node = 0;
+      bool found = false;
       if (ok) {
-        // window [lo, hi] plus entry hi+1 (a sentinel exists at n_leaves)
-        uint32_t c = 0;
-        bool above = false;
-        for (long long b = lo; b <= hi + 1; b += G) {
-          const long long e = b + g;
-          if (e <= hi + 1) {
-            const uint64_t low = __ldg(&M.tab[e].low);
-            if (e <= hi) c += (low <= key) ? 1u : 0u;
-            else above = low > key;
+        long long p0 = pc - (G / 2 - 1);
+        if (p0 > L - G) p0 = L - G;
+        if (p0 < 0) p0 = 0;
+        const long long e = p0 + g;
+        ulonglong2 ent = make_ulonglong2(kKeyMax, 0);
+        if (e <= L) ent = __ldg(reinterpret_cast<const ulonglong2*>(M.tab) + e);
+        uint64_t above = kKeyMax;
+        if (g == 0 && p0 + G <= L) above = __ldg(&M.tab[p0 + G].low);
+        above = __shfl_sync(gmask, above, 0, G);
+        const uint32_t c = group_sum<G>(ent.x <= key ? 1u : 0u, gmask);
+        if (c >= 1 && (c < (uint32_t)G || above > key)) {
+          slot = (uint32_t)(p0 + c - 1);
+          node = (uint32_t)__shfl_sync(gmask, ent.y, c - 1, G);
+          found = true;
+        } else if (sp.err <= M.window) {
+          // second chance: the segment's whole error window
+          long long lo = (long long)floorf(pred) - (long long)sp.err - 1;
+          long long hi = (long long)ceilf(pred) + (long long)sp.err + 1;
+          if (lo < 0) lo = 0;
+          if (hi > L - 1) hi = L - 1;
+          if (lo <= hi) {
+            uint32_t cw = 0;
+            bool ab = false;
+            for (long long b = lo; b <= hi + 1; b += 4 * G) {
+              uint64_t lw[4];
+#pragma unroll
+              for (int u = 0; u < 4; u++) {
+                const long long ee = b + u * G + g;
+                lw[u] = ee <= hi + 1 ? __ldg(&M.tab[ee].low) : 0;
+              }
+#pragma unroll
+              for (int u = 0; u < 4; u++) {
+                const long long ee = b + u * G + g;
+                if (ee <= hi) cw += (lw[u] <= key) ? 1u : 0u;
+                else if (ee == hi + 1) ab = lw[u] > key;
+              }
+            }
+            cw = group_sum<G>(cw, gmask);
+            ab = __any_sync(gmask, ab);
+            if (cw >= 1 && (cw < (uint32_t)(hi - lo + 1) || ab)) {
+              slot = (uint32_t)(lo + cw - 1);
+              node = (uint32_t)__ldg(&M.tab[slot].id);
+              found = true;
+            }
           }
         }
-        c = group_sum<G>(c, gmask);
-        above = __any_sync(gmask, above);
-        ok = c >= 1 && (c < (uint32_t)(hi - lo + 1) || above);
-        slot = (uint32_t)(lo + c - 1);
       }
       bool done = false;
-      if (ok) {
-        const uint32_t node = (uint32_t)__ldg(&M.tab[slot].id);
+      if (found) {
         uint64_t k[S], v[S];
         load_slots<S>(t.keys + (size_t)node * 32 + g * S, k);
         const uint64_t fence = __shfl_sync(gmask, g == G - 1 ? __ldg(t.vals + (size_t)node * 32 + 31) : 0, G - 1, G);
@@ -438,8 +470,7 @@ __global__ void __launch_bounds__(256) learned_search_kernel(DevTree t, LearnedD
           st = group_leaf_lookup<G, false>(t, node, key, g, gmask, k, v, c, ans);
           done = true;
           hits++;
-          const float d = fabsf(floorf(pred + 0.5f) - (float)slot);
-          probe += (unsigned long long)d;
+          probe += (unsigned long long)(pc > (long long)slot ? pc - (long long)slot : (long long)slot - pc);
         }
       }
       if (!done) {

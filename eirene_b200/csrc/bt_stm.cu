@@ -110,7 +110,7 @@ __device__ int commit_split(const DevTree& t, uint32_t node, uint64_t h, uint64_
   }
   const uint32_t right = base;
   // new right node (unreachable until the parent / root is published)
-  write_row(t, right, rk, rv, true, make_hdr(rsize, level, 0));
+  write_row(t, right, rk, rv, false, 0);
   if (lane == 0) t.low[right] = up;
   write_row(t, node, lk, lv, false, 0);
   uint32_t psize = 0;
@@ -123,14 +123,21 @@ __device__ int commit_split(const DevTree& t, uint32_t node, uint64_t h, uint64_
     const uint32_t nr = base + 1;
     const uint64_t nk = lane == 0 ? up : kKeyMax;
     const uint64_t nv = lane == 0 ? (uint64_t)node : (lane == 1 ? (uint64_t)right : 0);
-    write_row(t, nr, nk, nv, true, make_hdr(1, level + 1, 0));
+    write_row(t, nr, nk, nv, false, 0);
     if (lane == 0) t.low[nr] = t.low[node];
   }
+  // new nodes become valid with a release store of their header after their
+  // rows and low fences, so a reader that acquires the header sees them whole
+  __threadfence();
+  __syncwarp();
+  const uint32_t ep = hdr_epoch(h);
+  if (lane == 2) st_release(hdr_ptr(t, right), make_hdr(rsize, level, 0, ep));
+  if (new_root && lane == 3) st_release(hdr_ptr(t, base + 1), make_hdr(1, level + 1, 0, ep));
   __threadfence();
   __syncwarp();
   if (lane == 0) st_release(hdr_ptr(t, node), lhdr);
   if (!new_root) {
-    if (lane == 1) st_release(hdr_ptr(t, parent), make_hdr(psize + 1, hdr_level(ph), hdr_version(ph) + 1));
+    if (lane == 1) st_release(hdr_ptr(t, parent), hdr_next(ph, psize + 1));
   } else if (lane == 0) {
     C->root_level = level + 1;
     C->root = base + 1;
@@ -179,8 +186,11 @@ __device__ int tx_attempt(const DevTree& t, const uint64_t key, const uint64_t v
       unlock_unchanged(t, kNil, 0, kNil, 0, true, rl);
       return TX_NOCAP;
     }
-    write_row(t, id, kKeyMax, lane == 31 ? kKeyMax : 0, true, make_hdr(0, 0, 0));
+    write_row(t, id, kKeyMax, lane == 31 ? kKeyMax : 0, false, 0);
     if (lane == 0) t.low[id] = 0;
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) st_release(hdr_ptr(t, id), make_hdr(0, 0, 0, ld_relaxed32(&C->epoch)));
     __threadfence();
     __syncwarp();
     if (lane == 0) {
@@ -222,7 +232,7 @@ __device__ int tx_attempt(const DevTree& t, const uint64_t key, const uint64_t v
       const uint64_t lv = lane <= mid ? v : 0;
       const uint64_t rk = lane < mid ? rk0 : kKeyMax;
       const uint64_t rv = lane <= mid ? rv0 : 0;
-      const int r = commit_split(t, node, h, lk, lv, make_hdr(mid, level, hdr_version(h) + 1), rk, rv, mid, level, up,
+      const int r = commit_split(t, node, h, lk, lv, hdr_next(h, mid), rk, rv, mid, level, up,
                                  parent, ph, pslot, pk, pv, rl);
       return r == TX_DONE ? TX_AGAIN : r;
     }
@@ -257,7 +267,7 @@ __device__ int tx_attempt(const DevTree& t, const uint64_t key, const uint64_t v
     if (lane == at) t.vals[(size_t)node * 32 + at] = val;
     __threadfence();
     __syncwarp();
-    if (lane == 0) st_release(hdr_ptr(t, node), make_hdr(size, 0, hdr_version(h) + 1));
+    if (lane == 0) st_release(hdr_ptr(t, node), hdr_next(h, size));
     __syncwarp();
     ans = old;
     st = kFound;
@@ -278,7 +288,7 @@ __device__ int tx_attempt(const DevTree& t, const uint64_t key, const uint64_t v
     __threadfence();
     __syncwarp();
     if (lane == 0) {
-      st_release(hdr_ptr(t, node), make_hdr(size + 1, 0, hdr_version(h) + 1));
+      st_release(hdr_ptr(t, node), hdr_next(h, size + 1));
       atomicAdd(&C->n_keys, 1ull);
     }
     __syncwarp();
@@ -296,13 +306,100 @@ __device__ int tx_attempt(const DevTree& t, const uint64_t key, const uint64_t v
   const uint64_t lv = lane < 16 ? nv : (lane == 31 ? up : 0);
   const uint64_t rk = lane < 16 ? rk0 : kKeyMax;
   const uint64_t rv = lane < 16 ? rv0 : (lane == 31 ? old_fence : 0);
-  const int r = commit_split(t, node, h, lk, lv, make_hdr(16, 0, hdr_version(h) + 1), rk, rv, 16, 0, up, parent, ph,
+  const int r = commit_split(t, node, h, lk, lv, hdr_next(h, 16), rk, rv, 16, 0, up, parent, ph,
                              pslot, pk, pv, rl);
   if (r != TX_DONE) return r;
   if (lane == 0) atomicAdd(&C->n_keys, 1ull);
   ans = 0;
   st = kAbsent;
   return TX_DONE;
+}
+
+// Optimistic attempt (the idea of the reference's RADICAL_SEARCH_FOR_INSERT,
+// src/gpu-stm-tree-v27/bpt-gpustm-kernel-radical-search.cuh:13-266, made
+// exact): inner levels are read with plain loads and no validation; only the
+// leaf is validated -- seqlock on its header, the tree epoch, and its fences
+// low <= key < right fence.  A complete leaf image whose fence range holds the
+// key is that key's leaf whatever path led to it, so the answer and an
+// in-leaf update are exact.  Splits and failed checks go to tx_attempt.
+enum : int { FAST_DONE = 0, FAST_SLOW = 1, FAST_RETRY = 2 };
+
+__device__ int tx_fast(const DevTree& t, const uint32_t epoch, const uint64_t key, const uint64_t val,
+                       const bool is_insert, uint64_t& ans, uint8_t& st) {
+  const uint32_t lane = lane_id();
+  Ctrl* C = t.ctrl;
+  uint32_t node = ld_relaxed32(&C->root);
+  if (node == kNil) return FAST_SLOW;
+  for (int depth = 0;; depth++) {
+    if (depth > 40 || node >= t.cap) return FAST_SLOW;
+    const uint64_t* krow = t.keys + (size_t)node * 32;
+    const uint64_t kr = krow[lane];
+    const uint64_t hdr = __shfl_sync(kFull, kr, 31);
+    if (hdr_level(hdr) == 0) break;
+    const uint64_t v = t.vals[(size_t)node * 32 + lane];
+    const uint32_t c = __popc(__ballot_sync(kFull, lane < 31 && kr <= key));
+    node = (uint32_t)__shfl_sync(kFull, v, c);
+  }
+  // seqlock read of the leaf
+  const uint64_t* krow = t.keys + (size_t)node * 32;
+  const uint64_t h = ld_acquire(krow + 31);
+  uint64_t k = ld_relaxed(krow + lane);
+  const uint64_t v = ld_relaxed(t.vals + (size_t)node * 32 + lane);
+  const uint64_t lo = ld_relaxed(t.low + node);
+  fence_acq_rel();
+  const uint64_t h2 = ld_relaxed(krow + 31);
+  const uint64_t h_lane0 = __shfl_sync(kFull, h, 0);
+  const uint64_t fence_key = __shfl_sync(kFull, v, 31);
+  const bool bad = hdr_locked(h) || h2 != h || h != h_lane0 || hdr_level(h) != 0 || hdr_epoch(h) != epoch ||
+                   !(lo <= key && key < fence_key);
+  if (__any_sync(kFull, bad)) return FAST_RETRY;
+  if (lane == 31) k = kKeyMax;
+  const uint32_t size = hdr_size(h);
+  const uint32_t mm = __ballot_sync(kFull, lane < size && k == key);
+  if (!is_insert) {
+    if (mm) {
+      ans = __shfl_sync(kFull, v, __ffs(mm) - 1);
+      st = kFound;
+    } else {
+      ans = 0;
+      st = kAbsent;
+    }
+    return FAST_DONE;
+  }
+  if (mm) {
+    const uint32_t at = __ffs(mm) - 1;
+    const uint64_t old = __shfl_sync(kFull, v, at);
+    if (!acquire_locks(t, node, h, kNil, 0, false, 0)) return FAST_RETRY;
+    if (lane == at) t.vals[(size_t)node * 32 + at] = val;
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) st_release(hdr_ptr(t, node), hdr_next(h, size));
+    __syncwarp();
+    ans = old;
+    st = kFound;
+    return FAST_DONE;
+  }
+  if (size >= (uint32_t)kMaxKeys) return FAST_SLOW;  // needs a split: validated path
+  const uint32_t p = __popc(__ballot_sync(kFull, lane < size && k < key));
+  const uint64_t uk = __shfl_up_sync(kFull, k, 1);
+  const uint64_t uv = __shfl_up_sync(kFull, v, 1);
+  const uint64_t nk = lane < p ? k : (lane == p ? key : uk);
+  const uint64_t nv = lane < p ? v : (lane == p ? val : uv);
+  if (!acquire_locks(t, node, h, kNil, 0, false, 0)) return FAST_RETRY;
+  if (lane <= size && lane < 31) {
+    t.keys[(size_t)node * 32 + lane] = nk;
+    t.vals[(size_t)node * 32 + lane] = nv;
+  }
+  __threadfence();
+  __syncwarp();
+  if (lane == 0) {
+    st_release(hdr_ptr(t, node), hdr_next(h, size + 1));
+    atomicAdd(&C->n_keys, 1ull);
+  }
+  __syncwarp();
+  ans = 0;
+  st = kAbsent;
+  return FAST_DONE;
 }
 
 __global__ void __launch_bounds__(256) stm_kernel(DevTree t, const uint64_t* __restrict__ keys,
@@ -315,6 +412,7 @@ __global__ void __launch_bounds__(256) stm_kernel(DevTree t, const uint64_t* __r
   const size_t n = n_dev ? (size_t)*n_dev : n_host;
   const size_t n_warps = ((size_t)gridDim.x * blockDim.x) >> 5;
   unsigned long long commits = 0, aborts = 0, exhausted = 0;
+  const uint32_t epoch = t.ctrl->epoch;
   for (size_t q = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < n; q += n_warps) {
     const uint32_t r = list ? list[q] : (uint32_t)q;
     const uint64_t key = keys[r];
@@ -325,7 +423,22 @@ __global__ void __launch_bounds__(256) stm_kernel(DevTree t, const uint64_t* __r
       const bool ins = (op == kOpInsert);
       const uint64_t val = ins ? vals[r] : 0;
       uint32_t attempts = 0, fails = 0;
-      for (;;) {
+      bool done = false;
+      // optimistic attempts first; a split or repeated failed checks go to
+      // the validated path below
+      for (int f = 0; f < 4 && !done; f++) {
+        attempts++;
+        const int res = tx_fast(t, epoch, key, val, ins, ans, st);
+        if (res == FAST_DONE) {
+          if (ins) commits++;
+          done = true;
+        } else if (res == FAST_SLOW) {
+          break;
+        } else {
+          aborts++;
+        }
+      }
+      for (; !done;) {
         if (attempts++ >= retry_limit) {
           st = kRetryExhausted;
           exhausted++;

@@ -21,8 +21,9 @@ namespace bt {
 
 namespace {
 
-__global__ void reset_kernel(Ctrl* c) {
+__global__ void reset_kernel(Ctrl* c, uint32_t epoch) {
   c->root = kNil;
+  c->epoch = epoch;
   c->root_lock = 0;
   c->n_nodes = 0;
   c->error = 0;
@@ -52,7 +53,7 @@ __global__ void dedupe_kernel(const uint64_t* __restrict__ sk, const uint32_t* _
 
 // one warp per leaf; leaves get base or base+1 keys (the first `rem` get one more)
 __global__ void build_leaves_kernel(DevTree t, const uint64_t* __restrict__ uk, const uint64_t* __restrict__ uv,
-                                    size_t m, uint32_t nl) {
+                                    size_t m, uint32_t nl, uint32_t epoch) {
   const uint32_t lane = threadIdx.x & 31;
   const size_t j = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (j >= nl) return;
@@ -65,7 +66,7 @@ __global__ void build_leaves_kernel(DevTree t, const uint64_t* __restrict__ uk, 
     kr[lane] = lane < k ? uk[start + lane] : kKeyMax;
     vr[lane] = lane < k ? uv[start + lane] : 0;
   } else {
-    kr[31] = make_hdr((uint32_t)k, 0, 0);
+    kr[31] = make_hdr((uint32_t)k, 0, 0, epoch);
     vr[31] = (j + 1 < nl) ? uk[start + k] : kKeyMax;
   }
   if (lane == 0) t.low[j] = j == 0 ? 0 : uk[start];
@@ -73,7 +74,7 @@ __global__ void build_leaves_kernel(DevTree t, const uint64_t* __restrict__ uk, 
 
 // one warp per inner node of a level: node p groups children [c, c + k)
 __global__ void build_inner_kernel(DevTree t, uint32_t first_child, uint32_t n_children, uint32_t first_node,
-                                   uint32_t n_nodes_level, uint32_t level) {
+                                   uint32_t n_nodes_level, uint32_t level, uint32_t epoch) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t p = (uint32_t)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   if (p >= n_nodes_level) return;
@@ -85,7 +86,7 @@ __global__ void build_inner_kernel(DevTree t, uint32_t first_child, uint32_t n_c
   uint64_t* vr = t.vals + (size_t)id * 32;
   // key slot i (i < k-1) = low fence of child i+1
   if (lane < 31) kr[lane] = (lane + 1 < k) ? t.low[c + lane + 1] : kKeyMax;
-  else kr[31] = make_hdr(k - 1, level, 0);
+  else kr[31] = make_hdr(k - 1, level, 0, epoch);
   vr[lane] = lane < k ? (uint64_t)(c + lane) : 0;
   if (lane == 0) t.low[id] = t.low[c];
 }
@@ -164,7 +165,8 @@ inline unsigned blocks_for(size_t n, int per) { return (unsigned)((n + per - 1) 
 }  // namespace
 
 cudaError_t tree_reset(Handle* h, cudaStream_t s) {
-  reset_kernel<<<1, 1, 0, s>>>(h->tree.ctrl);
+  h->epoch = (h->epoch % 0x7fffu) + 1;  // 1 .. 0x7fff; 0 marks never-written rows
+  reset_kernel<<<1, 1, 0, s>>>(h->tree.ctrl, h->epoch);
   count_launch();
   return cudaGetLastError();
 }
@@ -224,13 +226,13 @@ int tree_bulk_build(Handle* h, const uint64_t* keys, const uint64_t* vals, size_
       height++;
     }
     if (total > h->tree.cap) { rc = -4; goto done; }
-    build_leaves_kernel<<<blocks_for((size_t)nl * 32, 256), 256, 0, s>>>(h->tree, uk, uv, m, nl);
+    build_leaves_kernel<<<blocks_for((size_t)nl * 32, 256), 256, 0, s>>>(h->tree, uk, uv, m, nl, h->epoch);
     count_launch();
     uint32_t first_child = 0, n_children = nl, next = nl, level = 1;
     while (n_children > 1) {
       uint32_t nn = (n_children + per - 1) / per;
       build_inner_kernel<<<blocks_for((size_t)nn * 32, 256), 256, 0, s>>>(h->tree, first_child, n_children, next,
-                                                                          nn, level);
+                                                                          nn, level, h->epoch);
       count_launch();
       first_child = next;
       next += nn;
@@ -292,13 +294,13 @@ int tree_bulk_build_scratch(Handle* h, const uint64_t* keys, const uint64_t* val
     height++;
   }
   if (total > h->tree.cap) return -4;
-  build_leaves_kernel<<<blocks_for((size_t)nl * 32, 256), 256, 0, s>>>(h->tree, uk, sc.uv, m, nl);
+  build_leaves_kernel<<<blocks_for((size_t)nl * 32, 256), 256, 0, s>>>(h->tree, uk, sc.uv, m, nl, h->epoch);
   count_launch();
   uint32_t first_child = 0, n_children = nl, next = nl, level = 1;
   while (n_children > 1) {
     const uint32_t nn = (n_children + per - 1) / per;
     build_inner_kernel<<<blocks_for((size_t)nn * 32, 256), 256, 0, s>>>(h->tree, first_child, n_children, next, nn,
-                                                                        level);
+                                                                        level, h->epoch);
     count_launch();
     first_child = next;
     next += nn;

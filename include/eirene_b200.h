@@ -175,7 +175,7 @@ int bt_set_descent(bt_handle *h, int descent);
 /* stage 1 root model: 1 = 1->32->1 MLP (default), 0 = linear */
 int bt_set_root_model(bt_handle *h, int mlp);
 int bt_set_search_group(bt_handle *h, uint32_t lanes);
-/* lanes per request in the learned search kernel: 8, 16 or 32 (default 32) */
+/* lanes per request in the learned search kernel: 8, 16 or 32 (default 8) */
 int bt_set_learned_group(bt_handle *h, uint32_t lanes);
 /* info[8]: valid, n_leaves, n_segments, segments over the window, window,
  * final training loss, root model (1 MLP, 0 linear), training steps */
