@@ -358,7 +358,7 @@ int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const ui
   uint64_t* sk = nullptr;
   uint32_t* sv = nullptr;
   prof_mark(h, 0, s);
-  if (radix_sort_pairs(keys, nullptr, ops, w.k_a, w.v_a, w.k_b, w.v_b, n, 0, 64, w.sort_scratch, s, &sk, &sv) !=
+  if (radix_sort_pairs(keys, nullptr, ops, w.k_a, w.v_a, w.k_b, w.v_b, n, 0, 64, w.sort_scratch, s, &sk, &sv, &h->tree.ctrl->error) !=
       cudaSuccess)
     return -2;
   const uint32_t n_tiles = (uint32_t)sort_tiles(n);

@@ -28,7 +28,7 @@ cudaError_t sort_prepare();
 size_t sort_scratch_words(size_t n);
 cudaError_t radix_sort_pairs(const uint64_t* keys_in, const uint32_t* vals_in, const uint8_t* ops, uint64_t* k_a,
                              uint32_t* v_a, uint64_t* k_b, uint32_t* v_b, size_t n, int begin_bit, int end_bit,
-                             uint32_t* scratch, cudaStream_t s, uint64_t** k_out, uint32_t** v_out);
+                             uint32_t* scratch, cudaStream_t s, uint64_t** k_out, uint32_t** v_out, uint32_t* err);
 
 // ---- per-batch work buffers, sized for max_batch requests ----
 struct BatchCounts {

@@ -3,14 +3,17 @@
 // DeviceRadixSort::SortPairs, DeviceRunLengthEncode::Encode and
 // DeviceScan::ExclusiveSum (src/gpu-stm-tree-v38/bpt-gpustm-kernel.cu:289-324).
 //
-// Sort pass structure (8-bit digits, tile = 4096 items, 512 threads):
-//   1. tile histogram      reads 8 B/item
-//   2. exclusive scan of the digit-major [256 x tiles] count table
-//   3. scatter             reads 12 B/item, writes 12 B/item
-// The scatter ranks items stably inside the tile with __match_any_sync
-// (each warp owns a contiguous 256-item chunk and walks it in 8 rounds),
-// stages the tile in shared memory in digit order and writes each digit run
-// contiguously, so global writes are coalesced.  No inter-CTA waits.
+// The sort follows the single-pass-per-digit scheme of Adinets & Merrill,
+// "Onesweep: A Faster Least Significant Digit Radix Sort for GPUs" (2022):
+//   1. one up-front kernel counts all eight 8-bit digits of every key;
+//   2. per digit, one kernel: a tile of 4096 items takes a dynamic tile id,
+//      ranks its items stably with __match_any_sync (each warp owns a
+//      contiguous 256-item chunk and walks it in 8 rounds), publishes its
+//      per-digit counts, and finds its global offsets by decoupled look-back
+//      over the preceding tiles; it then stages the tile in shared memory in
+//      digit order and writes each digit run contiguously (coalesced).
+// The look-back spins on words other tiles write; every spin is bounded and a
+// timeout sets kErrSpin in the tree's error word instead of hanging.
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -32,6 +35,9 @@ constexpr int kScanItems = 4;
 constexpr int kScanTile = kScanThreads * kScanItems;  // 4096
 
 __device__ __forceinline__ uint32_t digit_of(uint64_t k, int shift) { return (uint32_t)(k >> shift) & 0xff; }
+__device__ __forceinline__ void st_relaxed32(uint32_t* p, uint32_t v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 // 2-bit op code carried in the payload: 0 insert, 1 get, 3 anything else (rejected)
 __device__ __forceinline__ uint32_t op_code(uint8_t op) { return op <= 1 ? (uint32_t)op : 3u; }
 
@@ -124,24 +130,39 @@ __global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(const uint32_t
 }
 
 // ---------------------------------------------------------------- sort ----
-__global__ void __launch_bounds__(kSortThreads) sort_hist_kernel(const uint64_t* __restrict__ keys, size_t n,
-                                                                 int shift, uint32_t* __restrict__ tile_hist,
-                                                                 uint32_t n_tiles) {
-  __shared__ uint32_t h[kRadix];
-  for (int i = threadIdx.x; i < kRadix; i += kSortThreads) h[i] = 0;
+constexpr int kMaxPasses = 8;
+constexpr uint32_t kFlagAgg = 1u << 30;
+constexpr uint32_t kFlagPrefix = 2u << 30;
+constexpr uint32_t kValMask = (1u << 30) - 1u;
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+// all digit histograms in one read of the keys: hist[pass][256]
+__global__ void __launch_bounds__(kSortThreads) sort_upfront_hist_kernel(const uint64_t* __restrict__ keys,
+                                                                         size_t n, int begin_bit, int passes,
+                                                                         uint32_t* __restrict__ hist) {
+  __shared__ uint32_t h[kMaxPasses][kRadix];
+  for (int i = threadIdx.x; i < kMaxPasses * kRadix; i += kSortThreads) (&h[0][0])[i] = 0;
   __syncthreads();
-  const size_t base = (size_t)blockIdx.x * kTile;
-#pragma unroll
-  for (int i = 0; i < kSortItems; i++) {
-    size_t idx = base + (size_t)i * kSortThreads + threadIdx.x;
-    bool valid = idx < n;
-    uint32_t d = valid ? digit_of(keys[idx], shift) : 0xFFFFu;
-    // warp-aggregated shared atomics: one add per distinct digit per warp
-    uint32_t peers = __match_any_sync(0xffffffffu, d);
-    if (valid && (lane_id() == (uint32_t)(__ffs(peers) - 1))) atomicAdd(&h[d], (uint32_t)__popc(peers));
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint64_t k = keys[i];
+    for (int p = 0; p < passes; p++) atomicAdd(&h[p][digit_of(k, begin_bit + 8 * p)], 1u);
   }
   __syncthreads();
-  for (int d = threadIdx.x; d < kRadix; d += kSortThreads) tile_hist[(size_t)d * n_tiles + blockIdx.x] = h[d];
+  for (int i = threadIdx.x; i < passes * kRadix; i += kSortThreads) {
+    const uint32_t c = (&h[0][0])[i];
+    if (c) atomicAdd(hist + i, c);
+  }
+}
+
+// exclusive scan of each pass's 256 counts -> global bucket starts
+__global__ void sort_digit_scan_kernel(uint32_t* __restrict__ hist, int passes) {
+  __shared__ uint32_t ws[32];
+  for (int p = 0; p < passes; p++) {
+    const uint32_t c = hist[p * kRadix + threadIdx.x];
+    const uint32_t e = block_exclusive_scan(c, ws, nullptr);
+    hist[p * kRadix + threadIdx.x] = e;
+  }
 }
 
 struct ScatterSmem {
@@ -151,22 +172,23 @@ struct ScatterSmem {
   uint32_t tstart[kRadix];
   uint32_t gofs[kRadix];
   uint32_t ws[32];
+  uint32_t tile;
 };
 
-// payload_mode: 0 = read vals_in; 1 = generate (ops[i] << 30 | i), ops nullable
-__global__ void __launch_bounds__(kSortThreads) sort_scatter_kernel(
+// payload_mode: 0 = read vals_in; 1 = generate (op code << 30 | i), ops nullable
+__global__ void __launch_bounds__(kSortThreads) sort_onesweep_kernel(
     const uint64_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, const uint8_t* __restrict__ ops,
     int payload_mode, uint64_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, size_t n, int shift,
-    const uint32_t* __restrict__ tile_off, uint32_t n_tiles) {
+    const uint32_t* __restrict__ gbase, uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ status,
+    uint32_t* __restrict__ err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   ScatterSmem& S = *reinterpret_cast<ScatterSmem*>(smem_raw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) S.tile = atomicAdd(tile_counter, 1u);
   for (int i = threadIdx.x; i < kWarps * kRadix; i += kSortThreads) (&S.wh[0][0])[i] = 0;
-  for (int d = threadIdx.x; d < kRadix; d += kSortThreads)
-    S.gofs[d] = tile_off[(size_t)d * n_tiles + blockIdx.x];
   __syncthreads();
-
-  const size_t tile_base = (size_t)blockIdx.x * kTile;
+  const uint32_t tile = S.tile;
+  const size_t tile_base = (size_t)tile * kTile;
   const size_t warp_base = tile_base + (size_t)warp * (32 * kSortItems);
   uint64_t key[kSortItems];
   uint32_t val[kSortItems];
@@ -174,13 +196,13 @@ __global__ void __launch_bounds__(kSortThreads) sort_scatter_kernel(
   const uint32_t lt_mask = (1u << lane) - 1u;
 #pragma unroll
   for (int r = 0; r < kSortItems; r++) {
-    size_t idx = warp_base + (size_t)r * 32 + lane;
-    bool valid = idx < n;
+    const size_t idx = warp_base + (size_t)r * 32 + lane;
+    const bool valid = idx < n;
     key[r] = valid ? keys_in[idx] : 0;
     if (payload_mode == 0) val[r] = valid ? vals_in[idx] : 0;
     else val[r] = (uint32_t)idx | (ops && valid ? (op_code(ops[idx]) << 30) : 0u);
-    uint32_t d = valid ? digit_of(key[r], shift) : 0xFFFFu;
-    uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t d = valid ? digit_of(key[r], shift) : 0xFFFFu;
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
     uint32_t before = 0;
     if (valid) before = S.wh[warp][d];
     __syncwarp();
@@ -189,27 +211,54 @@ __global__ void __launch_bounds__(kSortThreads) sort_scatter_kernel(
     rank[r] = before + __popc(peers & lt_mask);
   }
   __syncthreads();
-  // per digit: prefix over warps, and tile totals
+  // per digit: prefix over warps and the tile total
   uint32_t total = 0;
   if (threadIdx.x < kRadix) {
     const int d = threadIdx.x;
 #pragma unroll
     for (int w = 0; w < kWarps; w++) {
-      uint32_t c = S.wh[w][d];
+      const uint32_t c = S.wh[w][d];
       S.wh[w][d] = total;
       total += c;
     }
+    // publish this tile's count, then look back for the exclusive prefix
+    uint32_t* my = status + (size_t)tile * kRadix + d;
+    if (tile == 0) {
+      st_relaxed32(my, kFlagPrefix | total);
+      S.gofs[d] = gbase[d];
+    } else {
+      st_relaxed32(my, kFlagAgg | total);
+      uint32_t excl = 0;
+      int64_t t = (int64_t)tile - 1;
+      uint32_t spins = 0;
+      while (t >= 0) {
+        const uint32_t w = ld_relaxed32(status + (size_t)t * kRadix + d);
+        const uint32_t f = w & ~kValMask;
+        if (f == 0) {
+          if (++spins > kSpinLimit) {
+            atomicOr(err, kErrSpin);
+            break;
+          }
+          if (spins > 64) __nanosleep(64);
+          continue;
+        }
+        excl += w & kValMask;
+        if (f == kFlagPrefix) break;
+        t--;
+      }
+      st_relaxed32(my, kFlagPrefix | (excl + total));
+      S.gofs[d] = gbase[d] + excl;
+    }
   }
-  // exclusive scan of the 256 digit totals (threads >= 256 contribute 0)
-  uint32_t st = block_exclusive_scan(threadIdx.x < kRadix ? total : 0u, S.ws, nullptr);
+  const uint32_t st = block_exclusive_scan(threadIdx.x < kRadix ? total : 0u, S.ws, nullptr);
   if (threadIdx.x < kRadix) S.tstart[threadIdx.x] = st;
   __syncthreads();
 #pragma unroll
   for (int r = 0; r < kSortItems; r++) {
-    size_t idx = warp_base + (size_t)r * 32 + lane;
+    const size_t idx = warp_base + (size_t)r * 32 + lane;
     if (idx < n) {
-      uint32_t d = digit_of(key[r], shift);
-      uint32_t pos = S.tstart[d] + S.wh[warp][d] + rank[r];
+      const uint32_t d = digit_of(key[r], shift);
+      const uint32_t pos = S.tstart[d] + S.wh[warp][d] + rank[r];
       S.k[pos] = key[r];
       S.v[pos] = val[r];
     }
@@ -217,9 +266,9 @@ __global__ void __launch_bounds__(kSortThreads) sort_scatter_kernel(
   __syncthreads();
   const uint32_t tile_n = (uint32_t)min((size_t)kTile, n - tile_base);
   for (uint32_t i = threadIdx.x; i < tile_n; i += kSortThreads) {
-    uint64_t k = S.k[i];
-    uint32_t d = digit_of(k, shift);
-    uint32_t g = S.gofs[d] + (i - S.tstart[d]);
+    const uint64_t k = S.k[i];
+    const uint32_t d = digit_of(k, shift);
+    const uint32_t g = S.gofs[d] + (i - S.tstart[d]);
     keys_out[g] = k;
     vals_out[g] = S.v[i];
   }
@@ -266,41 +315,63 @@ cudaError_t scan_exclusive_u32(const uint32_t* in, uint32_t* out, size_t n, uint
 
 size_t sort_tiles(size_t n) { return (n + kTile - 1) / kTile; }
 
-// Opt the scatter kernel into >48 KB of shared memory on the current device.
+// Opt the onesweep kernel into >48 KB of shared memory on the current device.
 cudaError_t sort_prepare() {
-  return cudaFuncSetAttribute(sort_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  return cudaFuncSetAttribute(sort_onesweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)sizeof(ScatterSmem));
 }
+
+// scratch: hist[8][256] | tile counters[8] (+pad) | status[8][tiles][256]
 size_t sort_scratch_words(size_t n) {
-  size_t t = sort_tiles(n);
-  return t * kRadix + scan_scratch_words(t * kRadix);
+  const size_t t = sort_tiles(n ? n : 1);
+  const size_t w = (size_t)kMaxPasses * kRadix + 64 + (size_t)kMaxPasses * t * kRadix;
+  const size_t sc = scan_scratch_words(n);  // callers reuse this scratch for scans
+  return w > sc ? w : sc;
 }
 
 // Sorts n pairs by bits [begin_bit, end_bit) of the key.  Input keys_in (and
 // vals_in, or generated payload when vals_in == nullptr) are not modified.
-// Result lands in (k_a, v_a) or (k_b, v_b); *k_out/*v_out name which.
+// Result lands in (k_a, v_a) or (k_b, v_b); *k_out/*v_out name which.  A look-
+// back timeout sets kErrSpin in *err (the result is then not sorted).
 cudaError_t radix_sort_pairs(const uint64_t* keys_in, const uint32_t* vals_in, const uint8_t* ops, uint64_t* k_a,
                              uint32_t* v_a, uint64_t* k_b, uint32_t* v_b, size_t n, int begin_bit, int end_bit,
-                             uint32_t* scratch, cudaStream_t s, uint64_t** k_out, uint32_t** v_out) {
+                             uint32_t* scratch, cudaStream_t s, uint64_t** k_out, uint32_t** v_out, uint32_t* err) {
   *k_out = k_a;
   *v_out = v_a;
   if (n == 0) return cudaSuccess;
+  const int passes = (end_bit - begin_bit + 7) / 8;
+  if (passes <= 0) {
+    copy_keys_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(keys_in, k_a, n);
+    count_launch();
+    if (vals_in) cudaMemcpyAsync(v_a, vals_in, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
+    else {
+      iota_payload_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(v_a, ops, n);
+      count_launch();
+    }
+    return cudaGetLastError();
+  }
+  if (passes > kMaxPasses) return cudaErrorInvalidValue;
   const uint32_t n_tiles = (uint32_t)sort_tiles(n);
-  uint32_t* tile_hist = scratch;
-  uint32_t* scan_tmp = scratch + (size_t)n_tiles * kRadix;
+  uint32_t* hist = scratch;
+  uint32_t* counters = scratch + kMaxPasses * kRadix;
+  uint32_t* status = counters + 64;
+  cudaError_t e = cudaMemsetAsync(scratch, 0,
+                                  ((size_t)kMaxPasses * kRadix + 64 + (size_t)passes * n_tiles * kRadix) * 4, s);
+  if (e != cudaSuccess) return e;
+  unsigned hb = (unsigned)min((size_t)n_tiles, (size_t)1024);
+  sort_upfront_hist_kernel<<<hb, kSortThreads, 0, s>>>(keys_in, n, begin_bit, passes, hist);
+  count_launch();
+  sort_digit_scan_kernel<<<1, kRadix, 0, s>>>(hist, passes);
+  count_launch();
   const uint64_t* src_k = keys_in;
   const uint32_t* src_v = vals_in;
   int mode = vals_in ? 0 : 1;
   uint64_t* dst_k = k_a;
   uint32_t* dst_v = v_a;
-  int passes = 0;
-  for (int bit = begin_bit; bit < end_bit; bit += 8) {
-    sort_hist_kernel<<<n_tiles, kSortThreads, 0, s>>>(src_k, n, bit, tile_hist, n_tiles);
-    count_launch();
-    cudaError_t e = scan_exclusive_u32(tile_hist, tile_hist, (size_t)n_tiles * kRadix, nullptr, scan_tmp, s);
-    if (e != cudaSuccess) return e;
-    sort_scatter_kernel<<<n_tiles, kSortThreads, sizeof(ScatterSmem), s>>>(src_k, src_v, ops, mode, dst_k, dst_v, n,
-                                                                           bit, tile_hist, n_tiles);
+  for (int p = 0; p < passes; p++) {
+    sort_onesweep_kernel<<<n_tiles, kSortThreads, sizeof(ScatterSmem), s>>>(
+        src_k, src_v, ops, mode, dst_k, dst_v, n, begin_bit + 8 * p, hist + p * kRadix, counters + p,
+        status + (size_t)p * n_tiles * kRadix, err);
     count_launch();
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -309,16 +380,6 @@ cudaError_t radix_sort_pairs(const uint64_t* keys_in, const uint32_t* vals_in, c
     mode = 0;
     dst_k = (dst_k == k_a) ? k_b : k_a;
     dst_v = (dst_v == v_a) ? v_b : v_a;
-    passes++;
-  }
-  if (passes == 0) {
-    // nothing to sort: copy through with generated payload
-    copy_keys_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(keys_in, k_a, n);
-    count_launch();
-    if (vals_in) cudaMemcpyAsync(v_a, vals_in, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
-    else iota_payload_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(v_a, ops, n);
-    count_launch();
-    return cudaGetLastError();
   }
   *k_out = const_cast<uint64_t*>(src_k);
   *v_out = const_cast<uint32_t*>(src_v);

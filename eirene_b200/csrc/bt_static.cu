@@ -33,7 +33,8 @@ namespace {
 constexpr size_t kStaticMaxKeys = BT_STATIC_BUILD_MAX_KEYS;
 constexpr size_t up256(size_t x) { return (x + 255) & ~size_t(255); }
 constexpr size_t kTiles = (kStaticMaxKeys + 4095) / 4096;
-constexpr size_t kSortWords = kTiles * 256 + (kTiles * 256 + 4095) / 4096 + 1;
+// radix sort scratch: 8 digit histograms, tile counters, 8 look-back tables
+constexpr size_t kSortWords = 8 * 256 + 64 + 8 * kTiles * 256;
 constexpr size_t kOffKa = 0;
 constexpr size_t kOffKb = kOffKa + up256(kStaticMaxKeys * 8);
 constexpr size_t kOffVa = kOffKb + up256(kStaticMaxKeys * 8);

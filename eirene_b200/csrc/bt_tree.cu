@@ -193,7 +193,8 @@ int tree_bulk_build(Handle* h, const uint64_t* keys, const uint64_t* vals, size_
   uint64_t last_key = 0;
   uint32_t m32 = 0;
   if (!ok) { rc = -3; goto done; }
-  if (radix_sort_pairs(keys, nullptr, nullptr, ka, va, kb, vb, n, 0, 64, scratch, s, &sk, &si) != cudaSuccess) {
+  if (radix_sort_pairs(keys, nullptr, nullptr, ka, va, kb, vb, n, 0, 64, scratch, s, &sk, &si, &h->tree.ctrl->error) !=
+      cudaSuccess) {
     rc = -2;
     goto done;
   }
@@ -266,7 +267,7 @@ int tree_bulk_build_scratch(Handle* h, const uint64_t* keys, const uint64_t* val
   if (n == 0) return cudaStreamSynchronize(s) == cudaSuccess ? 0 : -2;
   uint64_t* sk = nullptr;
   uint32_t* si = nullptr;
-  if (radix_sort_pairs(keys, nullptr, nullptr, sc.ka, sc.va, sc.kb, sc.vb, n, 0, 64, sc.sort_scratch, s, &sk, &si) !=
+  if (radix_sort_pairs(keys, nullptr, nullptr, sc.ka, sc.va, sc.kb, sc.vb, n, 0, 64, sc.sort_scratch, s, &sk, &si, &h->tree.ctrl->error) !=
       cudaSuccess)
     return -2;
   uint32_t* flags = (si == sc.va) ? sc.vb : sc.va;
