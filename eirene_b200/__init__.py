@@ -83,8 +83,9 @@ EXPORTS = [
     "bt_stats_get", "bt_stats_reset", "bt_retrain", "bt_set_descent", "bt_set_root_model", "bt_set_search_group",
     "bt_host_alloc", "bt_host_free", "bt_gen_keys", "bt_gen_requests", "bt_status_string",
     "bt_profile", "bt_profile_read", "bt_launch_count", "bt_bulk_build_static",
-    "bt_set_learned_group", "bt_learned_info", "bt_mlp_grad",
+    "bt_set_learned_group", "bt_learned_info", "bt_mlp_grad", "bt_set_option",
 ]
+OPT_SORTED_SEARCH, OPT_RETRY_LIMIT, OPT_TRAIN_STEPS = 1, 2, 3
 PHASES = ["sort", "merge", "search", "insert", "writeback"]
 
 _lib = None
@@ -137,6 +138,7 @@ def lib():
             "bt_set_learned_group": [_P, ctypes.c_uint32],
             "bt_learned_info": [_P, _P],
             "bt_mlp_grad": [_P, _P, _P, _P, _SZ, _P, _P, _P],
+            "bt_set_option": [_P, ctypes.c_int, ctypes.c_int64],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -295,6 +297,9 @@ class BTree:
         b = ctypes.c_uint64(0)
         _check(lib().bt_profile_read(self._h, ms, ctypes.byref(b), 1 if reset else 0), "bt_profile_read")
         return {"batches": b.value, **{p: ms[i] for i, p in enumerate(PHASES)}}
+
+    def set_option(self, option: int, value: int):
+        _check(lib().bt_set_option(self._h, option, value), "bt_set_option")
 
     def set_learned_group(self, lanes: int):
         _check(lib().bt_set_learned_group(self._h, lanes), "bt_set_learned_group")

@@ -396,6 +396,22 @@ int bt_profile_read(bt_handle* H, double* phase_ms, uint64_t* batches, int reset
 
 uint64_t bt_launch_count(void) { return bt::g_launches.load(); }
 
+int bt_set_option(bt_handle* H, int option, int64_t value) {
+  if (!H) return BT_ERR_INVALID_ARG;
+  switch (option) {
+    case BT_OPT_SORTED_SEARCH: H->h.sorted_search = value ? 1 : 0; return BT_OK;
+    case BT_OPT_RETRY_LIMIT:
+      if (value < 1 || value > 0x7fffffff) return BT_ERR_INVALID_ARG;
+      H->h.retry_limit = (uint32_t)value;
+      return BT_OK;
+    case BT_OPT_TRAIN_STEPS:
+      if (value < 0 || value > 1000000) return BT_ERR_INVALID_ARG;
+      H->h.L.train_steps = (uint32_t)value;
+      return BT_OK;
+    default: return BT_ERR_INVALID_ARG;
+  }
+}
+
 int bt_set_learned_group(bt_handle* H, uint32_t lanes) {
   if (!H) return BT_ERR_INVALID_ARG;
   if (lanes != 8 && lanes != 16 && lanes != 32) return BT_ERR_INVALID_ARG;

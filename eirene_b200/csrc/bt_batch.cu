@@ -376,6 +376,8 @@ int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const ui
   cudaError_t e;
   if (h->descent == 1 && h->L.valid)
     e = launch_learned_search(h, w.ukeys, w.get_list, &w.counts->n_get, n, w.uans, w.uans_st, s);
+  else if (h->sorted_search)
+    e = launch_search_sorted(h, w.ukeys, w.get_list, &w.counts->n_get, n, w.uans, w.uans_st, s);
   else
     e = launch_search(h, w.ukeys, w.get_list, &w.counts->n_get, n, w.uans, w.uans_st, s);
   if (e != cudaSuccess) return -2;

@@ -98,6 +98,7 @@ struct Handle {
   uint32_t epoch = 0;  // tree epoch, bumped by every reset / bulk build
   int search_group = 8;  // lanes per request in the lock-free search
   int learned_group = 8;  // lanes per request in the learned search
+  int sorted_search = 1;  // batch GET phase: 1 = path-reusing search over the sorted keys
   int sm_count = 148;
   Work w;
   Learned L;
@@ -140,6 +141,9 @@ int tree_bulk_build_scratch(Handle* h, const uint64_t* keys, const uint64_t* val
                             const BuildScratch& sc);
 cudaError_t launch_search(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev, size_t n,
                           uint64_t* out_vals, uint8_t* out_st, cudaStream_t s);
+// search over keys in ascending order (path reuse); needs root_level < 8
+cudaError_t launch_search_sorted(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev,
+                                 size_t n, uint64_t* out_vals, uint8_t* out_st, cudaStream_t s);
 // ids of the leaves in key order; returns count (synchronises the stream)
 int enumerate_leaves(Handle* h, cudaStream_t s, uint32_t** leaf_ids, size_t* n_leaves);
 // leaf sizes in key order into a device buffer (after enumerate_leaves)

@@ -340,13 +340,64 @@ struct LearnedDev {
   uint32_t window;
 };
 
+// Predicted leaf for `key`: stage 1 (MLP) -> segment -> line -> one probe of
+// the G leaf-table entries around the predicted slot.  Returns the leaf's node
+// id, or kNil when the probe does not bracket the key (caller falls back).
 template <int G>
-__global__ void __launch_bounds__(256) learned_search_kernel(DevTree t, LearnedDev M,
-                                                             const uint64_t* __restrict__ qkeys,
-                                                             const uint32_t* __restrict__ list,
-                                                             const uint32_t* __restrict__ n_dev, size_t n_host,
-                                                             uint64_t* __restrict__ out_vals,
-                                                             uint8_t* __restrict__ out_st) {
+__device__ __forceinline__ uint32_t learned_leaf(const LearnedDev& M, const float* p, uint64_t key, uint32_t g,
+                                                 uint32_t gmask, uint32_t& dist) {
+  const float x = norm_x(key, M.kmin, M.inv_range);
+  float y = 0.f;
+#pragma unroll
+  for (int jj = 0; jj < kHidden / G; jj++) {
+    const int j = g + jj * G;
+    const float h = fmaf(p[j], x, p[kHidden + j]);
+    if (h > 0.f) y = fmaf(p[2 * kHidden + j], h, y);
+  }
+#pragma unroll
+  for (int o = G / 2; o >= 1; o >>= 1) y += __shfl_xor_sync(gmask, y, o, G);
+  y += p[3 * kHidden];
+  const uint64_t* w = reinterpret_cast<const uint64_t*>(M.seg + seg_of_y(y, M.n_seg));
+  SegParam sp;
+  sp.base = __ldg(w);
+  const uint64_t w1 = __ldg(w + 1), w2 = __ldg(w + 2);
+  sp.inv_span = __uint_as_float((uint32_t)w1);
+  sp.a = __uint_as_float((uint32_t)(w1 >> 32));
+  sp.b = __uint_as_float((uint32_t)w2);
+  if ((uint32_t)(w2 >> 32) == kErrNone) return kNil;  // segment without a model
+  const float pred = seg_predict(sp, key);
+  const int L = (int)M.n_leaves;
+  int pc = (pred > 0.f) ? (pred < (float)(L - 1) ? __float2int_rn(pred) : L - 1) : 0;
+  // probe the G entries [p0, p0 + G) and the one above them
+  int p0 = pc - (G / 2 - 1);
+  p0 = p0 > L - G ? L - G : p0;
+  p0 = p0 < 0 ? 0 : p0;
+  const int e = p0 + (int)g;
+  ulonglong2 ent = make_ulonglong2(kKeyMax, 0);
+  if (e <= L) ent = __ldg(reinterpret_cast<const ulonglong2*>(M.tab) + e);
+  uint64_t above = kKeyMax;
+  if (g == 0 && p0 + G <= L) above = __ldg(&M.tab[p0 + G].low);
+  above = __shfl_sync(gmask, above, 0, G);
+  const uint32_t c = group_sum<G>(ent.x <= key ? 1u : 0u, gmask);
+  const uint32_t node = (uint32_t)__shfl_sync(gmask, ent.y, (c + G - 1) % G, G);
+  if (c >= 1 && (c < (uint32_t)G || above > key)) {
+    const int slot = p0 + (int)c - 1;
+    dist = (uint32_t)(pc > slot ? pc - slot : slot - pc);
+    return node;
+  }
+  return kNil;
+}
+
+// kSorted: keys arrive in ascending order (the batch's unique GETs); each
+// group walks a contiguous chunk and reuses the previous leaf while the key
+// stays below its fence.  Otherwise a grid-stride loop over any keys.
+template <int G, bool kSorted>
+__global__ void __launch_bounds__(256, 6) learned_search_kernel(DevTree t, LearnedDev M,
+                                                                const uint64_t* __restrict__ qkeys,
+                                                                const uint32_t* __restrict__ list,
+                                                                const uint32_t* __restrict__ n_dev, size_t n_host,
+                                                                uint64_t* __restrict__ out_vals,
+                                                                uint8_t* __restrict__ out_st) {
   constexpr int S = 32 / G;
   __shared__ float p[kParams];
   for (int i = threadIdx.x; i < kParams; i += blockDim.x) p[i] = M.params[i];
@@ -357,9 +408,24 @@ __global__ void __launch_bounds__(256) learned_search_kernel(DevTree t, LearnedD
   const size_t n = n_dev ? (size_t)*n_dev : n_host;
   const uint32_t root = t.ctrl->root;
   const uint32_t root_level = t.ctrl->root_level;
-  const size_t stride = ((size_t)gridDim.x * blockDim.x) / G;
+  const size_t n_groups = ((size_t)gridDim.x * blockDim.x) / G;
+  const size_t gid = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
+  size_t q, q_end, stride;
+  if (kSorted) {
+    const size_t chunk = (n + n_groups - 1) / n_groups;
+    q = gid * chunk;
+    q_end = min(n, q + chunk);
+    stride = 1;
+  } else {
+    q = gid;
+    q_end = n;
+    stride = n_groups;
+  }
   unsigned long long hits = 0, falls = 0, probe = 0;
-  for (size_t q = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) / G; q < n; q += stride) {
+  uint32_t leaf = kNil;
+  uint64_t fence = 0;
+  uint64_t k[S], v[S];
+  for (; q < q_end; q += stride) {
     const uint32_t r = list ? __ldg(list + q) : (uint32_t)q;
     const uint64_t key = __ldg(qkeys + r);
     uint8_t st = kAbsent;
@@ -367,114 +433,31 @@ __global__ void __launch_bounds__(256) learned_search_kernel(DevTree t, LearnedD
     if (key == kKeyMax) {
       st = kRejected;
     } else if (root != kNil) {
-      // stage 1: MLP (each lane evaluates 32/G hidden units)
-      const float x = norm_x(key, M.kmin, M.inv_range);
-      float y = 0.f;
-#pragma unroll
-      for (int jj = 0; jj < kHidden / G; jj++) {
-        const int j = g + jj * G;
-        const float h = fmaf(p[j], x, p[kHidden + j]);
-        if (h > 0.f) y = fmaf(p[2 * kHidden + j], h, y);
-      }
-#pragma unroll
-      for (int o = G / 2; o >= 1; o >>= 1) y += __shfl_xor_sync(gmask, y, o, G);
-      y += p[3 * kHidden];
-      const uint32_t sj = seg_of_y(y, M.n_seg);
-      // stage 2: segment line and its error bound
-      SegParam sp;
-      {
-        const uint64_t* w = reinterpret_cast<const uint64_t*>(M.seg + sj);
-        sp.base = __ldg(w);
-        const uint64_t w1 = __ldg(w + 1), w2 = __ldg(w + 2);
-        sp.inv_span = __uint_as_float((uint32_t)w1);
-        sp.a = __uint_as_float((uint32_t)(w1 >> 32));
-        sp.b = __uint_as_float((uint32_t)w2);
-        sp.err = (uint32_t)(w2 >> 32);
-      }
-      // first probe: the G table entries around the prediction in one load
-      // (entries are {low, id}; the sentinel at n_leaves has low = UINT64_MAX)
-      const long long L = (long long)M.n_leaves;
-      bool ok = sp.err != kErrNone;
-      float pred = 0.f;
-      long long pc = 0;
-      if (ok) {
-        pred = seg_predict(sp, key);
-        if (!(pred > -1.0e9f && pred < 1.0e10f)) ok = false;
-        else {
-          pc = (long long)floorf(pred + 0.5f);
-          if (pc < 0) pc = 0;
-          if (pc > L - 1) pc = L - 1;
-        }
-      }
-      uint32_t slot = 0, node = 0;
-      bool found = false;
-      if (ok) {
-        long long p0 = pc - (G / 2 - 1);
-        if (p0 > L - G) p0 = L - G;
-        if (p0 < 0) p0 = 0;
-        const long long e = p0 + g;
-        ulonglong2 ent = make_ulonglong2(kKeyMax, 0);
-        if (e <= L) ent = __ldg(reinterpret_cast<const ulonglong2*>(M.tab) + e);
-        uint64_t above = kKeyMax;
-        if (g == 0 && p0 + G <= L) above = __ldg(&M.tab[p0 + G].low);
-        above = __shfl_sync(gmask, above, 0, G);
-        const uint32_t c = group_sum<G>(ent.x <= key ? 1u : 0u, gmask);
-        if (c >= 1 && (c < (uint32_t)G || above > key)) {
-          slot = (uint32_t)(p0 + c - 1);
-          node = (uint32_t)__shfl_sync(gmask, ent.y, c - 1, G);
-          found = true;
-        } else if (sp.err <= M.window) {
-          // second chance: the segment's whole error window
-          long long lo = (long long)floorf(pred) - (long long)sp.err - 1;
-          long long hi = (long long)ceilf(pred) + (long long)sp.err + 1;
-          if (lo < 0) lo = 0;
-          if (hi > L - 1) hi = L - 1;
-          if (lo <= hi) {
-            uint32_t cw = 0;
-            bool ab = false;
-            for (long long b = lo; b <= hi + 1; b += 4 * G) {
-              uint64_t lw[4];
-#pragma unroll
-              for (int u = 0; u < 4; u++) {
-                const long long ee = b + u * G + g;
-                lw[u] = ee <= hi + 1 ? __ldg(&M.tab[ee].low) : 0;
-              }
-#pragma unroll
-              for (int u = 0; u < 4; u++) {
-                const long long ee = b + u * G + g;
-                if (ee <= hi) cw += (lw[u] <= key) ? 1u : 0u;
-                else if (ee == hi + 1) ab = lw[u] > key;
-              }
-            }
-            cw = group_sum<G>(cw, gmask);
-            ab = __any_sync(gmask, ab);
-            if (cw >= 1 && (cw < (uint32_t)(hi - lo + 1) || ab)) {
-              slot = (uint32_t)(lo + cw - 1);
-              node = (uint32_t)__ldg(&M.tab[slot].id);
-              found = true;
-            }
+      bool have = kSorted && leaf != kNil && key < fence;  // same leaf as the previous key
+      if (!have) {
+        uint32_t dist = 0;
+        const uint32_t node = learned_leaf<G>(M, p, key, g, gmask, dist);
+        if (node != kNil) {
+          load_slots<S>(t.keys + (size_t)node * 32 + g * S, k);
+          fence = __shfl_sync(gmask, g == G - 1 ? __ldg(t.vals + (size_t)node * 32 + 31) : 0, G - 1, G);
+          if (g == G - 1) k[S - 1] = kKeyMax;
+          leaf = node;
+          have = key < fence;  // the leaf may have split since training
+          if (have) {
+            hits++;
+            probe += dist;
           }
         }
       }
-      bool done = false;
-      if (found) {
-        uint64_t k[S], v[S];
-        load_slots<S>(t.keys + (size_t)node * 32 + g * S, k);
-        const uint64_t fence = __shfl_sync(gmask, g == G - 1 ? __ldg(t.vals + (size_t)node * 32 + 31) : 0, G - 1, G);
-        if (key < fence) {
-          if (g == G - 1) k[S - 1] = kKeyMax;
-          uint32_t c = 0;
+      if (have) {
+        uint32_t c = 0;
 #pragma unroll
-          for (int i = 0; i < S; i++) c += (k[i] <= key) ? 1u : 0u;
-          c = group_sum<G>(c, gmask);
-          st = group_leaf_lookup<G, false>(t, node, key, g, gmask, k, v, c, ans);
-          done = true;
-          hits++;
-          probe += (unsigned long long)(pc > (long long)slot ? pc - (long long)slot : (long long)slot - pc);
-        }
-      }
-      if (!done) {
+        for (int i = 0; i < S; i++) c += (k[i] <= key) ? 1u : 0u;
+        c = group_sum<G>(c, gmask);
+        st = group_leaf_lookup<G, false>(t, leaf, key, g, gmask, k, v, c, ans);
+      } else {
         falls++;
+        leaf = kNil;
         st = group_descend<G, false>(t, root, root_level, key, g, gmask, ans);
       }
     }
@@ -667,14 +650,26 @@ cudaError_t launch_learned_search(Handle* h, const uint64_t* qkeys, const uint32
   M.window = L.window;
   const int threads = 256;
   const int G = h->learned_group;
-  size_t blocks = (n * (size_t)G + threads - 1) / threads;
-  const size_t cap = (size_t)h->sm_count * 8 * 4;
-  if (blocks > cap) blocks = cap;
-  switch (G) {
-    case 8: learned_search_kernel<8><<<(unsigned)blocks, threads, 0, s>>>(h->tree, M, qkeys, list, n_dev, n, out_vals, out_st); break;
-    case 16: learned_search_kernel<16><<<(unsigned)blocks, threads, 0, s>>>(h->tree, M, qkeys, list, n_dev, n, out_vals, out_st); break;
-    default: learned_search_kernel<32><<<(unsigned)blocks, threads, 0, s>>>(h->tree, M, qkeys, list, n_dev, n, out_vals, out_st); break;
+  const bool sorted = list != nullptr && h->sorted_search;  // batch lists are in ascending key order
+  size_t blocks;
+  if (sorted) {
+    blocks = (size_t)h->sm_count * 6;  // one resident wave (6 blocks per SM at 256 threads)
+  } else {
+    blocks = (n * (size_t)G + threads - 1) / threads;
+    const size_t cap = (size_t)h->sm_count * 8 * 4;
+    if (blocks > cap) blocks = cap;
   }
+#define BT_LSK(GG, SS) learned_search_kernel<GG, SS><<<(unsigned)blocks, threads, 0, s>>>(h->tree, M, qkeys, list, n_dev, n, out_vals, out_st)
+  if (sorted) {
+    if (G == 16) BT_LSK(16, true);
+    else if (G == 32) BT_LSK(32, true);
+    else BT_LSK(8, true);
+  } else {
+    if (G == 16) BT_LSK(16, false);
+    else if (G == 32) BT_LSK(32, false);
+    else BT_LSK(8, false);
+  }
+#undef BT_LSK
   count_launch();
   return cudaGetLastError();
 }

@@ -324,6 +324,76 @@ __device__ int tx_attempt(const DevTree& t, const uint64_t key, const uint64_t v
 // in-leaf update are exact.  Splits and failed checks go to tx_attempt.
 enum : int { FAST_DONE = 0, FAST_SLOW = 1, FAST_RETRY = 2 };
 
+// Insert into a candidate leaf by locking it first: CAS its header, then read
+// the row under the lock (no concurrent writer can change it), check epoch and
+// fences, and apply the update or the shift-insert.  A wrong leaf is unlocked
+// unchanged (retry); a full leaf is unlocked unchanged and goes to the
+// validated split path.
+__device__ int fast_insert_locked(const DevTree& t, const uint32_t epoch, const uint32_t node, const uint64_t key,
+                                  const uint64_t val, uint64_t& ans, uint8_t& st) {
+  const uint32_t lane = lane_id();
+  uint64_t* hp = hdr_ptr(t, node);
+  int ok = 0;
+  uint64_t h = 0;
+  if (lane == 0) {
+    h = ld_relaxed(hp);
+    if (!hdr_locked(h) && hdr_level(h) == 0 && hdr_epoch(h) == epoch)
+      ok = atomicCAS((unsigned long long*)hp, h, hdr_lock(h)) == h;
+  }
+  ok = __shfl_sync(kFull, ok, 0);
+  if (!ok) return FAST_RETRY;
+  h = __shfl_sync(kFull, h, 0);
+  __threadfence();
+  uint64_t k = ld_relaxed(t.keys + (size_t)node * 32 + lane);
+  const uint64_t v = ld_relaxed(t.vals + (size_t)node * 32 + lane);
+  const uint64_t lo = __shfl_sync(kFull, lane == 0 ? ld_relaxed(t.low + node) : 0, 0);
+  const uint64_t fence_key = __shfl_sync(kFull, v, 31);
+  const uint32_t size = hdr_size(h);
+  if (!(lo <= key && key < fence_key)) {
+    if (lane == 0) st_release(hp, h);
+    __syncwarp();
+    return FAST_RETRY;
+  }
+  if (lane == 31) k = kKeyMax;
+  const uint32_t mm = __ballot_sync(kFull, lane < size && k == key);
+  if (mm) {
+    const uint32_t at = __ffs(mm) - 1;
+    const uint64_t old = __shfl_sync(kFull, v, at);
+    if (lane == at) t.vals[(size_t)node * 32 + at] = val;
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) st_release(hp, hdr_next(h, size));
+    __syncwarp();
+    ans = old;
+    st = kFound;
+    return FAST_DONE;
+  }
+  if (size >= (uint32_t)kMaxKeys) {
+    if (lane == 0) st_release(hp, h);
+    __syncwarp();
+    return FAST_SLOW;
+  }
+  const uint32_t p = __popc(__ballot_sync(kFull, lane < size && k < key));
+  const uint64_t uk = __shfl_up_sync(kFull, k, 1);
+  const uint64_t uv = __shfl_up_sync(kFull, v, 1);
+  const uint64_t nk = lane < p ? k : (lane == p ? key : uk);
+  const uint64_t nv = lane < p ? v : (lane == p ? val : uv);
+  if (lane <= size && lane < 31) {
+    t.keys[(size_t)node * 32 + lane] = nk;
+    t.vals[(size_t)node * 32 + lane] = nv;
+  }
+  __threadfence();
+  __syncwarp();
+  if (lane == 0) {
+    st_release(hp, hdr_next(h, size + 1));
+    atomicAdd(&t.ctrl->n_keys, 1ull);
+  }
+  __syncwarp();
+  ans = 0;
+  st = kAbsent;
+  return FAST_DONE;
+}
+
 __device__ int tx_fast(const DevTree& t, const uint32_t epoch, const uint64_t key, const uint64_t val,
                        const bool is_insert, uint64_t& ans, uint8_t& st) {
   const uint32_t lane = lane_id();
@@ -340,8 +410,9 @@ __device__ int tx_fast(const DevTree& t, const uint32_t epoch, const uint64_t ke
     const uint32_t c = __popc(__ballot_sync(kFull, lane < 31 && kr <= key));
     node = (uint32_t)__shfl_sync(kFull, v, c);
   }
-  // seqlock read of the leaf
   const uint64_t* krow = t.keys + (size_t)node * 32;
+  if (is_insert) return fast_insert_locked(t, epoch, node, key, val, ans, st);
+  // seqlock read of the leaf
   const uint64_t h = ld_acquire(krow + 31);
   uint64_t k = ld_relaxed(krow + lane);
   const uint64_t v = ld_relaxed(t.vals + (size_t)node * 32 + lane);
@@ -402,7 +473,7 @@ __device__ int tx_fast(const DevTree& t, const uint32_t epoch, const uint64_t ke
   return FAST_DONE;
 }
 
-__global__ void __launch_bounds__(256) stm_kernel(DevTree t, const uint64_t* __restrict__ keys,
+__global__ void __launch_bounds__(256, 4) stm_kernel(DevTree t, const uint64_t* __restrict__ keys,
                                                   const uint64_t* __restrict__ vals, const uint8_t* __restrict__ ops,
                                                   uint32_t op_override, const uint32_t* __restrict__ list,
                                                   const uint32_t* __restrict__ n_dev, size_t n_host,
@@ -413,7 +484,13 @@ __global__ void __launch_bounds__(256) stm_kernel(DevTree t, const uint64_t* __r
   const size_t n_warps = ((size_t)gridDim.x * blockDim.x) >> 5;
   unsigned long long commits = 0, aborts = 0, exhausted = 0;
   const uint32_t epoch = t.ctrl->epoch;
-  for (size_t q = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < n; q += n_warps) {
+  // each warp takes a contiguous run of requests (the reference gives each
+  // warp 16 consecutive requests, bpt-gpustm-kernel.cu:41-56): neighbouring
+  // keys of a sorted list then land in one warp, not in concurrent warps
+  const size_t chunk = (n + n_warps - 1) / n_warps;
+  const size_t q_begin = (((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * chunk;
+  const size_t q_end = min(n, q_begin + chunk);
+  for (size_t q = q_begin; q < q_end; q++) {
     const uint32_t r = list ? list[q] : (uint32_t)q;
     const uint64_t key = keys[r];
     const uint32_t op = op_override <= 1 ? op_override : (uint32_t)ops[r];
@@ -484,8 +561,15 @@ cudaError_t launch_stm(Handle* h, const uint64_t* keys, const uint64_t* vals, co
                        cudaStream_t s) {
   if (n == 0) return cudaSuccess;
   const int threads = 256;  // 8 warps
+  // one resident wave: every warp runs at once, each on a contiguous run
+  static int per_sm[64] = {};
+  if (h->device < 64 && per_sm[h->device] == 0) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, stm_kernel, threads, 0) != cudaSuccess || b < 1) b = 2;
+    per_sm[h->device] = b;
+  }
   size_t blocks = (n * 32 + threads - 1) / threads;
-  const size_t cap = (size_t)h->sm_count * 8;  // 64 resident warps per SM
+  const size_t cap = (size_t)h->sm_count * (h->device < 64 ? per_sm[h->device] : 2);
   if (blocks > cap) blocks = cap;
   stm_kernel<<<(unsigned)blocks, threads, 0, s>>>(h->tree, keys, vals, ops, op_override, list, n_dev, n, out_vals,
                                                    out_st, h->retry_limit);

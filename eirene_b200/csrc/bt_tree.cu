@@ -125,6 +125,106 @@ __global__ void __launch_bounds__(256) search_kernel(DevTree t, const uint64_t* 
   }
 }
 
+// Search over keys given in ascending order (the batch executor's unique
+// GET list).  Each group walks a contiguous chunk of the list and keeps the
+// path of its previous lookup: lane l of the group caches level l's node id
+// and the exclusive upper bound of its key range.  A key restarts its descent
+// at the lowest cached level whose range still holds it (keys ascend, so only
+// the upper bound needs checking); a key in the previous leaf reuses the leaf
+// row already in registers.  Requires root_level < G.
+template <int G>
+__global__ void __launch_bounds__(256) search_sorted_kernel(DevTree t, const uint64_t* __restrict__ qkeys,
+                                                            const uint32_t* __restrict__ list,
+                                                            const uint32_t* __restrict__ n_dev, size_t n_host,
+                                                            uint64_t* __restrict__ out_vals,
+                                                            uint8_t* __restrict__ out_st) {
+  constexpr int S = 32 / G;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t g = lane % G;
+  const uint32_t gmask = group_mask<G>(lane);
+  const size_t n = n_dev ? (size_t)*n_dev : n_host;
+  const uint32_t root = t.ctrl->root;
+  const uint32_t root_level = t.ctrl->root_level;
+  const size_t n_groups = ((size_t)gridDim.x * blockDim.x) / G;
+  const size_t gid = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const size_t chunk = (n + n_groups - 1) / n_groups;
+  const size_t q0 = gid * chunk;
+  const size_t q1 = min(n, q0 + chunk);
+  // path cache (lane g holds level g)
+  uint32_t c_node = root;
+  uint64_t c_hi = 0;       // exclusive upper bound; 0 with c_valid = false
+  bool c_valid = (g == root_level);
+  if (c_valid) c_hi = kKeyMax;  // the root covers everything
+  uint64_t k[S];
+  uint64_t v[S];
+  uint32_t leaf = kNil;
+  for (size_t q = q0; q < q1; q++) {
+    const uint32_t r = list ? __ldg(list + q) : (uint32_t)q;
+    const uint64_t key = __ldg(qkeys + r);
+    uint8_t st = kAbsent;
+    uint64_t ans = 0;
+    if (key == kKeyMax) {
+      st = kRejected;
+    } else if (root != kNil) {
+      if (root_level >= (uint32_t)G) {  // tree taller than the cache: plain descent
+        st = group_descend<G, false>(t, root, root_level, key, g, gmask, ans);
+        if (g == 0) {
+          out_vals[r] = ans;
+          out_st[r] = st;
+        }
+        continue;
+      }
+      // lowest cached level whose range holds the key
+      const uint32_t hit = (__ballot_sync(gmask, c_valid && key < c_hi) >> (lane - g)) & ((1u << G) - 1u);
+      uint32_t level = hit ? (uint32_t)(__ffs(hit) - 1) : root_level;
+      uint32_t node = __shfl_sync(gmask, c_node, level, G);
+      uint64_t hi = __shfl_sync(gmask, c_hi, level, G);
+      if (!hit) {
+        node = root;
+        hi = kKeyMax;
+      }
+      // levels below `level` are now stale
+      if (g < level) c_valid = false;
+      uint32_t cnt = 0;
+      if (level == 0 && node == leaf) {
+        uint32_t c = 0;
+#pragma unroll
+        for (int i = 0; i < S; i++) c += (k[i] <= key) ? 1u : 0u;
+        cnt = group_sum<G>(c, gmask);
+      } else {
+        for (;;) {
+          const size_t row = (size_t)node * 32 + g * S;
+          load_slots<S>(t.keys + row, k);
+          if (level > 0) load_slots<S>(t.vals + row, v);
+          if (g == G - 1) k[S - 1] = kKeyMax;
+          uint32_t c = 0;
+#pragma unroll
+          for (int i = 0; i < S; i++) c += (k[i] <= key) ? 1u : 0u;
+          cnt = group_sum<G>(c, gmask);
+          if (level == 0) break;
+          // child range upper bound: key[cnt] (padding is UINT64_MAX) capped by ours
+          const uint64_t sep = __shfl_sync(gmask, pick<S>(k, cnt % S), cnt / S, G);
+          const uint64_t child_hi = sep < hi ? sep : hi;
+          node = (uint32_t)__shfl_sync(gmask, pick<S>(v, cnt % S), cnt / S, G);
+          hi = child_hi;
+          level--;
+          if (g == level) {
+            c_node = node;
+            c_hi = hi;
+            c_valid = true;
+          }
+        }
+        leaf = node;
+      }
+      st = group_leaf_lookup<G, false>(t, leaf, key, g, gmask, k, v, cnt, ans);
+    }
+    if (g == 0) {
+      out_vals[r] = ans;
+      out_st[r] = st;
+    }
+  }
+}
+
 // ---------------------------------------------------------- enumeration ----
 __global__ void child_count_kernel(DevTree t, const uint32_t* __restrict__ nodes, size_t n, uint32_t* cnt,
                                    int leaf_sizes) {
@@ -312,6 +412,24 @@ int tree_bulk_build_scratch(Handle* h, const uint64_t* keys, const uint64_t* val
   count_launch();
   if (cudaGetLastError() != cudaSuccess) return -2;
   return cudaStreamSynchronize(s) == cudaSuccess ? 0 : -2;
+}
+
+cudaError_t launch_search_sorted(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev,
+                                 size_t n, uint64_t* out_vals, uint8_t* out_st, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  // one resident wave of groups; each group takes a contiguous chunk
+  const int threads = 256;
+  static int per_sm[64] = {};
+  if (h->device < 64 && per_sm[h->device] == 0) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, search_sorted_kernel<8>, threads, 0) != cudaSuccess || b < 1)
+      b = 4;
+    per_sm[h->device] = b;
+  }
+  const size_t blocks = (size_t)h->sm_count * (h->device < 64 ? per_sm[h->device] : 4);
+  search_sorted_kernel<8><<<(unsigned)blocks, threads, 0, s>>>(h->tree, qkeys, list, n_dev, n, out_vals, out_st);
+  count_launch();
+  return cudaGetLastError();
 }
 
 cudaError_t launch_search(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev, size_t n,

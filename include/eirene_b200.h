@@ -175,6 +175,12 @@ int bt_set_descent(bt_handle *h, int descent);
 /* stage 1 root model: 1 = 1->32->1 MLP (default), 0 = linear */
 int bt_set_root_model(bt_handle *h, int mlp);
 int bt_set_search_group(bt_handle *h, uint32_t lanes);
+/* Tuning options (bt_set_option). */
+#define BT_OPT_SORTED_SEARCH 1 /* 1 (default): the batch's GET phase reuses the descent path across its
+                                  ascending unique keys; 0: one root descent per key */
+#define BT_OPT_RETRY_LIMIT 2   /* STM attempts per request */
+#define BT_OPT_TRAIN_STEPS 3   /* Adam steps of the learned root model per bt_retrain */
+int bt_set_option(bt_handle *h, int option, int64_t value);
 /* lanes per request in the learned search kernel: 8, 16 or 32 (default 8) */
 int bt_set_learned_group(bt_handle *h, uint32_t lanes);
 /* info[8]: valid, n_leaves, n_segments, segments over the window, window,
