@@ -270,6 +270,10 @@ def main():
             tree.set_descent(True)
         else:
             tree.set_descent(False)
+        # autotune lane counts / leaf loads on this tree with the first batch's keys,
+        # then pin the batch descent to the form being measured
+        tune = tree.autotune(batches[0][0], stream)
+        tree.set_option(E.OPT_BATCH_DESCENT, 1 if learned else 0)
         for i in range(args.warmup):
             tree.execute(*batches[i], ov, ost, mode=E.MODE_SORTED, stream=stream)
         tree.reset_stats()
@@ -295,7 +299,7 @@ def main():
         st = tree.stats()
         del batches
         return {"total_ms": total_ms, "step_ms": step_ms, "phases": phases, "counts": counts,
-                "launches": launches, "clocks": clocks, "stats": st, "learned_info": info}
+                "launches": launches, "clocks": clocks, "stats": st, "learned_info": info, "tune": tune}
 
     forms = {}
     if args.descent in ("plain", "both"):
@@ -305,8 +309,34 @@ def main():
             forms["learned"] = run_form(True, 20_000)
         except E.BTError as e:
             forms["learned_error"] = str(e)
-    head = "learned" if "learned" in forms else "plain"
+    # headline: the faster of the two forms (both are reported under "forms")
+    cands = [f for f in ("plain", "learned") if f in forms]
+    head = min(cands, key=lambda f: forms[f]["total_ms"])
     R = forms[head]
+
+    # unsorted point lookups (bt_search_batch on random keys): plain vs learned
+    random_lookup = {}
+    try:
+        rk = torch.empty(n_b, dtype=torch.int64, device="cuda")
+        rv = torch.empty(n_b, dtype=torch.int64, device="cuda")
+        ro = torch.empty(n_b, dtype=torch.uint8, device="cuda")
+        E.gen_requests(args.dist, 40_000 + rank, tk, n_b, 100, rk, rv, ro, stream)
+        for form in ("plain", "learned"):
+            if form == "learned" and "learned" not in forms:
+                continue
+            tree.set_descent(form == "learned")
+            for _ in range(3):
+                tree.search(rk, ov, ost, stream)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(5):
+                tree.search(rk, ov, ost, stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            random_lookup[form] = n_b * 5 / (e0.elapsed_time(e1) / 1e3) / 1e6
+        del rk, rv, ro
+    except E.BTError as ex:
+        random_lookup["error"] = str(ex)
     total_ms = allmax(R["total_ms"])
     value = world * n_b * args.steps / (total_ms / 1e3) / 1e6
 
@@ -394,6 +424,7 @@ def main():
                 "learned_hits": s["learned_hits"], "learned_fallbacks": s["learned_fallbacks"],
                 "mean_probe": s["learned_probe_sum"] / max(1, s["learned_hits"]),
                 "model": F.get("learned_info"),
+                "autotune": F.get("tune"),
             }
 
         line = {
@@ -417,6 +448,7 @@ def main():
             "p50_batch_ms": form_summary(R)["p50_batch_ms"],
             "p99_batch_ms": form_summary(R)["p99_batch_ms"],
             "forms": {k: form_summary(v) for k, v in forms.items() if isinstance(v, dict)},
+            "random_lookup_mops": random_lookup,
         }
         if "learned_error" in forms:
             line["learned_error"] = forms["learned_error"]

@@ -83,9 +83,9 @@ EXPORTS = [
     "bt_stats_get", "bt_stats_reset", "bt_retrain", "bt_set_descent", "bt_set_root_model", "bt_set_search_group",
     "bt_host_alloc", "bt_host_free", "bt_gen_keys", "bt_gen_requests", "bt_status_string",
     "bt_profile", "bt_profile_read", "bt_launch_count", "bt_bulk_build_static",
-    "bt_set_learned_group", "bt_learned_info", "bt_mlp_grad", "bt_set_option",
+    "bt_set_learned_group", "bt_learned_info", "bt_mlp_grad", "bt_set_option", "bt_autotune",
 ]
-OPT_SORTED_SEARCH, OPT_RETRY_LIMIT, OPT_TRAIN_STEPS = 1, 2, 3
+OPT_SORTED_SEARCH, OPT_RETRY_LIMIT, OPT_TRAIN_STEPS, OPT_SORTED_LEAF_VALS, OPT_BATCH_DESCENT = 1, 2, 3, 4, 5
 PHASES = ["sort", "merge", "search", "insert", "writeback"]
 
 _lib = None
@@ -139,6 +139,7 @@ def lib():
             "bt_learned_info": [_P, _P],
             "bt_mlp_grad": [_P, _P, _P, _P, _SZ, _P, _P, _P],
             "bt_set_option": [_P, ctypes.c_int, ctypes.c_int64],
+            "bt_autotune": [_P, _P, _SZ, _P, _P],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -300,6 +301,16 @@ class BTree:
 
     def set_option(self, option: int, value: int):
         _check(lib().bt_set_option(self._h, option, value), "bt_set_option")
+
+    def autotune(self, sample_keys, stream=None) -> dict:
+        rep = (ctypes.c_double * 16)()
+        _check(lib().bt_autotune(self._h, _ptr(sample_keys), sample_keys.numel(), _stream_ptr(stream), rep),
+               "bt_autotune")
+        r = list(rep)
+        return {"plain_lanes": int(r[0]), "learned_lanes": int(r[1]), "sorted_leaf_vals": int(r[2]),
+                "batch_descent": "learned" if r[3] == 1 else "plain",
+                "plain_ms": dict(zip([4, 8, 16, 32], r[4:8])), "learned_ms": dict(zip([8, 16, 32], r[8:11])),
+                "sorted_plain_ms": r[12:14], "sorted_learned_ms": r[14]}
 
     def set_learned_group(self, lanes: int):
         _check(lib().bt_set_learned_group(self._h, lanes), "bt_set_learned_group")

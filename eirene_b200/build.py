@@ -24,6 +24,7 @@ SOURCES = [
     "bt_api.cu",
     "bt_workload.cu",
     "bt_static.cu",
+    "bt_tune.cu",
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

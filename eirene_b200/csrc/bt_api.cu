@@ -231,7 +231,7 @@ int bt_search_batch(bt_handle* H, const uint64_t* keys, uint64_t* out_vals, uint
   // searches alone never conflict: run the search kernel directly on the batch
   cudaError_t e;
   if (h.descent == BT_DESCENT_LEARNED && h.L.valid)
-    e = bt::launch_learned_search(&h, keys, nullptr, nullptr, n, out_vals, out_status, S(stream));
+    e = bt::launch_learned_search(&h, keys, nullptr, nullptr, n, out_vals, out_status, S(stream), false);
   else
     e = bt::launch_search(&h, keys, nullptr, nullptr, n, out_vals, out_status, S(stream));
   return e == cudaSuccess ? BT_OK : BT_ERR_CUDA;
@@ -400,6 +400,11 @@ int bt_set_option(bt_handle* H, int option, int64_t value) {
   if (!H) return BT_ERR_INVALID_ARG;
   switch (option) {
     case BT_OPT_SORTED_SEARCH: H->h.sorted_search = value ? 1 : 0; return BT_OK;
+    case BT_OPT_SORTED_LEAF_VALS: H->h.sorted_leaf_vals = value ? 1 : 0; return BT_OK;
+    case BT_OPT_BATCH_DESCENT:
+      if (value < -1 || value > 1) return BT_ERR_INVALID_ARG;
+      H->h.batch_descent = (int)value;
+      return BT_OK;
     case BT_OPT_RETRY_LIMIT:
       if (value < 1 || value > 0x7fffffff) return BT_ERR_INVALID_ARG;
       H->h.retry_limit = (uint32_t)value;
@@ -410,6 +415,14 @@ int bt_set_option(bt_handle* H, int option, int64_t value) {
       return BT_OK;
     default: return BT_ERR_INVALID_ARG;
   }
+}
+
+int bt_autotune(bt_handle* H, const uint64_t* sample_keys, size_t n, void* stream, double* report) {
+  if (!H || !sample_keys || n == 0) return BT_ERR_INVALID_ARG;
+  DeviceGuard g(H->h.device);
+  cudaStream_t s = stream ? S(stream) : H->h.internal_stream;
+  if (stream == nullptr) cudaDeviceSynchronize();
+  return map_internal(bt::autotune(&H->h, sample_keys, n, s, report));
 }
 
 int bt_set_learned_group(bt_handle* H, uint32_t lanes) {

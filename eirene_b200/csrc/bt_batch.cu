@@ -374,8 +374,10 @@ int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const ui
   // search phase on the pre-batch tree, then the insert phase
   prof_mark(h, 2, s);
   cudaError_t e;
-  if (h->descent == 1 && h->L.valid)
-    e = launch_learned_search(h, w.ukeys, w.get_list, &w.counts->n_get, n, w.uans, w.uans_st, s);
+  const int desc = h->batch_descent >= 0 ? h->batch_descent : h->descent;
+  if (desc == 1 && h->L.valid)
+    e = launch_learned_search(h, w.ukeys, w.get_list, &w.counts->n_get, n, w.uans, w.uans_st, s,
+                              h->sorted_search != 0);
   else if (h->sorted_search)
     e = launch_search_sorted(h, w.ukeys, w.get_list, &w.counts->n_get, n, w.uans, w.uans_st, s);
   else

@@ -99,6 +99,8 @@ struct Handle {
   int search_group = 8;  // lanes per request in the lock-free search
   int learned_group = 8;  // lanes per request in the learned search
   int sorted_search = 1;  // batch GET phase: 1 = path-reusing search over the sorted keys
+  int sorted_leaf_vals = 0;  // sorted search: load the leaf's values with its keys (1) or only the match (0)
+  int batch_descent = -1;    // autotuned choice for the batch GET phase: -1 = follow `descent`
   int sm_count = 148;
   Work w;
   Learned L;
@@ -161,11 +163,14 @@ void work_free(Work* w);
 int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, uint64_t* out_vals,
                  uint8_t* out_st, size_t n, int engine, cudaStream_t s);
 
+// ---- autotuner (bt_tune.cu) ----
+int autotune(Handle* h, const uint64_t* keys, size_t n, cudaStream_t s, double* rep);
+
 // ---- learned predictor (bt_learned.cu) ----
 int learned_retrain(Handle* h, cudaStream_t s);
 void learned_free(Learned* L);
 cudaError_t launch_learned_search(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev,
-                                  size_t n, uint64_t* out_vals, uint8_t* out_st, cudaStream_t s);
+                                  size_t n, uint64_t* out_vals, uint8_t* out_st, cudaStream_t s, bool sorted);
 int learned_mlp_grad(Handle* h, const float* params, const float* x, const float* y, size_t n, float* grad_out,
                      float* loss_out, cudaStream_t s);
 

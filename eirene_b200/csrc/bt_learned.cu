@@ -636,7 +636,7 @@ int learned_retrain(Handle* h, cudaStream_t s) {
 }
 
 cudaError_t launch_learned_search(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev,
-                                  size_t n, uint64_t* out_vals, uint8_t* out_st, cudaStream_t s) {
+                                  size_t n, uint64_t* out_vals, uint8_t* out_st, cudaStream_t s, bool sorted) {
   if (n == 0) return cudaSuccess;
   Learned& L = h->L;
   LearnedDev M;
@@ -650,7 +650,6 @@ cudaError_t launch_learned_search(Handle* h, const uint64_t* qkeys, const uint32
   M.window = L.window;
   const int threads = 256;
   const int G = h->learned_group;
-  const bool sorted = list != nullptr && h->sorted_search;  // batch lists are in ascending key order
   size_t blocks;
   if (sorted) {
     blocks = (size_t)h->sm_count * 6;  // one resident wave (6 blocks per SM at 256 threads)

@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(256) search_kernel(DevTree t, const uint64_t* 
 // at the lowest cached level whose range still holds it (keys ascend, so only
 // the upper bound needs checking); a key in the previous leaf reuses the leaf
 // row already in registers.  Requires root_level < G.
-template <int G>
+template <int G, bool kLeafVals>
 __global__ void __launch_bounds__(256) search_sorted_kernel(DevTree t, const uint64_t* __restrict__ qkeys,
                                                             const uint32_t* __restrict__ list,
                                                             const uint32_t* __restrict__ n_dev, size_t n_host,
@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(256) search_sorted_kernel(DevTree t, const uin
         for (;;) {
           const size_t row = (size_t)node * 32 + g * S;
           load_slots<S>(t.keys + row, k);
-          if (level > 0) load_slots<S>(t.vals + row, v);
+          if (level > 0 || kLeafVals) load_slots<S>(t.vals + row, v);
           if (g == G - 1) k[S - 1] = kKeyMax;
           uint32_t c = 0;
 #pragma unroll
@@ -216,7 +216,7 @@ __global__ void __launch_bounds__(256) search_sorted_kernel(DevTree t, const uin
         }
         leaf = node;
       }
-      st = group_leaf_lookup<G, false>(t, leaf, key, g, gmask, k, v, cnt, ans);
+      st = group_leaf_lookup<G, kLeafVals>(t, leaf, key, g, gmask, k, v, cnt, ans);
     }
     if (g == 0) {
       out_vals[r] = ans;
@@ -419,15 +419,18 @@ cudaError_t launch_search_sorted(Handle* h, const uint64_t* qkeys, const uint32_
   if (n == 0) return cudaSuccess;
   // one resident wave of groups; each group takes a contiguous chunk
   const int threads = 256;
-  static int per_sm[64] = {};
-  if (h->device < 64 && per_sm[h->device] == 0) {
+  static int per_sm[64][2] = {};
+  const int lv = h->sorted_leaf_vals ? 1 : 0;
+  if (h->device < 64 && per_sm[h->device][lv] == 0) {
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, search_sorted_kernel<8>, threads, 0) != cudaSuccess || b < 1)
-      b = 4;
-    per_sm[h->device] = b;
+    cudaError_t e = lv ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, search_sorted_kernel<8, true>, threads, 0)
+                       : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, search_sorted_kernel<8, false>, threads, 0);
+    if (e != cudaSuccess || b < 1) b = 4;
+    per_sm[h->device][lv] = b;
   }
-  const size_t blocks = (size_t)h->sm_count * (h->device < 64 ? per_sm[h->device] : 4);
-  search_sorted_kernel<8><<<(unsigned)blocks, threads, 0, s>>>(h->tree, qkeys, list, n_dev, n, out_vals, out_st);
+  const size_t blocks = (size_t)h->sm_count * (h->device < 64 ? per_sm[h->device][lv] : 4);
+  if (lv) search_sorted_kernel<8, true><<<(unsigned)blocks, threads, 0, s>>>(h->tree, qkeys, list, n_dev, n, out_vals, out_st);
+  else search_sorted_kernel<8, false><<<(unsigned)blocks, threads, 0, s>>>(h->tree, qkeys, list, n_dev, n, out_vals, out_st);
   count_launch();
   return cudaGetLastError();
 }

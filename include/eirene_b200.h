@@ -180,7 +180,19 @@ int bt_set_search_group(bt_handle *h, uint32_t lanes);
                                   ascending unique keys; 0: one root descent per key */
 #define BT_OPT_RETRY_LIMIT 2   /* STM attempts per request */
 #define BT_OPT_TRAIN_STEPS 3   /* Adam steps of the learned root model per bt_retrain */
+#define BT_OPT_SORTED_LEAF_VALS 4 /* sorted search loads leaf values with the keys (1) or only the match (0) */
+#define BT_OPT_BATCH_DESCENT 5 /* batch GET phase: -1 follow bt_set_descent (default), 0 plain, 1 learned */
 int bt_set_option(bt_handle *h, int option, int64_t value);
+/* Autotuner: times the lookup configurations on this tree with n sample keys
+ * (device pointer, n <= max_batch) and keeps the fastest: lanes per request of
+ * the plain and the learned search, the sorted search's leaf-value load, and
+ * the descent used by the batch GET phase.  Read-only; synchronous.
+ * report (nullable, 16 doubles): [0] plain lanes, [1] learned lanes, [2] leaf
+ * values mode, [3] batch descent, [4..7] plain ms for 4/8/16/32 lanes,
+ * [8..10] learned ms for 8/16/32, [12..13] sorted plain ms (mode 0/1),
+ * [14] sorted learned ms.  No reference counterpart (the reference's launch
+ * shape is compile-time, src/gpu-stm-tree-v39/bpt-gpustm.h:25-38). */
+int bt_autotune(bt_handle *h, const uint64_t *sample_keys, size_t n, void *stream, double *report);
 /* lanes per request in the learned search kernel: 8, 16 or 32 (default 8) */
 int bt_set_learned_group(bt_handle *h, uint32_t lanes);
 /* info[8]: valid, n_leaves, n_segments, segments over the window, window,

@@ -127,3 +127,26 @@ def test_trained_mlp_root_beats_linear_root(gpu):
     lin, mlp = res[False], res[True]
     assert mlp[0] < lin[0], res
     assert mlp[2] <= lin[2], res
+
+
+def test_autotune_then_batches_stay_exact(gpu):
+    keys = O.gen_keys("uniform", 21, 300_000)
+    vals = O.value_of(keys)
+    t = E.BTree(max_keys=1 << 21, max_batch=1 << 18)
+    t.bulk_build(dev(keys), dev(vals))
+    o = O.OracleTree()
+    o.bulk_build(keys, vals)
+    t.retrain()
+    t.set_descent(True)
+    rk, rv, ro = O.gen_requests("uniform", 22, keys, 100_000, 95)
+    rep = t.autotune(dev(rk))
+    assert rep["plain_lanes"] in (4, 8, 16, 32) and rep["learned_lanes"] in (8, 16, 32)
+    assert all(v > 0 for v in rep["plain_ms"].values())
+    for desc in (0, 1, -1):
+        t.set_option(E.OPT_BATCH_DESCENT, desc)
+        for lv in (0, 1):
+            t.set_option(E.OPT_SORTED_LEAF_VALS, lv)
+            rk, rv, ro = O.gen_requests("uniform", 30 + desc * 2 + lv, keys, 50_000, 95)
+            ov, os_ = o.execute_merged(rk, rv, ro)
+            gv, gs = run_batch(t, rk, rv, ro, E.MODE_SORTED)
+            assert (gs == os_).all() and (gv == ov).all()
