@@ -25,6 +25,7 @@ SOURCES = [
     "bt_workload.cu",
     "bt_static.cu",
     "bt_tune.cu",
+    "bt_merge.cu",
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

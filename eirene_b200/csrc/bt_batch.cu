@@ -328,6 +328,18 @@ int work_alloc(Work* w, size_t cap) {
   A((void**)&w->pend, cap * 4);
   A((void**)&w->tiles, tiles * sizeof(TileSummary));
   A((void**)&w->counts, sizeof(BatchCounts));
+  A((void**)&w->m_path, cap * 32);
+  A((void**)&w->m_leaf, cap * 4);
+  A((void**)&w->m_isnew, cap * 4);
+  A((void**)&w->m_pos, cap * 4);
+  A((void**)&w->m_newk, cap * 8);
+  A((void**)&w->m_newv, cap * 8);
+  A((void**)&w->m_nq, cap * 4 + 64);
+  A((void**)&w->m_nleaf, cap * 4);
+  A((void**)&w->m_seg, cap * 4);
+  A((void**)&w->m_ent_a, cap * 16);
+  A((void**)&w->m_ent_b, cap * 16);
+  A((void**)&w->m_counts, 64);
   A((void**)&w->d_in_keys, cap * 8);
   A((void**)&w->d_in_vals, cap * 8);
   A((void**)&w->d_in_ops, cap);
@@ -342,9 +354,11 @@ int work_alloc(Work* w, size_t cap) {
 }
 
 void work_free(Work* w) {
-  void* ps[] = {w->k_a,     w->k_b,      w->v_a,       w->v_b,      w->sort_scratch, w->ukeys,     w->uvals,
-                w->uans,    w->uans_st,  w->ins_list,  w->get_list, w->pend,         w->tiles,     w->counts,
-                w->d_in_keys, w->d_in_vals, w->d_in_ops, w->d_out_vals, w->d_out_st};
+  void* ps[] = {w->k_a,      w->k_b,       w->v_a,       w->v_b,       w->sort_scratch, w->ukeys,   w->uvals,
+                w->uans,     w->uans_st,   w->ins_list,  w->get_list,  w->pend,         w->tiles,   w->counts,
+                w->m_path,   w->m_leaf,    w->m_isnew,   w->m_pos,     w->m_newk,       w->m_newv,  w->m_nq,
+                w->m_nleaf,  w->m_seg,     w->m_ent_a,   w->m_ent_b,   w->m_counts,     w->d_in_keys,
+                w->d_in_vals, w->d_in_ops, w->d_out_vals, w->d_out_st};
   for (void* p : ps)
     if (p) cudaFree(p);
   *w = Work{};
@@ -383,10 +397,15 @@ int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const ui
   else
     e = launch_search(h, w.ukeys, w.get_list, &w.counts->n_get, n, w.uans, w.uans_st, s);
   if (e != cudaSuccess) return -2;
-  (void)engine;
   prof_mark(h, 3, s);
-  e = launch_stm(h, w.ukeys, w.uvals, nullptr, kOpInsert, w.ins_list, &w.counts->n_ins, n, w.uans, w.uans_st, s);
-  if (e != cudaSuccess) return -2;
+  // the merge engine needs leaf_fill >= 16 and inner_fill >= 16: then a split
+  // emits at most one separator per new key or entry, which bounds its buffers
+  if (engine == 1 && h->leaf_fill >= 16 && h->inner_fill >= 16) {
+    if (merge_engine(h, n, s) != 0) return -2;
+  } else {
+    e = launch_stm(h, w.ukeys, w.uvals, nullptr, kOpInsert, w.ins_list, &w.counts->n_ins, n, w.uans, w.uans_st, s);
+    if (e != cudaSuccess) return -2;
+  }
   prof_mark(h, 4, s);
   const unsigned wb_blocks = (unsigned)min((size_t)h->sm_count * 8, (n + 255) / 256);
   writeback_kernel<<<wb_blocks, 256, 0, s>>>(sv, w.pend, n, w.uans, w.uans_st, out_vals, out_st);

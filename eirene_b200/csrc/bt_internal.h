@@ -57,6 +57,19 @@ struct Work {
   TileSummary* tiles = nullptr;
   uint64_t* tile_carry = nullptr;  // scratch for the tile pass
   BatchCounts* counts = nullptr;
+  // segmented leaf merge (bt_merge.cu)
+  uint32_t* m_path = nullptr;   // [cap][8] root-to-leaf path of each unique insert
+  uint32_t* m_leaf = nullptr;
+  uint32_t* m_isnew = nullptr;
+  uint32_t* m_pos = nullptr;
+  uint64_t* m_newk = nullptr;
+  uint64_t* m_newv = nullptr;
+  uint32_t* m_nq = nullptr;
+  uint32_t* m_nleaf = nullptr;
+  uint32_t* m_seg = nullptr;
+  void* m_ent_a = nullptr;      // separator entries, 16 B each
+  void* m_ent_b = nullptr;
+  void* m_counts = nullptr;
   // host staging for the host-buffer entry point
   uint64_t* d_in_keys = nullptr;
   uint64_t* d_in_vals = nullptr;
@@ -162,6 +175,9 @@ int work_alloc(Work* w, size_t cap);
 void work_free(Work* w);
 int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, uint64_t* out_vals,
                  uint8_t* out_st, size_t n, int engine, cudaStream_t s);
+
+// ---- segmented leaf merge (bt_merge.cu) ----
+int merge_engine(Handle* h, size_t n_upper, cudaStream_t s);
 
 // ---- autotuner (bt_tune.cu) ----
 int autotune(Handle* h, const uint64_t* keys, size_t n, cudaStream_t s, double* rep);

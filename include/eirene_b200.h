@@ -56,7 +56,8 @@ extern "C" {
 /* ---- batch modes (bt_execute_batch `mode`) ---- */
 #define BT_MODE_SORTED 0      /* sort-based batch merge, deterministic (reference v38 meaning) */
 #define BT_MODE_STM 1         /* unsorted warp-per-request STM (reference v39 meaning) */
-#define BT_MODE_MERGE_ENGINE 0x10 /* with BT_MODE_SORTED: apply new keys by segmented leaf merge */
+#define BT_MODE_MERGE_ENGINE 0x10 /* with BT_MODE_SORTED: apply new keys by segmented leaf merge
+                                      (needs leaf_fill >= 16 and inner_fill >= 16, else the STM engine runs) */
 
 /* ---- descent (bt_set_descent) ---- */
 #define BT_DESCENT_PLAIN 0

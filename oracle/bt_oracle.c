@@ -375,9 +375,12 @@ typedef struct entry { uint64_t key; uint32_t child; uint32_t parent; uint32_t p
 
 static void merge_engine(bto_tree *t, const uint64_t *nk, const uint64_t *nv, size_t m) {
     if (m == 0) return;
-    if (t->root == BTO_NIL) {
-        bto_bulk_build(t, nk, nv, m);
-        return;
+    if (t->root == BTO_NIL) { /* an empty leaf root to merge into (CREATE_NEW_TREE) */
+        uint32_t r = alloc_node(t);
+        n_set_info(t, r, 0, 0);
+        t->vals[r][31] = BTO_KEY_MAX;
+        t->low[r] = 0;
+        t->root = r;
     }
     uint32_t H = n_level(t, t->root) + 1;
     /* path of every new key: path[l] = node at level l, slots[l] = child slot */
