@@ -186,6 +186,8 @@ def main():
     ap.add_argument("--dist", default="uniform", choices=["uniform", "zipf", "normal", "gamma"])
     ap.add_argument("--descent", default="both", choices=["plain", "learned", "both"])
     ap.add_argument("--search-group", type=int, default=8)
+    ap.add_argument("--engine", default="merge", choices=["merge", "stm"],
+                    help="insert engine of the sorted batch: segmented leaf merge or warp STM")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-log2", type=int, default=20)
     args = ap.parse_args()
@@ -257,6 +259,7 @@ def main():
 
     ov = torch.empty(n_b, dtype=torch.int64, device="cuda")
     ost = torch.empty(n_b, dtype=torch.uint8, device="cuda")
+    MODE = E.MODE_SORTED | (E.MODE_MERGE_ENGINE if args.engine == "merge" else 0)
 
     def run_form(learned: bool, seed0: int):
         batches = make_batches(seed0)
@@ -275,7 +278,7 @@ def main():
         tune = tree.autotune(batches[0][0], stream)
         tree.set_option(E.OPT_BATCH_DESCENT, 1 if learned else 0)
         for i in range(args.warmup):
-            tree.execute(*batches[i], ov, ost, mode=E.MODE_SORTED, stream=stream)
+            tree.execute(*batches[i], ov, ost, mode=MODE, stream=stream)
         tree.reset_stats()
         tree.profile(True)
         tree.profile_read(reset=True)
@@ -286,7 +289,7 @@ def main():
         l0 = E.launch_count()
         ev[0].record(stream)
         for s in range(args.steps):
-            tree.execute(*batches[args.warmup + s], ov, ost, mode=E.MODE_SORTED, stream=stream)
+            tree.execute(*batches[args.warmup + s], ov, ost, mode=MODE, stream=stream)
             ev[s + 1].record(stream)
         torch.cuda.synchronize()
         launches = E.launch_count() - l0
@@ -383,7 +386,7 @@ def main():
         def host_step(b):
             k, v, o = b
             rc = L.bt_execute_batch_host(tree._h, k.data_ptr(), v.data_ptr(), o.data_ptr(), hov.data_ptr(),
-                                         hos.data_ptr(), n_b, E.MODE_SORTED, sp)
+                                         hos.data_ptr(), n_b, MODE, sp)
             if rc != 0:
                 raise E.BTError(rc, "bt_execute_batch_host")
 
@@ -434,7 +437,7 @@ def main():
             "config": {
                 "workload": f"2^{args.tree_log2} {args.dist} uint64 keys per GPU, batches of 2^{args.batch_log2} "
                             f"requests, {args.search_pct}% search / {100 - args.search_pct}% insert, "
-                            "sort-merged (v38 meaning)",
+                            f"sort-merged (v38 meaning), {args.engine} insert engine",
                 "descent": head, "tree_keys": n_tree, "batch": n_b, "search_group": args.search_group,
                 "l2": "inputs larger than L2: tree ~1.5 GB; every step reads its own 71 MB batch",
                 "parallelism": f"{world} independent tree(s), one per GPU",
