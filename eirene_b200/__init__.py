@@ -25,6 +25,8 @@ ERRORS = {
     -6: "batch larger than max_batch",
     -7: "learned predictor not trained",
     -8: "more keys than BT_STATIC_BUILD_MAX_KEYS",
+    -9: "no free slot or arena space",
+    -10: "timed out",
 }
 STATIC_BUILD_MAX_KEYS = 65536
 OP_INSERT, OP_GET = 0, 1
@@ -76,6 +78,17 @@ class Stats(ctypes.Structure):
     ]
 
 
+class ServeConfig(ctypes.Structure):
+    _fields_ = [("arena_bytes", ctypes.c_uint64), ("max_batches", ctypes.c_uint32), ("idle_us", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32 * 6)]
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [("batches", ctypes.c_uint64), ("requests", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint64),
+                ("in_flight", ctypes.c_uint64), ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
+                ("max_ms", ctypes.c_double), ("mean_ms", ctypes.c_double), ("mops", ctypes.c_double)]
+
+
 # every symbol the C header declares (checked by the CPU tests)
 EXPORTS = [
     "bt_config_init", "bt_create", "bt_destroy", "bt_bulk_build", "bt_execute_batch", "bt_execute_batch_host",
@@ -84,6 +97,7 @@ EXPORTS = [
     "bt_host_alloc", "bt_host_free", "bt_gen_keys", "bt_gen_requests", "bt_status_string",
     "bt_profile", "bt_profile_read", "bt_launch_count", "bt_bulk_build_static",
     "bt_set_learned_group", "bt_learned_info", "bt_mlp_grad", "bt_set_option", "bt_autotune",
+    "bt_serve_config_init", "bt_serve_start", "bt_submit", "bt_poll", "bt_wait", "bt_serve_get_stats", "bt_serve_stop",
 ]
 OPT_SORTED_SEARCH, OPT_RETRY_LIMIT, OPT_TRAIN_STEPS, OPT_SORTED_LEAF_VALS, OPT_BATCH_DESCENT = 1, 2, 3, 4, 5
 PHASES = ["sort", "merge", "search", "insert", "writeback"]
@@ -140,6 +154,13 @@ def lib():
             "bt_mlp_grad": [_P, _P, _P, _P, _SZ, _P, _P, _P],
             "bt_set_option": [_P, ctypes.c_int, ctypes.c_int64],
             "bt_autotune": [_P, _P, _SZ, _P, _P],
+            "bt_serve_config_init": [ctypes.POINTER(ServeConfig)],
+            "bt_serve_start": [_P, ctypes.POINTER(ServeConfig), ctypes.POINTER(_P)],
+            "bt_submit": [_P, _P, _P, _P, _SZ, _P, _P, ctypes.POINTER(ctypes.c_uint64)],
+            "bt_poll": [_P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int)],
+            "bt_wait": [_P, ctypes.c_uint64, ctypes.c_uint32],
+            "bt_serve_get_stats": [_P, ctypes.POINTER(ServeStats), ctypes.c_int],
+            "bt_serve_stop": [_P],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -341,3 +362,56 @@ def gen_requests(dist: str, seed: int, tree_keys, n: int, search_pct: int, keys,
     nt = 0 if tree_keys is None else tree_keys.numel()
     _check(lib().bt_gen_requests(DIST[dist], seed, _ptr(tree_keys), nt, n, search_pct, _ptr(keys), _ptr(vals),
                                  _ptr(ops), _stream_ptr(stream)), "bt_gen_requests")
+
+
+class Server:
+    """Continuous-batching server over one BTree (host numpy buffers)."""
+
+    def __init__(self, tree: "BTree", arena_bytes: int = 1 << 30, max_batches: int = 256, idle_us: int = 2000):
+        cfg = ServeConfig()
+        _check(lib().bt_serve_config_init(ctypes.byref(cfg)), "bt_serve_config_init")
+        cfg.arena_bytes, cfg.max_batches, cfg.idle_us = arena_bytes, max_batches, idle_us
+        h = _P()
+        _check(lib().bt_serve_start(tree._h, ctypes.byref(cfg), ctypes.byref(h)), "bt_serve_start")
+        self._s = h
+        self.tree = tree
+        self._keep = {}
+
+    def submit(self, keys, vals, ops, out_vals, out_status):
+        """Returns a ticket, or None when the server is busy (no slot / arena space)."""
+        t = ctypes.c_uint64(0)
+        rc = lib().bt_submit(self._s, keys.ctypes.data, vals.ctypes.data, ops.ctypes.data, keys.size,
+                             out_vals.ctypes.data, out_status.ctypes.data, ctypes.byref(t))
+        if rc == -9:
+            return None
+        _check(rc, "bt_submit")
+        self._keep[t.value] = (keys, vals, ops, out_vals, out_status)
+        return t.value
+
+    def poll(self, ticket) -> bool:
+        d = ctypes.c_int(0)
+        _check(lib().bt_poll(self._s, ticket, ctypes.byref(d)), "bt_poll")
+        if d.value == 1:
+            self._keep.pop(ticket, None)
+        return d.value == 1
+
+    def wait(self, ticket, timeout_ms: int = 120000):
+        _check(lib().bt_wait(self._s, ticket, timeout_ms), "bt_wait")
+        self._keep.pop(ticket, None)
+
+    def stats(self, reset: bool = False) -> dict:
+        st = ServeStats()
+        _check(lib().bt_serve_get_stats(self._s, ctypes.byref(st), 1 if reset else 0), "bt_serve_get_stats")
+        return {f: getattr(st, f) for f, _ in ServeStats._fields_}
+
+    def stop(self):
+        if getattr(self, "_s", None):
+            lib().bt_serve_stop(self._s)
+            self._s = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.stop()
+        except Exception:
+            pass

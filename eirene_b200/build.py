@@ -26,6 +26,7 @@ SOURCES = [
     "bt_static.cu",
     "bt_tune.cu",
     "bt_merge.cu",
+    "bt_serve.cu",
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -471,6 +471,8 @@ const char* bt_status_string(int code) {
     case BT_ERR_BATCH_TOO_LARGE: return "batch larger than max_batch";
     case BT_ERR_NOT_TRAINED: return "learned predictor not trained";
     case BT_ERR_STATIC_LIMIT: return "more keys than BT_STATIC_BUILD_MAX_KEYS";
+    case BT_ERR_BUSY: return "no free slot or arena space";
+    case BT_ERR_TIMEOUT: return "timed out";
     default: return "unknown status";
   }
 }

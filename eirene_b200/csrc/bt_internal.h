@@ -165,6 +165,31 @@ int enumerate_leaves(Handle* h, cudaStream_t s, uint32_t** leaf_ids, size_t* n_l
 cudaError_t leaf_sizes_device(Handle* h, const uint32_t* leaves, size_t n, uint32_t* out, cudaStream_t s);
 int tree_dump(Handle* h, uint64_t* out_keys, uint64_t* out_vals, size_t cap, size_t* n_out, cudaStream_t s);
 
+// ---- serving loop (bt_stm.cu device side, bt_serve.cu host side) ----
+constexpr int kServeChunk = 32;
+struct ServeDesc {
+  const uint64_t* keys;
+  const uint64_t* vals;
+  const uint8_t* ops;
+  uint64_t* out_vals;
+  uint8_t* out_st;
+  uint32_t n;
+  uint32_t seq;
+};
+struct ServeDev {
+  const ServeDesc* desc;  // [cap]
+  const uint32_t* tail;   // batches published
+  uint32_t* cursor;       // oldest batch with unclaimed requests
+  unsigned long long* claimed;  // [cap] per slot: batch seq << 32 | requests claimed
+  uint32_t* done;         // [cap] requests finished per slot
+  const uint32_t* stop;
+  uint32_t* host_done;              // [cap] mapped host memory: seq of the finished batch
+  unsigned long long* host_tend;    // [cap] mapped host memory: device clock at completion
+  uint32_t cap;
+  unsigned long long idle_ns;
+};
+cudaError_t launch_serve(Handle* h, const ServeDev& S, cudaStream_t s);
+
 // ---- STM kernels (bt_stm.cu) ----
 cudaError_t launch_stm(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, uint8_t op_override,
                        const uint32_t* list, const uint32_t* n_dev, size_t n, uint64_t* out_vals, uint8_t* out_st,

@@ -473,16 +473,83 @@ __device__ int tx_fast(const DevTree& t, const uint32_t epoch, const uint64_t ke
   return FAST_DONE;
 }
 
+struct TxCounters {
+  unsigned long long commits = 0, aborts = 0, exhausted = 0;
+};
+
+// One request, all 32 lanes: optimistic attempts, then the validated path.
+__device__ __forceinline__ void run_request(const DevTree& t, const uint32_t epoch, const uint64_t key,
+                                            const uint32_t op, const uint64_t val_in, const uint32_t retry_limit,
+                                            uint64_t& ans, uint8_t& st, TxCounters& cnt) {
+  const uint32_t lane = lane_id();
+  ans = 0;
+  st = kRejected;
+  if (key == kKeyMax || op > 1) return;
+  const bool ins = (op == kOpInsert);
+  const uint64_t val = ins ? val_in : 0;
+  uint32_t attempts = 0, fails = 0;
+  bool done = false;
+  // optimistic attempts first; a split or repeated failed checks go to the
+  // validated path below
+  for (int f = 0; f < 4 && !done; f++) {
+    attempts++;
+    const int res = tx_fast(t, epoch, key, val, ins, ans, st);
+    if (res == FAST_DONE) {
+      if (ins) cnt.commits++;
+      done = true;
+    } else if (res == FAST_SLOW) {
+      break;
+    } else {
+      cnt.aborts++;
+    }
+  }
+  while (!done) {
+    if (attempts++ >= retry_limit) {
+      st = kRetryExhausted;
+      ans = 0;
+      cnt.exhausted++;
+      if (lane == 0) atomicOr(&t.ctrl->error, kErrRetry);
+      break;
+    }
+    const int res = tx_attempt(t, key, val, ins, ans, st);
+    if (res == TX_DONE) {
+      if (ins) cnt.commits++;
+      break;
+    }
+    if (res == TX_AGAIN) {
+      cnt.commits++;
+      fails = 0;
+      continue;
+    }
+    if (res == TX_NOCAP) {
+      st = kNoCapacity;
+      ans = 0;
+      break;
+    }
+    cnt.aborts++;
+    fails++;
+    if (fails > 2) __nanosleep(32u << (fails < 8 ? fails : 8));
+  }
+}
+
+__device__ __forceinline__ void flush_counters(const DevTree& t, const TxCounters& c) {
+  if (lane_id() == 0) {
+    if (c.commits) atomicAdd(&t.ctrl->commits, c.commits);
+    if (c.aborts) atomicAdd(&t.ctrl->aborts, c.aborts);
+    if (c.exhausted) atomicAdd(&t.ctrl->retry_exhausted, c.exhausted);
+  }
+}
+
 __global__ void __launch_bounds__(256, 4) stm_kernel(DevTree t, const uint64_t* __restrict__ keys,
-                                                  const uint64_t* __restrict__ vals, const uint8_t* __restrict__ ops,
-                                                  uint32_t op_override, const uint32_t* __restrict__ list,
-                                                  const uint32_t* __restrict__ n_dev, size_t n_host,
-                                                  uint64_t* __restrict__ out_vals, uint8_t* __restrict__ out_st,
-                                                  uint32_t retry_limit) {
+                                                     const uint64_t* __restrict__ vals, const uint8_t* __restrict__ ops,
+                                                     uint32_t op_override, const uint32_t* __restrict__ list,
+                                                     const uint32_t* __restrict__ n_dev, size_t n_host,
+                                                     uint64_t* __restrict__ out_vals, uint8_t* __restrict__ out_st,
+                                                     uint32_t retry_limit) {
   const uint32_t lane = lane_id();
   const size_t n = n_dev ? (size_t)*n_dev : n_host;
   const size_t n_warps = ((size_t)gridDim.x * blockDim.x) >> 5;
-  unsigned long long commits = 0, aborts = 0, exhausted = 0;
+  TxCounters cnt;
   const uint32_t epoch = t.ctrl->epoch;
   // each warp takes a contiguous run of requests (the reference gives each
   // warp 16 consecutive requests, bpt-gpustm-kernel.cu:41-56): neighbouring
@@ -492,69 +559,131 @@ __global__ void __launch_bounds__(256, 4) stm_kernel(DevTree t, const uint64_t* 
   const size_t q_end = min(n, q_begin + chunk);
   for (size_t q = q_begin; q < q_end; q++) {
     const uint32_t r = list ? list[q] : (uint32_t)q;
-    const uint64_t key = keys[r];
     const uint32_t op = op_override <= 1 ? op_override : (uint32_t)ops[r];
-    uint64_t ans = 0;
-    uint8_t st = kRejected;
-    if (key != kKeyMax && op <= 1) {
-      const bool ins = (op == kOpInsert);
-      const uint64_t val = ins ? vals[r] : 0;
-      uint32_t attempts = 0, fails = 0;
-      bool done = false;
-      // optimistic attempts first; a split or repeated failed checks go to
-      // the validated path below
-      for (int f = 0; f < 4 && !done; f++) {
-        attempts++;
-        const int res = tx_fast(t, epoch, key, val, ins, ans, st);
-        if (res == FAST_DONE) {
-          if (ins) commits++;
-          done = true;
-        } else if (res == FAST_SLOW) {
-          break;
-        } else {
-          aborts++;
-        }
-      }
-      for (; !done;) {
-        if (attempts++ >= retry_limit) {
-          st = kRetryExhausted;
-          exhausted++;
-          if (lane == 0) atomicOr(&t.ctrl->error, kErrRetry);
-          break;
-        }
-        const int res = tx_attempt(t, key, val, ins, ans, st);
-        if (res == TX_DONE) {
-          if (ins) commits++;
-          break;
-        }
-        if (res == TX_AGAIN) {
-          commits++;
-          fails = 0;
-          continue;
-        }
-        if (res == TX_NOCAP) {
-          st = kNoCapacity;
-          ans = 0;
-          break;
-        }
-        aborts++;
-        fails++;
-        if (fails > 2) __nanosleep(32u << (fails < 8 ? fails : 8));
-      }
-    }
+    uint64_t ans;
+    uint8_t st;
+    run_request(t, epoch, keys[r], op, op == kOpInsert ? vals[r] : 0, retry_limit, ans, st, cnt);
     if (lane == 0) {
       out_vals[r] = ans;
       out_st[r] = st;
     }
   }
-  if (lane == 0) {
-    if (commits) atomicAdd(&t.ctrl->commits, commits);
-    if (aborts) atomicAdd(&t.ctrl->aborts, aborts);
-    if (exhausted) atomicAdd(&t.ctrl->retry_exhausted, exhausted);
+  flush_counters(t, cnt);
+}
+
+// ----------------------------------------------------------- serving ----
+// Persistent request loop of the server (bt_serve.cu).  Batches are published
+// into a ring of descriptors; `tail` counts published batches and `cursor` is
+// the oldest batch that still has unclaimed requests.  Every warp claims
+// kServeChunk consecutive requests of the cursor batch, runs them (v39
+// meaning: batches in flight together interleave), and the warp that
+// completes a batch writes its sequence number and the device clock to host
+// memory.  A warp that finds no work sleeps; after idle_ns without work (or
+// when stop is set) the kernel exits and the host relaunches it on demand.
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long v;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(v));
+  return v;
+}
+
+__global__ void __launch_bounds__(256, 4) serve_kernel(DevTree t, ServeDev S, uint32_t retry_limit) {
+  const uint32_t lane = lane_id();
+  TxCounters cnt;
+  const uint32_t epoch = t.ctrl->epoch;
+  unsigned long long idle_since = 0;
+  for (;;) {
+    uint32_t cur = 0, tail = 0, stop = 0;
+    if (lane == 0) {
+      tail = ld_acquire32(S.tail);
+      cur = ld_relaxed32(S.cursor);
+      stop = ld_relaxed32(S.stop);
+    }
+    cur = __shfl_sync(kFull, cur, 0);
+    tail = __shfl_sync(kFull, tail, 0);
+    stop = __shfl_sync(kFull, stop, 0);
+    if (cur >= tail) {
+      const unsigned long long now = global_ns();
+      if (stop) break;
+      if (idle_since == 0) idle_since = now;
+      else if (now - idle_since > S.idle_ns) break;
+      __nanosleep(2000);
+      continue;
+    }
+    idle_since = 0;
+    const uint32_t slot = cur % S.cap;
+    const ServeDesc d = S.desc[slot];
+    // claim a chunk of batch `cur` only: the slot's claim word carries the
+    // batch sequence in its high half, and a claim is a CAS against that
+    // sequence, so a warp holding a stale view never claims from the batch
+    // that later reuses the slot
+    uint32_t c = 0xFFFFFFFFu;
+    int action = 0;  // 0 retry, 1 claimed, 2 batch fully claimed
+    if (lane == 0) {
+      if (d.seq == cur) {
+        unsigned long long w = ld_relaxed(reinterpret_cast<const uint64_t*>(S.claimed + slot));
+        for (int tries = 0; tries < 64; tries++) {
+          if ((uint32_t)(w >> 32) != cur) break;
+          const uint32_t got = (uint32_t)w;
+          if (got >= d.n) {
+            action = 2;
+            break;
+          }
+          const unsigned long long prev = atomicCAS(S.claimed + slot, w, w + kServeChunk);
+          if (prev == w) {
+            c = got;
+            action = 1;
+            break;
+          }
+          w = prev;
+        }
+      }
+    }
+    action = __shfl_sync(kFull, action, 0);
+    c = __shfl_sync(kFull, c, 0);
+    if (action == 2) {
+      if (lane == 0) atomicCAS(S.cursor, cur, cur + 1);
+      continue;
+    }
+    if (action == 0) continue;
+    const uint32_t end = min(d.n, c + (uint32_t)kServeChunk);
+    for (uint32_t q = c; q < end; q++) {
+      uint64_t ans;
+      uint8_t st;
+      const uint32_t op = d.ops[q];
+      run_request(t, epoch, d.keys[q], op, op == kOpInsert ? d.vals[q] : 0, retry_limit, ans, st, cnt);
+      if (lane == 0) {
+        d.out_vals[q] = ans;
+        d.out_st[q] = st;
+      }
+    }
+    if (lane == 0) {
+      __threadfence();
+      const uint32_t prev = atomicAdd(&S.done[slot], end - c);
+      if (prev + (end - c) == d.n) {
+        __threadfence_system();
+        S.host_tend[slot] = global_ns();
+        asm volatile("st.release.sys.global.u32 [%0], %1;" ::"l"(S.host_done + slot), "r"(d.seq) : "memory");
+      }
+    }
+    __syncwarp();
   }
+  flush_counters(t, cnt);
 }
 
 }  // namespace
+
+cudaError_t launch_serve(Handle* h, const ServeDev& S, cudaStream_t s) {
+  static int per_sm[64] = {};
+  if (h->device < 64 && per_sm[h->device] == 0) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, serve_kernel, 256, 0) != cudaSuccess || b < 1) b = 2;
+    per_sm[h->device] = b;
+  }
+  const unsigned blocks = (unsigned)(h->sm_count * (h->device < 64 ? per_sm[h->device] : 2));
+  serve_kernel<<<blocks, 256, 0, s>>>(h->tree, S, h->retry_limit);
+  count_launch();
+  return cudaGetLastError();
+}
 
 cudaError_t launch_stm(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, uint8_t op_override,
                        const uint32_t* list, const uint32_t* n_dev, size_t n, uint64_t* out_vals, uint8_t* out_st,

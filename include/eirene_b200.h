@@ -41,6 +41,8 @@ extern "C" {
 #define BT_ERR_BATCH_TOO_LARGE -6 /* n > bt_config.max_batch */
 #define BT_ERR_NOT_TRAINED -7     /* learned descent requested before bt_retrain */
 #define BT_ERR_STATIC_LIMIT -8    /* n > BT_STATIC_BUILD_MAX_KEYS in bt_bulk_build_static */
+#define BT_ERR_BUSY -9            /* serving: no free slot or arena space now; retry after a completion */
+#define BT_ERR_TIMEOUT -10        /* serving: bt_wait ran out of time */
 
 /* ---- request op codes (same numbering as src/input-helper.h:14-17) ---- */
 #define BT_OP_INSERT 0
@@ -219,6 +221,45 @@ uint64_t bt_launch_count(void);
 /* Pinned host memory helpers for bt_execute_batch_host callers. */
 int bt_host_alloc(void **p, size_t bytes);
 int bt_host_free(void *p);
+
+/* ---- serving loop (continuous batching) ----
+ * No reference counterpart: the reference runs batches one after another from
+ * one host thread (src/gpu-stm-tree-v39/bpt-gpustm.cpp:78-105).
+ * A server owns a device arena and a ring of batch slots.  bt_submit admits a
+ * batch when a slot and enough arena bytes are free (else BT_ERR_BUSY), copies
+ * it in and publishes it to a persistent kernel (graph-launched, relaunched on
+ * demand) whose warps take chunks of the oldest unfinished batch, so batches
+ * submitted while others run overlap on the device.  Requests run under the
+ * STM meaning (BT_MODE_STM): batches in flight together may interleave on
+ * shared keys; a batch whose keys no other in-flight batch touches gets the
+ * answers it would get alone.  Host buffers: pageable inputs may be reused
+ * when bt_submit returns, pinned inputs only after completion; output buffers
+ * must stay valid until completion.  One server per handle; do not mix with
+ * other batch calls on that handle while it runs. */
+typedef struct bt_server bt_server;
+typedef struct bt_serve_config {
+    uint64_t arena_bytes;  /* device memory for batches in flight: 26 B per request (default 1 GiB) */
+    uint32_t max_batches;  /* ring slots (default 256) */
+    uint32_t idle_us;      /* the persistent kernel exits after this long without work (default 2000) */
+    uint32_t reserved[6];
+} bt_serve_config;
+typedef struct bt_serve_stats {
+    uint64_t batches;          /* completed since start / last reset */
+    uint64_t requests;
+    uint64_t kernel_launches;  /* persistent-kernel launches (graph replays) */
+    uint64_t in_flight;
+    double p50_ms, p99_ms, max_ms, mean_ms;  /* batch latency: submit -> answers in host memory */
+    double mops;                             /* completed requests / (last completion - first submit) */
+} bt_serve_stats;
+int bt_serve_config_init(bt_serve_config *cfg);
+int bt_serve_start(bt_handle *h, const bt_serve_config *cfg, bt_server **out);
+int bt_submit(bt_server *s, const uint64_t *keys_host, const uint64_t *vals_host, const uint8_t *ops_host,
+              size_t n, uint64_t *out_vals_host, uint8_t *out_status_host, uint64_t *ticket);
+/* *done = 1 when the batch's answers are in its output buffers, 0 if not yet, -1 unknown ticket */
+int bt_poll(bt_server *s, uint64_t ticket, int *done);
+int bt_wait(bt_server *s, uint64_t ticket, uint32_t timeout_ms /* 0 = no limit */);
+int bt_serve_get_stats(bt_server *s, bt_serve_stats *st, int reset);
+int bt_serve_stop(bt_server *s);
 
 /* ---- benchmark input generators (seeded, counter based; device output) ----
  * dist: 0 uniform keys in [0, 2^63), 1 Zipf(0.99) ranks over 2^32 hashed to
