@@ -165,6 +165,82 @@ def run_reference(args):
 
 
 # ----------------------------------------------------------------------------
+def serve_bench(E, np, tree, tk_host, n_tree, seconds=1.5, seed=5):
+    """Serving loop (continuous batching): batch sizes log-uniform over
+    2^10..2^22, per-batch search fraction uniform in [0.5, 1], Poisson arrivals.
+    Phase 1 submits as fast as admission allows (capacity); phase 2 offers 50 %
+    of that capacity with Poisson arrivals and reports the batch latency."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    n_pool = 1 << 22
+    fracs = [0.5, 0.6, 0.7, 0.8, 0.9, 1.0]
+    pools = []
+    keep = []
+    for i, f in enumerate(fracs):
+        k = torch.empty(n_pool, dtype=torch.int64, device="cuda")
+        v = torch.empty(n_pool, dtype=torch.int64, device="cuda")
+        o = torch.empty(n_pool, dtype=torch.uint8, device="cuda")
+        E.gen_requests("uniform", 50_000 + i, tk_host, n_pool, int(round(f * 100)), k, v, o)
+        kp, vp, op = k.cpu().pin_memory(), v.cpu().pin_memory(), o.cpu().pin_memory()  # pinned host pools
+        keep.append((kp, vp, op))
+        pools.append((kp.numpy().view(np.uint64), vp.numpy().view(np.uint64), op.numpy()))
+        del k, v, o
+    ov_t = torch.empty(n_pool, dtype=torch.int64).pin_memory()
+    os_t = torch.empty(n_pool, dtype=torch.uint8).pin_memory()
+    out_v = ov_t.numpy().view(np.uint64)
+    out_s = os_t.numpy()
+    srv = E.Server(tree, arena_bytes=3 << 30, max_batches=512)
+
+    def draw():
+        n = int(2 ** rng.uniform(10, 22))
+        p = pools[int(np.argmin([abs(f - rng.uniform(0.5, 1.0)) for f in fracs]))]
+        off = int(rng.integers(0, n_pool - n + 1))
+        return p[0][off:off + n], p[1][off:off + n], p[2][off:off + n], out_v[:n], out_s[:n]
+
+    def run(duration, rate):
+        srv.stats(reset=True)
+        t0 = time.perf_counter()
+        pending = []
+        next_t = t0
+        n_sub = 0
+        while True:
+            now = time.perf_counter()
+            if now - t0 > duration:
+                break
+            if rate is None or now >= next_t:
+                b = draw()
+                tk = srv.submit(*b)
+                if tk is None:
+                    if pending:
+                        srv.wait(pending.pop(0))
+                    continue
+                pending.append(tk)
+                n_sub += 1
+                if rate is not None:
+                    next_t += rng.exponential(1.0 / rate)
+            else:
+                while pending and srv.poll(pending[0]):
+                    pending.pop(0)
+                time.sleep(min(0.0002, max(0.0, next_t - now)))
+        for tk in pending:
+            srv.wait(tk)
+        return srv.stats(reset=False), n_sub
+
+    cap, _ = run(seconds, None)
+    mean_batch = (2.0 ** 22 - 2.0 ** 10) / np.log(2.0 ** 12)  # mean of the log-uniform size law
+    rate = 0.5 * cap["mops"] * 1e6 / mean_batch
+    lat, n_sub = run(seconds, rate)
+    srv.stop()
+    return {"capacity_mops": cap["mops"], "capacity_batches": cap["batches"],
+            "offered_batches_per_s": rate, "mops": lat["mops"], "batches": lat["batches"],
+            "p50_batch_ms": lat["p50_ms"], "p99_batch_ms": lat["p99_ms"], "max_batch_ms": lat["max_ms"],
+            "kernel_launches": lat["kernel_launches"],
+            "workload": "batch sizes log-uniform 2^10..2^22, search fraction U[0.5,1] per batch, Poisson arrivals "
+                        "at 50% of the measured capacity; latency = submit to answers in host memory"}
+
+
+# ----------------------------------------------------------------------------
 def unique_op_counts(torch, k, o):
     """(unique GET keys, unique INSERT keys) of a batch under the merged meaning."""
     u, inv = torch.unique(k, return_inverse=True)
@@ -190,6 +266,8 @@ def main():
                     help="insert engine of the sorted batch: segmented leaf merge or warp STM")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-log2", type=int, default=20)
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=1.5)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -405,6 +483,17 @@ def main():
                "h2d_bytes_per_step": n_b * 17, "d2h_bytes_per_step": n_b * 9,
                "steps": e2e_steps, "descent": head}
 
+    serving = {}
+    if not args.no_serve:
+        for form in ("plain", "learned"):
+            if form == "learned" and "learned" not in forms:
+                continue
+            try:
+                tree.set_descent(form == "learned")
+                serving[form] = serve_bench(E, np, tree, tk, n_tree, seconds=args.serve_seconds, seed=5 + rank)
+            except Exception as ex:  # reported, not fatal
+                serving[form] = {"error": str(ex)}
+
     launches = allsum(R["launches"])
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -452,6 +541,7 @@ def main():
             "p99_batch_ms": form_summary(R)["p99_batch_ms"],
             "forms": {k: form_summary(v) for k, v in forms.items() if isinstance(v, dict)},
             "random_lookup_mops": random_lookup,
+            "serving": serving,
         }
         if "learned_error" in forms:
             line["learned_error"] = forms["learned_error"]

@@ -204,6 +204,10 @@ int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const ui
 // ---- segmented leaf merge (bt_merge.cu) ----
 int merge_engine(Handle* h, size_t n_upper, cudaStream_t s);
 
+// device view of the learned model when the learned descent is on and trained
+struct LearnedDev;
+int learned_dev(Handle* h, LearnedDev* out);
+
 // ---- autotuner (bt_tune.cu) ----
 int autotune(Handle* h, const uint64_t* keys, size_t n, cudaStream_t s, double* rep);
 

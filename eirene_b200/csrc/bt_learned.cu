@@ -27,22 +27,10 @@
 
 #include "bt_common.cuh"
 #include "bt_internal.h"
+#include "bt_learned.cuh"
 #include "bt_search.cuh"
 
 namespace bt {
-
-struct LeafEnt {
-  uint64_t low;
-  uint64_t id;
-};
-
-struct SegParam {
-  uint64_t base;
-  float inv_span;
-  float a;
-  float b;
-  uint32_t err;
-};
 
 struct SegAcc {
   unsigned long long kmin;
@@ -54,18 +42,10 @@ struct SegAcc {
 
 namespace {
 
-constexpr int kHidden = 32;
-constexpr int kParams = 3 * kHidden + 1;  // w1[32] b1[32] w2[32] b2
 constexpr int kGradBlocks = 148;
 constexpr int kGradThreads = 256;
 constexpr int kPartStride = kParams + 1;  // + loss
-constexpr uint32_t kErrNone = 0xFFFFFFFFu;
 
-__device__ __forceinline__ float norm_x(uint64_t key, uint64_t kmin, double inv_range) {
-  if (key <= kmin) return 0.f;
-  const double x = (double)(key - kmin) * inv_range;
-  return x >= 1.0 ? 1.f : (float)x;
-}
 
 __device__ __forceinline__ float mlp_fwd(const float* p, float x) {
   float y = p[3 * kHidden];
@@ -77,18 +57,7 @@ __device__ __forceinline__ float mlp_fwd(const float* p, float x) {
   return y;
 }
 
-__device__ __forceinline__ uint32_t seg_of_y(float y, uint32_t n_seg) {
-  float f = y * (float)n_seg;
-  if (!(f > 0.f)) return 0;
-  if (f >= (float)(n_seg - 1)) return n_seg - 1;
-  return (uint32_t)f;
-}
 
-// slot predicted by a segment line, in the exact arithmetic the lookup uses
-__device__ __forceinline__ float seg_predict(const SegParam& sp, uint64_t key) {
-  const float d = key >= sp.base ? (float)(key - sp.base) : -(float)(sp.base - key);
-  return fmaf(sp.b, d * sp.inv_span, sp.a);
-}
 
 // ---------------------------------------------------------------- tables ----
 __global__ void leaf_table_kernel(DevTree t, const uint32_t* __restrict__ ids, size_t L, LeafEnt* __restrict__ tab) {
@@ -329,65 +298,6 @@ __global__ void seg_count_bad_kernel(const SegParam* __restrict__ sp, uint32_t n
 }
 
 // ----------------------------------------------------------------- lookup ----
-struct LearnedDev {
-  const LeafEnt* tab;
-  const SegParam* seg;
-  const float* params;
-  uint64_t kmin;
-  double inv_range;
-  uint32_t n_leaves;
-  uint32_t n_seg;
-  uint32_t window;
-};
-
-// Predicted leaf for `key`: stage 1 (MLP) -> segment -> line -> one probe of
-// the G leaf-table entries around the predicted slot.  Returns the leaf's node
-// id, or kNil when the probe does not bracket the key (caller falls back).
-template <int G>
-__device__ __forceinline__ uint32_t learned_leaf(const LearnedDev& M, const float* p, uint64_t key, uint32_t g,
-                                                 uint32_t gmask, uint32_t& dist) {
-  const float x = norm_x(key, M.kmin, M.inv_range);
-  float y = 0.f;
-#pragma unroll
-  for (int jj = 0; jj < kHidden / G; jj++) {
-    const int j = g + jj * G;
-    const float h = fmaf(p[j], x, p[kHidden + j]);
-    if (h > 0.f) y = fmaf(p[2 * kHidden + j], h, y);
-  }
-#pragma unroll
-  for (int o = G / 2; o >= 1; o >>= 1) y += __shfl_xor_sync(gmask, y, o, G);
-  y += p[3 * kHidden];
-  const uint64_t* w = reinterpret_cast<const uint64_t*>(M.seg + seg_of_y(y, M.n_seg));
-  SegParam sp;
-  sp.base = __ldg(w);
-  const uint64_t w1 = __ldg(w + 1), w2 = __ldg(w + 2);
-  sp.inv_span = __uint_as_float((uint32_t)w1);
-  sp.a = __uint_as_float((uint32_t)(w1 >> 32));
-  sp.b = __uint_as_float((uint32_t)w2);
-  if ((uint32_t)(w2 >> 32) == kErrNone) return kNil;  // segment without a model
-  const float pred = seg_predict(sp, key);
-  const int L = (int)M.n_leaves;
-  int pc = (pred > 0.f) ? (pred < (float)(L - 1) ? __float2int_rn(pred) : L - 1) : 0;
-  // probe the G entries [p0, p0 + G) and the one above them
-  int p0 = pc - (G / 2 - 1);
-  p0 = p0 > L - G ? L - G : p0;
-  p0 = p0 < 0 ? 0 : p0;
-  const int e = p0 + (int)g;
-  ulonglong2 ent = make_ulonglong2(kKeyMax, 0);
-  if (e <= L) ent = __ldg(reinterpret_cast<const ulonglong2*>(M.tab) + e);
-  uint64_t above = kKeyMax;
-  if (g == 0 && p0 + G <= L) above = __ldg(&M.tab[p0 + G].low);
-  above = __shfl_sync(gmask, above, 0, G);
-  const uint32_t c = group_sum<G>(ent.x <= key ? 1u : 0u, gmask);
-  const uint32_t node = (uint32_t)__shfl_sync(gmask, ent.y, (c + G - 1) % G, G);
-  if (c >= 1 && (c < (uint32_t)G || above > key)) {
-    const int slot = p0 + (int)c - 1;
-    dist = (uint32_t)(pc > slot ? pc - slot : slot - pc);
-    return node;
-  }
-  return kNil;
-}
-
 // kSorted: keys arrive in ascending order (the batch's unique GETs); each
 // group walks a contiguous chunk and reuses the previous leaf while the key
 // stays below its fence.  Otherwise a grid-stride loop over any keys.
@@ -671,6 +581,20 @@ cudaError_t launch_learned_search(Handle* h, const uint64_t* qkeys, const uint32
 #undef BT_LSK
   count_launch();
   return cudaGetLastError();
+}
+
+int learned_dev(Handle* h, LearnedDev* M) {
+  Learned& L = h->L;
+  if (!(h->descent == 1 && L.valid)) return 0;
+  M->tab = reinterpret_cast<const LeafEnt*>(L.leaf_low);
+  M->seg = reinterpret_cast<const SegParam*>(L.seg);
+  M->params = L.mlp;
+  M->kmin = L.kmin;
+  M->inv_range = 1.0 / (double)(L.kmax - L.kmin);
+  M->n_leaves = L.n_leaves;
+  M->n_seg = L.n_segments;
+  M->window = L.window;
+  return 1;
 }
 
 // gradient of the MSE of the MLP over (x, y) on the device (diagnostics / tests)

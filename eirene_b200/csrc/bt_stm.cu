@@ -16,6 +16,7 @@
 
 #include "bt_common.cuh"
 #include "bt_internal.h"
+#include "bt_learned.cuh"
 
 namespace bt {
 
@@ -395,12 +396,21 @@ __device__ int fast_insert_locked(const DevTree& t, const uint32_t epoch, const 
 }
 
 __device__ int tx_fast(const DevTree& t, const uint32_t epoch, const uint64_t key, const uint64_t val,
-                       const bool is_insert, uint64_t& ans, uint8_t& st) {
+                       const bool is_insert, uint64_t& ans, uint8_t& st, const LearnedDev* M) {
   const uint32_t lane = lane_id();
   Ctrl* C = t.ctrl;
   uint32_t node = ld_relaxed32(&C->root);
   if (node == kNil) return FAST_SLOW;
-  for (int depth = 0;; depth++) {
+  // the learned model proposes the leaf; the leaf checks below make any
+  // proposal safe, and a miss falls back to the descent
+  uint32_t guess = kNil;
+  if (M) {
+    uint32_t dist = 0;
+    guess = learned_leaf<32>(*M, M->params, key, lane, kFull, dist);
+    if (guess >= t.cap) guess = kNil;
+  }
+  if (guess != kNil) node = guess;
+  for (int depth = 0; guess == kNil; depth++) {
     if (depth > 40 || node >= t.cap) return FAST_SLOW;
     const uint64_t* krow = t.keys + (size_t)node * 32;
     const uint64_t kr = krow[lane];
@@ -480,7 +490,7 @@ struct TxCounters {
 // One request, all 32 lanes: optimistic attempts, then the validated path.
 __device__ __forceinline__ void run_request(const DevTree& t, const uint32_t epoch, const uint64_t key,
                                             const uint32_t op, const uint64_t val_in, const uint32_t retry_limit,
-                                            uint64_t& ans, uint8_t& st, TxCounters& cnt) {
+                                            uint64_t& ans, uint8_t& st, TxCounters& cnt, const LearnedDev* M) {
   const uint32_t lane = lane_id();
   ans = 0;
   st = kRejected;
@@ -493,7 +503,7 @@ __device__ __forceinline__ void run_request(const DevTree& t, const uint32_t epo
   // validated path below
   for (int f = 0; f < 4 && !done; f++) {
     attempts++;
-    const int res = tx_fast(t, epoch, key, val, ins, ans, st);
+    const int res = tx_fast(t, epoch, key, val, ins, ans, st, f == 0 ? M : nullptr);
     if (res == FAST_DONE) {
       if (ins) cnt.commits++;
       done = true;
@@ -545,9 +555,10 @@ __global__ void __launch_bounds__(256, 4) stm_kernel(DevTree t, const uint64_t* 
                                                      uint32_t op_override, const uint32_t* __restrict__ list,
                                                      const uint32_t* __restrict__ n_dev, size_t n_host,
                                                      uint64_t* __restrict__ out_vals, uint8_t* __restrict__ out_st,
-                                                     uint32_t retry_limit) {
+                                                     uint32_t retry_limit, LearnedDev lm, int use_learned) {
   const uint32_t lane = lane_id();
   const size_t n = n_dev ? (size_t)*n_dev : n_host;
+  const LearnedDev* M = use_learned ? &lm : nullptr;
   const size_t n_warps = ((size_t)gridDim.x * blockDim.x) >> 5;
   TxCounters cnt;
   const uint32_t epoch = t.ctrl->epoch;
@@ -562,7 +573,7 @@ __global__ void __launch_bounds__(256, 4) stm_kernel(DevTree t, const uint64_t* 
     const uint32_t op = op_override <= 1 ? op_override : (uint32_t)ops[r];
     uint64_t ans;
     uint8_t st;
-    run_request(t, epoch, keys[r], op, op == kOpInsert ? vals[r] : 0, retry_limit, ans, st, cnt);
+    run_request(t, epoch, keys[r], op, op == kOpInsert ? vals[r] : 0, retry_limit, ans, st, cnt, M);
     if (lane == 0) {
       out_vals[r] = ans;
       out_st[r] = st;
@@ -580,14 +591,32 @@ __global__ void __launch_bounds__(256, 4) stm_kernel(DevTree t, const uint64_t* 
 // completes a batch writes its sequence number and the device clock to host
 // memory.  A warp that finds no work sleeps; after idle_ns without work (or
 // when stop is set) the kernel exits and the host relaunches it on demand.
+// descriptor written by the copy engine while the kernel runs: coherent loads
+__device__ __forceinline__ ServeDesc load_desc(const ServeDesc* p) {
+  static_assert(sizeof(ServeDesc) == 48, "ServeDesc layout");
+  const uint64_t* w = reinterpret_cast<const uint64_t*>(p);
+  ServeDesc d;
+  d.keys = reinterpret_cast<const uint64_t*>(ld_relaxed(w + 0));
+  d.vals = reinterpret_cast<const uint64_t*>(ld_relaxed(w + 1));
+  d.ops = reinterpret_cast<const uint8_t*>(ld_relaxed(w + 2));
+  d.out_vals = reinterpret_cast<uint64_t*>(ld_relaxed(w + 3));
+  d.out_st = reinterpret_cast<uint8_t*>(ld_relaxed(w + 4));
+  const uint64_t ns = ld_relaxed(w + 5);
+  d.n = (uint32_t)ns;
+  d.seq = (uint32_t)(ns >> 32);
+  return d;
+}
+
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long v;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(v));
   return v;
 }
 
-__global__ void __launch_bounds__(256, 4) serve_kernel(DevTree t, ServeDev S, uint32_t retry_limit) {
+__global__ void __launch_bounds__(256, 4) serve_kernel(DevTree t, ServeDev S, uint32_t retry_limit, LearnedDev lm,
+                                                       int use_learned) {
   const uint32_t lane = lane_id();
+  const LearnedDev* M = use_learned ? &lm : nullptr;
   TxCounters cnt;
   const uint32_t epoch = t.ctrl->epoch;
   unsigned long long idle_since = 0;
@@ -611,46 +640,61 @@ __global__ void __launch_bounds__(256, 4) serve_kernel(DevTree t, ServeDev S, ui
     }
     idle_since = 0;
     const uint32_t slot = cur % S.cap;
-    const ServeDesc d = S.desc[slot];
-    // claim a chunk of batch `cur` only: the slot's claim word carries the
-    // batch sequence in its high half, and a claim is a CAS against that
-    // sequence, so a warp holding a stale view never claims from the batch
-    // that later reuses the slot
-    uint32_t c = 0xFFFFFFFFu;
-    int action = 0;  // 0 retry, 1 claimed, 2 batch fully claimed
+    // Claim kServeChunk requests with one atomicAdd on the slot's word
+    // (batch seq << 32 | requests claimed); every claim succeeds, so thousands
+    // of warps do not serialise on a compare-and-swap.  The returned tag names
+    // the batch the claim landed in: normally `cur`; if the host has already
+    // retired `cur` and reused the slot for a newer batch, the claim belongs to
+    // that batch, and this warp runs exactly that range once its descriptor
+    // has landed, so no claimed range is ever dropped or run twice.
+    unsigned long long w = 0;
     if (lane == 0) {
-      if (d.seq == cur) {
-        unsigned long long w = ld_relaxed(reinterpret_cast<const uint64_t*>(S.claimed + slot));
-        for (int tries = 0; tries < 64; tries++) {
-          if ((uint32_t)(w >> 32) != cur) break;
-          const uint32_t got = (uint32_t)w;
-          if (got >= d.n) {
-            action = 2;
-            break;
-          }
-          const unsigned long long prev = atomicCAS(S.claimed + slot, w, w + kServeChunk);
-          if (prev == w) {
-            c = got;
-            action = 1;
-            break;
-          }
-          w = prev;
-        }
-      }
+      const uint32_t dseq = (uint32_t)(ld_relaxed(reinterpret_cast<const uint64_t*>(S.desc + slot) + 5) >> 32);
+      if (dseq == cur) w = atomicAdd(S.claimed + slot, (unsigned long long)kServeChunk);
+      else w = ~0ull;  // descriptor of `cur` not visible yet, or slot already reused
     }
-    action = __shfl_sync(kFull, action, 0);
-    c = __shfl_sync(kFull, c, 0);
-    if (action == 2) {
-      if (lane == 0) atomicCAS(S.cursor, cur, cur + 1);
+    w = __shfl_sync(kFull, w, 0);
+    if (w == ~0ull) {
+      __nanosleep(200);
       continue;
     }
-    if (action == 0) continue;
+    const uint32_t tag = (uint32_t)(w >> 32);
+    const uint32_t c = (uint32_t)w;
+    ServeDesc d;
+    bool have = true;
+    if (lane == 0) {
+      d = load_desc(S.desc + slot);
+      // a claim in a newer batch: wait (bounded) for its descriptor
+      uint32_t spins = 0;
+      while (d.seq != tag && spins < (1u << 20)) {
+        __nanosleep(256);
+        spins++;
+        d = load_desc(S.desc + slot);
+      }
+      if (d.seq != tag) {
+        atomicOr(&t.ctrl->error, kErrSpin);
+        have = false;
+      }
+    }
+    have = __shfl_sync(kFull, have ? 1 : 0, 0);
+    if (!have) continue;
+    d.keys = (const uint64_t*)__shfl_sync(kFull, (unsigned long long)d.keys, 0);
+    d.vals = (const uint64_t*)__shfl_sync(kFull, (unsigned long long)d.vals, 0);
+    d.ops = (const uint8_t*)__shfl_sync(kFull, (unsigned long long)d.ops, 0);
+    d.out_vals = (uint64_t*)__shfl_sync(kFull, (unsigned long long)d.out_vals, 0);
+    d.out_st = (uint8_t*)__shfl_sync(kFull, (unsigned long long)d.out_st, 0);
+    d.n = __shfl_sync(kFull, d.n, 0);
+    d.seq = __shfl_sync(kFull, d.seq, 0);
+    if (c >= d.n) {
+      if (lane == 0 && tag == cur) atomicCAS(S.cursor, cur, cur + 1);
+      continue;
+    }
     const uint32_t end = min(d.n, c + (uint32_t)kServeChunk);
     for (uint32_t q = c; q < end; q++) {
       uint64_t ans;
       uint8_t st;
       const uint32_t op = d.ops[q];
-      run_request(t, epoch, d.keys[q], op, op == kOpInsert ? d.vals[q] : 0, retry_limit, ans, st, cnt);
+      run_request(t, epoch, d.keys[q], op, op == kOpInsert ? d.vals[q] : 0, retry_limit, ans, st, cnt, M);
       if (lane == 0) {
         d.out_vals[q] = ans;
         d.out_st[q] = st;
@@ -680,7 +724,9 @@ cudaError_t launch_serve(Handle* h, const ServeDev& S, cudaStream_t s) {
     per_sm[h->device] = b;
   }
   const unsigned blocks = (unsigned)(h->sm_count * (h->device < 64 ? per_sm[h->device] : 2));
-  serve_kernel<<<blocks, 256, 0, s>>>(h->tree, S, h->retry_limit);
+  LearnedDev lm{};
+  const int use = learned_dev(h, &lm);
+  serve_kernel<<<blocks, 256, 0, s>>>(h->tree, S, h->retry_limit, lm, use);
   count_launch();
   return cudaGetLastError();
 }
@@ -700,8 +746,10 @@ cudaError_t launch_stm(Handle* h, const uint64_t* keys, const uint64_t* vals, co
   size_t blocks = (n * 32 + threads - 1) / threads;
   const size_t cap = (size_t)h->sm_count * (h->device < 64 ? per_sm[h->device] : 2);
   if (blocks > cap) blocks = cap;
+  LearnedDev lm{};
+  const int use = learned_dev(h, &lm);
   stm_kernel<<<(unsigned)blocks, threads, 0, s>>>(h->tree, keys, vals, ops, op_override, list, n_dev, n, out_vals,
-                                                   out_st, h->retry_limit);
+                                                   out_st, h->retry_limit, lm, use);
   count_launch();
   return cudaGetLastError();
 }

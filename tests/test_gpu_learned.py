@@ -7,7 +7,7 @@ import pytest
 
 import eirene_b200 as E
 from oracle import oracle as O
-from tests.helpers import dev, empty_u64, empty_u8, host_u64, host_u8, run_batch
+from tests.helpers import dev, dump, empty_u64, empty_u8, host_u64, host_u8, run_batch
 
 pytestmark = pytest.mark.gpu
 
@@ -150,3 +150,37 @@ def test_autotune_then_batches_stay_exact(gpu):
             ov, os_ = o.execute_merged(rk, rv, ro)
             gv, gs = run_batch(t, rk, rv, ro, E.MODE_SORTED)
             assert (gs == os_).all() and (gv == ov).all()
+
+
+def test_learned_in_stm_mode_and_serving(gpu):
+    # the learned model proposes leaves in the STM fast path; answers and
+    # contents must equal the serial oracle
+    keys = O.gen_keys("uniform", 31, 200_000)
+    vals = O.value_of(keys)
+    t = E.BTree(max_keys=1 << 21, max_batch=1 << 17)
+    t.bulk_build(dev(keys), dev(vals))
+    o = O.OracleTree()
+    o.bulk_build(keys, vals)
+    t.retrain()
+    t.set_descent(True)
+    rk, rv, ro = O.gen_requests("uniform", 32, keys, 60_000, 70)
+    _, first = np.unique(rk, return_index=True)
+    sel = np.sort(first)
+    rk, rv, ro = rk[sel], rv[sel], ro[sel]
+    ov, os_ = o.execute_serial(rk, rv, ro)
+    gv, gs = run_batch(t, rk, rv, ro, E.MODE_STM)
+    assert (gs == os_).all() and (gv == ov).all()
+    srv = E.Server(t)
+    qk, qv, qo = O.gen_requests("uniform", 33, keys, 30_000, 90)
+    _, first = np.unique(qk, return_index=True)
+    sel = np.sort(first)
+    qk, qv, qo = qk[sel], qv[sel], qo[sel]
+    ov2, os2 = o.execute_serial(qk, qv, qo)
+    out_v = np.zeros(qk.size, np.uint64)
+    out_s = np.zeros(qk.size, np.uint8)
+    srv.wait(srv.submit(qk, qv, qo, out_v, out_s))
+    srv.stop()
+    assert (out_s == os2).all() and (out_v == ov2).all()
+    gk, gvv = dump(t)
+    ok, ovv = o.dump()
+    assert (gk == ok).all() and (gvv == ovv).all()
