@@ -7,7 +7,7 @@
 // "Onesweep: A Faster Least Significant Digit Radix Sort for GPUs" (2022):
 //   1. one up-front kernel counts all eight 8-bit digits of every key;
 //   2. per digit, one kernel: a tile of 4096 items takes a dynamic tile id,
-//      ranks its items stably with __match_any_sync (each warp owns a
+//      ranks its items stably with eight bit ballots per item (each warp owns a
 //      contiguous 256-item chunk and walks it in 8 rounds), publishes its
 //      per-digit counts, and finds its global offsets by decoupled look-back
 //      over the preceding tiles; it then stages the tile in shared memory in
@@ -201,8 +201,15 @@ __global__ void __launch_bounds__(kSortThreads) sort_onesweep_kernel(
     key[r] = valid ? keys_in[idx] : 0;
     if (payload_mode == 0) val[r] = valid ? vals_in[idx] : 0;
     else val[r] = (uint32_t)idx | (ops && valid ? (op_code(ops[idx]) << 30) : 0u);
-    const uint32_t d = valid ? digit_of(key[r], shift) : 0xFFFFu;
-    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t d = valid ? digit_of(key[r], shift) : 0x1FFu;
+    // lanes holding the same digit: AND of eight bit ballots (plus a validity bit)
+    uint32_t peers = __ballot_sync(0xffffffffu, valid);
+    peers = valid ? peers : ~peers;
+#pragma unroll
+    for (int b = 0; b < 8; b++) {
+      const uint32_t bal = __ballot_sync(0xffffffffu, (d >> b) & 1u);
+      peers &= ((d >> b) & 1u) ? bal : ~bal;
+    }
     uint32_t before = 0;
     if (valid) before = S.wh[warp][d];
     __syncwarp();
