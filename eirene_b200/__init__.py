@@ -111,7 +111,14 @@ def build(force: bool = False) -> str:
     """Compile libeirene_b200.so in place (nvcc, sm_100a)."""
     import importlib
 
-    return importlib.import_module(__name__ + ".build").build(force=force)
+    mod = importlib.import_module(__name__ + ".build")
+    # importing the submodule binds it as this package's `build` attribute:
+    # put the function back so that later calls still reach it
+    globals()["build"] = _build_fn
+    return mod.build(force=force)
+
+
+_build_fn = build
 
 
 def lib():

@@ -43,6 +43,7 @@ def _stale() -> bool:
         return True
     t = os.path.getmtime(LIB)
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(ROOT, "include", "eirene_b200.h")]
+    deps += [os.path.join(HERE, "host", f) for f in os.listdir(os.path.join(HERE, "host"))]
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
@@ -76,7 +77,21 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
     cmd = [nvcc(), "-shared", "-o", tmp] + objs + ARCH + ["-lcudart"]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
+    build_cli()
     return LIB
+
+
+CLI = os.path.join(HERE, "bt_stm_test")
+
+
+def build_cli() -> str:
+    """The reference-compatible command-line driver (g++, links the library)."""
+    host = os.path.join(HERE, "host")
+    cmd = ["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include",
+           os.path.join(host, "gpu_btree.cpp"), os.path.join(host, "bt_stm_test.cpp"), "-o", CLI,
+           "-L", HERE, "-leirene_b200", "-L", "/usr/local/cuda/lib64", "-lcudart", "-Wl,-rpath,$ORIGIN", "-Wl,-rpath,/usr/local/cuda/lib64"]
+    subprocess.run(cmd, check=True)
+    return CLI
 
 
 if __name__ == "__main__":
