@@ -10,8 +10,12 @@ generator reproduces their shape: 95% reads, half of them existing keys).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Under torchrun each rank owns an independent tree (key-range shard stand-in,
-weak scaling, no data-path collective); rank 0 prints one JSON line.
+Under torchrun the ranks hold one key-range-sharded tree (eirene_b200.shard):
+each rank builds from its own 2^26 keys, the splitters are quantiles of all
+ranks' keys, and every step each rank submits its own 2^22-request batch,
+which is routed to the owning GPUs by an all-to-all over NCCL, run there, and
+answered by the reverse all-to-all (weak scaling: keys and requests per GPU are
+fixed).  Rank 0 prints one JSON line.
 """
 from __future__ import annotations
 
@@ -313,12 +317,24 @@ def main():
     n_steps_total = args.warmup + args.steps
     stream = torch.cuda.current_stream()
     # ---- tree
-    tree = E.BTree(max_keys=2 * n_tree + 32 * n_b, max_batch=n_b, device=local, search_group=args.search_group)
+    sharded = None
+    if world > 1:
+        from eirene_b200.shard import ShardedBTree
+
+        # an owner receives about n_b requests per step; headroom keeps that one local batch
+        sharded = ShardedBTree.on_gpu(max_keys=2 * n_tree + 32 * n_b, max_batch=n_b + n_b // 8, device=local,
+                                      search_group=args.search_group)
+        tree = sharded.ops.tree
+    else:
+        tree = E.BTree(max_keys=2 * n_tree + 32 * n_b, max_batch=n_b, device=local, search_group=args.search_group)
     tk = torch.empty(n_tree, dtype=torch.int64, device="cuda")
     tv = torch.empty(n_tree, dtype=torch.int64, device="cuda")
     E.gen_keys(args.dist, 1 + rank, n_tree, tk, tv, stream)
     t0 = time.time()
-    tree.bulk_build(tk, tv, stream)
+    if sharded is not None:
+        sharded.bulk_build(tk, tv)
+    else:
+        tree.bulk_build(tk, tv, stream)
     torch.cuda.synchronize()
     build_s = time.time() - t0
     del tv
@@ -339,6 +355,12 @@ def main():
     ost = torch.empty(n_b, dtype=torch.uint8, device="cuda")
     MODE = E.MODE_SORTED | (E.MODE_MERGE_ENGINE if args.engine == "merge" else 0)
 
+    def step(k, v, o):
+        if sharded is not None:
+            sharded.execute(k, v, o, ov, ost, mode=MODE)
+        else:
+            tree.execute(k, v, o, ov, ost, mode=MODE, stream=stream)
+
     def run_form(learned: bool, seed0: int):
         batches = make_batches(seed0)
         counts = [unique_op_counts(torch, k, o) for (k, v, o) in batches[args.warmup:]]
@@ -356,7 +378,7 @@ def main():
         tune = tree.autotune(batches[0][0], stream)
         tree.set_option(E.OPT_BATCH_DESCENT, 1 if learned else 0)
         for i in range(args.warmup):
-            tree.execute(*batches[i], ov, ost, mode=MODE, stream=stream)
+            step(*batches[i])
         tree.reset_stats()
         tree.profile(True)
         tree.profile_read(reset=True)
@@ -367,7 +389,7 @@ def main():
         l0 = E.launch_count()
         ev[0].record(stream)
         for s in range(args.steps):
-            tree.execute(*batches[args.warmup + s], ov, ost, mode=MODE, stream=stream)
+            step(*batches[args.warmup + s])
             ev[s + 1].record(stream)
         torch.cuda.synchronize()
         launches = E.launch_count() - l0
@@ -398,6 +420,8 @@ def main():
     # unsorted point lookups (bt_search_batch on random keys): plain vs learned
     random_lookup = {}
     try:
+        if sharded is not None:
+            raise E.BTError(-1, "per-GPU lookups are measured at n_gpus=1")
         rk = torch.empty(n_b, dtype=torch.int64, device="cuda")
         rv = torch.empty(n_b, dtype=torch.int64, device="cuda")
         ro = torch.empty(n_b, dtype=torch.uint8, device="cuda")
@@ -461,8 +485,21 @@ def main():
         L = E.lib()
         sp = stream.cuda_stream
 
+        dk = torch.empty(n_b, dtype=torch.int64, device="cuda")
+        dv = torch.empty(n_b, dtype=torch.int64, device="cuda")
+        do = torch.empty(n_b, dtype=torch.uint8, device="cuda")
+
         def host_step(b):
             k, v, o = b
+            if sharded is not None:
+                # host batch in, host answers out, through the sharded tree
+                dk.copy_(k, non_blocking=True)
+                dv.copy_(v, non_blocking=True)
+                do.copy_(o, non_blocking=True)
+                sharded.execute(dk, dv, do, ov, ost, mode=MODE)
+                hov.copy_(ov, non_blocking=True)
+                hos.copy_(ost, non_blocking=True)
+                return
             rc = L.bt_execute_batch_host(tree._h, k.data_ptr(), v.data_ptr(), o.data_ptr(), hov.data_ptr(),
                                          hos.data_ptr(), n_b, MODE, sp)
             if rc != 0:
@@ -484,7 +521,7 @@ def main():
                "steps": e2e_steps, "descent": head}
 
     serving = {}
-    if not args.no_serve:
+    if not args.no_serve and sharded is None:
         for form in ("plain", "learned"):
             if form == "learned" and "learned" not in forms:
                 continue
@@ -529,7 +566,8 @@ def main():
                             f"sort-merged (v38 meaning), {args.engine} insert engine",
                 "descent": head, "tree_keys": n_tree, "batch": n_b, "search_group": args.search_group,
                 "l2": "inputs larger than L2: tree ~1.5 GB; every step reads its own 71 MB batch",
-                "parallelism": f"{world} independent tree(s), one per GPU",
+                "parallelism": (f"{world} key-range shards, one tree per GPU, all-to-all request exchange over NCCL"
+                                if sharded is not None else "one tree on one GPU"),
                 "tree_build_s": build_s,
             },
             "roofline": roof,

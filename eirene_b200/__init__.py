@@ -98,7 +98,9 @@ EXPORTS = [
     "bt_profile", "bt_profile_read", "bt_launch_count", "bt_bulk_build_static",
     "bt_set_learned_group", "bt_learned_info", "bt_mlp_grad", "bt_set_option", "bt_autotune",
     "bt_serve_config_init", "bt_serve_start", "bt_submit", "bt_poll", "bt_wait", "bt_serve_get_stats", "bt_serve_stop",
+    "bt_route_batch", "bt_unroute_results",
 ]
+MAX_SHARDS = 256
 OPT_SORTED_SEARCH, OPT_RETRY_LIMIT, OPT_TRAIN_STEPS, OPT_SORTED_LEAF_VALS, OPT_BATCH_DESCENT = 1, 2, 3, 4, 5
 PHASES = ["sort", "merge", "search", "insert", "writeback"]
 
@@ -168,6 +170,8 @@ def lib():
             "bt_wait": [_P, ctypes.c_uint64, ctypes.c_uint32],
             "bt_serve_get_stats": [_P, ctypes.POINTER(ServeStats), ctypes.c_int],
             "bt_serve_stop": [_P],
+            "bt_route_batch": [_P, _P, ctypes.c_int, _P, _P, _P, _SZ, _P, _P, _P, _P, _P, _P],
+            "bt_unroute_results": [_P, _P, _P, _P, _SZ, _P, _P, _P],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -352,6 +356,18 @@ class BTree:
     def mlp_grad(self, params, x, y, grad_out, loss_out, stream=None):
         _check(lib().bt_mlp_grad(self._h, _ptr(params), _ptr(x), _ptr(y), x.numel(), _ptr(grad_out),
                                  _ptr(loss_out), _stream_ptr(stream)), "bt_mlp_grad")
+
+    def route(self, splitters, n_shards: int, keys, vals, ops, out_keys, out_vals, out_ops, out_perm, out_counts,
+              stream=None):
+        """Stable partition of a batch by owning shard (bt_route_batch)."""
+        _check(lib().bt_route_batch(self._h, _ptr(splitters), n_shards, _ptr(keys), _ptr(vals), _ptr(ops), keys.numel(),
+                                    _ptr(out_keys), _ptr(out_vals), _ptr(out_ops), _ptr(out_perm), _ptr(out_counts),
+                                    _stream_ptr(stream)), "bt_route_batch")
+
+    def unroute(self, perm, in_vals, in_status, out_vals, out_status, stream=None):
+        """Scatter answers in routed order back to input order (bt_unroute_results)."""
+        _check(lib().bt_unroute_results(self._h, _ptr(perm), _ptr(in_vals), _ptr(in_status), perm.numel(),
+                                        _ptr(out_vals), _ptr(out_status), _stream_ptr(stream)), "bt_unroute_results")
 
     def set_search_group(self, lanes: int):
         _check(lib().bt_set_search_group(self._h, lanes), "bt_set_search_group")

@@ -27,6 +27,7 @@ SOURCES = [
     "bt_tune.cu",
     "bt_merge.cu",
     "bt_serve.cu",
+    "bt_shard.cu",
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -460,6 +460,27 @@ int bt_host_alloc(void** p, size_t bytes) {
 
 int bt_host_free(void* p) { return cudaFreeHost(p) == cudaSuccess ? BT_OK : BT_ERR_CUDA; }
 
+int bt_route_batch(bt_handle* H, const uint64_t* splitters, int n_shards, const uint64_t* keys, const uint64_t* vals,
+                   const uint8_t* ops, size_t n, uint64_t* out_keys, uint64_t* out_vals, uint8_t* out_ops,
+                   uint32_t* out_perm, uint64_t* out_counts, void* stream) {
+  if (!H || n_shards < 1 || n_shards > BT_MAX_SHARDS || !out_counts) return BT_ERR_INVALID_ARG;
+  if (n_shards > 1 && !splitters) return BT_ERR_INVALID_ARG;
+  if (n && (!keys || !out_keys || !out_perm || (vals && !out_vals) || (ops && !out_ops))) return BT_ERR_INVALID_ARG;
+  if (n > H->h.w.cap) return BT_ERR_BATCH_TOO_LARGE;
+  DeviceGuard g(H->h.device);
+  return bt::route_batch(&H->h, splitters, n_shards, keys, vals, ops, n, out_keys, out_vals, out_ops, out_perm,
+                         out_counts, S(stream));
+}
+
+int bt_unroute_results(bt_handle* H, const uint32_t* perm, const uint64_t* in_vals, const uint8_t* in_status,
+                       size_t n, uint64_t* out_vals, uint8_t* out_status, void* stream) {
+  if (!H) return BT_ERR_INVALID_ARG;
+  if (n == 0) return BT_OK;
+  if (!perm || !in_vals || !in_status || !out_vals || !out_status) return BT_ERR_INVALID_ARG;
+  DeviceGuard g(H->h.device);
+  return bt::unroute_results(&H->h, perm, in_vals, in_status, n, out_vals, out_status, S(stream));
+}
+
 const char* bt_status_string(int code) {
   switch (code) {
     case BT_OK: return "ok";

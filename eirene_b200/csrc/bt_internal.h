@@ -195,6 +195,13 @@ cudaError_t launch_stm(Handle* h, const uint64_t* keys, const uint64_t* vals, co
                        const uint32_t* list, const uint32_t* n_dev, size_t n, uint64_t* out_vals, uint8_t* out_st,
                        cudaStream_t s);
 
+// ---- key-range sharding (bt_shard.cu) ----
+int route_batch(Handle* h, const uint64_t* splitters, int n_shards, const uint64_t* keys, const uint64_t* vals,
+                const uint8_t* ops, size_t n, uint64_t* out_keys, uint64_t* out_vals, uint8_t* out_ops,
+                uint32_t* out_perm, uint64_t* out_counts, cudaStream_t s);
+int unroute_results(Handle* h, const uint32_t* perm, const uint64_t* in_vals, const uint8_t* in_st, size_t n,
+                    uint64_t* out_vals, uint8_t* out_st, cudaStream_t s);
+
 // ---- sorted-merge batch (bt_batch.cu) ----
 int work_alloc(Work* w, size_t cap);
 void work_free(Work* w);

@@ -272,6 +272,28 @@ int bt_gen_keys(int dist, uint64_t seed, size_t n, uint64_t *keys, uint64_t *val
 int bt_gen_requests(int dist, uint64_t seed, const uint64_t *tree_keys, size_t n_tree, size_t n,
                     uint32_t search_pct, uint64_t *keys, uint64_t *vals, uint8_t *ops, void *stream);
 
+/* ---- key-range sharding (one tree per GPU) ----
+ * No counterpart in the reference, which runs one tree on one GPU
+ * (src/gpu-stm-tree-v39/bpt-gpustm.cpp:14-28).  Shard s owns the keys in
+ * [splitters[s-1], splitters[s]); splitters holds n_shards - 1 non-decreasing
+ * keys (device memory; equal neighbours leave a shard empty),
+ * 1 <= n_shards <= BT_MAX_SHARDS.
+ *
+ * bt_route_batch reorders a batch by owning shard, stably (each shard's run
+ * keeps the input order): out_keys/out_vals/out_ops[i] = input[out_perm[i]],
+ * out_counts[s] (device, uint64) = length of shard s's run.  vals and ops may
+ * be NULL (their outputs are then not written).  n <= max_batch.  Uses the
+ * handle's batch work buffers: stream-ordered with the handle's other calls.
+ *
+ * bt_unroute_results scatters answers that came back in routed order to
+ * input order: out_vals[perm[i]] = in_vals[i], out_status[perm[i]] = in_status[i]. */
+#define BT_MAX_SHARDS 256
+int bt_route_batch(bt_handle *h, const uint64_t *splitters, int n_shards, const uint64_t *keys,
+                   const uint64_t *vals, const uint8_t *ops, size_t n, uint64_t *out_keys, uint64_t *out_vals,
+                   uint8_t *out_ops, uint32_t *out_perm, uint64_t *out_counts, void *stream);
+int bt_unroute_results(bt_handle *h, const uint32_t *perm, const uint64_t *in_vals, const uint8_t *in_status,
+                       size_t n, uint64_t *out_vals, uint8_t *out_status, void *stream);
+
 /* Static text for a status code. */
 const char *bt_status_string(int code);
 
