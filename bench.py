@@ -55,53 +55,111 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle-reason samples while the timed region runs."""
+    """SM clock and throttle-reason samples taken while the timed region runs.
 
+    Reads NVML (nvidia-ml-py) every 2 ms from a host thread (the timed region
+    is tens of milliseconds, too short for nvidia-smi's sampling interval);
+    falls back to `nvidia-smi -lms 200` where NVML is not importable.  Only
+    reads: it changes no setting of the GPU."""
+
+    NVML_REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+                    ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+                    ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+                    ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
+                    ("hw_power_brake_slowdown", "nvmlClocksEventReasonHwPowerBrakeSlowdown"))
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index: int):
-        self.gpu = gpu_index
+    def __init__(self, cuda_index: int):
+        self.cuda_index = cuda_index
         self.proc = None
-        self.path = os.path.join("/tmp", f"bt_clocks_{os.getpid()}.csv")
+        self.thread = None
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = 0.0
+        self.source = None
 
     def start(self):
+        import threading
+
         try:
+            import pynvml
+            import torch
+
+            pynvml.nvmlInit()
+            try:
+                idx = torch.cuda._get_nvml_device_index(self.cuda_index)
+            except Exception:
+                idx = self.cuda_index
+            h = pynvml.nvmlDeviceGetHandleByIndex(idx)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            bits = [(nm, getattr(pynvml, c)) for nm, c in self.NVML_REASONS if hasattr(pynvml, c)]
+            self.stop_flag = threading.Event()
+
+            def run():
+                while not self.stop_flag.is_set():
+                    try:
+                        self.samples.append(float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)))
+                        r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        for nm, b in bits:
+                            if r & b:
+                                self.reasons.add(nm)
+                    except Exception:
+                        pass
+                    self.stop_flag.wait(0.002)
+
+            self.thread = threading.Thread(target=run, daemon=True)
+            self.thread.start()
+            self.source = "nvml, 2 ms"
+            return
+        except Exception:
+            self.thread = None
+        try:
+            self.path = os.path.join("/tmp", f"bt_clocks_{os.getpid()}.csv")
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+                ["nvidia-smi", f"--id={self.cuda_index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+            self.source = "nvidia-smi, 200 ms"
         except Exception:
             self.proc = None
 
     def stop(self):
-        if self.proc is None:
-            return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        self.fh.close()
-        sm, mx, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
-                continue
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join(2)
             try:
-                sm.append(float(f[1]))
-                mx = max(mx, float(f[2]))
-            except ValueError:
-                continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
-        if not sm:
+                import pynvml
+
+                pynvml.nvmlShutdown()
+            except Exception:
+                pass
+        elif self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    self.samples.append(float(f[1]))
+                    self.max_mhz = max(self.max_mhz, float(f[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, f[5:9]):
+                    if v.lower().startswith("active"):
+                        self.reasons.add(nm)
+        if not self.samples:
             return None
-        sm.sort()
-        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        sm = sorted(self.samples)
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                "samples": len(sm), "source": self.source}
 
 
 # ----------------------------------------------------------------------------
@@ -257,7 +315,7 @@ def unique_op_counts(torch, k, o):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--tree-log2", type=int, default=26)
@@ -272,6 +330,10 @@ def main():
     ap.add_argument("--cpu-sample-log2", type=int, default=20)
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=1.5)
+    ap.add_argument("--front-end", default="hash", choices=["hash", "sort"],
+                    help="sorted batches: hash front end (sort only INSERT-coupled requests) or full sort")
+    ap.add_argument("--pool-keys-log2", type=int, default=0,
+                    help="size the node pool for 2^x keys (default: 2 x tree + 32 x batch)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -317,16 +379,18 @@ def main():
     n_steps_total = args.warmup + args.steps
     stream = torch.cuda.current_stream()
     # ---- tree
+    pool_keys = (1 << args.pool_keys_log2) if args.pool_keys_log2 else 2 * n_tree + 32 * n_b
     sharded = None
     if world > 1:
         from eirene_b200.shard import ShardedBTree
 
         # an owner receives about n_b requests per step; headroom keeps that one local batch
-        sharded = ShardedBTree.on_gpu(max_keys=2 * n_tree + 32 * n_b, max_batch=n_b + n_b // 8, device=local,
+        sharded = ShardedBTree.on_gpu(max_keys=pool_keys, max_batch=n_b + n_b // 8, device=local,
                                       search_group=args.search_group)
         tree = sharded.ops.tree
     else:
-        tree = E.BTree(max_keys=2 * n_tree + 32 * n_b, max_batch=n_b, device=local, search_group=args.search_group)
+        tree = E.BTree(max_keys=pool_keys, max_batch=n_b, device=local, search_group=args.search_group)
+    tree.set_option(E.OPT_FRONT_END, 1 if args.front_end == "hash" else 0)
     tk = torch.empty(n_tree, dtype=torch.int64, device="cuda")
     tv = torch.empty(n_tree, dtype=torch.int64, device="cuda")
     E.gen_keys(args.dist, 1 + rank, n_tree, tk, tv, stream)
@@ -563,7 +627,7 @@ def main():
             "config": {
                 "workload": f"2^{args.tree_log2} {args.dist} uint64 keys per GPU, batches of 2^{args.batch_log2} "
                             f"requests, {args.search_pct}% search / {100 - args.search_pct}% insert, "
-                            f"sort-merged (v38 meaning), {args.engine} insert engine",
+                            f"sort-merged (v38 meaning), {args.front_end} front end, {args.engine} insert engine",
                 "descent": head, "tree_keys": n_tree, "batch": n_b, "search_group": args.search_group,
                 "l2": "inputs larger than L2: tree ~1.5 GB; every step reads its own 71 MB batch",
                 "parallelism": (f"{world} key-range shards, one tree per GPU, all-to-all request exchange over NCCL"

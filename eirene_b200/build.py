@@ -28,6 +28,7 @@ SOURCES = [
     "bt_merge.cu",
     "bt_serve.cu",
     "bt_shard.cu",
+    "bt_front.cu",
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

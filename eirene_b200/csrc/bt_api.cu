@@ -401,6 +401,7 @@ int bt_set_option(bt_handle* H, int option, int64_t value) {
   switch (option) {
     case BT_OPT_SORTED_SEARCH: H->h.sorted_search = value ? 1 : 0; return BT_OK;
     case BT_OPT_SORTED_LEAF_VALS: H->h.sorted_leaf_vals = value ? 1 : 0; return BT_OK;
+    case BT_OPT_FRONT_END: H->h.front_end = value ? 1 : 0; return BT_OK;
     case BT_OPT_BATCH_DESCENT:
       if (value < -1 || value > 1) return BT_ERR_INVALID_ARG;
       H->h.batch_descent = (int)value;
@@ -466,7 +467,7 @@ int bt_route_batch(bt_handle* H, const uint64_t* splitters, int n_shards, const 
   if (!H || n_shards < 1 || n_shards > BT_MAX_SHARDS || !out_counts) return BT_ERR_INVALID_ARG;
   if (n_shards > 1 && !splitters) return BT_ERR_INVALID_ARG;
   if (n && (!keys || !out_keys || !out_perm || (vals && !out_vals) || (ops && !out_ops))) return BT_ERR_INVALID_ARG;
-  if (n > H->h.w.cap) return BT_ERR_BATCH_TOO_LARGE;
+  if (n > 0xFFFFFFFFull) return BT_ERR_BATCH_TOO_LARGE;  // 32-bit permutation
   DeviceGuard g(H->h.device);
   return bt::route_batch(&H->h, splitters, n_shards, keys, vals, ops, n, out_keys, out_vals, out_ops, out_perm,
                          out_counts, S(stream));

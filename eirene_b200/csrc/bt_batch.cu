@@ -108,7 +108,10 @@ __device__ __forceinline__ Seg item_seg(const Item& x, const uint64_t* __restric
 __global__ void __launch_bounds__(kThreads) merge_pass1(const uint64_t* __restrict__ sk,
                                                         const uint32_t* __restrict__ sv,
                                                         const uint64_t* __restrict__ vals, size_t n,
+                                                        const uint32_t* __restrict__ n_dev,
                                                         TileSummary* __restrict__ tiles) {
+  if (n_dev) n = min(n, (size_t)*n_dev);
+  if ((size_t)blockIdx.x * kTile >= n) return;  // grid sized for the host bound
   __shared__ uint32_t wsf[32];
   __shared__ uint64_t wsv[32];
   __shared__ uint32_t ws[32];
@@ -169,7 +172,9 @@ __global__ void __launch_bounds__(kThreads) merge_pass1(const uint64_t* __restri
 
 // pass 2 (one block): carries and prefix counts across tiles; writes totals
 __global__ void __launch_bounds__(1024) merge_pass2(TileSummary* __restrict__ tiles, uint32_t n_tiles,
+                                                    const uint32_t* __restrict__ n_dev,
                                                     BatchCounts* __restrict__ counts) {
+  if (n_dev) n_tiles = min(n_tiles, (uint32_t)(((size_t)*n_dev + kTile - 1) / kTile));
   __shared__ uint32_t wsf[32];
   __shared__ uint64_t wsv[32];
   __shared__ uint32_t ws[32];
@@ -225,9 +230,11 @@ __global__ void __launch_bounds__(1024) merge_pass2(TileSummary* __restrict__ ti
 // pass 3: per request resolution, unique ops and the two work lists
 __global__ void __launch_bounds__(kThreads) merge_pass3(
     const uint64_t* __restrict__ sk, const uint32_t* __restrict__ sv, const uint64_t* __restrict__ vals, size_t n,
-    const TileSummary* __restrict__ tiles, uint64_t* __restrict__ ukeys, uint64_t* __restrict__ uvals,
-    uint32_t* __restrict__ ins_list, uint32_t* __restrict__ get_list, uint32_t* __restrict__ pend,
-    uint64_t* __restrict__ out_vals, uint8_t* __restrict__ out_st) {
+    const uint32_t* __restrict__ n_dev, const TileSummary* __restrict__ tiles, uint64_t* __restrict__ ukeys,
+    uint64_t* __restrict__ uvals, uint32_t* __restrict__ ins_list, uint32_t* __restrict__ get_list,
+    uint32_t* __restrict__ pend, uint64_t* __restrict__ out_vals, uint8_t* __restrict__ out_st) {
+  if (n_dev) n = min(n, (size_t)*n_dev);
+  if ((size_t)blockIdx.x * kTile >= n) return;
   __shared__ uint32_t wsf[32];
   __shared__ uint64_t wsv[32];
   __shared__ uint32_t ws[32];
@@ -291,8 +298,10 @@ __global__ void __launch_bounds__(kThreads) merge_pass3(
 }
 
 __global__ void writeback_kernel(const uint32_t* __restrict__ sv, const uint32_t* __restrict__ pend, size_t n,
-                                 const uint64_t* __restrict__ uans, const uint8_t* __restrict__ uans_st,
-                                 uint64_t* __restrict__ out_vals, uint8_t* __restrict__ out_st) {
+                                 const uint32_t* __restrict__ n_dev, const uint64_t* __restrict__ uans,
+                                 const uint8_t* __restrict__ uans_st, uint64_t* __restrict__ out_vals,
+                                 uint8_t* __restrict__ out_st) {
+  if (n_dev) n = min(n, (size_t)*n_dev);
   const size_t stride = (size_t)gridDim.x * blockDim.x;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
     const uint32_t u = pend[i];
@@ -340,11 +349,23 @@ int work_alloc(Work* w, size_t cap) {
   A((void**)&w->m_ent_a, cap * 16);
   A((void**)&w->m_ent_b, cap * 16);
   A((void**)&w->m_counts, 64);
+  A(&w->m_sync, 8192);
   A((void**)&w->d_in_keys, cap * 8);
   A((void**)&w->d_in_vals, cap * 8);
   A((void**)&w->d_in_ops, cap);
   A((void**)&w->d_out_vals, cap * 8);
   A((void**)&w->d_out_st, cap);
+  {
+    size_t tc = 1024;
+    while (tc < 2 * cap) tc <<= 1;
+    A(&w->f_tab, tc * 16);
+    w->f_tab_cap = tc;
+  }
+  A((void**)&w->f_flags, cap * 4);
+  A((void**)&w->f_pos, cap * 4);
+  A((void**)&w->f_list, cap * 4);
+  A((void**)&w->f_tk, cap * 8);
+  A((void**)&w->f_tv, cap * 4);
   if (!ok) {
     work_free(w);
     return -3;
@@ -357,11 +378,69 @@ void work_free(Work* w) {
   void* ps[] = {w->k_a,      w->k_b,       w->v_a,       w->v_b,       w->sort_scratch, w->ukeys,   w->uvals,
                 w->uans,     w->uans_st,   w->ins_list,  w->get_list,  w->pend,         w->tiles,   w->counts,
                 w->m_path,   w->m_leaf,    w->m_isnew,   w->m_pos,     w->m_newk,       w->m_newv,  w->m_nq,
-                w->m_nleaf,  w->m_seg,     w->m_ent_a,   w->m_ent_b,   w->m_counts,     w->d_in_keys,
-                w->d_in_vals, w->d_in_ops, w->d_out_vals, w->d_out_st};
+                w->m_nleaf,  w->m_seg,     w->m_ent_a,   w->m_ent_b,   w->m_counts,     w->m_sync,      w->d_in_keys,
+                w->d_in_vals, w->d_in_ops, w->d_out_vals, w->d_out_st, w->f_tab, w->f_flags,
+                w->f_pos,    w->f_list,    w->f_tk,      w->f_tv};
   for (void* p : ps)
     if (p) cudaFree(p);
   *w = Work{};
+}
+
+// insert phase shared by both front ends: the unique INSERT runs of
+// (w.ukeys, w.uvals, w.ins_list, count w.counts->n_ins) reach the tree
+static int insert_phase(Handle* h, size_t n, int engine, cudaStream_t s) {
+  Work& w = h->w;
+  // the merge engine needs leaf_fill >= 16 and inner_fill >= 16: then a split
+  // emits at most one separator per new key or entry, which bounds its buffers
+  if (engine == 1 && h->leaf_fill >= 16 && h->inner_fill >= 16) return merge_engine(h, n, s) != 0 ? -2 : 0;
+  const cudaError_t e =
+      launch_stm(h, w.ukeys, w.uvals, nullptr, kOpInsert, w.ins_list, &w.counts->n_ins, n, w.uans, w.uans_st, s);
+  return e == cudaSuccess ? 0 : -2;
+}
+
+// The hash front end (bt_front.cu): only the requests coupled by an INSERT
+// of their key are sorted and merged; the rest are plain lookups of the
+// pre-batch tree, answered in place.  Same meaning as the full-sort path.
+static int batch_hashed(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops,
+                        uint64_t* out_vals, uint8_t* out_st, size_t n, int engine, cudaStream_t s) {
+  Work& w = h->w;
+  BatchCounts* c = w.counts;
+  const uint32_t* n_touch = &c->n_touch;
+  prof_mark(h, 0, s);
+  if (front_classify(h, keys, ops, n, s) != 0) return -2;
+  uint64_t* sk = nullptr;
+  uint32_t* sv = nullptr;
+  if (radix_sort_pairs(w.f_tk, w.f_tv, nullptr, w.k_a, w.v_a, w.k_b, w.v_b, n, 0, 64, w.sort_scratch, s, &sk, &sv,
+                       &h->tree.ctrl->error, n_touch) != cudaSuccess)
+    return -2;
+  const uint32_t n_tiles = (uint32_t)sort_tiles(n);
+  prof_mark(h, 1, s);
+  merge_pass1<<<n_tiles, kThreads, 0, s>>>(sk, sv, vals, n, n_touch, w.tiles);
+  count_launch();
+  merge_pass2<<<1, 1024, 0, s>>>(w.tiles, n_tiles, n_touch, c);
+  count_launch();
+  merge_pass3<<<n_tiles, kThreads, 0, s>>>(sk, sv, vals, n, n_touch, w.tiles, w.ukeys, w.uvals, w.ins_list,
+                                           w.get_list, w.pend, out_vals, out_st);
+  count_launch();
+  if (cudaGetLastError() != cudaSuccess) return -2;
+  // every touched run begins with an INSERT (n_get is zero); the plain
+  // lookups read the pre-batch tree before the insert phase
+  prof_mark(h, 2, s);
+  cudaError_t e;
+  const int desc = h->batch_descent >= 0 ? h->batch_descent : h->descent;
+  if (desc == 1 && h->L.valid)
+    e = launch_learned_search(h, keys, w.f_list, &c->n_lookup, n, out_vals, out_st, s, false);
+  else
+    e = launch_search(h, keys, w.f_list, &c->n_lookup, n, out_vals, out_st, s);
+  if (e != cudaSuccess) return -2;
+  prof_mark(h, 3, s);
+  if (insert_phase(h, n, engine, s) != 0) return -2;
+  prof_mark(h, 4, s);
+  const unsigned wb_blocks = (unsigned)min((size_t)h->sm_count * 8, (n + 255) / 256);
+  writeback_kernel<<<wb_blocks, 256, 0, s>>>(sv, w.pend, n, n_touch, w.uans, w.uans_st, out_vals, out_st);
+  count_launch();
+  prof_mark(h, 5, s);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
 int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, uint64_t* out_vals,
@@ -369,6 +448,7 @@ int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const ui
   if (n == 0) return 0;
   Work& w = h->w;
   if (n > w.cap || n > kIdxMask) return -6;
+  if (h->front_end == 1) return batch_hashed(h, keys, vals, ops, out_vals, out_st, n, engine, s);
   uint64_t* sk = nullptr;
   uint32_t* sv = nullptr;
   prof_mark(h, 0, s);
@@ -377,12 +457,12 @@ int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const ui
     return -2;
   const uint32_t n_tiles = (uint32_t)sort_tiles(n);
   prof_mark(h, 1, s);
-  merge_pass1<<<n_tiles, kThreads, 0, s>>>(sk, sv, vals, n, w.tiles);
+  merge_pass1<<<n_tiles, kThreads, 0, s>>>(sk, sv, vals, n, nullptr, w.tiles);
   count_launch();
-  merge_pass2<<<1, 1024, 0, s>>>(w.tiles, n_tiles, w.counts);
+  merge_pass2<<<1, 1024, 0, s>>>(w.tiles, n_tiles, nullptr, w.counts);
   count_launch();
-  merge_pass3<<<n_tiles, kThreads, 0, s>>>(sk, sv, vals, n, w.tiles, w.ukeys, w.uvals, w.ins_list, w.get_list,
-                                           w.pend, out_vals, out_st);
+  merge_pass3<<<n_tiles, kThreads, 0, s>>>(sk, sv, vals, n, nullptr, w.tiles, w.ukeys, w.uvals, w.ins_list,
+                                           w.get_list, w.pend, out_vals, out_st);
   count_launch();
   if (cudaGetLastError() != cudaSuccess) return -2;
   // search phase on the pre-batch tree, then the insert phase
@@ -398,17 +478,10 @@ int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const ui
     e = launch_search(h, w.ukeys, w.get_list, &w.counts->n_get, n, w.uans, w.uans_st, s);
   if (e != cudaSuccess) return -2;
   prof_mark(h, 3, s);
-  // the merge engine needs leaf_fill >= 16 and inner_fill >= 16: then a split
-  // emits at most one separator per new key or entry, which bounds its buffers
-  if (engine == 1 && h->leaf_fill >= 16 && h->inner_fill >= 16) {
-    if (merge_engine(h, n, s) != 0) return -2;
-  } else {
-    e = launch_stm(h, w.ukeys, w.uvals, nullptr, kOpInsert, w.ins_list, &w.counts->n_ins, n, w.uans, w.uans_st, s);
-    if (e != cudaSuccess) return -2;
-  }
+  if (insert_phase(h, n, engine, s) != 0) return -2;
   prof_mark(h, 4, s);
   const unsigned wb_blocks = (unsigned)min((size_t)h->sm_count * 8, (n + 255) / 256);
-  writeback_kernel<<<wb_blocks, 256, 0, s>>>(sv, w.pend, n, w.uans, w.uans_st, out_vals, out_st);
+  writeback_kernel<<<wb_blocks, 256, 0, s>>>(sv, w.pend, n, nullptr, w.uans, w.uans_st, out_vals, out_st);
   count_launch();
   prof_mark(h, 5, s);
   if (cudaGetLastError() != cudaSuccess) return -2;

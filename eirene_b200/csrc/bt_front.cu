@@ -1,0 +1,279 @@
+// Hash front end of the sorted-merge batch (the v38 meaning,
+// src/gpu-stm-tree-v38/bpt-gpustm-kernel-aux.cuh:16-56).
+//
+// The meaning only couples requests whose key is INSERTed somewhere in the
+// batch: a request for a key with no INSERT in the batch, or one that comes
+// before the first INSERT of its key, sees the pre-batch tree.  So instead
+// of sorting the whole batch, the front end
+//
+//   1. counts the INSERT requests and sizes an open-addressing table for
+//      their keys (a power of two >= 2x the count, at least 1024 slots),
+//   2. records, per INSERTed key, the index of its first INSERT,
+//   3. classifies every request: "touched" if its op code is invalid or its
+//      key has an INSERT at or before it; otherwise it is a plain lookup,
+//      and compacts both classes in input order, in one pass with a
+//      decoupled look-back over tiles.
+//
+// The touched requests go through the sort + segmented-scan path (their
+// runs all start with an INSERT, so the pre-batch value reaches them from the
+// insert phase, which returns each key's previous value); the plain lookups
+// run on the pre-batch tree, unsorted, writing their answers in place.  For a
+// read-mostly batch the sort shrinks to the INSERTs.
+//
+// HBM traffic per request: count (1 B op), table insert (1 B op, plus the key
+// of an INSERT), classify + compaction (8 B key + 1 B op + the probe, which is
+// L2-resident for small INSERT counts, then 4 B list entry or 12 B touched
+// entry).
+#include <cuda_runtime.h>
+
+#include "bt_block.cuh"
+#include "bt_common.cuh"
+#include "bt_internal.h"
+
+namespace bt {
+
+namespace {
+
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+constexpr int kThreads = 256;
+
+struct Slot {
+  unsigned long long key;  // kKeyMax = empty
+  uint32_t first;          // index of the first INSERT of the key
+  uint32_t pad;
+};
+
+// SplitMix64's finaliser (Steele, Lea, Flood 2014) as the slot hash
+__device__ __forceinline__ uint64_t slot_hash(uint64_t x) {
+  x ^= x >> 30;
+  x *= 0xBF58476D1CE4E5B9ull;
+  x ^= x >> 27;
+  x *= 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+__device__ __forceinline__ uint32_t table_cap(uint32_t n_ins, size_t cap_max) {
+  uint64_t c = 1024;
+  while (c < 2ull * n_ins) c <<= 1;
+  return (uint32_t)(c < cap_max ? c : cap_max);
+}
+
+// INSERT op codes (an upper bound of the keys to hold: reserved keys count too)
+__global__ void __launch_bounds__(kThreads) front_count_kernel(const uint8_t* __restrict__ ops, size_t n,
+                                                               BatchCounts* __restrict__ counts) {
+  uint32_t c = 0;
+  const size_t n4 = n / 4;
+  const uchar4* o4 = reinterpret_cast<const uchar4*>(ops);
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += (size_t)gridDim.x * blockDim.x) {
+    const uchar4 o = o4[i];
+    c += (o.x == kOpInsert) + (o.y == kOpInsert) + (o.z == kOpInsert) + (o.w == kOpInsert);
+  }
+  if (blockIdx.x == 0 && threadIdx.x < n - n4 * 4) c += ops[n4 * 4 + threadIdx.x] == kOpInsert ? 1u : 0u;
+  c = __reduce_add_sync(0xffffffffu, c);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(&counts->n_ins_req, c);
+}
+
+__global__ void __launch_bounds__(kThreads) front_clear_kernel(Slot* __restrict__ tab, size_t cap_max,
+                                                               BatchCounts* __restrict__ counts) {
+  const uint32_t cap = table_cap(counts->n_ins_req, cap_max);
+  if (blockIdx.x == 0 && threadIdx.x == 0) counts->cap = cap;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += (size_t)gridDim.x * blockDim.x) {
+    tab[i].key = kKeyMax;
+    tab[i].first = kNone;
+  }
+}
+
+// linear probing; the table holds at most half its slots, so a probe ends
+__global__ void __launch_bounds__(kThreads) front_insert_kernel(const uint64_t* __restrict__ keys,
+                                                                const uint8_t* __restrict__ ops, size_t n,
+                                                                Slot* __restrict__ tab,
+                                                                const BatchCounts* __restrict__ counts) {
+  const uint32_t mask = counts->cap - 1;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    if (ops[i] != kOpInsert) continue;
+    const uint64_t k = keys[i];
+    if (k == kKeyMax) continue;
+    uint32_t h = (uint32_t)slot_hash(k) & mask;
+    for (uint32_t probe = 0; probe <= mask; probe++) {
+      const unsigned long long prev = atomicCAS(&tab[h].key, (unsigned long long)kKeyMax, (unsigned long long)k);
+      if (prev == kKeyMax || prev == k) {
+        atomicMin(&tab[h].first, (uint32_t)i);
+        break;
+      }
+      h = (h + 1) & mask;
+    }
+  }
+}
+
+__device__ __forceinline__ uint32_t find_first(const Slot* __restrict__ tab, uint32_t mask, uint64_t k) {
+  uint32_t h = (uint32_t)slot_hash(k) & mask;
+  for (uint32_t probe = 0; probe <= mask; probe++) {
+    const uint64_t sk = tab[h].key;
+    if (sk == k) return tab[h].first;
+    if (sk == kKeyMax) return kNone;
+    h = (h + 1) & mask;
+  }
+  return kNone;
+}
+
+// Classify + compact in one pass (decoupled look-back over tiles of
+// kScanTile requests): a request is "touched" if its op code is invalid or its
+// key has an INSERT at or before it.  Touched requests go to (tk, tv) and the
+// rest to list, both in input order; the block holding the last tile writes
+// the two counts.  A look-back that waits past kSpinLimit sets kErrSpin.
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 16;
+constexpr int kScanTile = kScanThreads * kScanItems;  // 4096
+constexpr int kScanWarps = kScanThreads / 32;
+constexpr uint32_t kFlagAgg = 1u << 30;
+constexpr uint32_t kFlagPrefix = 2u << 30;
+constexpr uint32_t kValMask = (1u << 30) - 1u;
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+__global__ void __launch_bounds__(kScanThreads) front_split_kernel(
+    const uint64_t* __restrict__ keys, const uint8_t* __restrict__ ops, size_t n, const Slot* __restrict__ tab,
+    BatchCounts* __restrict__ counts, uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ status,
+    uint64_t* __restrict__ tk, uint32_t* __restrict__ tv, uint32_t* __restrict__ list, uint32_t* __restrict__ err) {
+  __shared__ uint32_t cnt[kScanItems][kScanWarps];
+  __shared__ uint32_t s_tile, s_excl;
+  const uint32_t n_tiles = (uint32_t)((n + kScanTile - 1) / kScanTile);
+  const uint32_t mask = counts->cap - 1;
+  const bool any = counts->n_ins_req != 0;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t lt = (1u << lane) - 1u;
+  for (;;) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    if (tile >= n_tiles) return;
+    const size_t base = (size_t)tile * kScanTile;
+    uint64_t k[kScanItems];
+    uint8_t op[kScanItems];
+    uint32_t bal[kScanItems];
+#pragma unroll
+    for (int j = 0; j < kScanItems; j++) {
+      const size_t i = base + (size_t)j * kScanThreads + threadIdx.x;
+      bool f = false;
+      k[j] = 0;
+      op[j] = 0;
+      if (i < n) {
+        k[j] = keys[i];
+        op[j] = ops[i];
+        f = op[j] > 1;  // invalid op codes are rejected on the sorted path
+        if (!f && any && k[j] != kKeyMax) {
+          const uint32_t first = find_first(tab, mask, k[j]);
+          f = first != kNone && (uint32_t)i >= first;
+        }
+      }
+      bal[j] = __ballot_sync(0xffffffffu, f);
+      if (lane == 0) cnt[j][warp] = __popc(bal[j]);
+    }
+    __syncthreads();
+    // exclusive prefix over (item, warp) in index order, and the tile total
+    if (warp == 0) {
+      uint32_t carry = 0;
+      for (int j = 0; j < kScanItems; j++) {
+        const uint32_t c = lane < kScanWarps ? cnt[j][lane] : 0u;
+        uint32_t incl = c;
+#pragma unroll
+        for (int o = 1; o < kScanWarps; o <<= 1) {
+          const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += y;
+        }
+        if (lane < kScanWarps) cnt[j][lane] = carry + incl - c;
+        carry += __shfl_sync(0xffffffffu, incl, kScanWarps - 1);
+      }
+      // publish, then look back for the exclusive prefix of this tile: the
+      // warp reads 32 predecessors per step and stops at the first one that
+      // holds an inclusive prefix
+      uint32_t excl = 0;
+      if (tile == 0) {
+        if (lane == 0) st_relaxed32(status, kFlagPrefix | carry);
+      } else {
+        if (lane == 0) st_relaxed32(status + tile, kFlagAgg | carry);
+        int64_t top = (int64_t)tile - 1;
+        uint32_t spins = 0;
+        for (;;) {
+          const int64_t idx = top - lane;
+          const uint32_t v = idx >= 0 ? ld_relaxed32(status + idx) : kFlagPrefix;
+          const uint32_t f = v & ~kValMask;
+          const uint32_t notready = __ballot_sync(0xffffffffu, f == 0);
+          const uint32_t prefix = __ballot_sync(0xffffffffu, f == kFlagPrefix);
+          const uint32_t stop = notready | prefix;
+          if (stop && ((notready >> (__ffs(stop) - 1)) & 1u)) {  // wait for that predecessor
+            if (++spins > kSpinLimit) {
+              if (lane == 0) atomicOr(err, kErrSpin);
+              break;
+            }
+            if (spins > 16) __nanosleep(64);
+            continue;
+          }
+          const int last = stop ? __ffs(stop) - 1 : 31;
+          excl += __reduce_add_sync(0xffffffffu, lane <= (uint32_t)last ? (v & kValMask) : 0u);
+          if (stop) break;
+          top -= 32;
+        }
+        if (lane == 0) st_relaxed32(status + tile, kFlagPrefix | (excl + carry));
+      }
+      if (lane == 0) {
+        s_excl = excl;
+        if (tile == n_tiles - 1) {
+          counts->n_touch = excl + carry;
+          counts->n_lookup = (uint32_t)n - (excl + carry);
+        }
+      }
+    }
+    __syncthreads();
+    const uint32_t excl = s_excl;
+#pragma unroll
+    for (int j = 0; j < kScanItems; j++) {
+      const size_t i = base + (size_t)j * kScanThreads + threadIdx.x;
+      if (i < n) {
+        const uint32_t p = excl + cnt[j][warp] + __popc(bal[j] & lt);  // touched before i
+        if ((bal[j] >> lane) & 1u) {
+          tk[p] = k[j];
+          tv[p] = (uint32_t)i | ((op[j] <= 1 ? (uint32_t)op[j] : 3u) << 30);
+        } else {
+          list[i - p] = (uint32_t)i;
+        }
+      }
+    }
+    __syncthreads();  // cnt, s_tile and s_excl are reused by the next tile
+  }
+}
+
+}  // namespace
+
+// Fills w.f_tk/w.f_tv (touched requests, input order, count counts->n_touch)
+// and w.f_list (plain lookups, input order, count counts->n_lookup).
+int front_classify(Handle* h, const uint64_t* keys, const uint8_t* ops, size_t n, cudaStream_t s) {
+  Work& w = h->w;
+  BatchCounts* c = w.counts;
+  const size_t n_tiles = (n + kScanTile - 1) / kScanTile;
+  // scratch: tile counter, then one status word per tile
+  uint32_t* counter = w.sort_scratch;
+  uint32_t* status = w.sort_scratch + 32;
+  if (cudaMemsetAsync(c, 0, sizeof(BatchCounts), s) != cudaSuccess) return -2;
+  if (cudaMemsetAsync(w.sort_scratch, 0, (32 + n_tiles) * 4, s) != cudaSuccess) return -2;
+  const unsigned g = (unsigned)min((size_t)h->sm_count * 8, (n + kThreads - 1) / kThreads);
+  Slot* tab = reinterpret_cast<Slot*>(w.f_tab);
+  front_count_kernel<<<(unsigned)h->sm_count * 2, kThreads, 0, s>>>(ops, n, c);
+  front_clear_kernel<<<(unsigned)h->sm_count * 4, kThreads, 0, s>>>(tab, w.f_tab_cap, c);
+  front_insert_kernel<<<g, kThreads, 0, s>>>(keys, ops, n, tab, c);
+  static unsigned resident[64] = {};
+  const int dev = h->device;
+  if (dev >= 0 && dev < 64 && !resident[dev]) {
+    int per = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, front_split_kernel, kScanThreads, 0) != cudaSuccess ||
+        per < 1)
+      per = 1;
+    resident[dev] = (unsigned)per * (unsigned)h->sm_count;
+  }
+  const unsigned rb = (dev >= 0 && dev < 64) ? resident[dev] : (unsigned)h->sm_count;
+  front_split_kernel<<<(unsigned)min(n_tiles, (size_t)rb), kScanThreads, 0, s>>>(
+      keys, ops, n, tab, c, counter, status, w.f_tk, w.f_tv, w.f_list, &h->tree.ctrl->error);
+  count_launch(4);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+}  // namespace bt

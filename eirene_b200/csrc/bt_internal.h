@@ -28,7 +28,8 @@ cudaError_t sort_prepare();
 size_t sort_scratch_words(size_t n);
 cudaError_t radix_sort_pairs(const uint64_t* keys_in, const uint32_t* vals_in, const uint8_t* ops, uint64_t* k_a,
                              uint32_t* v_a, uint64_t* k_b, uint32_t* v_b, size_t n, int begin_bit, int end_bit,
-                             uint32_t* scratch, cudaStream_t s, uint64_t** k_out, uint32_t** v_out, uint32_t* err);
+                             uint32_t* scratch, cudaStream_t s, uint64_t** k_out, uint32_t** v_out, uint32_t* err,
+                             const uint32_t* n_dev = nullptr);
 
 // ---- per-batch work buffers, sized for max_batch requests ----
 struct BatchCounts {
@@ -36,6 +37,11 @@ struct BatchCounts {
   uint32_t n_ins;
   uint32_t n_get;
   uint32_t pad;
+  // hash front end (bt_front.cu)
+  uint32_t n_ins_req;  // INSERT requests with a valid key
+  uint32_t cap;        // hash table slots this batch (power of two)
+  uint32_t n_touch;    // requests resolved through the sorted path
+  uint32_t n_lookup;   // requests answered by a plain lookup
 };
 
 struct TileSummary;  // bt_batch.cu
@@ -70,6 +76,15 @@ struct Work {
   void* m_ent_a = nullptr;      // separator entries, 16 B each
   void* m_ent_b = nullptr;
   void* m_counts = nullptr;
+  void* m_sync = nullptr;       // grid barrier + per-block partials of the inner merge
+  // hash front end (bt_front.cu)
+  void* f_tab = nullptr;         // 16 B slots
+  size_t f_tab_cap = 0;          // slots allocated (power of two)
+  uint32_t* f_flags = nullptr;   // [cap]
+  uint32_t* f_pos = nullptr;     // [cap]
+  uint32_t* f_list = nullptr;    // [cap] requests for the plain lookup, in input order
+  uint64_t* f_tk = nullptr;      // [cap] keys of the touched requests, in input order
+  uint32_t* f_tv = nullptr;      // [cap] index | op << 30 of the touched requests
   // host staging for the host-buffer entry point
   uint64_t* d_in_keys = nullptr;
   uint64_t* d_in_vals = nullptr;
@@ -114,6 +129,7 @@ struct Handle {
   int sorted_search = 1;  // batch GET phase: 1 = path-reusing search over the sorted keys
   int sorted_leaf_vals = 0;  // sorted search: load the leaf's values with its keys (1) or only the match (0)
   int batch_descent = -1;    // autotuned choice for the batch GET phase: -1 = follow `descent`
+  int front_end = 1;         // sorted batches: 1 = hash front end (sort only INSERT-coupled requests), 0 = full sort
   int sm_count = 148;
   Work w;
   Learned L;
@@ -194,6 +210,9 @@ cudaError_t launch_serve(Handle* h, const ServeDev& S, cudaStream_t s);
 cudaError_t launch_stm(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, uint8_t op_override,
                        const uint32_t* list, const uint32_t* n_dev, size_t n, uint64_t* out_vals, uint8_t* out_st,
                        cudaStream_t s);
+
+// ---- hash front end of the sorted batch (bt_front.cu) ----
+int front_classify(Handle* h, const uint64_t* keys, const uint8_t* ops, size_t n, cudaStream_t s);
 
 // ---- key-range sharding (bt_shard.cu) ----
 int route_batch(Handle* h, const uint64_t* splitters, int n_shards, const uint64_t* keys, const uint64_t* vals,

@@ -372,28 +372,98 @@ __global__ void __launch_bounds__(256) merge_leaf_kernel(DevTree t, uint32_t lea
 }
 
 // ------------------------------------------------------------- inner ----
-// One block applies the separator entries level by level.  Entries are in
-// ascending key order; those of one parent are contiguous.
-constexpr int kInnerThreads = 1024;
+// The separator entries are applied level by level by one cooperative grid
+// (all blocks resident), with a grid barrier between the steps of a level.
+// Entries are in ascending key order; those of one parent are contiguous.
+// The barrier's wait is bounded: past kBarrierSpin it sets kErrSpin and every
+// block leaves.
+constexpr int kInnerThreads = 512;
+constexpr int kInnerWarps = kInnerThreads / 32;
+constexpr uint32_t kBarrierSpin = 1u << 24;
 
-// block-wide exclusive scan over n values produced by f(i); writes out[i];
-// returns the total.  All threads call it.
+struct InnerSync {
+  unsigned count;
+  unsigned gen;
+  uint32_t fail;
+  uint32_t n_groups;
+  uint32_t total;  // 1 when the capacity check failed
+  uint32_t base;
+  uint32_t pad[2];
+  uint32_t partial[1024];  // per block
+};
+
+__device__ bool grid_sync(InnerSync* gs, uint32_t* err) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    const unsigned g = ld_acquire32(&gs->gen);
+    __threadfence();
+    if (atomicAdd(&gs->count, 1u) == gridDim.x - 1) {
+      gs->count = 0;
+      __threadfence();
+      atomicAdd(&gs->gen, 1u);
+    } else {
+      uint32_t spins = 0;
+      while (ld_acquire32(&gs->gen) == g) {
+        if (++spins > kBarrierSpin) {
+          atomicOr(err, kErrSpin);
+          atomicExch(&gs->fail, 1u);
+          ok = 0;
+          break;
+        }
+        if (spins > 32) __nanosleep(128);
+      }
+    }
+    __threadfence();
+    if (ld_acquire32(&gs->fail)) ok = 0;
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// grid-wide exclusive scan of f(i), i < n: out[i] and the total.  Each block
+// takes one contiguous chunk.  Contains two grid barriers.
 template <typename F>
-__device__ uint32_t blk_scan_n(uint32_t n, F f, uint32_t* out, uint32_t* ws) {
-  uint32_t carry = 0;
-  for (uint32_t base = 0; base < n; base += kInnerThreads) {
+__device__ bool grid_scan_n(uint32_t n, F f, uint32_t* out, InnerSync* gs, uint32_t* err, uint32_t* ws,
+                            uint32_t* total) {
+  const uint32_t chunk = ceil_div(n, gridDim.x);
+  const uint32_t c0 = min(n, blockIdx.x * chunk), c1 = min(n, c0 + chunk);
+  uint32_t sum = 0;
+  for (uint32_t base = c0; base < c1; base += kInnerThreads) {
     const uint32_t i = base + threadIdx.x;
-    const uint32_t v = i < n ? f(i) : 0u;
+    uint32_t tot;
+    blk_exclusive_sum(i < c1 ? f(i) : 0u, ws, &tot);
+    sum += tot;
+  }
+  if (threadIdx.x == 0) gs->partial[blockIdx.x] = sum;
+  if (!grid_sync(gs, err)) return false;
+  // this block's offset: sum of the lower blocks' partials
+  uint32_t off = 0, all = 0;
+  for (uint32_t b = threadIdx.x; b < gridDim.x; b += kInnerThreads) {
+    const uint32_t v = gs->partial[b];
+    all += v;
+    if (b < blockIdx.x) off += v;
+  }
+  uint32_t t0, t1;
+  blk_exclusive_sum(off, ws, &t0);
+  blk_exclusive_sum(all, ws, &t1);
+  uint32_t carry = t0;
+  for (uint32_t base = c0; base < c1; base += kInnerThreads) {
+    const uint32_t i = base + threadIdx.x;
+    const uint32_t v = i < c1 ? f(i) : 0u;
     uint32_t tot;
     const uint32_t ex = blk_exclusive_sum(v, ws, &tot);
-    if (i < n) out[i] = carry + ex;
+    if (i < c1) out[i] = carry + ex;
     carry += tot;
   }
-  return carry;
+  *total = t1;
+  return grid_sync(gs, err);  // out[] complete before anyone reads it
 }
 
 __global__ void __launch_bounds__(kInnerThreads) merge_inner_kernel(DevTree t, uint32_t inner_fill, uint32_t entry_cap,
-                                                                    MergeCounts* mc,
+                                                                    MergeCounts* mc, InnerSync* gs,
                                                                     MergeEntry* ea, MergeEntry* eb,
                                                                     const uint32_t* __restrict__ path,
                                                                     uint32_t* __restrict__ gstart,
@@ -401,11 +471,13 @@ __global__ void __launch_bounds__(kInnerThreads) merge_inner_kernel(DevTree t, u
                                                                     uint32_t* __restrict__ kids_a,
                                                                     uint32_t* __restrict__ kids_b) {
   __shared__ uint32_t ws[32];
-  __shared__ uint32_t s_base, s_ng, s_total;
-  __shared__ uint64_t s_keys[kInnerThreads / 32][32];
+  __shared__ uint32_t s_base;
+  __shared__ uint64_t s_keys[kInnerWarps][32];
   if (mc->cap_fail) return;
   Ctrl* C = t.ctrl;
+  uint32_t* err = &C->error;
   const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t gw = blockIdx.x * kInnerWarps + w, n_warps = gridDim.x * kInnerWarps;
   const uint32_t epoch = C->epoch;
   uint32_t n_e = mc->n_leaf_entries;
   MergeEntry* cur = ea;
@@ -414,7 +486,8 @@ __global__ void __launch_bounds__(kInnerThreads) merge_inner_kernel(DevTree t, u
   for (uint32_t lvl = 1; n_e > 0; lvl++) {
     const uint32_t root_level = C->root_level;
     if (lvl > root_level) {
-      // the root split: rebuild upward from [root, pieces...] with the bulk rule
+      // the root split: block 0 rebuilds upward from [root, pieces...] with the bulk rule
+      if (blockIdx.x != 0) break;
       uint32_t cnt = n_e + 1;
       if ((uint64_t)C->n_nodes + cnt > t.cap) {
         if (threadIdx.x == 0) atomicOr(&C->error, kErrCapacity);
@@ -431,7 +504,7 @@ __global__ void __launch_bounds__(kInnerThreads) merge_inner_kernel(DevTree t, u
         if (threadIdx.x == 0) s_base = atomicAdd(&C->n_nodes, nn);
         __syncthreads();
         const uint32_t nb = s_base;
-        for (uint32_t pidx = w; pidx < nn; pidx += kInnerThreads / 32) {
+        for (uint32_t pidx = w; pidx < nn; pidx += kInnerWarps) {
           const uint32_t kc = piece_size(pidx, cnt, nn), cs = piece_start(pidx, cnt, nn);
           const uint32_t nd = nb + pidx;
           if (lane < 31) t.keys[(size_t)nd * 32 + lane] = (lane + 1 < kc) ? t.low[ka[cs + lane + 1]] : kKeyMax;
@@ -460,13 +533,12 @@ __global__ void __launch_bounds__(kInnerThreads) merge_inner_kernel(DevTree t, u
     }
     // groups of entries sharing a parent at this level
     auto parent_of = [&](uint32_t i) { return path[(size_t)cur[i].rep * kPathLevels + lvl]; };
-    const uint32_t ng = blk_scan_n(
-        n_e, [&](uint32_t i) { return (i == 0 || parent_of(i) != parent_of(i - 1)) ? 1u : 0u; }, goff, ws);
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < n_e; i += kInnerThreads)
-      if (i == 0 || parent_of(i) != parent_of(i - 1)) gstart[goff[i]] = i;
-    if (threadIdx.x == 0) s_ng = ng;
-    __syncthreads();
+    auto is_head = [&](uint32_t i) -> uint32_t { return (i == 0 || parent_of(i) != parent_of(i - 1)) ? 1u : 0u; };
+    uint32_t ng = 0;
+    if (!grid_scan_n(n_e, is_head, goff, gs, err, ws, &ng)) return;
+    for (uint32_t i = blockIdx.x * kInnerThreads + threadIdx.x; i < n_e; i += gridDim.x * kInnerThreads)
+      if (is_head(i)) gstart[goff[i]] = i;
+    if (!grid_sync(gs, err)) return;
     // pieces - 1 per group
     auto group_extra = [&](uint32_t gi) -> uint32_t {
       const uint32_t a = gstart[gi], b = gi + 1 < ng ? gstart[gi + 1] : n_e;
@@ -474,21 +546,24 @@ __global__ void __launch_bounds__(kInnerThreads) merge_inner_kernel(DevTree t, u
       const uint32_t tot = hdr_size(t.keys[(size_t)P * 32 + 31]) + (b - a);
       return tot <= (uint32_t)kMaxKeys ? 0u : ceil_div(tot + 1, inner_fill + 1) - 1;
     };
-    const uint32_t total = blk_scan_n(ng, group_extra, goff, ws);
-    __syncthreads();
-    if (total > entry_cap || (uint64_t)C->n_nodes + total > t.cap) {
-      // cannot happen with inner_fill >= 16 and the headroom reserved above;
-      // stop before writing out of bounds and flag the error
-      if (threadIdx.x == 0) atomicOr(&C->error, kErrCapacity);
-      return;
+    uint32_t total = 0;
+    if (!grid_scan_n(ng, group_extra, goff, gs, err, ws, &total)) return;
+    // one thread checks the capacity and allocates; everyone reads the outcome
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      if (total > entry_cap || (uint64_t)C->n_nodes + total > t.cap) {
+        // cannot happen with inner_fill >= 16 and the headroom reserved
+        // above; stop before writing out of bounds and flag the error
+        atomicOr(&C->error, kErrCapacity);
+        gs->total = 1;
+      } else {
+        gs->total = 0;
+        gs->base = total ? atomicAdd(&C->n_nodes, total) : 0;
+      }
     }
-    if (threadIdx.x == 0) {
-      s_total = total;
-      s_base = total ? atomicAdd(&C->n_nodes, total) : 0;
-    }
-    __syncthreads();
-    const uint32_t nb = s_base;
-    for (uint32_t gi = w; gi < ng; gi += kInnerThreads / 32) {
+    if (!grid_sync(gs, err)) return;
+    if (gs->total) return;
+    const uint32_t nb = gs->base;
+    for (uint32_t gi = gw; gi < ng; gi += n_warps) {
       const uint32_t a = gstart[gi], b = gi + 1 < ng ? gstart[gi + 1] : n_e;
       const uint32_t cnt = b - a;
       const uint32_t P = parent_of(a);
@@ -550,14 +625,14 @@ __global__ void __launch_bounds__(kInnerThreads) merge_inner_kernel(DevTree t, u
       }
       __syncwarp();
     }
-    inner_new += total;
-    __syncthreads();
+    if (blockIdx.x == 0) inner_new += total;
+    if (!grid_sync(gs, err)) return;  // this level's nodes and the next entries are written
     n_e = total;
     MergeEntry* tmp = cur;
     cur = nxt;
     nxt = tmp;
   }
-  if (threadIdx.x == 0 && (inner_new | roots_new)) {
+  if (blockIdx.x == 0 && threadIdx.x == 0 && (inner_new | roots_new)) {
     atomicAdd(&C->inner_splits, inner_new + roots_new);
     atomicAdd(&C->new_roots, roots_new);
   }
@@ -566,6 +641,41 @@ __global__ void __launch_bounds__(kInnerThreads) merge_inner_kernel(DevTree t, u
 inline unsigned nblk(size_t n, int per) { return (unsigned)((n + per - 1) / per); }
 
 }  // namespace
+
+// cooperative launch of merge_inner_kernel: at most the resident blocks
+static cudaError_t launch_inner(Handle* h, uint32_t entry_cap, MergeCounts* mc, cudaStream_t s) {
+  Work& w = h->w;
+  static unsigned resident[64] = {};
+  const int dev = h->device;
+  unsigned blocks = (unsigned)h->sm_count;
+  if (dev >= 0 && dev < 64) {
+    if (!resident[dev]) {
+      int per = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, merge_inner_kernel, kInnerThreads, 0) != cudaSuccess ||
+          per < 1)
+        per = 1;
+      resident[dev] = (unsigned)per * (unsigned)h->sm_count;
+    }
+    blocks = resident[dev];
+  }
+  if (blocks > 1024) blocks = 1024;  // InnerSync::partial
+  InnerSync* gs = reinterpret_cast<InnerSync*>(w.m_sync);
+  cudaError_t e = cudaMemsetAsync(gs, 0, sizeof(InnerSync), s);
+  if (e != cudaSuccess) return e;
+  DevTree tree = h->tree;
+  uint32_t fill = h->inner_fill;
+  MergeEntry* ea = reinterpret_cast<MergeEntry*>(w.m_ent_a);
+  MergeEntry* eb = reinterpret_cast<MergeEntry*>(w.m_ent_b);
+  const uint32_t* path = w.m_path;
+  uint32_t* gstart = w.m_seg;
+  uint32_t* goff = w.m_nleaf;
+  uint32_t* kids_a = w.m_nq;
+  uint32_t* kids_b = w.m_pos;
+  void* args[] = {&tree, &fill, &entry_cap, &mc, &gs, &ea, &eb, &path, &gstart, &goff, &kids_a, &kids_b};
+  e = cudaLaunchCooperativeKernel((const void*)merge_inner_kernel, dim3(blocks), dim3(kInnerThreads), args, 0, s);
+  count_launch();
+  return e;
+}
 
 // Runs the merge engine for the unique INSERT keys of the current batch
 // (w.ins_list, count on the device).  n_upper bounds the count.
@@ -607,11 +717,8 @@ int merge_engine(Handle* h, size_t n_upper, cudaStream_t s) {
   merge_leaf_kernel<<<(unsigned)((size_t)h->sm_count * 8), 256, 0, s>>>(
       h->tree, h->leaf_fill, mc, w.m_seg, w.m_pos, w.m_newk, w.m_newv, w.m_nq, w.m_nleaf, w.ins_list,
       reinterpret_cast<MergeEntry*>(w.m_ent_a), w.uans, w.uans_st);
-  merge_inner_kernel<<<1, kInnerThreads, 0, s>>>(h->tree, h->inner_fill, entry_cap, mc,
-                                                 reinterpret_cast<MergeEntry*>(w.m_ent_a),
-                                                 reinterpret_cast<MergeEntry*>(w.m_ent_b), w.m_path, w.m_seg,
-                                                 w.m_nleaf, w.m_nq, w.m_pos);
-  count_launch(3);
+  count_launch(2);
+  if (launch_inner(h, entry_cap, mc, s) != cudaSuccess) return -2;
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 

@@ -99,21 +99,54 @@ int route_batch(Handle* h, const uint64_t* splitters, int n_shards, const uint64
   Work& w = h->w;
   const int n_split = n_shards - 1;
   if (n == 0) return cudaMemsetAsync(out_counts, 0, (size_t)n_shards * 8, s) == cudaSuccess ? BT_OK : BT_ERR_CUDA;
+  // batches up to the handle's capacity use its work buffers; larger inputs
+  // (a bulk build's keys) take stream-ordered temporaries for this call
+  uint64_t *ids = w.ukeys, *ka = w.k_a, *kb = w.k_b;
+  uint32_t *va = w.v_a, *vb = w.v_b, *scratch = w.sort_scratch;
+  const bool tmp = n > w.cap;
+  if (tmp) {
+    void* p[6] = {};
+    const size_t sz[6] = {n * 8, n * 8, n * 8, n * 4, n * 4, sort_scratch_words(n) * 4};
+    for (int i = 0; i < 6; i++) {
+      if (cudaMallocAsync(&p[i], sz[i], s) != cudaSuccess) {
+        for (int j = 0; j < i; j++) cudaFreeAsync(p[j], s);
+        return BT_ERR_NO_MEMORY;
+      }
+    }
+    ids = (uint64_t*)p[0];
+    ka = (uint64_t*)p[1];
+    kb = (uint64_t*)p[2];
+    va = (uint32_t*)p[3];
+    vb = (uint32_t*)p[4];
+    scratch = (uint32_t*)p[5];
+  }
+  int rc = BT_OK;
   const unsigned g = grid_for(n, h->sm_count);
-  shard_id_kernel<<<g, kThreads, 0, s>>>(keys, n, splitters, n_split, w.ukeys);
+  shard_id_kernel<<<g, kThreads, 0, s>>>(keys, n, splitters, n_split, ids);
   count_launch();
-  if (cudaGetLastError() != cudaSuccess) return BT_ERR_CUDA;
   uint64_t* sk = nullptr;
   uint32_t* perm = nullptr;
   // one stable pass over the low 8 bits (n_shards <= 256) with the index as payload
-  if (radix_sort_pairs(w.ukeys, nullptr, nullptr, w.k_a, w.v_a, w.k_b, w.v_b, n, 0, 8, w.sort_scratch, s, &sk, &perm,
-                       &h->tree.ctrl->error) != cudaSuccess)
-    return BT_ERR_CUDA;
-  route_gather_kernel<<<g, kThreads, 0, s>>>(perm, n, keys, vals, ops, out_keys, out_vals, out_ops, out_perm);
-  count_launch();
-  shard_count_kernel<<<(n_shards + 255) / 256, 256, 0, s>>>(sk, n, n_shards, out_counts);
-  count_launch();
-  return cudaGetLastError() == cudaSuccess ? BT_OK : BT_ERR_CUDA;
+  if (cudaGetLastError() != cudaSuccess ||
+      radix_sort_pairs(ids, nullptr, nullptr, ka, va, kb, vb, n, 0, 8, scratch, s, &sk, &perm,
+                       &h->tree.ctrl->error) != cudaSuccess) {
+    rc = BT_ERR_CUDA;
+  } else {
+    route_gather_kernel<<<g, kThreads, 0, s>>>(perm, n, keys, vals, ops, out_keys, out_vals, out_ops, out_perm);
+    count_launch();
+    shard_count_kernel<<<(n_shards + 255) / 256, 256, 0, s>>>(sk, n, n_shards, out_counts);
+    count_launch();
+    if (cudaGetLastError() != cudaSuccess) rc = BT_ERR_CUDA;
+  }
+  if (tmp) {
+    cudaFreeAsync(ids, s);
+    cudaFreeAsync(ka, s);
+    cudaFreeAsync(kb, s);
+    cudaFreeAsync(va, s);
+    cudaFreeAsync(vb, s);
+    cudaFreeAsync(scratch, s);
+  }
+  return rc;
 }
 
 int unroute_results(Handle* h, const uint32_t* perm, const uint64_t* in_vals, const uint8_t* in_st, size_t n,

@@ -35,9 +35,6 @@ constexpr int kScanItems = 4;
 constexpr int kScanTile = kScanThreads * kScanItems;  // 4096
 
 __device__ __forceinline__ uint32_t digit_of(uint64_t k, int shift) { return (uint32_t)(k >> shift) & 0xff; }
-__device__ __forceinline__ void st_relaxed32(uint32_t* p, uint32_t v) {
-  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
 // 2-bit op code carried in the payload: 0 insert, 1 get, 3 anything else (rejected)
 __device__ __forceinline__ uint32_t op_code(uint8_t op) { return op <= 1 ? (uint32_t)op : 3u; }
 
@@ -138,9 +135,11 @@ constexpr uint32_t kSpinLimit = 1u << 22;
 
 // all digit histograms in one read of the keys: hist[pass][256]
 __global__ void __launch_bounds__(kSortThreads) sort_upfront_hist_kernel(const uint64_t* __restrict__ keys,
-                                                                         size_t n, int begin_bit, int passes,
+                                                                         size_t n, const uint32_t* __restrict__ n_dev,
+                                                                         int begin_bit, int passes,
                                                                          uint32_t* __restrict__ hist) {
   __shared__ uint32_t h[kMaxPasses][kRadix];
+  if (n_dev) n = min(n, (size_t)*n_dev);
   for (int i = threadIdx.x; i < kMaxPasses * kRadix; i += kSortThreads) (&h[0][0])[i] = 0;
   __syncthreads();
   const size_t stride = (size_t)gridDim.x * blockDim.x;
@@ -175,109 +174,132 @@ struct ScatterSmem {
   uint32_t tile;
 };
 
-// payload_mode: 0 = read vals_in; 1 = generate (op code << 30 | i), ops nullable
+// payload_mode: 0 = read vals_in; 1 = generate (op code << 30 | i), ops nullable.
+// Blocks take tiles in increasing order from tile_counter until the tiles run
+// out; a block only ever waits on lower tiles, which running blocks hold, so
+// any grid size is safe (the launcher uses at most the resident blocks).
 __global__ void __launch_bounds__(kSortThreads) sort_onesweep_kernel(
     const uint64_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, const uint8_t* __restrict__ ops,
-    int payload_mode, uint64_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, size_t n, int shift,
-    const uint32_t* __restrict__ gbase, uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ status,
-    uint32_t* __restrict__ err) {
+    int payload_mode, uint64_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, size_t n,
+    const uint32_t* __restrict__ n_dev, int shift, const uint32_t* __restrict__ gbase,
+    uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ status, uint32_t* __restrict__ err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   ScatterSmem& S = *reinterpret_cast<ScatterSmem*>(smem_raw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (threadIdx.x == 0) S.tile = atomicAdd(tile_counter, 1u);
-  for (int i = threadIdx.x; i < kWarps * kRadix; i += kSortThreads) (&S.wh[0][0])[i] = 0;
-  __syncthreads();
-  const uint32_t tile = S.tile;
-  const size_t tile_base = (size_t)tile * kTile;
-  const size_t warp_base = tile_base + (size_t)warp * (32 * kSortItems);
-  uint64_t key[kSortItems];
-  uint32_t val[kSortItems];
-  uint32_t rank[kSortItems];
+  if (n_dev) n = min(n, (size_t)*n_dev);
   const uint32_t lt_mask = (1u << lane) - 1u;
+  for (;;) {
+    if (threadIdx.x == 0) S.tile = atomicAdd(tile_counter, 1u);
+    for (int i = threadIdx.x; i < kWarps * kRadix; i += kSortThreads) (&S.wh[0][0])[i] = 0;
+    __syncthreads();
+    const uint32_t tile = S.tile;
+    const size_t tile_base = (size_t)tile * kTile;
+    if (tile_base >= n) return;  // tiles are handed out in order: later ones are empty too
+    const size_t warp_base = tile_base + (size_t)warp * (32 * kSortItems);
+    uint64_t key[kSortItems];
+    uint32_t val[kSortItems];
+    uint32_t rank[kSortItems];
 #pragma unroll
-  for (int r = 0; r < kSortItems; r++) {
-    const size_t idx = warp_base + (size_t)r * 32 + lane;
-    const bool valid = idx < n;
-    key[r] = valid ? keys_in[idx] : 0;
-    if (payload_mode == 0) val[r] = valid ? vals_in[idx] : 0;
-    else val[r] = (uint32_t)idx | (ops && valid ? (op_code(ops[idx]) << 30) : 0u);
-    const uint32_t d = valid ? digit_of(key[r], shift) : 0x1FFu;
-    // lanes holding the same digit: AND of eight bit ballots (plus a validity bit)
-    uint32_t peers = __ballot_sync(0xffffffffu, valid);
-    peers = valid ? peers : ~peers;
+    for (int r = 0; r < kSortItems; r++) {
+      const size_t idx = warp_base + (size_t)r * 32 + lane;
+      const bool valid = idx < n;
+      key[r] = valid ? keys_in[idx] : 0;
+      if (payload_mode == 0) val[r] = valid ? vals_in[idx] : 0;
+      else val[r] = (uint32_t)idx | (ops && valid ? (op_code(ops[idx]) << 30) : 0u);
+      const uint32_t d = valid ? digit_of(key[r], shift) : 0x1FFu;
+      // lanes holding the same digit: AND of eight bit ballots (plus a validity bit)
+      uint32_t peers = __ballot_sync(0xffffffffu, valid);
+      peers = valid ? peers : ~peers;
 #pragma unroll
-    for (int b = 0; b < 8; b++) {
-      const uint32_t bal = __ballot_sync(0xffffffffu, (d >> b) & 1u);
-      peers &= ((d >> b) & 1u) ? bal : ~bal;
-    }
-    uint32_t before = 0;
-    if (valid) before = S.wh[warp][d];
-    __syncwarp();
-    if (valid && lane == (uint32_t)(__ffs(peers) - 1)) S.wh[warp][d] = before + __popc(peers);
-    __syncwarp();
-    rank[r] = before + __popc(peers & lt_mask);
-  }
-  __syncthreads();
-  // per digit: prefix over warps and the tile total
-  uint32_t total = 0;
-  if (threadIdx.x < kRadix) {
-    const int d = threadIdx.x;
-#pragma unroll
-    for (int w = 0; w < kWarps; w++) {
-      const uint32_t c = S.wh[w][d];
-      S.wh[w][d] = total;
-      total += c;
-    }
-    // publish this tile's count, then look back for the exclusive prefix
-    uint32_t* my = status + (size_t)tile * kRadix + d;
-    if (tile == 0) {
-      st_relaxed32(my, kFlagPrefix | total);
-      S.gofs[d] = gbase[d];
-    } else {
-      st_relaxed32(my, kFlagAgg | total);
-      uint32_t excl = 0;
-      int64_t t = (int64_t)tile - 1;
-      uint32_t spins = 0;
-      while (t >= 0) {
-        const uint32_t w = ld_relaxed32(status + (size_t)t * kRadix + d);
-        const uint32_t f = w & ~kValMask;
-        if (f == 0) {
-          if (++spins > kSpinLimit) {
-            atomicOr(err, kErrSpin);
-            break;
-          }
-          if (spins > 64) __nanosleep(64);
-          continue;
-        }
-        excl += w & kValMask;
-        if (f == kFlagPrefix) break;
-        t--;
+      for (int b = 0; b < 8; b++) {
+        const uint32_t bal = __ballot_sync(0xffffffffu, (d >> b) & 1u);
+        peers &= ((d >> b) & 1u) ? bal : ~bal;
       }
-      st_relaxed32(my, kFlagPrefix | (excl + total));
-      S.gofs[d] = gbase[d] + excl;
+      uint32_t before = 0;
+      if (valid) before = S.wh[warp][d];
+      __syncwarp();
+      if (valid && lane == (uint32_t)(__ffs(peers) - 1)) S.wh[warp][d] = before + __popc(peers);
+      __syncwarp();
+      rank[r] = before + __popc(peers & lt_mask);
     }
-  }
-  const uint32_t st = block_exclusive_scan(threadIdx.x < kRadix ? total : 0u, S.ws, nullptr);
-  if (threadIdx.x < kRadix) S.tstart[threadIdx.x] = st;
-  __syncthreads();
+    __syncthreads();
+    // per digit: prefix over warps and the tile total
+    uint32_t total = 0;
+    if (threadIdx.x < kRadix) {
+      const int d = threadIdx.x;
 #pragma unroll
-  for (int r = 0; r < kSortItems; r++) {
-    const size_t idx = warp_base + (size_t)r * 32 + lane;
-    if (idx < n) {
-      const uint32_t d = digit_of(key[r], shift);
-      const uint32_t pos = S.tstart[d] + S.wh[warp][d] + rank[r];
-      S.k[pos] = key[r];
-      S.v[pos] = val[r];
+      for (int w = 0; w < kWarps; w++) {
+        const uint32_t c = S.wh[w][d];
+        S.wh[w][d] = total;
+        total += c;
+      }
+      // publish this tile's count, then look back for the exclusive prefix
+      uint32_t* my = status + (size_t)tile * kRadix + d;
+      if (tile == 0) {
+        st_relaxed32(my, kFlagPrefix | total);
+        S.gofs[d] = gbase[d];
+      } else {
+        st_relaxed32(my, kFlagAgg | total);
+        // look back eight predecessors per step (independent loads), in order
+        uint32_t excl = 0;
+        int64_t t = (int64_t)tile - 1;
+        uint32_t spins = 0;
+        while (t >= 0) {
+          uint32_t wv[8];
+#pragma unroll
+          for (int j = 0; j < 8; j++)
+            wv[j] = (t - j >= 0) ? ld_relaxed32(status + (size_t)(t - j) * kRadix + d) : kFlagPrefix;
+          int used = 0;
+          bool done = false, wait = false;
+#pragma unroll
+          for (int j = 0; j < 8; j++) {
+            if (done || wait) continue;
+            const uint32_t f = wv[j] & ~kValMask;
+            if (f == 0) {
+              wait = true;
+              continue;
+            }
+            excl += wv[j] & kValMask;
+            used++;
+            if (f == kFlagPrefix) done = true;
+          }
+          if (done) break;
+          t -= used;
+          if (wait) {
+            if (++spins > kSpinLimit) {
+              atomicOr(err, kErrSpin);
+              break;
+            }
+            if (spins > 64) __nanosleep(64);
+          }
+        }
+        st_relaxed32(my, kFlagPrefix | (excl + total));
+        S.gofs[d] = gbase[d] + excl;
+      }
     }
-  }
-  __syncthreads();
-  const uint32_t tile_n = (uint32_t)min((size_t)kTile, n - tile_base);
-  for (uint32_t i = threadIdx.x; i < tile_n; i += kSortThreads) {
-    const uint64_t k = S.k[i];
-    const uint32_t d = digit_of(k, shift);
-    const uint32_t g = S.gofs[d] + (i - S.tstart[d]);
-    keys_out[g] = k;
-    vals_out[g] = S.v[i];
+    const uint32_t st = block_exclusive_scan(threadIdx.x < kRadix ? total : 0u, S.ws, nullptr);
+    if (threadIdx.x < kRadix) S.tstart[threadIdx.x] = st;
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kSortItems; r++) {
+      const size_t idx = warp_base + (size_t)r * 32 + lane;
+      if (idx < n) {
+        const uint32_t d = digit_of(key[r], shift);
+        const uint32_t pos = S.tstart[d] + S.wh[warp][d] + rank[r];
+        S.k[pos] = key[r];
+        S.v[pos] = val[r];
+      }
+    }
+    __syncthreads();
+    const uint32_t tile_n = (uint32_t)min((size_t)kTile, n - tile_base);
+    for (uint32_t i = threadIdx.x; i < tile_n; i += kSortThreads) {
+      const uint64_t k = S.k[i];
+      const uint32_t d = digit_of(k, shift);
+      const uint32_t g = S.gofs[d] + (i - S.tstart[d]);
+      keys_out[g] = k;
+      vals_out[g] = S.v[i];
+    }
+    __syncthreads();  // the staging buffers and S.tile are reused by the next tile
   }
 }
 
@@ -328,6 +350,22 @@ cudaError_t sort_prepare() {
                               (int)sizeof(ScatterSmem));
 }
 
+// resident onesweep blocks on the current device (cached per device)
+static unsigned onesweep_resident() {
+  static unsigned cache[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (!cache[dev]) {
+    int per = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sort_onesweep_kernel, kSortThreads,
+                                                      sizeof(ScatterSmem)) != cudaSuccess || per < 1)
+      per = 1;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 148;
+    cache[dev] = (unsigned)(per * sms);
+  }
+  return cache[dev];
+}
+
 // scratch: hist[8][256] | tile counters[8] (+pad) | status[8][tiles][256]
 size_t sort_scratch_words(size_t n) {
   const size_t t = sort_tiles(n ? n : 1);
@@ -339,15 +377,18 @@ size_t sort_scratch_words(size_t n) {
 // Sorts n pairs by bits [begin_bit, end_bit) of the key.  Input keys_in (and
 // vals_in, or generated payload when vals_in == nullptr) are not modified.
 // Result lands in (k_a, v_a) or (k_b, v_b); *k_out/*v_out name which.  A look-
-// back timeout sets kErrSpin in *err (the result is then not sorted).
+// back timeout sets kErrSpin in *err (the result is then not sorted).  With
+// n_dev the count is min(n, *n_dev), read on the device (n sizes the grids).
 cudaError_t radix_sort_pairs(const uint64_t* keys_in, const uint32_t* vals_in, const uint8_t* ops, uint64_t* k_a,
                              uint32_t* v_a, uint64_t* k_b, uint32_t* v_b, size_t n, int begin_bit, int end_bit,
-                             uint32_t* scratch, cudaStream_t s, uint64_t** k_out, uint32_t** v_out, uint32_t* err) {
+                             uint32_t* scratch, cudaStream_t s, uint64_t** k_out, uint32_t** v_out, uint32_t* err,
+                             const uint32_t* n_dev) {
   *k_out = k_a;
   *v_out = v_a;
   if (n == 0) return cudaSuccess;
   const int passes = (end_bit - begin_bit + 7) / 8;
   if (passes <= 0) {
+    if (n_dev) return cudaErrorInvalidValue;
     copy_keys_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(keys_in, k_a, n);
     count_launch();
     if (vals_in) cudaMemcpyAsync(v_a, vals_in, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
@@ -366,18 +407,19 @@ cudaError_t radix_sort_pairs(const uint64_t* keys_in, const uint32_t* vals_in, c
                                   ((size_t)kMaxPasses * kRadix + 64 + (size_t)passes * n_tiles * kRadix) * 4, s);
   if (e != cudaSuccess) return e;
   unsigned hb = (unsigned)min((size_t)n_tiles, (size_t)1024);
-  sort_upfront_hist_kernel<<<hb, kSortThreads, 0, s>>>(keys_in, n, begin_bit, passes, hist);
+  sort_upfront_hist_kernel<<<hb, kSortThreads, 0, s>>>(keys_in, n, n_dev, begin_bit, passes, hist);
   count_launch();
   sort_digit_scan_kernel<<<1, kRadix, 0, s>>>(hist, passes);
   count_launch();
+  const unsigned grid = min(n_tiles, onesweep_resident());
   const uint64_t* src_k = keys_in;
   const uint32_t* src_v = vals_in;
   int mode = vals_in ? 0 : 1;
   uint64_t* dst_k = k_a;
   uint32_t* dst_v = v_a;
   for (int p = 0; p < passes; p++) {
-    sort_onesweep_kernel<<<n_tiles, kSortThreads, sizeof(ScatterSmem), s>>>(
-        src_k, src_v, ops, mode, dst_k, dst_v, n, begin_bit + 8 * p, hist + p * kRadix, counters + p,
+    sort_onesweep_kernel<<<grid, kSortThreads, sizeof(ScatterSmem), s>>>(
+        src_k, src_v, ops, mode, dst_k, dst_v, n, n_dev, begin_bit + 8 * p, hist + p * kRadix, counters + p,
         status + (size_t)p * n_tiles * kRadix, err);
     count_launch();
     e = cudaGetLastError();

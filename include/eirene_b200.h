@@ -185,6 +185,10 @@ int bt_set_search_group(bt_handle *h, uint32_t lanes);
 #define BT_OPT_TRAIN_STEPS 3   /* Adam steps of the learned root model per bt_retrain */
 #define BT_OPT_SORTED_LEAF_VALS 4 /* sorted search loads leaf values with the keys (1) or only the match (0) */
 #define BT_OPT_BATCH_DESCENT 5 /* batch GET phase: -1 follow bt_set_descent (default), 0 plain, 1 learned */
+#define BT_OPT_FRONT_END 6     /* BT_MODE_SORTED batches: 1 (default) hash front end - only requests whose key
+                                * has an INSERT at or before them in the batch are sorted and merged, the rest
+                                * are unsorted lookups of the pre-batch tree; 0 sort the whole batch (the
+                                * reference's layout, v38 bpt-gpustm-kernel.cu:289-324).  Same answers. */
 int bt_set_option(bt_handle *h, int option, int64_t value);
 /* Autotuner: times the lookup configurations on this tree with n sample keys
  * (device pointer, n <= max_batch) and keeps the fastest: lanes per request of
@@ -282,8 +286,10 @@ int bt_gen_requests(int dist, uint64_t seed, const uint64_t *tree_keys, size_t n
  * bt_route_batch reorders a batch by owning shard, stably (each shard's run
  * keeps the input order): out_keys/out_vals/out_ops[i] = input[out_perm[i]],
  * out_counts[s] (device, uint64) = length of shard s's run.  vals and ops may
- * be NULL (their outputs are then not written).  n <= max_batch.  Uses the
- * handle's batch work buffers: stream-ordered with the handle's other calls.
+ * be NULL (their outputs are then not written).  n < 2^32.  Up to max_batch
+ * requests it uses the handle's batch work buffers (stream-ordered with the
+ * handle's other calls); larger inputs, such as the keys of a sharded bulk
+ * build, take stream-ordered temporaries (cudaMallocAsync) for the call.
  *
  * bt_unroute_results scatters answers that came back in routed order to
  * input order: out_vals[perm[i]] = in_vals[i], out_status[perm[i]] = in_status[i]. */

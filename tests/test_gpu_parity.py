@@ -65,9 +65,11 @@ def test_search_matches_oracle(gpu):
         assert (host_u64(gv) == ov).all(), lanes
 
 
+@pytest.mark.parametrize("front", [1, 0])
 @pytest.mark.parametrize("mix", [95, 50, 0])
-def test_sorted_batch_uniform(gpu, mix):
+def test_sorted_batch_uniform(gpu, mix, front):
     t, o, keys = make_pair(100_000, seed=11)
+    t.set_option(E.OPT_FRONT_END, front)
     for b in range(3):
         rk, rv, ro = O.gen_requests("uniform", 100 + b, keys, 60_000, mix)
         ov, os_ = o.execute_merged(rk, rv, ro)
@@ -79,9 +81,11 @@ def test_sorted_batch_uniform(gpu, mix):
     assert st["error"] == 0 and st["retry_exhausted"] == 0
 
 
+@pytest.mark.parametrize("front", [1, 0])
 @pytest.mark.parametrize("dist", ["zipf", "normal", "gamma"])
-def test_sorted_batch_skewed_duplicates(gpu, dist):
+def test_sorted_batch_skewed_duplicates(gpu, dist, front):
     t, o, keys = make_pair(50_000, dist=dist, seed=21)
+    t.set_option(E.OPT_FRONT_END, front)
     for b in range(2):
         rk, rv, ro = O.gen_requests(dist, 200 + b, keys, 80_000, 95 if b == 0 else 50)
         ov, os_ = o.execute_merged(rk, rv, ro)
@@ -91,8 +95,10 @@ def test_sorted_batch_skewed_duplicates(gpu, dist):
     assert_same_contents(t, o)
 
 
-def test_sorted_batch_edge_cases(gpu):
+@pytest.mark.parametrize("front", [1, 0])
+def test_sorted_batch_edge_cases(gpu, front):
     t = E.BTree(max_keys=1 << 16, max_batch=1 << 15)
+    t.set_option(E.OPT_FRONT_END, front)
     o = O.OracleTree()
     # empty tree: gets are absent, inserts build the tree through STM
     cases = [

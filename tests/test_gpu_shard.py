@@ -25,12 +25,14 @@ def np_route(spl, keys, n_shards):
     return perm, np.bincount(ids, minlength=n_shards)
 
 
-@pytest.mark.parametrize("n,n_shards,dup", [(0, 4, False), (1, 1, False), (1, 8, False), (4095, 8, False),
-                                            (4096, 8, True), (100_000, 8, False), (1 << 20, 256, True),
-                                            (77_777, 2, False)])
-def test_route_matches_stable_partition(gpu, n, n_shards, dup):
+@pytest.mark.parametrize("n,n_shards,dup,cap", [(0, 4, False, 1), (1, 1, False, 1), (1, 8, False, 1),
+                                                (4095, 8, False, 4095), (4096, 8, True, 4096),
+                                                (100_000, 8, False, 100_000), (1 << 20, 256, True, 1 << 20),
+                                                (77_777, 2, False, 77_777), (300_001, 5, False, 4096)])
+def test_route_matches_stable_partition(gpu, n, n_shards, dup, cap):
+    # cap < n: the input is larger than the handle's batch buffers (temporaries)
     rng = np.random.default_rng(n + n_shards)
-    t = E.BTree(max_keys=1 << 12, max_batch=max(n, 1))
+    t = E.BTree(max_keys=1 << 12, max_batch=cap)
     keys = rng.integers(0, 2**64, n, dtype=np.uint64, endpoint=False)
     pool = keys if n else rng.integers(0, 2**64, 16, dtype=np.uint64)
     spl = np.sort(rng.choice(pool, n_shards - 1)) if n_shards > 1 else np.zeros(0, np.uint64)
