@@ -168,6 +168,7 @@ int bt_destroy(bt_handle* H) {
   cudaFree(h.enum_b);
   cudaFree(h.enum_cnt);
   cudaFree(h.enum_scan_scratch);
+  cudaFree(h.top);
   if (h.internal_stream) cudaStreamDestroy(h.internal_stream);
   for (cudaEvent_t e : h.prof_ev) cudaEventDestroy(e);
   delete H;
@@ -402,6 +403,11 @@ int bt_set_option(bt_handle* H, int option, int64_t value) {
     case BT_OPT_SORTED_SEARCH: H->h.sorted_search = value ? 1 : 0; return BT_OK;
     case BT_OPT_SORTED_LEAF_VALS: H->h.sorted_leaf_vals = value ? 1 : 0; return BT_OK;
     case BT_OPT_FRONT_END: H->h.front_end = value ? 1 : 0; return BT_OK;
+    case BT_OPT_TOP_CACHE: H->h.top_cache = value ? 1 : 0; return BT_OK;
+    case BT_OPT_SEARCH_PAIRS:
+      if (value < 0 || value > 2) return BT_ERR_INVALID_ARG;
+      H->h.search_pairs = (int)value;
+      return BT_OK;
     case BT_OPT_BATCH_DESCENT:
       if (value < -1 || value > 1) return BT_ERR_INVALID_ARG;
       H->h.batch_descent = (int)value;

@@ -62,13 +62,15 @@ __device__ __forceinline__ uint32_t table_cap(uint32_t n_ins, size_t cap_max) {
 __global__ void __launch_bounds__(kThreads) front_count_kernel(const uint8_t* __restrict__ ops, size_t n,
                                                                BatchCounts* __restrict__ counts) {
   uint32_t c = 0;
-  const size_t n4 = n / 4;
+  // four op codes per load when the array is 4-byte aligned
+  const size_t n4 = ((uintptr_t)ops & 3u) ? 0 : n / 4;
   const uchar4* o4 = reinterpret_cast<const uchar4*>(ops);
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += (size_t)gridDim.x * blockDim.x) {
     const uchar4 o = o4[i];
     c += (o.x == kOpInsert) + (o.y == kOpInsert) + (o.z == kOpInsert) + (o.w == kOpInsert);
   }
-  if (blockIdx.x == 0 && threadIdx.x < n - n4 * 4) c += ops[n4 * 4 + threadIdx.x] == kOpInsert ? 1u : 0u;
+  for (size_t i = n4 * 4 + (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    c += ops[i] == kOpInsert ? 1u : 0u;
   c = __reduce_add_sync(0xffffffffu, c);
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(&counts->n_ins_req, c);
 }
@@ -89,24 +91,35 @@ __global__ void __launch_bounds__(kThreads) front_insert_kernel(const uint64_t* 
                                                                 Slot* __restrict__ tab,
                                                                 const BatchCounts* __restrict__ counts) {
   const uint32_t mask = counts->cap - 1;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    if (ops[i] != kOpInsert) continue;
+  auto put = [&](size_t i) {
     const uint64_t k = keys[i];
-    if (k == kKeyMax) continue;
+    if (k == kKeyMax) return;
     uint32_t h = (uint32_t)slot_hash(k) & mask;
     for (uint32_t probe = 0; probe <= mask; probe++) {
       const unsigned long long prev = atomicCAS(&tab[h].key, (unsigned long long)kKeyMax, (unsigned long long)k);
       if (prev == kKeyMax || prev == k) {
         atomicMin(&tab[h].first, (uint32_t)i);
-        break;
+        return;
       }
       h = (h + 1) & mask;
     }
+  };
+  // four op codes per load when the array is 4-byte aligned
+  const size_t n4 = ((uintptr_t)ops & 3u) ? 0 : n / 4;
+  const uchar4* o4 = reinterpret_cast<const uchar4*>(ops);
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += (size_t)gridDim.x * blockDim.x) {
+    const uchar4 o = o4[i];
+    if (o.x == kOpInsert) put(4 * i);
+    if (o.y == kOpInsert) put(4 * i + 1);
+    if (o.z == kOpInsert) put(4 * i + 2);
+    if (o.w == kOpInsert) put(4 * i + 3);
   }
+  for (size_t i = n4 * 4 + (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    if (ops[i] == kOpInsert) put(i);
 }
 
-__device__ __forceinline__ uint32_t find_first(const Slot* __restrict__ tab, uint32_t mask, uint64_t k) {
-  uint32_t h = (uint32_t)slot_hash(k) & mask;
+__device__ __forceinline__ uint32_t find_first_from(const Slot* __restrict__ tab, uint32_t mask, uint64_t k,
+                                                    uint32_t h) {
   for (uint32_t probe = 0; probe <= mask; probe++) {
     const uint64_t sk = tab[h].key;
     if (sk == k) return tab[h].first;
@@ -121,8 +134,8 @@ __device__ __forceinline__ uint32_t find_first(const Slot* __restrict__ tab, uin
 // key has an INSERT at or before it.  Touched requests go to (tk, tv) and the
 // rest to list, both in input order; the block holding the last tile writes
 // the two counts.  A look-back that waits past kSpinLimit sets kErrSpin.
-constexpr int kScanThreads = 256;
-constexpr int kScanItems = 16;
+constexpr int kScanThreads = 512;
+constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;  // 4096
 constexpr int kScanWarps = kScanThreads / 32;
 constexpr uint32_t kFlagAgg = 1u << 30;
@@ -150,18 +163,37 @@ __global__ void __launch_bounds__(kScanThreads) front_split_kernel(
     uint64_t k[kScanItems];
     uint8_t op[kScanItems];
     uint32_t bal[kScanItems];
+    uint64_t sk[kScanItems];
+    uint32_t sf[kScanItems], sh[kScanItems];
+    // loads first, then every item's first probe slot (independent loads in
+    // flight), then the rare longer probes
+#pragma unroll
+    for (int j = 0; j < kScanItems; j++) {
+      const size_t i = base + (size_t)j * kScanThreads + threadIdx.x;
+      k[j] = i < n ? keys[i] : kKeyMax;
+      op[j] = i < n ? ops[i] : 0;
+    }
+#pragma unroll
+    for (int j = 0; j < kScanItems; j++) {
+      sh[j] = (uint32_t)slot_hash(k[j]) & mask;
+      sk[j] = kKeyMax;
+      sf[j] = kNone;
+      if (any && k[j] != kKeyMax) {
+        const ulonglong2 e = __ldg(reinterpret_cast<const ulonglong2*>(tab + sh[j]));
+        sk[j] = e.x;
+        sf[j] = (uint32_t)e.y;
+      }
+    }
 #pragma unroll
     for (int j = 0; j < kScanItems; j++) {
       const size_t i = base + (size_t)j * kScanThreads + threadIdx.x;
       bool f = false;
-      k[j] = 0;
-      op[j] = 0;
       if (i < n) {
-        k[j] = keys[i];
-        op[j] = ops[i];
         f = op[j] > 1;  // invalid op codes are rejected on the sorted path
         if (!f && any && k[j] != kKeyMax) {
-          const uint32_t first = find_first(tab, mask, k[j]);
+          uint32_t first = kNone;
+          if (sk[j] == k[j]) first = sf[j];
+          else if (sk[j] != kKeyMax) first = find_first_from(tab, mask, k[j], (sh[j] + 1) & mask);
           f = first != kNone && (uint32_t)i >= first;
         }
       }

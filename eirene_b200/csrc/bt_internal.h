@@ -22,7 +22,8 @@ enum Phase { kPhSort = 0, kPhMerge, kPhSearch, kPhInsert, kPhWriteback, kNumPhas
 // ---- scan / sort (bt_sort.cu) ----
 size_t scan_scratch_words(size_t n);
 cudaError_t scan_exclusive_u32(const uint32_t* in, uint32_t* out, size_t n, uint32_t* total_dev, uint32_t* scratch,
-                               cudaStream_t s);
+                               cudaStream_t s,
+                               const uint32_t* n_dev = nullptr);
 size_t sort_tiles(size_t n);
 cudaError_t sort_prepare();
 size_t sort_scratch_words(size_t n);
@@ -42,6 +43,14 @@ struct BatchCounts {
   uint32_t cap;        // hash table slots this batch (power of two)
   uint32_t n_touch;    // requests resolved through the sorted path
   uint32_t n_lookup;   // requests answered by a plain lookup
+};
+
+constexpr int kTopNodes = 256;  // nodes of the shared-memory top cache (384 B each)
+struct TopInfo {
+  uint32_t n_nodes;
+  uint32_t n_levels;     // cached levels below and including the root (0: no cache)
+  uint32_t below_level;  // level of the nodes the last cached level points to
+  uint32_t pad;
 };
 
 struct TileSummary;  // bt_batch.cu
@@ -130,6 +139,10 @@ struct Handle {
   int sorted_leaf_vals = 0;  // sorted search: load the leaf's values with its keys (1) or only the match (0)
   int batch_descent = -1;    // autotuned choice for the batch GET phase: -1 = follow `descent`
   int front_end = 1;         // sorted batches: 1 = hash front end (sort only INSERT-coupled requests), 0 = full sort
+  int top_cache = 1;         // unsorted searches descend the upper levels from shared memory
+  int search_pairs = 2;      // unsorted searches: 2 pairs of requests per lane group, child ids only; 1 pairs; 0 single
+  void* top = nullptr;       // top cache (kTopNodes nodes) + TopInfo
+  TopInfo* top_info = nullptr;
   int sm_count = 148;
   Work w;
   Learned L;
@@ -172,6 +185,9 @@ int tree_bulk_build_scratch(Handle* h, const uint64_t* keys, const uint64_t* val
                             const BuildScratch& sc);
 cudaError_t launch_search(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev, size_t n,
                           uint64_t* out_vals, uint8_t* out_st, cudaStream_t s);
+// the same search with the tree's upper levels cached in shared memory
+cudaError_t launch_search_top(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev,
+                              size_t n, uint64_t* out_vals, uint8_t* out_st, cudaStream_t s);
 // search over keys in ascending order (path reuse); needs root_level < 8
 cudaError_t launch_search_sorted(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev,
                                  size_t n, uint64_t* out_vals, uint8_t* out_st, cudaStream_t s);

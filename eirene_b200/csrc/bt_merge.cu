@@ -232,10 +232,10 @@ __global__ void merge_compact_kernel(const uint32_t* __restrict__ ins_list, cons
 
 __global__ void merge_seg_flags_kernel(const MergeCounts* __restrict__ mc, const uint32_t* __restrict__ nleaf,
                                        size_t n_upper, uint32_t* __restrict__ flags) {
-  const uint32_t n_new = mc->n_new;
+  const size_t n_new = min(n_upper, (size_t)mc->n_new);  // the scan reads n_new flags
   const size_t stride = (size_t)gridDim.x * blockDim.x;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_upper; i += stride)
-    flags[i] = (i < n_new && (i == 0 || nleaf[i] != nleaf[i - 1])) ? 1u : 0u;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_new; i += stride)
+    flags[i] = (i == 0 || nleaf[i] != nleaf[i - 1]) ? 1u : 0u;
 }
 
 __global__ void merge_seg_start_kernel(const MergeCounts* __restrict__ mc, const uint32_t* __restrict__ flags,
@@ -256,18 +256,14 @@ __device__ __forceinline__ void seg_bounds(const MergeCounts* mc, const uint32_t
 __global__ void merge_leaf_count_kernel(DevTree t, uint32_t leaf_fill, const MergeCounts* __restrict__ mc,
                                         const uint32_t* __restrict__ seg_start, const uint32_t* __restrict__ nleaf,
                                         size_t n_upper, uint32_t* __restrict__ extra) {
-  const uint32_t n_segs = mc->n_segs;
+  const size_t n_segs = min(n_upper, (size_t)mc->n_segs);  // the scan reads n_segs entries
   const size_t stride = (size_t)gridDim.x * blockDim.x;
-  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < n_upper; s += stride) {
-    uint32_t e = 0;
-    if (s < n_segs) {
-      uint32_t a, b;
-      seg_bounds(mc, seg_start, (uint32_t)s, a, b);
-      const uint32_t leaf = nleaf[a];
-      const uint32_t m = hdr_size(t.keys[(size_t)leaf * 32 + 31]) + (b - a);
-      e = m <= (uint32_t)kMaxKeys ? 0u : ceil_div(m, leaf_fill) - 1;
-    }
-    extra[s] = e;
+  for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < n_segs; s += stride) {
+    uint32_t a, b;
+    seg_bounds(mc, seg_start, (uint32_t)s, a, b);
+    const uint32_t leaf = nleaf[a];
+    const uint32_t m = hdr_size(t.keys[(size_t)leaf * 32 + 31]) + (b - a);
+    extra[s] = m <= (uint32_t)kMaxKeys ? 0u : ceil_div(m, leaf_fill) - 1;
   }
 }
 
@@ -685,7 +681,6 @@ int merge_engine(Handle* h, size_t n_upper, cudaStream_t s) {
   const uint32_t* n_ins = &w.counts->n_ins;
   merge_ensure_root_kernel<<<1, 1, 0, s>>>(h->tree);
   count_launch();
-  if (cudaMemsetAsync(w.m_isnew, 0, n_upper * 4, s) != cudaSuccess) return -2;
   if (cudaMemsetAsync(mc, 0, sizeof(MergeCounts), s) != cudaSuccess) return -2;
   {
     static int per_sm[64] = {};
@@ -700,17 +695,19 @@ int merge_engine(Handle* h, size_t n_upper, cudaStream_t s) {
                                                             w.m_leaf, w.m_isnew, w.uans, w.uans_st);
     count_launch();
   }
-  if (scan_exclusive_u32(w.m_isnew, w.m_pos, n_upper, &mc->n_new, w.sort_scratch, s) != cudaSuccess) return -2;
+  if (scan_exclusive_u32(w.m_isnew, w.m_pos, n_upper, &mc->n_new, w.sort_scratch, s, n_ins) != cudaSuccess) return -2;
   const unsigned gb = (unsigned)min((size_t)h->sm_count * 8, (n_upper + 255) / 256);
   merge_compact_kernel<<<gb, 256, 0, s>>>(w.ins_list, n_ins, w.m_isnew, w.m_pos, w.ukeys, w.uvals, w.m_leaf, w.m_newk,
                                           w.m_newv, w.m_nq, w.m_nleaf);
   merge_seg_flags_kernel<<<gb, 256, 0, s>>>(mc, w.m_nleaf, n_upper, w.m_isnew);
   count_launch(2);
-  if (scan_exclusive_u32(w.m_isnew, w.m_pos, n_upper, &mc->n_segs, w.sort_scratch, s) != cudaSuccess) return -2;
+  if (scan_exclusive_u32(w.m_isnew, w.m_pos, n_upper, &mc->n_segs, w.sort_scratch, s, &mc->n_new) != cudaSuccess)
+    return -2;
   merge_seg_start_kernel<<<gb, 256, 0, s>>>(mc, w.m_isnew, w.m_pos, w.m_seg);
   merge_leaf_count_kernel<<<gb, 256, 0, s>>>(h->tree, h->leaf_fill, mc, w.m_seg, w.m_nleaf, n_upper, w.m_isnew);
   count_launch(2);
-  if (scan_exclusive_u32(w.m_isnew, w.m_pos, n_upper, &mc->n_leaf_entries, w.sort_scratch, s) != cudaSuccess)
+  if (scan_exclusive_u32(w.m_isnew, w.m_pos, n_upper, &mc->n_leaf_entries, w.sort_scratch, s, &mc->n_segs) !=
+      cudaSuccess)
     return -2;
   const uint32_t entry_cap = (uint32_t)w.cap;
   merge_alloc_kernel<<<1, 1, 0, s>>>(h->tree, mc, entry_cap);

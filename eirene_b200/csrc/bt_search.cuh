@@ -88,4 +88,71 @@ __device__ __forceinline__ uint8_t group_descend(const DevTree& t, uint32_t node
   return group_leaf_lookup<G, kLeafVals>(t, node, key, g, gmask, k, v, cnt, ans);
 }
 
+// Two descents in lock step (same tree, same height): every level issues the
+// row loads of both requests before using either, doubling the loads a group
+// keeps in flight.  Results as group_descend for each key.
+// kChild: at inner levels load only the chosen child id (one 32 B sector)
+// after the key comparison instead of the whole 256 B child row with the keys:
+// fewer bytes per level, one more dependent load.
+template <int G, bool kLeafVals, bool kChild = false>
+__device__ __forceinline__ void group_descend2(const DevTree& t, uint32_t node, uint32_t level, uint64_t key_a,
+                                               uint64_t key_b, uint32_t g, uint32_t gmask, uint64_t& ans_a,
+                                               uint8_t& st_a, uint64_t& ans_b, uint8_t& st_b) {
+  constexpr int S = 32 / G;
+  uint64_t ka[S], va[S], kb[S], vb[S];
+  uint32_t na = node, nb = node;
+  uint32_t ca, cb;
+  for (;;) {
+    const size_t ra = (size_t)na * 32 + g * S, rb = (size_t)nb * 32 + g * S;
+    load_slots<S>(t.keys + ra, ka);
+    load_slots<S>(t.keys + rb, kb);
+    if ((level > 0 && !kChild) || (level == 0 && kLeafVals)) {
+      load_slots<S>(t.vals + ra, va);
+      load_slots<S>(t.vals + rb, vb);
+    }
+    if (g == G - 1) {
+      ka[S - 1] = kKeyMax;  // slot 31 holds the header
+      kb[S - 1] = kKeyMax;
+    }
+    uint32_t xa = 0, xb = 0;
+#pragma unroll
+    for (int i = 0; i < S; i++) {
+      xa += (ka[i] <= key_a) ? 1u : 0u;
+      xb += (kb[i] <= key_b) ? 1u : 0u;
+    }
+    ca = group_sum<G>(xa, gmask);
+    cb = group_sum<G>(xb, gmask);
+    if (level == 0) break;
+    if (kChild) {
+      const uint64_t* ca_p = t.vals + (size_t)na * 32 + ca;
+      const uint64_t* cb_p = t.vals + (size_t)nb * 32 + cb;
+      na = (uint32_t)__ldg(ca_p);
+      nb = (uint32_t)__ldg(cb_p);
+    } else {
+      const uint64_t ma = pick<S>(va, ca % S), mb = pick<S>(vb, cb % S);
+      na = (uint32_t)__shfl_sync(gmask, ma, ca / S, G);
+      nb = (uint32_t)__shfl_sync(gmask, mb, cb / S, G);
+    }
+    level--;
+  }
+  // leaf: find both slots, then issue both value loads together
+  const uint32_t sa = ca > 0 ? ca - 1 : 0, sb = cb > 0 ? cb - 1 : 0;
+  const uint64_t kka = __shfl_sync(gmask, pick<S>(ka, sa % S), sa / S, G);
+  const uint64_t kkb = __shfl_sync(gmask, pick<S>(kb, sb % S), sb / S, G);
+  const bool fa = ca > 0 && kka == key_a, fb = cb > 0 && kkb == key_b;
+  ans_a = 0;
+  ans_b = 0;
+  if (kLeafVals) {
+    const uint64_t xa = __shfl_sync(gmask, pick<S>(va, sa % S), sa / S, G);
+    const uint64_t xb = __shfl_sync(gmask, pick<S>(vb, sb % S), sb / S, G);
+    ans_a = fa ? xa : 0;
+    ans_b = fb ? xb : 0;
+  } else if (g == 0) {
+    if (fa) ans_a = __ldg(t.vals + (size_t)na * 32 + sa);
+    if (fb) ans_b = __ldg(t.vals + (size_t)nb * 32 + sb);
+  }
+  st_a = fa ? kFound : kAbsent;
+  st_b = fb ? kFound : kAbsent;
+}
+
 }  // namespace bt

@@ -68,9 +68,11 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* w
   return r;
 }
 
-__global__ void __launch_bounds__(kScanThreads) scan_reduce_kernel(const uint32_t* in, size_t n, uint32_t* sums) {
+__global__ void __launch_bounds__(kScanThreads) scan_reduce_kernel(const uint32_t* in, size_t n,
+                                                                   const uint32_t* n_dev, uint32_t* sums) {
   __shared__ uint32_t ws[32];
   __shared__ uint32_t tot;
+  if (n_dev) n = min(n, (size_t)*n_dev);
   size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanItems;
   uint32_t s = 0;
 #pragma unroll
@@ -107,9 +109,11 @@ __global__ void __launch_bounds__(kScanThreads) scan_single_kernel(uint32_t* dat
 }
 
 __global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(const uint32_t* in, uint32_t* out, size_t n,
-                                                                  const uint32_t* sums) {
+                                                                  const uint32_t* n_dev, const uint32_t* sums) {
   __shared__ uint32_t ws[32];
   __shared__ uint32_t tot;
+  if (n_dev) n = min(n, (size_t)*n_dev);
+  if ((size_t)blockIdx.x * kScanTile >= n) return;
   size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanItems;
   uint32_t v[kScanItems];
   uint32_t s = 0;
@@ -318,12 +322,12 @@ __global__ void copy_keys_kernel(const uint64_t* in, uint64_t* out, size_t n) {
 size_t scan_scratch_words(size_t n) { return (n + kScanTile - 1) / kScanTile + 1; }
 
 cudaError_t scan_exclusive_u32(const uint32_t* in, uint32_t* out, size_t n, uint32_t* total_dev, uint32_t* scratch,
-                               cudaStream_t s) {
+                               cudaStream_t s, const uint32_t* n_dev) {
   if (n == 0) {
     if (total_dev) return cudaMemsetAsync(total_dev, 0, sizeof(uint32_t), s);
     return cudaSuccess;
   }
-  if (n <= (size_t)kScanTile) {
+  if (n <= (size_t)kScanTile && !n_dev) {
     if (in != out) {
       cudaError_t e = cudaMemcpyAsync(out, in, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
       if (e != cudaSuccess) return e;
@@ -333,11 +337,11 @@ cudaError_t scan_exclusive_u32(const uint32_t* in, uint32_t* out, size_t n, uint
     return cudaGetLastError();
   }
   size_t nb = (n + kScanTile - 1) / kScanTile;
-  scan_reduce_kernel<<<(unsigned)nb, kScanThreads, 0, s>>>(in, n, scratch);
+  scan_reduce_kernel<<<(unsigned)nb, kScanThreads, 0, s>>>(in, n, n_dev, scratch);
   count_launch();
   scan_single_kernel<<<1, kScanThreads, 0, s>>>(scratch, nb, total_dev);
   count_launch();
-  scan_apply_kernel<<<(unsigned)nb, kScanThreads, 0, s>>>(in, out, n, scratch);
+  scan_apply_kernel<<<(unsigned)nb, kScanThreads, 0, s>>>(in, out, n, n_dev, scratch);
   count_launch();
   return cudaGetLastError();
 }

@@ -103,6 +103,13 @@ __device__ int commit_split(const DevTree& t, uint32_t node, uint64_t h, uint64_
   const uint64_t upk = __shfl_up_sync(kFull, pk, 1);
   const uint64_t upv = __shfl_up_sync(kFull, pv, 1);
   const bool new_root = (parent == kNil);
+  // an exhausted pool fails the split before any lock is taken, so readers of
+  // these nodes are not aborted by lock churn once nothing can grow
+  const uint32_t used = __shfl_sync(kFull, lane == 0 ? ld_relaxed32(&C->n_nodes) : 0u, 0);  // one value for the warp
+  if (used + (new_root ? 2u : 1u) > t.cap) {
+    if (lane == 0) atomicOr(&C->error, kErrCapacity);
+    return TX_NOCAP;
+  }
   if (!acquire_locks(t, node, h, parent, ph, new_root, rl)) return TX_ABORT;
   const uint32_t base = alloc_nodes(t, new_root ? 2u : 1u);
   if (base == kNil) {

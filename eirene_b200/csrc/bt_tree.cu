@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cuda_runtime.h>
 
+#include "bt_block.cuh"
 #include "bt_common.cuh"
 #include "bt_internal.h"
 #include "bt_search.cuh"
@@ -121,6 +122,53 @@ __global__ void __launch_bounds__(256) search_kernel(DevTree t, const uint64_t* 
     if (g == 0) {
       out_vals[r] = ans;
       out_st[r] = st;
+    }
+  }
+}
+
+// Two requests per group in lock step (group_descend2): requests q and
+// q + stride of the grid-stride loop share a group.
+template <int G, bool kLeafVals, bool kChild>
+__global__ void __launch_bounds__(256) search2_kernel(DevTree t, const uint64_t* __restrict__ qkeys,
+                                                      const uint32_t* __restrict__ list,
+                                                      const uint32_t* __restrict__ n_dev, size_t n_host,
+                                                      uint64_t* __restrict__ out_vals, uint8_t* __restrict__ out_st) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t g = lane % G;
+  const uint32_t gmask = group_mask<G>(lane);
+  const size_t n = n_dev ? (size_t)*n_dev : n_host;
+  const uint32_t root = t.ctrl->root;
+  const uint32_t root_level = t.ctrl->root_level;
+  const size_t groups = ((size_t)gridDim.x * blockDim.x) / G;
+  for (size_t q = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) / G; q < n; q += 2 * groups) {
+    const size_t q2 = q + groups;
+    const bool two = q2 < n;
+    const uint32_t ra = list ? __ldg(list + q) : (uint32_t)q;
+    const uint32_t rb = two ? (list ? __ldg(list + q2) : (uint32_t)q2) : ra;
+    const uint64_t key_a = __ldg(qkeys + ra);
+    const uint64_t key_b = __ldg(qkeys + rb);
+    uint8_t sa = kAbsent, sb = kAbsent;
+    uint64_t aa = 0, ab = 0;
+    if (root != kNil) {
+      // a reserved key descends as key 0 (keeping the pair in lock step) and is reported as rejected
+      group_descend2<G, kLeafVals, kChild>(t, root, root_level, key_a == kKeyMax ? 0 : key_a,
+                                   key_b == kKeyMax ? 0 : key_b, g, gmask, aa, sa, ab, sb);
+    }
+    if (key_a == kKeyMax) {
+      sa = kRejected;
+      aa = 0;
+    }
+    if (key_b == kKeyMax) {
+      sb = kRejected;
+      ab = 0;
+    }
+    if (g == 0) {
+      out_vals[ra] = aa;
+      out_st[ra] = sa;
+      if (two) {
+        out_vals[rb] = ab;
+        out_st[rb] = sb;
+      }
     }
   }
 }
@@ -262,7 +310,198 @@ __global__ void leaf_dump_kernel(DevTree t, const uint32_t* __restrict__ leaves,
 
 inline unsigned blocks_for(size_t n, int per) { return (unsigned)((n + per - 1) / per); }
 
+// ------------------------------------------------------------ top cache ----
+// The upper levels of the tree, copied into shared memory by every block of
+// the unsorted search: a request descends them there and continues from
+// global memory below.  Built per search launch by one block (breadth-first
+// from the root, whole levels while they fit kTopNodes, never the leaf
+// level), so it always matches the tree that the search reads.
+struct TopNode {
+  uint64_t keys[31];   // separators; unused slots hold kKeyMax
+  uint32_t child[32];  // next cached level: index into the cache; last cached level: node id
+  uint32_t pad[2];
+};
+static_assert(sizeof(TopNode) == 384, "TopNode layout");
+
+__global__ void __launch_bounds__(256) top_build_kernel(DevTree t, TopNode* __restrict__ top,
+                                                       TopInfo* __restrict__ info) {
+  __shared__ uint32_t ids[kTopNodes];
+  __shared__ uint32_t kids[kTopNodes];  // per node: index of its first child in ids
+  __shared__ uint32_t ws[32];
+  __shared__ uint32_t s_lvl_start, s_lvl_end, s_levels, s_stop;
+  const uint32_t root = t.ctrl->root;
+  const uint32_t rl = t.ctrl->root_level;
+  if (root == kNil || rl < 1) {
+    if (threadIdx.x == 0) info->n_levels = 0;
+    return;
+  }
+  if (threadIdx.x == 0) {
+    ids[0] = root;
+    s_lvl_start = 0;
+    s_lvl_end = 1;
+    s_levels = 1;
+    s_stop = 0;
+  }
+  __syncthreads();
+  // add whole levels while the next one is still an inner level and fits
+  for (uint32_t level = rl; level >= 2; level--) {
+    const uint32_t a = s_lvl_start, b = s_lvl_end;
+    uint32_t total = 0;
+    for (uint32_t base = a; base < b; base += blockDim.x) {
+      const uint32_t i = base + threadIdx.x;
+      const uint32_t c = i < b ? hdr_size(t.keys[(size_t)ids[i] * 32 + 31]) + 1 : 0u;
+      uint32_t tot;
+      const uint32_t ex = blk_exclusive_sum(c, ws, &tot);
+      if (i < b) kids[i] = b + total + ex;
+      total += tot;
+    }
+    __syncthreads();
+    if (b + total > (uint32_t)kTopNodes) break;  // uniform: every thread has the same total
+    for (uint32_t i = a + threadIdx.x / 32; i < b; i += blockDim.x / 32) {
+      const uint32_t lane = threadIdx.x & 31;
+      const uint32_t c = hdr_size(t.keys[(size_t)ids[i] * 32 + 31]) + 1;
+      if (lane < c) ids[kids[i] + lane] = (uint32_t)t.vals[(size_t)ids[i] * 32 + lane];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      s_lvl_start = b;
+      s_lvl_end = b + total;
+      s_levels++;
+    }
+    __syncthreads();
+  }
+  const uint32_t n_nodes = s_lvl_end, last = s_lvl_start, n_levels = s_levels;
+  // kids[] holds the child offsets of every level except the last cached one
+  for (uint32_t i = threadIdx.x / 32; i < n_nodes; i += blockDim.x / 32) {
+    const uint32_t lane = threadIdx.x & 31;
+    const size_t row = (size_t)ids[i] * 32;
+    const uint32_t c = hdr_size(t.keys[row + 31]) + 1;
+    if (lane < 31) top[i].keys[lane] = t.keys[row + lane];  // slots past the size hold kKeyMax
+    uint32_t ch = kNil;
+    if (lane < c) ch = i >= last ? (uint32_t)t.vals[row + lane] : kids[i] + lane;
+    top[i].child[lane] = ch;
+  }
+  if (threadIdx.x == 0) {
+    info->n_nodes = n_nodes;
+    info->n_levels = n_levels;
+    info->below_level = rl - n_levels;
+  }
+}
+
+template <int G, bool kLeafVals>
+__global__ void __launch_bounds__(512) search_top_kernel(DevTree t, const TopNode* __restrict__ top,
+                                                        const TopInfo* __restrict__ info,
+                                                        const uint64_t* __restrict__ qkeys,
+                                                        const uint32_t* __restrict__ list,
+                                                        const uint32_t* __restrict__ n_dev, size_t n_host,
+                                                        uint64_t* __restrict__ out_vals,
+                                                        uint8_t* __restrict__ out_st) {
+  constexpr int S = 32 / G;
+  extern __shared__ __align__(16) unsigned char top_raw[];
+  const TopNode* ts = reinterpret_cast<const TopNode*>(top_raw);
+  const uint32_t n_levels = info->n_levels;
+  const uint32_t n_nodes = n_levels ? info->n_nodes : 0;
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(top);
+    uint4* dst = reinterpret_cast<uint4*>(top_raw);
+    const uint32_t words = n_nodes * (uint32_t)(sizeof(TopNode) / 16);
+    for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+  }
+  __syncthreads();
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t g = lane % G;
+  const uint32_t gmask = group_mask<G>(lane);
+  const size_t n = n_dev ? (size_t)*n_dev : n_host;
+  const uint32_t root = t.ctrl->root;
+  const uint32_t root_level = t.ctrl->root_level;
+  const uint32_t below = info->below_level;
+  const size_t stride = ((size_t)gridDim.x * blockDim.x) / G;
+  for (size_t q = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) / G; q < n; q += stride) {
+    const uint32_t r = list ? __ldg(list + q) : (uint32_t)q;
+    const uint64_t key = __ldg(qkeys + r);
+    uint8_t st = kAbsent;
+    uint64_t ans = 0;
+    if (key == kKeyMax) {
+      st = kRejected;
+    } else if (root != kNil) {
+      uint32_t node = root, level = root_level;
+      if (n_levels) {
+        uint32_t idx = 0;
+        for (uint32_t l = 0; l < n_levels; l++) {
+          const TopNode& tn = ts[idx];
+          uint32_t c = 0;
+#pragma unroll
+          for (int i = 0; i < S; i++) {
+            const int slot = g * S + i;
+            c += (slot < 31 && tn.keys[slot] <= key) ? 1u : 0u;
+          }
+          c = group_sum<G>(c, gmask);
+          idx = tn.child[c];
+        }
+        node = idx;
+        level = below;
+      }
+      st = group_descend<G, kLeafVals>(t, node, level, key, g, gmask, ans);
+    }
+    if (g == 0) {
+      out_vals[r] = ans;
+      out_st[r] = st;
+    }
+  }
+}
+
 }  // namespace
+
+int top_alloc(Handle* h) {
+  if (h->top) return 0;
+  if (cudaMalloc(&h->top, (size_t)kTopNodes * sizeof(TopNode) + 64) != cudaSuccess) return -3;
+  h->top_info = reinterpret_cast<TopInfo*>(static_cast<char*>(h->top) + (size_t)kTopNodes * sizeof(TopNode));
+  return 0;
+}
+
+// unsorted search with the top levels in shared memory
+cudaError_t launch_search_top(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev,
+                              size_t n, uint64_t* out_vals, uint8_t* out_st, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  if (top_alloc(h) != 0) return cudaErrorMemoryAllocation;
+  TopNode* top = reinterpret_cast<TopNode*>(h->top);
+  top_build_kernel<<<1, 256, 0, s>>>(h->tree, top, h->top_info);
+  count_launch();
+  const int threads = 512;
+  const size_t smem = (size_t)kTopNodes * sizeof(TopNode);
+  const int G = h->search_group;
+  static int per_sm[64][5] = {};
+  const int gi = G == 4 ? 0 : G == 16 ? 2 : G == 32 ? 3 : G == -8 ? 4 : 1;
+  const void* kern;
+  switch (gi) {
+    case 0: kern = (const void*)search_top_kernel<4, false>; break;
+    case 2: kern = (const void*)search_top_kernel<16, false>; break;
+    case 3: kern = (const void*)search_top_kernel<32, false>; break;
+    case 4: kern = (const void*)search_top_kernel<8, true>; break;
+    default: kern = (const void*)search_top_kernel<8, false>; break;
+  }
+  const int dev = h->device;
+  int per = 1;
+  if (dev >= 0 && dev < 64 && per_sm[dev][gi]) {
+    per = per_sm[dev][gi];
+  } else {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+      return cudaErrorInvalidValue;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, threads, smem) != cudaSuccess || per < 1) per = 1;
+    if (dev >= 0 && dev < 64) per_sm[dev][gi] = per;
+  }
+  const int lanes = G < 0 ? -G : G;
+  size_t blocks = (n * (size_t)lanes + threads - 1) / threads;
+  const size_t cap = (size_t)h->sm_count * per;
+  if (blocks > cap) blocks = cap;
+  if (blocks == 0) blocks = 1;
+  DevTree tree = h->tree;
+  const TopInfo* info = h->top_info;
+  void* args[] = {&tree, &top, &info, (void*)&qkeys, (void*)&list, (void*)&n_dev, &n, &out_vals, &out_st};
+  cudaError_t e = cudaLaunchKernel(kern, dim3((unsigned)blocks), dim3(threads), args, smem, s);
+  count_launch();
+  return e;
+}
 
 cudaError_t tree_reset(Handle* h, cudaStream_t s) {
   h->epoch = (h->epoch % 0x7fffu) + 1;  // 1 .. 0x7fff; 0 marks never-written rows
@@ -438,6 +677,23 @@ cudaError_t launch_search_sorted(Handle* h, const uint64_t* qkeys, const uint32_
 cudaError_t launch_search(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev, size_t n,
                           uint64_t* out_vals, uint8_t* out_st, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
+  if (h->search_pairs && (h->search_group == 8 || h->search_group == 4 || h->search_group == 16)) {
+    const int threads = 256;
+    const int G = h->search_group;
+    size_t blocks = ((n + 1) / 2 * (size_t)G + threads - 1) / threads;
+    const size_t cap = (size_t)h->sm_count * 8 * 4;
+    if (blocks > cap) blocks = cap;
+    if (blocks == 0) blocks = 1;
+#define BT_S2(GG, CC) search2_kernel<GG, false, CC><<<(unsigned)blocks, threads, 0, s>>>(h->tree, qkeys, list, n_dev, n, out_vals, out_st)
+    const bool child = h->search_pairs == 2;
+    if (G == 4) { if (child) BT_S2(4, true); else BT_S2(4, false); }
+    else if (G == 16) { if (child) BT_S2(16, true); else BT_S2(16, false); }
+    else { if (child) BT_S2(8, true); else BT_S2(8, false); }
+#undef BT_S2
+    count_launch();
+    return cudaGetLastError();
+  }
+  if (h->top_cache) return launch_search_top(h, qkeys, list, n_dev, n, out_vals, out_st, s);
   const int threads = 256;
   const int G = h->search_group;
   // enough groups to cover the requests, capped at a few waves of resident blocks

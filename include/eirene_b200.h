@@ -189,6 +189,12 @@ int bt_set_search_group(bt_handle *h, uint32_t lanes);
                                 * has an INSERT at or before them in the batch are sorted and merged, the rest
                                 * are unsorted lookups of the pre-batch tree; 0 sort the whole batch (the
                                 * reference's layout, v38 bpt-gpustm-kernel.cu:289-324).  Same answers. */
+#define BT_OPT_TOP_CACHE 7     /* 1 (default): unsorted plain searches descend the tree's upper levels (up to
+                                * 256 nodes) from a per-launch copy in shared memory; 0 all from global */
+#define BT_OPT_SEARCH_PAIRS 8  /* unsorted plain searches: 2 (default) two requests per lane group in lock step,
+                                * loading only the chosen child id at inner levels (half the bytes of a full
+                                * row, one more dependent load); 1 the pairs with full rows; 0 one request
+                                * per group.  Nonzero takes precedence over BT_OPT_TOP_CACHE */
 int bt_set_option(bt_handle *h, int option, int64_t value);
 /* Autotuner: times the lookup configurations on this tree with n sample keys
  * (device pointer, n <= max_batch) and keeps the fastest: lanes per request of

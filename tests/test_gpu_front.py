@@ -83,3 +83,45 @@ def test_zipf_hot_keys_both_front_ends_agree(gpu):
         gk, gv = dump(t)
         ok, ov = o.dump()
         assert (gk == ok).all() and (gv == ov).all()
+
+
+@pytest.mark.parametrize("fills", [(24, 24), (16, 16)])
+def test_search_top_cache_matches_global_descent(gpu, fills):
+    # a taller tree (fill 16) has more cached levels; inserts between the
+    # searches split nodes of the cached levels, and the cache is rebuilt
+    keys = O.gen_keys("uniform", 70, 400_000)
+    vals = O.value_of(keys)
+    t = E.BTree(max_keys=1 << 22, max_batch=1 << 18, leaf_fill=fills[0], inner_fill=fills[1])
+    t.bulk_build(dev(keys), dev(vals))
+    o = O.OracleTree()
+    o.bulk_build(keys, vals)
+    for b in range(3):
+        qk, _, _ = O.gen_requests("uniform", 80 + b, o.dump()[0], 150_000, 100)
+        qk[:3] = [0, 2**64 - 1, 1]
+        ov, os_ = o.execute_merged(qk, np.zeros_like(qk), np.ones(qk.size, np.uint8))
+        for lanes in (4, 8, 16, 32):
+            t.set_search_group(lanes)
+            for cache in (1, 0):
+                t.set_option(E.OPT_TOP_CACHE, cache)
+                gv, gs = run_batch(t, qk, np.zeros_like(qk), np.ones(qk.size, np.uint8), E.MODE_SORTED)
+                assert (gs == os_).all() and (gv == ov).all(), (b, lanes, cache)
+        t.set_option(E.OPT_TOP_CACHE, 1)
+        rk, rv, ro = O.gen_requests("uniform", 90 + b, keys, 200_000, 0)
+        check(t, o, rk, rv, ro, E.MODE_SORTED | E.MODE_MERGE_ENGINE)
+    assert t.stats()["inner_splits"] > 0
+
+
+def test_unaligned_op_array_and_subranges(gpu):
+    # op codes at an odd byte offset (a slice of a larger array): the front end
+    # reads them one byte at a time
+    import torch
+
+    t, o, keys = pair(50_000, 5)
+    rk, rv, ro = O.gen_requests("uniform", 95, keys, 30_001, 60)
+    ov, os_ = o.execute_merged(rk, rv, ro)
+    big = torch.from_numpy(np.concatenate([[7], ro]).astype(np.uint8)).cuda()
+    gv = torch.zeros(rk.size, dtype=torch.int64, device="cuda")
+    gs = torch.zeros(rk.size, dtype=torch.uint8, device="cuda")
+    t.execute(dev(rk), dev(rv), big[1:], gv, gs, mode=E.MODE_SORTED)
+    torch.cuda.synchronize()
+    assert (gs.cpu().numpy() == os_).all() and (gv.cpu().numpy().view(np.uint64) == ov).all()
