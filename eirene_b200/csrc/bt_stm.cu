@@ -28,30 +28,33 @@ enum : int { TX_DONE = 0, TX_ABORT = 1, TX_AGAIN = 2, TX_NOCAP = 3 };
 __device__ __forceinline__ uint64_t* hdr_ptr(const DevTree& t, uint32_t n) { return t.keys + (size_t)n * 32 + 31; }
 
 // Lock node n1 (expected header h1), node n2 (h2) and/or the root lock (rl).
-// Lanes 0, 1, 2 each take one; on any failure the taken ones are restored.
+// One lane takes them one after the other in a fixed order -- root lock, then
+// the parent n2, then the node n1 -- and stops at the first that fails,
+// restoring what it took.  Taking them in parallel let two transactions
+// each hold one of a pair and fail each other again and again (observed: a
+// second-long livelock of warps splitting the same inner node); in a fixed
+// order whoever gets the first lock can go on to take the rest.
 __device__ bool acquire_locks(const DevTree& t, uint32_t n1, uint64_t h1, uint32_t n2, uint64_t h2, bool lock_root,
                               uint32_t rl) {
-  const uint32_t lane = lane_id();
-  bool ok = true, got = false;
-  if (lane == 0 && n1 != kNil) {
-    got = atomicCAS((unsigned long long*)hdr_ptr(t, n1), h1, hdr_lock(h1)) == h1;
-    ok = got;
-  } else if (lane == 1 && n2 != kNil) {
-    got = atomicCAS((unsigned long long*)hdr_ptr(t, n2), h2, hdr_lock(h2)) == h2;
-    ok = got;
-  } else if (lane == 2 && lock_root) {
-    got = atomicCAS(&t.ctrl->root_lock, rl, rl | 1u) == rl;
-    ok = got;
-  }
-  if (!__all_sync(kFull, ok)) {
-    if (got) {  // nothing was written: put the same version back
-      if (lane == 0) st_release(hdr_ptr(t, n1), h1);
-      else if (lane == 1) st_release(hdr_ptr(t, n2), h2);
-      else st_release32(&t.ctrl->root_lock, rl);
+  int ok = 1;
+  if (lane_id() == 0) {
+    bool got_root = false, got_n2 = false;
+    if (lock_root) {
+      got_root = atomicCAS(&t.ctrl->root_lock, rl, rl | 1u) == rl;
+      ok = got_root;
     }
-    __syncwarp();
-    return false;
+    if (ok && n2 != kNil) {
+      got_n2 = atomicCAS((unsigned long long*)hdr_ptr(t, n2), h2, hdr_lock(h2)) == h2;
+      ok = got_n2;
+    }
+    if (ok && n1 != kNil) ok = atomicCAS((unsigned long long*)hdr_ptr(t, n1), h1, hdr_lock(h1)) == h1;
+    if (!ok) {  // nothing was written: put the same versions back
+      if (got_n2) st_release(hdr_ptr(t, n2), h2);
+      if (got_root) st_release32(&t.ctrl->root_lock, rl);
+    }
   }
+  ok = __shfl_sync(kFull, ok, 0);
+  if (!ok) return false;
   __threadfence();
   return true;
 }
@@ -545,7 +548,12 @@ __device__ __forceinline__ void run_request(const DevTree& t, const uint32_t epo
     }
     cnt.aborts++;
     fails++;
-    if (fails > 2) __nanosleep(32u << (fails < 8 ? fails : 8));
+    if (fails > 2) {
+      // exponential backoff with a per-warp, per-attempt jitter so that
+      // colliding warps do not retry in step
+      const uint32_t jit = (uint32_t)(((key * 0x9E3779B97F4A7C15ull) >> 40) ^ (attempts * 0x85EBCA6Bu)) & 1023u;
+      __nanosleep((32u << (fails < 8 ? fails : 8)) + jit);
+    }
   }
 }
 

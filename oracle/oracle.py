@@ -115,7 +115,10 @@ class OracleTree:
 
     def __del__(self):
         if getattr(self, "_h", None):
-            lib().bto_destroy(self._h)
+            try:
+                lib().bto_destroy(self._h)
+            except Exception:  # interpreter shutdown: the module globals are gone
+                pass
             self._h = None
 
     def bulk_build(self, keys, vals):
