@@ -520,11 +520,16 @@ def main():
     dom_ms = ph[dom] / max(1, ph["batches"])
     dom_bytes = alg.get(dom)
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", f"traffic_{dom}.json")
+    # DRAM bytes per unit of the dominant kernel from an ncu capture, kept as a
+    # "bytes_per_unit: N" line in profiles/traffic_<phase>.md
+    tpath = os.path.join(ROOT, "profiles", f"traffic_{dom}.md")
     if os.path.exists(tpath):
         try:
-            t = json.load(open(tpath))
-            traffic = t.get("bytes_per_unit", 0) * (n_get if dom == "search" else n_ins if dom == "insert" else n_b)
+            import re
+
+            m = re.search(r"bytes_per_unit:\s*([0-9.]+)", open(tpath).read())
+            if m:
+                traffic = float(m.group(1)) * (n_get if dom == "search" else n_ins if dom == "insert" else n_b)
         except Exception:
             traffic = None
     roof = None
