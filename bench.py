@@ -227,7 +227,7 @@ def run_reference(args):
 
 
 # ----------------------------------------------------------------------------
-def serve_bench(E, np, tree, tk_host, n_tree, seconds=1.5, seed=5):
+def serve_bench(E, np, tree, tk_host, n_tree, seconds=1.5, seed=5, load=0.5):
     """Serving loop (continuous batching): batch sizes log-uniform over
     2^10..2^22, per-batch search fraction uniform in [0.5, 1], Poisson arrivals.
     Phase 1 submits as fast as admission allows (capacity); phase 2 offers 50 %
@@ -266,19 +266,20 @@ def serve_bench(E, np, tree, tk_host, n_tree, seconds=1.5, seed=5):
         pending = []
         next_t = t0
         n_sub = 0
+        b = draw()
         while True:
             now = time.perf_counter()
             if now - t0 > duration:
                 break
             if rate is None or now >= next_t:
-                b = draw()
                 tk = srv.submit(*b)
-                if tk is None:
+                if tk is None:  # admission full: wait for the oldest, then retry the same batch
                     if pending:
                         srv.wait(pending.pop(0))
                     continue
                 pending.append(tk)
                 n_sub += 1
+                b = draw()
                 if rate is not None:
                     next_t += rng.exponential(1.0 / rate)
             else:
@@ -291,7 +292,7 @@ def serve_bench(E, np, tree, tk_host, n_tree, seconds=1.5, seed=5):
 
     cap, _ = run(seconds, None)
     mean_batch = (2.0 ** 22 - 2.0 ** 10) / np.log(2.0 ** 12)  # mean of the log-uniform size law
-    rate = 0.5 * cap["mops"] * 1e6 / mean_batch
+    rate = load * cap["mops"] * 1e6 / mean_batch
     lat, n_sub = run(seconds, rate)
     srv.stop()
     return {"capacity_mops": cap["mops"], "capacity_batches": cap["batches"],

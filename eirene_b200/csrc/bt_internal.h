@@ -219,6 +219,7 @@ struct ServeDev {
   unsigned long long* host_tend;    // [cap] mapped host memory: device clock at completion
   uint32_t cap;
   unsigned long long idle_ns;
+  unsigned long long* last_busy;  // device clock of the latest claim of work by any warp
 };
 cudaError_t launch_serve(Handle* h, const ServeDev& S, cudaStream_t s);
 

@@ -13,7 +13,11 @@
 //               mapped host memory; the host then copies the answers out on a
 //               second stream and retires slots and arena space in order.
 // The kernel exits after idle_us without work; any host call that finds work
-// in flight and the kernel gone relaunches the graph.
+// in flight and the kernel gone relaunches the graph.  Everything on the copy
+// stream is a copy (the slot counters are reset from a pinned zero word, not
+// by a memset kernel): the persistent kernel holds the SMs, so a kernel queued
+// on the copy stream would not start until blocks of it idle out, and a batch
+// would not be published before that.
 #include <algorithm>
 #include <chrono>
 #include <cstring>
@@ -65,6 +69,7 @@ struct bt_server {
   uint32_t* st_tail = nullptr;
   unsigned long long* st_claim = nullptr;
   uint32_t* st_stop = nullptr;
+  uint32_t* st_zero = nullptr;  // pinned zero word: counters are reset by the copy engine
   uint32_t cap = 0;
   std::vector<Slot> slots;
   uint32_t next_seq = 0, retire_seq = 0;
@@ -203,6 +208,7 @@ int bt_serve_start(bt_handle* H, const bt_serve_config* cfg_in, bt_server** out)
             cudaMallocHost(&S->st_tail, S->cap * 4) == cudaSuccess &&
             cudaMallocHost(&S->st_claim, S->cap * 8) == cudaSuccess &&
             cudaMallocHost(&S->st_stop, 64) == cudaSuccess &&
+            cudaMallocHost(&S->st_zero, 64) == cudaSuccess &&
             cudaEventCreateWithFlags(&S->k_ev, cudaEventDisableTiming) == cudaSuccess;
   for (uint32_t i = 0; ok && i < S->cap; i++)
     ok = cudaEventCreateWithFlags(&S->slots[i].out_ev, cudaEventDisableTiming) == cudaSuccess;
@@ -210,6 +216,7 @@ int bt_serve_start(bt_handle* H, const bt_serve_config* cfg_in, bt_server** out)
     S->d_cursor = S->d_tail + 16;
     S->d_stop = S->d_tail + 32;
     std::memset(S->h_done, 0xFF, S->cap * 4);
+    std::memset(S->st_zero, 0, 64);
     ok = cudaMemset(S->d_tail, 0, 256) == cudaSuccess &&
          cudaMemset(S->d_claimed, 0xFF, S->cap * sizeof(unsigned long long)) == cudaSuccess &&
          cudaMemset(S->d_done, 0, S->cap * 4) == cudaSuccess;
@@ -230,6 +237,7 @@ int bt_serve_start(bt_handle* H, const bt_serve_config* cfg_in, bt_server** out)
     D.host_tend = h_tend_dev;
     D.cap = S->cap;
     D.idle_ns = (unsigned long long)(cfg.idle_us ? cfg.idle_us : 2000) * 1000ull;
+    D.last_busy = reinterpret_cast<unsigned long long*>(S->d_tail + 48);
     // the persistent kernel, captured once and relaunched as a graph
     ok = cudaStreamBeginCapture(S->s_k, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
     if (ok) {
@@ -286,7 +294,7 @@ int bt_submit(bt_server* S, const uint64_t* keys, const uint64_t* vals, const ui
               cudaMemcpyAsync(dops, ops, n, cudaMemcpyHostToDevice, S->s_in) == cudaSuccess &&
               cudaMemcpyAsync(S->d_claimed + slot, &S->st_claim[slot], 8, cudaMemcpyHostToDevice, S->s_in) ==
                   cudaSuccess &&
-              cudaMemsetAsync(S->d_done + slot, 0, 4, S->s_in) == cudaSuccess &&
+              cudaMemcpyAsync(S->d_done + slot, S->st_zero, 4, cudaMemcpyHostToDevice, S->s_in) == cudaSuccess &&
               cudaMemcpyAsync(S->d_desc + slot, &d, sizeof(d), cudaMemcpyHostToDevice, S->s_in) == cudaSuccess &&
               cudaMemcpyAsync(S->d_tail, &S->st_tail[slot], 4, cudaMemcpyHostToDevice, S->s_in) == cudaSuccess;
     if (!ok) {
@@ -397,6 +405,7 @@ int bt_serve_stop(bt_server* S) {
   if (S->st_tail) cudaFreeHost(S->st_tail);
   if (S->st_claim) cudaFreeHost(S->st_claim);
   if (S->st_stop) cudaFreeHost(S->st_stop);
+  if (S->st_zero) cudaFreeHost(S->st_zero);
   if (S->s_in) cudaStreamDestroy(S->s_in);
   if (S->s_out) cudaStreamDestroy(S->s_out);
   if (S->s_k) cudaStreamDestroy(S->s_k);

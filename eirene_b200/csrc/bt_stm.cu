@@ -634,7 +634,13 @@ __global__ void __launch_bounds__(256, 4) serve_kernel(DevTree t, ServeDev S, ui
   const LearnedDev* M = use_learned ? &lm : nullptr;
   TxCounters cnt;
   const uint32_t epoch = t.ctrl->epoch;
-  unsigned long long idle_since = 0;
+  // Idle exit is decided on the whole kernel's activity, not the warp's own:
+  // a warp that slept through a small batch claimed by others must not count
+  // that time as idle, or warps would leave one by one while work keeps
+  // coming and the grid would dwindle (the host relaunches only when the
+  // whole kernel has ended).
+  const unsigned long long t_start = global_ns();
+  unsigned long long my_mark = 0;
   for (;;) {
     uint32_t cur = 0, tail = 0, stop = 0;
     if (lane == 0) {
@@ -646,14 +652,25 @@ __global__ void __launch_bounds__(256, 4) serve_kernel(DevTree t, ServeDev S, ui
     tail = __shfl_sync(kFull, tail, 0);
     stop = __shfl_sync(kFull, stop, 0);
     if (cur >= tail) {
-      const unsigned long long now = global_ns();
       if (stop) break;
-      if (idle_since == 0) idle_since = now;
-      else if (now - idle_since > S.idle_ns) break;
+      int leave = 0;
+      if (lane == 0) {
+        const unsigned long long now = global_ns();
+        unsigned long long busy = ld_relaxed(reinterpret_cast<const uint64_t*>(S.last_busy));
+        if (busy < t_start) busy = t_start;
+        leave = now - busy > S.idle_ns;
+      }
+      if (__shfl_sync(kFull, leave, 0)) break;
       __nanosleep(2000);
       continue;
     }
-    idle_since = 0;
+    if (lane == 0) {
+      const unsigned long long now = global_ns();
+      if (now - my_mark > 20000) {  // publish activity at most every 20 us per warp
+        my_mark = now;
+        atomicMax(S.last_busy, now);
+      }
+    }
     const uint32_t slot = cur % S.cap;
     // Claim kServeChunk requests with one atomicAdd on the slot's word
     // (batch seq << 32 | requests claimed); every claim succeeds, so thousands
