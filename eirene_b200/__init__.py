@@ -27,6 +27,7 @@ ERRORS = {
     -8: "more keys than BT_STATIC_BUILD_MAX_KEYS",
     -9: "no free slot or arena space",
     -10: "timed out",
+    -11: "snapshot file error",
 }
 STATIC_BUILD_MAX_KEYS = 65536
 OP_INSERT, OP_GET = 0, 1
@@ -98,7 +99,7 @@ EXPORTS = [
     "bt_profile", "bt_profile_read", "bt_launch_count", "bt_bulk_build_static",
     "bt_set_learned_group", "bt_learned_info", "bt_mlp_grad", "bt_set_option", "bt_autotune",
     "bt_serve_config_init", "bt_serve_start", "bt_submit", "bt_poll", "bt_wait", "bt_serve_get_stats", "bt_serve_stop",
-    "bt_route_batch", "bt_unroute_results",
+    "bt_route_batch", "bt_unroute_results", "bt_save", "bt_load",
 ]
 MAX_SHARDS = 256
 OPT_SORTED_SEARCH, OPT_RETRY_LIMIT, OPT_TRAIN_STEPS, OPT_SORTED_LEAF_VALS, OPT_BATCH_DESCENT = 1, 2, 3, 4, 5
@@ -173,6 +174,8 @@ def lib():
             "bt_serve_stop": [_P],
             "bt_route_batch": [_P, _P, ctypes.c_int, _P, _P, _P, _SZ, _P, _P, _P, _P, _P, _P],
             "bt_unroute_results": [_P, _P, _P, _P, _SZ, _P, _P, _P],
+            "bt_save": [_P, ctypes.c_char_p],
+            "bt_load": [_P, ctypes.c_char_p],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -369,6 +372,14 @@ class BTree:
         """Scatter answers in routed order back to input order (bt_unroute_results)."""
         _check(lib().bt_unroute_results(self._h, _ptr(perm), _ptr(in_vals), _ptr(in_status), perm.numel(),
                                         _ptr(out_vals), _ptr(out_status), _stream_ptr(stream)), "bt_unroute_results")
+
+    def save(self, path: str):
+        """Write the tree's sorted pairs to a snapshot file (bt_save)."""
+        _check(lib().bt_save(self._h, os.fsencode(path)), "bt_save")
+
+    def load(self, path: str):
+        """Replace the contents with a snapshot file (bt_load; a fresh bulk load)."""
+        _check(lib().bt_load(self._h, os.fsencode(path)), "bt_load")
 
     def set_search_group(self, lanes: int):
         _check(lib().bt_set_search_group(self._h, lanes), "bt_set_search_group")

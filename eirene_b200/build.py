@@ -29,6 +29,7 @@ SOURCES = [
     "bt_serve.cu",
     "bt_shard.cu",
     "bt_front.cu",
+    "bt_snapshot.cu",
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

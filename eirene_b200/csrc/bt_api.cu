@@ -501,6 +501,7 @@ const char* bt_status_string(int code) {
     case BT_ERR_STATIC_LIMIT: return "more keys than BT_STATIC_BUILD_MAX_KEYS";
     case BT_ERR_BUSY: return "no free slot or arena space";
     case BT_ERR_TIMEOUT: return "timed out";
+    case BT_ERR_IO: return "snapshot file error";
     default: return "unknown status";
   }
 }

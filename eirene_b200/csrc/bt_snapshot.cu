@@ -1,0 +1,133 @@
+// Snapshot of a tree's contents to a file and back (checkpoint / resume).
+// The reference has no counterpart: its tree lives only as long as the
+// process (src/gpu-stm-tree-v39/bpt-gpustm.h:145).
+//
+// The snapshot is logical: the sorted (key, value) pairs, not the node pool.
+// Loading bulk-builds them with the loading handle's fill settings, so the
+// loaded tree has the same contents and answers every request the same way,
+// but its leaf layout is a fresh bulk load, not the saved one.
+//
+// File layout (little endian):
+//   0   8 B  magic "EIRB2SNP"
+//   8   4 B  format version (1)
+//   12  4 B  0
+//   16  8 B  n, the number of pairs
+//   24  8 B  FNV-1a 64 over the key and value arrays
+//   32  8n B keys, ascending
+//   ... 8n B values
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/eirene_b200.h"
+#include "bt_internal.h"
+
+namespace {
+
+constexpr char kMagic[8] = {'E', 'I', 'R', 'B', '2', 'S', 'N', 'P'};
+constexpr uint32_t kVersion = 1;
+
+uint64_t fnv1a(const void* p, size_t bytes, uint64_t h) {
+  const unsigned char* b = static_cast<const unsigned char*>(p);
+  for (size_t i = 0; i < bytes; i++) {
+    h ^= b[i];
+    h *= 0x100000001B3ull;
+  }
+  return h;
+}
+
+struct DevBuf {
+  void* p = nullptr;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+int bt_save(bt_handle* h, const char* path) {
+  if (!h || !path) return BT_ERR_INVALID_ARG;
+  uint64_t n = 0;
+  int rc = bt_size(h, &n);
+  if (rc != BT_OK) return rc;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(h->h.device);
+  std::vector<uint64_t> keys(n), vals(n);
+  if (n) {
+    DevBuf dk, dv;  // freed with the handle's device current
+    size_t got = 0;
+    if (cudaMalloc(&dk.p, n * 8) != cudaSuccess || cudaMalloc(&dv.p, n * 8) != cudaSuccess) rc = BT_ERR_NO_MEMORY;
+    if (rc == BT_OK) rc = bt_dump_sorted(h, (uint64_t*)dk.p, (uint64_t*)dv.p, n, &got, nullptr);
+    if (rc == BT_OK && got != n) rc = BT_ERR_CUDA;
+    if (rc == BT_OK && (cudaMemcpy(keys.data(), dk.p, n * 8, cudaMemcpyDeviceToHost) != cudaSuccess ||
+                        cudaMemcpy(vals.data(), dv.p, n * 8, cudaMemcpyDeviceToHost) != cudaSuccess))
+      rc = BT_ERR_CUDA;
+  }
+  if (prev >= 0) cudaSetDevice(prev);
+  if (rc != BT_OK) return rc;
+  uint64_t sum = fnv1a(keys.data(), n * 8, 0xCBF29CE484222325ull);
+  sum = fnv1a(vals.data(), n * 8, sum);
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return BT_ERR_IO;
+  const uint32_t ver[2] = {kVersion, 0};
+  bool ok = std::fwrite(kMagic, 1, 8, f) == 8 && std::fwrite(ver, 4, 2, f) == 2 && std::fwrite(&n, 8, 1, f) == 1 &&
+            std::fwrite(&sum, 8, 1, f) == 1 && (n == 0 || (std::fwrite(keys.data(), 8, n, f) == n &&
+                                                           std::fwrite(vals.data(), 8, n, f) == n));
+  ok = (std::fclose(f) == 0) && ok;
+  return ok ? BT_OK : BT_ERR_IO;
+}
+
+int bt_load(bt_handle* h, const char* path) {
+  if (!h || !path) return BT_ERR_INVALID_ARG;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return BT_ERR_IO;
+  char magic[8];
+  uint32_t ver[2];
+  uint64_t n = 0, sum = 0;
+  bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, kMagic, 8) == 0 && std::fread(ver, 4, 2, f) == 2 &&
+            ver[0] == kVersion && std::fread(&n, 8, 1, f) == 1 && std::fread(&sum, 8, 1, f) == 1;
+  // the pairs must fit the file that holds them
+  long here = ok ? std::ftell(f) : -1;
+  if (ok && std::fseek(f, 0, SEEK_END) == 0) {
+    const long end = std::ftell(f);
+    ok = here >= 0 && end >= here && (uint64_t)(end - here) == n * 16 && std::fseek(f, here, SEEK_SET) == 0;
+  } else {
+    ok = false;
+  }
+  std::vector<uint64_t> keys, vals;
+  if (ok) {
+    keys.resize(n);
+    vals.resize(n);
+    ok = n == 0 || (std::fread(keys.data(), 8, n, f) == n && std::fread(vals.data(), 8, n, f) == n);
+  }
+  std::fclose(f);
+  if (!ok) return BT_ERR_IO;
+  uint64_t chk = fnv1a(keys.data(), n * 8, 0xCBF29CE484222325ull);
+  chk = fnv1a(vals.data(), n * 8, chk);
+  if (chk != sum) return BT_ERR_IO;
+  for (uint64_t i = 1; i < n; i++)
+    if (keys[i] <= keys[i - 1]) return BT_ERR_IO;  // not strictly ascending: not a snapshot of a tree
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(h->h.device);
+  int rc = BT_OK;
+  {
+    DevBuf dk, dv;  // freed with the handle's device current
+    if (n && (cudaMalloc(&dk.p, n * 8) != cudaSuccess || cudaMalloc(&dv.p, n * 8) != cudaSuccess))
+      rc = BT_ERR_NO_MEMORY;
+    if (rc == BT_OK && n &&
+        (cudaMemcpy(dk.p, keys.data(), n * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+         cudaMemcpy(dv.p, vals.data(), n * 8, cudaMemcpyHostToDevice) != cudaSuccess))
+      rc = BT_ERR_CUDA;
+    if (rc == BT_OK) rc = bt_bulk_build(h, (const uint64_t*)dk.p, (const uint64_t*)dv.p, n, nullptr);
+  }
+  if (prev >= 0) cudaSetDevice(prev);
+  return rc;
+}
+
+}  // extern "C"

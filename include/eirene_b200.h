@@ -43,6 +43,7 @@ extern "C" {
 #define BT_ERR_STATIC_LIMIT -8    /* n > BT_STATIC_BUILD_MAX_KEYS in bt_bulk_build_static */
 #define BT_ERR_BUSY -9            /* serving: no free slot or arena space now; retry after a completion */
 #define BT_ERR_TIMEOUT -10        /* serving: bt_wait ran out of time */
+#define BT_ERR_IO -11             /* snapshot file: cannot open / read / write, or not a valid snapshot */
 
 /* ---- request op codes (same numbering as src/input-helper.h:14-17) ---- */
 #define BT_OP_INSERT 0
@@ -305,6 +306,16 @@ int bt_route_batch(bt_handle *h, const uint64_t *splitters, int n_shards, const 
                    uint8_t *out_ops, uint32_t *out_perm, uint64_t *out_counts, void *stream);
 int bt_unroute_results(bt_handle *h, const uint32_t *perm, const uint64_t *in_vals, const uint8_t *in_status,
                        size_t n, uint64_t *out_vals, uint8_t *out_status, void *stream);
+
+/* ---- snapshot (checkpoint / resume) ----
+ * No counterpart in the reference, whose tree lives only as long as the
+ * process (src/gpu-stm-tree-v39/bpt-gpustm.h:145).  bt_save writes the sorted
+ * (key, value) pairs and a checksum to `path`; bt_load replaces h's contents
+ * with a saved file by a bulk build (same contents and answers; the leaf
+ * layout is a fresh bulk load with h's fill settings).  Both synchronous;
+ * BT_ERR_IO for file errors, a bad magic, size, checksum or key order. */
+int bt_save(bt_handle *h, const char *path);
+int bt_load(bt_handle *h, const char *path);
 
 /* Static text for a status code. */
 const char *bt_status_string(int code);

@@ -1,0 +1,63 @@
+"""Snapshot save/load (bt_save / bt_load): a tree changed by batches is saved,
+loaded into a fresh handle and must hold the same pairs and answer a new
+batch exactly like the oracle; damaged files are refused with BT_ERR_IO."""
+import os
+
+import numpy as np
+import pytest
+
+import eirene_b200 as E
+from oracle import oracle as O
+from tests.helpers import dev, dump, run_batch
+
+pytestmark = pytest.mark.gpu
+
+
+def test_save_load_round_trip(gpu, tmp_path):
+    keys = O.gen_keys("zipf", 41, 120_000)
+    vals = O.value_of(keys)
+    t = E.BTree(max_keys=1 << 20, max_batch=1 << 17)
+    t.bulk_build(dev(keys), dev(vals))
+    o = O.OracleTree()
+    o.bulk_build(keys, vals)
+    for b in range(3):
+        rk, rv, ro = O.gen_requests("zipf", 42 + b, keys, 60_000, 60)
+        o.execute_merged(rk, rv, ro)
+        run_batch(t, rk, rv, ro, E.MODE_SORTED | E.MODE_MERGE_ENGINE)
+    path = str(tmp_path / "tree.snap")
+    t.save(path)
+    assert os.path.getsize(path) == 32 + 16 * t.size()
+    t2 = E.BTree(max_keys=1 << 20, max_batch=1 << 17, leaf_fill=20)
+    t2.load(path)
+    gk, gv = dump(t2)
+    ok, ov = o.dump()
+    assert (gk == ok).all() and (gv == ov).all()
+    rk, rv, ro = O.gen_requests("zipf", 50, ok, 50_000, 70)
+    ov2, os2 = o.execute_merged(rk, rv, ro)
+    gv2, gs2 = run_batch(t2, rk, rv, ro, E.MODE_SORTED)
+    assert (gs2 == os2).all() and (gv2 == ov2).all()
+
+
+def test_empty_tree_and_damaged_files(gpu, tmp_path):
+    t = E.BTree(max_keys=1 << 16, max_batch=1 << 12)
+    p = str(tmp_path / "empty.snap")
+    t.save(p)
+    t.load(p)
+    assert t.size() == 0
+    keys = O.gen_keys("uniform", 3, 1000)
+    t.bulk_build(dev(keys), dev(O.value_of(keys)))
+    good = str(tmp_path / "good.snap")
+    t.save(good)
+    raw = bytearray(open(good, "rb").read())
+    cases = {"truncated": raw[:-8], "flipped": raw[:40] + bytes([raw[40] ^ 1]) + raw[41:], "magic": b"X" + raw[1:]}
+    for name, data in cases.items():
+        bad = str(tmp_path / f"{name}.snap")
+        open(bad, "wb").write(bytes(data))
+        with pytest.raises(E.BTError) as ei:
+            t.load(bad)
+        assert ei.value.code == -11, name
+    with pytest.raises(E.BTError) as ei:
+        t.load(str(tmp_path / "missing.snap"))
+    assert ei.value.code == -11
+    # a failed load leaves the tree as it was
+    assert t.size() == 1000
