@@ -99,7 +99,7 @@ EXPORTS = [
     "bt_profile", "bt_profile_read", "bt_launch_count", "bt_bulk_build_static",
     "bt_set_learned_group", "bt_learned_info", "bt_mlp_grad", "bt_set_option", "bt_autotune",
     "bt_serve_config_init", "bt_serve_start", "bt_submit", "bt_poll", "bt_wait", "bt_serve_get_stats", "bt_serve_stop",
-    "bt_route_batch", "bt_unroute_results", "bt_save", "bt_load",
+    "bt_route_batch", "bt_unroute_results", "bt_save", "bt_load", "bt_range_batch",
 ]
 MAX_SHARDS = 256
 OPT_SORTED_SEARCH, OPT_RETRY_LIMIT, OPT_TRAIN_STEPS, OPT_SORTED_LEAF_VALS, OPT_BATCH_DESCENT = 1, 2, 3, 4, 5
@@ -175,6 +175,7 @@ def lib():
             "bt_route_batch": [_P, _P, ctypes.c_int, _P, _P, _P, _SZ, _P, _P, _P, _P, _P, _P],
             "bt_unroute_results": [_P, _P, _P, _P, _SZ, _P, _P, _P],
             "bt_save": [_P, ctypes.c_char_p],
+            "bt_range_batch": [_P, _P, _P, _SZ, ctypes.c_uint32, _P, _P, _P, _P],
             "bt_load": [_P, ctypes.c_char_p],
         }
         for name, args in sig.items():
@@ -372,6 +373,21 @@ class BTree:
         """Scatter answers in routed order back to input order (bt_unroute_results)."""
         _check(lib().bt_unroute_results(self._h, _ptr(perm), _ptr(in_vals), _ptr(in_status), perm.numel(),
                                         _ptr(out_vals), _ptr(out_status), _stream_ptr(stream)), "bt_unroute_results")
+
+    def range(self, lo, hi, max_per: int, stream=None):
+        """Range scan of [lo[i], hi[i]] (int64 CUDA tensors of uint64 bit patterns):
+        (counts int32 [n], keys [n, max_per], vals [n, max_per]); counts above
+        max_per mean the query was truncated."""
+        import torch
+
+        n = lo.numel()
+        dev_ = lo.device
+        keys = torch.zeros((n, max(max_per, 1)), dtype=torch.int64, device=dev_)[:, :max_per]
+        vals = torch.zeros((n, max(max_per, 1)), dtype=torch.int64, device=dev_)[:, :max_per]
+        counts = torch.zeros(max(n, 1), dtype=torch.int32, device=dev_)[:n]
+        _check(lib().bt_range_batch(self._h, _ptr(lo), _ptr(hi), n, max_per, _ptr(keys), _ptr(vals), _ptr(counts),
+                                    _stream_ptr(stream)), "bt_range_batch")
+        return counts, keys, vals
 
     def save(self, path: str):
         """Write the tree's sorted pairs to a snapshot file (bt_save)."""

@@ -238,6 +238,17 @@ int bt_search_batch(bt_handle* H, const uint64_t* keys, uint64_t* out_vals, uint
   return e == cudaSuccess ? BT_OK : BT_ERR_CUDA;
 }
 
+int bt_range_batch(bt_handle* H, const uint64_t* lo, const uint64_t* hi, size_t n, uint32_t max_per,
+                   uint64_t* out_keys, uint64_t* out_vals, uint32_t* out_counts, void* stream) {
+  if (!H) return BT_ERR_INVALID_ARG;
+  if (n == 0) return BT_OK;
+  if (!lo || !hi || !out_counts || (max_per && (!out_keys || !out_vals))) return BT_ERR_INVALID_ARG;
+  DeviceGuard g(H->h.device);
+  return bt::launch_range(&H->h, lo, hi, n, max_per, out_keys, out_vals, out_counts, S(stream)) == cudaSuccess
+             ? BT_OK
+             : BT_ERR_CUDA;
+}
+
 int bt_insert_batch(bt_handle* H, const uint64_t* keys, const uint64_t* vals, uint64_t* out_vals,
                     uint8_t* out_status, size_t n, void* stream) {
   if (!H) return BT_ERR_INVALID_ARG;

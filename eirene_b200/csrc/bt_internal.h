@@ -185,6 +185,9 @@ int tree_bulk_build_scratch(Handle* h, const uint64_t* keys, const uint64_t* val
                             const BuildScratch& sc);
 cudaError_t launch_search(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev, size_t n,
                           uint64_t* out_vals, uint8_t* out_st, cudaStream_t s);
+// range scan, one warp per query (bt_range_batch)
+cudaError_t launch_range(Handle* h, const uint64_t* lo, const uint64_t* hi, size_t n, uint32_t max_per,
+                         uint64_t* out_keys, uint64_t* out_vals, uint32_t* out_counts, cudaStream_t s);
 // the same search with the tree's upper levels cached in shared memory
 cudaError_t launch_search_top(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev,
                               size_t n, uint64_t* out_vals, uint8_t* out_st, cudaStream_t s);

@@ -450,6 +450,56 @@ __global__ void __launch_bounds__(512) search_top_kernel(DevTree t, const TopNod
   }
 }
 
+// Range scan, one warp per query: descend to the leaf that holds `lo`, take
+// the leaf's keys in [lo, hi] (lane i holds slot i; a ballot compacts them in
+// key order), and continue at the leaf that starts at this leaf's right fence
+// (found by a new descent: leaves carry no sibling pointer) until a leaf's
+// fence passes `hi`.  Read-only; runs only when no writer is active.
+__global__ void __launch_bounds__(256) range_kernel(DevTree t, const uint64_t* __restrict__ lo_keys,
+                                                   const uint64_t* __restrict__ hi_keys, size_t n, uint32_t max_per,
+                                                   uint64_t* __restrict__ out_keys, uint64_t* __restrict__ out_vals,
+                                                   uint32_t* __restrict__ out_counts) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t root = t.ctrl->root;
+  const uint32_t root_level = t.ctrl->root_level;
+  const uint64_t cap_nodes = t.cap;
+  const size_t warps = ((size_t)gridDim.x * blockDim.x) >> 5;
+  for (size_t q = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < n; q += warps) {
+    const uint64_t lo = __ldg(lo_keys + q), hi = __ldg(hi_keys + q);
+    uint32_t count = 0;
+    uint64_t from = lo;
+    bool more = root != kNil && lo <= hi && lo != kKeyMax;  // UINT64_MAX is never a stored key
+    for (uint64_t visited = 0; more && visited <= cap_nodes; visited++) {
+      // descend to the leaf holding `from`
+      uint32_t node = root;
+      for (uint32_t level = root_level; level > 0; level--) {
+        const uint64_t k = __ldg(t.keys + (size_t)node * 32 + lane);
+        const uint32_t c = __popc(__ballot_sync(0xffffffffu, lane < 31 && k <= from));
+        node = (uint32_t)__ldg(t.vals + (size_t)node * 32 + c);
+      }
+      const uint64_t k = __ldg(t.keys + (size_t)node * 32 + lane);
+      const uint64_t v = __ldg(t.vals + (size_t)node * 32 + lane);
+      const uint32_t size = hdr_size(__shfl_sync(0xffffffffu, k, 31));
+      const uint64_t fence = __shfl_sync(0xffffffffu, v, 31);
+      const bool in = lane < size && lane < 31 && k >= lo && k <= hi;
+      const uint32_t m = __ballot_sync(0xffffffffu, in);
+      if (in) {
+        const uint32_t pos = count + __popc(m & ((1u << lane) - 1u));
+        if (pos < max_per) {
+          out_keys[q * max_per + pos] = k;
+          out_vals[q * max_per + pos] = v;
+        }
+      }
+      count += __popc(m);
+      // the next leaf starts at the fence; stop when it lies past hi
+      more = fence != kKeyMax && fence <= hi && fence > from;
+      from = fence;
+    }
+    if (lane == 0) out_counts[q] = count;
+  }
+}
+
+
 }  // namespace
 
 int top_alloc(Handle* h) {
@@ -709,6 +759,17 @@ cudaError_t launch_search(Handle* h, const uint64_t* qkeys, const uint32_t* list
     case -8: search_kernel<8, true><<<(unsigned)blocks, threads, 0, s>>>(h->tree, qkeys, list, n_dev, n, out_vals, out_st); break;
     default: search_kernel<8, false><<<(unsigned)blocks, threads, 0, s>>>(h->tree, qkeys, list, n_dev, n, out_vals, out_st); break;
   }
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_range(Handle* h, const uint64_t* lo, const uint64_t* hi, size_t n, uint32_t max_per,
+                         uint64_t* out_keys, uint64_t* out_vals, uint32_t* out_counts, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  size_t blocks = (n * 32 + 255) / 256;
+  const size_t cap = (size_t)h->sm_count * 16;
+  if (blocks > cap) blocks = cap;
+  range_kernel<<<(unsigned)blocks, 256, 0, s>>>(h->tree, lo, hi, n, max_per, out_keys, out_vals, out_counts);
   count_launch();
   return cudaGetLastError();
 }

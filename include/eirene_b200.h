@@ -152,6 +152,16 @@ int bt_search_batch(bt_handle *h, const uint64_t *keys, uint64_t *out_vals, uint
 int bt_insert_batch(bt_handle *h, const uint64_t *keys, const uint64_t *vals, uint64_t *out_vals,
                     uint8_t *out_status, size_t n, void *stream);
 
+/* Range scan of n queries [lo[i], hi[i]] (both ends included, the reference's
+ * "G start end" request, src/input-helper.h:177-185; op code RANGE = 3 is
+ * declared there, src/input-helper.h:17, but no reference version implements
+ * it).  Query i writes its first min(count, max_per) pairs in ascending key
+ * order to out_keys/out_vals[i * max_per ...] and the full number of keys in
+ * its range to out_counts[i] (a count above max_per means truncation).
+ * Device buffers; stream ordered; must not overlap a batch that writes. */
+int bt_range_batch(bt_handle *h, const uint64_t *lo, const uint64_t *hi, size_t n, uint32_t max_per,
+                   uint64_t *out_keys, uint64_t *out_vals, uint32_t *out_counts, void *stream);
+
 /* Number of keys (synchronous). */
 int bt_size(bt_handle *h, uint64_t *n_keys);
 
