@@ -103,7 +103,7 @@ EXPORTS = [
 ]
 MAX_SHARDS = 256
 OPT_SORTED_SEARCH, OPT_RETRY_LIMIT, OPT_TRAIN_STEPS, OPT_SORTED_LEAF_VALS, OPT_BATCH_DESCENT = 1, 2, 3, 4, 5
-OPT_FRONT_END, OPT_TOP_CACHE, OPT_SEARCH_PAIRS = 6, 7, 8
+OPT_FRONT_END, OPT_TOP_CACHE, OPT_SEARCH_PAIRS, OPT_OVERLAP = 6, 7, 8, 9
 PHASES = ["sort", "merge", "search", "insert", "writeback"]
 
 _lib = None

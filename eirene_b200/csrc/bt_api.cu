@@ -55,17 +55,23 @@ std::atomic<unsigned long long> g_launches{0};
 
 void prof_mark(Handle* h, int which, cudaStream_t s) {
   if (!h->prof) return;
-  const size_t base = h->prof_batches * (kNumPhases + 1);
+  const size_t base = h->prof_batches * kProfEvents;
   if (which == 0) {
     // grow the event pool by one batch
-    while (h->prof_ev.size() < base + kNumPhases + 1) {
+    while (h->prof_ev.size() < base + kProfEvents) {
       cudaEvent_t e;
       if (cudaEventCreate(&e) != cudaSuccess) return;
       h->prof_ev.push_back(e);
     }
+    if (h->prof_overlap.size() <= h->prof_batches) h->prof_overlap.resize(h->prof_batches + 1);
+    h->prof_overlap[h->prof_batches] = 0;
   }
   if (base + which < h->prof_ev.size()) cudaEventRecord(h->prof_ev[base + which], s);
   if (which == kNumPhases) h->prof_batches++;
+}
+
+void prof_set_overlap(Handle* h) {
+  if (h->prof && h->prof_batches < h->prof_overlap.size()) h->prof_overlap[h->prof_batches] = 1;
 }
 }  // namespace bt
 
@@ -73,13 +79,22 @@ namespace {
 // fold recorded batches into phase_ms (synchronises on the events)
 int prof_resolve(bt::Handle& h) {
   for (size_t b = 0; b < h.prof_batches; b++) {
-    cudaEvent_t* e = &h.prof_ev[b * (bt::kNumPhases + 1)];
+    cudaEvent_t* e = &h.prof_ev[b * bt::kProfEvents];
     if (cudaEventSynchronize(e[bt::kNumPhases]) != cudaSuccess) return BT_ERR_CUDA;
-    for (int p = 0; p < bt::kNumPhases; p++) {
-      float ms = 0;
-      if (cudaEventElapsedTime(&ms, e[p], e[p + 1]) != cudaSuccess) return BT_ERR_CUDA;
-      h.phase_ms[p] += ms;
+    auto t = [&](int a, int z, float* ms) { return cudaEventElapsedTime(ms, e[a], e[z]) == cudaSuccess; };
+    float ms[bt::kNumPhases] = {};
+    bool ok = true;
+    if (b < h.prof_overlap.size() && h.prof_overlap[b]) {
+      // front + touched sort (side stream) | merge passes (side stream) |
+      // lookups (main stream, concurrent with both) | insert | writeback
+      ok = t(0, bt::kEvSortEnd, &ms[bt::kPhSort]) && t(bt::kEvSortEnd, 2, &ms[bt::kPhMerge]) &&
+           t(1, bt::kEvLookupEnd, &ms[bt::kPhSearch]) && t(3, 4, &ms[bt::kPhInsert]) &&
+           t(4, 5, &ms[bt::kPhWriteback]);
+    } else {
+      for (int p = 0; ok && p < bt::kNumPhases; p++) ok = t(p, p + 1, &ms[p]);
     }
+    if (!ok) return BT_ERR_CUDA;
+    for (int p = 0; p < bt::kNumPhases; p++) h.phase_ms[p] += ms[p];
     h.phase_batches++;
   }
   h.prof_batches = 0;
@@ -143,6 +158,13 @@ int bt_create(const bt_config* cfg_in, bt_handle** out) {
   ok = ok && cudaMemset(h.tree.low, 0, nodes * 8) == cudaSuccess;
   ok = ok && bt::work_alloc(&h.w, cfg.max_batch) == 0;
   ok = ok && cudaStreamCreateWithFlags(&h.internal_stream, cudaStreamNonBlocking) == cudaSuccess;
+  {
+    int lo_prio = 0, hi_prio = 0;
+    cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio);
+    ok = ok && cudaStreamCreateWithPriority(&h.hi_stream, cudaStreamNonBlocking, hi_prio) == cudaSuccess &&
+         cudaEventCreateWithFlags(&h.fork_ev, cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&h.join_ev, cudaEventDisableTiming) == cudaSuccess;
+  }
   ok = ok && bt::tree_reset(&h, h.internal_stream) == cudaSuccess;
   ok = ok && cudaStreamSynchronize(h.internal_stream) == cudaSuccess;
   if (!ok) {
@@ -170,6 +192,9 @@ int bt_destroy(bt_handle* H) {
   cudaFree(h.enum_scan_scratch);
   cudaFree(h.top);
   if (h.internal_stream) cudaStreamDestroy(h.internal_stream);
+  if (h.hi_stream) cudaStreamDestroy(h.hi_stream);
+  if (h.fork_ev) cudaEventDestroy(h.fork_ev);
+  if (h.join_ev) cudaEventDestroy(h.join_ev);
   for (cudaEvent_t e : h.prof_ev) cudaEventDestroy(e);
   delete H;
   return BT_OK;
@@ -415,6 +440,12 @@ int bt_set_option(bt_handle* H, int option, int64_t value) {
     case BT_OPT_SORTED_LEAF_VALS: H->h.sorted_leaf_vals = value ? 1 : 0; return BT_OK;
     case BT_OPT_FRONT_END: H->h.front_end = value ? 1 : 0; return BT_OK;
     case BT_OPT_TOP_CACHE: H->h.top_cache = value ? 1 : 0; return BT_OK;
+    case BT_OPT_OVERLAP:
+      // 0 off; 1 on (default reserve); > 1 on, leaving value - 1 lookup block slots for the sort
+      if (value < 0) return BT_ERR_INVALID_ARG;
+      H->h.overlap = value ? 1 : 0;
+      if (value > 1) H->h.overlap_reserve = (int)(value - 1);
+      return BT_OK;
     case BT_OPT_SEARCH_PAIRS:
       if (value < 0 || value > 2) return BT_ERR_INVALID_ARG;
       H->h.search_pairs = (int)value;

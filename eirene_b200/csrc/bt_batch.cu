@@ -408,31 +408,51 @@ static int batch_hashed(Handle* h, const uint64_t* keys, const uint64_t* vals, c
   const uint32_t* n_touch = &c->n_touch;
   prof_mark(h, 0, s);
   if (front_classify(h, keys, ops, n, s) != 0) return -2;
+  // The touched requests' sort + merge and the plain lookups are independent
+  // (the lookups read the pre-batch tree and write only their own answers):
+  // the former go to a high-priority side stream, the latter stay on `s`,
+  // and `s` waits for both before the insert phase.
+  const bool ov = h->overlap != 0;
+  cudaStream_t s2 = ov ? h->hi_stream : s;
+  if (ov) {
+    prof_set_overlap(h);
+    prof_mark(h, 1, s);
+    if (cudaEventRecord(h->fork_ev, s) != cudaSuccess || cudaStreamWaitEvent(s2, h->fork_ev, 0) != cudaSuccess)
+      return -2;
+  }
   uint64_t* sk = nullptr;
   uint32_t* sv = nullptr;
-  if (radix_sort_pairs(w.f_tk, w.f_tv, nullptr, w.k_a, w.v_a, w.k_b, w.v_b, n, 0, 64, w.sort_scratch, s, &sk, &sv,
+  if (radix_sort_pairs(w.f_tk, w.f_tv, nullptr, w.k_a, w.v_a, w.k_b, w.v_b, n, 0, 64, w.sort_scratch, s2, &sk, &sv,
                        &h->tree.ctrl->error, n_touch) != cudaSuccess)
     return -2;
   const uint32_t n_tiles = (uint32_t)sort_tiles(n);
-  prof_mark(h, 1, s);
-  merge_pass1<<<n_tiles, kThreads, 0, s>>>(sk, sv, vals, n, n_touch, w.tiles);
+  prof_mark(h, ov ? kEvSortEnd : 1, s2);
+  merge_pass1<<<n_tiles, kThreads, 0, s2>>>(sk, sv, vals, n, n_touch, w.tiles);
   count_launch();
-  merge_pass2<<<1, 1024, 0, s>>>(w.tiles, n_tiles, n_touch, c);
+  merge_pass2<<<1, 1024, 0, s2>>>(w.tiles, n_tiles, n_touch, c);
   count_launch();
-  merge_pass3<<<n_tiles, kThreads, 0, s>>>(sk, sv, vals, n, n_touch, w.tiles, w.ukeys, w.uvals, w.ins_list,
-                                           w.get_list, w.pend, out_vals, out_st);
+  merge_pass3<<<n_tiles, kThreads, 0, s2>>>(sk, sv, vals, n, n_touch, w.tiles, w.ukeys, w.uvals, w.ins_list,
+                                            w.get_list, w.pend, out_vals, out_st);
   count_launch();
   if (cudaGetLastError() != cudaSuccess) return -2;
-  // every touched run begins with an INSERT (n_get is zero); the plain
-  // lookups read the pre-batch tree before the insert phase
-  prof_mark(h, 2, s);
+  prof_mark(h, 2, s2);
+  if (ov && cudaEventRecord(h->join_ev, s2) != cudaSuccess) return -2;
+  // plain lookups of the pre-batch tree; every touched run begins with an
+  // INSERT, so the merged batch has no GET runs (n_get is zero)
   cudaError_t e;
   const int desc = h->batch_descent >= 0 ? h->batch_descent : h->descent;
   if (desc == 1 && h->L.valid)
     e = launch_learned_search(h, keys, w.f_list, &c->n_lookup, n, out_vals, out_st, s, false);
-  else
+  else {
+    h->lookup_reserve = ov ? h->overlap_reserve : 0;
     e = launch_search(h, keys, w.f_list, &c->n_lookup, n, out_vals, out_st, s);
+    h->lookup_reserve = 0;
+  }
   if (e != cudaSuccess) return -2;
+  if (ov) {
+    prof_mark(h, kEvLookupEnd, s);
+    if (cudaStreamWaitEvent(s, h->join_ev, 0) != cudaSuccess) return -2;
+  }
   prof_mark(h, 3, s);
   if (insert_phase(h, n, engine, s) != 0) return -2;
   prof_mark(h, 4, s);

@@ -18,6 +18,11 @@ inline void count_launch(unsigned n = 1) { g_launches.fetch_add(n, std::memory_o
 // phases timed with CUDA events when profiling is on (the reference's
 // Time_Measure phases, src/gpu-stm-tree-v38/bpt-gpustm-kernel.cu:289-324)
 enum Phase { kPhSort = 0, kPhMerge, kPhSearch, kPhInsert, kPhWriteback, kNumPhases };
+// boundary events per batch: 0..kNumPhases in order, plus two for the
+// overlapped layout (end of the touched sort on the side stream, end of the
+// lookups on the main stream)
+constexpr int kProfEvents = kNumPhases + 3;
+constexpr int kEvSortEnd = kNumPhases + 1, kEvLookupEnd = kNumPhases + 2;
 
 // ---- scan / sort (bt_sort.cu) ----
 size_t scan_scratch_words(size_t n);
@@ -156,15 +161,25 @@ struct Handle {
   cudaStream_t internal_stream = nullptr;
   // profiling: one event per phase boundary per batch, resolved on read
   bool prof = false;
-  std::vector<cudaEvent_t> prof_ev;  // kNumPhases + 1 events per recorded batch
+  std::vector<cudaEvent_t> prof_ev;  // kProfEvents events per recorded batch
+  std::vector<char> prof_overlap;    // per recorded batch: lookups overlapped the sort (see prof_resolve)
   size_t prof_batches = 0;
+  // hash front end: the touched requests' sort + merge run on a high-priority
+  // side stream while the lookups run on the caller's stream
+  cudaStream_t hi_stream = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+  int overlap = 1;
+  int lookup_reserve = 0;    // block slots the overlapped lookups leave free (set per batch)
+  int overlap_reserve = 16;  // ... in the overlapped layout (measured: 16 >= 32 > 64 > none)
   double phase_ms[kNumPhases] = {};
   unsigned long long phase_batches = 0;
   unsigned long long phase_items[kNumPhases] = {};
 };
 
-// record the boundary event `which` (0..kNumPhases) of the current batch
+// record the boundary event `which` (0..kProfEvents-1) of the current batch;
+// event kNumPhases closes the batch, so the extra events come before it
 void prof_mark(Handle* h, int which, cudaStream_t s);
+void prof_set_overlap(Handle* h);
 
 // ---- tree kernels (bt_tree.cu) ----
 cudaError_t tree_reset(Handle* h, cudaStream_t s);

@@ -731,7 +731,24 @@ cudaError_t launch_search(Handle* h, const uint64_t* qkeys, const uint32_t* list
     const int threads = 256;
     const int G = h->search_group;
     size_t blocks = ((n + 1) / 2 * (size_t)G + threads - 1) / threads;
-    const size_t cap = (size_t)h->sm_count * 8 * 4;
+    size_t cap = (size_t)h->sm_count * 8 * 4;
+    if (h->lookup_reserve > 0) {
+      // a resident, grid-striding launch that leaves `lookup_reserve` block
+      // slots free for kernels running beside it (the overlapped sort)
+      static int per_sm[64][3] = {};
+      const int gi = G == 4 ? 0 : G == 16 ? 2 : 1;
+      const int dev = h->device;
+      int per = (dev >= 0 && dev < 64) ? per_sm[dev][gi] : 0;
+      if (per == 0) {
+        const void* k = G == 4 ? (const void*)search2_kernel<4, false, true>
+                        : G == 16 ? (const void*)search2_kernel<16, false, true>
+                                  : (const void*)search2_kernel<8, false, true>;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, threads, 0) != cudaSuccess || per < 1) per = 1;
+        if (dev >= 0 && dev < 64) per_sm[dev][gi] = per;
+      }
+      const size_t resident = (size_t)h->sm_count * per;
+      cap = resident > (size_t)h->lookup_reserve + h->sm_count ? resident - h->lookup_reserve : h->sm_count;
+    }
     if (blocks > cap) blocks = cap;
     if (blocks == 0) blocks = 1;
 #define BT_S2(GG, CC) search2_kernel<GG, false, CC><<<(unsigned)blocks, threads, 0, s>>>(h->tree, qkeys, list, n_dev, n, out_vals, out_st)
