@@ -30,7 +30,7 @@ ERRORS = {
     -11: "snapshot file error",
 }
 STATIC_BUILD_MAX_KEYS = 65536
-OP_INSERT, OP_GET = 0, 1
+OP_INSERT, OP_GET, OP_DELETE = 0, 1, 2
 ST_ABSENT, ST_FOUND, ST_REJECTED, ST_RETRY_EXHAUSTED, ST_NO_CAPACITY = 0, 1, 2, 3, 4
 MODE_SORTED, MODE_STM, MODE_MERGE_ENGINE = 0, 1, 0x10
 DESCENT_PLAIN, DESCENT_LEARNED = 0, 1

@@ -30,6 +30,7 @@ SOURCES = [
     "bt_shard.cu",
     "bt_front.cu",
     "bt_snapshot.cu",
+    "bt_delete.cu",
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -37,9 +37,11 @@ struct TileSummary {
   uint32_t cont;  // bit0: tile holds the tail of a run begun in an earlier tile; bit1: that key is reserved
   uint32_t ins_local;
   uint32_t get_local;
+  uint32_t del_local;
   uint32_t heads_before;
   uint32_t ins_before;
   uint32_t get_before;
+  uint32_t del_before;
 };
 
 namespace {
@@ -54,7 +56,7 @@ struct Item {
   uint64_t k;
   uint32_t r;
   uint32_t op;
-  bool head, tail, valid, ins;
+  bool head, tail, valid, wr, del;  // wr: INSERT or DELETE of a usable key
 };
 
 __device__ __forceinline__ void load_items(const uint64_t* __restrict__ sk, const uint32_t* __restrict__ sv,
@@ -84,10 +86,12 @@ __device__ __forceinline__ void load_items(const uint64_t* __restrict__ sk, cons
     if (i < n) {
       const uint64_t nx = (j + 1 < kItems) ? it[j + 1].k : (i + 1 < n ? sk[i + 1] : 0);
       it[j].tail = (i + 1 == n) || (nx != it[j].k) || (j + 1 < kItems && !it[j + 1].valid);
-      it[j].ins = (it[j].op == kOpInsert) && it[j].k != kKeyMax;
+      it[j].wr = (it[j].op == kOpInsert || it[j].op == kOpDelete) && it[j].k != kKeyMax;
+      it[j].del = it[j].op == kOpDelete;
     } else {
       it[j].tail = false;
-      it[j].ins = false;
+      it[j].wr = false;
+      it[j].del = false;
     }
   }
 }
@@ -96,9 +100,9 @@ __device__ __forceinline__ Seg item_seg(const Item& x, const uint64_t* __restric
   Seg s;
   s.f = x.head ? 1u : 0u;
   s.v = 0;
-  if (x.valid && x.ins) {
-    s.f |= 2u;
-    s.v = vals[x.r];
+  if (x.valid && x.wr) {
+    s.f |= x.del ? 6u : 2u;
+    s.v = x.del ? 0 : vals[x.r];
   }
   return s;
 }
@@ -136,14 +140,15 @@ __global__ void __launch_bounds__(kThreads) merge_pass1(const uint64_t* __restri
   }
   Seg agg;
   Seg st = blk_exclusive_seg(tagg, Seg{0, 0}, wsf, wsv, &agg);
-  uint32_t ins_l = 0, get_l = 0;
+  uint32_t ins_l = 0, get_l = 0, del_l = 0;
 #pragma unroll
   for (int j = 0; j < kItems; j++) {
     st = seg_combine(st, seg[j]);
     if (it[j].valid && it[j].tail) {
       if (st.f & 1u) {  // run began inside this tile
         if (it[j].k != kKeyMax) {
-          if (st.f & 2u) ins_l++;
+          if (st.f & 4u) del_l++;
+          else if (st.f & 2u) ins_l++;
           else get_l++;
         }
       } else {  // tail of the run continued from the previous tile
@@ -153,10 +158,11 @@ __global__ void __launch_bounds__(kThreads) merge_pass1(const uint64_t* __restri
       }
     }
   }
-  uint32_t th, ti, tg;
+  uint32_t th, ti, tg, td;
   blk_exclusive_sum(heads, ws, &th);
   blk_exclusive_sum(ins_l, ws, &ti);
   blk_exclusive_sum(get_l, ws, &tg);
+  blk_exclusive_sum(del_l, ws, &td);
   if (threadIdx.x == 0) {
     TileSummary& T = tiles[blockIdx.x];
     T.agg_f = agg.f;
@@ -164,6 +170,7 @@ __global__ void __launch_bounds__(kThreads) merge_pass1(const uint64_t* __restri
     T.heads = th;
     T.ins_local = ti;
     T.get_local = tg;
+    T.del_local = td;
     T.cont = s_cont;
     T.pre_f = s_pre_f;
     T.pre_v = s_pre_v;
@@ -190,40 +197,47 @@ __global__ void __launch_bounds__(1024) merge_pass2(TileSummary* __restrict__ ti
   Seg carry = blk_exclusive_seg(a, Seg{0, 0}, wsf, wsv, nullptr);
   uint32_t htot;
   uint32_t hb = blk_exclusive_sum(hsum, ws, &htot);
-  uint32_t isum = 0, gsum = 0;
+  uint32_t isum = 0, gsum = 0, dsum = 0;
   for (uint32_t t = t0; t < t1; t++) {
     TileSummary& T = tiles[t];
     T.carry_f = carry.f;
     T.carry_v = carry.v;
     T.heads_before = hb;
     hb += T.heads;
-    uint32_t ic = T.ins_local, gc = T.get_local;
+    uint32_t ic = T.ins_local, gc = T.get_local, dc = T.del_local;
     if ((T.cont & 1u) && !(T.cont & 2u)) {
       const Seg s = seg_combine(carry, Seg{T.pre_f, T.pre_v});
-      if (s.f & 2u) ic++;
+      if (s.f & 4u) dc++;
+      else if (s.f & 2u) ic++;
       else gc++;
     }
     T.ins_before = ic;  // per-tile counts for now
     T.get_before = gc;
+    T.del_before = dc;
     isum += ic;
     gsum += gc;
+    dsum += dc;
     carry = seg_combine(carry, Seg{T.agg_f, T.agg_v});
   }
-  uint32_t itot, gtot;
+  uint32_t itot, gtot, dtot;
   uint32_t ib = blk_exclusive_sum(isum, ws, &itot);
   uint32_t gb = blk_exclusive_sum(gsum, ws, &gtot);
+  uint32_t db = blk_exclusive_sum(dsum, ws, &dtot);
   for (uint32_t t = t0; t < t1; t++) {
     TileSummary& T = tiles[t];
-    const uint32_t ic = T.ins_before, gc = T.get_before;
+    const uint32_t ic = T.ins_before, gc = T.get_before, dc = T.del_before;
     T.ins_before = ib;
     T.get_before = gb;
+    T.del_before = db;
     ib += ic;
     gb += gc;
+    db += dc;
   }
   if (threadIdx.x == 0) {
     counts->n_unique = htot;
     counts->n_ins = itot;
     counts->n_get = gtot;
+    counts->n_del = dtot;
   }
 }
 
@@ -232,7 +246,8 @@ __global__ void __launch_bounds__(kThreads) merge_pass3(
     const uint64_t* __restrict__ sk, const uint32_t* __restrict__ sv, const uint64_t* __restrict__ vals, size_t n,
     const uint32_t* __restrict__ n_dev, const TileSummary* __restrict__ tiles, uint64_t* __restrict__ ukeys,
     uint64_t* __restrict__ uvals, uint32_t* __restrict__ ins_list, uint32_t* __restrict__ get_list,
-    uint32_t* __restrict__ pend, uint64_t* __restrict__ out_vals, uint8_t* __restrict__ out_st) {
+    uint32_t* __restrict__ del_list, uint32_t* __restrict__ pend, uint64_t* __restrict__ out_vals,
+    uint8_t* __restrict__ out_st) {
   if (n_dev) n = min(n, (size_t)*n_dev);
   if ((size_t)blockIdx.x * kTile >= n) return;
   __shared__ uint32_t wsf[32];
@@ -253,14 +268,15 @@ __global__ void __launch_bounds__(kThreads) merge_pass3(
   }
   Seg st = blk_exclusive_seg(tagg, Seg{T.carry_f, T.carry_v}, wsf, wsv, nullptr);
   // tail kinds with the true carry
-  uint32_t n_ins = 0, n_get = 0;
+  uint32_t n_ins = 0, n_get = 0, n_del = 0;
   {
     Seg s = st;
 #pragma unroll
     for (int j = 0; j < kItems; j++) {
       s = seg_combine(s, seg[j]);
       if (it[j].valid && it[j].tail && it[j].k != kKeyMax) {
-        if (s.f & 2u) n_ins++;
+        if (s.f & 4u) n_del++;
+        else if (s.f & 2u) n_ins++;
         else n_get++;
       }
     }
@@ -268,6 +284,7 @@ __global__ void __launch_bounds__(kThreads) merge_pass3(
   uint32_t hpos = blk_exclusive_sum(heads, ws, nullptr) + T.heads_before;
   uint32_t ipos = blk_exclusive_sum(n_ins, ws, nullptr) + T.ins_before;
   uint32_t gpos = blk_exclusive_sum(n_get, ws, nullptr) + T.get_before;
+  uint32_t dpos = blk_exclusive_sum(n_del, ws, nullptr) + T.del_before;
   // hpos counts heads strictly before this thread's first item
 #pragma unroll
   for (int j = 0; j < kItems; j++) {
@@ -275,14 +292,15 @@ __global__ void __launch_bounds__(kThreads) merge_pass3(
     const size_t i = i0 + j;
     if (it[j].head) hpos++;
     const uint32_t u = hpos - 1;  // unique id of this item's run
-    const bool ok = it[j].k != kKeyMax && it[j].op <= 1u;
+    const bool ok = it[j].k != kKeyMax && it[j].op <= 2u;
     if (!ok) {
       out_vals[it[j].r] = 0;
       out_st[it[j].r] = kRejected;
       pend[i] = kResolved;
-    } else if (!it[j].head && (st.f & 2u)) {  // an earlier INSERT of this same run
-      out_vals[it[j].r] = st.v;
-      out_st[it[j].r] = kFound;
+    } else if (!it[j].head && (st.f & 2u)) {  // an earlier write of this same run
+      const bool gone = (st.f & 4u) != 0;
+      out_vals[it[j].r] = gone ? 0 : st.v;
+      out_st[it[j].r] = gone ? kAbsent : kFound;
       pend[i] = kResolved;
     } else {
       pend[i] = u;
@@ -291,7 +309,8 @@ __global__ void __launch_bounds__(kThreads) merge_pass3(
     if (it[j].tail && it[j].k != kKeyMax) {
       ukeys[u] = it[j].k;
       uvals[u] = st.v;
-      if (st.f & 2u) ins_list[ipos++] = u;
+      if (st.f & 4u) del_list[dpos++] = u;
+      else if (st.f & 2u) ins_list[ipos++] = u;
       else get_list[gpos++] = u;
     }
   }
@@ -334,6 +353,7 @@ int work_alloc(Work* w, size_t cap) {
   A((void**)&w->uans_st, cap);
   A((void**)&w->ins_list, cap * 4);
   A((void**)&w->get_list, cap * 4);
+  A((void**)&w->del_list, cap * 4);
   A((void**)&w->pend, cap * 4);
   A((void**)&w->tiles, tiles * sizeof(TileSummary));
   A((void**)&w->counts, sizeof(BatchCounts));
@@ -376,7 +396,7 @@ int work_alloc(Work* w, size_t cap) {
 
 void work_free(Work* w) {
   void* ps[] = {w->k_a,      w->k_b,       w->v_a,       w->v_b,       w->sort_scratch, w->ukeys,   w->uvals,
-                w->uans,     w->uans_st,   w->ins_list,  w->get_list,  w->pend,         w->tiles,   w->counts,
+                w->uans,     w->uans_st,   w->ins_list,  w->get_list,  w->del_list, w->pend,         w->tiles,   w->counts,
                 w->m_path,   w->m_leaf,    w->m_isnew,   w->m_pos,     w->m_newk,       w->m_newv,  w->m_nq,
                 w->m_nleaf,  w->m_seg,     w->m_ent_a,   w->m_ent_b,   w->m_counts,     w->m_sync,      w->d_in_keys,
                 w->d_in_vals, w->d_in_ops, w->d_out_vals, w->d_out_st, w->f_tab, w->f_flags,
@@ -386,10 +406,13 @@ void work_free(Work* w) {
   *w = Work{};
 }
 
-// insert phase shared by both front ends: the unique INSERT runs of
-// (w.ukeys, w.uvals, w.ins_list, count w.counts->n_ins) reach the tree
+// write phase shared by both front ends: the unique DELETE runs (w.del_list,
+// count w.counts->n_del), then the unique INSERT runs of (w.ukeys, w.uvals,
+// w.ins_list, count w.counts->n_ins) reach the tree
 static int insert_phase(Handle* h, size_t n, int engine, cudaStream_t s) {
   Work& w = h->w;
+  // the DELETE runs first: their keys differ from the INSERT runs' keys
+  if (delete_phase(h, n, s) != 0) return -2;
   // the merge engine needs leaf_fill >= 16 and inner_fill >= 16: then a split
   // emits at most one separator per new key or entry, which bounds its buffers
   if (engine == 1 && h->leaf_fill >= 16 && h->inner_fill >= 16) return merge_engine(h, n, s) != 0 ? -2 : 0;
@@ -432,7 +455,7 @@ static int batch_hashed(Handle* h, const uint64_t* keys, const uint64_t* vals, c
   merge_pass2<<<1, 1024, 0, s2>>>(w.tiles, n_tiles, n_touch, c);
   count_launch();
   merge_pass3<<<n_tiles, kThreads, 0, s2>>>(sk, sv, vals, n, n_touch, w.tiles, w.ukeys, w.uvals, w.ins_list,
-                                            w.get_list, w.pend, out_vals, out_st);
+                                            w.get_list, w.del_list, w.pend, out_vals, out_st);
   count_launch();
   if (cudaGetLastError() != cudaSuccess) return -2;
   prof_mark(h, 2, s2);
@@ -482,7 +505,7 @@ int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const ui
   merge_pass2<<<1, 1024, 0, s>>>(w.tiles, n_tiles, nullptr, w.counts);
   count_launch();
   merge_pass3<<<n_tiles, kThreads, 0, s>>>(sk, sv, vals, n, nullptr, w.tiles, w.ukeys, w.uvals, w.ins_list,
-                                           w.get_list, w.pend, out_vals, out_st);
+                                           w.get_list, w.del_list, w.pend, out_vals, out_st);
   count_launch();
   if (cudaGetLastError() != cudaSuccess) return -2;
   // search phase on the pre-batch tree, then the insert phase

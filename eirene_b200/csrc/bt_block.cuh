@@ -32,8 +32,9 @@ __device__ __forceinline__ uint32_t blk_exclusive_sum(uint32_t v, uint32_t* ws, 
   return base + x - v;
 }
 
-// "latest insert in the current run" segment state: flags bit0 = a run head
-// occurred, bit1 = an insert occurred after the last head; v = that insert's value.
+// "latest write in the current run" segment state: flags bit0 = a run head
+// occurred, bit1 = a write (INSERT or DELETE) occurred after the last head,
+// bit2 = that latest write was a DELETE; v = the latest INSERT's value.
 struct Seg {
   uint32_t f;
   uint64_t v;
@@ -42,12 +43,12 @@ __device__ __forceinline__ Seg seg_combine(Seg a, Seg b) {
   Seg r;
   r.f = (a.f | b.f) & 1u;
   if (b.f & 2u) {
-    r.f |= 2u;
+    r.f |= b.f & 6u;
     r.v = b.v;
   } else if (b.f & 1u) {
     r.v = 0;
   } else {
-    r.f |= a.f & 2u;
+    r.f |= a.f & 6u;
     r.v = a.v;
   }
   return r;

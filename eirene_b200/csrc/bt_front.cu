@@ -1,22 +1,22 @@
 // Hash front end of the sorted-merge batch (the v38 meaning,
 // src/gpu-stm-tree-v38/bpt-gpustm-kernel-aux.cuh:16-56).
 //
-// The meaning only couples requests whose key is INSERTed somewhere in the
-// batch: a request for a key with no INSERT in the batch, or one that comes
-// before the first INSERT of its key, sees the pre-batch tree.  So instead
+// The meaning only couples requests whose key is written (INSERT or DELETE)
+// somewhere in the batch: a request for a key with no write in the batch, or
+// one that comes before the first write of its key, sees the pre-batch tree.  So instead
 // of sorting the whole batch, the front end
 //
-//   1. counts the INSERT requests and sizes an open-addressing table for
+//   1. counts the write requests and sizes an open-addressing table for
 //      their keys (a power of two >= 2x the count, at least 1024 slots),
-//   2. records, per INSERTed key, the index of its first INSERT,
+//   2. records, per written key, the index of its first write,
 //   3. classifies every request: "touched" if its op code is invalid or its
-//      key has an INSERT at or before it; otherwise it is a plain lookup,
+//      key has a write at or before it; otherwise it is a plain lookup,
 //      and compacts both classes in input order, in one pass with a
 //      decoupled look-back over tiles.
 //
 // The touched requests go through the sort + segmented-scan path (their
-// runs all start with an INSERT, so the pre-batch value reaches them from the
-// insert phase, which returns each key's previous value); the plain lookups
+// runs all start with a write, so the pre-batch value reaches them from the
+// delete or insert phase, which return each key's previous value); the plain lookups
 // run on the pre-batch tree, unsorted, writing their answers in place.  For a
 // read-mostly batch the sort shrinks to the INSERTs.
 //
@@ -52,13 +52,16 @@ __device__ __forceinline__ uint64_t slot_hash(uint64_t x) {
   return x ^ (x >> 31);
 }
 
+// INSERT or DELETE: the requests that couple the others of their key
+__device__ __forceinline__ uint32_t is_write(uint8_t op) { return (op == kOpInsert || op == kOpDelete) ? 1u : 0u; }
+
 __device__ __forceinline__ uint32_t table_cap(uint32_t n_ins, size_t cap_max) {
   uint64_t c = 1024;
   while (c < 2ull * n_ins) c <<= 1;
   return (uint32_t)(c < cap_max ? c : cap_max);
 }
 
-// INSERT op codes (an upper bound of the keys to hold: reserved keys count too)
+// INSERT and DELETE op codes (an upper bound of the keys to hold: reserved keys count too)
 __global__ void __launch_bounds__(kThreads) front_count_kernel(const uint8_t* __restrict__ ops, size_t n,
                                                                BatchCounts* __restrict__ counts) {
   uint32_t c = 0;
@@ -67,10 +70,10 @@ __global__ void __launch_bounds__(kThreads) front_count_kernel(const uint8_t* __
   const uchar4* o4 = reinterpret_cast<const uchar4*>(ops);
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += (size_t)gridDim.x * blockDim.x) {
     const uchar4 o = o4[i];
-    c += (o.x == kOpInsert) + (o.y == kOpInsert) + (o.z == kOpInsert) + (o.w == kOpInsert);
+    c += is_write(o.x) + is_write(o.y) + is_write(o.z) + is_write(o.w);
   }
   for (size_t i = n4 * 4 + (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    c += ops[i] == kOpInsert ? 1u : 0u;
+    c += is_write(ops[i]);
   c = __reduce_add_sync(0xffffffffu, c);
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(&counts->n_ins_req, c);
 }
@@ -109,13 +112,13 @@ __global__ void __launch_bounds__(kThreads) front_insert_kernel(const uint64_t* 
   const uchar4* o4 = reinterpret_cast<const uchar4*>(ops);
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += (size_t)gridDim.x * blockDim.x) {
     const uchar4 o = o4[i];
-    if (o.x == kOpInsert) put(4 * i);
-    if (o.y == kOpInsert) put(4 * i + 1);
-    if (o.z == kOpInsert) put(4 * i + 2);
-    if (o.w == kOpInsert) put(4 * i + 3);
+    if (is_write(o.x)) put(4 * i);
+    if (is_write(o.y)) put(4 * i + 1);
+    if (is_write(o.z)) put(4 * i + 2);
+    if (is_write(o.w)) put(4 * i + 3);
   }
   for (size_t i = n4 * 4 + (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    if (ops[i] == kOpInsert) put(i);
+    if (is_write(ops[i])) put(i);
 }
 
 __device__ __forceinline__ uint32_t find_first_from(const Slot* __restrict__ tab, uint32_t mask, uint64_t k,
@@ -189,7 +192,7 @@ __global__ void __launch_bounds__(kScanThreads) front_split_kernel(
       const size_t i = base + (size_t)j * kScanThreads + threadIdx.x;
       bool f = false;
       if (i < n) {
-        f = op[j] > 1;  // invalid op codes are rejected on the sorted path
+        f = op[j] > 2;  // invalid op codes are rejected on the sorted path
         if (!f && any && k[j] != kKeyMax) {
           uint32_t first = kNone;
           if (sk[j] == k[j]) first = sf[j];
@@ -264,7 +267,7 @@ __global__ void __launch_bounds__(kScanThreads) front_split_kernel(
         const uint32_t p = excl + cnt[j][warp] + __popc(bal[j] & lt);  // touched before i
         if ((bal[j] >> lane) & 1u) {
           tk[p] = k[j];
-          tv[p] = (uint32_t)i | ((op[j] <= 1 ? (uint32_t)op[j] : 3u) << 30);
+          tv[p] = (uint32_t)i | ((op[j] <= 2 ? (uint32_t)op[j] : 3u) << 30);
         } else {
           list[i - p] = (uint32_t)i;
         }

@@ -42,7 +42,7 @@ struct BatchCounts {
   uint32_t n_unique;
   uint32_t n_ins;
   uint32_t n_get;
-  uint32_t pad;
+  uint32_t n_del;
   // hash front end (bt_front.cu)
   uint32_t n_ins_req;  // INSERT requests with a valid key
   uint32_t cap;        // hash table slots this batch (power of two)
@@ -73,6 +73,7 @@ struct Work {
   uint8_t* uans_st = nullptr;
   uint32_t* ins_list = nullptr;
   uint32_t* get_list = nullptr;
+  uint32_t* del_list = nullptr;
   uint32_t* pend = nullptr;
   TileSummary* tiles = nullptr;
   uint64_t* tile_carry = nullptr;  // scratch for the tile pass
@@ -245,6 +246,9 @@ cudaError_t launch_serve(Handle* h, const ServeDev& S, cudaStream_t s);
 cudaError_t launch_stm(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, uint8_t op_override,
                        const uint32_t* list, const uint32_t* n_dev, size_t n, uint64_t* out_vals, uint8_t* out_st,
                        cudaStream_t s);
+
+// ---- delete phase of the sorted batch (bt_delete.cu) ----
+int delete_phase(Handle* h, size_t n_upper, cudaStream_t s);
 
 // ---- hash front end of the sorted batch (bt_front.cu) ----
 int front_classify(Handle* h, const uint64_t* keys, const uint8_t* ops, size_t n, cudaStream_t s);

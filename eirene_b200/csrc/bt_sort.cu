@@ -35,8 +35,8 @@ constexpr int kScanItems = 4;
 constexpr int kScanTile = kScanThreads * kScanItems;  // 4096
 
 __device__ __forceinline__ uint32_t digit_of(uint64_t k, int shift) { return (uint32_t)(k >> shift) & 0xff; }
-// 2-bit op code carried in the payload: 0 insert, 1 get, 3 anything else (rejected)
-__device__ __forceinline__ uint32_t op_code(uint8_t op) { return op <= 1 ? (uint32_t)op : 3u; }
+// 2-bit op code carried in the payload: 0 insert, 1 get, 2 delete, 3 anything else (rejected)
+__device__ __forceinline__ uint32_t op_code(uint8_t op) { return op <= 2 ? (uint32_t)op : 3u; }
 
 // ---------------------------------------------------------------- scan ----
 // block-wide exclusive scan of one value per thread (1024 threads)

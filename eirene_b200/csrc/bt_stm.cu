@@ -167,9 +167,42 @@ __device__ int commit_split(const DevTree& t, uint32_t node, uint64_t h, uint64_
   return TX_DONE;
 }
 
+// DELETE in a leaf read under the seqlock (row k/v, header h): absent keys
+// answer ABSENT without a write; a present key is removed by a shift under
+// the leaf's lock (no merge with siblings; an emptied leaf stays).
+__device__ int leaf_delete(const DevTree& t, uint32_t node, uint64_t h, uint64_t k, uint64_t v, uint32_t size,
+                           uint32_t mm, uint64_t& ans, uint8_t& st) {
+  const uint32_t lane = lane_id();
+  if (!mm) {
+    ans = 0;
+    st = kAbsent;
+    return TX_DONE;
+  }
+  const uint32_t at = __ffs(mm) - 1;
+  const uint64_t old = __shfl_sync(kFull, v, at);
+  const uint64_t dk = __shfl_down_sync(kFull, k, 1);
+  const uint64_t dv = __shfl_down_sync(kFull, v, 1);
+  if (!acquire_locks(t, node, h, kNil, 0, false, 0)) return TX_ABORT;
+  if (lane >= at && lane < size) {
+    const bool last = lane + 1 == size;
+    t.keys[(size_t)node * 32 + lane] = last ? kKeyMax : dk;
+    t.vals[(size_t)node * 32 + lane] = last ? 0 : dv;
+  }
+  __threadfence();
+  __syncwarp();
+  if (lane == 0) {
+    st_release(hdr_ptr(t, node), hdr_next(h, size - 1));
+    atomicAdd(&t.ctrl->n_keys, ~0ull);  // - 1
+  }
+  __syncwarp();
+  ans = old;
+  st = kFound;
+  return TX_DONE;
+}
+
 // One transaction attempt for one request (all 32 lanes).
 __device__ int tx_attempt(const DevTree& t, const uint64_t key, const uint64_t val, const bool is_insert,
-                          uint64_t& ans, uint8_t& st) {
+                          const bool is_del, uint64_t& ans, uint8_t& st) {
   const uint32_t lane = lane_id();
   Ctrl* C = t.ctrl;
   // ---- root (reference TX_READ_ROOT, bpt-gpustm-kernel-tx.cuh:92-119)
@@ -260,6 +293,7 @@ __device__ int tx_attempt(const DevTree& t, const uint64_t key, const uint64_t v
   // ---- leaf (answer rule bpt-gpustm-kernel.cu:197-213)
   const uint32_t size = hdr_size(h);
   const uint32_t mm = __ballot_sync(kFull, lane < size && k == key);
+  if (is_del) return leaf_delete(t, node, h, k, v, size, mm, ans, st);
   if (!is_insert) {
     if (mm) {
       ans = __shfl_sync(kFull, v, __ffs(mm) - 1);
@@ -405,8 +439,65 @@ __device__ int fast_insert_locked(const DevTree& t, const uint32_t epoch, const 
   return FAST_DONE;
 }
 
+// DELETE in a candidate leaf, lock first (as fast_insert_locked): a wrong
+// leaf is unlocked unchanged (retry); an absent key answers ABSENT.
+__device__ int fast_delete_locked(const DevTree& t, const uint32_t epoch, const uint32_t node, const uint64_t key,
+                                  uint64_t& ans, uint8_t& st) {
+  const uint32_t lane = lane_id();
+  uint64_t* hp = hdr_ptr(t, node);
+  int ok = 0;
+  uint64_t h = 0;
+  if (lane == 0) {
+    h = ld_relaxed(hp);
+    if (!hdr_locked(h) && hdr_level(h) == 0 && hdr_epoch(h) == epoch)
+      ok = atomicCAS((unsigned long long*)hp, h, hdr_lock(h)) == h;
+  }
+  ok = __shfl_sync(kFull, ok, 0);
+  if (!ok) return FAST_RETRY;
+  h = __shfl_sync(kFull, h, 0);
+  __threadfence();
+  uint64_t k = ld_relaxed(t.keys + (size_t)node * 32 + lane);
+  const uint64_t v = ld_relaxed(t.vals + (size_t)node * 32 + lane);
+  const uint64_t lo = __shfl_sync(kFull, lane == 0 ? ld_relaxed(t.low + node) : 0, 0);
+  const uint64_t fence_key = __shfl_sync(kFull, v, 31);
+  const uint32_t size = hdr_size(h);
+  if (!(lo <= key && key < fence_key)) {
+    if (lane == 0) st_release(hp, h);
+    __syncwarp();
+    return FAST_RETRY;
+  }
+  if (lane == 31) k = kKeyMax;
+  const uint32_t mm = __ballot_sync(kFull, lane < size && k == key);
+  if (!mm) {
+    if (lane == 0) st_release(hp, h);
+    __syncwarp();
+    ans = 0;
+    st = kAbsent;
+    return FAST_DONE;
+  }
+  const uint32_t at = __ffs(mm) - 1;
+  const uint64_t old = __shfl_sync(kFull, v, at);
+  const uint64_t dk = __shfl_down_sync(kFull, k, 1);
+  const uint64_t dv = __shfl_down_sync(kFull, v, 1);
+  if (lane >= at && lane < size) {
+    const bool last = lane + 1 == size;
+    t.keys[(size_t)node * 32 + lane] = last ? kKeyMax : dk;
+    t.vals[(size_t)node * 32 + lane] = last ? 0 : dv;
+  }
+  __threadfence();
+  __syncwarp();
+  if (lane == 0) {
+    st_release(hp, hdr_next(h, size - 1));
+    atomicAdd(&t.ctrl->n_keys, ~0ull);  // - 1
+  }
+  __syncwarp();
+  ans = old;
+  st = kFound;
+  return FAST_DONE;
+}
+
 __device__ int tx_fast(const DevTree& t, const uint32_t epoch, const uint64_t key, const uint64_t val,
-                       const bool is_insert, uint64_t& ans, uint8_t& st, const LearnedDev* M) {
+                       const bool is_insert, const bool is_del, uint64_t& ans, uint8_t& st, const LearnedDev* M) {
   const uint32_t lane = lane_id();
   Ctrl* C = t.ctrl;
   uint32_t node = ld_relaxed32(&C->root);
@@ -432,6 +523,7 @@ __device__ int tx_fast(const DevTree& t, const uint32_t epoch, const uint64_t ke
   }
   const uint64_t* krow = t.keys + (size_t)node * 32;
   if (is_insert) return fast_insert_locked(t, epoch, node, key, val, ans, st);
+  if (is_del) return fast_delete_locked(t, epoch, node, key, ans, st);
   // seqlock read of the leaf
   const uint64_t h = ld_acquire(krow + 31);
   uint64_t k = ld_relaxed(krow + lane);
@@ -504,8 +596,9 @@ __device__ __forceinline__ void run_request(const DevTree& t, const uint32_t epo
   const uint32_t lane = lane_id();
   ans = 0;
   st = kRejected;
-  if (key == kKeyMax || op > 1) return;
+  if (key == kKeyMax || op > 2) return;
   const bool ins = (op == kOpInsert);
+  const bool del = (op == kOpDelete);
   const uint64_t val = ins ? val_in : 0;
   uint32_t attempts = 0, fails = 0;
   bool done = false;
@@ -513,9 +606,9 @@ __device__ __forceinline__ void run_request(const DevTree& t, const uint32_t epo
   // validated path below
   for (int f = 0; f < 4 && !done; f++) {
     attempts++;
-    const int res = tx_fast(t, epoch, key, val, ins, ans, st, f == 0 ? M : nullptr);
+    const int res = tx_fast(t, epoch, key, val, ins, del, ans, st, f == 0 ? M : nullptr);
     if (res == FAST_DONE) {
-      if (ins) cnt.commits++;
+      if (ins || del) cnt.commits++;
       done = true;
     } else if (res == FAST_SLOW) {
       break;
@@ -531,7 +624,7 @@ __device__ __forceinline__ void run_request(const DevTree& t, const uint32_t epo
       if (lane == 0) atomicOr(&t.ctrl->error, kErrRetry);
       break;
     }
-    const int res = tx_attempt(t, key, val, ins, ans, st);
+    const int res = tx_attempt(t, key, val, ins, del, ans, st);
     if (res == TX_DONE) {
       if (ins) cnt.commits++;
       break;

@@ -48,6 +48,9 @@ extern "C" {
 /* ---- request op codes (same numbering as src/input-helper.h:14-17) ---- */
 #define BT_OP_INSERT 0
 #define BT_OP_GET 1
+#define BT_OP_DELETE 2   /* src/input-helper.h:16 declares it; no reference version implements it.
+                          * Answer: the previous value (FOUND) or ABSENT; the leaf shrinks in place
+                          * (no merge with siblings). */
 
 /* ---- per-request status byte written to out_status ---- */
 #define BT_ST_ABSENT 0          /* key was not present (out_vals = 0) */

@@ -253,6 +253,25 @@ restart:;
     return BTO_ABSENT;
 }
 
+int bto_delete(bto_tree *t, uint64_t key, uint64_t *old_val) {
+    if (key == BTO_KEY_MAX) return BTO_REJECTED;
+    if (t->root == BTO_NIL) return BTO_ABSENT;
+    uint32_t n = find_leaf(t, key, NULL, NULL);
+    uint32_t sz = n_size(t, n);
+    uint32_t p = lower_slot(t->keys[n], sz, key);
+    if (p >= sz || t->keys[n][p] != key) return BTO_ABSENT;
+    if (old_val) *old_val = t->vals[n][p];
+    for (uint32_t i = p; i + 1 < sz; i++) {
+        t->keys[n][i] = t->keys[n][i + 1];
+        t->vals[n][i] = t->vals[n][i + 1];
+    }
+    t->keys[n][sz - 1] = BTO_KEY_MAX;
+    t->vals[n][sz - 1] = 0;
+    n_set_info(t, n, sz - 1, 0);
+    t->n_keys--;
+    return BTO_FOUND;
+}
+
 /* ------------------------------------------------------------------------ */
 /* stable LSD radix sort, 8-bit digits, constant digits skipped */
 void bto_sort_pairs(const uint64_t *keys, size_t n, uint64_t *keys_out, uint32_t *idx_out) {
@@ -588,6 +607,7 @@ void bto_execute_serial(bto_tree *t, const uint64_t *keys, const uint64_t *vals,
         int st;
         if (ops[i] == BTO_OP_GET) st = bto_get(t, keys[i], &v);
         else if (ops[i] == BTO_OP_INSERT) st = bto_insert(t, keys[i], vals[i], &v);
+        else if (ops[i] == BTO_OP_DELETE) st = bto_delete(t, keys[i], &v);
         else st = BTO_REJECTED;
         out_vals[i] = st == BTO_FOUND ? v : 0;
         out_status[i] = (uint8_t)st;
@@ -612,10 +632,12 @@ static void *lookup_worker(void *arg) {
     return NULL;
 }
 
-/* v38 batch meaning (src/gpu-stm-tree-v38/bpt-gpustm-kernel-aux.cuh:16-56):
- * within a run of equal keys in stable order, each request sees the tree's
- * pre-batch value until the first INSERT, and afterwards the value of the
- * latest INSERT before it; the run collapses to INSERT(last value) or GET. */
+/* v38 batch meaning (src/gpu-stm-tree-v38/bpt-gpustm-kernel-aux.cuh:16-56),
+ * extended to DELETE: within a run of equal keys in stable order, each
+ * request sees the tree's pre-batch state until the first write (INSERT or
+ * DELETE), and afterwards the state the latest write before it left (the
+ * value of an INSERT, or absent after a DELETE); the run collapses to its last
+ * write, or to a GET.  The batch then applies its deletes, then its inserts. */
 void bto_execute_merged(bto_tree *t, const uint64_t *keys, const uint64_t *vals,
                         const uint8_t *ops, size_t n, uint64_t *out_vals, uint8_t *out_status,
                         int engine, int n_threads) {
@@ -654,15 +676,16 @@ void bto_execute_merged(bto_tree *t, const uint64_t *keys, const uint64_t *vals,
     uint64_t *iv = (uint64_t *)malloc(sizeof(uint64_t) * nu);
     uint64_t *nk = (uint64_t *)malloc(sizeof(uint64_t) * nu);
     uint64_t *nv = (uint64_t *)malloc(sizeof(uint64_t) * nu);
-    size_t ni = 0, nnew = 0;
+    uint64_t *dk = (uint64_t *)malloc(sizeof(uint64_t) * nu);
+    size_t ni = 0, nnew = 0, nd = 0;
     for (size_t u = 0; u < nu; u++) {
-        int have = 0;
+        int have = 0, gone = 0;
         uint64_t cur = 0;
         int rejected_key = (uk[u] == BTO_KEY_MAX);
         for (size_t p = ustart[u]; p < ustart[u + 1]; p++) {
             uint32_t r = si[p];
             uint8_t op = ops[r];
-            if (rejected_key || (op != BTO_OP_GET && op != BTO_OP_INSERT)) {
+            if (rejected_key || (op != BTO_OP_GET && op != BTO_OP_INSERT && op != BTO_OP_DELETE)) {
                 out_status[r] = BTO_REJECTED;
                 out_vals[r] = 0;
                 continue;
@@ -671,16 +694,21 @@ void bto_execute_merged(bto_tree *t, const uint64_t *keys, const uint64_t *vals,
                 out_status[r] = ust[u];
                 out_vals[r] = ust[u] == BTO_FOUND ? uval[u] : 0;
             } else {
-                out_status[r] = BTO_FOUND;
-                out_vals[r] = cur;
+                out_status[r] = gone ? BTO_ABSENT : BTO_FOUND;
+                out_vals[r] = gone ? 0 : cur;
             }
-            if (op == BTO_OP_INSERT) { have = 1; cur = vals[r]; }
+            if (op == BTO_OP_INSERT) { have = 1; gone = 0; cur = vals[r]; }
+            else if (op == BTO_OP_DELETE) { have = 1; gone = 1; cur = 0; }
         }
-        if (have) {
+        if (have && gone) {
+            dk[nd++] = uk[u];
+        } else if (have) {
             ik[ni] = uk[u]; iv[ni] = cur; ni++;
             if (ust[u] != BTO_FOUND) { nk[nnew] = uk[u]; nv[nnew] = cur; nnew++; }
         }
     }
+    for (size_t x = 0; x < nd; x++) bto_delete(t, dk[x], NULL);
+    free(dk);
     if (engine == BTO_ENGINE_MERGE) {
         /* updates in place, then the segmented merge of the new keys */
         for (size_t x = 0; x < ni; x++) {

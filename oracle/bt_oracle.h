@@ -44,6 +44,7 @@ extern "C" {
 /* operation codes: same numbering as the reference (src/input-helper.h:14-17) */
 #define BTO_OP_INSERT 0
 #define BTO_OP_GET 1
+#define BTO_OP_DELETE 2 /* src/input-helper.h:16 (declared there, implemented by no reference version) */
 
 /* per-request result status */
 #define BTO_ABSENT 0
@@ -77,6 +78,10 @@ int bto_bulk_build(bto_tree *t, const uint64_t *keys, const uint64_t *vals, size
 /* Single-request operations (reference rules). Return BTO_FOUND/BTO_ABSENT/BTO_REJECTED. */
 int bto_get(const bto_tree *t, uint64_t key, uint64_t *val);
 int bto_insert(bto_tree *t, uint64_t key, uint64_t val, uint64_t *old_val);
+/* Remove `key`; *old_val = its value.  The leaf shrinks in place: no merge
+ * or redistribution with siblings, an emptied leaf stays in the tree (its
+ * separators keep routing).  Returns BTO_FOUND or BTO_ABSENT. */
+int bto_delete(bto_tree *t, uint64_t key, uint64_t *old_val);
 
 /* Requests applied one at a time in input order (the serial meaning of the
  * unsorted STM batch). */

@@ -18,6 +18,7 @@ LIB_PATH = os.path.join(HERE, "liboracle.so")
 
 OP_INSERT = 0
 OP_GET = 1
+OP_DELETE = 2
 ABSENT, FOUND, REJECTED = 0, 1, 2
 ENGINE_STM, ENGINE_MERGE = 0, 1
 DIST = {"uniform": 0, "zipf": 1, "normal": 2, "gamma": 3}

@@ -136,3 +136,46 @@ def test_mlp_gradient_finite_difference():
         pm[j] -= eps
         lm = np.mean([(O.mlp_forward(pm.astype(np.float32), xi) - yi) ** 2 for xi, yi in zip(x, y)])
         assert abs((lp - lm) / (2 * eps) - g[j]) < 2e-3 * max(1.0, abs(g[j]))
+
+
+def _with_deletes(keys, vals, ops, seed, frac=0.15):
+    """Turn a share of the requests into DELETEs (op code 2)."""
+    rng = np.random.default_rng(seed)
+    ops = ops.copy()
+    ops[rng.random(ops.size) < frac] = 2
+    return keys, vals, ops
+
+
+@pytest.mark.parametrize("engine", [O.ENGINE_STM, O.ENGINE_MERGE])
+def test_merged_equals_serial_with_deletes(engine):
+    # per key, the merged meaning is the serial meaning; keys are independent
+    keys = O.gen_keys("zipf", 71, 20_000)
+    vals = O.value_of(keys)
+    a, b = O.OracleTree(), O.OracleTree()
+    a.bulk_build(keys, vals)
+    b.bulk_build(keys, vals)
+    for i in range(4):
+        rk, rv, ro = _with_deletes(*O.gen_requests("zipf", 72 + i, keys, 30_000, 60), seed=i)
+        sv, ss = a.execute_serial(rk, rv, ro)
+        mv, ms = b.execute_merged(rk, rv, ro, engine=engine)
+        assert (ss == ms).all() and (sv == mv).all()
+    ak, av = a.dump()
+    bk, bv = b.dump()
+    assert (ak == bk).all() and (av == bv).all()
+    assert a.check() == 0 and b.check() == 0
+
+
+def test_delete_basics():
+    t = O.OracleTree()
+    k = np.arange(1, 200, dtype=np.uint64) * np.uint64(10)
+    t.bulk_build(k, k + np.uint64(1))
+    rk = np.array([10, 10, 10, 15, 2**64 - 1, 20], np.uint64)
+    ro = np.array([2, 1, 2, 2, 2, 3], np.uint8)
+    v, s = t.execute_serial(rk, np.zeros_like(rk), ro)
+    assert s.tolist() == [1, 0, 0, 0, 2, 2] and v.tolist() == [11, 0, 0, 0, 0, 0]
+    assert t.size() == 198
+    # empty leaves stay and keep routing: delete everything, then insert again
+    v, s = t.execute_serial(k, np.zeros_like(k), np.full(k.size, 2, np.uint8))
+    assert t.size() == 0 and t.check() == 0
+    v, s = t.execute_serial(k, k, np.zeros(k.size, np.uint8))
+    assert (s == 0).all() and t.size() == k.size and t.check() == 0
