@@ -284,6 +284,11 @@ __global__ void merge_alloc_kernel(DevTree t, MergeCounts* mc, uint32_t entry_ca
 }
 
 // ------------------------------------------------------------- leaf ----
+// One group of G lanes per touched leaf (segment); lane g holds slots
+// g*S .. g*S+S-1 of the row.  Several leaves per warp keep more row loads in
+// flight than a warp per leaf (the kernel is bound by the dependent chain
+// segment bounds -> leaf id -> row).
+template <int G>
 __global__ void __launch_bounds__(256) merge_leaf_kernel(DevTree t, uint32_t leaf_fill, const MergeCounts* mc,
                                                          const uint32_t* __restrict__ seg_start,
                                                          const uint32_t* __restrict__ eoff,
@@ -294,29 +299,38 @@ __global__ void __launch_bounds__(256) merge_leaf_kernel(DevTree t, uint32_t lea
                                                          const uint32_t* __restrict__ ins_list,
                                                          MergeEntry* __restrict__ ent, uint64_t* __restrict__ uans,
                                                          uint8_t* __restrict__ uans_st) {
-  __shared__ uint64_t s_keys[8][32];
-  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  constexpr int S = 32 / G;
+  __shared__ uint64_t s_keys[256 / G][32];
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t g = lane % G;
+  const uint32_t grp = threadIdx.x / G;
+  const uint32_t gmask = group_mask<G>(lane);
   const uint32_t n_segs = mc->n_segs;
   const bool fail = mc->cap_fail != 0;
   const uint32_t base = mc->node_base;
-  const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t n_groups = (gridDim.x * blockDim.x) / G;
   unsigned long long added = 0, splits = 0;
-  for (uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < n_segs; s += n_warps) {
+  for (uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) / G; s < n_segs; s += n_groups) {
     uint32_t a, b;
     seg_bounds(mc, seg_start, s, a, b);
     const uint32_t cnt = b - a;
     if (fail) {
-      for (uint32_t j = lane; j < cnt; j += 32) uans_st[ins_list[nq[a + j]]] = kNoCapacity;
+      for (uint32_t j = g; j < cnt; j += G) uans_st[ins_list[nq[a + j]]] = kNoCapacity;
       continue;
     }
     const uint32_t leaf = nleaf[a];
-    const uint64_t ok = t.keys[(size_t)leaf * 32 + lane];
-    const uint64_t ov = t.vals[(size_t)leaf * 32 + lane];
-    const uint64_t h = __shfl_sync(kFull, ok, 31);
-    const uint64_t fence = __shfl_sync(kFull, ov, 31);
+    uint64_t ok[S], ov[S];
+    load_slots<S>(t.keys + (size_t)leaf * 32 + g * S, ok);
+    load_slots<S>(t.vals + (size_t)leaf * 32 + g * S, ov);
+    const uint64_t h = __shfl_sync(gmask, ok[S - 1], G - 1, G);
+    const uint64_t fence = __shfl_sync(gmask, ov[S - 1], G - 1, G);
     const uint32_t sz = hdr_size(h);
-    s_keys[w][lane] = lane < sz ? ok : kKeyMax;
-    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < S; i++) {
+      const uint32_t slot = g * S + i;
+      s_keys[grp][slot] = slot < sz ? ok[i] : kKeyMax;
+    }
+    __syncwarp(gmask);
     const uint32_t m = sz + cnt;
     const uint32_t p = m <= (uint32_t)kMaxKeys ? 1u : ceil_div(m, leaf_fill);
     const uint32_t eo = eoff[s];
@@ -338,30 +352,40 @@ __global__ void __launch_bounds__(256) merge_leaf_kernel(DevTree t, uint32_t lea
       }
     };
     // old keys and new keys to their merged positions (all reads happened above)
-    if (lane < sz) place(lane + count_less(newk + a, cnt, ok), ok, ov);
-    for (uint32_t j = lane; j < cnt; j += 32) {
-      const uint64_t key = newk[a + j];
-      place(j + count_less(s_keys[w], sz, key), key, newv[a + j]);
+#pragma unroll
+    for (int i = 0; i < S; i++) {
+      const uint32_t slot = g * S + i;
+      if (slot < sz) place(slot + count_less(newk + a, cnt, ok[i]), ok[i], ov[i]);
     }
-    __syncwarp();
+    for (uint32_t j = g; j < cnt; j += G) {
+      const uint64_t key = newk[a + j];
+      place(j + count_less(s_keys[grp], sz, key), key, newv[a + j]);
+    }
+    __syncwarp(gmask);
     // padding, headers, last fence
     for (uint32_t c = 0; c < p; c++) {
       const uint32_t nd = node_of(c);
       const uint32_t kc = piece_size(c, m, p);
-      if (lane >= kc && lane < 31) {
-        t.keys[(size_t)nd * 32 + lane] = kKeyMax;
-        t.vals[(size_t)nd * 32 + lane] = 0;
+#pragma unroll
+      for (int i = 0; i < S; i++) {
+        const uint32_t slot = g * S + i;
+        if (slot >= kc && slot < 31) {
+          t.keys[(size_t)nd * 32 + slot] = kKeyMax;
+          t.vals[(size_t)nd * 32 + slot] = 0;
+        }
       }
-      if (lane == 31) {
+      if (g == G - 1) {
         t.keys[(size_t)nd * 32 + 31] = make_hdr(kc, 0, c == 0 ? hdr_version(h) + 1 : 0, hdr_epoch(h));
         if (c == p - 1) t.vals[(size_t)nd * 32 + 31] = fence;
       }
     }
-    __syncwarp();
-    added += cnt;
-    splits += p - 1;
+    __syncwarp(gmask);
+    if (g == 0) {
+      added += cnt;
+      splits += p - 1;
+    }
   }
-  if (lane == 0 && (added | splits)) {
+  if (g == 0 && (added | splits)) {
     atomicAdd(&t.ctrl->n_keys, added);
     atomicAdd(&t.ctrl->leaf_splits, splits);
   }
@@ -711,7 +735,7 @@ int merge_engine(Handle* h, size_t n_upper, cudaStream_t s) {
     return -2;
   const uint32_t entry_cap = (uint32_t)w.cap;
   merge_alloc_kernel<<<1, 1, 0, s>>>(h->tree, mc, entry_cap);
-  merge_leaf_kernel<<<(unsigned)((size_t)h->sm_count * 8), 256, 0, s>>>(
+  merge_leaf_kernel<8><<<(unsigned)((size_t)h->sm_count * 8), 256, 0, s>>>(
       h->tree, h->leaf_fill, mc, w.m_seg, w.m_pos, w.m_newk, w.m_newv, w.m_nq, w.m_nleaf, w.ins_list,
       reinterpret_cast<MergeEntry*>(w.m_ent_a), w.uans, w.uans_st);
   count_launch(2);
