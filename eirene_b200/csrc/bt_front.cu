@@ -7,7 +7,7 @@
 // of sorting the whole batch, the front end
 //
 //   1. counts the write requests and sizes an open-addressing table for
-//      their keys (a power of two >= 2x the count, at least 1024 slots),
+//      their keys (a power of two >= 1.5x the count, at least 1024 slots),
 //   2. records, per written key, the index of its first write,
 //   3. classifies every request: "touched" if its op code is invalid or its
 //      key has a write at or before it; otherwise it is a plain lookup,
@@ -57,7 +57,7 @@ __device__ __forceinline__ uint32_t is_write(uint8_t op) { return (op == kOpInse
 
 __device__ __forceinline__ uint32_t table_cap(uint32_t n_ins, size_t cap_max) {
   uint64_t c = 1024;
-  while (c < 2ull * n_ins) c <<= 1;
+  while (2 * c < 3ull * n_ins) c <<= 1;  // load factor at most 2/3
   return (uint32_t)(c < cap_max ? c : cap_max);
 }
 
@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(kThreads) front_clear_kernel(Slot* __restrict_
   }
 }
 
-// linear probing; the table holds at most half its slots, so a probe ends
+// linear probing; the table holds at most 2/3 of its slots, so a probe ends
 __global__ void __launch_bounds__(kThreads) front_insert_kernel(const uint64_t* __restrict__ keys,
                                                                 const uint8_t* __restrict__ ops, size_t n,
                                                                 Slot* __restrict__ tab,

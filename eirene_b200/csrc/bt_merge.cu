@@ -238,12 +238,18 @@ __global__ void merge_seg_flags_kernel(const MergeCounts* __restrict__ mc, const
     flags[i] = (i == 0 || nleaf[i] != nleaf[i - 1]) ? 1u : 0u;
 }
 
+// segment starts and each segment's leaf (so the leaf merge loads it without
+// a dependent hop through the segment start)
 __global__ void merge_seg_start_kernel(const MergeCounts* __restrict__ mc, const uint32_t* __restrict__ flags,
-                                       const uint32_t* __restrict__ idx, uint32_t* __restrict__ seg_start) {
+                                       const uint32_t* __restrict__ idx, const uint32_t* __restrict__ nleaf,
+                                       uint32_t* __restrict__ seg_start, uint32_t* __restrict__ seg_leaf) {
   const uint32_t n_new = mc->n_new;
   const size_t stride = (size_t)gridDim.x * blockDim.x;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_new; i += stride)
-    if (flags[i]) seg_start[idx[i]] = (uint32_t)i;
+    if (flags[i]) {
+      seg_start[idx[i]] = (uint32_t)i;
+      seg_leaf[idx[i]] = nleaf[i];
+    }
 }
 
 __device__ __forceinline__ void seg_bounds(const MergeCounts* mc, const uint32_t* seg_start, uint32_t s,
@@ -295,7 +301,7 @@ __global__ void __launch_bounds__(256) merge_leaf_kernel(DevTree t, uint32_t lea
                                                          const uint64_t* __restrict__ newk,
                                                          const uint64_t* __restrict__ newv,
                                                          const uint32_t* __restrict__ nq,
-                                                         const uint32_t* __restrict__ nleaf,
+                                                         const uint32_t* __restrict__ seg_leaf,
                                                          const uint32_t* __restrict__ ins_list,
                                                          MergeEntry* __restrict__ ent, uint64_t* __restrict__ uans,
                                                          uint8_t* __restrict__ uans_st) {
@@ -313,12 +319,12 @@ __global__ void __launch_bounds__(256) merge_leaf_kernel(DevTree t, uint32_t lea
   for (uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) / G; s < n_segs; s += n_groups) {
     uint32_t a, b;
     seg_bounds(mc, seg_start, s, a, b);
+    const uint32_t leaf = seg_leaf[s];
     const uint32_t cnt = b - a;
     if (fail) {
       for (uint32_t j = g; j < cnt; j += G) uans_st[ins_list[nq[a + j]]] = kNoCapacity;
       continue;
     }
-    const uint32_t leaf = nleaf[a];
     uint64_t ok[S], ov[S];
     load_slots<S>(t.keys + (size_t)leaf * 32 + g * S, ok);
     load_slots<S>(t.vals + (size_t)leaf * 32 + g * S, ov);
@@ -727,7 +733,7 @@ int merge_engine(Handle* h, size_t n_upper, cudaStream_t s) {
   count_launch(2);
   if (scan_exclusive_u32(w.m_isnew, w.m_pos, n_upper, &mc->n_segs, w.sort_scratch, s, &mc->n_new) != cudaSuccess)
     return -2;
-  merge_seg_start_kernel<<<gb, 256, 0, s>>>(mc, w.m_isnew, w.m_pos, w.m_seg);
+  merge_seg_start_kernel<<<gb, 256, 0, s>>>(mc, w.m_isnew, w.m_pos, w.m_nleaf, w.m_seg, w.m_leaf);
   merge_leaf_count_kernel<<<gb, 256, 0, s>>>(h->tree, h->leaf_fill, mc, w.m_seg, w.m_nleaf, n_upper, w.m_isnew);
   count_launch(2);
   if (scan_exclusive_u32(w.m_isnew, w.m_pos, n_upper, &mc->n_leaf_entries, w.sort_scratch, s, &mc->n_segs) !=
@@ -736,7 +742,7 @@ int merge_engine(Handle* h, size_t n_upper, cudaStream_t s) {
   const uint32_t entry_cap = (uint32_t)w.cap;
   merge_alloc_kernel<<<1, 1, 0, s>>>(h->tree, mc, entry_cap);
   merge_leaf_kernel<8><<<(unsigned)((size_t)h->sm_count * 8), 256, 0, s>>>(
-      h->tree, h->leaf_fill, mc, w.m_seg, w.m_pos, w.m_newk, w.m_newv, w.m_nq, w.m_nleaf, w.ins_list,
+      h->tree, h->leaf_fill, mc, w.m_seg, w.m_pos, w.m_newk, w.m_newv, w.m_nq, w.m_leaf, w.ins_list,
       reinterpret_cast<MergeEntry*>(w.m_ent_a), w.uans, w.uans_st);
   count_launch(2);
   if (launch_inner(h, entry_cap, mc, s) != cudaSuccess) return -2;
