@@ -164,6 +164,11 @@ int bt_create(const bt_config* cfg_in, bt_handle** out) {
     ok = ok && cudaStreamCreateWithPriority(&h.hi_stream, cudaStreamNonBlocking, hi_prio) == cudaSuccess &&
          cudaEventCreateWithFlags(&h.fork_ev, cudaEventDisableTiming) == cudaSuccess &&
          cudaEventCreateWithFlags(&h.join_ev, cudaEventDisableTiming) == cudaSuccess;
+    ok = ok && cudaStreamCreateWithFlags(&h.xfer_stream, cudaStreamNonBlocking) == cudaSuccess &&
+         cudaEventCreateWithFlags(&h.xfer_keys_ev, cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&h.xfer_vals_ev, cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&h.xfer_ans_ev, cudaEventDisableTiming) == cudaSuccess &&
+         cudaHostAlloc((void**)&h.host_word, 64, cudaHostAllocDefault) == cudaSuccess;
   }
   ok = ok && bt::tree_reset(&h, h.internal_stream) == cudaSuccess;
   ok = ok && cudaStreamSynchronize(h.internal_stream) == cudaSuccess;
@@ -195,6 +200,11 @@ int bt_destroy(bt_handle* H) {
   if (h.hi_stream) cudaStreamDestroy(h.hi_stream);
   if (h.fork_ev) cudaEventDestroy(h.fork_ev);
   if (h.join_ev) cudaEventDestroy(h.join_ev);
+  if (h.xfer_stream) cudaStreamDestroy(h.xfer_stream);
+  if (h.xfer_keys_ev) cudaEventDestroy(h.xfer_keys_ev);
+  if (h.xfer_vals_ev) cudaEventDestroy(h.xfer_vals_ev);
+  if (h.xfer_ans_ev) cudaEventDestroy(h.xfer_ans_ev);
+  if (h.host_word) cudaFreeHost(h.host_word);
   for (cudaEvent_t e : h.prof_ev) cudaEventDestroy(e);
   delete H;
   return BT_OK;
@@ -225,6 +235,13 @@ int bt_execute_batch(bt_handle* H, const uint64_t* keys, const uint64_t* vals, c
   return map_internal(bt::batch_sorted(&h, keys, vals, ops, out_vals, out_status, n, engine, S(stream)));
 }
 
+// Sorted batches overlap the copies with the kernels: the ops and keys go
+// first on the caller's stream (the front end reads them), the values follow
+// on the transfer stream while the front end and the sort run (the merge
+// passes wait for them), and the answers leave on the transfer stream as soon
+// as they are final, while the write phase changes the tree.  A batch whose
+// leaf merge found the node pool full rewrites its kNoCapacity answers after
+// the write phase; the host then copies the answers once more.
 int bt_execute_batch_host(bt_handle* H, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops,
                           uint64_t* out_vals, uint8_t* out_status, size_t n, int mode, void* stream) {
   if (!H) return BT_ERR_INVALID_ARG;
@@ -235,16 +252,53 @@ int bt_execute_batch_host(bt_handle* H, const uint64_t* keys, const uint64_t* va
   DeviceGuard g(h.device);
   cudaStream_t s = S(stream);
   bt::Work& w = h.w;
-  if (cudaMemcpyAsync(w.d_in_keys, keys, n * 8, cudaMemcpyHostToDevice, s) != cudaSuccess ||
-      cudaMemcpyAsync(w.d_in_vals, vals, n * 8, cudaMemcpyHostToDevice, s) != cudaSuccess ||
-      cudaMemcpyAsync(w.d_in_ops, ops, n, cudaMemcpyHostToDevice, s) != cudaSuccess)
+  const auto H2D = cudaMemcpyHostToDevice;
+  const auto D2H = cudaMemcpyDeviceToHost;
+  if ((mode & 0xF) != BT_MODE_SORTED) {
+    if (cudaMemcpyAsync(w.d_in_keys, keys, n * 8, H2D, s) != cudaSuccess ||
+        cudaMemcpyAsync(w.d_in_vals, vals, n * 8, H2D, s) != cudaSuccess ||
+        cudaMemcpyAsync(w.d_in_ops, ops, n, H2D, s) != cudaSuccess)
+      return BT_ERR_CUDA;
+    int rc = bt_execute_batch(H, w.d_in_keys, w.d_in_vals, w.d_in_ops, w.d_out_vals, w.d_out_st, n, mode, stream);
+    if (rc != BT_OK) return rc;
+    if (cudaMemcpyAsync(out_vals, w.d_out_vals, n * 8, D2H, s) != cudaSuccess ||
+        cudaMemcpyAsync(out_status, w.d_out_st, n, D2H, s) != cudaSuccess)
+      return BT_ERR_CUDA;
+    return cudaStreamSynchronize(s) == cudaSuccess ? BT_OK : BT_ERR_CUDA;
+  }
+  cudaStream_t x = h.xfer_stream;
+  if (cudaMemcpyAsync(w.d_in_ops, ops, n, H2D, s) != cudaSuccess ||
+      cudaMemcpyAsync(w.d_in_keys, keys, n * 8, H2D, s) != cudaSuccess ||
+      cudaEventRecord(h.xfer_keys_ev, s) != cudaSuccess || cudaStreamWaitEvent(x, h.xfer_keys_ev, 0) != cudaSuccess ||
+      cudaMemcpyAsync(w.d_in_vals, vals, n * 8, H2D, x) != cudaSuccess ||
+      cudaEventRecord(h.xfer_vals_ev, x) != cudaSuccess)
     return BT_ERR_CUDA;
-  int rc = bt_execute_batch(H, w.d_in_keys, w.d_in_vals, w.d_in_ops, w.d_out_vals, w.d_out_st, n, mode, stream);
-  if (rc != BT_OK) return rc;
-  if (cudaMemcpyAsync(out_vals, w.d_out_vals, n * 8, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-      cudaMemcpyAsync(out_status, w.d_out_st, n, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+  h.vals_wait = h.xfer_vals_ev;
+  h.ans_ready = h.xfer_ans_ev;
+  const int engine = (mode & BT_MODE_MERGE_ENGINE) ? 1 : 0;
+  int rc = map_internal(bt::batch_sorted(&h, w.d_in_keys, w.d_in_vals, w.d_in_ops, w.d_out_vals, w.d_out_st, n,
+                                         engine, s));
+  h.vals_wait = nullptr;
+  h.ans_ready = nullptr;
+  if (rc != BT_OK) {
+    cudaStreamSynchronize(x);
+    return rc;
+  }
+  const uint32_t* fix = h.ans_fix;
+  if (cudaStreamWaitEvent(x, h.xfer_ans_ev, 0) != cudaSuccess ||
+      cudaMemcpyAsync(out_vals, w.d_out_vals, n * 8, D2H, x) != cudaSuccess ||
+      cudaMemcpyAsync(out_status, w.d_out_st, n, D2H, x) != cudaSuccess)
     return BT_ERR_CUDA;
-  return cudaStreamSynchronize(s) == cudaSuccess ? BT_OK : BT_ERR_CUDA;
+  *h.host_word = 0;
+  if (fix && cudaMemcpyAsync(h.host_word, fix, 4, D2H, s) != cudaSuccess) return BT_ERR_CUDA;
+  if (cudaStreamSynchronize(x) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) return BT_ERR_CUDA;
+  if (fix && *h.host_word) {
+    if (cudaMemcpyAsync(out_vals, w.d_out_vals, n * 8, D2H, s) != cudaSuccess ||
+        cudaMemcpyAsync(out_status, w.d_out_st, n, D2H, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+      return BT_ERR_CUDA;
+  }
+  return BT_OK;
 }
 
 int bt_search_batch(bt_handle* H, const uint64_t* keys, uint64_t* out_vals, uint8_t* out_status, size_t n,

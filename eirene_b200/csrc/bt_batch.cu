@@ -316,10 +316,12 @@ __global__ void __launch_bounds__(kThreads) merge_pass3(
   }
 }
 
+// cond (optional): write only when *cond is nonzero (the kNoCapacity fix-up)
 __global__ void writeback_kernel(const uint32_t* __restrict__ sv, const uint32_t* __restrict__ pend, size_t n,
                                  const uint32_t* __restrict__ n_dev, const uint64_t* __restrict__ uans,
                                  const uint8_t* __restrict__ uans_st, uint64_t* __restrict__ out_vals,
-                                 uint8_t* __restrict__ out_st) {
+                                 uint8_t* __restrict__ out_st, const uint32_t* __restrict__ cond) {
+  if (cond && *cond == 0) return;
   if (n_dev) n = min(n, (size_t)*n_dev);
   const size_t stride = (size_t)gridDim.x * blockDim.x;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
@@ -366,6 +368,8 @@ int work_alloc(Work* w, size_t cap) {
   A((void**)&w->m_nq, cap * 4 + 64);
   A((void**)&w->m_nleaf, cap * 4);
   A((void**)&w->m_seg, cap * 4);
+  A((void**)&w->d_leaf, cap * 4);
+  A((void**)&w->d_slot, cap * 4);
   A((void**)&w->m_ent_a, cap * 16);
   A((void**)&w->m_ent_b, cap * 16);
   A((void**)&w->m_counts, 64);
@@ -398,7 +402,7 @@ void work_free(Work* w) {
   void* ps[] = {w->k_a,      w->k_b,       w->v_a,       w->v_b,       w->sort_scratch, w->ukeys,   w->uvals,
                 w->uans,     w->uans_st,   w->ins_list,  w->get_list,  w->del_list, w->pend,         w->tiles,   w->counts,
                 w->m_path,   w->m_leaf,    w->m_isnew,   w->m_pos,     w->m_newk,       w->m_newv,  w->m_nq,
-                w->m_nleaf,  w->m_seg,     w->m_ent_a,   w->m_ent_b,   w->m_counts,     w->m_sync,      w->d_in_keys,
+                w->m_nleaf,  w->m_seg,     w->d_leaf,    w->d_slot,    w->m_ent_a,   w->m_ent_b,   w->m_counts,     w->m_sync,      w->d_in_keys,
                 w->d_in_vals, w->d_in_ops, w->d_out_vals, w->d_out_st, w->f_tab, w->f_flags,
                 w->f_pos,    w->f_list,    w->f_tk,      w->f_tv};
   for (void* p : ps)
@@ -406,24 +410,52 @@ void work_free(Work* w) {
   *w = Work{};
 }
 
-// write phase shared by both front ends: the unique DELETE runs (w.del_list,
-// count w.counts->n_del), then the unique INSERT runs of (w.ukeys, w.uvals,
-// w.ins_list, count w.counts->n_ins) reach the tree
-static int insert_phase(Handle* h, size_t n, int engine, cudaStream_t s) {
-  Work& w = h->w;
-  // the DELETE runs first: their keys differ from the INSERT runs' keys
-  if (delete_phase(h, n, s) != 0) return -2;
+static bool merge_usable(const Handle* h, int engine) {
   // the merge engine needs leaf_fill >= 16 and inner_fill >= 16: then a split
   // emits at most one separator per new key or entry, which bounds its buffers
-  if (engine == 1 && h->leaf_fill >= 16 && h->inner_fill >= 16) return merge_engine(h, n, s) != 0 ? -2 : 0;
+  return engine == 1 && h->leaf_fill >= 16 && h->inner_fill >= 16;
+}
+
+// write phase shared by both front ends: the unique DELETE runs (w.del_list,
+// count w.counts->n_del), then the unique INSERT runs of (w.ukeys, w.uvals,
+// w.ins_list, count w.counts->n_ins) reach the tree.  located: the merge
+// engine's and the delete phase's locates already ran.
+static int insert_phase(Handle* h, size_t n, int engine, bool located, cudaStream_t s) {
+  Work& w = h->w;
+  // the DELETE runs first: their keys differ from the INSERT runs' keys
+  if (!located && delete_locate(h, n, s) != 0) return -2;
+  if (delete_apply(h, n, s) != 0) return -2;
+  if (merge_usable(h, engine)) {
+    if (!located && merge_locate_phase(h, s) != 0) return -2;
+    return merge_apply_phase(h, n, s) != 0 ? -2 : 0;
+  }
   const cudaError_t e =
       launch_stm(h, w.ukeys, w.uvals, nullptr, kOpInsert, w.ins_list, &w.counts->n_ins, n, w.uans, w.uans_st, s);
   return e == cudaSuccess ? 0 : -2;
 }
 
-// The hash front end (bt_front.cu): only the requests coupled by an INSERT
-// of their key are sorted and merged; the rest are plain lookups of the
+static int wait_vals(Handle* h, cudaStream_t s) {
+  return h->vals_wait && cudaStreamWaitEvent(s, h->vals_wait, 0) != cudaSuccess ? -2 : 0;
+}
+
+static int answers_ready(Handle* h, cudaStream_t s, const uint32_t* fix) {
+  h->ans_fix = fix;
+  return h->ans_ready && cudaEventRecord(h->ans_ready, s) != cudaSuccess ? -2 : 0;
+}
+
+// The hash front end (bt_front.cu): only the requests coupled by a write of
+// their key are sorted and merged; the rest are plain lookups of the
 // pre-batch tree, answered in place.  Same meaning as the full-sort path.
+//
+// Streams (overlap on): `s` runs the front end, then the lookups; a
+// high-priority side stream runs the touched requests' sort and merge passes
+// and, with the merge engine, the two locates (they read the pre-batch tree,
+// move no key and write only values of keys the lookups do not ask for) and
+// the write-back of the touched answers.  `s` waits for the side stream,
+// then the DELETE apply and the leaf/inner merge change the tree.  Every
+// answer is final before that write phase except kNoCapacity, which the
+// leaf merge sets on a full node pool; a second, conditional write-back
+// after it copies those.
 static int batch_hashed(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops,
                         uint64_t* out_vals, uint8_t* out_st, size_t n, int engine, cudaStream_t s) {
   Work& w = h->w;
@@ -431,11 +463,8 @@ static int batch_hashed(Handle* h, const uint64_t* keys, const uint64_t* vals, c
   const uint32_t* n_touch = &c->n_touch;
   prof_mark(h, 0, s);
   if (front_classify(h, keys, ops, n, s) != 0) return -2;
-  // The touched requests' sort + merge and the plain lookups are independent
-  // (the lookups read the pre-batch tree and write only their own answers):
-  // the former go to a high-priority side stream, the latter stay on `s`,
-  // and `s` waits for both before the insert phase.
   const bool ov = h->overlap != 0;
+  const bool early = merge_usable(h, engine);
   cudaStream_t s2 = ov ? h->hi_stream : s;
   if (ov) {
     prof_set_overlap(h);
@@ -450,6 +479,7 @@ static int batch_hashed(Handle* h, const uint64_t* keys, const uint64_t* vals, c
     return -2;
   const uint32_t n_tiles = (uint32_t)sort_tiles(n);
   prof_mark(h, ov ? kEvSortEnd : 1, s2);
+  if (wait_vals(h, s2) != 0) return -2;
   merge_pass1<<<n_tiles, kThreads, 0, s2>>>(sk, sv, vals, n, n_touch, w.tiles);
   count_launch();
   merge_pass2<<<1, 1024, 0, s2>>>(w.tiles, n_tiles, n_touch, c);
@@ -458,10 +488,17 @@ static int batch_hashed(Handle* h, const uint64_t* keys, const uint64_t* vals, c
                                             w.get_list, w.del_list, w.pend, out_vals, out_st);
   count_launch();
   if (cudaGetLastError() != cudaSuccess) return -2;
+  const unsigned wb_blocks = (unsigned)min((size_t)h->sm_count * 8, (n + 255) / 256);
+  if (early) {
+    if (delete_locate(h, n, s2) != 0 || merge_locate_phase(h, s2) != 0) return -2;
+    writeback_kernel<<<wb_blocks, 256, 0, s2>>>(sv, w.pend, n, n_touch, w.uans, w.uans_st, out_vals, out_st,
+                                                nullptr);
+    count_launch();
+  }
   prof_mark(h, 2, s2);
   if (ov && cudaEventRecord(h->join_ev, s2) != cudaSuccess) return -2;
-  // plain lookups of the pre-batch tree; every touched run begins with an
-  // INSERT, so the merged batch has no GET runs (n_get is zero)
+  // plain lookups of the pre-batch tree; every touched run begins with a
+  // write, so the merged batch has no GET runs (n_get is zero)
   cudaError_t e;
   const int desc = h->batch_descent >= 0 ? h->batch_descent : h->descent;
   if (desc == 1 && h->L.valid)
@@ -476,18 +513,21 @@ static int batch_hashed(Handle* h, const uint64_t* keys, const uint64_t* vals, c
     prof_mark(h, kEvLookupEnd, s);
     if (cudaStreamWaitEvent(s, h->join_ev, 0) != cudaSuccess) return -2;
   }
+  if (early && answers_ready(h, s, merge_fail_flag(h)) != 0) return -2;
   prof_mark(h, 3, s);
-  if (insert_phase(h, n, engine, s) != 0) return -2;
+  if (insert_phase(h, n, engine, early, s) != 0) return -2;
   prof_mark(h, 4, s);
-  const unsigned wb_blocks = (unsigned)min((size_t)h->sm_count * 8, (n + 255) / 256);
-  writeback_kernel<<<wb_blocks, 256, 0, s>>>(sv, w.pend, n, n_touch, w.uans, w.uans_st, out_vals, out_st);
+  writeback_kernel<<<wb_blocks, 256, 0, s>>>(sv, w.pend, n, n_touch, w.uans, w.uans_st, out_vals, out_st,
+                                             early ? merge_fail_flag(h) : nullptr);
   count_launch();
   prof_mark(h, 5, s);
+  if (!early && answers_ready(h, s, nullptr) != 0) return -2;
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
 int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, uint64_t* out_vals,
                  uint8_t* out_st, size_t n, int engine, cudaStream_t s) {
+  h->ans_fix = nullptr;
   if (n == 0) return 0;
   Work& w = h->w;
   if (n > w.cap || n > kIdxMask) return -6;
@@ -500,6 +540,7 @@ int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const ui
     return -2;
   const uint32_t n_tiles = (uint32_t)sort_tiles(n);
   prof_mark(h, 1, s);
+  if (wait_vals(h, s) != 0) return -2;
   merge_pass1<<<n_tiles, kThreads, 0, s>>>(sk, sv, vals, n, nullptr, w.tiles);
   count_launch();
   merge_pass2<<<1, 1024, 0, s>>>(w.tiles, n_tiles, nullptr, w.counts);
@@ -521,12 +562,13 @@ int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const ui
     e = launch_search(h, w.ukeys, w.get_list, &w.counts->n_get, n, w.uans, w.uans_st, s);
   if (e != cudaSuccess) return -2;
   prof_mark(h, 3, s);
-  if (insert_phase(h, n, engine, s) != 0) return -2;
+  if (insert_phase(h, n, engine, false, s) != 0) return -2;
   prof_mark(h, 4, s);
   const unsigned wb_blocks = (unsigned)min((size_t)h->sm_count * 8, (n + 255) / 256);
-  writeback_kernel<<<wb_blocks, 256, 0, s>>>(sv, w.pend, n, nullptr, w.uans, w.uans_st, out_vals, out_st);
+  writeback_kernel<<<wb_blocks, 256, 0, s>>>(sv, w.pend, n, nullptr, w.uans, w.uans_st, out_vals, out_st, nullptr);
   count_launch();
   prof_mark(h, 5, s);
+  if (answers_ready(h, s, nullptr) != 0) return -2;
   if (cudaGetLastError() != cudaSuccess) return -2;
   return 0;
 }

@@ -13,8 +13,8 @@
 //                      order and the header gets the new size.
 // Leaves shrink in place: no merge with siblings; an emptied leaf stays and
 // its separators keep routing (searches in it find nothing, inserts refill
-// it).  Runs before the insert phase; no other kernel touches the tree
-// meanwhile.  HBM traffic per deleted key: the descent (288 B at the leaf)
+// it).  The locate may run beside lookups of other keys (it writes no node);
+// the apply runs before the insert phase with no other kernel on the tree.  HBM traffic per deleted key: the descent (288 B at the leaf)
 // and, per touched leaf, one 512 B row read and written.
 #include <cuda_runtime.h>
 
@@ -128,17 +128,23 @@ __global__ void __launch_bounds__(256) del_apply_kernel(DevTree t, const uint32_
 
 }  // namespace
 
-// Applies the batch's DELETE runs (before its inserts).  n_upper bounds the
-// device count w.counts->n_del.
-int delete_phase(Handle* h, size_t n_upper, cudaStream_t s) {
+// The batch's DELETE runs (before its inserts), in two launches: the locate
+// reads the tree only, the apply removes the keys.  n_upper bounds the device
+// count w.counts->n_del.
+int delete_locate(Handle* h, size_t n_upper, cudaStream_t s) {
   Work& w = h->w;
-  const uint32_t* n_del = &w.counts->n_del;
   const unsigned blocks = (unsigned)min((size_t)h->sm_count * 8, (n_upper * kG + 255) / 256 + 1);
-  del_locate_kernel<<<blocks, 256, 0, s>>>(h->tree, w.ukeys, w.del_list, n_del, w.m_leaf, w.m_isnew, w.uans,
-                                           w.uans_st);
+  del_locate_kernel<<<blocks, 256, 0, s>>>(h->tree, w.ukeys, w.del_list, &w.counts->n_del, w.d_leaf, w.d_slot,
+                                           w.uans, w.uans_st);
+  count_launch();
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int delete_apply(Handle* h, size_t n_upper, cudaStream_t s) {
+  Work& w = h->w;
   del_apply_kernel<<<(unsigned)min((size_t)h->sm_count * 8, (n_upper * 32 + 255) / 256 + 1), 256, 0, s>>>(
-      h->tree, n_del, w.m_leaf, w.m_isnew);
-  count_launch(2);
+      h->tree, &w.counts->n_del, w.d_leaf, w.d_slot);
+  count_launch();
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 

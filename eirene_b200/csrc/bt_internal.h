@@ -88,6 +88,10 @@ struct Work {
   uint32_t* m_nq = nullptr;
   uint32_t* m_nleaf = nullptr;
   uint32_t* m_seg = nullptr;
+  // delete phase (bt_delete.cu): leaf and slot of each unique DELETE key,
+  // apart from the merge scratch so the two locates can run back to back
+  uint32_t* d_leaf = nullptr;
+  uint32_t* d_slot = nullptr;
   void* m_ent_a = nullptr;      // separator entries, 16 B each
   void* m_ent_b = nullptr;
   void* m_counts = nullptr;
@@ -172,6 +176,18 @@ struct Handle {
   int overlap = 1;
   int lookup_reserve = 0;    // block slots the overlapped lookups leave free (set per batch)
   int overlap_reserve = 16;  // ... in the overlapped layout (measured: 16 >= 32 > 64 > none)
+  // host-buffer entry point: the value copy and the answer copies run on
+  // their own stream, overlapped with the batch's kernels
+  cudaStream_t xfer_stream = nullptr;
+  cudaEvent_t xfer_keys_ev = nullptr, xfer_vals_ev = nullptr, xfer_ans_ev = nullptr;
+  uint32_t* host_word = nullptr;  // pinned host word (answer fix-up flag)
+  // per-batch hooks of the sorted batch, set by the host-buffer entry point:
+  // the stream that first reads `vals` waits for vals_wait; ans_ready is
+  // recorded once every answer is in the output arrays, except the
+  // kNoCapacity fix-up signalled by *ans_fix (nullptr: no fix-up pending)
+  cudaEvent_t vals_wait = nullptr;
+  cudaEvent_t ans_ready = nullptr;
+  const uint32_t* ans_fix = nullptr;
   double phase_ms[kNumPhases] = {};
   unsigned long long phase_batches = 0;
   unsigned long long phase_items[kNumPhases] = {};
@@ -248,7 +264,9 @@ cudaError_t launch_stm(Handle* h, const uint64_t* keys, const uint64_t* vals, co
                        cudaStream_t s);
 
 // ---- delete phase of the sorted batch (bt_delete.cu) ----
-int delete_phase(Handle* h, size_t n_upper, cudaStream_t s);
+// locate: reads the tree only (answers the DELETE runs); apply: removes the keys
+int delete_locate(Handle* h, size_t n_upper, cudaStream_t s);
+int delete_apply(Handle* h, size_t n_upper, cudaStream_t s);
 
 // ---- hash front end of the sorted batch (bt_front.cu) ----
 int front_classify(Handle* h, const uint64_t* keys, const uint8_t* ops, size_t n, cudaStream_t s);
@@ -268,6 +286,13 @@ int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const ui
 
 // ---- segmented leaf merge (bt_merge.cu) ----
 int merge_engine(Handle* h, size_t n_upper, cudaStream_t s);
+// the same in two parts: locate (descents of the pre-batch tree, answers of
+// the INSERT runs, in-place value updates of existing keys; no key moves)
+// and apply (leaf merge and inner levels).  merge_fail_flag is nonzero after
+// apply when the node pool could not take the batch's new keys.
+int merge_locate_phase(Handle* h, cudaStream_t s);
+int merge_apply_phase(Handle* h, size_t n_upper, cudaStream_t s);
+const uint32_t* merge_fail_flag(Handle* h);
 
 // device view of the learned model when the learned descent is on and trained
 struct LearnedDev;

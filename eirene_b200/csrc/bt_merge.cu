@@ -3,13 +3,12 @@
 // which inserts one key per warp under STM (src/gpu-stm-tree-v39/
 // bpt-gpustm-kernel.cu:14-256); the batch meaning is still v38's.
 //
-// After the search phase, with the batch's unique INSERT keys in ascending
-// order:
+// With the batch's unique INSERT keys in ascending order:
 //   locate    each 8-lane group walks a contiguous run of the keys (path reuse,
 //             as in the sorted search), records the root-to-leaf path, answers
 //             the previous value and updates existing keys in place;
 //   compact   the new keys, then runs of new keys sharing a leaf (segments);
-//   leaf      one warp per touched leaf merges its new keys by rank scatter
+//   leaf      one 8-lane group per touched leaf merges its new keys by rank scatter
 //             (each element computes its merged position by binary search in
 //             the other sequence) and cuts an overflowing leaf into
 //             p = ceil(m / leaf_fill) leaves of even size; the first keys of
@@ -18,7 +17,10 @@
 //             (children spread evenly over q = ceil((s+1)/(inner_fill+1))
 //             nodes, the key between two pieces moves up) and rebuilds an
 //             overflowing root with the bulk-load rule.
-// Nothing runs concurrently with it, so no locks are taken.  The rules are
+// Locate moves no key and writes only the values of keys that the batch
+// inserts, so it may run beside the lookups of the keys the batch does not
+// write (the hash front end does so); compact, leaf and inner run alone, so
+// no locks are taken.  The rules are
 // restated by the CPU oracle (bto_execute_merged with BTO_ENGINE_MERGE) and
 // the resulting leaf layout is compared exactly.
 #include <cuda_runtime.h>
@@ -705,26 +707,31 @@ static cudaError_t launch_inner(Handle* h, uint32_t entry_cap, MergeCounts* mc, 
 
 // Runs the merge engine for the unique INSERT keys of the current batch
 // (w.ins_list, count on the device).  n_upper bounds the count.
-int merge_engine(Handle* h, size_t n_upper, cudaStream_t s) {
+int merge_locate_phase(Handle* h, cudaStream_t s) {
   Work& w = h->w;
   MergeCounts* mc = reinterpret_cast<MergeCounts*>(w.m_counts);
   const uint32_t* n_ins = &w.counts->n_ins;
   merge_ensure_root_kernel<<<1, 1, 0, s>>>(h->tree);
   count_launch();
   if (cudaMemsetAsync(mc, 0, sizeof(MergeCounts), s) != cudaSuccess) return -2;
-  {
-    static int per_sm[64] = {};
-    if (h->device < 64 && per_sm[h->device] == 0) {
-      int b = 0;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, merge_locate_kernel<8>, 256, 0) != cudaSuccess || b < 1)
-        b = 4;
-      per_sm[h->device] = b;
-    }
-    const size_t blocks = (size_t)h->sm_count * (h->device < 64 ? per_sm[h->device] : 4);
-    merge_locate_kernel<8><<<(unsigned)blocks, 256, 0, s>>>(h->tree, w.ukeys, w.uvals, w.ins_list, n_ins, w.m_path,
-                                                            w.m_leaf, w.m_isnew, w.uans, w.uans_st);
-    count_launch();
+  static int per_sm[64] = {};
+  if (h->device < 64 && per_sm[h->device] == 0) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, merge_locate_kernel<8>, 256, 0) != cudaSuccess || b < 1)
+      b = 4;
+    per_sm[h->device] = b;
   }
+  const size_t blocks = (size_t)h->sm_count * (h->device < 64 ? per_sm[h->device] : 4);
+  merge_locate_kernel<8><<<(unsigned)blocks, 256, 0, s>>>(h->tree, w.ukeys, w.uvals, w.ins_list, n_ins, w.m_path,
+                                                          w.m_leaf, w.m_isnew, w.uans, w.uans_st);
+  count_launch();
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int merge_apply_phase(Handle* h, size_t n_upper, cudaStream_t s) {
+  Work& w = h->w;
+  MergeCounts* mc = reinterpret_cast<MergeCounts*>(w.m_counts);
+  const uint32_t* n_ins = &w.counts->n_ins;
   if (scan_exclusive_u32(w.m_isnew, w.m_pos, n_upper, &mc->n_new, w.sort_scratch, s, n_ins) != cudaSuccess) return -2;
   const unsigned gb = (unsigned)min((size_t)h->sm_count * 8, (n_upper + 255) / 256);
   merge_compact_kernel<<<gb, 256, 0, s>>>(w.ins_list, n_ins, w.m_isnew, w.m_pos, w.ukeys, w.uvals, w.m_leaf, w.m_newk,
@@ -747,6 +754,13 @@ int merge_engine(Handle* h, size_t n_upper, cudaStream_t s) {
   count_launch(2);
   if (launch_inner(h, entry_cap, mc, s) != cudaSuccess) return -2;
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+const uint32_t* merge_fail_flag(Handle* h) { return &reinterpret_cast<MergeCounts*>(h->w.m_counts)->cap_fail; }
+
+int merge_engine(Handle* h, size_t n_upper, cudaStream_t s) {
+  if (merge_locate_phase(h, s) != 0) return -2;
+  return merge_apply_phase(h, n_upper, s);
 }
 
 }  // namespace bt

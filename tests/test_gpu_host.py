@@ -1,0 +1,124 @@
+"""The host-buffer entry point (bt_execute_batch_host) against the oracle and
+against the device-buffer entry point on a twin tree.  Sorted batches overlap
+the value copy with the front end and the answer copy with the write phase;
+these tests cover every layout of that pipeline: both front ends, both
+insert engines, the side stream on and off, DELETE runs, repeated keys, and a
+node pool that runs out (the kNoCapacity answers are rewritten after the
+write phase and copied again)."""
+import numpy as np
+import pytest
+
+import eirene_b200 as E
+from oracle import oracle as O
+from tests.helpers import dev, dump, run_batch
+
+pytestmark = pytest.mark.gpu
+MERGE = E.MODE_SORTED | E.MODE_MERGE_ENGINE
+
+
+def with_deletes(k, v, o, seed, frac):
+    rng = np.random.default_rng(seed)
+    o = o.copy()
+    o[rng.random(o.size) < frac] = E.OP_DELETE
+    return k, v, o
+
+
+def twins(dist, seed, n=80_000):
+    keys = O.gen_keys(dist, seed, n)
+    vals = O.value_of(keys)
+    th = E.BTree(max_keys=1 << 21, max_batch=1 << 18)
+    td = E.BTree(max_keys=1 << 21, max_batch=1 << 18)
+    for t in (th, td):
+        t.bulk_build(dev(keys), dev(vals))
+    o = O.OracleTree()
+    o.bulk_build(keys, vals)
+    return th, td, o, keys
+
+
+def same_contents(t, o):
+    gk, gv = dump(t)
+    ok, ov = o.dump()
+    assert gk.size == ok.size and (gk == ok).all() and (gv == ov).all()
+
+
+@pytest.mark.parametrize("overlap", [1, 0])
+@pytest.mark.parametrize("front", [1, 0])
+@pytest.mark.parametrize("engine", [E.MODE_MERGE_ENGINE, 0])
+def test_host_batches_match_oracle_and_device(gpu, overlap, front, engine):
+    th, td, o, keys = twins("zipf", 101)
+    for t in (th, td):
+        t.set_option(E.OPT_FRONT_END, front)
+        t.set_option(E.OPT_OVERLAP, overlap)
+    mode = E.MODE_SORTED | engine
+    for b, (mix, frac) in enumerate([(95, 0.0), (50, 0.2), (80, 0.5), (0, 0.0)]):
+        rk, rv, ro = with_deletes(*O.gen_requests("zipf", 102 + b, keys, 70_000, mix), seed=b, frac=frac)
+        ov, os_ = o.execute_merged(rk, rv, ro, engine=O.ENGINE_MERGE if engine else O.ENGINE_STM)
+        hv, hs = th.execute_host(rk, rv, ro, mode=mode)
+        gv, gs = run_batch(td, rk, rv, ro, mode)
+        bad = np.nonzero((hs != os_) | (hv != ov))[0]
+        assert bad.size == 0, (b, bad[:5], ro[bad[:5]], hs[bad[:5]], os_[bad[:5]])
+        assert (gs == hs).all() and (gv == hv).all()
+        same_contents(th, o)
+    if engine:
+        assert (th.leaf_sizes() == o.leaf_sizes()).all()
+
+
+def test_host_batches_from_empty_tree(gpu):
+    # the first batch creates the root while the lookups of the same batch run
+    t = E.BTree(max_keys=1 << 20, max_batch=1 << 16)
+    o = O.OracleTree()
+    rng = np.random.default_rng(7)
+    for b in range(3):
+        rk = rng.integers(1, 2**63, 40_000, dtype=np.uint64)
+        rk[rng.random(rk.size) < 0.3] = rk[0]  # one hot key
+        rv = rk ^ np.uint64(b + 1)
+        ro = (rng.random(rk.size) < 0.4).astype(np.uint8)  # 60 % INSERT, 40 % GET
+        ov, os_ = o.execute_merged(rk, rv, ro, engine=O.ENGINE_MERGE)
+        hv, hs = t.execute_host(rk, rv, ro, mode=MERGE)
+        assert (hs == os_).all() and (hv == ov).all()
+    same_contents(t, o)
+
+
+@pytest.mark.parametrize("host", [True, False])
+def test_merge_engine_pool_exhaustion(gpu, host):
+    # a pool too small for the batches: a batch whose new keys do not fit
+    # answers kNoCapacity for every new key (all or nothing), updates of
+    # existing keys still answer the old value, and the tree stays intact
+    t = E.BTree(max_keys=0, max_batch=1 << 16)  # pool = 4096 nodes
+    rng = np.random.default_rng(11)
+    ins_ok = np.zeros(0, np.uint64)
+    vals_now = {}
+    failed = 0
+    for b in range(12):
+        new = rng.choice(2**40, 16384, replace=False).astype(np.uint64) + np.uint64(1)
+        new = np.setdiff1d(new, ins_ok)
+        old = ins_ok[rng.integers(0, ins_ok.size, 2048)] if ins_ok.size else np.zeros(0, np.uint64)
+        old = np.unique(old)
+        gets = ins_ok[rng.integers(0, ins_ok.size, 2048)] if ins_ok.size else np.zeros(0, np.uint64)
+        gets = np.setdiff1d(gets, old)
+        rk = np.concatenate([new, old, gets])
+        rv = np.concatenate([new * np.uint64(3), old + np.uint64(b), gets])
+        ro = np.concatenate([np.zeros(new.size + old.size, np.uint8), np.ones(gets.size, np.uint8)])
+        perm = rng.permutation(rk.size)
+        rk, rv, ro = rk[perm], rv[perm], ro[perm]
+        if host:
+            gv, gs = t.execute_host(rk, rv, ro, mode=MERGE)
+        else:
+            gv, gs = run_batch(t, rk, rv, ro, MERGE)
+        is_new = np.isin(rk, new)
+        st_new = np.unique(gs[is_new])
+        assert st_new.size == 1 and st_new[0] in (E.ST_ABSENT, E.ST_NO_CAPACITY), st_new
+        for i in np.nonzero(~is_new)[0]:
+            assert gs[i] == E.ST_FOUND and gv[i] == vals_now[int(rk[i])]
+        for i in np.nonzero(ro == 0)[0]:
+            if not is_new[i] or st_new[0] == E.ST_ABSENT:
+                vals_now[int(rk[i])] = int(rv[i])
+        if st_new[0] == E.ST_ABSENT:
+            ins_ok = np.union1d(ins_ok, new)
+        else:
+            failed += 1
+    assert failed > 0 and ins_ok.size > 0
+    assert t.stats()["error"] & 1
+    k, v = dump(t)
+    assert (k == ins_ok).all()
+    assert all(int(vv) == vals_now[int(kk)] for kk, vv in zip(k[::97], v[::97]))
