@@ -456,7 +456,7 @@ def main():
         tree.reset_stats()
         tree.profile(True)
         tree.profile_read(reset=True)
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 2)]
         barrier()
         sampler = ClockSampler(local)
         sampler.start()
@@ -464,13 +464,15 @@ def main():
         ev[0].record(stream)
         for s in range(args.steps):
             step(*batches[args.warmup + s])
-            ev[s + 1].record(stream)
+            ev[s + 1].record(stream)  # the batch's answers are final
+        tree.sync(stream)  # the last batch's deferred leaf/inner merge
+        ev[-1].record(stream)
         torch.cuda.synchronize()
         launches = E.launch_count() - l0
         clocks = sampler.stop()
         barrier()
         step_ms = [ev[s].elapsed_time(ev[s + 1]) for s in range(args.steps)]
-        total_ms = ev[0].elapsed_time(ev[-1])
+        total_ms = ev[0].elapsed_time(ev[-1])  # up to the end of every batch's write phase
         phases = tree.profile_read(reset=True)
         tree.profile(False)
         st = tree.stats()
@@ -553,19 +555,35 @@ def main():
                 "peak_source": peak_kind, "traffic": traffic, "alg_bytes_per_launch": dom_bytes,
                 "launch_ms": dom_ms}
 
-    # ---- e2e through the host entry point (pinned host buffers, copies timed)
+    # ---- e2e through the host entry point (pinned host buffers, copies timed),
+    # with the headline form's descent
     e2e = None
+    tree.set_descent(head == "learned")
+    tree.set_option(E.OPT_BATCH_DESCENT, 1 if head == "learned" else 0)
     if True:
         hb = []
         e2e_steps = 5
+        # page-locked host buffers from the library's own allocator (bt_host_alloc)
+        pinned = []
+
+        def host_buf(n, dtype):
+            b = E.HostBuffer(n, dtype)
+            pinned.append(b)
+            return b.tensor
+
         for i in range(1 + e2e_steps):
             k = torch.empty(n_b, dtype=torch.int64, device="cuda")
             v = torch.empty(n_b, dtype=torch.int64, device="cuda")
             o = torch.empty(n_b, dtype=torch.uint8, device="cuda")
             E.gen_requests(args.dist, 30_000 + 1000 * rank + i, tk, n_b, args.search_pct, k, v, o, stream)
-            hb.append((k.cpu().pin_memory(), v.cpu().pin_memory(), o.cpu().pin_memory()))
-        hov = torch.empty(n_b, dtype=torch.int64).pin_memory()
-        hos = torch.empty(n_b, dtype=torch.uint8).pin_memory()
+            torch.cuda.synchronize()
+            hk, hv, ho = host_buf(n_b, torch.int64), host_buf(n_b, torch.int64), host_buf(n_b, torch.uint8)
+            hk.copy_(k)
+            hv.copy_(v)
+            ho.copy_(o)
+            hb.append((hk, hv, ho))
+        hov = host_buf(n_b, torch.int64)
+        hos = host_buf(n_b, torch.uint8)
         L = E.lib()
         sp = stream.cuda_stream
 
@@ -596,10 +614,14 @@ def main():
         e0.record(stream)
         for s in range(e2e_steps):
             host_step(hb[1 + s])
+        tree.sync(stream)
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
         e2e_ms = allmax(e0.elapsed_time(e1))
+        del hb, hov, hos
+        for b in pinned:
+            b.free()
         e2e = {"value": world * n_b * e2e_steps / (e2e_ms / 1e3) / 1e6, "unit": "Mops/s",
                "h2d_bytes_per_step": n_b * 17, "d2h_bytes_per_step": n_b * 9,
                "steps": e2e_steps, "descent": head}

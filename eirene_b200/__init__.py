@@ -99,11 +99,11 @@ EXPORTS = [
     "bt_profile", "bt_profile_read", "bt_launch_count", "bt_bulk_build_static",
     "bt_set_learned_group", "bt_learned_info", "bt_mlp_grad", "bt_set_option", "bt_autotune",
     "bt_serve_config_init", "bt_serve_start", "bt_submit", "bt_poll", "bt_wait", "bt_serve_get_stats", "bt_serve_stop",
-    "bt_route_batch", "bt_unroute_results", "bt_save", "bt_load", "bt_range_batch",
+    "bt_route_batch", "bt_unroute_results", "bt_save", "bt_load", "bt_range_batch", "bt_sync",
 ]
 MAX_SHARDS = 256
 OPT_SORTED_SEARCH, OPT_RETRY_LIMIT, OPT_TRAIN_STEPS, OPT_SORTED_LEAF_VALS, OPT_BATCH_DESCENT = 1, 2, 3, 4, 5
-OPT_FRONT_END, OPT_TOP_CACHE, OPT_SEARCH_PAIRS, OPT_OVERLAP = 6, 7, 8, 9
+OPT_FRONT_END, OPT_TOP_CACHE, OPT_SEARCH_PAIRS, OPT_OVERLAP, OPT_ASYNC_WRITE = 6, 7, 8, 9, 10
 PHASES = ["sort", "merge", "search", "insert", "writeback"]
 
 _lib = None
@@ -176,6 +176,7 @@ def lib():
             "bt_unroute_results": [_P, _P, _P, _P, _SZ, _P, _P, _P],
             "bt_save": [_P, ctypes.c_char_p],
             "bt_range_batch": [_P, _P, _P, _SZ, ctypes.c_uint32, _P, _P, _P, _P],
+            "bt_sync": [_P, _P],
             "bt_load": [_P, ctypes.c_char_p],
         }
         for name, args in sig.items():
@@ -336,6 +337,11 @@ class BTree:
         _check(lib().bt_profile_read(self._h, ms, ctypes.byref(b), 1 if reset else 0), "bt_profile_read")
         return {"batches": b.value, **{p: ms[i] for i, p in enumerate(PHASES)}}
 
+    def sync(self, stream=None):
+        """Order `stream` (or, with None, the host) after every batch issued so
+        far, the deferred leaf/inner merge included (OPT_ASYNC_WRITE)."""
+        _check(lib().bt_sync(self._h, _stream_ptr(stream)), "bt_sync")
+
     def set_option(self, option: int, value: int):
         _check(lib().bt_set_option(self._h, option, value), "bt_set_option")
 
@@ -399,6 +405,29 @@ class BTree:
 
     def set_search_group(self, lanes: int):
         _check(lib().bt_set_search_group(self._h, lanes), "bt_set_search_group")
+
+
+class HostBuffer:
+    """Page-locked host memory from bt_host_alloc for the host-buffer entry
+    point (copies to and from it run at the link's full speed without a
+    staging copy); `tensor` is a CPU tensor over it.  free() releases it:
+    the tensor must not be used after that."""
+
+    def __init__(self, n: int, dtype):
+        import torch
+
+        nbytes = max(1, n * torch.empty(0, dtype=dtype).element_size())
+        p = _P()
+        _check(lib().bt_host_alloc(ctypes.byref(p), nbytes), "bt_host_alloc")
+        self._p = p.value
+        buf = (ctypes.c_uint8 * nbytes).from_address(self._p)
+        self.tensor = torch.from_numpy(np.ctypeslib.as_array(buf)).view(dtype)[:n]
+
+    def free(self):
+        if self._p:
+            self.tensor = None
+            _check(lib().bt_host_free(self._p), "bt_host_free")
+            self._p = None
 
 
 def launch_count() -> int:

@@ -63,15 +63,26 @@ void prof_mark(Handle* h, int which, cudaStream_t s) {
       if (cudaEventCreate(&e) != cudaSuccess) return;
       h->prof_ev.push_back(e);
     }
-    if (h->prof_overlap.size() <= h->prof_batches) h->prof_overlap.resize(h->prof_batches + 1);
-    h->prof_overlap[h->prof_batches] = 0;
+    if (h->prof_layout.size() <= h->prof_batches) h->prof_layout.resize(h->prof_batches + 1);
+    h->prof_layout[h->prof_batches] = 0;
   }
   if (base + which < h->prof_ev.size()) cudaEventRecord(h->prof_ev[base + which], s);
   if (which == kNumPhases) h->prof_batches++;
 }
 
-void prof_set_overlap(Handle* h) {
-  if (h->prof && h->prof_batches < h->prof_overlap.size()) h->prof_overlap[h->prof_batches] = 1;
+void prof_set_layout(Handle* h, int layout) {
+  if (h->prof && h->prof_batches < h->prof_layout.size()) h->prof_layout[h->prof_batches] = (char)layout;
+}
+
+cudaError_t tree_join(Handle* h, cudaStream_t s) {
+  return h->tree_pending ? cudaStreamWaitEvent(s, h->tree_ev, 0) : cudaSuccess;
+}
+
+cudaError_t tree_sync(Handle* h) {
+  if (!h->tree_pending) return cudaSuccess;
+  const cudaError_t e = cudaEventSynchronize(h->tree_ev);
+  if (e == cudaSuccess) h->tree_pending = false;
+  return e;
 }
 }  // namespace bt
 
@@ -84,14 +95,23 @@ int prof_resolve(bt::Handle& h) {
     auto t = [&](int a, int z, float* ms) { return cudaEventElapsedTime(ms, e[a], e[z]) == cudaSuccess; };
     float ms[bt::kNumPhases] = {};
     bool ok = true;
-    if (b < h.prof_overlap.size() && h.prof_overlap[b]) {
-      // front + touched sort (side stream) | merge passes (side stream) |
-      // lookups (main stream, concurrent with both) | insert | writeback
+    const int layout = b < h.prof_layout.size() ? h.prof_layout[b] : 0;
+    if (layout & bt::kLayoutOverlap) {
+      // front + touched sort | merge passes, then the locates (side stream) |
+      // lookups (main stream, beside the locates)
       ok = t(0, bt::kEvSortEnd, &ms[bt::kPhSort]) && t(bt::kEvSortEnd, 2, &ms[bt::kPhMerge]) &&
-           t(1, bt::kEvLookupEnd, &ms[bt::kPhSearch]) && t(3, 4, &ms[bt::kPhInsert]) &&
-           t(4, 5, &ms[bt::kPhWriteback]);
+           t(1, bt::kEvLookupEnd, &ms[bt::kPhSearch]);
     } else {
-      for (int p = 0; ok && p < bt::kNumPhases; p++) ok = t(p, p + 1, &ms[p]);
+      for (int p = 0; ok && p < bt::kPhInsert; p++) ok = t(p, p + 1, &ms[p]);
+    }
+    if (layout & bt::kLayoutEarly) {
+      // insert = DELETE apply + leaf reservation, then the leaf/inner merge
+      // (on the tree stream when deferred); writeback between the two
+      float a = 0, z = 0;
+      ok = ok && t(3, bt::kEvWbStart, &a) && t(4, 5, &z) && t(bt::kEvWbStart, 4, &ms[bt::kPhWriteback]);
+      ms[bt::kPhInsert] = a + z;
+    } else {
+      ok = ok && t(3, 4, &ms[bt::kPhInsert]) && t(4, 5, &ms[bt::kPhWriteback]);
     }
     if (!ok) return BT_ERR_CUDA;
     for (int p = 0; p < bt::kNumPhases; p++) h.phase_ms[p] += ms[p];
@@ -167,8 +187,10 @@ int bt_create(const bt_config* cfg_in, bt_handle** out) {
     ok = ok && cudaStreamCreateWithFlags(&h.xfer_stream, cudaStreamNonBlocking) == cudaSuccess &&
          cudaEventCreateWithFlags(&h.xfer_keys_ev, cudaEventDisableTiming) == cudaSuccess &&
          cudaEventCreateWithFlags(&h.xfer_vals_ev, cudaEventDisableTiming) == cudaSuccess &&
-         cudaEventCreateWithFlags(&h.xfer_ans_ev, cudaEventDisableTiming) == cudaSuccess &&
-         cudaHostAlloc((void**)&h.host_word, 64, cudaHostAllocDefault) == cudaSuccess;
+         cudaEventCreateWithFlags(&h.xfer_ans_ev, cudaEventDisableTiming) == cudaSuccess;
+    ok = ok && cudaStreamCreateWithFlags(&h.tree_stream, cudaStreamNonBlocking) == cudaSuccess &&
+         cudaEventCreateWithFlags(&h.tree_ev, cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&h.ans_ev, cudaEventDisableTiming) == cudaSuccess;
   }
   ok = ok && bt::tree_reset(&h, h.internal_stream) == cudaSuccess;
   ok = ok && cudaStreamSynchronize(h.internal_stream) == cudaSuccess;
@@ -204,7 +226,9 @@ int bt_destroy(bt_handle* H) {
   if (h.xfer_keys_ev) cudaEventDestroy(h.xfer_keys_ev);
   if (h.xfer_vals_ev) cudaEventDestroy(h.xfer_vals_ev);
   if (h.xfer_ans_ev) cudaEventDestroy(h.xfer_ans_ev);
-  if (h.host_word) cudaFreeHost(h.host_word);
+  if (h.tree_stream) cudaStreamDestroy(h.tree_stream);
+  if (h.tree_ev) cudaEventDestroy(h.tree_ev);
+  if (h.ans_ev) cudaEventDestroy(h.ans_ev);
   for (cudaEvent_t e : h.prof_ev) cudaEventDestroy(e);
   delete H;
   return BT_OK;
@@ -214,6 +238,7 @@ int bt_bulk_build(bt_handle* H, const uint64_t* keys, const uint64_t* vals, size
   if (!H || (n && (!keys || !vals))) return BT_ERR_INVALID_ARG;
   DeviceGuard g(H->h.device);
   H->h.L.valid = false;
+  if (bt::tree_join(&H->h, S(stream)) != cudaSuccess) return BT_ERR_CUDA;
   return map_internal(bt::tree_bulk_build(&H->h, keys, vals, n, S(stream)));
 }
 
@@ -227,6 +252,7 @@ int bt_execute_batch(bt_handle* H, const uint64_t* keys, const uint64_t* vals, c
   DeviceGuard g(h.device);
   const int base = mode & 0xF;
   if (base == BT_MODE_STM) {
+    if (bt::tree_join(&h, S(stream)) != cudaSuccess) return BT_ERR_CUDA;
     cudaError_t e = bt::launch_stm(&h, keys, vals, ops, 0xFF, nullptr, nullptr, n, out_vals, out_status, S(stream));
     return e == cudaSuccess ? BT_OK : BT_ERR_CUDA;
   }
@@ -239,9 +265,7 @@ int bt_execute_batch(bt_handle* H, const uint64_t* keys, const uint64_t* vals, c
 // first on the caller's stream (the front end reads them), the values follow
 // on the transfer stream while the front end and the sort run (the merge
 // passes wait for them), and the answers leave on the transfer stream as soon
-// as they are final, while the write phase changes the tree.  A batch whose
-// leaf merge found the node pool full rewrites its kNoCapacity answers after
-// the write phase; the host then copies the answers once more.
+// as they are final, while the write phase changes the tree.
 int bt_execute_batch_host(bt_handle* H, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops,
                           uint64_t* out_vals, uint8_t* out_status, size_t n, int mode, void* stream) {
   if (!H) return BT_ERR_INVALID_ARG;
@@ -284,20 +308,11 @@ int bt_execute_batch_host(bt_handle* H, const uint64_t* keys, const uint64_t* va
     cudaStreamSynchronize(x);
     return rc;
   }
-  const uint32_t* fix = h.ans_fix;
   if (cudaStreamWaitEvent(x, h.xfer_ans_ev, 0) != cudaSuccess ||
       cudaMemcpyAsync(out_vals, w.d_out_vals, n * 8, D2H, x) != cudaSuccess ||
       cudaMemcpyAsync(out_status, w.d_out_st, n, D2H, x) != cudaSuccess)
     return BT_ERR_CUDA;
-  *h.host_word = 0;
-  if (fix && cudaMemcpyAsync(h.host_word, fix, 4, D2H, s) != cudaSuccess) return BT_ERR_CUDA;
   if (cudaStreamSynchronize(x) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) return BT_ERR_CUDA;
-  if (fix && *h.host_word) {
-    if (cudaMemcpyAsync(out_vals, w.d_out_vals, n * 8, D2H, s) != cudaSuccess ||
-        cudaMemcpyAsync(out_status, w.d_out_st, n, D2H, s) != cudaSuccess ||
-        cudaStreamSynchronize(s) != cudaSuccess)
-      return BT_ERR_CUDA;
-  }
   return BT_OK;
 }
 
@@ -309,7 +324,8 @@ int bt_search_batch(bt_handle* H, const uint64_t* keys, uint64_t* out_vals, uint
   bt::Handle& h = H->h;
   DeviceGuard g(h.device);
   // searches alone never conflict: run the search kernel directly on the batch
-  cudaError_t e;
+  cudaError_t e = bt::tree_join(&h, S(stream));
+  if (e != cudaSuccess) return BT_ERR_CUDA;
   if (h.descent == BT_DESCENT_LEARNED && h.L.valid)
     e = bt::launch_learned_search(&h, keys, nullptr, nullptr, n, out_vals, out_status, S(stream), false);
   else
@@ -323,6 +339,7 @@ int bt_range_batch(bt_handle* H, const uint64_t* lo, const uint64_t* hi, size_t 
   if (n == 0) return BT_OK;
   if (!lo || !hi || !out_counts || (max_per && (!out_keys || !out_vals))) return BT_ERR_INVALID_ARG;
   DeviceGuard g(H->h.device);
+  if (bt::tree_join(&H->h, S(stream)) != cudaSuccess) return BT_ERR_CUDA;
   return bt::launch_range(&H->h, lo, hi, n, max_per, out_keys, out_vals, out_counts, S(stream)) == cudaSuccess
              ? BT_OK
              : BT_ERR_CUDA;
@@ -345,6 +362,7 @@ int bt_size(bt_handle* H, uint64_t* n_keys) {
   if (!H || !n_keys) return BT_ERR_INVALID_ARG;
   DeviceGuard g(H->h.device);
   bt::Ctrl c;
+  if (bt::tree_sync(&H->h) != cudaSuccess) return BT_ERR_CUDA;
   if (cudaMemcpy(&c, H->h.tree.ctrl, sizeof(c), cudaMemcpyDeviceToHost) != cudaSuccess) return BT_ERR_CUDA;
   *n_keys = c.n_keys;
   return BT_OK;
@@ -355,6 +373,7 @@ int bt_dump_sorted(bt_handle* H, uint64_t* keys, uint64_t* vals, size_t cap, siz
   DeviceGuard g(H->h.device);
   cudaStream_t s = stream ? S(stream) : H->h.internal_stream;
   if (stream == nullptr) cudaDeviceSynchronize();
+  if (bt::tree_join(&H->h, s) != cudaSuccess) return BT_ERR_CUDA;
   return map_internal(bt::tree_dump(&H->h, keys, vals, cap, n_out, s));
 }
 
@@ -439,6 +458,7 @@ int bt_retrain(bt_handle* H, void* stream) {
   DeviceGuard g(H->h.device);
   cudaStream_t s = stream ? S(stream) : H->h.internal_stream;
   if (stream == nullptr) cudaDeviceSynchronize();
+  if (bt::tree_join(&H->h, s) != cudaSuccess) return BT_ERR_CUDA;
   return map_internal(bt::learned_retrain(&H->h, s));
 }
 
@@ -485,6 +505,13 @@ int bt_profile_read(bt_handle* H, double* phase_ms, uint64_t* batches, int reset
   return BT_OK;
 }
 
+int bt_sync(bt_handle* H, void* stream) {
+  if (!H) return BT_ERR_INVALID_ARG;
+  DeviceGuard g(H->h.device);
+  const cudaError_t e = stream ? bt::tree_join(&H->h, S(stream)) : bt::tree_sync(&H->h);
+  return e == cudaSuccess ? BT_OK : BT_ERR_CUDA;
+}
+
 uint64_t bt_launch_count(void) { return bt::g_launches.load(); }
 
 int bt_set_option(bt_handle* H, int option, int64_t value) {
@@ -493,6 +520,7 @@ int bt_set_option(bt_handle* H, int option, int64_t value) {
     case BT_OPT_SORTED_SEARCH: H->h.sorted_search = value ? 1 : 0; return BT_OK;
     case BT_OPT_SORTED_LEAF_VALS: H->h.sorted_leaf_vals = value ? 1 : 0; return BT_OK;
     case BT_OPT_FRONT_END: H->h.front_end = value ? 1 : 0; return BT_OK;
+    case BT_OPT_ASYNC_WRITE: H->h.async_write = value ? 1 : 0; return BT_OK;
     case BT_OPT_TOP_CACHE: H->h.top_cache = value ? 1 : 0; return BT_OK;
     case BT_OPT_OVERLAP:
       // 0 off; 1 on (default reserve); > 1 on, leaving value - 1 lookup block slots for the sort
@@ -525,6 +553,7 @@ int bt_autotune(bt_handle* H, const uint64_t* sample_keys, size_t n, void* strea
   DeviceGuard g(H->h.device);
   cudaStream_t s = stream ? S(stream) : H->h.internal_stream;
   if (stream == nullptr) cudaDeviceSynchronize();
+  if (bt::tree_join(&H->h, s) != cudaSuccess) return BT_ERR_CUDA;
   return map_internal(bt::autotune(&H->h, sample_keys, n, s, report));
 }
 

@@ -316,12 +316,10 @@ __global__ void __launch_bounds__(kThreads) merge_pass3(
   }
 }
 
-// cond (optional): write only when *cond is nonzero (the kNoCapacity fix-up)
 __global__ void writeback_kernel(const uint32_t* __restrict__ sv, const uint32_t* __restrict__ pend, size_t n,
                                  const uint32_t* __restrict__ n_dev, const uint64_t* __restrict__ uans,
                                  const uint8_t* __restrict__ uans_st, uint64_t* __restrict__ out_vals,
-                                 uint8_t* __restrict__ out_st, const uint32_t* __restrict__ cond) {
-  if (cond && *cond == 0) return;
+                                 uint8_t* __restrict__ out_st) {
   if (n_dev) n = min(n, (size_t)*n_dev);
   const size_t stride = (size_t)gridDim.x * blockDim.x;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
@@ -360,6 +358,7 @@ int work_alloc(Work* w, size_t cap) {
   A((void**)&w->tiles, tiles * sizeof(TileSummary));
   A((void**)&w->counts, sizeof(BatchCounts));
   A((void**)&w->m_path, cap * 32);
+  A((void**)&w->m_vpos, cap * 8);
   A((void**)&w->m_leaf, cap * 4);
   A((void**)&w->m_isnew, cap * 4);
   A((void**)&w->m_pos, cap * 4);
@@ -401,7 +400,7 @@ int work_alloc(Work* w, size_t cap) {
 void work_free(Work* w) {
   void* ps[] = {w->k_a,      w->k_b,       w->v_a,       w->v_b,       w->sort_scratch, w->ukeys,   w->uvals,
                 w->uans,     w->uans_st,   w->ins_list,  w->get_list,  w->del_list, w->pend,         w->tiles,   w->counts,
-                w->m_path,   w->m_leaf,    w->m_isnew,   w->m_pos,     w->m_newk,       w->m_newv,  w->m_nq,
+                w->m_path,   w->m_vpos,   w->m_leaf,    w->m_isnew,   w->m_pos,     w->m_newk,       w->m_newv,  w->m_nq,
                 w->m_nleaf,  w->m_seg,     w->d_leaf,    w->d_slot,    w->m_ent_a,   w->m_ent_b,   w->m_counts,     w->m_sync,      w->d_in_keys,
                 w->d_in_vals, w->d_in_ops, w->d_out_vals, w->d_out_st, w->f_tab, w->f_flags,
                 w->f_pos,    w->f_list,    w->f_tk,      w->f_tv};
@@ -418,17 +417,13 @@ static bool merge_usable(const Handle* h, int engine) {
 
 // write phase shared by both front ends: the unique DELETE runs (w.del_list,
 // count w.counts->n_del), then the unique INSERT runs of (w.ukeys, w.uvals,
-// w.ins_list, count w.counts->n_ins) reach the tree.  located: the merge
-// engine's and the delete phase's locates already ran.
-static int insert_phase(Handle* h, size_t n, int engine, bool located, cudaStream_t s) {
+// w.ins_list, count w.counts->n_ins) reach the tree.
+static int insert_phase(Handle* h, size_t n, int engine, cudaStream_t s) {
   Work& w = h->w;
   // the DELETE runs first: their keys differ from the INSERT runs' keys
-  if (!located && delete_locate(h, n, s) != 0) return -2;
+  if (delete_locate(h, n, s) != 0) return -2;
   if (delete_apply(h, n, s) != 0) return -2;
-  if (merge_usable(h, engine)) {
-    if (!located && merge_locate_phase(h, s) != 0) return -2;
-    return merge_apply_phase(h, n, s) != 0 ? -2 : 0;
-  }
+  if (merge_usable(h, engine)) return merge_engine(h, n, s) != 0 ? -2 : 0;
   const cudaError_t e =
       launch_stm(h, w.ukeys, w.uvals, nullptr, kOpInsert, w.ins_list, &w.counts->n_ins, n, w.uans, w.uans_st, s);
   return e == cudaSuccess ? 0 : -2;
@@ -438,8 +433,7 @@ static int wait_vals(Handle* h, cudaStream_t s) {
   return h->vals_wait && cudaStreamWaitEvent(s, h->vals_wait, 0) != cudaSuccess ? -2 : 0;
 }
 
-static int answers_ready(Handle* h, cudaStream_t s, const uint32_t* fix) {
-  h->ans_fix = fix;
+static int answers_ready(Handle* h, cudaStream_t s) {
   return h->ans_ready && cudaEventRecord(h->ans_ready, s) != cudaSuccess ? -2 : 0;
 }
 
@@ -447,58 +441,69 @@ static int answers_ready(Handle* h, cudaStream_t s, const uint32_t* fix) {
 // their key are sorted and merged; the rest are plain lookups of the
 // pre-batch tree, answered in place.  Same meaning as the full-sort path.
 //
-// Streams (overlap on): `s` runs the front end, then the lookups; a
-// high-priority side stream runs the touched requests' sort and merge passes
-// and, with the merge engine, the two locates (they read the pre-batch tree,
-// move no key and write only values of keys the lookups do not ask for) and
-// the write-back of the touched answers.  `s` waits for the side stream,
-// then the DELETE apply and the leaf/inner merge change the tree.  Every
-// answer is final before that write phase except kNoCapacity, which the
-// leaf merge sets on a full node pool; a second, conditional write-back
-// after it copies those.
+// Streams (overlap on): `s` runs the front end, the touched requests' sort
+// and merge passes, then the lookups; with the merge engine a high-priority
+// side stream runs the two locates and the grouping of the new keys by leaf
+// beside the lookups (the locates only read the pre-batch tree: a plain
+// lookup may ask for a key that a later request of the batch writes).  `s`
+// then waits for the side stream, writes the new values of existing keys,
+// applies the DELETE runs, reserves the leaf pieces (a full node pool
+// answers kNoCapacity here) and writes the touched answers back: every
+// answer is final before the leaf merge.  With async_write the leaf
+// and inner merge run on tree_stream, so the caller's stream goes on to the
+// next batch, whose front end and sort need neither the tree nor the merge
+// scratch; its first tree access waits for tree_ev.
 static int batch_hashed(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops,
                         uint64_t* out_vals, uint8_t* out_st, size_t n, int engine, cudaStream_t s) {
   Work& w = h->w;
   BatchCounts* c = w.counts;
   const uint32_t* n_touch = &c->n_touch;
-  prof_mark(h, 0, s);
-  if (front_classify(h, keys, ops, n, s) != 0) return -2;
   const bool ov = h->overlap != 0;
   const bool early = merge_usable(h, engine);
-  cudaStream_t s2 = ov ? h->hi_stream : s;
-  if (ov) {
-    prof_set_overlap(h);
-    prof_mark(h, 1, s);
-    if (cudaEventRecord(h->fork_ev, s) != cudaSuccess || cudaStreamWaitEvent(s2, h->fork_ev, 0) != cudaSuccess)
-      return -2;
-  }
+  const bool defer = early && h->async_write != 0;
+  prof_mark(h, 0, s);
+  prof_set_layout(h, (ov ? kLayoutOverlap : 0) | (early ? kLayoutEarly : 0));
+  if (front_classify(h, keys, ops, n, s) != 0) return -2;
+  // the touched requests' sort and merge passes need no tree: they run on
+  // `s` at full width (beside the previous batch's deferred merge)
   uint64_t* sk = nullptr;
   uint32_t* sv = nullptr;
-  if (radix_sort_pairs(w.f_tk, w.f_tv, nullptr, w.k_a, w.v_a, w.k_b, w.v_b, n, 0, 64, w.sort_scratch, s2, &sk, &sv,
+  if (radix_sort_pairs(w.f_tk, w.f_tv, nullptr, w.k_a, w.v_a, w.k_b, w.v_b, n, 0, 64, w.sort_scratch, s, &sk, &sv,
                        &h->tree.ctrl->error, n_touch) != cudaSuccess)
     return -2;
   const uint32_t n_tiles = (uint32_t)sort_tiles(n);
-  prof_mark(h, ov ? kEvSortEnd : 1, s2);
-  if (wait_vals(h, s2) != 0) return -2;
-  merge_pass1<<<n_tiles, kThreads, 0, s2>>>(sk, sv, vals, n, n_touch, w.tiles);
+  prof_mark(h, ov ? kEvSortEnd : 1, s);
+  // the locates (side stream) run beside the lookups (`s`); so do the merge
+  // passes when the values are still being copied in (vals_wait): the
+  // lookups do not need them
+  cudaStream_t s2 = ov ? h->hi_stream : s;
+  const bool pass_side = ov && h->vals_wait != nullptr;
+  auto fork = [&]() {
+    return cudaEventRecord(h->fork_ev, s) == cudaSuccess && cudaStreamWaitEvent(s2, h->fork_ev, 0) == cudaSuccess;
+  };
+  if (pass_side && !fork()) return -2;
+  cudaStream_t sp = pass_side ? s2 : s;
+  if (wait_vals(h, sp) != 0) return -2;
+  merge_pass1<<<n_tiles, kThreads, 0, sp>>>(sk, sv, vals, n, n_touch, w.tiles);
   count_launch();
-  merge_pass2<<<1, 1024, 0, s2>>>(w.tiles, n_tiles, n_touch, c);
+  merge_pass2<<<1, 1024, 0, sp>>>(w.tiles, n_tiles, n_touch, c);
   count_launch();
-  merge_pass3<<<n_tiles, kThreads, 0, s2>>>(sk, sv, vals, n, n_touch, w.tiles, w.ukeys, w.uvals, w.ins_list,
+  merge_pass3<<<n_tiles, kThreads, 0, sp>>>(sk, sv, vals, n, n_touch, w.tiles, w.ukeys, w.uvals, w.ins_list,
                                             w.get_list, w.del_list, w.pend, out_vals, out_st);
   count_launch();
   if (cudaGetLastError() != cudaSuccess) return -2;
-  const unsigned wb_blocks = (unsigned)min((size_t)h->sm_count * 8, (n + 255) / 256);
+  if (ov && !pass_side && !fork()) return -2;
   if (early) {
-    if (delete_locate(h, n, s2) != 0 || merge_locate_phase(h, s2) != 0) return -2;
-    writeback_kernel<<<wb_blocks, 256, 0, s2>>>(sv, w.pend, n, n_touch, w.uans, w.uans_st, out_vals, out_st,
-                                                nullptr);
-    count_launch();
+    if (tree_join(h, s2) != cudaSuccess || delete_locate(h, n, s2) != 0 || merge_locate_phase(h, s2) != 0 ||
+        merge_group_phase(h, n, s2) != 0)
+      return -2;
   }
   prof_mark(h, 2, s2);
   if (ov && cudaEventRecord(h->join_ev, s2) != cudaSuccess) return -2;
   // plain lookups of the pre-batch tree; every touched run begins with a
   // write, so the merged batch has no GET runs (n_get is zero)
+  if (tree_join(h, s) != cudaSuccess) return -2;
+  if (ov) prof_mark(h, 1, s);
   cudaError_t e;
   const int desc = h->batch_descent >= 0 ? h->batch_descent : h->descent;
   if (desc == 1 && h->L.valid)
@@ -513,25 +518,45 @@ static int batch_hashed(Handle* h, const uint64_t* keys, const uint64_t* vals, c
     prof_mark(h, kEvLookupEnd, s);
     if (cudaStreamWaitEvent(s, h->join_ev, 0) != cudaSuccess) return -2;
   }
-  if (early && answers_ready(h, s, merge_fail_flag(h)) != 0) return -2;
   prof_mark(h, 3, s);
-  if (insert_phase(h, n, engine, early, s) != 0) return -2;
-  prof_mark(h, 4, s);
-  writeback_kernel<<<wb_blocks, 256, 0, s>>>(sv, w.pend, n, n_touch, w.uans, w.uans_st, out_vals, out_st,
-                                             early ? merge_fail_flag(h) : nullptr);
+  const unsigned wb_blocks = (unsigned)min((size_t)h->sm_count * 8, (n + 255) / 256);
+  if (!early) {
+    if (insert_phase(h, n, engine, s) != 0) return -2;
+    prof_mark(h, 4, s);
+    writeback_kernel<<<wb_blocks, 256, 0, s>>>(sv, w.pend, n, n_touch, w.uans, w.uans_st, out_vals, out_st);
+    count_launch();
+    prof_mark(h, 5, s);
+    return answers_ready(h, s) != 0 || cudaGetLastError() != cudaSuccess ? -2 : 0;
+  }
+  if (merge_update_phase(h, n, s) != 0 || delete_apply(h, n, s) != 0 || merge_reserve_phase(h, n, s) != 0)
+    return -2;
+  prof_mark(h, kEvWbStart, s);
+  writeback_kernel<<<wb_blocks, 256, 0, s>>>(sv, w.pend, n, n_touch, w.uans, w.uans_st, out_vals, out_st);
   count_launch();
-  prof_mark(h, 5, s);
-  if (!early && answers_ready(h, s, nullptr) != 0) return -2;
+  prof_mark(h, 4, s);
+  if (answers_ready(h, s) != 0 || cudaGetLastError() != cudaSuccess) return -2;
+  cudaStream_t t = s;
+  if (defer) {
+    t = h->tree_stream;
+    if (cudaEventRecord(h->ans_ev, s) != cudaSuccess || cudaStreamWaitEvent(t, h->ans_ev, 0) != cudaSuccess)
+      return -2;
+  }
+  if (merge_write_phase(h, t) != 0) return -2;
+  prof_mark(h, 5, t);
+  if (defer) {
+    if (cudaEventRecord(h->tree_ev, t) != cudaSuccess) return -2;
+    h->tree_pending = true;
+  }
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
 int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, uint64_t* out_vals,
                  uint8_t* out_st, size_t n, int engine, cudaStream_t s) {
-  h->ans_fix = nullptr;
   if (n == 0) return 0;
   Work& w = h->w;
   if (n > w.cap || n > kIdxMask) return -6;
   if (h->front_end == 1) return batch_hashed(h, keys, vals, ops, out_vals, out_st, n, engine, s);
+  if (tree_join(h, s) != cudaSuccess) return -2;
   uint64_t* sk = nullptr;
   uint32_t* sv = nullptr;
   prof_mark(h, 0, s);
@@ -562,13 +587,13 @@ int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const ui
     e = launch_search(h, w.ukeys, w.get_list, &w.counts->n_get, n, w.uans, w.uans_st, s);
   if (e != cudaSuccess) return -2;
   prof_mark(h, 3, s);
-  if (insert_phase(h, n, engine, false, s) != 0) return -2;
+  if (insert_phase(h, n, engine, s) != 0) return -2;
   prof_mark(h, 4, s);
   const unsigned wb_blocks = (unsigned)min((size_t)h->sm_count * 8, (n + 255) / 256);
-  writeback_kernel<<<wb_blocks, 256, 0, s>>>(sv, w.pend, n, nullptr, w.uans, w.uans_st, out_vals, out_st, nullptr);
+  writeback_kernel<<<wb_blocks, 256, 0, s>>>(sv, w.pend, n, nullptr, w.uans, w.uans_st, out_vals, out_st);
   count_launch();
   prof_mark(h, 5, s);
-  if (answers_ready(h, s, nullptr) != 0) return -2;
+  if (answers_ready(h, s) != 0) return -2;
   if (cudaGetLastError() != cudaSuccess) return -2;
   return 0;
 }

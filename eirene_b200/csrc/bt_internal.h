@@ -18,11 +18,14 @@ inline void count_launch(unsigned n = 1) { g_launches.fetch_add(n, std::memory_o
 // phases timed with CUDA events when profiling is on (the reference's
 // Time_Measure phases, src/gpu-stm-tree-v38/bpt-gpustm-kernel.cu:289-324)
 enum Phase { kPhSort = 0, kPhMerge, kPhSearch, kPhInsert, kPhWriteback, kNumPhases };
-// boundary events per batch: 0..kNumPhases in order, plus two for the
-// overlapped layout (end of the touched sort on the side stream, end of the
-// lookups on the main stream)
-constexpr int kProfEvents = kNumPhases + 3;
-constexpr int kEvSortEnd = kNumPhases + 1, kEvLookupEnd = kNumPhases + 2;
+// boundary events per batch: 0..kNumPhases in order, plus three for the
+// other layouts (end of the touched sort on the side stream, end of the
+// lookups on the main stream, start of the write-back before the leaf merge)
+constexpr int kProfEvents = kNumPhases + 4;
+constexpr int kEvSortEnd = kNumPhases + 1, kEvLookupEnd = kNumPhases + 2, kEvWbStart = kNumPhases + 3;
+// per-batch event layout bits (prof_resolve)
+constexpr int kLayoutOverlap = 1;  // sort and merge passes on the side stream, beside the lookups
+constexpr int kLayoutEarly = 2;    // answers written back before the leaf merge
 
 // ---- scan / sort (bt_sort.cu) ----
 size_t scan_scratch_words(size_t n);
@@ -80,6 +83,7 @@ struct Work {
   BatchCounts* counts = nullptr;
   // segmented leaf merge (bt_merge.cu)
   uint32_t* m_path = nullptr;   // [cap][8] root-to-leaf path of each unique insert
+  uint64_t* m_vpos = nullptr;   // [cap] value slot (node * 32 + slot) of an existing key, or ~0
   uint32_t* m_leaf = nullptr;
   uint32_t* m_isnew = nullptr;
   uint32_t* m_pos = nullptr;
@@ -167,7 +171,7 @@ struct Handle {
   // profiling: one event per phase boundary per batch, resolved on read
   bool prof = false;
   std::vector<cudaEvent_t> prof_ev;  // kProfEvents events per recorded batch
-  std::vector<char> prof_overlap;    // per recorded batch: lookups overlapped the sort (see prof_resolve)
+  std::vector<char> prof_layout;     // per recorded batch: kLayout* bits (see prof_resolve)
   size_t prof_batches = 0;
   // hash front end: the touched requests' sort + merge run on a high-priority
   // side stream while the lookups run on the caller's stream
@@ -180,23 +184,35 @@ struct Handle {
   // their own stream, overlapped with the batch's kernels
   cudaStream_t xfer_stream = nullptr;
   cudaEvent_t xfer_keys_ev = nullptr, xfer_vals_ev = nullptr, xfer_ans_ev = nullptr;
-  uint32_t* host_word = nullptr;  // pinned host word (answer fix-up flag)
   // per-batch hooks of the sorted batch, set by the host-buffer entry point:
   // the stream that first reads `vals` waits for vals_wait; ans_ready is
-  // recorded once every answer is in the output arrays, except the
-  // kNoCapacity fix-up signalled by *ans_fix (nullptr: no fix-up pending)
+  // recorded once every answer is in the output arrays
   cudaEvent_t vals_wait = nullptr;
   cudaEvent_t ans_ready = nullptr;
-  const uint32_t* ans_fix = nullptr;
+  // deferred write phase: a sorted batch (hash front end, merge engine)
+  // completes on the caller's stream once its answers are final and leaves
+  // the leaf/inner merge on tree_stream; tree_ev marks its end.  Every later
+  // access to the tree or the merge scratch waits for tree_ev first
+  // (tree_join on a stream, tree_sync on the host).
+  cudaStream_t tree_stream = nullptr;
+  cudaEvent_t tree_ev = nullptr;
+  cudaEvent_t ans_ev = nullptr;
+  bool tree_pending = false;
+  int async_write = 1;
   double phase_ms[kNumPhases] = {};
   unsigned long long phase_batches = 0;
   unsigned long long phase_items[kNumPhases] = {};
 };
 
+// make stream `s` wait for the deferred write phase (no-op when none is pending)
+cudaError_t tree_join(Handle* h, cudaStream_t s);
+// block the host until the deferred write phase has finished
+cudaError_t tree_sync(Handle* h);
+
 // record the boundary event `which` (0..kProfEvents-1) of the current batch;
 // event kNumPhases closes the batch, so the extra events come before it
 void prof_mark(Handle* h, int which, cudaStream_t s);
-void prof_set_overlap(Handle* h);
+void prof_set_layout(Handle* h, int layout);
 
 // ---- tree kernels (bt_tree.cu) ----
 cudaError_t tree_reset(Handle* h, cudaStream_t s);
@@ -286,13 +302,21 @@ int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const ui
 
 // ---- segmented leaf merge (bt_merge.cu) ----
 int merge_engine(Handle* h, size_t n_upper, cudaStream_t s);
-// the same in two parts: locate (descents of the pre-batch tree, answers of
-// the INSERT runs, in-place value updates of existing keys; no key moves)
-// and apply (leaf merge and inner levels).  merge_fail_flag is nonzero after
-// apply when the node pool could not take the batch's new keys.
+// the same in five parts:
+//   locate   descents of the pre-batch tree, answers of the INSERT runs
+//            (reads the tree only);
+//   update   new values of the existing keys, in place (after the batch's
+//            plain lookups, before its DELETE apply);
+//   group    the new keys and their runs per leaf (no tree access);
+//   reserve  pieces per touched leaf (reads leaf sizes: after the DELETE
+//            apply), node reservation, kNoCapacity answers when it fails;
+//   write    leaf merge and inner levels: reads only the merge scratch
+//            (m_*), so the next batch's front end and sort may run beside it.
 int merge_locate_phase(Handle* h, cudaStream_t s);
-int merge_apply_phase(Handle* h, size_t n_upper, cudaStream_t s);
-const uint32_t* merge_fail_flag(Handle* h);
+int merge_update_phase(Handle* h, size_t n_upper, cudaStream_t s);
+int merge_group_phase(Handle* h, size_t n_upper, cudaStream_t s);
+int merge_reserve_phase(Handle* h, size_t n_upper, cudaStream_t s);
+int merge_write_phase(Handle* h, cudaStream_t s);
 
 // device view of the learned model when the learned descent is on and trained
 struct LearnedDev;

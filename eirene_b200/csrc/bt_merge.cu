@@ -6,7 +6,9 @@
 // With the batch's unique INSERT keys in ascending order:
 //   locate    each 8-lane group walks a contiguous run of the keys (path reuse,
 //             as in the sorted search), records the root-to-leaf path, answers
-//             the previous value and updates existing keys in place;
+//             the previous value and records where an existing key's value
+//             lives;
+//   update    writes the new values of the existing keys in place;
 //   compact   the new keys, then runs of new keys sharing a leaf (segments);
 //   leaf      one 8-lane group per touched leaf merges its new keys by rank scatter
 //             (each element computes its merged position by binary search in
@@ -17,10 +19,9 @@
 //             (children spread evenly over q = ceil((s+1)/(inner_fill+1))
 //             nodes, the key between two pieces moves up) and rebuilds an
 //             overflowing root with the bulk-load rule.
-// Locate moves no key and writes only the values of keys that the batch
-// inserts, so it may run beside the lookups of the keys the batch does not
-// write (the hash front end does so); compact, leaf and inner run alone, so
-// no locks are taken.  The rules are
+// Locate only reads the tree, so it may run beside the batch's plain
+// lookups (the hash front end does so); the in-place value update, compact,
+// leaf and inner run after them and alone, so no locks are taken.  The rules are
 // restated by the CPU oracle (bto_execute_merged with BTO_ENGINE_MERGE) and
 // the resulting leaf layout is compared exactly.
 #include <cuda_runtime.h>
@@ -50,6 +51,7 @@ struct MergeCounts {
 namespace {
 
 constexpr int kPathLevels = 8;
+constexpr uint64_t kNoPos = ~0ull;  // merge_locate_kernel: no value to update in place
 constexpr unsigned kFull = 0xffffffffu;
 
 __device__ __forceinline__ uint32_t ceil_div(uint32_t a, uint32_t b) { return (a + b - 1) / b; }
@@ -114,7 +116,8 @@ __global__ void __launch_bounds__(256) merge_locate_kernel(DevTree t, const uint
                                                            const uint32_t* __restrict__ ins_list,
                                                            const uint32_t* __restrict__ n_dev,
                                                            uint32_t* __restrict__ path, uint32_t* __restrict__ mleaf,
-                                                           uint32_t* __restrict__ isnew, uint64_t* __restrict__ uans,
+                                                           uint32_t* __restrict__ isnew,
+                                                           uint64_t* __restrict__ vpos, uint64_t* __restrict__ uans,
                                                            uint8_t* __restrict__ uans_st) {
   constexpr int S = 32 / G;
   const uint32_t lane = threadIdx.x & 31;
@@ -144,6 +147,7 @@ __global__ void __launch_bounds__(256) merge_locate_kernel(DevTree t, const uint
         uans[u] = 0;
         uans_st[u] = kNoCapacity;
         isnew[q] = 0;
+        vpos[q] = kNoPos;
       }
       continue;
     }
@@ -197,18 +201,34 @@ __global__ void __launch_bounds__(256) merge_locate_kernel(DevTree t, const uint
     }
     if (g == 0) {
       if (exists) {
-        uint64_t* vp = t.vals + (size_t)leaf * 32 + slot;
-        uans[u] = *vp;
+        // the new value goes in later (merge_update_kernel): a plain lookup
+        // of this key that comes before its first write must still see it
+        const uint64_t p = (uint64_t)leaf * 32 + slot;
+        uans[u] = t.vals[p];
         uans_st[u] = kFound;
-        *vp = uvals[u];  // update in place; keys do not move
+        vpos[q] = p;
         isnew[q] = 0;
       } else {
         uans[u] = 0;
         uans_st[u] = kAbsent;
         isnew[q] = 1;
+        vpos[q] = kNoPos;
         mleaf[q] = leaf;
       }
     }
+  }
+}
+
+// new values of the keys the batch finds in the tree, in place (keys do not
+// move); after the batch's plain lookups, before its DELETE apply
+__global__ void merge_update_kernel(DevTree t, const uint64_t* __restrict__ uvals,
+                                    const uint32_t* __restrict__ ins_list, const uint32_t* __restrict__ n_dev,
+                                    const uint64_t* __restrict__ vpos) {
+  const size_t n = *n_dev;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) {
+    const uint64_t p = vpos[q];
+    if (p != kNoPos) t.vals[p] = uvals[ins_list[q]];
   }
 }
 
@@ -291,6 +311,16 @@ __global__ void merge_alloc_kernel(DevTree t, MergeCounts* mc, uint32_t entry_ca
   mc->node_base = atomicAdd(&t.ctrl->n_nodes, T);
 }
 
+// a batch whose pieces did not fit answers kNoCapacity for all its new keys
+__global__ void merge_fail_mark_kernel(const MergeCounts* __restrict__ mc, const uint32_t* __restrict__ nq,
+                                       const uint32_t* __restrict__ ins_list, uint8_t* __restrict__ uans_st) {
+  if (mc->cap_fail == 0) return;
+  const uint32_t n_new = mc->n_new;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_new; i += stride)
+    uans_st[ins_list[nq[i]]] = kNoCapacity;
+}
+
 // ------------------------------------------------------------- leaf ----
 // One group of G lanes per touched leaf (segment); lane g holds slots
 // g*S .. g*S+S-1 of the row.  Several leaves per warp keep more row loads in
@@ -304,9 +334,7 @@ __global__ void __launch_bounds__(256) merge_leaf_kernel(DevTree t, uint32_t lea
                                                          const uint64_t* __restrict__ newv,
                                                          const uint32_t* __restrict__ nq,
                                                          const uint32_t* __restrict__ seg_leaf,
-                                                         const uint32_t* __restrict__ ins_list,
-                                                         MergeEntry* __restrict__ ent, uint64_t* __restrict__ uans,
-                                                         uint8_t* __restrict__ uans_st) {
+                                                         MergeEntry* __restrict__ ent) {
   constexpr int S = 32 / G;
   __shared__ uint64_t s_keys[256 / G][32];
   const uint32_t lane = threadIdx.x & 31;
@@ -323,10 +351,7 @@ __global__ void __launch_bounds__(256) merge_leaf_kernel(DevTree t, uint32_t lea
     seg_bounds(mc, seg_start, s, a, b);
     const uint32_t leaf = seg_leaf[s];
     const uint32_t cnt = b - a;
-    if (fail) {
-      for (uint32_t j = g; j < cnt; j += G) uans_st[ins_list[nq[a + j]]] = kNoCapacity;
-      continue;
-    }
+    if (fail) continue;  // merge_fail_mark_kernel answered these keys
     uint64_t ok[S], ov[S];
     load_slots<S>(t.keys + (size_t)leaf * 32 + g * S, ok);
     load_slots<S>(t.vals + (size_t)leaf * 32 + g * S, ov);
@@ -723,12 +748,20 @@ int merge_locate_phase(Handle* h, cudaStream_t s) {
   }
   const size_t blocks = (size_t)h->sm_count * (h->device < 64 ? per_sm[h->device] : 4);
   merge_locate_kernel<8><<<(unsigned)blocks, 256, 0, s>>>(h->tree, w.ukeys, w.uvals, w.ins_list, n_ins, w.m_path,
-                                                          w.m_leaf, w.m_isnew, w.uans, w.uans_st);
+                                                          w.m_leaf, w.m_isnew, w.m_vpos, w.uans, w.uans_st);
   count_launch();
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
-int merge_apply_phase(Handle* h, size_t n_upper, cudaStream_t s) {
+int merge_update_phase(Handle* h, size_t n_upper, cudaStream_t s) {
+  Work& w = h->w;
+  const unsigned gb = (unsigned)min((size_t)h->sm_count * 8, (n_upper + 255) / 256);
+  merge_update_kernel<<<gb, 256, 0, s>>>(h->tree, w.uvals, w.ins_list, &w.counts->n_ins, w.m_vpos);
+  count_launch();
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int merge_group_phase(Handle* h, size_t n_upper, cudaStream_t s) {
   Work& w = h->w;
   MergeCounts* mc = reinterpret_cast<MergeCounts*>(w.m_counts);
   const uint32_t* n_ins = &w.counts->n_ins;
@@ -741,26 +774,42 @@ int merge_apply_phase(Handle* h, size_t n_upper, cudaStream_t s) {
   if (scan_exclusive_u32(w.m_isnew, w.m_pos, n_upper, &mc->n_segs, w.sort_scratch, s, &mc->n_new) != cudaSuccess)
     return -2;
   merge_seg_start_kernel<<<gb, 256, 0, s>>>(mc, w.m_isnew, w.m_pos, w.m_nleaf, w.m_seg, w.m_leaf);
+  count_launch();
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int merge_reserve_phase(Handle* h, size_t n_upper, cudaStream_t s) {
+  Work& w = h->w;
+  MergeCounts* mc = reinterpret_cast<MergeCounts*>(w.m_counts);
+  const unsigned gb = (unsigned)min((size_t)h->sm_count * 8, (n_upper + 255) / 256);
   merge_leaf_count_kernel<<<gb, 256, 0, s>>>(h->tree, h->leaf_fill, mc, w.m_seg, w.m_nleaf, n_upper, w.m_isnew);
-  count_launch(2);
+  count_launch();
   if (scan_exclusive_u32(w.m_isnew, w.m_pos, n_upper, &mc->n_leaf_entries, w.sort_scratch, s, &mc->n_segs) !=
       cudaSuccess)
     return -2;
-  const uint32_t entry_cap = (uint32_t)w.cap;
-  merge_alloc_kernel<<<1, 1, 0, s>>>(h->tree, mc, entry_cap);
-  merge_leaf_kernel<8><<<(unsigned)((size_t)h->sm_count * 8), 256, 0, s>>>(
-      h->tree, h->leaf_fill, mc, w.m_seg, w.m_pos, w.m_newk, w.m_newv, w.m_nq, w.m_leaf, w.ins_list,
-      reinterpret_cast<MergeEntry*>(w.m_ent_a), w.uans, w.uans_st);
+  merge_alloc_kernel<<<1, 1, 0, s>>>(h->tree, mc, (uint32_t)w.cap);
+  merge_fail_mark_kernel<<<gb, 256, 0, s>>>(mc, w.m_nq, w.ins_list, w.uans_st);
   count_launch(2);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int merge_write_phase(Handle* h, cudaStream_t s) {
+  Work& w = h->w;
+  MergeCounts* mc = reinterpret_cast<MergeCounts*>(w.m_counts);
+  const uint32_t entry_cap = (uint32_t)w.cap;
+  merge_leaf_kernel<8><<<(unsigned)((size_t)h->sm_count * 8), 256, 0, s>>>(
+      h->tree, h->leaf_fill, mc, w.m_seg, w.m_pos, w.m_newk, w.m_newv, w.m_nq, w.m_leaf,
+      reinterpret_cast<MergeEntry*>(w.m_ent_a));
+  count_launch();
   if (launch_inner(h, entry_cap, mc, s) != cudaSuccess) return -2;
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
-const uint32_t* merge_fail_flag(Handle* h) { return &reinterpret_cast<MergeCounts*>(h->w.m_counts)->cap_fail; }
-
 int merge_engine(Handle* h, size_t n_upper, cudaStream_t s) {
-  if (merge_locate_phase(h, s) != 0) return -2;
-  return merge_apply_phase(h, n_upper, s);
+  if (merge_locate_phase(h, s) != 0 || merge_update_phase(h, n_upper, s) != 0 ||
+      merge_group_phase(h, n_upper, s) != 0 || merge_reserve_phase(h, n_upper, s) != 0)
+    return -2;
+  return merge_write_phase(h, s);
 }
 
 }  // namespace bt

@@ -28,6 +28,41 @@ __device__ __forceinline__ void load_slots(const uint64_t* p, uint64_t (&x)[S]) 
   }
 }
 
+// L2 eviction priorities for the descent (createpolicy + ld.global.nc with
+// an L2 cache hint, PTX ISA 7.4+): inner rows are read by every lookup and
+// should stay in L2 (evict_last); a leaf row or value is read once per
+// lookup and should not push them out (evict_first).
+__device__ __forceinline__ uint64_t l2_keep() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+__device__ __forceinline__ uint64_t l2_stream() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+__device__ __forceinline__ uint64_t ldg_hint(const uint64_t* p, uint64_t pol) {
+  uint64_t r;
+  asm("ld.global.nc.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(r) : "l"(p), "l"(pol));
+  return r;
+}
+
+template <int S>
+__device__ __forceinline__ void load_slots_hint(const uint64_t* p, uint64_t (&x)[S], uint64_t pol) {
+  if constexpr (S == 1) {
+    x[0] = ldg_hint(p, pol);
+  } else {
+#pragma unroll
+    for (int i = 0; i < S; i += 2)
+      asm("ld.global.nc.L2::cache_hint.v2.u64 {%0, %1}, [%2], %3;"
+          : "=l"(x[i]), "=l"(x[i + 1])
+          : "l"(p + i), "l"(pol));
+  }
+}
+
 template <int S>
 __device__ __forceinline__ uint64_t pick(const uint64_t (&x)[S], uint32_t e) {
   uint64_t r = x[0];
@@ -102,10 +137,17 @@ __device__ __forceinline__ void group_descend2(const DevTree& t, uint32_t node, 
   uint64_t ka[S], va[S], kb[S], vb[S];
   uint32_t na = node, nb = node;
   uint32_t ca, cb;
+  const uint64_t keep = l2_keep(), stream = l2_stream();
   for (;;) {
     const size_t ra = (size_t)na * 32 + g * S, rb = (size_t)nb * 32 + g * S;
-    load_slots<S>(t.keys + ra, ka);
-    load_slots<S>(t.keys + rb, kb);
+    if (kChild) {
+      const uint64_t pol = level > 0 ? keep : stream;
+      load_slots_hint<S>(t.keys + ra, ka, pol);
+      load_slots_hint<S>(t.keys + rb, kb, pol);
+    } else {
+      load_slots<S>(t.keys + ra, ka);
+      load_slots<S>(t.keys + rb, kb);
+    }
     if ((level > 0 && !kChild) || (level == 0 && kLeafVals)) {
       load_slots<S>(t.vals + ra, va);
       load_slots<S>(t.vals + rb, vb);
@@ -124,10 +166,8 @@ __device__ __forceinline__ void group_descend2(const DevTree& t, uint32_t node, 
     cb = group_sum<G>(xb, gmask);
     if (level == 0) break;
     if (kChild) {
-      const uint64_t* ca_p = t.vals + (size_t)na * 32 + ca;
-      const uint64_t* cb_p = t.vals + (size_t)nb * 32 + cb;
-      na = (uint32_t)__ldg(ca_p);
-      nb = (uint32_t)__ldg(cb_p);
+      na = (uint32_t)ldg_hint(t.vals + (size_t)na * 32 + ca, keep);
+      nb = (uint32_t)ldg_hint(t.vals + (size_t)nb * 32 + cb, keep);
     } else {
       const uint64_t ma = pick<S>(va, ca % S), mb = pick<S>(vb, cb % S);
       na = (uint32_t)__shfl_sync(gmask, ma, ca / S, G);
@@ -148,8 +188,8 @@ __device__ __forceinline__ void group_descend2(const DevTree& t, uint32_t node, 
     ans_a = fa ? xa : 0;
     ans_b = fb ? xb : 0;
   } else if (g == 0) {
-    if (fa) ans_a = __ldg(t.vals + (size_t)na * 32 + sa);
-    if (fb) ans_b = __ldg(t.vals + (size_t)nb * 32 + sb);
+    if (fa) ans_a = kChild ? ldg_hint(t.vals + (size_t)na * 32 + sa, stream) : __ldg(t.vals + (size_t)na * 32 + sa);
+    if (fb) ans_b = kChild ? ldg_hint(t.vals + (size_t)nb * 32 + sb, stream) : __ldg(t.vals + (size_t)nb * 32 + sb);
   }
   st_a = fa ? kFound : kAbsent;
   st_b = fb ? kFound : kAbsent;

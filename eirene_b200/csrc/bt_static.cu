@@ -90,6 +90,7 @@ extern "C" int bt_bulk_build_static(bt_handle* H, const uint64_t* keys, const ui
   if (prev != dev && cudaSetDevice(dev) != cudaSuccess) return BT_ERR_CUDA;
   unsigned char* base = nullptr;
   int rc = scratch_for_device(dev, &base);
+  if (rc == BT_OK && bt::tree_join(&H->h, static_cast<cudaStream_t>(stream)) != cudaSuccess) rc = BT_ERR_CUDA;
   if (rc == BT_OK) {
     if (bt::sort_scratch_words(n ? n : 1) > kSortWords) {
       rc = BT_ERR_STATIC_LIMIT;

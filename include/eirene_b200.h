@@ -211,7 +211,21 @@ int bt_set_search_group(bt_handle *h, uint32_t lanes);
                                 * loading only the chosen child id at inner levels (half the bytes of a full
                                 * row, one more dependent load); 1 the pairs with full rows; 0 one request
                                 * per group.  Nonzero takes precedence over BT_OPT_TOP_CACHE */
+#define BT_OPT_ASYNC_WRITE 10  /* 1 (default): a BT_MODE_SORTED | BT_MODE_MERGE_ENGINE batch with the hash front
+                                * end completes on the caller's stream once its answers are final; its leaf and
+                                * inner merge finish on an internal stream, beside the next batch's front end and
+                                * sort.  Every later call on this handle, on any stream, waits for them before it
+                                * touches the tree (bt_sync waits explicitly); 0 the merge runs on the caller's
+                                * stream.  Same answers and tree. */
 int bt_set_option(bt_handle *h, int option, int64_t value);
+/* Orders work after every batch issued so far on this handle, its deferred
+ * leaf/inner merge included (BT_OPT_ASYNC_WRITE): with a stream, the stream
+ * waits; with NULL, the host blocks.  A CUDA stream sync or event on the
+ * caller's stream covers a batch's answers but not its deferred merge; the
+ * library's own calls need no bt_sync.  No reference counterpart (the
+ * reference synchronises after every batch kernel, src/gpu-stm-tree-v38/
+ * bpt-gpustm-kernel.cu:289-324). */
+int bt_sync(bt_handle *h, void *stream);
 /* Autotuner: times the lookup configurations on this tree with n sample keys
  * (device pointer, n <= max_batch) and keeps the fastest: lanes per request of
  * the plain and the learned search, the sorted search's leaf-value load, and
