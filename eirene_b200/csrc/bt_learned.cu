@@ -334,7 +334,8 @@ __global__ void __launch_bounds__(256, 6) learned_search_kernel(DevTree t, Learn
   unsigned long long hits = 0, falls = 0, probe = 0;
   uint32_t leaf = kNil;
   uint64_t fence = 0;
-  uint64_t k[S], v[S];
+  uint64_t k[S];
+  const uint64_t stream = l2_stream();
   for (; q < q_end; q += stride) {
     const uint32_t r = list ? __ldg(list + q) : (uint32_t)q;
     const uint64_t key = __ldg(qkeys + r);
@@ -348,8 +349,9 @@ __global__ void __launch_bounds__(256, 6) learned_search_kernel(DevTree t, Learn
         uint32_t dist = 0;
         const uint32_t node = learned_leaf<G>(M, p, key, g, gmask, dist);
         if (node != kNil) {
-          load_slots<S>(t.keys + (size_t)node * 32 + g * S, k);
-          fence = __shfl_sync(gmask, g == G - 1 ? __ldg(t.vals + (size_t)node * 32 + 31) : 0, G - 1, G);
+          // a leaf row is read once per lookup: let it leave L2 first
+          load_slots_hint<S>(t.keys + (size_t)node * 32 + g * S, k, stream);
+          fence = __shfl_sync(gmask, g == G - 1 ? ldg_hint(t.vals + (size_t)node * 32 + 31, stream) : 0, G - 1, G);
           if (g == G - 1) k[S - 1] = kKeyMax;
           leaf = node;
           have = key < fence;  // the leaf may have split since training
@@ -364,7 +366,7 @@ __global__ void __launch_bounds__(256, 6) learned_search_kernel(DevTree t, Learn
 #pragma unroll
         for (int i = 0; i < S; i++) c += (k[i] <= key) ? 1u : 0u;
         c = group_sum<G>(c, gmask);
-        st = group_leaf_lookup<G, false>(t, leaf, key, g, gmask, k, v, c, ans);
+        st = group_leaf_lookup_hint<G>(t, leaf, key, g, gmask, k, c, stream, ans);
       } else {
         falls++;
         leaf = kNil;

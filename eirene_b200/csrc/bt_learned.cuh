@@ -87,10 +87,12 @@ __device__ __forceinline__ uint32_t learned_leaf(const LearnedDev& M, const floa
   p0 = p0 > L - G ? L - G : p0;
   p0 = p0 < 0 ? 0 : p0;
   const int e = p0 + (int)g;
+  // the leaf table is read by every lookup: keep it in L2
+  const uint64_t keep = l2_keep();
   ulonglong2 ent = make_ulonglong2(kKeyMax, 0);
-  if (e <= L) ent = __ldg(reinterpret_cast<const ulonglong2*>(M.tab) + e);
+  if (e <= L) ent = ldg2_hint(reinterpret_cast<const ulonglong2*>(M.tab) + e, keep);
   uint64_t above = kKeyMax;
-  if (g == 0 && p0 + G <= L) above = __ldg(&M.tab[p0 + G].low);
+  if (g == 0 && p0 + G <= L) above = ldg_hint(&M.tab[p0 + G].low, keep);
   above = __shfl_sync(gmask, above, 0, G);
   const uint32_t c = group_sum<G>(ent.x <= key ? 1u : 0u, gmask);
   const uint32_t node = (uint32_t)__shfl_sync(gmask, ent.y, (c + G - 1) % G, G);

@@ -50,6 +50,12 @@ __device__ __forceinline__ uint64_t ldg_hint(const uint64_t* p, uint64_t pol) {
   return r;
 }
 
+__device__ __forceinline__ ulonglong2 ldg2_hint(const void* p, uint64_t pol) {
+  ulonglong2 r;
+  asm("ld.global.nc.L2::cache_hint.v2.u64 {%0, %1}, [%2], %3;" : "=l"(r.x), "=l"(r.y) : "l"(p), "l"(pol));
+  return r;
+}
+
 template <int S>
 __device__ __forceinline__ void load_slots_hint(const uint64_t* p, uint64_t (&x)[S], uint64_t pol) {
   if constexpr (S == 1) {
@@ -94,6 +100,22 @@ __device__ __forceinline__ uint8_t group_leaf_lookup(const DevTree& t, uint32_t 
   if (kk != key) return kAbsent;
   if (kLeafVals) ans = __shfl_sync(gmask, pick<S>(v, e), owner, G);
   else ans = (g == 0) ? __ldg(t.vals + (size_t)node * 32 + slot) : 0;
+  return kFound;
+}
+
+// The same for a leaf row loaded without its values, with the value load
+// given L2 eviction policy `pol`.
+template <int G>
+__device__ __forceinline__ uint8_t group_leaf_lookup_hint(const DevTree& t, uint32_t node, uint64_t key, uint32_t g,
+                                                          uint32_t gmask, const uint64_t (&k)[32 / G], uint32_t cnt,
+                                                          uint64_t pol, uint64_t& ans) {
+  constexpr int S = 32 / G;
+  ans = 0;
+  if (cnt == 0) return kAbsent;
+  const uint32_t slot = cnt - 1;
+  const uint64_t kk = __shfl_sync(gmask, pick<S>(k, slot % S), slot / S, G);
+  if (kk != key) return kAbsent;
+  ans = (g == 0) ? ldg_hint(t.vals + (size_t)node * 32 + slot, pol) : 0;
   return kFound;
 }
 
