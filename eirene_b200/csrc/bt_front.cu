@@ -11,8 +11,8 @@
 //   2. records, per written key, the index of its first write,
 //   3. classifies every request: "touched" if its op code is invalid or its
 //      key has a write at or before it; otherwise it is a plain lookup,
-//      and compacts both classes in input order, in one pass with a
-//      decoupled look-back over tiles.
+//      and compacts both classes in input order (a flag pass, a scan of
+//      the per-tile counts, a scatter pass).
 //
 // The touched requests go through the sort + segmented-scan path (their
 // runs all start with a write, so the pre-batch value reaches them from the
@@ -21,9 +21,9 @@
 // read-mostly batch the sort shrinks to the INSERTs.
 //
 // HBM traffic per request: count (1 B op), table insert (1 B op, plus the key
-// of an INSERT), classify + compaction (8 B key + 1 B op + the probe, which is
-// L2-resident for small INSERT counts, then 4 B list entry or 12 B touched
-// entry).
+// of a write), flag (8 B key + 1 B op + the probe, which is L2-resident for
+// small write counts, then a 1 B flag), scatter (1 B flag, then a 4 B list
+// entry, or 9 B read and a 12 B touched entry).
 #include <cuda_runtime.h>
 
 #include "bt_block.cuh"
@@ -132,148 +132,170 @@ __device__ __forceinline__ uint32_t find_first_from(const Slot* __restrict__ tab
   return kNone;
 }
 
-// Classify + compact in one pass (decoupled look-back over tiles of
-// kScanTile requests): a request is "touched" if its op code is invalid or its
-// key has an INSERT at or before it.  Touched requests go to (tk, tv) and the
-// rest to list, both in input order; the block holding the last tile writes
-// the two counts.  A look-back that waits past kSpinLimit sets kErrSpin.
-constexpr int kScanThreads = 512;
-constexpr int kScanItems = 8;
-constexpr int kScanTile = kScanThreads * kScanItems;  // 4096
-constexpr int kScanWarps = kScanThreads / 32;
-constexpr uint32_t kFlagAgg = 1u << 30;
-constexpr uint32_t kFlagPrefix = 2u << 30;
-constexpr uint32_t kValMask = (1u << 30) - 1u;
-constexpr uint32_t kSpinLimit = 1u << 22;
+// Classify, then compact, in three launches over tiles of kTile requests:
+//   front_flag_kernel     one flag byte per request ("touched": invalid op
+//                         code, or its key has a write at or before it) and
+//                         the touched count of each tile;
+//   front_tile_scan_kernel  exclusive offsets of the tiles (one block) and
+//                         the two class counts;
+//   front_scatter_kernel  touched requests to (tk, tv), the rest to list,
+//                         both in input order.
+// Every launch is fully parallel (no look-back chain between tiles): the
+// probes of the flag pass are its only dependent loads, and the scatter
+// reads the request's key and op again only when it is touched.
+constexpr int kTileThreads = 256;
+constexpr int kTileItems = 8;
+constexpr int kTile = kTileThreads * kTileItems;  // 2048
+constexpr int kTileWarps = kTileThreads / 32;
 
-__global__ void __launch_bounds__(kScanThreads) front_split_kernel(
-    const uint64_t* __restrict__ keys, const uint8_t* __restrict__ ops, size_t n, const Slot* __restrict__ tab,
-    BatchCounts* __restrict__ counts, uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ status,
-    uint64_t* __restrict__ tk, uint32_t* __restrict__ tv, uint32_t* __restrict__ list, uint32_t* __restrict__ err) {
-  __shared__ uint32_t cnt[kScanItems][kScanWarps];
-  __shared__ uint32_t s_tile, s_excl;
-  const uint32_t n_tiles = (uint32_t)((n + kScanTile - 1) / kScanTile);
+__global__ void __launch_bounds__(kTileThreads) front_flag_kernel(const uint64_t* __restrict__ keys,
+                                                                  const uint8_t* __restrict__ ops, size_t n,
+                                                                  const Slot* __restrict__ tab,
+                                                                  const BatchCounts* __restrict__ counts,
+                                                                  uint8_t* __restrict__ flags,
+                                                                  uint32_t* __restrict__ tile_cnt) {
+  __shared__ uint32_t wsum[kTileWarps];
   const uint32_t mask = counts->cap - 1;
   const bool any = counts->n_ins_req != 0;
+  const size_t base = (size_t)blockIdx.x * kTile;
+  uint64_t k[kTileItems];
+  uint8_t op[kTileItems];
+  uint64_t sk[kTileItems];
+  uint32_t sf[kTileItems], sh[kTileItems];
+  // loads first, then every item's first probe slot (independent loads in
+  // flight), then the rare longer probes
+#pragma unroll
+  for (int j = 0; j < kTileItems; j++) {
+    const size_t i = base + (size_t)j * kTileThreads + threadIdx.x;
+    k[j] = i < n ? keys[i] : kKeyMax;
+    op[j] = i < n ? ops[i] : 0;
+  }
+#pragma unroll
+  for (int j = 0; j < kTileItems; j++) {
+    sh[j] = (uint32_t)slot_hash(k[j]) & mask;
+    sk[j] = kKeyMax;
+    sf[j] = kNone;
+    if (any && k[j] != kKeyMax) {
+      const ulonglong2 e = __ldg(reinterpret_cast<const ulonglong2*>(tab + sh[j]));
+      sk[j] = e.x;
+      sf[j] = (uint32_t)e.y;
+    }
+  }
+  uint32_t c = 0;
+#pragma unroll
+  for (int j = 0; j < kTileItems; j++) {
+    const size_t i = base + (size_t)j * kTileThreads + threadIdx.x;
+    if (i < n) {
+      bool f = op[j] > 2;  // invalid op codes are rejected on the sorted path
+      if (!f && any && k[j] != kKeyMax) {
+        uint32_t first = kNone;
+        if (sk[j] == k[j]) first = sf[j];
+        else if (sk[j] != kKeyMax) first = find_first_from(tab, mask, k[j], (sh[j] + 1) & mask);
+        f = first != kNone && (uint32_t)i >= first;
+      }
+      flags[i] = f ? 1 : 0;
+      c += f ? 1u : 0u;
+    }
+  }
+  c = __reduce_add_sync(0xffffffffu, c);
+  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+#pragma unroll
+    for (int w = 0; w < kTileWarps; w++) t += wsum[w];
+    tile_cnt[blockIdx.x] = t;
+  }
+}
+
+// exclusive offsets of n_tiles counts, in place, with one block
+__global__ void __launch_bounds__(1024) front_tile_scan_kernel(uint32_t* __restrict__ tile, uint32_t n_tiles,
+                                                               size_t n, BatchCounts* __restrict__ counts) {
+  __shared__ uint32_t wtot[32];
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t carry = 0;
+  for (uint32_t b = 0; b < n_tiles; b += 1024) {
+    const uint32_t i = b + threadIdx.x;
+    const uint32_t v = i < n_tiles ? tile[i] : 0u;
+    uint32_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= (uint32_t)o) incl += y;
+    }
+    if (lane == 31) wtot[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t t = wtot[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+        if (lane >= (uint32_t)o) t += y;
+      }
+      wtot[lane] = t;  // inclusive over warps
+    }
+    __syncthreads();
+    const uint32_t before = warp ? wtot[warp - 1] : 0u;
+    if (i < n_tiles) tile[i] = carry + before + incl - v;
+    carry += wtot[31];
+    __syncthreads();  // wtot is reused by the next chunk
+  }
+  if (threadIdx.x == 0) {
+    counts->n_touch = carry;
+    counts->n_lookup = (uint32_t)n - carry;
+  }
+}
+
+__global__ void __launch_bounds__(kTileThreads) front_scatter_kernel(const uint64_t* __restrict__ keys,
+                                                                     const uint8_t* __restrict__ ops, size_t n,
+                                                                     const uint8_t* __restrict__ flags,
+                                                                     const uint32_t* __restrict__ tile_off,
+                                                                     uint64_t* __restrict__ tk,
+                                                                     uint32_t* __restrict__ tv,
+                                                                     uint32_t* __restrict__ list) {
+  __shared__ uint32_t cnt[kTileItems][kTileWarps];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t lt = (1u << lane) - 1u;
-  for (;;) {
-    if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
-    __syncthreads();
-    const uint32_t tile = s_tile;
-    if (tile >= n_tiles) return;
-    const size_t base = (size_t)tile * kScanTile;
-    uint64_t k[kScanItems];
-    uint8_t op[kScanItems];
-    uint32_t bal[kScanItems];
-    uint64_t sk[kScanItems];
-    uint32_t sf[kScanItems], sh[kScanItems];
-    // loads first, then every item's first probe slot (independent loads in
-    // flight), then the rare longer probes
+  const size_t base = (size_t)blockIdx.x * kTile;
+  uint32_t bal[kTileItems];
 #pragma unroll
-    for (int j = 0; j < kScanItems; j++) {
-      const size_t i = base + (size_t)j * kScanThreads + threadIdx.x;
-      k[j] = i < n ? keys[i] : kKeyMax;
-      op[j] = i < n ? ops[i] : 0;
-    }
+  for (int j = 0; j < kTileItems; j++) {
+    const size_t i = base + (size_t)j * kTileThreads + threadIdx.x;
+    bal[j] = __ballot_sync(0xffffffffu, i < n && flags[i] != 0);
+    if (lane == 0) cnt[j][warp] = __popc(bal[j]);
+  }
+  __syncthreads();
+  // exclusive prefix over (item, warp) in index order
+  if (warp == 0) {
+    uint32_t carry = 0;
 #pragma unroll
-    for (int j = 0; j < kScanItems; j++) {
-      sh[j] = (uint32_t)slot_hash(k[j]) & mask;
-      sk[j] = kKeyMax;
-      sf[j] = kNone;
-      if (any && k[j] != kKeyMax) {
-        const ulonglong2 e = __ldg(reinterpret_cast<const ulonglong2*>(tab + sh[j]));
-        sk[j] = e.x;
-        sf[j] = (uint32_t)e.y;
+    for (int j = 0; j < kTileItems; j++) {
+      const uint32_t c = lane < kTileWarps ? cnt[j][lane] : 0u;
+      uint32_t incl = c;
+#pragma unroll
+      for (int o = 1; o < kTileWarps; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
       }
+      if (lane < kTileWarps) cnt[j][lane] = carry + incl - c;
+      carry += __shfl_sync(0xffffffffu, incl, kTileWarps - 1);
     }
+  }
+  __syncthreads();
+  const uint32_t excl = tile_off[blockIdx.x];
 #pragma unroll
-    for (int j = 0; j < kScanItems; j++) {
-      const size_t i = base + (size_t)j * kScanThreads + threadIdx.x;
-      bool f = false;
-      if (i < n) {
-        f = op[j] > 2;  // invalid op codes are rejected on the sorted path
-        if (!f && any && k[j] != kKeyMax) {
-          uint32_t first = kNone;
-          if (sk[j] == k[j]) first = sf[j];
-          else if (sk[j] != kKeyMax) first = find_first_from(tab, mask, k[j], (sh[j] + 1) & mask);
-          f = first != kNone && (uint32_t)i >= first;
-        }
-      }
-      bal[j] = __ballot_sync(0xffffffffu, f);
-      if (lane == 0) cnt[j][warp] = __popc(bal[j]);
-    }
-    __syncthreads();
-    // exclusive prefix over (item, warp) in index order, and the tile total
-    if (warp == 0) {
-      uint32_t carry = 0;
-      for (int j = 0; j < kScanItems; j++) {
-        const uint32_t c = lane < kScanWarps ? cnt[j][lane] : 0u;
-        uint32_t incl = c;
-#pragma unroll
-        for (int o = 1; o < kScanWarps; o <<= 1) {
-          const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-          if (lane >= o) incl += y;
-        }
-        if (lane < kScanWarps) cnt[j][lane] = carry + incl - c;
-        carry += __shfl_sync(0xffffffffu, incl, kScanWarps - 1);
-      }
-      // publish, then look back for the exclusive prefix of this tile: the
-      // warp reads 32 predecessors per step and stops at the first one that
-      // holds an inclusive prefix
-      uint32_t excl = 0;
-      if (tile == 0) {
-        if (lane == 0) st_relaxed32(status, kFlagPrefix | carry);
+  for (int j = 0; j < kTileItems; j++) {
+    const size_t i = base + (size_t)j * kTileThreads + threadIdx.x;
+    if (i < n) {
+      const uint32_t p = excl + cnt[j][warp] + __popc(bal[j] & lt);  // touched before i
+      if ((bal[j] >> lane) & 1u) {
+        const uint8_t op = ops[i];
+        tk[p] = keys[i];
+        tv[p] = (uint32_t)i | ((op <= 2 ? (uint32_t)op : 3u) << 30);
       } else {
-        if (lane == 0) st_relaxed32(status + tile, kFlagAgg | carry);
-        int64_t top = (int64_t)tile - 1;
-        uint32_t spins = 0;
-        for (;;) {
-          const int64_t idx = top - lane;
-          const uint32_t v = idx >= 0 ? ld_relaxed32(status + idx) : kFlagPrefix;
-          const uint32_t f = v & ~kValMask;
-          const uint32_t notready = __ballot_sync(0xffffffffu, f == 0);
-          const uint32_t prefix = __ballot_sync(0xffffffffu, f == kFlagPrefix);
-          const uint32_t stop = notready | prefix;
-          if (stop && ((notready >> (__ffs(stop) - 1)) & 1u)) {  // wait for that predecessor
-            if (++spins > kSpinLimit) {
-              if (lane == 0) atomicOr(err, kErrSpin);
-              break;
-            }
-            if (spins > 16) __nanosleep(64);
-            continue;
-          }
-          const int last = stop ? __ffs(stop) - 1 : 31;
-          excl += __reduce_add_sync(0xffffffffu, lane <= (uint32_t)last ? (v & kValMask) : 0u);
-          if (stop) break;
-          top -= 32;
-        }
-        if (lane == 0) st_relaxed32(status + tile, kFlagPrefix | (excl + carry));
-      }
-      if (lane == 0) {
-        s_excl = excl;
-        if (tile == n_tiles - 1) {
-          counts->n_touch = excl + carry;
-          counts->n_lookup = (uint32_t)n - (excl + carry);
-        }
+        list[i - p] = (uint32_t)i;
       }
     }
-    __syncthreads();
-    const uint32_t excl = s_excl;
-#pragma unroll
-    for (int j = 0; j < kScanItems; j++) {
-      const size_t i = base + (size_t)j * kScanThreads + threadIdx.x;
-      if (i < n) {
-        const uint32_t p = excl + cnt[j][warp] + __popc(bal[j] & lt);  // touched before i
-        if ((bal[j] >> lane) & 1u) {
-          tk[p] = k[j];
-          tv[p] = (uint32_t)i | ((op[j] <= 2 ? (uint32_t)op[j] : 3u) << 30);
-        } else {
-          list[i - p] = (uint32_t)i;
-        }
-      }
-    }
-    __syncthreads();  // cnt, s_tile and s_excl are reused by the next tile
   }
 }
 
@@ -284,30 +306,20 @@ __global__ void __launch_bounds__(kScanThreads) front_split_kernel(
 int front_classify(Handle* h, const uint64_t* keys, const uint8_t* ops, size_t n, cudaStream_t s) {
   Work& w = h->w;
   BatchCounts* c = w.counts;
-  const size_t n_tiles = (n + kScanTile - 1) / kScanTile;
-  // scratch: tile counter, then one status word per tile
-  uint32_t* counter = w.sort_scratch;
-  uint32_t* status = w.sort_scratch + 32;
+  const size_t n_tiles = (n + kTile - 1) / kTile;
   if (cudaMemsetAsync(c, 0, sizeof(BatchCounts), s) != cudaSuccess) return -2;
-  if (cudaMemsetAsync(w.sort_scratch, 0, (32 + n_tiles) * 4, s) != cudaSuccess) return -2;
   const unsigned g = (unsigned)min((size_t)h->sm_count * 8, (n + kThreads - 1) / kThreads);
   Slot* tab = reinterpret_cast<Slot*>(w.f_tab);
+  uint8_t* flags = reinterpret_cast<uint8_t*>(w.f_flags);
+  uint32_t* tile = w.f_pos;  // per-tile counts, then offsets
   front_count_kernel<<<(unsigned)h->sm_count * 2, kThreads, 0, s>>>(ops, n, c);
   front_clear_kernel<<<(unsigned)h->sm_count * 4, kThreads, 0, s>>>(tab, w.f_tab_cap, c);
   front_insert_kernel<<<g, kThreads, 0, s>>>(keys, ops, n, tab, c);
-  static unsigned resident[64] = {};
-  const int dev = h->device;
-  if (dev >= 0 && dev < 64 && !resident[dev]) {
-    int per = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, front_split_kernel, kScanThreads, 0) != cudaSuccess ||
-        per < 1)
-      per = 1;
-    resident[dev] = (unsigned)per * (unsigned)h->sm_count;
-  }
-  const unsigned rb = (dev >= 0 && dev < 64) ? resident[dev] : (unsigned)h->sm_count;
-  front_split_kernel<<<(unsigned)min(n_tiles, (size_t)rb), kScanThreads, 0, s>>>(
-      keys, ops, n, tab, c, counter, status, w.f_tk, w.f_tv, w.f_list, &h->tree.ctrl->error);
-  count_launch(4);
+  front_flag_kernel<<<(unsigned)n_tiles, kTileThreads, 0, s>>>(keys, ops, n, tab, c, flags, tile);
+  front_tile_scan_kernel<<<1, 1024, 0, s>>>(tile, (uint32_t)n_tiles, n, c);
+  front_scatter_kernel<<<(unsigned)n_tiles, kTileThreads, 0, s>>>(keys, ops, n, flags, tile, w.f_tk, w.f_tv,
+                                                                  w.f_list);
+  count_launch(6);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
