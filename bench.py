@@ -230,8 +230,9 @@ def run_reference(args):
 def serve_bench(E, np, tree, tk_host, n_tree, seconds=1.5, seed=5, load=0.5):
     """Serving loop (continuous batching): batch sizes log-uniform over
     2^10..2^22, per-batch search fraction uniform in [0.5, 1], Poisson arrivals.
-    Phase 1 submits as fast as admission allows (capacity); phase 2 offers 50 %
-    of that capacity with Poisson arrivals and reports the batch latency."""
+    After a warm-up pass, phase 1 submits as fast as admission allows
+    (capacity); phase 2 offers 25 % and 50 % of that capacity with Poisson
+    arrivals and reports the batch latency."""
     import torch
 
     rng = np.random.default_rng(seed)
@@ -290,6 +291,7 @@ def serve_bench(E, np, tree, tk_host, n_tree, seconds=1.5, seed=5, load=0.5):
             srv.wait(tk)
         return srv.stats(reset=False), n_sub
 
+    run(seconds / 2, None)  # warm-up: the first pass inserts the pools' new keys (the tree grows once)
     cap, _ = run(seconds, None)
     mean_batch = (2.0 ** 22 - 2.0 ** 10) / np.log(2.0 ** 12)  # mean of the log-uniform size law
     out = {"capacity_mops": cap["mops"], "capacity_batches": cap["batches"]}

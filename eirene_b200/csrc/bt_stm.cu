@@ -585,6 +585,66 @@ __device__ int tx_fast(const DevTree& t, const uint32_t epoch, const uint64_t ke
   return FAST_DONE;
 }
 
+// A GET by an 8-lane group (lane g owns slots 4g..4g+3), so that a warp
+// serves four at once.  Lock-free like tx_fast's read: the descent takes the
+// rows as they are, and the leaf is read under its seqlock and checked
+// (unlocked and unchanged header, leaf level, current epoch,
+// low <= key < right fence), the matched value inside the same window.
+// Returns false when a check fails; the caller then runs the request on the
+// warp path.
+constexpr int kGetG = 8, kGetS = 32 / kGetG;
+
+__device__ bool group_get(const DevTree& t, const uint32_t epoch, const uint64_t key, const uint32_t g,
+                          const uint32_t gmask, uint64_t& ans, uint8_t& st) {
+  uint32_t node = ld_relaxed32(&t.ctrl->root);
+  if (node == kNil) return false;
+  uint64_t k[kGetS];
+  for (int depth = 0;; depth++) {
+    if (depth > 40 || node >= t.cap) return false;
+    const ulonglong2* row = reinterpret_cast<const ulonglong2*>(t.keys + (size_t)node * 32 + g * kGetS);
+#pragma unroll
+    for (int i = 0; i < kGetS / 2; i++) {
+      const ulonglong2 w = row[i];
+      k[2 * i] = w.x;
+      k[2 * i + 1] = w.y;
+    }
+    const uint64_t hdr = __shfl_sync(gmask, k[kGetS - 1], kGetG - 1, kGetG);
+    if (hdr_level(hdr) == 0) break;
+    if (g == kGetG - 1) k[kGetS - 1] = kKeyMax;  // slot 31 holds the header
+    uint32_t c = 0;
+#pragma unroll
+    for (int i = 0; i < kGetS; i++) c += (k[i] <= key) ? 1u : 0u;
+    c = group_sum<kGetG>(c, gmask);
+    node = (uint32_t)t.vals[(size_t)node * 32 + c];
+  }
+  // the leaf, under its seqlock
+  const uint64_t* krow = t.keys + (size_t)node * 32;
+  const uint64_t h = ld_acquire(krow + 31);
+#pragma unroll
+  for (int i = 0; i < kGetS; i++) k[i] = ld_relaxed(krow + g * kGetS + i);
+  const uint64_t lo = ld_relaxed(t.low + node);
+  const uint64_t fence = ld_relaxed(t.vals + (size_t)node * 32 + 31);
+  const uint32_t size = hdr_size(h);
+  uint32_t c = 0;
+#pragma unroll
+  for (int i = 0; i < kGetS; i++) c += (g * kGetS + i < size && k[i] <= key) ? 1u : 0u;
+  c = group_sum<kGetG>(c, gmask);
+  const uint32_t slot = c > 0 ? c - 1 : 0;
+  const uint64_t kk = __shfl_sync(gmask, pick<kGetS>(k, slot % kGetS), slot / kGetS, kGetG);
+  const bool found = c > 0 && kk == key;
+  uint64_t v = 0;
+  if (found) v = ld_relaxed(t.vals + (size_t)node * 32 + slot);
+  fence_acq_rel();
+  const uint64_t h2 = ld_relaxed(krow + 31);
+  const uint64_t h0 = __shfl_sync(gmask, h, 0, kGetG);
+  const bool bad = hdr_locked(h) || h2 != h || h != h0 || hdr_level(h) != 0 || hdr_epoch(h) != epoch ||
+                   !(lo <= key && key < fence);
+  if (group_sum<kGetG>(bad ? 1u : 0u, gmask) != 0) return false;
+  ans = found ? v : 0;
+  st = found ? kFound : kAbsent;
+  return true;
+}
+
 struct TxCounters {
   unsigned long long commits = 0, aborts = 0, exhausted = 0;
 };
@@ -815,7 +875,38 @@ __global__ void __launch_bounds__(256, 4) serve_kernel(DevTree t, ServeDev S, ui
       continue;
     }
     const uint32_t end = min(d.n, c + (uint32_t)kServeChunk);
-    for (uint32_t q = c; q < end; q++) {
+    // GETs first, four at a time (8 lanes each); the writes and any GET whose
+    // leaf check failed then run one at a time on the whole warp.  Requests
+    // of a batch are concurrent transactions, so this order is as good as any.
+    uint32_t rest = 0;  // bit q - c: the request still needs the warp path
+    {
+      const uint32_t g = lane % kGetG, grp = lane / kGetG;
+      const uint32_t gmask = group_mask<kGetG>(lane);
+      for (uint32_t b = c; b < end; b += 32 / kGetG) {
+        const uint32_t q = b + grp;
+        bool get = false;
+        uint64_t key = 0;
+        if (q < end) {
+          key = d.keys[q];
+          get = d.ops[q] == kOpGet && key != kKeyMax;
+        }
+        bool ok = false;
+        uint64_t ans = 0;
+        uint8_t st = kAbsent;
+        if (get) ok = group_get(t, epoch, key, g, gmask, ans, st);
+        if (ok && g == 0) {
+          d.out_vals[q] = ans;
+          d.out_st[q] = st;
+        }
+        const uint32_t need = __ballot_sync(kFull, g == 0 && q < end && !ok);
+#pragma unroll
+        for (int j = 0; j < 32 / kGetG; j++)
+          if ((need >> (j * kGetG)) & 1u) rest |= 1u << (b - c + (uint32_t)j);
+      }
+    }
+    while (rest) {
+      const uint32_t q = c + (uint32_t)(__ffs(rest) - 1);
+      rest &= rest - 1;
       uint64_t ans;
       uint8_t st;
       const uint32_t op = d.ops[q];
