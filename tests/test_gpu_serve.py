@@ -157,3 +157,47 @@ def test_relaunch_after_idle(gpu):
     ref, _ = oracle_answers(keys, vals, [b1, b2])
     for (gv, gs), (ov, os_) in zip(r1 + r2, ref):
         assert (gs == os_).all() and (gv == ov).all()
+
+
+def test_gets_beside_splitting_inserts(gpu):
+    # reader batches run while writer batches split the leaves they read: a
+    # GET of a key that is in the tree throughout must find it with its value
+    # (the group lookup's seqlock check sends torn reads to the warp path),
+    # and a GET of a key being inserted sees it absent or with its new value
+    t, keys, vals = build(seed=7)
+    rng = np.random.default_rng(8)
+    fresh = np.setdiff1d(O.gen_keys("uniform", 777, 260_000), keys)[:240_000]
+    fresh = rng.permutation(fresh)
+    fval = fresh ^ np.uint64(0x5A5A)
+    batches, kinds = [], []
+    for b in range(8):
+        w = fresh[b * 30_000:(b + 1) * 30_000]
+        batches.append((w, fval[b * 30_000:(b + 1) * 30_000], np.zeros(w.size, np.uint8)))
+        kinds.append(("w", b))
+        old = rng.choice(keys, 20_000, replace=False)
+        soon = fresh[rng.integers(0, (b + 1) * 30_000, 10_000)]
+        rk = np.concatenate([old, soon])
+        batches.append((rk, np.zeros(rk.size, np.uint64), np.ones(rk.size, np.uint8)))
+        kinds.append(("r", old.size))
+    srv = E.Server(t, arena_bytes=64 << 20, max_batches=64)
+    try:
+        outs = serve_all(srv, batches)
+    finally:
+        srv.stop()
+    fmap = dict(zip(fresh.tolist(), fval.tolist()))
+    vmap = dict(zip(keys.tolist(), vals.tolist()))
+    for (kind, x), (rk, _, _), (ov, os_) in zip(kinds, batches, outs):
+        if kind == "w":
+            assert (os_ == E.ST_ABSENT).all()
+            continue
+        n_old = x
+        assert (os_[:n_old] == E.ST_FOUND).all()
+        assert all(int(v) == vmap[int(k)] for k, v in zip(rk[:n_old], ov[:n_old]))
+        st = os_[n_old:]
+        assert set(np.unique(st).tolist()) <= {E.ST_ABSENT, E.ST_FOUND}
+        for k, v, s in zip(rk[n_old:], ov[n_old:], st):
+            if s == E.ST_FOUND:
+                assert int(v) == fmap[int(k)]
+    gk, gv = dump(t)
+    assert gk.size == keys.size + fresh.size
+    assert (gk == np.union1d(keys, fresh)).all()
