@@ -645,6 +645,45 @@ __device__ bool group_get(const DevTree& t, const uint32_t epoch, const uint64_t
   return true;
 }
 
+// The GETs among requests [b0, b1) (at most 32; request q is list[q], or q
+// without a list), four at a time by 8-lane groups.  Returns the bits q - b0
+// of the requests left for the warp path: the writes, and the GETs whose
+// leaf check failed.  op_override as in stm_kernel.
+__device__ uint32_t get_pass(const DevTree& t, const uint32_t epoch, const uint64_t* __restrict__ keys,
+                             const uint8_t* __restrict__ ops, const uint32_t op_override,
+                             const uint32_t* __restrict__ list, const size_t b0, const size_t b1,
+                             uint64_t* __restrict__ out_vals, uint8_t* __restrict__ out_st) {
+  const uint32_t lane = lane_id();
+  const uint32_t g = lane % kGetG, grp = lane / kGetG;
+  const uint32_t gmask = group_mask<kGetG>(lane);
+  uint32_t rest = 0;
+  for (size_t b = b0; b < b1; b += 32 / kGetG) {
+    const size_t q = b + grp;
+    bool get = false;
+    uint64_t key = 0;
+    uint32_t r = 0;
+    if (q < b1) {
+      r = list ? list[q] : (uint32_t)q;
+      key = keys[r];
+      const uint32_t op = op_override <= 1 ? op_override : (uint32_t)ops[r];
+      get = op == kOpGet && key != kKeyMax;
+    }
+    bool ok = false;
+    uint64_t ans = 0;
+    uint8_t st = kAbsent;
+    if (get) ok = group_get(t, epoch, key, g, gmask, ans, st);
+    if (ok && g == 0) {
+      out_vals[r] = ans;
+      out_st[r] = st;
+    }
+    const uint32_t need = __ballot_sync(kFull, g == 0 && q < b1 && !ok);
+#pragma unroll
+    for (int j = 0; j < 32 / kGetG; j++)
+      if ((need >> (j * kGetG)) & 1u) rest |= 1u << (uint32_t)(b - b0 + (size_t)j);
+  }
+  return rest;
+}
+
 struct TxCounters {
   unsigned long long commits = 0, aborts = 0, exhausted = 0;
 };
@@ -736,15 +775,26 @@ __global__ void __launch_bounds__(256, 4) stm_kernel(DevTree t, const uint64_t* 
   const size_t chunk = (n + n_warps - 1) / n_warps;
   const size_t q_begin = (((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * chunk;
   const size_t q_end = min(n, q_begin + chunk);
-  for (size_t q = q_begin; q < q_end; q++) {
-    const uint32_t r = list ? list[q] : (uint32_t)q;
-    const uint32_t op = op_override <= 1 ? op_override : (uint32_t)ops[r];
-    uint64_t ans;
-    uint8_t st;
-    run_request(t, epoch, keys[r], op, op == kOpInsert ? vals[r] : 0, retry_limit, ans, st, cnt, M);
-    if (lane == 0) {
-      out_vals[r] = ans;
-      out_st[r] = st;
+  // in windows of 32: the GETs four at a time (8 lanes each), then the
+  // writes and any GET whose leaf check failed on the whole warp (requests of
+  // a batch are concurrent transactions, so this order is as good as any)
+  const bool all_ins = op_override == kOpInsert;
+  for (size_t w0 = q_begin; w0 < q_end; w0 += 32) {
+    const size_t w1 = min(q_end, w0 + 32);
+    uint32_t rest = all_ins ? (w1 - w0 == 32 ? 0xffffffffu : (1u << (w1 - w0)) - 1u)
+                            : get_pass(t, epoch, keys, ops, op_override, list, w0, w1, out_vals, out_st);
+    while (rest) {
+      const size_t q = w0 + (size_t)(__ffs(rest) - 1);
+      rest &= rest - 1;
+      const uint32_t r = list ? list[q] : (uint32_t)q;
+      const uint32_t op = op_override <= 1 ? op_override : (uint32_t)ops[r];
+      uint64_t ans;
+      uint8_t st;
+      run_request(t, epoch, keys[r], op, op == kOpInsert ? vals[r] : 0, retry_limit, ans, st, cnt, M);
+      if (lane == 0) {
+        out_vals[r] = ans;
+        out_st[r] = st;
+      }
     }
   }
   flush_counters(t, cnt);
@@ -878,32 +928,7 @@ __global__ void __launch_bounds__(256, 4) serve_kernel(DevTree t, ServeDev S, ui
     // GETs first, four at a time (8 lanes each); the writes and any GET whose
     // leaf check failed then run one at a time on the whole warp.  Requests
     // of a batch are concurrent transactions, so this order is as good as any.
-    uint32_t rest = 0;  // bit q - c: the request still needs the warp path
-    {
-      const uint32_t g = lane % kGetG, grp = lane / kGetG;
-      const uint32_t gmask = group_mask<kGetG>(lane);
-      for (uint32_t b = c; b < end; b += 32 / kGetG) {
-        const uint32_t q = b + grp;
-        bool get = false;
-        uint64_t key = 0;
-        if (q < end) {
-          key = d.keys[q];
-          get = d.ops[q] == kOpGet && key != kKeyMax;
-        }
-        bool ok = false;
-        uint64_t ans = 0;
-        uint8_t st = kAbsent;
-        if (get) ok = group_get(t, epoch, key, g, gmask, ans, st);
-        if (ok && g == 0) {
-          d.out_vals[q] = ans;
-          d.out_st[q] = st;
-        }
-        const uint32_t need = __ballot_sync(kFull, g == 0 && q < end && !ok);
-#pragma unroll
-        for (int j = 0; j < 32 / kGetG; j++)
-          if ((need >> (j * kGetG)) & 1u) rest |= 1u << (b - c + (uint32_t)j);
-      }
-    }
+    uint32_t rest = get_pass(t, epoch, d.keys, d.ops, 0xFF, nullptr, c, end, d.out_vals, d.out_st);
     while (rest) {
       const uint32_t q = c + (uint32_t)(__ffs(rest) - 1);
       rest &= rest - 1;
