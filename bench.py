@@ -342,6 +342,8 @@ def main():
     ap.add_argument("--cpu-sample-log2", type=int, default=20)
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=1.5)
+    ap.add_argument("--retrain-every", type=int, default=0,
+                    help="learned form: retrain the model after every K timed batches (0: trained once, before)")
     ap.add_argument("--front-end", default="hash", choices=["hash", "sort"],
                     help="sorted batches: hash front end (sort only INSERT-coupled requests) or full sort")
     ap.add_argument("--pool-keys-log2", type=int, default=0,
@@ -466,6 +468,8 @@ def main():
         ev[0].record(stream)
         for s in range(args.steps):
             step(*batches[args.warmup + s])
+            if learned and args.retrain_every > 0 and (s + 1) % args.retrain_every == 0:
+                tree.retrain(stream)  # inside the timed region: the model follows the tree
             ev[s + 1].record(stream)  # the batch's answers are final
         tree.sync(stream)  # the last batch's deferred leaf/inner merge
         ev[-1].record(stream)
@@ -677,6 +681,7 @@ def main():
                 "parallelism": (f"{world} key-range shards, one tree per GPU, all-to-all request exchange over NCCL"
                                 if sharded is not None else "one tree on one GPU"),
                 "tree_build_s": build_s,
+                "learned_retrain_every": args.retrain_every,
             },
             "roofline": roof,
             "cpu_baseline": cpu,
