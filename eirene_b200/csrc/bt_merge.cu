@@ -337,6 +337,8 @@ __global__ void __launch_bounds__(256) merge_leaf_kernel(DevTree t, uint32_t lea
                                                          MergeEntry* __restrict__ ent) {
   constexpr int S = 32 / G;
   __shared__ uint64_t s_keys[256 / G][32];
+  __shared__ __align__(16) uint64_t s_mk[256 / G][32];  // merged row when it fits one leaf
+  __shared__ __align__(16) uint64_t s_mv[256 / G][32];
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t g = lane % G;
   const uint32_t grp = threadIdx.x / G;
@@ -366,6 +368,47 @@ __global__ void __launch_bounds__(256) merge_leaf_kernel(DevTree t, uint32_t lea
     __syncwarp(gmask);
     const uint32_t m = sz + cnt;
     const uint32_t p = m <= (uint32_t)kMaxKeys ? 1u : ceil_div(m, leaf_fill);
+    if (p == 1) {
+      // no split (the common case): merge into shared memory, then write
+      // the row with one 16-byte store per lane and pair of slots
+#pragma unroll
+      for (int i = 0; i < S; i++) {
+        const uint32_t slot = g * S + i;
+        if (slot < sz) {
+          const uint32_t pos = slot + count_less(newk + a, cnt, ok[i]);
+          s_mk[grp][pos] = ok[i];
+          s_mv[grp][pos] = ov[i];
+        }
+      }
+      for (uint32_t j = g; j < cnt; j += G) {
+        const uint64_t key = newk[a + j];
+        const uint32_t pos = j + count_less(s_keys[grp], sz, key);
+        s_mk[grp][pos] = key;
+        s_mv[grp][pos] = newv[a + j];
+      }
+      __syncwarp(gmask);
+      uint64_t wk[S], wv[S];
+#pragma unroll
+      for (int i = 0; i < S; i++) {
+        const uint32_t slot = g * S + i;
+        wk[i] = slot < m ? s_mk[grp][slot] : kKeyMax;
+        wv[i] = slot < m ? s_mv[grp][slot] : 0;
+      }
+      if (g == G - 1) {
+        wk[S - 1] = make_hdr(m, 0, hdr_version(h) + 1, hdr_epoch(h));
+        wv[S - 1] = fence;
+      }
+      uint64_t* kr = t.keys + (size_t)leaf * 32 + g * S;
+      uint64_t* vr = t.vals + (size_t)leaf * 32 + g * S;
+#pragma unroll
+      for (int i = 0; i < S; i += 2) {
+        *reinterpret_cast<ulonglong2*>(kr + i) = make_ulonglong2(wk[i], wk[i + 1]);
+        *reinterpret_cast<ulonglong2*>(vr + i) = make_ulonglong2(wv[i], wv[i + 1]);
+      }
+      __syncwarp(gmask);  // s_mk / s_mv are reused by the next segment
+      if (g == 0) added += cnt;
+      continue;
+    }
     const uint32_t eo = eoff[s];
     auto node_of = [&](uint32_t c) -> uint32_t { return c == 0 ? leaf : base + eo + c - 1; };
     auto place = [&](uint32_t pos, uint64_t key, uint64_t val) {
