@@ -171,11 +171,13 @@ int bt_create(const bt_config* cfg_in, bt_handle** out) {
   ok = ok && cudaMalloc(&h.tree.keys, nodes * 256) == cudaSuccess;
   ok = ok && cudaMalloc(&h.tree.vals, nodes * 256) == cudaSuccess;
   ok = ok && cudaMalloc(&h.tree.low, nodes * 8) == cudaSuccess;
+  ok = ok && cudaMalloc(&h.tree.pfx, nodes * 128) == cudaSuccess;
   ok = ok && cudaMalloc(&h.tree.ctrl, sizeof(bt::Ctrl)) == cudaSuccess;
   // zeroed rows read as epoch 0, which no tree uses (see hdr_epoch)
   ok = ok && cudaMemset(h.tree.keys, 0, nodes * 256) == cudaSuccess;
   ok = ok && cudaMemset(h.tree.vals, 0, nodes * 256) == cudaSuccess;
   ok = ok && cudaMemset(h.tree.low, 0, nodes * 8) == cudaSuccess;
+  ok = ok && cudaMemset(h.tree.pfx, 0xff, nodes * 128) == cudaSuccess;
   ok = ok && bt::work_alloc(&h.w, cfg.max_batch) == 0;
   ok = ok && cudaStreamCreateWithFlags(&h.internal_stream, cudaStreamNonBlocking) == cudaSuccess;
   {
@@ -210,6 +212,7 @@ int bt_destroy(bt_handle* H) {
   cudaFree(h.tree.keys);
   cudaFree(h.tree.vals);
   cudaFree(h.tree.low);
+  cudaFree(h.tree.pfx);
   cudaFree(h.tree.ctrl);
   bt::work_free(&h.w);
   bt::learned_free(&h.L);

@@ -87,6 +87,11 @@ struct DevTree {
   uint64_t* low;
   Ctrl* ctrl;
   uint32_t cap;  // node capacity
+  // [cap][32] high 32 bits of an inner node's separators (slot 31 unused):
+  // the batch lookups compare these first and read the full keys of a row
+  // only when a prefix equals the key's.  Kept by the merge engine's inner
+  // merge; rebuilt from the rows after other writers (Handle::pfx_valid).
+  uint32_t* pfx;
 };
 
 // ---- memory-order helpers --------------------------------------------------

@@ -155,6 +155,8 @@ struct Handle {
   int front_end = 1;         // sorted batches: 1 = hash front end (sort only INSERT-coupled requests), 0 = full sort
   int top_cache = 1;         // unsorted searches descend the upper levels from shared memory
   int search_pairs = 2;      // unsorted searches: 2 pairs of requests per lane group, child ids only; 1 pairs; 0 single
+  bool pfx_valid = false;    // tree.pfx matches every inner row (false after bulk builds and STM writers)
+  int use_pfx = 1;           // paired searches compare the separators' 32-bit prefixes first
   void* top = nullptr;       // top cache (kTopNodes nodes) + TopInfo
   TopInfo* top_info = nullptr;
   int sm_count = 148;

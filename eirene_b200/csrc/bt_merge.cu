@@ -603,8 +603,13 @@ __global__ void __launch_bounds__(kInnerThreads) merge_inner_kernel(DevTree t, u
         for (uint32_t pidx = w; pidx < nn; pidx += kInnerWarps) {
           const uint32_t kc = piece_size(pidx, cnt, nn), cs = piece_start(pidx, cnt, nn);
           const uint32_t nd = nb + pidx;
-          if (lane < 31) t.keys[(size_t)nd * 32 + lane] = (lane + 1 < kc) ? t.low[ka[cs + lane + 1]] : kKeyMax;
-          else t.keys[(size_t)nd * 32 + 31] = make_hdr(kc - 1, level, 0, epoch);
+          if (lane < 31) {
+            const uint64_t sep = (lane + 1 < kc) ? t.low[ka[cs + lane + 1]] : kKeyMax;
+            t.keys[(size_t)nd * 32 + lane] = sep;
+            t.pfx[(size_t)nd * 32 + lane] = (uint32_t)(sep >> 32);
+          } else {
+            t.keys[(size_t)nd * 32 + 31] = make_hdr(kc - 1, level, 0, epoch);
+          }
           t.vals[(size_t)nd * 32 + lane] = lane < kc ? (uint64_t)ka[cs + lane] : 0;
           if (lane == 0) {
             t.low[nd] = t.low[ka[cs]];
@@ -690,6 +695,7 @@ __global__ void __launch_bounds__(kInnerThreads) merge_inner_kernel(DevTree t, u
           nxt[go + c - 1] = e;
         } else {
           t.keys[(size_t)nd * 32 + slot - 1] = key;
+          t.pfx[(size_t)nd * 32 + slot - 1] = (uint32_t)(key >> 32);
           t.vals[(size_t)nd * 32 + slot] = rc;
         }
       };
@@ -714,7 +720,10 @@ __global__ void __launch_bounds__(kInnerThreads) merge_inner_kernel(DevTree t, u
         const uint32_t nd = node_of(c);
         const uint32_t kc = piece_size(c, ch, q);
         if (c == 0 && lane == 0) t.vals[(size_t)nd * 32] = child0;
-        if (lane + 1 >= kc && lane < 31) t.keys[(size_t)nd * 32 + lane] = kKeyMax;
+        if (lane + 1 >= kc && lane < 31) {
+          t.keys[(size_t)nd * 32 + lane] = kKeyMax;
+          t.pfx[(size_t)nd * 32 + lane] = 0xffffffffu;
+        }
         if (lane >= kc) t.vals[(size_t)nd * 32 + lane] = 0;
         if (lane == 31) t.keys[(size_t)nd * 32 + 31] =
             make_hdr(kc - 1, lvl, c == 0 ? hdr_version(h) + 1 : 0, hdr_epoch(h));

@@ -69,6 +69,20 @@ __device__ __forceinline__ void load_slots_hint(const uint64_t* p, uint64_t (&x)
   }
 }
 
+// S 32-bit separator prefixes of a row (S = 2, 4 or 8)
+template <int S>
+__device__ __forceinline__ void load_pfx(const uint32_t* p, uint32_t (&x)[S], uint64_t pol) {
+  if constexpr (S == 2) {
+    asm("ld.global.nc.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;" : "=r"(x[0]), "=r"(x[1]) : "l"(p), "l"(pol));
+  } else {
+#pragma unroll
+    for (int i = 0; i < S; i += 4)
+      asm("ld.global.nc.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+          : "=r"(x[i]), "=r"(x[i + 1]), "=r"(x[i + 2]), "=r"(x[i + 3])
+          : "l"(p + i), "l"(pol));
+  }
+}
+
 template <int S>
 __device__ __forceinline__ uint64_t pick(const uint64_t (&x)[S], uint32_t e) {
   uint64_t r = x[0];
@@ -83,6 +97,19 @@ __device__ __forceinline__ uint32_t group_sum(uint32_t c, uint32_t gmask) {
 #pragma unroll
   for (int o = G / 2; o >= 1; o >>= 1) c += __shfl_xor_sync(gmask, c, o, G);
   return c;
+}
+
+// Rank of `key` in an inner row from the prefixes: slots whose prefix is
+// below the key's count, slots with an equal prefix are counted in bits
+// 16.. (the caller then ranks with the full keys); slot 31 is the header.
+template <int G, int S>
+__device__ __forceinline__ uint32_t pfx_rank(const uint32_t (&p)[S], uint64_t key, uint32_t g, uint32_t gmask) {
+  const uint32_t kp = (uint32_t)(key >> 32);
+  uint32_t x = 0;
+#pragma unroll
+  for (int i = 0; i < S; i++)
+    if (!(g == (uint32_t)(G - 1) && i == S - 1)) x += p[i] < kp ? 1u : (p[i] == kp ? 0x10000u : 0u);
+  return group_sum<G>(x, gmask);
 }
 
 // Look `key` up in leaf `node` (slots loaded by the group); returns the status
@@ -151,10 +178,14 @@ __device__ __forceinline__ uint8_t group_descend(const DevTree& t, uint32_t node
 // kChild: at inner levels load only the chosen child id (one 32 B sector)
 // after the key comparison instead of the whole 256 B child row with the keys:
 // fewer bytes per level, one more dependent load.
+// use_pfx (kChild only): inner levels compare the 32-bit separator prefixes
+// (half the bytes of the key row) and read the full keys only when a prefix
+// equals the key's.
 template <int G, bool kLeafVals, bool kChild = false>
 __device__ __forceinline__ void group_descend2(const DevTree& t, uint32_t node, uint32_t level, uint64_t key_a,
                                                uint64_t key_b, uint32_t g, uint32_t gmask, uint64_t& ans_a,
-                                               uint8_t& st_a, uint64_t& ans_b, uint8_t& st_b) {
+                                               uint8_t& st_a, uint64_t& ans_b, uint8_t& st_b,
+                                               bool use_pfx = false) {
   constexpr int S = 32 / G;
   uint64_t ka[S], va[S], kb[S], vb[S];
   uint32_t na = node, nb = node;
@@ -162,6 +193,34 @@ __device__ __forceinline__ void group_descend2(const DevTree& t, uint32_t node, 
   const uint64_t keep = l2_keep(), stream = l2_stream();
   for (;;) {
     const size_t ra = (size_t)na * 32 + g * S, rb = (size_t)nb * 32 + g * S;
+    if (kChild && use_pfx && level > 0) {
+      uint32_t pa[S], pb[S];
+      load_pfx<S>(t.pfx + ra, pa, keep);
+      load_pfx<S>(t.pfx + rb, pb, keep);
+      const uint32_t xa = pfx_rank<G, S>(pa, key_a, g, gmask), xb = pfx_rank<G, S>(pb, key_b, g, gmask);
+      ca = xa & 0xffffu;
+      cb = xb & 0xffffu;
+      if (xa >> 16) {  // a separator shares the key's prefix: rank with the full keys
+        load_slots_hint<S>(t.keys + ra, ka, keep);
+        if (g == G - 1) ka[S - 1] = kKeyMax;
+        uint32_t c = 0;
+#pragma unroll
+        for (int i = 0; i < S; i++) c += (ka[i] <= key_a) ? 1u : 0u;
+        ca = group_sum<G>(c, gmask);
+      }
+      if (xb >> 16) {
+        load_slots_hint<S>(t.keys + rb, kb, keep);
+        if (g == G - 1) kb[S - 1] = kKeyMax;
+        uint32_t c = 0;
+#pragma unroll
+        for (int i = 0; i < S; i++) c += (kb[i] <= key_b) ? 1u : 0u;
+        cb = group_sum<G>(c, gmask);
+      }
+      na = (uint32_t)ldg_hint(t.vals + (size_t)na * 32 + ca, keep);
+      nb = (uint32_t)ldg_hint(t.vals + (size_t)nb * 32 + cb, keep);
+      level--;
+      continue;
+    }
     if (kChild) {
       const uint64_t pol = level > 0 ? keep : stream;
       load_slots_hint<S>(t.keys + ra, ka, pol);

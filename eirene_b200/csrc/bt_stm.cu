@@ -967,6 +967,7 @@ cudaError_t launch_serve(Handle* h, const ServeDev& S, cudaStream_t s) {
   const unsigned blocks = (unsigned)(h->sm_count * (h->device < 64 ? per_sm[h->device] : 2));
   LearnedDev lm{};
   const int use = learned_dev(h, &lm);
+  h->pfx_valid = false;  // STM writes inner rows without their prefixes
   serve_kernel<<<blocks, 256, 0, s>>>(h->tree, S, h->retry_limit, lm, use);
   count_launch();
   return cudaGetLastError();
@@ -989,6 +990,7 @@ cudaError_t launch_stm(Handle* h, const uint64_t* keys, const uint64_t* vals, co
   if (blocks > cap) blocks = cap;
   LearnedDev lm{};
   const int use = learned_dev(h, &lm);
+  h->pfx_valid = false;  // STM writes inner rows without their prefixes
   stm_kernel<<<(unsigned)blocks, threads, 0, s>>>(h->tree, keys, vals, ops, op_override, list, n_dev, n, out_vals,
                                                    out_st, h->retry_limit, lm, use);
   count_launch();

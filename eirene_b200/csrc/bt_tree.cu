@@ -132,7 +132,8 @@ template <int G, bool kLeafVals, bool kChild>
 __global__ void __launch_bounds__(256) search2_kernel(DevTree t, const uint64_t* __restrict__ qkeys,
                                                       const uint32_t* __restrict__ list,
                                                       const uint32_t* __restrict__ n_dev, size_t n_host,
-                                                      uint64_t* __restrict__ out_vals, uint8_t* __restrict__ out_st) {
+                                                      uint64_t* __restrict__ out_vals, uint8_t* __restrict__ out_st,
+                                                      int use_pfx) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t g = lane % G;
   const uint32_t gmask = group_mask<G>(lane);
@@ -152,7 +153,7 @@ __global__ void __launch_bounds__(256) search2_kernel(DevTree t, const uint64_t*
     if (root != kNil) {
       // a reserved key descends as key 0 (keeping the pair in lock step) and is reported as rejected
       group_descend2<G, kLeafVals, kChild>(t, root, root_level, key_a == kKeyMax ? 0 : key_a,
-                                   key_b == kKeyMax ? 0 : key_b, g, gmask, aa, sa, ab, sb);
+                                   key_b == kKeyMax ? 0 : key_b, g, gmask, aa, sa, ab, sb, use_pfx != 0);
     }
     if (key_a == kKeyMax) {
       sa = kRejected;
@@ -554,6 +555,7 @@ cudaError_t launch_search_top(Handle* h, const uint64_t* qkeys, const uint32_t* 
 }
 
 cudaError_t tree_reset(Handle* h, cudaStream_t s) {
+  h->pfx_valid = false;  // the bulk loader writes inner rows without prefixes
   h->epoch = (h->epoch % 0x7fffu) + 1;  // 1 .. 0x7fff; 0 marks never-written rows
   reset_kernel<<<1, 1, 0, s>>>(h->tree.ctrl, h->epoch);
   count_launch();
@@ -724,6 +726,33 @@ cudaError_t launch_search_sorted(Handle* h, const uint64_t* qkeys, const uint32_
   return cudaGetLastError();
 }
 
+// Prefix rows of every inner node from its keys: one warp per 32 nodes reads
+// their headers (one sector each), then writes the rows of the inner ones.
+__global__ void __launch_bounds__(256) pfx_rebuild_kernel(DevTree t) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t n_nodes = min(t.ctrl->n_nodes, t.cap);
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t b = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; b < n_nodes; b += warps * 32) {
+    const uint32_t mine = b + lane;
+    const bool inner = mine < n_nodes && hdr_level(t.keys[(size_t)mine * 32 + 31]) > 0;
+    uint32_t todo = __ballot_sync(0xffffffffu, inner);
+    while (todo) {
+      const uint32_t nd = b + (uint32_t)(__ffs(todo) - 1);
+      todo &= todo - 1;
+      const uint64_t k = t.keys[(size_t)nd * 32 + lane];
+      t.pfx[(size_t)nd * 32 + lane] = lane < 31 ? (uint32_t)(k >> 32) : 0xffffffffu;
+    }
+  }
+}
+
+static cudaError_t ensure_pfx(Handle* h, cudaStream_t s) {
+  if (h->pfx_valid) return cudaSuccess;
+  pfx_rebuild_kernel<<<(unsigned)h->sm_count * 8, 256, 0, s>>>(h->tree);
+  count_launch();
+  h->pfx_valid = true;
+  return cudaGetLastError();
+}
+
 cudaError_t launch_search(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev, size_t n,
                           uint64_t* out_vals, uint8_t* out_st, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
@@ -751,8 +780,14 @@ cudaError_t launch_search(Handle* h, const uint64_t* qkeys, const uint32_t* list
     }
     if (blocks > cap) blocks = cap;
     if (blocks == 0) blocks = 1;
-#define BT_S2(GG, CC) search2_kernel<GG, false, CC><<<(unsigned)blocks, threads, 0, s>>>(h->tree, qkeys, list, n_dev, n, out_vals, out_st)
     const bool child = h->search_pairs == 2;
+    // the separators' prefixes (child-id form only)
+    const int use_pfx = child && h->use_pfx ? 1 : 0;
+    if (use_pfx) {
+      const cudaError_t pe = ensure_pfx(h, s);
+      if (pe != cudaSuccess) return pe;
+    }
+#define BT_S2(GG, CC) search2_kernel<GG, false, CC><<<(unsigned)blocks, threads, 0, s>>>(h->tree, qkeys, list, n_dev, n, out_vals, out_st, use_pfx)
     if (G == 4) { if (child) BT_S2(4, true); else BT_S2(4, false); }
     else if (G == 16) { if (child) BT_S2(16, true); else BT_S2(16, false); }
     else { if (child) BT_S2(8, true); else BT_S2(8, false); }
