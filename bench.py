@@ -335,7 +335,7 @@ def main():
     ap.add_argument("--search-pct", type=int, default=95)
     ap.add_argument("--dist", default="uniform", choices=["uniform", "zipf", "normal", "gamma"])
     ap.add_argument("--descent", default="both", choices=["plain", "learned", "both"])
-    ap.add_argument("--search-group", type=int, default=8)
+    ap.add_argument("--search-group", type=int, default=4)
     ap.add_argument("--engine", default="merge", choices=["merge", "stm"],
                     help="insert engine of the sorted batch: segmented leaf merge or warp STM")
     ap.add_argument("--no-cpu-baseline", action="store_true")

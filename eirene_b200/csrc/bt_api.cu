@@ -133,7 +133,7 @@ int bt_config_init(bt_config* c) {
   c->inner_fill = 24;
   c->retry_limit = 1u << 16;
   c->device = 0;
-  c->search_group = 8;
+  c->search_group = 4;
   c->n_segments = 4096;
   c->window = 64;
   return BT_OK;

@@ -147,7 +147,7 @@ struct Handle {
   uint32_t retry_limit = 1u << 16;
   int descent = 0;     // 0 plain, 1 learned
   uint32_t epoch = 0;  // tree epoch, bumped by every reset / bulk build
-  int search_group = 8;  // lanes per request in the lock-free search
+  int search_group = 4;  // lanes per request in the lock-free search
   int learned_group = 8;  // lanes per request in the learned search
   int sorted_search = 1;  // batch GET phase: 1 = path-reusing search over the sorted keys
   int sorted_leaf_vals = 0;  // sorted search: load the leaf's values with its keys (1) or only the match (0)

@@ -76,7 +76,8 @@ typedef struct bt_config {
     uint32_t inner_fill;   /* keys per inner node for bulk build and merge splits (default 24) */
     uint32_t retry_limit;  /* STM attempts per request before BT_ST_RETRY_EXHAUSTED (default 65536) */
     int32_t device;        /* CUDA device ordinal (default 0) */
-    uint32_t search_group; /* lanes per request in the search kernel: 4, 8, 16 or 32 (default 8) */
+    uint32_t search_group; /* lanes per request in the search kernel: 4, 8, 16 or 32 (default 4; bt_autotune
+                            * picks the fastest on the live tree) */
     uint32_t n_segments;   /* learned predictor: leaf segments (default 4096) */
     uint32_t window;       /* learned predictor: max error window in leaf slots (default 64) */
     uint32_t reserved[7];
