@@ -479,6 +479,9 @@ static int batch_hashed(Handle* h, const uint64_t* keys, const uint64_t* vals, c
   cudaStream_t s2 = ov ? h->hi_stream : s;
   const bool pass_side = ov && h->vals_wait != nullptr;
   auto fork = [&]() {
+    // a stale prefix table is rebuilt before the fork, so that the locates
+    // (side stream) and the lookups (`s`) both come after the rebuild
+    if (early && h->use_pfx && (tree_join(h, s) != cudaSuccess || ensure_pfx(h, s) != cudaSuccess)) return false;
     return cudaEventRecord(h->fork_ev, s) == cudaSuccess && cudaStreamWaitEvent(s2, h->fork_ev, 0) == cudaSuccess;
   };
   if (pass_side && !fork()) return -2;

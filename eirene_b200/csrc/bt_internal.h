@@ -217,6 +217,8 @@ void prof_mark(Handle* h, int which, cudaStream_t s);
 void prof_set_layout(Handle* h, int layout);
 
 // ---- tree kernels (bt_tree.cu) ----
+// make tree.pfx match every inner row (a rebuild when stale), stream ordered
+cudaError_t ensure_pfx(Handle* h, cudaStream_t s);
 cudaError_t tree_reset(Handle* h, cudaStream_t s);
 int tree_bulk_build(Handle* h, const uint64_t* keys, const uint64_t* vals, size_t n, cudaStream_t s);
 // caller-provided scratch for the bulk build (used by the no-allocation entry point)

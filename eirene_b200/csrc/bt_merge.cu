@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(256) merge_locate_kernel(DevTree t, const uint
                                                            uint32_t* __restrict__ path, uint32_t* __restrict__ mleaf,
                                                            uint32_t* __restrict__ isnew,
                                                            uint64_t* __restrict__ vpos, uint64_t* __restrict__ uans,
-                                                           uint8_t* __restrict__ uans_st) {
+                                                           uint8_t* __restrict__ uans_st, int use_pfx) {
   constexpr int S = 32 / G;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t g = lane % G;
@@ -169,6 +169,34 @@ __global__ void __launch_bounds__(256) merge_locate_kernel(DevTree t, const uint
     } else {
       for (;;) {
         const size_t row = (size_t)node * 32 + g * S;
+        if (use_pfx && level > 0) {
+          // inner level from the separators' prefixes, then the one separator
+          // (the child's upper bound) and the one child id
+          uint32_t pf[S];
+          load_pfx<S>(t.pfx + row, pf, l2_keep());
+          const uint32_t x = pfx_rank<G, S>(pf, key, g, gmask);
+          cnt = x & 0xffffu;
+          if (x >> 16) {  // a separator shares the key's prefix: rank with the full keys
+            load_slots<S>(t.keys + row, k);
+            if (g == G - 1) k[S - 1] = kKeyMax;
+            uint32_t c = 0;
+#pragma unroll
+            for (int i = 0; i < S; i++) c += (k[i] <= key) ? 1u : 0u;
+            cnt = group_sum<G>(c, gmask);
+          }
+          // the separator after the chosen child (slot 31 is the header: none)
+          const uint64_t sep = cnt < 31 ? t.keys[(size_t)node * 32 + cnt] : kKeyMax;
+          const uint64_t child_hi = sep < hi ? sep : hi;
+          node = (uint32_t)t.vals[(size_t)node * 32 + cnt];
+          hi = child_hi;
+          level--;
+          if (g == level) {
+            c_node = node;
+            c_hi = hi;
+            c_valid = true;
+          }
+          continue;
+        }
         load_slots<S>(t.keys + row, k);
         if (level > 0) load_slots<S>(t.vals + row, v);
         if (g == G - 1) k[S - 1] = kKeyMax;
@@ -790,6 +818,8 @@ int merge_locate_phase(Handle* h, cudaStream_t s) {
   const uint32_t* n_ins = &w.counts->n_ins;
   merge_ensure_root_kernel<<<1, 1, 0, s>>>(h->tree);
   count_launch();
+  const int use_pfx = h->use_pfx ? 1 : 0;
+  if (use_pfx && ensure_pfx(h, s) != cudaSuccess) return -2;
   if (cudaMemsetAsync(mc, 0, sizeof(MergeCounts), s) != cudaSuccess) return -2;
   static int per_sm[64] = {};
   if (h->device < 64 && per_sm[h->device] == 0) {
@@ -800,7 +830,7 @@ int merge_locate_phase(Handle* h, cudaStream_t s) {
   }
   const size_t blocks = (size_t)h->sm_count * (h->device < 64 ? per_sm[h->device] : 4);
   merge_locate_kernel<8><<<(unsigned)blocks, 256, 0, s>>>(h->tree, w.ukeys, w.uvals, w.ins_list, n_ins, w.m_path,
-                                                          w.m_leaf, w.m_isnew, w.m_vpos, w.uans, w.uans_st);
+                                                          w.m_leaf, w.m_isnew, w.m_vpos, w.uans, w.uans_st, use_pfx);
   count_launch();
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }

@@ -745,7 +745,7 @@ __global__ void __launch_bounds__(256) pfx_rebuild_kernel(DevTree t) {
   }
 }
 
-static cudaError_t ensure_pfx(Handle* h, cudaStream_t s) {
+cudaError_t ensure_pfx(Handle* h, cudaStream_t s) {
   if (h->pfx_valid) return cudaSuccess;
   pfx_rebuild_kernel<<<(unsigned)h->sm_count * 8, 256, 0, s>>>(h->tree);
   count_launch();
