@@ -99,7 +99,7 @@ EXPORTS = [
     "bt_profile", "bt_profile_read", "bt_launch_count", "bt_bulk_build_static",
     "bt_set_learned_group", "bt_learned_info", "bt_mlp_grad", "bt_set_option", "bt_autotune",
     "bt_serve_config_init", "bt_serve_start", "bt_submit", "bt_poll", "bt_wait", "bt_serve_get_stats", "bt_serve_stop",
-    "bt_route_batch", "bt_unroute_results", "bt_save", "bt_load", "bt_range_batch", "bt_sync",
+    "bt_route_batch", "bt_unroute_results", "bt_save", "bt_load", "bt_range_batch", "bt_sync", "bt_save_image", "bt_load_image",
 ]
 MAX_SHARDS = 256
 OPT_SORTED_SEARCH, OPT_RETRY_LIMIT, OPT_TRAIN_STEPS, OPT_SORTED_LEAF_VALS, OPT_BATCH_DESCENT = 1, 2, 3, 4, 5
@@ -177,6 +177,8 @@ def lib():
             "bt_save": [_P, ctypes.c_char_p],
             "bt_range_batch": [_P, _P, _P, _SZ, ctypes.c_uint32, _P, _P, _P, _P],
             "bt_sync": [_P, _P],
+            "bt_save_image": [_P, ctypes.c_char_p],
+            "bt_load_image": [_P, ctypes.c_char_p],
             "bt_load": [_P, ctypes.c_char_p],
         }
         for name, args in sig.items():
@@ -402,6 +404,14 @@ class BTree:
     def load(self, path: str):
         """Replace the contents with a snapshot file (bt_load; a fresh bulk load)."""
         _check(lib().bt_load(self._h, os.fsencode(path)), "bt_load")
+
+    def save_image(self, path: str):
+        """Write the node pool itself to a file (bt_save_image)."""
+        _check(lib().bt_save_image(self._h, os.fsencode(path)), "bt_save_image")
+
+    def load_image(self, path: str):
+        """Restore a pool image, leaf layout included (bt_load_image)."""
+        _check(lib().bt_load_image(self._h, os.fsencode(path)), "bt_load_image")
 
     def set_search_group(self, lanes: int):
         _check(lib().bt_set_search_group(self._h, lanes), "bt_set_search_group")

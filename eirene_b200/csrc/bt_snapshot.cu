@@ -28,6 +28,8 @@ namespace {
 
 constexpr char kMagic[8] = {'E', 'I', 'R', 'B', '2', 'S', 'N', 'P'};
 constexpr uint32_t kVersion = 1;
+constexpr char kImgMagic[8] = {'E', 'I', 'R', 'B', '2', 'I', 'M', 'G'};
+constexpr uint32_t kImgVersion = 1;
 
 uint64_t fnv1a(const void* p, size_t bytes, uint64_t h) {
   const unsigned char* b = static_cast<const unsigned char*>(p);
@@ -125,6 +127,117 @@ int bt_load(bt_handle* h, const char* path) {
          cudaMemcpy(dv.p, vals.data(), n * 8, cudaMemcpyHostToDevice) != cudaSuccess))
       rc = BT_ERR_CUDA;
     if (rc == BT_OK) rc = bt_bulk_build(h, (const uint64_t*)dk.p, (const uint64_t*)dv.p, n, nullptr);
+  }
+  if (prev >= 0) cudaSetDevice(prev);
+  return rc;
+}
+
+// Pool image: the node pool itself (the rows of every allocated node, their
+// low fences and the control block), so a loaded tree keeps the saved leaf
+// layout and goes on exactly as the saved one would (the merge engine is
+// deterministic).  The loading handle needs a pool of at least n_nodes
+// nodes; its learned model and separator prefixes are rebuilt on demand.
+//
+// File layout (little endian):
+//   0   8 B  magic "EIRB2IMG"
+//   8   4 B  format version (1)
+//   12  4 B  sizeof(Ctrl)
+//   16  8 B  n_nodes
+//   24  8 B  FNV-1a 64 over the control block, key rows, value rows, lows
+//   32       control block
+//   ...      n_nodes key rows (256 B), n_nodes value rows, n_nodes low fences (8 B)
+int bt_save_image(bt_handle* h, const char* path) {
+  if (!h || !path) return BT_ERR_INVALID_ARG;
+  bt::Handle& H = h->h;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(H.device);
+  int rc = BT_OK;
+  bt::Ctrl c{};
+  std::vector<uint64_t> keys, vals, low;
+  uint64_t nn = 0;
+  if (cudaDeviceSynchronize() != cudaSuccess || bt::tree_sync(&H) != cudaSuccess ||
+      cudaMemcpy(&c, H.tree.ctrl, sizeof(c), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    rc = BT_ERR_CUDA;
+  } else {
+    nn = c.n_nodes < H.tree.cap ? c.n_nodes : H.tree.cap;
+    keys.resize(nn * 32);
+    vals.resize(nn * 32);
+    low.resize(nn);
+    if (nn && (cudaMemcpy(keys.data(), H.tree.keys, nn * 256, cudaMemcpyDeviceToHost) != cudaSuccess ||
+               cudaMemcpy(vals.data(), H.tree.vals, nn * 256, cudaMemcpyDeviceToHost) != cudaSuccess ||
+               cudaMemcpy(low.data(), H.tree.low, nn * 8, cudaMemcpyDeviceToHost) != cudaSuccess))
+      rc = BT_ERR_CUDA;
+  }
+  if (prev >= 0) cudaSetDevice(prev);
+  if (rc != BT_OK) return rc;
+  uint64_t sum = fnv1a(&c, sizeof(c), 0xCBF29CE484222325ull);
+  sum = fnv1a(keys.data(), nn * 256, sum);
+  sum = fnv1a(vals.data(), nn * 256, sum);
+  sum = fnv1a(low.data(), nn * 8, sum);
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return BT_ERR_IO;
+  const uint32_t ver[2] = {kImgVersion, (uint32_t)sizeof(c)};
+  bool ok = std::fwrite(kImgMagic, 1, 8, f) == 8 && std::fwrite(ver, 4, 2, f) == 2 &&
+            std::fwrite(&nn, 8, 1, f) == 1 && std::fwrite(&sum, 8, 1, f) == 1 && std::fwrite(&c, sizeof(c), 1, f) == 1 &&
+            (nn == 0 || (std::fwrite(keys.data(), 256, nn, f) == nn && std::fwrite(vals.data(), 256, nn, f) == nn &&
+                         std::fwrite(low.data(), 8, nn, f) == nn));
+  ok = (std::fclose(f) == 0) && ok;
+  return ok ? BT_OK : BT_ERR_IO;
+}
+
+int bt_load_image(bt_handle* h, const char* path) {
+  if (!h || !path) return BT_ERR_INVALID_ARG;
+  bt::Handle& H = h->h;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return BT_ERR_IO;
+  char magic[8];
+  uint32_t ver[2];
+  uint64_t nn = 0, sum = 0;
+  bt::Ctrl c{};
+  bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, kImgMagic, 8) == 0 && std::fread(ver, 4, 2, f) == 2 &&
+            ver[0] == kImgVersion && ver[1] == sizeof(c) && std::fread(&nn, 8, 1, f) == 1 &&
+            std::fread(&sum, 8, 1, f) == 1 && std::fread(&c, sizeof(c), 1, f) == 1;
+  // the rows must fill the rest of the file exactly
+  long here = ok ? std::ftell(f) : -1;
+  if (ok && std::fseek(f, 0, SEEK_END) == 0) {
+    const long end = std::ftell(f);
+    ok = here >= 0 && end >= here && (uint64_t)(end - here) == nn * 520 && std::fseek(f, here, SEEK_SET) == 0;
+  } else {
+    ok = false;
+  }
+  std::vector<uint64_t> keys, vals, low;
+  if (ok) {
+    keys.resize(nn * 32);
+    vals.resize(nn * 32);
+    low.resize(nn);
+    ok = nn == 0 || (std::fread(keys.data(), 256, nn, f) == nn && std::fread(vals.data(), 256, nn, f) == nn &&
+                     std::fread(low.data(), 8, nn, f) == nn);
+  }
+  std::fclose(f);
+  if (!ok) return BT_ERR_IO;
+  uint64_t chk = fnv1a(&c, sizeof(c), 0xCBF29CE484222325ull);
+  chk = fnv1a(keys.data(), nn * 256, chk);
+  chk = fnv1a(vals.data(), nn * 256, chk);
+  chk = fnv1a(low.data(), nn * 8, chk);
+  if (chk != sum || c.n_nodes != nn || (c.root != bt::kNil && c.root >= nn) || c.epoch == 0 || c.epoch > 0x7fffu)
+    return BT_ERR_IO;
+  if (nn > H.tree.cap) return BT_ERR_NO_MEMORY;  // the pool cannot hold the saved nodes
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(H.device);
+  int rc = BT_OK;
+  c.root_lock &= ~1u;  // saved at rest: unlocked
+  if (cudaDeviceSynchronize() != cudaSuccess || bt::tree_sync(&H) != cudaSuccess ||
+      (nn && (cudaMemcpy(H.tree.keys, keys.data(), nn * 256, cudaMemcpyHostToDevice) != cudaSuccess ||
+              cudaMemcpy(H.tree.vals, vals.data(), nn * 256, cudaMemcpyHostToDevice) != cudaSuccess ||
+              cudaMemcpy(H.tree.low, low.data(), nn * 8, cudaMemcpyHostToDevice) != cudaSuccess)) ||
+      cudaMemcpy(H.tree.ctrl, &c, sizeof(c), cudaMemcpyHostToDevice) != cudaSuccess)
+    rc = BT_ERR_CUDA;
+  if (rc == BT_OK) {
+    H.epoch = c.epoch;  // the rows carry the saved tree's epoch
+    H.L.valid = false;
+    H.pfx_valid = false;
   }
   if (prev >= 0) cudaSetDevice(prev);
   return rc;

@@ -346,6 +346,14 @@ int bt_unroute_results(bt_handle *h, const uint32_t *perm, const uint64_t *in_va
  * BT_ERR_IO for file errors, a bad magic, size, checksum or key order. */
 int bt_save(bt_handle *h, const char *path);
 int bt_load(bt_handle *h, const char *path);
+/* Pool image: bt_save_image writes the node pool itself (every allocated
+ * node's key and value rows, low fences and the control block);
+ * bt_load_image restores it into h, whose pool must hold as many nodes
+ * (else BT_ERR_NO_MEMORY), so the loaded tree keeps the saved leaf layout
+ * and continues exactly as the saved one would.  Synchronous; BT_ERR_IO for
+ * file errors, a bad magic, size or checksum. */
+int bt_save_image(bt_handle *h, const char *path);
+int bt_load_image(bt_handle *h, const char *path);
 
 /* Static text for a status code. */
 const char *bt_status_string(int code);

@@ -61,3 +61,48 @@ def test_empty_tree_and_damaged_files(gpu, tmp_path):
     assert ei.value.code == -11
     # a failed load leaves the tree as it was
     assert t.size() == 1000
+
+
+def test_pool_image_keeps_layout_and_continues(gpu, tmp_path):
+    # the image holds the pool itself: the loaded tree has the saved leaf
+    # layout, and the next merge-engine batch runs identically on both
+    keys = O.gen_keys("gamma", 61, 100_000)
+    vals = O.value_of(keys)
+    t = E.BTree(max_keys=1 << 20, max_batch=1 << 17)
+    t.bulk_build(dev(keys), dev(vals))
+    o = O.OracleTree()
+    o.bulk_build(keys, vals)
+    for b in range(3):
+        rk, rv, ro = O.gen_requests("gamma", 62 + b, keys, 60_000, 50)
+        o.execute_merged(rk, rv, ro, engine=O.ENGINE_MERGE)
+        run_batch(t, rk, rv, ro, E.MODE_SORTED | E.MODE_MERGE_ENGINE)
+    path = str(tmp_path / "tree.img")
+    t.save_image(path)
+    n_nodes = t.stats()["n_nodes"]
+    assert os.path.getsize(path) == 32 + 104 + 520 * n_nodes  # header, control block, rows and lows
+    t2 = E.BTree(max_keys=1 << 20, max_batch=1 << 17)
+    t2.load_image(path)
+    ak, av = dump(t)
+    bk, bv = dump(t2)
+    assert (ak == bk).all() and (av == bv).all()
+    assert (t.leaf_sizes() == t2.leaf_sizes()).all() and (t.level_counts() == t2.level_counts()).all()
+    assert t2.size() == t.size() == o.size()
+    rk, rv, ro = O.gen_requests("gamma", 70, keys, 60_000, 50)
+    ov, os_ = o.execute_merged(rk, rv, ro, engine=O.ENGINE_MERGE)
+    g1 = run_batch(t, rk, rv, ro, E.MODE_SORTED | E.MODE_MERGE_ENGINE)
+    g2 = run_batch(t2, rk, rv, ro, E.MODE_SORTED | E.MODE_MERGE_ENGINE)
+    assert (g2[1] == os_).all() and (g2[0] == ov).all()
+    assert (g1[1] == g2[1]).all() and (g1[0] == g2[0]).all()
+    assert (t.leaf_sizes() == t2.leaf_sizes()).all()
+    assert (t2.leaf_sizes() == o.leaf_sizes()).all()
+    # damaged image, and a pool too small for it
+    raw = bytearray(open(path, "rb").read())
+    raw[200] ^= 1
+    bad = str(tmp_path / "bad.img")
+    open(bad, "wb").write(bytes(raw))
+    with pytest.raises(E.BTError) as ei:
+        E.BTree(max_keys=1 << 20, max_batch=1 << 12).load_image(bad)
+    assert ei.value.code == -11
+    with pytest.raises(E.BTError) as ei:
+        E.BTree(max_keys=0, max_batch=1 << 12).load_image(path)
+    assert ei.value.code == -3  # BT_ERR_NO_MEMORY
