@@ -53,7 +53,7 @@ int main(int argc, char* argv[]) {
         if (test_flag) tree->test();
         break;
       case 'r':
-        std::fprintf(stderr, "-r (range files): not supported by this build\n");
+        std::fprintf(stderr, "-r (range files): not supported by this driver\n");
         return 2;
       default:
         std::fprintf(stderr, "usage: %s -v{38,39,40,41} [-t] -i file [-i file ...]\n", argv[0]);

@@ -9,7 +9,7 @@ time of its kernels, transfers excluded: v39 times the kernel only, v38 all
 phases); this library is timed the same way (device time of bt_execute_batch
 over resident inputs).
 
-    python oracle/ref_bench.py --batches 10 > gpurun_out/ref_bench.json
+    python oracle/ref_bench.py --batches 10 > ref_bench.json
 """
 from __future__ import annotations
 
