@@ -103,8 +103,8 @@ struct Work {
   // hash front end (bt_front.cu)
   void* f_tab = nullptr;         // 16 B slots
   size_t f_tab_cap = 0;          // slots allocated (power of two)
-  uint32_t* f_flags = nullptr;   // [cap]
-  uint32_t* f_pos = nullptr;     // [cap]
+  uint32_t* f_flags = nullptr;   // [cap] words; the flag pass uses them as one "touched" byte per request
+  uint32_t* f_pos = nullptr;     // [cap] per-tile touched counts, then the tiles' exclusive offsets
   uint32_t* f_list = nullptr;    // [cap] requests for the plain lookup, in input order
   uint64_t* f_tk = nullptr;      // [cap] keys of the touched requests, in input order
   uint32_t* f_tv = nullptr;      // [cap] index | op << 30 of the touched requests
