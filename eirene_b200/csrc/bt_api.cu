@@ -526,7 +526,7 @@ int bt_set_option(bt_handle* H, int option, int64_t value) {
     case BT_OPT_ASYNC_WRITE: H->h.async_write = value ? 1 : 0; return BT_OK;
     case BT_OPT_TOP_CACHE: H->h.top_cache = value ? 1 : 0; return BT_OK;
     case BT_OPT_OVERLAP:
-      // 0 off; 1 on (default reserve); > 1 on, leaving value - 1 lookup block slots for the sort
+      // 0 off; 1 on (default reserve); > 1 on, leaving value - 1 lookup block slots for the side stream
       if (value < 0) return BT_ERR_INVALID_ARG;
       H->h.overlap = value ? 1 : 0;
       if (value > 1) H->h.overlap_reserve = (int)(value - 1);

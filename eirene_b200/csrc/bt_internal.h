@@ -175,8 +175,9 @@ struct Handle {
   std::vector<cudaEvent_t> prof_ev;  // kProfEvents events per recorded batch
   std::vector<char> prof_layout;     // per recorded batch: kLayout* bits (see prof_resolve)
   size_t prof_batches = 0;
-  // hash front end: the touched requests' sort + merge run on a high-priority
-  // side stream while the lookups run on the caller's stream
+  // hash front end: the merge engine's locates and grouping (and, while the
+  // values are still being copied in, the merge passes) run on a
+  // high-priority side stream while the lookups run on the caller's stream
   cudaStream_t hi_stream = nullptr;
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   int overlap = 1;
