@@ -805,7 +805,8 @@ __global__ void __launch_bounds__(256, 4) stm_kernel(DevTree t, const uint64_t* 
 // into a ring of descriptors; `tail` counts published batches and `cursor` is
 // the oldest batch that still has unclaimed requests.  Every warp claims
 // kServeChunk consecutive requests of the cursor batch, runs them (v39
-// meaning: batches in flight together interleave), and the warp that
+// meaning: batches in flight together interleave; the chunk's GETs go first,
+// four at a time, get_pass), and the warp that
 // completes a batch writes its sequence number and the device clock to host
 // memory.  A warp that finds no work sleeps; after idle_ns without work (or
 // when stop is set) the kernel exits and the host relaunches it on demand.
