@@ -150,7 +150,9 @@ int bt_execute_batch(bt_handle *h, const uint64_t *keys, const uint64_t *vals, c
 int bt_execute_batch_host(bt_handle *h, const uint64_t *keys, const uint64_t *vals, const uint8_t *ops,
                           uint64_t *out_vals, uint8_t *out_status, size_t n, int mode, void *stream);
 
-/* Convenience wrappers: all-GET and all-INSERT batches in BT_MODE_SORTED. */
+/* Convenience wrappers: all-GET and all-INSERT batches in BT_MODE_SORTED,
+ * the reference's single-mission input (prepareInput(file, mission),
+ * src/tree.h:34). */
 int bt_search_batch(bt_handle *h, const uint64_t *keys, uint64_t *out_vals, uint8_t *out_status, size_t n,
                     void *stream);
 int bt_insert_batch(bt_handle *h, const uint64_t *keys, const uint64_t *vals, uint64_t *out_vals,
@@ -166,7 +168,7 @@ int bt_insert_batch(bt_handle *h, const uint64_t *keys, const uint64_t *vals, ui
 int bt_range_batch(bt_handle *h, const uint64_t *lo, const uint64_t *hi, size_t n, uint32_t max_per,
                    uint64_t *out_keys, uint64_t *out_vals, uint32_t *out_counts, void *stream);
 
-/* Number of keys (synchronous). */
+/* Number of keys (synchronous).  No reference counterpart. */
 int bt_size(bt_handle *h, uint64_t *n_keys);
 
 /* All pairs in ascending key order into device buffers of `cap` entries;
@@ -175,7 +177,8 @@ int bt_size(bt_handle *h, uint64_t *n_keys);
 int bt_dump_sorted(bt_handle *h, uint64_t *keys, uint64_t *vals, size_t cap, size_t *n_out, void *stream);
 
 /* Host arrays: leaf sizes in key order (cap entries) and node counts per level
- * (leaf level first).  Synchronous.  Used to check split counts. */
+ * (leaf level first).  Synchronous.  Used to check split counts against the
+ * oracle; no reference counterpart. */
 int bt_leaf_sizes(bt_handle *h, uint32_t *sizes_host, size_t cap, size_t *n_leaves);
 int bt_level_counts(bt_handle *h, uint64_t *counts_host, uint32_t cap, uint32_t *height);
 
@@ -192,8 +195,11 @@ int bt_retrain(bt_handle *h, void *stream);
 int bt_set_descent(bt_handle *h, int descent);
 /* stage 1 root model: 1 = 1->32->1 MLP (default), 0 = linear */
 int bt_set_root_model(bt_handle *h, int mlp);
+/* lanes per request of the unsorted search (the reference fixes one warp per
+ * request at compile time, src/gpu-stm-tree-v39/bpt-gpustm.h:25-38) */
 int bt_set_search_group(bt_handle *h, uint32_t lanes);
-/* Tuning options (bt_set_option). */
+/* Tuning options (bt_set_option); no reference counterpart (its variants are
+ * compile-time, src/gpu-stm-tree-v39/bpt-gpustm.h:25-38). */
 #define BT_OPT_SORTED_SEARCH 1 /* 1 (default): the batch's GET phase reuses the descent path across its
                                   ascending unique keys; 0: one root descent per key */
 #define BT_OPT_RETRY_LIMIT 2   /* STM attempts per request */
@@ -239,7 +245,9 @@ int bt_sync(bt_handle *h, void *stream);
  * [14] sorted learned ms.  No reference counterpart (the reference's launch
  * shape is compile-time, src/gpu-stm-tree-v39/bpt-gpustm.h:25-38). */
 int bt_autotune(bt_handle *h, const uint64_t *sample_keys, size_t n, void *stream, double *report);
-/* lanes per request in the learned search kernel: 8, 16 or 32 (default 8) */
+/* Learned predictor settings and diagnostics (no reference counterpart: the
+ * reference has no learned model).
+ * Lanes per request in the learned search kernel: 8, 16 or 32 (default 8). */
 int bt_set_learned_group(bt_handle *h, uint32_t lanes);
 /* info[8]: valid, n_leaves, n_segments, segments over the window, window,
  * final training loss, root model (1 MLP, 0 linear), training steps */
@@ -258,10 +266,12 @@ int bt_mlp_grad(bt_handle *h, const float *params, const float *x, const float *
  * synchronises on the recorded events and returns summed milliseconds. */
 int bt_profile(bt_handle *h, int enable);
 int bt_profile_read(bt_handle *h, double *phase_ms /* [5] */, uint64_t *batches, int reset);
-/* Kernels launched by this library in this process so far. */
+/* Kernels launched by this library in this process so far (no reference
+ * counterpart). */
 uint64_t bt_launch_count(void);
 
-/* Pinned host memory helpers for bt_execute_batch_host callers. */
+/* Pinned host memory helpers for bt_execute_batch_host callers (the
+ * reference copies from pageable vectors, src/gpu-stm-tree-v39/bpt-gpustm.cpp:78-105). */
 int bt_host_alloc(void **p, size_t bytes);
 int bt_host_free(void *p);
 
