@@ -322,6 +322,58 @@ def serve_bench(E, np, tree, tk_host, n_tree, seconds=1.5, seed=5, load=0.5):
 
 
 # ----------------------------------------------------------------------------
+def run_lookups(args):
+    """Unsorted point lookups only (one GPU): build a 2^tree-log2 tree, train
+    the model when the learned form is asked for, then time `steps` calls of
+    bt_search_batch over 2^batch-log2 keys (half present) per form."""
+    import torch
+
+    import eirene_b200 as E
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+    n_tree, n_b = 1 << args.tree_log2, 1 << args.batch_log2
+    pool = (1 << args.pool_keys_log2) if args.pool_keys_log2 else 2 * n_tree
+    tree = E.BTree(max_keys=pool, max_batch=n_b, search_group=args.search_group)
+    tk = torch.empty(n_tree, dtype=torch.int64, device="cuda")
+    tv = torch.empty(n_tree, dtype=torch.int64, device="cuda")
+    E.gen_keys(args.dist, 1, n_tree, tk, tv, stream)
+    tree.bulk_build(tk, tv, stream)
+    del tv
+    qk = torch.empty(n_b, dtype=torch.int64, device="cuda")
+    qv = torch.empty(n_b, dtype=torch.int64, device="cuda")
+    qo = torch.empty(n_b, dtype=torch.uint8, device="cuda")
+    E.gen_requests(args.dist, 40_000, tk, n_b, 100, qk, qv, qo, stream)
+    ov = torch.empty(n_b, dtype=torch.int64, device="cuda")
+    ost = torch.empty(n_b, dtype=torch.uint8, device="cuda")
+    out = {"workload": f"unsorted lookups of 2^{args.batch_log2} keys (half present) in a 2^{args.tree_log2}-key "
+                       f"{args.dist} tree", "steps": args.steps, "warmup": args.warmup}
+    forms = ["plain", "learned"] if args.descent == "both" else [args.descent]
+    for form in forms:
+        if form == "learned":
+            tree.retrain(stream)
+        tree.set_descent(form == "learned")
+        tune = None if args.no_autotune else tree.autotune(qk, stream)
+        for _ in range(args.warmup):
+            tree.search(qk, ov, ost, stream)
+        tree.reset_stats()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            tree.search(qk, ov, ost, stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        st = tree.stats()
+        out[form] = {"mops": n_b / ms / 1e3, "ms_per_call": ms,
+                     "dram_alg_gbs": BYTES_SEARCH * n_b / ms / 1e6,
+                     "learned_fallbacks": st["learned_fallbacks"], "learned_hits": st["learned_hits"],
+                     "autotune": tune}
+    print(json.dumps(out), flush=True)
+    tree.close()
+    return 0
+
+
 def unique_op_counts(torch, k, o):
     """(unique GET keys, unique INSERT keys) of a batch under the merged meaning."""
     u, inv = torch.unique(k, return_inverse=True)
@@ -351,16 +403,26 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=1.5)
     ap.add_argument("--retrain-every", type=int, default=0,
                     help="learned form: retrain the model after every K timed batches (0: trained once, before)")
+    ap.add_argument("--retrain-mode", default="refit", choices=["refit", "full"],
+                    help="retraining inside the timed region: refit (leaf array and segment lines follow the "
+                         "leaves, stage 1 kept) or full (stage 1 trained again from its initial parameters)")
     ap.add_argument("--front-end", default="hash", choices=["hash", "sort"],
                     help="sorted batches: hash front end (sort only INSERT-coupled requests) or full sort")
     ap.add_argument("--pool-keys-log2", type=int, default=0,
                     help="size the node pool for 2^x keys (default: 2 x tree + 32 x batch)")
+    ap.add_argument("--lookups-only", action="store_true",
+                    help="time only unsorted point lookups (bt_search_batch) of 2^batch-log2 keys, half present, "
+                         "with the --descent form(s); a small, bounded workload for kernel profiles")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="--lookups-only: keep the default launch shapes (no autotuner launches before timing)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
 
     if args.impl == "reference":
         return run_reference(args)
+    if args.lookups_only:
+        return run_lookups(args)
 
     import numpy as np
     import torch
@@ -476,7 +538,11 @@ def main():
         for s in range(args.steps):
             step(*batches[args.warmup + s])
             if learned and args.retrain_every > 0 and (s + 1) % args.retrain_every == 0:
-                tree.retrain(stream)  # inside the timed region: the model follows the tree
+                # inside the timed region: the model follows the tree
+                if args.retrain_mode == "refit":
+                    tree.refit(stream)
+                else:
+                    tree.retrain(stream)
             ev[s + 1].record(stream)  # the batch's answers are final
         tree.sync(stream)  # the last batch's deferred leaf/inner merge
         ev[-1].record(stream)
@@ -689,6 +755,7 @@ def main():
                                 if sharded is not None else "one tree on one GPU"),
                 "tree_build_s": build_s,
                 "learned_retrain_every": args.retrain_every,
+                "learned_retrain_mode": args.retrain_mode,
             },
             "roofline": roof,
             "cpu_baseline": cpu,

@@ -100,10 +100,12 @@ EXPORTS = [
     "bt_set_learned_group", "bt_learned_info", "bt_mlp_grad", "bt_set_option", "bt_autotune",
     "bt_serve_config_init", "bt_serve_start", "bt_submit", "bt_poll", "bt_wait", "bt_serve_get_stats", "bt_serve_stop",
     "bt_route_batch", "bt_unroute_results", "bt_save", "bt_load", "bt_range_batch", "bt_sync", "bt_save_image", "bt_load_image",
+    "bt_refit",
 ]
 MAX_SHARDS = 256
 OPT_SORTED_SEARCH, OPT_RETRY_LIMIT, OPT_TRAIN_STEPS, OPT_SORTED_LEAF_VALS, OPT_BATCH_DESCENT = 1, 2, 3, 4, 5
 OPT_FRONT_END, OPT_TOP_CACHE, OPT_SEARCH_PAIRS, OPT_OVERLAP, OPT_ASYNC_WRITE = 6, 7, 8, 9, 10
+OPT_REFIT_STEPS, OPT_LEARNED_MODE = 11, 12
 PHASES = ["sort", "merge", "search", "insert", "writeback"]
 
 _lib = None
@@ -148,6 +150,7 @@ def lib():
             "bt_stats_get": [_P, ctypes.POINTER(Stats), ctypes.c_int],
             "bt_stats_reset": [_P],
             "bt_retrain": [_P, _P],
+            "bt_refit": [_P, _P],
             "bt_set_descent": [_P, ctypes.c_int],
             "bt_set_root_model": [_P, ctypes.c_int],
             "bt_set_search_group": [_P, ctypes.c_uint32],
@@ -324,6 +327,11 @@ class BTree:
     def retrain(self, stream=None):
         _check(lib().bt_retrain(self._h, _stream_ptr(stream)), "bt_retrain")
 
+    def refit(self, stream=None):
+        """Incremental retraining: the leaf array and segment lines follow the
+        current leaves; the trained stage-1 model is kept."""
+        _check(lib().bt_refit(self._h, _stream_ptr(stream)), "bt_refit")
+
     def set_descent(self, learned: bool):
         _check(lib().bt_set_descent(self._h, DESCENT_LEARNED if learned else DESCENT_PLAIN), "bt_set_descent")
 
@@ -354,7 +362,9 @@ class BTree:
         r = list(rep)
         return {"plain_lanes": int(r[0]), "learned_lanes": int(r[1]), "sorted_leaf_vals": int(r[2]),
                 "batch_descent": "learned" if r[3] == 1 else "plain",
-                "plain_ms": dict(zip([4, 8, 16, 32], r[4:8])), "learned_ms": dict(zip([8, 16, 32], r[8:11])),
+                "learned_mode": int(r[15]),
+                "plain_ms": dict(zip([4, 8, 16, 32], r[4:8])),
+                "learned_ms": dict(zip(["4 pipelined", "8 pipelined", "4x1", "4x2"], r[8:12])),
                 "sorted_plain_ms": r[12:14], "sorted_learned_ms": r[14]}
 
     def set_learned_group(self, lanes: int):

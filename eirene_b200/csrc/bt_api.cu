@@ -330,7 +330,7 @@ int bt_search_batch(bt_handle* H, const uint64_t* keys, uint64_t* out_vals, uint
   cudaError_t e = bt::tree_join(&h, S(stream));
   if (e != cudaSuccess) return BT_ERR_CUDA;
   if (h.descent == BT_DESCENT_LEARNED && h.L.valid)
-    e = bt::launch_learned_search(&h, keys, nullptr, nullptr, n, out_vals, out_status, S(stream), false);
+    e = bt::launch_learned_lookup(&h, keys, nullptr, nullptr, n, out_vals, out_status, S(stream));
   else
     e = bt::launch_search(&h, keys, nullptr, nullptr, n, out_vals, out_status, S(stream));
   return e == cudaSuccess ? BT_OK : BT_ERR_CUDA;
@@ -465,6 +465,18 @@ int bt_retrain(bt_handle* H, void* stream) {
   return map_internal(bt::learned_retrain(&H->h, s));
 }
 
+int bt_refit(bt_handle* H, void* stream) {
+  if (!H) return BT_ERR_INVALID_ARG;
+  if (!H->h.L.trained) return BT_ERR_NOT_TRAINED;
+  DeviceGuard g(H->h.device);
+  cudaStream_t s = stream ? S(stream) : H->h.internal_stream;
+  if (stream == nullptr) cudaDeviceSynchronize();
+  if (bt::tree_join(&H->h, s) != cudaSuccess) return BT_ERR_CUDA;
+  const int rc = map_internal(bt::learned_retrain(&H->h, s, true));
+  if (rc == BT_OK && stream == nullptr && cudaStreamSynchronize(s) != cudaSuccess) return BT_ERR_CUDA;
+  return rc;
+}
+
 int bt_set_descent(bt_handle* H, int descent) {
   if (!H || (descent != BT_DESCENT_PLAIN && descent != BT_DESCENT_LEARNED)) return BT_ERR_INVALID_ARG;
   if (descent == BT_DESCENT_LEARNED && !H->h.L.valid) return BT_ERR_NOT_TRAINED;
@@ -547,6 +559,14 @@ int bt_set_option(bt_handle* H, int option, int64_t value) {
       if (value < 0 || value > 1000000) return BT_ERR_INVALID_ARG;
       H->h.L.train_steps = (uint32_t)value;
       return BT_OK;
+    case BT_OPT_REFIT_STEPS:
+      if (value < 0 || value > 1000000) return BT_ERR_INVALID_ARG;
+      H->h.L.refit_steps = (uint32_t)value;
+      return BT_OK;
+    case BT_OPT_LEARNED_MODE:
+      if (value < 1 || value > 3) return BT_ERR_INVALID_ARG;
+      H->h.learned_mode = (int)value;
+      return BT_OK;
     default: return BT_ERR_INVALID_ARG;
   }
 }
@@ -562,20 +582,29 @@ int bt_autotune(bt_handle* H, const uint64_t* sample_keys, size_t n, void* strea
 
 int bt_set_learned_group(bt_handle* H, uint32_t lanes) {
   if (!H) return BT_ERR_INVALID_ARG;
-  if (lanes != 8 && lanes != 16 && lanes != 32) return BT_ERR_INVALID_ARG;
+  if (lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32) return BT_ERR_INVALID_ARG;
   H->h.learned_group = (int)lanes;
   return BT_OK;
 }
 
 int bt_learned_info(bt_handle* H, double* info) {
   if (!H || !info) return BT_ERR_INVALID_ARG;
+  DeviceGuard g(H->h.device);
   const bt::Learned& L = H->h.L;
+  // the last (re)training's loss and segment count arrive in page-locked host words
+  if (cudaDeviceSynchronize() != cudaSuccess) return BT_ERR_CUDA;
+  float loss = 0.f;
+  uint32_t bad = 0;
+  if (L.host_words) {
+    std::memcpy(&loss, &L.host_words[0], 4);
+    bad = L.host_words[1];
+  }
   info[0] = L.valid ? 1.0 : 0.0;
   info[1] = (double)L.n_leaves;
   info[2] = (double)L.n_segments;
-  info[3] = (double)L.seg_fallback;
+  info[3] = (double)bad;
   info[4] = (double)L.window;
-  info[5] = L.last_loss;
+  info[5] = (double)loss;
   info[6] = (double)L.stage1;
   info[7] = (double)L.train_steps;
   return BT_OK;

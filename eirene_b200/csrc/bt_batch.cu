@@ -387,6 +387,7 @@ int work_alloc(Work* w, size_t cap) {
   A((void**)&w->f_flags, cap * 4);
   A((void**)&w->f_pos, cap * 4);
   A((void**)&w->f_list, cap * 4);
+  A((void**)&w->f_lk, cap * 8);
   A((void**)&w->f_tk, cap * 8);
   A((void**)&w->f_tv, cap * 4);
   if (!ok) {
@@ -403,7 +404,7 @@ void work_free(Work* w) {
                 w->m_path,   w->m_vpos,   w->m_leaf,    w->m_isnew,   w->m_pos,     w->m_newk,       w->m_newv,  w->m_nq,
                 w->m_nleaf,  w->m_seg,     w->d_leaf,    w->d_slot,    w->m_ent_a,   w->m_ent_b,   w->m_counts,     w->m_sync,      w->d_in_keys,
                 w->d_in_vals, w->d_in_ops, w->d_out_vals, w->d_out_st, w->f_tab, w->f_flags,
-                w->f_pos,    w->f_list,    w->f_tk,      w->f_tv};
+                w->f_pos,    w->f_list,    w->f_lk,      w->f_tk,      w->f_tv};
   for (void* p : ps)
     if (p) cudaFree(p);
   *w = Work{};
@@ -509,13 +510,14 @@ static int batch_hashed(Handle* h, const uint64_t* keys, const uint64_t* vals, c
   if (ov) prof_mark(h, 1, s);
   cudaError_t e;
   const int desc = h->batch_descent >= 0 ? h->batch_descent : h->descent;
+  h->lookup_reserve = ov ? h->overlap_reserve : 0;
+  // the lookups read their keys compacted (w.f_lk[q], written by the front
+  // end) instead of through the list (keys[f_list[q]]): one dependent load less
   if (desc == 1 && h->L.valid)
-    e = launch_learned_search(h, keys, w.f_list, &c->n_lookup, n, out_vals, out_st, s, false);
-  else {
-    h->lookup_reserve = ov ? h->overlap_reserve : 0;
-    e = launch_search(h, keys, w.f_list, &c->n_lookup, n, out_vals, out_st, s);
-    h->lookup_reserve = 0;
-  }
+    e = launch_learned_lookup(h, keys, w.f_list, &c->n_lookup, n, out_vals, out_st, s, w.f_lk);
+  else
+    e = launch_search(h, keys, w.f_list, &c->n_lookup, n, out_vals, out_st, s, w.f_lk);
+  h->lookup_reserve = 0;
   if (e != cudaSuccess) return -2;
   if (ov) {
     prof_mark(h, kEvLookupEnd, s);

@@ -138,8 +138,8 @@ __device__ __forceinline__ uint32_t find_first_from(const Slot* __restrict__ tab
 //                         the touched count of each tile;
 //   front_tile_scan_kernel  exclusive offsets of the tiles (one block) and
 //                         the two class counts;
-//   front_scatter_kernel  touched requests to (tk, tv), the rest to list,
-//                         both in input order.
+//   front_scatter_kernel  touched requests to (tk, tv), the rest to list and
+//                         their keys to lk, both in input order.
 // Every launch is fully parallel (no look-back chain between tiles): the
 // probes of the flag pass are its only dependent loads, and the scatter
 // reads the request's key and op again only when it is touched.
@@ -252,7 +252,8 @@ __global__ void __launch_bounds__(kTileThreads) front_scatter_kernel(const uint6
                                                                      const uint32_t* __restrict__ tile_off,
                                                                      uint64_t* __restrict__ tk,
                                                                      uint32_t* __restrict__ tv,
-                                                                     uint32_t* __restrict__ list) {
+                                                                     uint32_t* __restrict__ list,
+                                                                     uint64_t* __restrict__ lk) {
   __shared__ uint32_t cnt[kTileItems][kTileWarps];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t lt = (1u << lane) - 1u;
@@ -288,12 +289,14 @@ __global__ void __launch_bounds__(kTileThreads) front_scatter_kernel(const uint6
     const size_t i = base + (size_t)j * kTileThreads + threadIdx.x;
     if (i < n) {
       const uint32_t p = excl + cnt[j][warp] + __popc(bal[j] & lt);  // touched before i
+      const uint64_t k = keys[i];
       if ((bal[j] >> lane) & 1u) {
         const uint8_t op = ops[i];
-        tk[p] = keys[i];
+        tk[p] = k;
         tv[p] = (uint32_t)i | ((op <= 2 ? (uint32_t)op : 3u) << 30);
       } else {
         list[i - p] = (uint32_t)i;
+        lk[i - p] = k;
       }
     }
   }
@@ -302,7 +305,8 @@ __global__ void __launch_bounds__(kTileThreads) front_scatter_kernel(const uint6
 }  // namespace
 
 // Fills w.f_tk/w.f_tv (touched requests, input order, count counts->n_touch)
-// and w.f_list (plain lookups, input order, count counts->n_lookup).
+// and w.f_list/w.f_lk (plain lookups and their keys, input order, count
+// counts->n_lookup).
 int front_classify(Handle* h, const uint64_t* keys, const uint8_t* ops, size_t n, cudaStream_t s) {
   Work& w = h->w;
   BatchCounts* c = w.counts;
@@ -318,7 +322,7 @@ int front_classify(Handle* h, const uint64_t* keys, const uint8_t* ops, size_t n
   front_flag_kernel<<<(unsigned)n_tiles, kTileThreads, 0, s>>>(keys, ops, n, tab, c, flags, tile);
   front_tile_scan_kernel<<<1, 1024, 0, s>>>(tile, (uint32_t)n_tiles, n, c);
   front_scatter_kernel<<<(unsigned)n_tiles, kTileThreads, 0, s>>>(keys, ops, n, flags, tile, w.f_tk, w.f_tv,
-                                                                  w.f_list);
+                                                                  w.f_list, w.f_lk);
   count_launch(6);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }

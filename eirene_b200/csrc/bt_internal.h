@@ -106,6 +106,7 @@ struct Work {
   uint32_t* f_flags = nullptr;   // [cap] words; the flag pass uses them as one "touched" byte per request
   uint32_t* f_pos = nullptr;     // [cap] per-tile touched counts, then the tiles' exclusive offsets
   uint32_t* f_list = nullptr;    // [cap] requests for the plain lookup, in input order
+  uint64_t* f_lk = nullptr;      // [cap] their keys, in the same order
   uint64_t* f_tk = nullptr;      // [cap] keys of the touched requests, in input order
   uint32_t* f_tv = nullptr;      // [cap] index | op << 30 of the touched requests
   // host staging for the host-buffer entry point
@@ -127,16 +128,25 @@ struct Learned {
   size_t leaf_cap = 0;
   float* mlp = nullptr;          // 97 params
   float* mlp_grad = nullptr;     // 97 floats (device gradient buffer)
-  double* seg = nullptr;         // per segment: base(key as double bits), slope, intercept, err (4 doubles)
+  double* seg = nullptr;         // SegParam[n_segments], 16 B each (bt_learned.cuh)
   uint32_t* seg_scratch = nullptr;
+  uint32_t* seg_of = nullptr;    // [leaf_cap] segment of each leaf (training scratch)
   size_t seg_cap = 0;
   uint64_t kmin = 0, kmax = 0;
   int stage1 = 1;  // 1 = MLP root model, 0 = linear root model
   uint32_t train_steps = 300;
+  uint32_t refit_steps = 0;  // warm-started Adam steps of stage 1 per refit
   uint32_t train_batch = 16384;
   float lr = 0.05f;
-  double last_loss = 0;
-  uint64_t seg_fallback = 0;  // segments whose error exceeds the window
+  bool trained = false;      // stage 1 and its key normalisation hold a full training
+  uint64_t refits = 0;
+  // page-locked host words written by the device after a (re)training:
+  // [0] final training loss (float), [1] segments over the window
+  uint32_t* host_words = nullptr;
+  // requests the learned lookup leaves to the plain descent, and their count
+  uint32_t* miss = nullptr;
+  uint32_t* n_miss = nullptr;
+  size_t miss_cap = 0;
 };
 
 struct Handle {
@@ -148,7 +158,9 @@ struct Handle {
   int descent = 0;     // 0 plain, 1 learned
   uint32_t epoch = 0;  // tree epoch, bumped by every reset / bulk build
   int search_group = 4;  // lanes per request in the lock-free search
-  int learned_group = 8;  // lanes per request in the learned search
+  int learned_group = 4;  // lanes per request in the learned search
+  int learned_mode = 3;   // unsorted learned lookup: 1 one request per lane group, 2 two in lock step,
+                          // 3 software-pipelined (up to five requests per group in successive rounds)
   int sorted_search = 1;  // batch GET phase: 1 = path-reusing search over the sorted keys
   int sorted_leaf_vals = 0;  // sorted search: load the leaf's values with its keys (1) or only the match (0)
   int batch_descent = -1;    // autotuned choice for the batch GET phase: -1 = follow `descent`
@@ -236,8 +248,10 @@ struct BuildScratch {
 };
 int tree_bulk_build_scratch(Handle* h, const uint64_t* keys, const uint64_t* vals, size_t n, cudaStream_t s,
                             const BuildScratch& sc);
+// ckeys (nullable): the keys of the listed requests compacted, ckeys[q] =
+// qkeys[list[q]], read instead of the indirection where the kernel supports it
 cudaError_t launch_search(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev, size_t n,
-                          uint64_t* out_vals, uint8_t* out_st, cudaStream_t s);
+                          uint64_t* out_vals, uint8_t* out_st, cudaStream_t s, const uint64_t* ckeys = nullptr);
 // range scan, one warp per query (bt_range_batch)
 cudaError_t launch_range(Handle* h, const uint64_t* lo, const uint64_t* hi, size_t n, uint32_t max_per,
                          uint64_t* out_keys, uint64_t* out_vals, uint32_t* out_counts, cudaStream_t s);
@@ -331,10 +345,15 @@ int learned_dev(Handle* h, LearnedDev* out);
 int autotune(Handle* h, const uint64_t* keys, size_t n, cudaStream_t s, double* rep);
 
 // ---- learned predictor (bt_learned.cu) ----
-int learned_retrain(Handle* h, cudaStream_t s);
+int learned_retrain(Handle* h, cudaStream_t s, bool refit = false);
 void learned_free(Learned* L);
 cudaError_t launch_learned_search(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev,
                                   size_t n, uint64_t* out_vals, uint8_t* out_st, cudaStream_t s, bool sorted);
+// unsorted learned lookups (paired groups, misses deferred to a plain descent
+// over a miss list); n <= max_batch when list or n_dev is given
+cudaError_t launch_learned_lookup(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev,
+                                  size_t n, uint64_t* out_vals, uint8_t* out_st, cudaStream_t s,
+                                  const uint64_t* ckeys = nullptr);
 int learned_mlp_grad(Handle* h, const float* params, const float* x, const float* y, size_t n, float* grad_out,
                      float* loss_out, cudaStream_t s);
 

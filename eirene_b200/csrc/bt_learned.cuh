@@ -12,22 +12,25 @@ struct LeafEnt {
   uint64_t id;
 };
 
+// Segment line, 16 B: predicted slot = a + slope * (key - base).  A segment
+// with no usable line (no training leaf, or a maximum error above the
+// window) has a = NaN, so its keys skip the probe and go to the fallback.
 struct SegParam {
   uint64_t base;
-  float inv_span;
   float a;
-  float b;
-  uint32_t err;
+  float slope;
 };
 
 constexpr int kHidden = 32;
 constexpr int kParams = 3 * kHidden + 1;  // w1[32] b1[32] w2[32] b2
 constexpr uint32_t kErrNone = 0xFFFFFFFFu;
 
-__device__ __forceinline__ float norm_x(uint64_t key, uint64_t kmin, double inv_range) {
+// the key mapped to [0, 1] over the training key range (float arithmetic:
+// training and lookups evaluate the same expression)
+__device__ __forceinline__ float norm_x(uint64_t key, uint64_t kmin, float inv_range) {
   if (key <= kmin) return 0.f;
-  const double x = (double)(key - kmin) * inv_range;
-  return x >= 1.0 ? 1.f : (float)x;
+  const float x = __ull2float_rn(key - kmin) * inv_range;
+  return x >= 1.f ? 1.f : x;
 }
 
 __device__ __forceinline__ uint32_t seg_of_y(float y, uint32_t n_seg) {
@@ -37,10 +40,38 @@ __device__ __forceinline__ uint32_t seg_of_y(float y, uint32_t n_seg) {
   return (uint32_t)f;
 }
 
-// slot predicted by a segment line, in the exact arithmetic the lookup uses
+// slot predicted by a segment line, in the exact arithmetic the lookup uses;
+// the offset from the segment's base as a signed 64-bit value (a key more
+// than 2^63 away from it wraps: a wrong prediction, which the probe rejects)
 __device__ __forceinline__ float seg_predict(const SegParam& sp, uint64_t key) {
-  const float d = key >= sp.base ? (float)(key - sp.base) : -(float)(sp.base - key);
-  return fmaf(sp.b, d * sp.inv_span, sp.a);
+  const float d = __ll2float_rn((long long)(key - sp.base));
+  return fmaf(sp.slope, d, sp.a);
+}
+
+// one 16-byte load of segment j's line
+__device__ __forceinline__ SegParam load_seg(const SegParam* seg, uint32_t j) {
+  const ulonglong2 w = __ldg(reinterpret_cast<const ulonglong2*>(seg + j));
+  SegParam sp;
+  sp.base = w.x;
+  sp.a = __uint_as_float((uint32_t)w.y);
+  sp.slope = __uint_as_float((uint32_t)(w.y >> 32));
+  return sp;
+}
+
+// stage 1 for one request served by a group of G lanes: lane g evaluates the
+// hidden units g, g + G, ...; the group sums the output with xor-shuffles
+template <int G>
+__device__ __forceinline__ float mlp_group(const float* p, float x, uint32_t g, uint32_t gmask) {
+  float y = 0.f;
+#pragma unroll
+  for (int jj = 0; jj < kHidden / G; jj++) {
+    const int j = g + jj * G;
+    const float h = fmaf(p[j], x, p[kHidden + j]);
+    if (h > 0.f) y = fmaf(p[2 * kHidden + j], h, y);
+  }
+#pragma unroll
+  for (int o = G / 2; o >= 1; o >>= 1) y += __shfl_xor_sync(gmask, y, o, G);
+  return y + p[3 * kHidden];
 }
 
 struct LearnedDev {
@@ -48,7 +79,7 @@ struct LearnedDev {
   const SegParam* seg;
   const float* params;
   uint64_t kmin;
-  double inv_range;
+  float inv_range;
   uint32_t n_leaves;
   uint32_t n_seg;
   uint32_t window;
@@ -60,25 +91,9 @@ struct LearnedDev {
 template <int G>
 __device__ __forceinline__ uint32_t learned_leaf(const LearnedDev& M, const float* p, uint64_t key, uint32_t g,
                                                  uint32_t gmask, uint32_t& dist) {
-  const float x = norm_x(key, M.kmin, M.inv_range);
-  float y = 0.f;
-#pragma unroll
-  for (int jj = 0; jj < kHidden / G; jj++) {
-    const int j = g + jj * G;
-    const float h = fmaf(p[j], x, p[kHidden + j]);
-    if (h > 0.f) y = fmaf(p[2 * kHidden + j], h, y);
-  }
-#pragma unroll
-  for (int o = G / 2; o >= 1; o >>= 1) y += __shfl_xor_sync(gmask, y, o, G);
-  y += p[3 * kHidden];
-  const uint64_t* w = reinterpret_cast<const uint64_t*>(M.seg + seg_of_y(y, M.n_seg));
-  SegParam sp;
-  sp.base = __ldg(w);
-  const uint64_t w1 = __ldg(w + 1), w2 = __ldg(w + 2);
-  sp.inv_span = __uint_as_float((uint32_t)w1);
-  sp.a = __uint_as_float((uint32_t)(w1 >> 32));
-  sp.b = __uint_as_float((uint32_t)w2);
-  if ((uint32_t)(w2 >> 32) == kErrNone) return kNil;  // segment without a model
+  const float y = mlp_group<G>(p, norm_x(key, M.kmin, M.inv_range), g, gmask);
+  const SegParam sp = load_seg(M.seg, seg_of_y(y, M.n_seg));
+  if (sp.a != sp.a) return kNil;  // segment without a usable line
   const float pred = seg_predict(sp, key);
   const int L = (int)M.n_leaves;
   int pc = (pred > 0.f) ? (pred < (float)(L - 1) ? __float2int_rn(pred) : L - 1) : 0;

@@ -69,6 +69,37 @@ __device__ __forceinline__ void load_slots_hint(const uint64_t* p, uint64_t (&x)
   }
 }
 
+// A row of 32 slots read by a group of G lanes in 16-byte chunks interleaved
+// across the lanes: load i of lane g reads chunk i * G + g (slots 2(iG + g)
+// and 2(iG + g) + 1), so one warp-wide load instruction covers one contiguous
+// 16G-byte piece of each group's row instead of G pieces 64 bytes apart:
+// half the 128-byte lines per instruction at G = 4, the unit the L1 data
+// pipe works in.  Slot s lives in lane (s / 2) % G, element 2 * (s / 2 / G) +
+// s % 2; slot 31 (the header) in lane G - 1, element S - 1.
+template <int G>
+__device__ __forceinline__ void load_row_il(const uint64_t* row, uint32_t g, uint64_t (&x)[32 / G], uint64_t pol) {
+  constexpr int S = 32 / G;
+  if constexpr (S == 1) {
+    x[0] = ldg_hint(row + g, pol);
+  } else {
+#pragma unroll
+    for (int i = 0; i < S / 2; i++)
+      asm("ld.global.nc.L2::cache_hint.v2.u64 {%0, %1}, [%2], %3;"
+          : "=l"(x[2 * i]), "=l"(x[2 * i + 1])
+          : "l"(row + 2 * (i * G + g)), "l"(pol));
+  }
+}
+
+// owner lane and element of slot s in an interleaved row
+template <int G>
+__device__ __forceinline__ uint32_t il_lane(uint32_t s) {
+  return G == 32 ? s : (s >> 1) % G;
+}
+template <int G>
+__device__ __forceinline__ uint32_t il_elem(uint32_t s) {
+  return G == 32 ? 0 : 2 * ((s >> 1) / G) + (s & 1);
+}
+
 // S 32-bit separator prefixes of a row (S = 2, 4 or 8)
 template <int S>
 __device__ __forceinline__ void load_pfx(const uint32_t* p, uint32_t (&x)[S], uint64_t pol) {
@@ -97,6 +128,13 @@ __device__ __forceinline__ uint32_t group_sum(uint32_t c, uint32_t gmask) {
 #pragma unroll
   for (int o = G / 2; o >= 1; o >>= 1) c += __shfl_xor_sync(gmask, c, o, G);
   return c;
+}
+
+// The same sum in one warp-level reduction instruction (redux.sync, sm_80+)
+// instead of log2(G) shuffle and add steps
+template <int G>
+__device__ __forceinline__ uint32_t group_add(uint32_t c, uint32_t gmask) {
+  return __reduce_add_sync(gmask, c);
 }
 
 // Rank of `key` in an inner row from the prefixes: slots whose prefix is

@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(256) search2_kernel(DevTree t, const uint64_t*
                                                       const uint32_t* __restrict__ list,
                                                       const uint32_t* __restrict__ n_dev, size_t n_host,
                                                       uint64_t* __restrict__ out_vals, uint8_t* __restrict__ out_st,
-                                                      int use_pfx) {
+                                                      int use_pfx, const uint64_t* __restrict__ ckeys) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t g = lane % G;
   const uint32_t gmask = group_mask<G>(lane);
@@ -146,8 +146,8 @@ __global__ void __launch_bounds__(256) search2_kernel(DevTree t, const uint64_t*
     const bool two = q2 < n;
     const uint32_t ra = list ? __ldg(list + q) : (uint32_t)q;
     const uint32_t rb = two ? (list ? __ldg(list + q2) : (uint32_t)q2) : ra;
-    const uint64_t key_a = __ldg(qkeys + ra);
-    const uint64_t key_b = __ldg(qkeys + rb);
+    const uint64_t key_a = ckeys ? __ldg(ckeys + q) : __ldg(qkeys + ra);
+    const uint64_t key_b = ckeys ? __ldg(ckeys + (two ? q2 : q)) : __ldg(qkeys + rb);
     uint8_t sa = kAbsent, sb = kAbsent;
     uint64_t aa = 0, ab = 0;
     if (root != kNil) {
@@ -754,7 +754,7 @@ cudaError_t ensure_pfx(Handle* h, cudaStream_t s) {
 }
 
 cudaError_t launch_search(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev, size_t n,
-                          uint64_t* out_vals, uint8_t* out_st, cudaStream_t s) {
+                          uint64_t* out_vals, uint8_t* out_st, cudaStream_t s, const uint64_t* ckeys) {
   if (n == 0) return cudaSuccess;
   if (h->search_pairs && (h->search_group == 8 || h->search_group == 4 || h->search_group == 16)) {
     const int threads = 256;
@@ -787,7 +787,7 @@ cudaError_t launch_search(Handle* h, const uint64_t* qkeys, const uint32_t* list
       const cudaError_t pe = ensure_pfx(h, s);
       if (pe != cudaSuccess) return pe;
     }
-#define BT_S2(GG, CC) search2_kernel<GG, false, CC><<<(unsigned)blocks, threads, 0, s>>>(h->tree, qkeys, list, n_dev, n, out_vals, out_st, use_pfx)
+#define BT_S2(GG, CC) search2_kernel<GG, false, CC><<<(unsigned)blocks, threads, 0, s>>>(h->tree, qkeys, list, n_dev, n, out_vals, out_st, use_pfx, list ? ckeys : nullptr)
     if (G == 4) { if (child) BT_S2(4, true); else BT_S2(4, false); }
     else if (G == 16) { if (child) BT_S2(16, true); else BT_S2(16, false); }
     else { if (child) BT_S2(8, true); else BT_S2(8, false); }

@@ -1,7 +1,8 @@
 // Autotuner: times the candidate lookup configurations on the live tree with
 // a caller-supplied sample of keys and keeps the fastest.  Tuned: lanes per
-// request of the unsorted plain and learned searches, the sorted search's
-// leaf-value load, and which descent serves the batch GET phase.  Lookups
+// request of the unsorted plain search, lanes per request and requests per
+// group of the unsorted learned lookup, the sorted search's leaf-value load,
+// and which descent serves the batch GET phase.  Lookups
 // only: the tree is not modified.  Node fanout (32, fixed by the node layout)
 // and the sort tile (4096) are compile-time constants.
 #include <cuda_runtime.h>
@@ -47,23 +48,26 @@ int autotune(Handle* h, const uint64_t* keys, size_t n, cudaStream_t s, double* 
   }
   h->search_group = best_g;
   out[0] = best_g;
-  // unsorted learned search
+  // unsorted learned lookup: lanes per request x requests per group
+  float best_learned = 1e30f;
   if (h->L.valid) {
-    const int lg[3] = {8, 16, 32};
-    float bl = 1e30f;
-    int best_l = h->learned_group;
-    for (int i = 0; i < 3; i++) {
-      h->learned_group = lg[i];
-      const float ms =
-          time_ms(s, [&] { launch_learned_search(h, keys, nullptr, nullptr, n, w.uans, w.uans_st, s, false); });
+    // (lanes, mode): pipelined 4 and 8 lanes, one request per 4 lanes, pairs of 4 lanes
+    const int lg[4][2] = {{4, 3}, {8, 3}, {4, 1}, {4, 2}};
+    int best_i = 0;
+    for (int i = 0; i < 4; i++) {
+      h->learned_group = lg[i][0];
+      h->learned_mode = lg[i][1];
+      const float ms = time_ms(s, [&] { launch_learned_lookup(h, keys, nullptr, nullptr, n, w.uans, w.uans_st, s); });
       out[8 + i] = ms;
-      if (ms < bl) {
-        bl = ms;
-        best_l = lg[i];
+      if (ms < best_learned) {
+        best_learned = ms;
+        best_i = i;
       }
     }
-    h->learned_group = best_l;
-    out[1] = best_l;
+    h->learned_group = lg[best_i][0];
+    h->learned_mode = lg[best_i][1];
+    out[1] = lg[best_i][0];
+    out[15] = lg[best_i][1];
   }
   // sorted sample for the batch GET phase
   uint64_t* sk = nullptr;
@@ -89,7 +93,8 @@ int autotune(Handle* h, const uint64_t* keys, size_t n, cudaStream_t s, double* 
     const float ms =
         time_ms(s, [&] { launch_learned_search(h, sk, nullptr, nullptr, n, w.uans, w.uans_st, s, true); });
     out[14] = ms;
-    if (ms < bs) desc = 1;
+    // the hash front end's lookups are unsorted; the full-sort front end's are sorted
+    if (h->front_end == 1 ? best_learned < best : ms < bs) desc = 1;
   }
   h->batch_descent = desc;
   out[3] = desc;

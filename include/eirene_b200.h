@@ -192,6 +192,13 @@ int bt_stats_reset(bt_handle *h);
  * bt_retrain rebuilds the leaf array and trains the model on the GPU
  * (synchronous); bt_set_descent picks plain or learned search. */
 int bt_retrain(bt_handle *h, void *stream);
+/* Incremental retraining after the tree has changed: rebuilds the leaf array
+ * from the current leaves and re-fits the per-segment lines, keeping the
+ * trained stage-1 model and its key normalisation (plus BT_OPT_REFIT_STEPS
+ * warm-started Adam steps of it, default 0).  Stream ordered when `stream` is
+ * given (its leaf enumeration synchronises the stream), synchronous with NULL.
+ * BT_ERR_NOT_TRAINED before the first bt_retrain. */
+int bt_refit(bt_handle *h, void *stream);
 int bt_set_descent(bt_handle *h, int descent);
 /* stage 1 root model: 1 = 1->32->1 MLP (default), 0 = linear */
 int bt_set_root_model(bt_handle *h, int mlp);
@@ -226,6 +233,11 @@ int bt_set_search_group(bt_handle *h, uint32_t lanes);
                                 * sort.  Every later call on this handle, on any stream, waits for them before it
                                 * touches the tree (bt_sync waits explicitly); 0 the merge runs on the caller's
                                 * stream.  Same answers and tree. */
+#define BT_OPT_REFIT_STEPS 11  /* warm-started Adam steps of the stage-1 model per bt_refit (default 0) */
+#define BT_OPT_LEARNED_MODE 12 /* unsorted learned lookups: 1 one request per lane group, 2 two requests per
+                                * group in lock step, 3 (default) software-pipelined: a group carries up to five
+                                * requests, one in each round of loads (list entry, key, leaf-table probe, leaf
+                                * row, value); bt_autotune picks */
 int bt_set_option(bt_handle *h, int option, int64_t value);
 /* Orders work after every batch issued so far on this handle, its deferred
  * leaf/inner merge included (BT_OPT_ASYNC_WRITE): with a stream, the stream
@@ -237,17 +249,19 @@ int bt_set_option(bt_handle *h, int option, int64_t value);
 int bt_sync(bt_handle *h, void *stream);
 /* Autotuner: times the lookup configurations on this tree with n sample keys
  * (device pointer, n <= max_batch) and keeps the fastest: lanes per request of
- * the plain and the learned search, the sorted search's leaf-value load, and
- * the descent used by the batch GET phase.  Read-only; synchronous.
+ * the plain search, lanes per request and requests per group of the learned
+ * lookup, the sorted search's leaf-value load, and the descent used by the
+ * batch GET phase.  Read-only; synchronous.
  * report (nullable, 16 doubles): [0] plain lanes, [1] learned lanes, [2] leaf
  * values mode, [3] batch descent, [4..7] plain ms for 4/8/16/32 lanes,
- * [8..10] learned ms for 8/16/32, [12..13] sorted plain ms (mode 0/1),
- * [14] sorted learned ms.  No reference counterpart (the reference's launch
+ * [8..11] learned ms for 4 lanes pipelined, 8 lanes pipelined, 4 lanes one
+ * request, 4 lanes two requests, [12..13] sorted plain ms (mode 0/1), [14]
+ * sorted learned ms, [15] learned mode (BT_OPT_LEARNED_MODE).  No reference counterpart (the reference's launch
  * shape is compile-time, src/gpu-stm-tree-v39/bpt-gpustm.h:25-38). */
 int bt_autotune(bt_handle *h, const uint64_t *sample_keys, size_t n, void *stream, double *report);
 /* Learned predictor settings and diagnostics (no reference counterpart: the
  * reference has no learned model).
- * Lanes per request in the learned search kernel: 8, 16 or 32 (default 8). */
+ * Lanes per request in the learned search kernel: 4, 8, 16 or 32 (default 4). */
 int bt_set_learned_group(bt_handle *h, uint32_t lanes);
 /* info[8]: valid, n_leaves, n_segments, segments over the window, window,
  * final training loss, root model (1 MLP, 0 linear), training steps */

@@ -140,7 +140,7 @@ def test_autotune_then_batches_stay_exact(gpu):
     t.set_descent(True)
     rk, rv, ro = O.gen_requests("uniform", 22, keys, 100_000, 95)
     rep = t.autotune(dev(rk))
-    assert rep["plain_lanes"] in (4, 8, 16, 32) and rep["learned_lanes"] in (8, 16, 32)
+    assert rep["plain_lanes"] in (4, 8, 16, 32) and rep["learned_lanes"] in (4, 8) and rep["learned_mode"] in (1, 2, 3)
     assert all(v > 0 for v in rep["plain_ms"].values())
     for desc in (0, 1, -1):
         t.set_option(E.OPT_BATCH_DESCENT, desc)
@@ -184,3 +184,79 @@ def test_learned_in_stm_mode_and_serving(gpu):
     gk, gvv = dump(t)
     ok, ovv = o.dump()
     assert (gk == ok).all() and (gvv == ovv).all()
+
+
+@pytest.mark.parametrize("lanes,mode", [(4, 3), (8, 3), (16, 3), (4, 2), (4, 1), (8, 2), (8, 1), (16, 1), (32, 1)])
+def test_learned_lookup_shapes_bit_exact(gpu, lanes, mode):
+    # every lane-group shape of the unsorted learned lookup against the plain
+    # descent and the oracle: present, absent, reserved and extreme keys, and a
+    # search larger than the miss list (it runs in pieces)
+    keys = O.gen_keys("normal", 41, 120_000)
+    vals = O.value_of(keys)
+    t = E.BTree(max_keys=1 << 19, max_batch=1 << 12)
+    t.bulk_build(dev(keys), dev(vals))
+    o = O.OracleTree()
+    o.bulk_build(keys, vals)
+    qk, _, _ = O.gen_requests("normal", 42, keys, 150_000, 100)
+    qk[:4] = np.array([0, 1, 2**64 - 1, 2**64 - 2], np.uint64)
+    qk[4] = keys.min()
+    qk[5] = keys.max()
+    ov, os_ = o.execute_merged(qk, np.zeros_like(qk), np.ones(qk.size, np.uint8))
+    t.retrain()
+    t.set_descent(True)
+    t.set_learned_group(lanes)
+    t.set_option(E.OPT_LEARNED_MODE, mode)
+    t.reset_stats()
+    lv, ls = lookups(t, qk)
+    assert (ls == os_).all() and (lv == ov).all()
+    st = t.stats()
+    assert st["learned_hits"] + st["learned_fallbacks"] == qk.size - 1  # the reserved key is neither
+    assert st["learned_hits"] > 0.8 * qk.size, st
+
+
+def test_refit_follows_splits_and_deletes(gpu):
+    # after insert batches split leaves and delete batches empty some, a refit
+    # (stage 1 kept) restores the hit rate; answers stay exact throughout
+    keys = O.gen_keys("uniform", 51, 200_000)
+    vals = O.value_of(keys)
+    t = E.BTree(max_keys=1 << 21, max_batch=1 << 17)
+    t.bulk_build(dev(keys), dev(vals))
+    o = O.OracleTree()
+    o.bulk_build(keys, vals)
+    with pytest.raises(E.BTError):
+        t.refit()
+    t.retrain()
+    t.set_descent(True)
+    for b in range(3):
+        rk, rv, ro = O.gen_requests("uniform", 60 + b, keys, 80_000, 50)
+        ov, os_ = o.execute_merged(rk, rv, ro)
+        gv, gs = run_batch(t, rk, rv, ro, E.MODE_SORTED | E.MODE_MERGE_ENGINE)
+        assert (gs == os_).all() and (gv == ov).all()
+    # delete a contiguous run of keys: whole leaves empty and keep routing
+    cur = o.dump()[0]
+    dk = cur[1000:3000]
+    ops = np.full(dk.size, E.OP_DELETE, np.uint8)
+    ov, os_ = o.execute_merged(dk, np.zeros_like(dk), ops)
+    gv, gs = run_batch(t, dk, np.zeros_like(dk), ops, E.MODE_SORTED | E.MODE_MERGE_ENGINE)
+    assert (gs == os_).all() and (gv == ov).all()
+    qk, _, _ = O.gen_requests("uniform", 70, o.dump()[0], 100_000, 100)
+    qk[:2000] = dk  # deleted keys, in emptied leaves
+    ov, os_ = o.execute_merged(qk, np.zeros_like(qk), np.ones(qk.size, np.uint8))
+    t.reset_stats()
+    lv, ls = lookups(t, qk)
+    assert (ls == os_).all() and (lv == ov).all()
+    before = t.stats()["learned_fallbacks"]
+    loss0 = t.learned_info()["loss"]
+    t.refit()
+    info = t.learned_info()
+    assert info["valid"] == 1 and info["loss"] == loss0  # stage 1 untouched
+    t.reset_stats()
+    lv, ls = lookups(t, qk)
+    assert (ls == os_).all() and (lv == ov).all()
+    after = t.stats()["learned_fallbacks"]
+    assert after < before, (before, after)
+    # a refit with warm-started steps trains stage 1 further and stays exact
+    t.set_option(E.OPT_REFIT_STEPS, 20)
+    t.refit()
+    lv, ls = lookups(t, qk)
+    assert (ls == os_).all() and (lv == ov).all()
