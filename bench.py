@@ -234,12 +234,15 @@ def run_reference(args):
 
 
 # ----------------------------------------------------------------------------
-def serve_bench(E, np, tree, tk_host, n_tree, seconds=1.5, seed=5, load=0.5):
+def serve_bench(E, np, tree, tk_host, n_tree, seconds=1.5, seed=5, load=0.5, policy=1, loads=(0.25, 0.5, 0.75)):
     """Serving loop (continuous batching): batch sizes log-uniform over
     2^10..2^22, per-batch search fraction uniform in [0.5, 1], Poisson arrivals.
     After a warm-up pass, phase 1 submits as fast as admission allows
-    (capacity); phase 2 offers 25 % and 50 % of that capacity with Poisson
-    arrivals and reports the batch latency."""
+    (saturated rate); then Poisson arrivals offer each fraction in `loads` of
+    that rate, and each phase reports what was served, the batch latency and
+    its device-side part (first claimed chunk to last finished one).  The
+    sustainable rate is the highest offered one that was served in full
+    (served >= 95 % of offered) with p99 <= 10 x p50."""
     import torch
 
     rng = np.random.default_rng(seed)
@@ -260,7 +263,7 @@ def serve_bench(E, np, tree, tk_host, n_tree, seconds=1.5, seed=5, load=0.5):
     os_t = torch.empty(n_pool, dtype=torch.uint8).pin_memory()
     out_v = ov_t.numpy().view(np.uint64)
     out_s = os_t.numpy()
-    srv = E.Server(tree, arena_bytes=3 << 30, max_batches=512)
+    srv = E.Server(tree, arena_bytes=3 << 30, max_batches=512, policy=policy)
 
     def draw():
         n = int(2 ** rng.uniform(10, 22))
@@ -301,27 +304,102 @@ def serve_bench(E, np, tree, tk_host, n_tree, seconds=1.5, seed=5, load=0.5):
     run(seconds / 2, None)  # warm-up: the first pass inserts the pools' new keys (the tree grows once)
     cap, _ = run(seconds, None)
     mean_batch = (2.0 ** 22 - 2.0 ** 10) / np.log(2.0 ** 12)  # mean of the log-uniform size law
-    out = {"capacity_mops": cap["mops"], "capacity_batches": cap["batches"]}
-    loads = {}
-    for frac in (0.25, load):
+    out = {"capacity_mops": cap["mops"], "capacity_batches": cap["batches"], "policy": policy}
+    res = {}
+    sustainable = 0.0
+    for frac in sorted(set(loads) | {load}):
         rate = frac * cap["mops"] * 1e6 / mean_batch
         lat, n_sub = run(seconds, rate)
-        loads[f"{int(round(frac * 100))}%"] = {
-            "offered_batches_per_s": rate, "mops": lat["mops"], "batches": lat["batches"],
+        offered = rate * mean_batch / 1e6
+        res[f"{int(round(frac * 100))}%"] = {
+            "offered_batches_per_s": rate, "offered_mops": offered, "mops": lat["mops"], "batches": lat["batches"],
             "p50_batch_ms": lat["p50_ms"], "p99_batch_ms": lat["p99_ms"], "max_batch_ms": lat["max_ms"],
+            "p50_service_ms": lat["p50_service_ms"], "p99_service_ms": lat["p99_service_ms"],
             "kernel_launches": lat["kernel_launches"]}
+        if lat["mops"] >= 0.95 * offered and lat["p99_ms"] <= 10 * max(lat["p50_ms"], 1e-9):
+            sustainable = max(sustainable, offered)
     srv.stop()
-    head = loads[f"{int(round(load * 100))}%"]
-    out.update({k: head[k] for k in ("offered_batches_per_s", "mops", "batches", "p50_batch_ms", "p99_batch_ms",
-                                     "max_batch_ms", "kernel_launches")})
-    out["loads"] = loads
+    head = res[f"{int(round(load * 100))}%"]
+    out.update({k: head[k] for k in ("offered_batches_per_s", "offered_mops", "mops", "batches", "p50_batch_ms",
+                                     "p99_batch_ms", "max_batch_ms", "kernel_launches")})
+    out["sustainable_mops"] = sustainable
+    out["loads"] = res
     out["workload"] = ("batch sizes log-uniform 2^10..2^22, search fraction U[0.5,1] per batch, Poisson arrivals "
-                       "at 25% and 50% of the measured capacity (top-level figures: 50%); latency = submit to "
-                       "answers in host memory")
+                       "at fractions of the saturated rate (top-level figures: 50%); latency = submit to answers "
+                       "in host memory; service = device time from the first claimed chunk to the last")
     return out
 
 
+def run_serve_only(args):
+    """Serving only (one GPU): a 2^tree-log2-key tree, then serve_bench for
+    the --descent form(s) with --serve-policy."""
+    import numpy as np
+    import torch
+
+    import eirene_b200 as E
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+    n_tree = 1 << args.tree_log2
+    pool = (1 << args.pool_keys_log2) if args.pool_keys_log2 else 2 * n_tree + (32 << 22)
+    tree = E.BTree(max_keys=pool, max_batch=1 << 22, search_group=args.search_group)
+    tk = torch.empty(n_tree, dtype=torch.int64, device="cuda")
+    tv = torch.empty(n_tree, dtype=torch.int64, device="cuda")
+    E.gen_keys(args.dist, 1, n_tree, tk, tv, stream)
+    tree.bulk_build(tk, tv, stream)
+    del tv
+    out = {"workload": f"serving on a 2^{args.tree_log2}-key {args.dist} tree"}
+    forms = ["plain", "learned"] if args.descent == "both" else [args.descent]
+    for form in forms:
+        if form == "learned":
+            tree.retrain(stream)
+        tree.set_descent(form == "learned")
+        out[form] = serve_bench(E, np, tree, tk, n_tree, seconds=args.serve_seconds, seed=5,
+                                policy=args.serve_policy)
+    print(json.dumps(out), flush=True)
+    tree.close()
+    return 0
+
+
 # ----------------------------------------------------------------------------
+def oracle_check(args, n_b, check_out, tk, draw):
+    """Replays the run's batches through the CPU oracle in the order the GPU
+    ran them (each form: warm-up batches, then the timed ones; the plain form
+    first) and compares each form's first timed batch request by request.
+    The batches are drawn again by the device generator, which is
+    deterministic (`draw(seed)` returns host arrays), and copied to the host
+    one at a time; the tree keys are the device's `tk`."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    threads = os.cpu_count() or 1
+    t0 = time.time()
+    keys = tk.cpu().numpy().view(np.uint64)
+    tree = O.OracleTree(24, 24)
+    tree.bulk_build(keys, O.value_of(keys))
+    engine = O.ENGINE_MERGE if args.engine == "merge" else O.ENGINE_STM
+    out = {}
+    for form in ("plain", "learned"):
+        if form not in check_out:
+            continue
+        seed0, gv, gs = check_out[form]
+        n_run = args.warmup + args.steps
+        for i in range(args.warmup + 1):
+            rk, rv, ro = draw(seed0 + i)
+            ov, os_ = tree.execute_merged(rk, rv, ro, engine, threads)
+            if i == args.warmup:
+                bad = int(((ov != gv) | (os_ != gs)).sum())
+                out[form] = {"requests": n_b, "mismatches": bad}
+        # the rest of the form's timed batches, so the next form starts from the same tree
+        for i in range(args.warmup + 1, n_run):
+            tree.execute_merged(*draw(seed0 + i), engine, threads)
+    out["oracle_s"] = time.time() - t0
+    out["batch"] = "first timed batch of each form, answers (value + status) per request"
+    del tree
+    return out
+
+
 def run_lookups(args):
     """Unsorted point lookups only (one GPU): build a 2^tree-log2 tree, train
     the model when the learned form is asked for, then time `steps` calls of
@@ -410,6 +488,13 @@ def main():
                     help="sorted batches: hash front end (sort only INSERT-coupled requests) or full sort")
     ap.add_argument("--pool-keys-log2", type=int, default=0,
                     help="size the node pool for 2^x keys (default: 2 x tree + 32 x batch)")
+    ap.add_argument("--serve-only", action="store_true",
+                    help="run only the serving benchmark (continuous batching) on a 2^tree-log2-key tree")
+    ap.add_argument("--serve-policy", type=int, default=1, choices=[0, 1],
+                    help="serving: which admitted batch a free warp takes work from (0 oldest, 1 fewest unclaimed)")
+    ap.add_argument("--check", action="store_true",
+                    help="compare the answers of each form's first timed batch with the CPU oracle, which "
+                         "replays every batch of the run before it (outside the timed region; one GPU)")
     ap.add_argument("--lookups-only", action="store_true",
                     help="time only unsorted point lookups (bt_search_batch) of 2^batch-log2 keys, half present, "
                          "with the --descent form(s); a small, bounded workload for kernel profiles")
@@ -423,6 +508,8 @@ def main():
         return run_reference(args)
     if args.lookups_only:
         return run_lookups(args)
+    if args.serve_only:
+        return run_serve_only(args)
 
     import numpy as np
     import torch
@@ -502,11 +589,17 @@ def main():
     ost = torch.empty(n_b, dtype=torch.uint8, device="cuda")
     MODE = E.MODE_SORTED | (E.MODE_MERGE_ENGINE if args.engine == "merge" else 0)
 
-    def step(k, v, o):
+    def step(k, v, o, out=None):
+        a, b = out if out is not None else (ov, ost)
         if sharded is not None:
-            sharded.execute(k, v, o, ov, ost, mode=MODE)
+            sharded.execute(k, v, o, a, b, mode=MODE)
         else:
-            tree.execute(k, v, o, ov, ost, mode=MODE, stream=stream)
+            tree.execute(k, v, o, a, b, mode=MODE, stream=stream)
+
+    # --check: the first timed batch of each form answers into its own
+    # buffers (no extra work in the timed region); the oracle replays the
+    # same seeded batches afterwards and compares
+    check_out = {}
 
     def run_form(learned: bool, seed0: int):
         batches = make_batches(seed0)
@@ -535,8 +628,12 @@ def main():
         sampler.start()
         l0 = E.launch_count()
         ev[0].record(stream)
+        first = None
+        if args.check:
+            first = (torch.empty(n_b, dtype=torch.int64, device="cuda"),
+                     torch.empty(n_b, dtype=torch.uint8, device="cuda"))
         for s in range(args.steps):
-            step(*batches[args.warmup + s])
+            step(*batches[args.warmup + s], out=first if s == 0 else None)
             if learned and args.retrain_every > 0 and (s + 1) % args.retrain_every == 0:
                 # inside the timed region: the model follows the tree
                 if args.retrain_mode == "refit":
@@ -555,6 +652,9 @@ def main():
         phases = tree.profile_read(reset=True)
         tree.profile(False)
         st = tree.stats()
+        if first is not None:
+            check_out["learned" if learned else "plain"] = (seed0, first[0].cpu().numpy().view(np.uint64),
+                                                            first[1].cpu().numpy())
         del batches
         return {"total_ms": total_ms, "step_ms": step_ms, "phases": phases, "counts": counts,
                 "launches": launches, "clocks": clocks, "stats": st, "learned_info": info, "tune": tune}
@@ -641,7 +741,7 @@ def main():
     tree.set_option(E.OPT_BATCH_DESCENT, 1 if head == "learned" else 0)
     if True:
         hb = []
-        e2e_steps = 5
+        e2e_steps = 10
         # page-locked host buffers from the library's own allocator (bt_host_alloc)
         pinned = []
 
@@ -650,28 +750,30 @@ def main():
             pinned.append(b)
             return b.tensor
 
+        n_writes = []
         for i in range(1 + e2e_steps):
             k = torch.empty(n_b, dtype=torch.int64, device="cuda")
             v = torch.empty(n_b, dtype=torch.int64, device="cuda")
             o = torch.empty(n_b, dtype=torch.uint8, device="cuda")
             E.gen_requests(args.dist, 30_000 + 1000 * rank + i, tk, n_b, args.search_pct, k, v, o, stream)
             torch.cuda.synchronize()
+            n_writes.append(int((o != 1).sum().item()))
             hk, hv, ho = host_buf(n_b, torch.int64), host_buf(n_b, torch.int64), host_buf(n_b, torch.uint8)
             hk.copy_(k)
             hv.copy_(v)
             ho.copy_(o)
             hb.append((hk, hv, ho))
-        hov = host_buf(n_b, torch.int64)
-        hos = host_buf(n_b, torch.uint8)
-        L = E.lib()
+        # two answer buffers: batch i + 1 is submitted before batch i is waited for
+        outs = [(host_buf(n_b, torch.int64), host_buf(n_b, torch.uint8)) for _ in range(2)]
         sp = stream.cuda_stream
 
         dk = torch.empty(n_b, dtype=torch.int64, device="cuda")
         dv = torch.empty(n_b, dtype=torch.int64, device="cuda")
         do = torch.empty(n_b, dtype=torch.uint8, device="cuda")
 
-        def host_step(b):
+        def host_submit(b, out):
             k, v, o = b
+            hov, hos = out
             if sharded is not None:
                 # host batch in, host answers out, through the sharded tree
                 dk.copy_(k, non_blocking=True)
@@ -680,29 +782,47 @@ def main():
                 sharded.execute(dk, dv, do, ov, ost, mode=MODE)
                 hov.copy_(ov, non_blocking=True)
                 hos.copy_(ost, non_blocking=True)
-                return
-            rc = L.bt_execute_batch_host(tree._h, k.data_ptr(), v.data_ptr(), o.data_ptr(), hov.data_ptr(),
-                                         hos.data_ptr(), n_b, MODE, sp)
-            if rc != 0:
-                raise E.BTError(rc, "bt_execute_batch_host")
+                return None
+            # bt_execute_batch_host_async: two batches in flight, the next
+            # batch's copy-in and this batch's copy-out beside the kernels
+            return tree.submit_host(k, v, o, hov, hos, mode=MODE, stream=stream)
+
+        def host_wait(t):
+            if t is not None:
+                tree.wait_host(t)
 
         for _ in range(3):
-            host_step(hb[0])
+            host_wait(host_submit(hb[0], outs[0]))
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        w0 = time.perf_counter()
         e0.record(stream)
+        prev = None
         for s in range(e2e_steps):
-            host_step(hb[1 + s])
+            t = host_submit(hb[1 + s], outs[s % 2])
+            host_wait(prev)
+            prev = t
+        host_wait(prev)
         tree.sync(stream)
         e1.record(stream)
         torch.cuda.synchronize()
+        wall_ms = (time.perf_counter() - w0) * 1e3
         barrier()
         e2e_ms = allmax(e0.elapsed_time(e1))
-        del hb, hov, hos
+        del hb, outs
         for b in pinned:
             b.free()
+        # bytes over the bus per step: keys and op codes copied in; the values
+        # of the writes read by the kernels from page-locked memory (two merge
+        # passes read each); values and status bytes copied out
+        writes = sum(n_writes[1:]) / e2e_steps
+        zc = 0 if sharded is not None else int(16 * writes)
         e2e = {"value": world * n_b * e2e_steps / (e2e_ms / 1e3) / 1e6, "unit": "Mops/s",
-               "h2d_bytes_per_step": n_b * 17, "d2h_bytes_per_step": n_b * 9,
+               "h2d_bytes_per_step": (n_b * 17 if sharded is not None else n_b * 9 + zc),
+               "d2h_bytes_per_step": n_b * 9,
+               "values_read_over_bus_per_step": zc,
+               "host_wall_ms_per_step": wall_ms / e2e_steps,
+               "pipelined": sharded is None,
                "steps": e2e_steps, "descent": head}
 
     serving = {}
@@ -712,11 +832,23 @@ def main():
                 continue
             try:
                 tree.set_descent(form == "learned")
-                serving[form] = serve_bench(E, np, tree, tk, n_tree, seconds=args.serve_seconds, seed=5 + rank)
+                serving[form] = serve_bench(E, np, tree, tk, n_tree, seconds=args.serve_seconds, seed=5 + rank,
+                                            policy=args.serve_policy)
             except Exception as ex:  # reported, not fatal
                 serving[form] = {"error": str(ex)}
 
     launches = allsum(R["launches"])
+    check = None
+    if args.check and world == 1 and check_out:
+        def draw(seed):
+            k = torch.empty(n_b, dtype=torch.int64, device="cuda")
+            v = torch.empty(n_b, dtype=torch.int64, device="cuda")
+            o = torch.empty(n_b, dtype=torch.uint8, device="cuda")
+            E.gen_requests(args.dist, seed, tk, n_b, args.search_pct, k, v, o, stream)
+            torch.cuda.synchronize()
+            return k.cpu().numpy().view(np.uint64), v.cpu().numpy().view(np.uint64), o.cpu().numpy()
+
+        check = oracle_check(args, n_b, check_out, tk, draw)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -770,6 +902,8 @@ def main():
         }
         if "learned_error" in forms:
             line["learned_error"] = forms["learned_error"]
+        if check is not None:
+            line["check"] = check
         print(json.dumps(line), flush=True)
     tree.close()
     if dist is not None:

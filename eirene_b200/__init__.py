@@ -81,13 +81,14 @@ class Stats(ctypes.Structure):
 
 class ServeConfig(ctypes.Structure):
     _fields_ = [("arena_bytes", ctypes.c_uint64), ("max_batches", ctypes.c_uint32), ("idle_us", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32 * 6)]
+                ("policy", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 5)]
 
 
 class ServeStats(ctypes.Structure):
     _fields_ = [("batches", ctypes.c_uint64), ("requests", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint64),
                 ("in_flight", ctypes.c_uint64), ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
-                ("max_ms", ctypes.c_double), ("mean_ms", ctypes.c_double), ("mops", ctypes.c_double)]
+                ("max_ms", ctypes.c_double), ("mean_ms", ctypes.c_double), ("mops", ctypes.c_double),
+                ("p50_service_ms", ctypes.c_double), ("p99_service_ms", ctypes.c_double)]
 
 
 # every symbol the C header declares (checked by the CPU tests)
@@ -100,7 +101,7 @@ EXPORTS = [
     "bt_set_learned_group", "bt_learned_info", "bt_mlp_grad", "bt_set_option", "bt_autotune",
     "bt_serve_config_init", "bt_serve_start", "bt_submit", "bt_poll", "bt_wait", "bt_serve_get_stats", "bt_serve_stop",
     "bt_route_batch", "bt_unroute_results", "bt_save", "bt_load", "bt_range_batch", "bt_sync", "bt_save_image", "bt_load_image",
-    "bt_refit",
+    "bt_refit", "bt_execute_batch_host_async", "bt_host_wait",
 ]
 MAX_SHARDS = 256
 OPT_SORTED_SEARCH, OPT_RETRY_LIMIT, OPT_TRAIN_STEPS, OPT_SORTED_LEAF_VALS, OPT_BATCH_DESCENT = 1, 2, 3, 4, 5
@@ -151,6 +152,9 @@ def lib():
             "bt_stats_reset": [_P],
             "bt_retrain": [_P, _P],
             "bt_refit": [_P, _P],
+            "bt_execute_batch_host_async": [_P, _P, _P, _P, _P, _P, _SZ, ctypes.c_int, _P,
+                                            ctypes.POINTER(ctypes.c_uint64)],
+            "bt_host_wait": [_P, ctypes.c_uint64],
             "bt_set_descent": [_P, ctypes.c_int],
             "bt_set_root_model": [_P, ctypes.c_int],
             "bt_set_search_group": [_P, ctypes.c_uint32],
@@ -285,6 +289,23 @@ class BTree:
                                            out_vals.ctypes.data, out_status.ctypes.data, n, mode,
                                            _stream_ptr(stream)), "bt_execute_batch_host")
         return out_vals, out_status
+
+    def submit_host(self, keys, vals, ops, out_vals, out_status, mode=MODE_SORTED, stream=None) -> int:
+        """bt_execute_batch_host_async over host buffers (numpy arrays or CPU
+        tensors, kept alive and unchanged by the caller until wait_host);
+        returns the ticket."""
+        def addr(a):
+            return a.data_ptr() if hasattr(a, "data_ptr") else a.ctypes.data
+
+        n = keys.numel() if hasattr(keys, "numel") else keys.size
+        t = ctypes.c_uint64(0)
+        _check(lib().bt_execute_batch_host_async(self._h, addr(keys), addr(vals), addr(ops), addr(out_vals),
+                                                 addr(out_status), n, mode, _stream_ptr(stream), ctypes.byref(t)),
+               "bt_execute_batch_host_async")
+        return t.value
+
+    def wait_host(self, ticket: int):
+        _check(lib().bt_host_wait(self._h, ticket), "bt_host_wait")
 
     def size(self) -> int:
         v = ctypes.c_uint64(0)
@@ -467,10 +488,11 @@ def gen_requests(dist: str, seed: int, tree_keys, n: int, search_pct: int, keys,
 class Server:
     """Continuous-batching server over one BTree (host numpy buffers)."""
 
-    def __init__(self, tree: "BTree", arena_bytes: int = 1 << 30, max_batches: int = 256, idle_us: int = 2000):
+    def __init__(self, tree: "BTree", arena_bytes: int = 1 << 30, max_batches: int = 256, idle_us: int = 2000,
+                 policy: int = 1):
         cfg = ServeConfig()
         _check(lib().bt_serve_config_init(ctypes.byref(cfg)), "bt_serve_config_init")
-        cfg.arena_bytes, cfg.max_batches, cfg.idle_us = arena_bytes, max_batches, idle_us
+        cfg.arena_bytes, cfg.max_batches, cfg.idle_us, cfg.policy = arena_bytes, max_batches, idle_us, policy
         h = _P()
         _check(lib().bt_serve_start(tree._h, ctypes.byref(cfg), ctypes.byref(h)), "bt_serve_start")
         self._s = h

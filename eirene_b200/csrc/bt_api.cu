@@ -139,6 +139,8 @@ int bt_config_init(bt_config* c) {
   return BT_OK;
 }
 
+static void hostpipe_free(bt::HostPipe& p);
+
 int bt_create(const bt_config* cfg_in, bt_handle** out) {
   if (!out) return BT_ERR_INVALID_ARG;
   *out = nullptr;
@@ -186,10 +188,6 @@ int bt_create(const bt_config* cfg_in, bt_handle** out) {
     ok = ok && cudaStreamCreateWithPriority(&h.hi_stream, cudaStreamNonBlocking, hi_prio) == cudaSuccess &&
          cudaEventCreateWithFlags(&h.fork_ev, cudaEventDisableTiming) == cudaSuccess &&
          cudaEventCreateWithFlags(&h.join_ev, cudaEventDisableTiming) == cudaSuccess;
-    ok = ok && cudaStreamCreateWithFlags(&h.xfer_stream, cudaStreamNonBlocking) == cudaSuccess &&
-         cudaEventCreateWithFlags(&h.xfer_keys_ev, cudaEventDisableTiming) == cudaSuccess &&
-         cudaEventCreateWithFlags(&h.xfer_vals_ev, cudaEventDisableTiming) == cudaSuccess &&
-         cudaEventCreateWithFlags(&h.xfer_ans_ev, cudaEventDisableTiming) == cudaSuccess;
     ok = ok && cudaStreamCreateWithFlags(&h.tree_stream, cudaStreamNonBlocking) == cudaSuccess &&
          cudaEventCreateWithFlags(&h.tree_ev, cudaEventDisableTiming) == cudaSuccess &&
          cudaEventCreateWithFlags(&h.ans_ev, cudaEventDisableTiming) == cudaSuccess;
@@ -225,10 +223,7 @@ int bt_destroy(bt_handle* H) {
   if (h.hi_stream) cudaStreamDestroy(h.hi_stream);
   if (h.fork_ev) cudaEventDestroy(h.fork_ev);
   if (h.join_ev) cudaEventDestroy(h.join_ev);
-  if (h.xfer_stream) cudaStreamDestroy(h.xfer_stream);
-  if (h.xfer_keys_ev) cudaEventDestroy(h.xfer_keys_ev);
-  if (h.xfer_vals_ev) cudaEventDestroy(h.xfer_vals_ev);
-  if (h.xfer_ans_ev) cudaEventDestroy(h.xfer_ans_ev);
+  hostpipe_free(h.hp);
   if (h.tree_stream) cudaStreamDestroy(h.tree_stream);
   if (h.tree_ev) cudaEventDestroy(h.tree_ev);
   if (h.ans_ev) cudaEventDestroy(h.ans_ev);
@@ -264,59 +259,159 @@ int bt_execute_batch(bt_handle* H, const uint64_t* keys, const uint64_t* vals, c
   return map_internal(bt::batch_sorted(&h, keys, vals, ops, out_vals, out_status, n, engine, S(stream)));
 }
 
-// Sorted batches overlap the copies with the kernels: the ops and keys go
-// first on the caller's stream (the front end reads them), the values follow
-// on the transfer stream while the front end and the sort run (the merge
-// passes wait for them), and the answers leave on the transfer stream as soon
-// as they are final, while the write phase changes the tree.
+// ---- host-buffer entry points ----
+// A batch from host buffers runs as: op codes and keys copied in on the copy-in
+// stream; the values copied in after them (the front end and the sort need
+// none; the merge passes wait for them) or, when the caller's value array is
+// page-locked, not copied at all: the merge passes read the values of the
+// batch's writes over the bus; the batch's kernels on the caller's stream;
+// the answers copied out on the copy-out stream as soon as they are final,
+// while the leaf merge still runs.  Two staging sets let the next batch's
+// copy-in and this batch's copy-out run beside the kernels of the other.
+
+static void hostpipe_free(bt::HostPipe& p) {
+  for (bt::Staging& st : p.set) {
+    cudaFree(st.keys);
+    cudaFree(st.vals);
+    cudaFree(st.ops);
+    cudaFree(st.out_vals);
+    cudaFree(st.out_st);
+    for (cudaEvent_t e : {st.in_ev, st.vals_ev, st.ans_ev, st.done_ev})
+      if (e) cudaEventDestroy(e);
+    st = bt::Staging{};
+  }
+  if (p.in_stream) cudaStreamDestroy(p.in_stream);
+  if (p.out_stream) cudaStreamDestroy(p.out_stream);
+  p = bt::HostPipe{};
+}
+
+static int hostpipe_init(bt::Handle& h) {
+  bt::HostPipe& p = h.hp;
+  if (p.cap) return BT_OK;
+  const size_t cap = h.w.cap;
+  bool ok = cudaStreamCreateWithFlags(&p.in_stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&p.out_stream, cudaStreamNonBlocking) == cudaSuccess;
+  for (bt::Staging& st : p.set) {
+    ok = ok && cudaMalloc(&st.keys, cap * 8) == cudaSuccess && cudaMalloc(&st.vals, cap * 8) == cudaSuccess &&
+         cudaMalloc(&st.ops, cap) == cudaSuccess && cudaMalloc(&st.out_vals, cap * 8) == cudaSuccess &&
+         cudaMalloc(&st.out_st, cap) == cudaSuccess;
+    for (cudaEvent_t* e : {&st.in_ev, &st.vals_ev, &st.ans_ev, &st.done_ev})
+      ok = ok && cudaEventCreateWithFlags(e, cudaEventDisableTiming) == cudaSuccess;
+  }
+  if (!ok) {
+    hostpipe_free(p);
+    return BT_ERR_NO_MEMORY;
+  }
+  p.cap = cap;
+  return BT_OK;
+}
+
+// the device-side alias of a page-locked host array, or nullptr for
+// pageable memory (which the kernels cannot read)
+static const uint64_t* mapped_alias(const uint64_t* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return a.type == cudaMemoryTypeHost && a.devicePointer ? static_cast<const uint64_t*>(a.devicePointer) : nullptr;
+}
+
+static int host_submit(bt_handle* H, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops,
+                       uint64_t* out_vals, uint8_t* out_status, size_t n, int mode, cudaStream_t s,
+                       uint64_t* ticket) {
+  bt::Handle& h = H->h;
+  const int base = mode & 0xF;
+  if (base != BT_MODE_SORTED && base != BT_MODE_STM) return BT_ERR_INVALID_ARG;
+  int rc = hostpipe_init(h);
+  if (rc != BT_OK) return rc;
+  bt::HostPipe& p = h.hp;
+  bt::Staging& st = p.set[p.issued % 2];
+  // the set was used two batches ago: its answers must be out before its
+  // buffers are written again
+  if (st.ticket && cudaEventSynchronize(st.done_ev) != cudaSuccess) return BT_ERR_CUDA;
+  const auto H2D = cudaMemcpyHostToDevice;
+  const auto D2H = cudaMemcpyDeviceToHost;
+  const uint64_t* remote = base == BT_MODE_SORTED ? mapped_alias(vals) : nullptr;
+  cudaStream_t in = p.in_stream;
+  if (cudaMemcpyAsync(st.ops, ops, n, H2D, in) != cudaSuccess ||
+      cudaMemcpyAsync(st.keys, keys, n * 8, H2D, in) != cudaSuccess || cudaEventRecord(st.in_ev, in) != cudaSuccess)
+    return BT_ERR_CUDA;
+  if (!remote && (cudaMemcpyAsync(st.vals, vals, n * 8, H2D, in) != cudaSuccess ||
+                  cudaEventRecord(st.vals_ev, in) != cudaSuccess))
+    return BT_ERR_CUDA;
+  if (cudaStreamWaitEvent(s, st.in_ev, 0) != cudaSuccess) return BT_ERR_CUDA;
+  if (base == BT_MODE_SORTED) {
+    h.vals_wait = remote ? nullptr : st.vals_ev;
+    h.vals_remote = remote != nullptr;
+    h.ans_ready = st.ans_ev;
+    const int engine = (mode & BT_MODE_MERGE_ENGINE) ? 1 : 0;
+    rc = map_internal(bt::batch_sorted(&h, st.keys, remote ? remote : st.vals, st.ops, st.out_vals, st.out_st, n,
+                                       engine, s));
+    h.vals_wait = nullptr;
+    h.vals_remote = false;
+    h.ans_ready = nullptr;
+  } else {
+    rc = cudaStreamWaitEvent(s, st.vals_ev, 0) == cudaSuccess
+             ? bt_execute_batch(H, st.keys, st.vals, st.ops, st.out_vals, st.out_st, n, mode, s)
+             : BT_ERR_CUDA;
+    if (rc == BT_OK && cudaEventRecord(st.ans_ev, s) != cudaSuccess) rc = BT_ERR_CUDA;
+  }
+  if (rc != BT_OK) {
+    cudaStreamSynchronize(in);
+    return rc;
+  }
+  cudaStream_t out = p.out_stream;
+  if (cudaStreamWaitEvent(out, st.ans_ev, 0) != cudaSuccess ||
+      cudaMemcpyAsync(out_vals, st.out_vals, n * 8, D2H, out) != cudaSuccess ||
+      cudaMemcpyAsync(out_status, st.out_st, n, D2H, out) != cudaSuccess ||
+      cudaEventRecord(st.done_ev, out) != cudaSuccess)
+    return BT_ERR_CUDA;
+  st.ticket = ++p.issued;
+  if (ticket) *ticket = st.ticket;
+  return BT_OK;
+}
+
+static int host_wait(bt::Handle& h, uint64_t ticket) {
+  const bt::HostPipe& p = h.hp;
+  if (ticket == 0 || ticket > p.issued) return BT_ERR_INVALID_ARG;
+  for (const bt::Staging& st : p.set)
+    if (st.ticket == ticket) return cudaEventSynchronize(st.done_ev) == cudaSuccess ? BT_OK : BT_ERR_CUDA;
+  return BT_OK;  // an older batch: its set has been reused, so it has finished
+}
+
+int bt_execute_batch_host_async(bt_handle* H, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops,
+                                uint64_t* out_vals, uint8_t* out_status, size_t n, int mode, void* stream,
+                                uint64_t* ticket) {
+  if (!H || !ticket) return BT_ERR_INVALID_ARG;
+  *ticket = 0;
+  if (n == 0) return BT_OK;
+  if (!keys || !ops || !out_vals || !out_status || !vals) return BT_ERR_INVALID_ARG;
+  if (n > H->h.w.cap) return BT_ERR_BATCH_TOO_LARGE;
+  DeviceGuard g(H->h.device);
+  return host_submit(H, keys, vals, ops, out_vals, out_status, n, mode, S(stream), ticket);
+}
+
+int bt_host_wait(bt_handle* H, uint64_t ticket) {
+  if (!H) return BT_ERR_INVALID_ARG;
+  if (ticket == 0) return BT_OK;  // an empty batch
+  DeviceGuard g(H->h.device);
+  return host_wait(H->h, ticket);
+}
+
 int bt_execute_batch_host(bt_handle* H, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops,
                           uint64_t* out_vals, uint8_t* out_status, size_t n, int mode, void* stream) {
   if (!H) return BT_ERR_INVALID_ARG;
   if (n == 0) return BT_OK;
   if (!keys || !ops || !out_vals || !out_status || !vals) return BT_ERR_INVALID_ARG;
-  bt::Handle& h = H->h;
-  if (n > h.w.cap) return BT_ERR_BATCH_TOO_LARGE;
-  DeviceGuard g(h.device);
-  cudaStream_t s = S(stream);
-  bt::Work& w = h.w;
-  const auto H2D = cudaMemcpyHostToDevice;
-  const auto D2H = cudaMemcpyDeviceToHost;
-  if ((mode & 0xF) != BT_MODE_SORTED) {
-    if (cudaMemcpyAsync(w.d_in_keys, keys, n * 8, H2D, s) != cudaSuccess ||
-        cudaMemcpyAsync(w.d_in_vals, vals, n * 8, H2D, s) != cudaSuccess ||
-        cudaMemcpyAsync(w.d_in_ops, ops, n, H2D, s) != cudaSuccess)
-      return BT_ERR_CUDA;
-    int rc = bt_execute_batch(H, w.d_in_keys, w.d_in_vals, w.d_in_ops, w.d_out_vals, w.d_out_st, n, mode, stream);
-    if (rc != BT_OK) return rc;
-    if (cudaMemcpyAsync(out_vals, w.d_out_vals, n * 8, D2H, s) != cudaSuccess ||
-        cudaMemcpyAsync(out_status, w.d_out_st, n, D2H, s) != cudaSuccess)
-      return BT_ERR_CUDA;
-    return cudaStreamSynchronize(s) == cudaSuccess ? BT_OK : BT_ERR_CUDA;
-  }
-  cudaStream_t x = h.xfer_stream;
-  if (cudaMemcpyAsync(w.d_in_ops, ops, n, H2D, s) != cudaSuccess ||
-      cudaMemcpyAsync(w.d_in_keys, keys, n * 8, H2D, s) != cudaSuccess ||
-      cudaEventRecord(h.xfer_keys_ev, s) != cudaSuccess || cudaStreamWaitEvent(x, h.xfer_keys_ev, 0) != cudaSuccess ||
-      cudaMemcpyAsync(w.d_in_vals, vals, n * 8, H2D, x) != cudaSuccess ||
-      cudaEventRecord(h.xfer_vals_ev, x) != cudaSuccess)
-    return BT_ERR_CUDA;
-  h.vals_wait = h.xfer_vals_ev;
-  h.ans_ready = h.xfer_ans_ev;
-  const int engine = (mode & BT_MODE_MERGE_ENGINE) ? 1 : 0;
-  int rc = map_internal(bt::batch_sorted(&h, w.d_in_keys, w.d_in_vals, w.d_in_ops, w.d_out_vals, w.d_out_st, n,
-                                         engine, s));
-  h.vals_wait = nullptr;
-  h.ans_ready = nullptr;
-  if (rc != BT_OK) {
-    cudaStreamSynchronize(x);
-    return rc;
-  }
-  if (cudaStreamWaitEvent(x, h.xfer_ans_ev, 0) != cudaSuccess ||
-      cudaMemcpyAsync(out_vals, w.d_out_vals, n * 8, D2H, x) != cudaSuccess ||
-      cudaMemcpyAsync(out_status, w.d_out_st, n, D2H, x) != cudaSuccess)
-    return BT_ERR_CUDA;
-  if (cudaStreamSynchronize(x) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) return BT_ERR_CUDA;
-  return BT_OK;
+  if (n > H->h.w.cap) return BT_ERR_BATCH_TOO_LARGE;
+  DeviceGuard g(H->h.device);
+  uint64_t t = 0;
+  int rc = host_submit(H, keys, vals, ops, out_vals, out_status, n, mode, S(stream), &t);
+  if (rc != BT_OK) return rc;
+  rc = host_wait(H->h, t);
+  if (rc != BT_OK) return rc;
+  return cudaStreamSynchronize(S(stream)) == cudaSuccess ? BT_OK : BT_ERR_CUDA;
 }
 
 int bt_search_batch(bt_handle* H, const uint64_t* keys, uint64_t* out_vals, uint8_t* out_status, size_t n,
@@ -356,9 +451,9 @@ int bt_insert_batch(bt_handle* H, const uint64_t* keys, const uint64_t* vals, ui
   bt::Handle& h = H->h;
   if (n > h.w.cap) return BT_ERR_BATCH_TOO_LARGE;
   DeviceGuard g(h.device);
-  // an all-insert op array in the staging buffer
-  if (cudaMemsetAsync(h.w.d_in_ops, BT_OP_INSERT, n, S(stream)) != cudaSuccess) return BT_ERR_CUDA;
-  return map_internal(bt::batch_sorted(&h, keys, vals, h.w.d_in_ops, out_vals, out_status, n, 0, S(stream)));
+  // an all-insert op array
+  if (cudaMemsetAsync(h.w.ins_ops, BT_OP_INSERT, n, S(stream)) != cudaSuccess) return BT_ERR_CUDA;
+  return map_internal(bt::batch_sorted(&h, keys, vals, h.w.ins_ops, out_vals, out_status, n, 0, S(stream)));
 }
 
 int bt_size(bt_handle* H, uint64_t* n_keys) {

@@ -373,11 +373,7 @@ int work_alloc(Work* w, size_t cap) {
   A((void**)&w->m_ent_b, cap * 16);
   A((void**)&w->m_counts, 64);
   A(&w->m_sync, 8192);
-  A((void**)&w->d_in_keys, cap * 8);
-  A((void**)&w->d_in_vals, cap * 8);
-  A((void**)&w->d_in_ops, cap);
-  A((void**)&w->d_out_vals, cap * 8);
-  A((void**)&w->d_out_st, cap);
+  A((void**)&w->ins_ops, cap);
   {
     size_t tc = 1024;
     while (tc < 2 * cap) tc <<= 1;
@@ -402,8 +398,8 @@ void work_free(Work* w) {
   void* ps[] = {w->k_a,      w->k_b,       w->v_a,       w->v_b,       w->sort_scratch, w->ukeys,   w->uvals,
                 w->uans,     w->uans_st,   w->ins_list,  w->get_list,  w->del_list, w->pend,         w->tiles,   w->counts,
                 w->m_path,   w->m_vpos,   w->m_leaf,    w->m_isnew,   w->m_pos,     w->m_newk,       w->m_newv,  w->m_nq,
-                w->m_nleaf,  w->m_seg,     w->d_leaf,    w->d_slot,    w->m_ent_a,   w->m_ent_b,   w->m_counts,     w->m_sync,      w->d_in_keys,
-                w->d_in_vals, w->d_in_ops, w->d_out_vals, w->d_out_st, w->f_tab, w->f_flags,
+                w->m_nleaf,  w->m_seg,     w->d_leaf,    w->d_slot,    w->m_ent_a,   w->m_ent_b,   w->m_counts,     w->m_sync,
+                w->ins_ops,  w->f_tab, w->f_flags,
                 w->f_pos,    w->f_list,    w->f_lk,      w->f_tk,      w->f_tv};
   for (void* p : ps)
     if (p) cudaFree(p);
@@ -478,7 +474,7 @@ static int batch_hashed(Handle* h, const uint64_t* keys, const uint64_t* vals, c
   // passes when the values are still being copied in (vals_wait): the
   // lookups do not need them
   cudaStream_t s2 = ov ? h->hi_stream : s;
-  const bool pass_side = ov && h->vals_wait != nullptr;
+  const bool pass_side = ov && (h->vals_wait != nullptr || h->vals_remote);
   auto fork = [&]() {
     // a stale prefix table is rebuilt before the fork, so that the locates
     // (side stream) and the lookups (`s`) both come after the rebuild

@@ -28,6 +28,16 @@ constexpr int kLayoutOverlap = 1;  // sort and merge passes on the side stream, 
 constexpr int kLayoutEarly = 2;    // answers written back before the leaf merge
 
 // ---- scan / sort (bt_sort.cu) ----
+// layout of the radix sort's scratch: kSortMaxPasses digit histograms of
+// kSortRadix counters, 64 tile counters, and one look-back table of
+// kSortRadix words per pass and tile of kSortTileKeys keys
+// (sort_scratch_words computes the same; bt_sort.cu checks the constants)
+constexpr size_t kSortTileKeys = 4096;
+constexpr size_t kSortMaxPasses = 8;
+constexpr size_t kSortRadix = 256;
+constexpr size_t sort_scratch_words_for(size_t n) {
+  return kSortMaxPasses * kSortRadix + 64 + kSortMaxPasses * ((n ? n : 1) + kSortTileKeys - 1) / kSortTileKeys * kSortRadix;
+}
 size_t scan_scratch_words(size_t n);
 cudaError_t scan_exclusive_u32(const uint32_t* in, uint32_t* out, size_t n, uint32_t* total_dev, uint32_t* scratch,
                                cudaStream_t s,
@@ -109,12 +119,30 @@ struct Work {
   uint64_t* f_lk = nullptr;      // [cap] their keys, in the same order
   uint64_t* f_tk = nullptr;      // [cap] keys of the touched requests, in input order
   uint32_t* f_tv = nullptr;      // [cap] index | op << 30 of the touched requests
-  // host staging for the host-buffer entry point
-  uint64_t* d_in_keys = nullptr;
-  uint64_t* d_in_vals = nullptr;
-  uint8_t* d_in_ops = nullptr;
-  uint64_t* d_out_vals = nullptr;
-  uint8_t* d_out_st = nullptr;
+  // all-INSERT op codes of bt_insert_batch
+  uint8_t* ins_ops = nullptr;
+};
+
+// ---- host-buffer entry points (bt_api.cu) ----
+// Two staging sets: while one batch's answers are copied out and the next
+// batch's inputs are copied in, the kernels of the batch between them run.
+struct Staging {
+  uint64_t* keys = nullptr;
+  uint64_t* vals = nullptr;
+  uint8_t* ops = nullptr;
+  uint64_t* out_vals = nullptr;
+  uint8_t* out_st = nullptr;
+  cudaEvent_t in_ev = nullptr;    // keys and op codes are on the device
+  cudaEvent_t vals_ev = nullptr;  // values are on the device
+  cudaEvent_t ans_ev = nullptr;   // every answer is final in out_vals / out_st
+  cudaEvent_t done_ev = nullptr;  // the answers are in host memory: the set is free
+  uint64_t ticket = 0;            // the batch that last used the set (0: none)
+};
+struct HostPipe {
+  size_t cap = 0;
+  Staging set[2];
+  cudaStream_t in_stream = nullptr, out_stream = nullptr;
+  uint64_t issued = 0;  // tickets handed out so far
 };
 
 // ---- learned leaf predictor state (bt_learned.cu) ----
@@ -195,14 +223,15 @@ struct Handle {
   int overlap = 1;
   int lookup_reserve = 0;    // block slots the overlapped lookups leave free (set per batch)
   int overlap_reserve = 16;  // ... in the overlapped layout (measured: 16 >= 32 > 64 > none)
-  // host-buffer entry point: the value copy and the answer copies run on
-  // their own stream, overlapped with the batch's kernels
-  cudaStream_t xfer_stream = nullptr;
-  cudaEvent_t xfer_keys_ev = nullptr, xfer_vals_ev = nullptr, xfer_ans_ev = nullptr;
-  // per-batch hooks of the sorted batch, set by the host-buffer entry point:
-  // the stream that first reads `vals` waits for vals_wait; ans_ready is
-  // recorded once every answer is in the output arrays
+  // host-buffer entry points: staging sets and copy streams
+  HostPipe hp;
+  // per-batch hooks of the sorted batch, set by the host-buffer entry points:
+  // the stream that first reads `vals` waits for vals_wait; vals_remote says
+  // that `vals` is page-locked host memory read over the bus (the merge
+  // passes then run beside the lookups as when they wait for a copy);
+  // ans_ready is recorded once every answer is in the output arrays
   cudaEvent_t vals_wait = nullptr;
+  bool vals_remote = false;
   cudaEvent_t ans_ready = nullptr;
   // deferred write phase: a sorted batch (hash front end, merge engine)
   // completes on the caller's stream once its answers are final and leaves
@@ -233,6 +262,8 @@ void prof_set_layout(Handle* h, int layout);
 // make tree.pfx match every inner row (a rebuild when stale), stream ordered
 cudaError_t ensure_pfx(Handle* h, cudaStream_t s);
 cudaError_t tree_reset(Handle* h, cudaStream_t s);
+// header word of node rows [first, last) set to 0 (epoch 0: never written)
+cudaError_t clear_headers(Handle* h, uint32_t first, uint32_t last, cudaStream_t s);
 int tree_bulk_build(Handle* h, const uint64_t* keys, const uint64_t* vals, size_t n, cudaStream_t s);
 // caller-provided scratch for the bulk build (used by the no-allocation entry point)
 struct BuildScratch {
@@ -269,6 +300,7 @@ int tree_dump(Handle* h, uint64_t* out_keys, uint64_t* out_vals, size_t cap, siz
 
 // ---- serving loop (bt_stm.cu device side, bt_serve.cu host side) ----
 constexpr int kServeChunk = 32;
+constexpr int kServeWindow = 32;  // batches a warp considers under the fewest-unclaimed policy
 struct ServeDesc {
   const uint64_t* keys;
   const uint64_t* vals;
@@ -287,7 +319,9 @@ struct ServeDev {
   const uint32_t* stop;
   uint32_t* host_done;              // [cap] mapped host memory: seq of the finished batch
   unsigned long long* host_tend;    // [cap] mapped host memory: device clock at completion
+  unsigned long long* host_tclaim;  // [cap] mapped host memory: device clock of the batch's first claim
   uint32_t cap;
+  uint32_t policy;                  // 0 oldest batch first, 1 fewest unclaimed requests first
   unsigned long long idle_ns;
   unsigned long long* last_busy;  // device clock of the latest claim of work by any warp
 };

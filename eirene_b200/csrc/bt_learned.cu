@@ -569,11 +569,12 @@ __global__ void __launch_bounds__(256) learned_lookup_kernel(DevTree t, LearnedD
 // probe entries of one, ...).  Results and misses as learned_lookup_kernel.
 // kCompact: the listed requests' keys come compacted (ckeys[q]), loaded in
 // the same round as the list entry: four rounds instead of five.
-// 128-thread blocks, at most 72 registers: seven blocks (28 warps) per SM
-// without spills.
-constexpr int kPipeThreads = 128;
+// 256-thread blocks without a register cap: capping registers to fit more
+// warps (64 per thread, or 72 at 128 threads) made the compiler hold fewer
+// rounds of loads in flight, and the kernel got 1.5x slower
+constexpr int kPipeThreads = 256;
 template <int G, bool kCompact>
-__global__ void __launch_bounds__(kPipeThreads, 7) learned_pipe_kernel(DevTree t, LearnedDev M,
+__global__ void __launch_bounds__(kPipeThreads) learned_pipe_kernel(DevTree t, LearnedDev M,
                                                            const uint64_t* __restrict__ qkeys,
                                                            const uint32_t* __restrict__ list,
                                                            const uint32_t* __restrict__ n_dev, size_t n_host,

@@ -65,6 +65,8 @@ struct bt_server {
   uint32_t* d_stop = nullptr;
   uint32_t* h_done = nullptr;  // mapped
   unsigned long long* h_tend = nullptr;
+  unsigned long long* h_tclaim = nullptr;  // mapped: device clock of each batch's first claim
+  uint32_t policy = 1;
   bt::ServeDesc* st_desc = nullptr;  // pinned staging (outlives the async copies)
   uint32_t* st_tail = nullptr;
   unsigned long long* st_claim = nullptr;
@@ -81,6 +83,7 @@ struct bt_server {
   bool k_launched = false;
   unsigned long long launches = 0;
   std::vector<double> lat_ms;
+  std::vector<double> svc_ms;
   unsigned long long completed = 0, requests = 0;
   double t_first = -1, t_last = 0;
   std::mutex mu;
@@ -148,6 +151,9 @@ int pump(bt_server* S) {
       sl.state = 3;
       const double t = now_ms();
       S->lat_ms.push_back(t - sl.t_submit);
+      const volatile unsigned long long* te = S->h_tend + (q % S->cap);
+      const volatile unsigned long long* tc = S->h_tclaim + (q % S->cap);
+      if (*te >= *tc) S->svc_ms.push_back((double)(*te - *tc) * 1e-6);
       S->completed++;
       S->requests += sl.n;
       S->t_last = t;
@@ -175,6 +181,7 @@ int bt_serve_config_init(bt_serve_config* c) {
   c->arena_bytes = 1ull << 30;
   c->max_batches = 256;
   c->idle_us = 2000;
+  c->policy = 1;
   return BT_OK;
 }
 
@@ -184,7 +191,8 @@ int bt_serve_start(bt_handle* H, const bt_serve_config* cfg_in, bt_server** out)
   bt_serve_config cfg;
   if (cfg_in) cfg = *cfg_in;
   else bt_serve_config_init(&cfg);
-  if (cfg.max_batches < 2 || cfg.max_batches > 65536 || cfg.arena_bytes < 4096) return BT_ERR_INVALID_ARG;
+  if (cfg.max_batches < 2 || cfg.max_batches > 65536 || cfg.arena_bytes < 4096 || cfg.policy > 1)
+    return BT_ERR_INVALID_ARG;
   int prev = -1;
   cudaGetDevice(&prev);
   if (cudaSetDevice(H->h.device) != cudaSuccess) return BT_ERR_CUDA;
@@ -194,6 +202,7 @@ int bt_serve_start(bt_handle* H, const bt_serve_config* cfg_in, bt_server** out)
   S->cap = cfg.max_batches;
   S->arena_bytes = cfg.arena_bytes;
   S->slots.resize(S->cap);
+  S->policy = cfg.policy;
   bool ok = cudaStreamCreateWithFlags(&S->s_in, cudaStreamNonBlocking) == cudaSuccess &&
             cudaStreamCreateWithFlags(&S->s_out, cudaStreamNonBlocking) == cudaSuccess &&
             cudaStreamCreateWithFlags(&S->s_k, cudaStreamNonBlocking) == cudaSuccess &&
@@ -204,6 +213,7 @@ int bt_serve_start(bt_handle* H, const bt_serve_config* cfg_in, bt_server** out)
             cudaMalloc(&S->d_done, S->cap * 4) == cudaSuccess &&
             cudaHostAlloc(&S->h_done, S->cap * 4, cudaHostAllocMapped) == cudaSuccess &&
             cudaHostAlloc(&S->h_tend, S->cap * 8, cudaHostAllocMapped) == cudaSuccess &&
+            cudaHostAlloc(&S->h_tclaim, S->cap * 8, cudaHostAllocMapped) == cudaSuccess &&
             cudaMallocHost(&S->st_desc, S->cap * sizeof(bt::ServeDesc)) == cudaSuccess &&
             cudaMallocHost(&S->st_tail, S->cap * 4) == cudaSuccess &&
             cudaMallocHost(&S->st_claim, S->cap * 8) == cudaSuccess &&
@@ -216,6 +226,8 @@ int bt_serve_start(bt_handle* H, const bt_serve_config* cfg_in, bt_server** out)
     S->d_cursor = S->d_tail + 16;
     S->d_stop = S->d_tail + 32;
     std::memset(S->h_done, 0xFF, S->cap * 4);
+    std::memset(S->h_tclaim, 0, S->cap * 8);
+    std::memset(S->h_tend, 0, S->cap * 8);
     std::memset(S->st_zero, 0, 64);
     ok = cudaMemset(S->d_tail, 0, 256) == cudaSuccess &&
          cudaMemset(S->d_claimed, 0xFF, S->cap * sizeof(unsigned long long)) == cudaSuccess &&
@@ -223,8 +235,10 @@ int bt_serve_start(bt_handle* H, const bt_serve_config* cfg_in, bt_server** out)
   }
   uint32_t* h_done_dev = nullptr;
   unsigned long long* h_tend_dev = nullptr;
+  unsigned long long* h_tclaim_dev = nullptr;
   ok = ok && cudaHostGetDevicePointer((void**)&h_done_dev, S->h_done, 0) == cudaSuccess &&
-       cudaHostGetDevicePointer((void**)&h_tend_dev, S->h_tend, 0) == cudaSuccess;
+       cudaHostGetDevicePointer((void**)&h_tend_dev, S->h_tend, 0) == cudaSuccess &&
+       cudaHostGetDevicePointer((void**)&h_tclaim_dev, S->h_tclaim, 0) == cudaSuccess;
   if (ok) {
     bt::ServeDev D;
     D.desc = S->d_desc;
@@ -235,6 +249,8 @@ int bt_serve_start(bt_handle* H, const bt_serve_config* cfg_in, bt_server** out)
     D.stop = S->d_stop;
     D.host_done = h_done_dev;
     D.host_tend = h_tend_dev;
+    D.host_tclaim = h_tclaim_dev;
+    D.policy = S->policy;
     D.cap = S->cap;
     D.idle_ns = (unsigned long long)(cfg.idle_us ? cfg.idle_us : 2000) * 1000ull;
     D.last_busy = reinterpret_cast<unsigned long long*>(S->d_tail + 48);
@@ -366,9 +382,16 @@ int bt_serve_get_stats(bt_server* S, bt_serve_stats* st, int reset) {
     for (double x : v) s += x;
     st->mean_ms = s / v.size();
   }
+  if (!S->svc_ms.empty()) {
+    std::vector<double> v = S->svc_ms;
+    std::sort(v.begin(), v.end());
+    st->p50_service_ms = v[std::min(v.size() - 1, (size_t)(0.50 * (v.size() - 1) + 0.5))];
+    st->p99_service_ms = v[std::min(v.size() - 1, (size_t)(0.99 * (v.size() - 1) + 0.5))];
+  }
   if (S->t_first >= 0 && S->t_last > S->t_first) st->mops = S->requests / ((S->t_last - S->t_first) * 1e3);
   if (reset) {
     S->lat_ms.clear();
+    S->svc_ms.clear();
     S->completed = S->requests = 0;
     S->t_first = -1;
     S->t_last = 0;
@@ -401,6 +424,7 @@ int bt_serve_stop(bt_server* S) {
   cudaFree(S->d_done);
   if (S->h_done) cudaFreeHost(S->h_done);
   if (S->h_tend) cudaFreeHost(S->h_tend);
+  if (S->h_tclaim) cudaFreeHost(S->h_tclaim);
   if (S->st_desc) cudaFreeHost(S->st_desc);
   if (S->st_tail) cudaFreeHost(S->st_tail);
   if (S->st_claim) cudaFreeHost(S->st_claim);

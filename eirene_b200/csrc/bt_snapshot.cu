@@ -29,7 +29,7 @@ namespace {
 constexpr char kMagic[8] = {'E', 'I', 'R', 'B', '2', 'S', 'N', 'P'};
 constexpr uint32_t kVersion = 1;
 constexpr char kImgMagic[8] = {'E', 'I', 'R', 'B', '2', 'I', 'M', 'G'};
-constexpr uint32_t kImgVersion = 1;
+constexpr uint32_t kImgVersion = 2;
 
 uint64_t fnv1a(const void* p, size_t bytes, uint64_t h) {
   const unsigned char* b = static_cast<const unsigned char*>(p);
@@ -136,15 +136,17 @@ int bt_load(bt_handle* h, const char* path) {
 // low fences and the control block), so a loaded tree keeps the saved leaf
 // layout and goes on exactly as the saved one would (the merge engine is
 // deterministic).  The loading handle needs a pool of at least n_nodes
-// nodes; its learned model and separator prefixes are rebuilt on demand.
+// nodes and the saving handle's leaf and inner fills (later splits follow
+// them); its learned model and separator prefixes are rebuilt on demand.
 //
 // File layout (little endian):
 //   0   8 B  magic "EIRB2IMG"
-//   8   4 B  format version (1)
+//   8   4 B  format version (2)
 //   12  4 B  sizeof(Ctrl)
 //   16  8 B  n_nodes
-//   24  8 B  FNV-1a 64 over the control block, key rows, value rows, lows
-//   32       control block
+//   24  8 B  FNV-1a 64 over the fills, control block, key rows, value rows, lows
+//   32  4 B  leaf fill, 4 B inner fill
+//   40       control block
 //   ...      n_nodes key rows (256 B), n_nodes value rows, n_nodes low fences (8 B)
 int bt_save_image(bt_handle* h, const char* path) {
   if (!h || !path) return BT_ERR_INVALID_ARG;
@@ -171,7 +173,9 @@ int bt_save_image(bt_handle* h, const char* path) {
   }
   if (prev >= 0) cudaSetDevice(prev);
   if (rc != BT_OK) return rc;
-  uint64_t sum = fnv1a(&c, sizeof(c), 0xCBF29CE484222325ull);
+  const uint32_t fills[2] = {H.leaf_fill, H.inner_fill};
+  uint64_t sum = fnv1a(fills, sizeof(fills), 0xCBF29CE484222325ull);
+  sum = fnv1a(&c, sizeof(c), sum);
   sum = fnv1a(keys.data(), nn * 256, sum);
   sum = fnv1a(vals.data(), nn * 256, sum);
   sum = fnv1a(low.data(), nn * 8, sum);
@@ -179,7 +183,8 @@ int bt_save_image(bt_handle* h, const char* path) {
   if (!f) return BT_ERR_IO;
   const uint32_t ver[2] = {kImgVersion, (uint32_t)sizeof(c)};
   bool ok = std::fwrite(kImgMagic, 1, 8, f) == 8 && std::fwrite(ver, 4, 2, f) == 2 &&
-            std::fwrite(&nn, 8, 1, f) == 1 && std::fwrite(&sum, 8, 1, f) == 1 && std::fwrite(&c, sizeof(c), 1, f) == 1 &&
+            std::fwrite(&nn, 8, 1, f) == 1 && std::fwrite(&sum, 8, 1, f) == 1 && std::fwrite(fills, 4, 2, f) == 2 &&
+            std::fwrite(&c, sizeof(c), 1, f) == 1 &&
             (nn == 0 || (std::fwrite(keys.data(), 256, nn, f) == nn && std::fwrite(vals.data(), 256, nn, f) == nn &&
                          std::fwrite(low.data(), 8, nn, f) == nn));
   ok = (std::fclose(f) == 0) && ok;
@@ -194,10 +199,11 @@ int bt_load_image(bt_handle* h, const char* path) {
   char magic[8];
   uint32_t ver[2];
   uint64_t nn = 0, sum = 0;
+  uint32_t fills[2] = {0, 0};
   bt::Ctrl c{};
   bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, kImgMagic, 8) == 0 && std::fread(ver, 4, 2, f) == 2 &&
             ver[0] == kImgVersion && ver[1] == sizeof(c) && std::fread(&nn, 8, 1, f) == 1 &&
-            std::fread(&sum, 8, 1, f) == 1 && std::fread(&c, sizeof(c), 1, f) == 1;
+            std::fread(&sum, 8, 1, f) == 1 && std::fread(fills, 4, 2, f) == 2 && std::fread(&c, sizeof(c), 1, f) == 1;
   // the rows must fill the rest of the file exactly
   long here = ok ? std::ftell(f) : -1;
   if (ok && std::fseek(f, 0, SEEK_END) == 0) {
@@ -216,23 +222,36 @@ int bt_load_image(bt_handle* h, const char* path) {
   }
   std::fclose(f);
   if (!ok) return BT_ERR_IO;
-  uint64_t chk = fnv1a(&c, sizeof(c), 0xCBF29CE484222325ull);
+  uint64_t chk = fnv1a(fills, sizeof(fills), 0xCBF29CE484222325ull);
+  chk = fnv1a(&c, sizeof(c), chk);
   chk = fnv1a(keys.data(), nn * 256, chk);
   chk = fnv1a(vals.data(), nn * 256, chk);
   chk = fnv1a(low.data(), nn * 8, chk);
   if (chk != sum || c.n_nodes != nn || (c.root != bt::kNil && c.root >= nn) || c.epoch == 0 || c.epoch > 0x7fffu)
     return BT_ERR_IO;
   if (nn > H.tree.cap) return BT_ERR_NO_MEMORY;  // the pool cannot hold the saved nodes
+  // later splits follow the fills: a handle with other fills would not go on as the saved one
+  if (fills[0] != H.leaf_fill || fills[1] != H.inner_fill) return BT_ERR_INVALID_ARG;
   int prev = -1;
   cudaGetDevice(&prev);
   cudaSetDevice(H.device);
   int rc = BT_OK;
   c.root_lock &= ~1u;  // saved at rest: unlocked
+  // the loading handle starts with its own record: no sticky error bits or
+  // counters of the saving one (the key count is the tree's)
+  c.error = 0;
+  c.commits = c.aborts = c.leaf_splits = c.inner_splits = c.new_roots = c.retry_exhausted = 0;
+  c.learned_hits = c.learned_fallbacks = c.learned_probe_sum = 0;
   if (cudaDeviceSynchronize() != cudaSuccess || bt::tree_sync(&H) != cudaSuccess ||
       (nn && (cudaMemcpy(H.tree.keys, keys.data(), nn * 256, cudaMemcpyHostToDevice) != cudaSuccess ||
               cudaMemcpy(H.tree.vals, vals.data(), nn * 256, cudaMemcpyHostToDevice) != cudaSuccess ||
               cudaMemcpy(H.tree.low, low.data(), nn * 8, cudaMemcpyHostToDevice) != cudaSuccess)) ||
       cudaMemcpy(H.tree.ctrl, &c, sizeof(c), cudaMemcpyHostToDevice) != cudaSuccess)
+    rc = BT_ERR_CUDA;
+  // rows past the loaded ones may hold an earlier tree's nodes; clear their
+  // headers (epoch 0, never used) so that none can pass for a row of this tree
+  if (rc == BT_OK && (bt::clear_headers(&H, (uint32_t)nn, H.tree.cap, H.internal_stream) != cudaSuccess ||
+                      cudaStreamSynchronize(H.internal_stream) != cudaSuccess))
     rc = BT_ERR_CUDA;
   if (rc == BT_OK) {
     H.epoch = c.epoch;  // the rows carry the saved tree's epoch

@@ -371,9 +371,12 @@ static unsigned onesweep_resident() {
 }
 
 // scratch: hist[8][256] | tile counters[8] (+pad) | status[8][tiles][256]
+static_assert(kSortTileKeys == (size_t)kTile && kSortMaxPasses == (size_t)kMaxPasses &&
+                  kSortRadix == (size_t)kRadix,
+              "the scratch layout in bt_internal.h must match the sort");
+
 size_t sort_scratch_words(size_t n) {
-  const size_t t = sort_tiles(n ? n : 1);
-  const size_t w = (size_t)kMaxPasses * kRadix + 64 + (size_t)kMaxPasses * t * kRadix;
+  const size_t w = sort_scratch_words_for(n);
   const size_t sc = scan_scratch_words(n);  // callers reuse this scratch for scans
   return w > sc ? w : sc;
 }

@@ -19,7 +19,9 @@
 // shadow); the device address is fetched once per device with
 // cudaGetSymbolAddress, with that device current, on the first call made on
 // that device.  That first call should therefore come before any stream
-// capture begins on the device.
+// capture begins on the device.  The address is kept for the life of the
+// process: calls after cudaDeviceReset on that device are not supported (the
+// reset unloads the module the address belongs to).
 #include <mutex>
 
 #include <cuda_runtime.h>
@@ -32,9 +34,9 @@ namespace {
 
 constexpr size_t kStaticMaxKeys = BT_STATIC_BUILD_MAX_KEYS;
 constexpr size_t up256(size_t x) { return (x + 255) & ~size_t(255); }
-constexpr size_t kTiles = (kStaticMaxKeys + 4095) / 4096;
-// radix sort scratch: 8 digit histograms, tile counters, 8 look-back tables
-constexpr size_t kSortWords = 8 * 256 + 64 + 8 * kTiles * 256;
+// the radix sort's scratch for kStaticMaxKeys keys (the sort's own layout,
+// bt_internal.h); the scan's scratch, which shares it, is far smaller
+constexpr size_t kSortWords = bt::sort_scratch_words_for(kStaticMaxKeys);
 constexpr size_t kOffKa = 0;
 constexpr size_t kOffKb = kOffKa + up256(kStaticMaxKeys * 8);
 constexpr size_t kOffVa = kOffKb + up256(kStaticMaxKeys * 8);
@@ -93,7 +95,9 @@ extern "C" int bt_bulk_build_static(bt_handle* H, const uint64_t* keys, const ui
   if (rc == BT_OK && bt::tree_join(&H->h, static_cast<cudaStream_t>(stream)) != cudaSuccess) rc = BT_ERR_CUDA;
   if (rc == BT_OK) {
     if (bt::sort_scratch_words(n ? n : 1) > kSortWords) {
-      rc = BT_ERR_STATIC_LIMIT;
+      // n is within the limit, so this means the sort's scratch layout and
+      // the array's sizing disagree: an internal error, not a size error
+      rc = BT_ERR_CUDA;
     } else {
       bt::BuildScratch sc;
       sc.ka = reinterpret_cast<uint64_t*>(base + kOffKa);

@@ -875,7 +875,34 @@ __global__ void __launch_bounds__(256, 4) serve_kernel(DevTree t, ServeDev S, ui
         atomicMax(S.last_busy, now);
       }
     }
-    const uint32_t slot = cur % S.cap;
+    // the batch to claim from: the oldest one with unclaimed requests, or
+    // (policy 1) the one with the fewest unclaimed requests among the
+    // kServeWindow oldest, so that a large batch does not hold the small
+    // ones behind it (shortest remaining work first)
+    uint32_t pick = cur;
+    if (S.policy == 1) {
+      if (lane == 0) {
+        uint32_t best = 0xFFFFFFFFu;
+        const uint32_t lim = tail - cur > (uint32_t)kServeWindow ? cur + (uint32_t)kServeWindow : tail;
+        for (uint32_t q = cur; q != lim; q++) {
+          const uint32_t sq = q % S.cap;
+          const uint64_t ns = ld_relaxed(reinterpret_cast<const uint64_t*>(S.desc + sq) + 5);
+          const unsigned long long cw = ld_relaxed(reinterpret_cast<const uint64_t*>(S.claimed + sq));
+          if ((uint32_t)(ns >> 32) != q || (uint32_t)(cw >> 32) != q) continue;  // not this batch's yet
+          const uint32_t dn = (uint32_t)ns, cl = (uint32_t)cw;
+          if (cl >= dn) {
+            if (q == cur) atomicCAS(S.cursor, cur, cur + 1);  // the oldest is fully claimed
+            continue;
+          }
+          if (dn - cl < best) {
+            best = dn - cl;
+            pick = q;
+          }
+        }
+      }
+      pick = __shfl_sync(kFull, pick, 0);
+    }
+    const uint32_t slot = pick % S.cap;
     // Claim kServeChunk requests with one atomicAdd on the slot's word
     // (batch seq << 32 | requests claimed); every claim succeeds, so thousands
     // of warps do not serialise on a compare-and-swap.  The returned tag names
@@ -886,8 +913,8 @@ __global__ void __launch_bounds__(256, 4) serve_kernel(DevTree t, ServeDev S, ui
     unsigned long long w = 0;
     if (lane == 0) {
       const uint32_t dseq = (uint32_t)(ld_relaxed(reinterpret_cast<const uint64_t*>(S.desc + slot) + 5) >> 32);
-      if (dseq == cur) w = atomicAdd(S.claimed + slot, (unsigned long long)kServeChunk);
-      else w = ~0ull;  // descriptor of `cur` not visible yet, or slot already reused
+      if (dseq == pick) w = atomicAdd(S.claimed + slot, (unsigned long long)kServeChunk);
+      else w = ~0ull;  // descriptor of `pick` not visible yet, or slot already reused
     }
     w = __shfl_sync(kFull, w, 0);
     if (w == ~0ull) {
@@ -925,6 +952,7 @@ __global__ void __launch_bounds__(256, 4) serve_kernel(DevTree t, ServeDev S, ui
       if (lane == 0 && tag == cur) atomicCAS(S.cursor, cur, cur + 1);
       continue;
     }
+    if (c == 0 && lane == 0) S.host_tclaim[slot] = global_ns();  // the batch's first claim
     const uint32_t end = min(d.n, c + (uint32_t)kServeChunk);
     // GETs first, four at a time (8 lanes each); the writes and any GET whose
     // leaf check failed then run one at a time on the whole warp.  Requests

@@ -554,9 +554,34 @@ cudaError_t launch_search_top(Handle* h, const uint64_t* qkeys, const uint32_t* 
   return e;
 }
 
+__global__ void clear_headers_kernel(DevTree t, uint32_t first, uint32_t last) {
+  for (size_t i = (size_t)first + (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < last;
+       i += (size_t)gridDim.x * blockDim.x)
+    t.keys[i * 32 + 31] = 0;
+}
+
+cudaError_t clear_headers(Handle* h, uint32_t first, uint32_t last, cudaStream_t s) {
+  if (first >= last) return cudaSuccess;
+  const size_t n = last - first;
+  const unsigned blocks = (unsigned)min((size_t)h->sm_count * 8, (n + 255) / 256);
+  clear_headers_kernel<<<blocks, 256, 0, s>>>(h->tree, first, last);
+  count_launch();
+  return cudaGetLastError();
+}
+
 cudaError_t tree_reset(Handle* h, cudaStream_t s) {
   h->pfx_valid = false;  // the bulk loader writes inner rows without prefixes
-  h->epoch = (h->epoch % 0x7fffu) + 1;  // 1 .. 0x7fff; 0 marks never-written rows
+  // The epoch has 15 bits (1 .. 0x7fff; 0 marks never-written rows).  When
+  // it comes round to 1 again, rows written by the trees of the last cycle
+  // may still carry that number: clear every row's header first, so that a
+  // reader which reaches a row without a validated path (the optimistic STM
+  // descent, the learned leaf guess) cannot take a row of an older tree for
+  // one of the new tree.
+  if (h->epoch == 0x7fffu) {
+    const cudaError_t e = clear_headers(h, 0, h->tree.cap, s);
+    if (e != cudaSuccess) return e;
+  }
+  h->epoch = (h->epoch % 0x7fffu) + 1;
   reset_kernel<<<1, 1, 0, s>>>(h->tree.ctrl, h->epoch);
   count_launch();
   return cudaGetLastError();

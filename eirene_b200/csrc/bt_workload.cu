@@ -4,7 +4,9 @@
 // Counter-based: element i depends only on (seed, i), so any slice can be
 // regenerated.  The uniform generator is integer-only and bit-identical to the
 // CPU generator in the tests; the Zipf / normal / gamma generators use
-// double-precision math and can differ from a CPU libm in rare last-ulp cases.
+// double-precision math, whose last bit can differ from a CPU libm's: such a
+// key then differs by a few units in its 40th bit (Zipf tree keys are hashed
+// ranks, integer only).
 #include <cuda_runtime.h>
 
 #include "../../include/eirene_b200.h"

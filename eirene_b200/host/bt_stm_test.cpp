@@ -3,7 +3,8 @@
 // -v 39: warp STM batches (v39 meaning); -v 38: sort-merged batches (v38
 // meaning); -v 40: sort-merged with the segmented leaf merge; -v 41: as 40
 // with the learned descent after the first file.  -t prints the answers of
-// the following files; -i runs a file of R/P/G lines; -s is a synonym of -i.
+// the following files; -i runs a file of R/P/G lines; -s is a synonym of -i;
+// -r runs a file of range queries, one "lo [hi]" per line (src/main.cpp:30-34).
 #include <getopt.h>
 
 #include <cstdio>
@@ -53,10 +54,16 @@ int main(int argc, char* argv[]) {
         if (test_flag) tree->test();
         break;
       case 'r':
-        std::fprintf(stderr, "-r (range files): not supported by this driver\n");
-        return 2;
+        if (!tree) {
+          std::fprintf(stderr, "-v must come first\n");
+          return 2;
+        }
+        tree->prepareInput(optarg, eirene_b200::RANGE);
+        tree->gpu_work_range();
+        if (test_flag) tree->test_range();
+        break;
       default:
-        std::fprintf(stderr, "usage: %s -v{38,39,40,41} [-t] -i file [-i file ...]\n", argv[0]);
+        std::fprintf(stderr, "usage: %s -v{38,39,40,41} [-t] -i file [-i file ...] [-r file]\n", argv[0]);
         return 2;
     }
   }

@@ -94,6 +94,11 @@ void BTree::prepareInput(const std::string& fileName, Mission m) {
     if (m == INSERT) {
       vals.push_back(warehouse.size());
       warehouse.push_back(k);
+    } else if (m == RANGE) {
+      // "lo hi"; a line without an end ranges to the largest key
+      // (the reference's INT_MAX, src/input-helper.h:105-116)
+      uint64_t hi = 0;
+      vals.push_back((ss >> hi) ? hi : ~0ull);
     } else {
       vals.push_back(0);
     }
@@ -149,6 +154,69 @@ void BTree::gpu_work() {
   cudaFree(dov);
   cudaFree(dop);
   cudaFree(dos);
+}
+
+// range queries keys[i] .. vals[i] (both included), batch_size at a time
+void BTree::gpu_work_range() {
+  const size_t n = keys.size();
+  const size_t b = batch_size_;
+  range_counts.assign(n, 0);
+  range_keys.assign(n * range_max, 0);
+  range_vals.assign(n * range_max, 0);
+  uint64_t *dlo = nullptr, *dhi = nullptr, *dk = nullptr, *dv = nullptr;
+  uint32_t* dc = nullptr;
+  BT_CUDA(cudaMalloc(&dlo, b * 8));
+  BT_CUDA(cudaMalloc(&dhi, b * 8));
+  BT_CUDA(cudaMalloc(&dc, b * 4));
+  BT_CUDA(cudaMalloc(&dk, b * range_max * 8 + 8));
+  BT_CUDA(cudaMalloc(&dv, b * range_max * 8 + 8));
+  cudaEvent_t e0, e1;
+  BT_CUDA(cudaEventCreate(&e0));
+  BT_CUDA(cudaEventCreate(&e1));
+  float total_ms = 0;
+  std::cout << "bucket size\t" << b << std::endl;
+  std::cout << "total size\t" << n << std::endl;
+  for (size_t s = 0; s < n; s += b) {
+    const size_t m = std::min(b, n - s);
+    BT_CUDA(cudaMemcpy(dlo, keys.data() + s, m * 8, cudaMemcpyHostToDevice));
+    BT_CUDA(cudaMemcpy(dhi, vals.data() + s, m * 8, cudaMemcpyHostToDevice));
+    BT_CUDA(cudaEventRecord(e0));
+    BT_CHECK(bt_range_batch(h_, dlo, dhi, m, range_max, dk, dv, dc, nullptr));
+    BT_CUDA(cudaEventRecord(e1));
+    BT_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    BT_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    total_ms += ms;
+    BT_CUDA(cudaMemcpy(range_counts.data() + s, dc, m * 4, cudaMemcpyDeviceToHost));
+    BT_CUDA(cudaMemcpy(range_keys.data() + s * range_max, dk, m * range_max * 8, cudaMemcpyDeviceToHost));
+    BT_CUDA(cudaMemcpy(range_vals.data() + s * range_max, dv, m * range_max * 8, cudaMemcpyDeviceToHost));
+  }
+  gpu_seconds_ = total_ms / 1e3;
+  std::cout << "total gpu exec time: " << gpu_seconds_ << std::endl;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(dlo);
+  cudaFree(dhi);
+  cudaFree(dc);
+  cudaFree(dk);
+  cudaFree(dv);
+}
+
+// per query: its bounds and full count, then its first range_max pairs (the
+// stored value is a warehouse offset when the tree was loaded from P lines)
+void BTree::test_range() {
+  for (size_t i = 0; i < keys.size(); i++) {
+    const uint32_t c = range_counts[i];
+    std::cout << "range: " << keys[i] << " " << vals[i] << "\t count: " << c << "\n";
+    const uint32_t shown = c < range_max ? c : range_max;
+    for (uint32_t j = 0; j < shown; j++) {
+      const uint64_t v = range_vals[i * range_max + j];
+      std::cout << "  key: " << range_keys[i * range_max + j] << "\t ans: " << v;
+      if (v < warehouse.size()) std::cout << "\t vals: " << warehouse[v];
+      std::cout << "\n";
+    }
+  }
+  std::cout.flush();
 }
 
 // one line per request; a found answer prints the warehouse offset and value

@@ -43,6 +43,11 @@ class BTree : public GPU_BTree {
   void prepareInput(const std::string& fileName, Mission m) override;
   void gpu_work() override;
   void gpu_work_sp() override { gpu_work(); }
+  // range files (-r): the reference declares these members but leaves them
+  // empty in every version (src/tree.h:37-39); here each "lo [hi]" query runs
+  // through bt_range_batch and test_range prints its count and first pairs
+  void gpu_work_range() override;
+  void test_range() override;
   void test() override;
   double last_gpu_seconds() const { return gpu_seconds_; }
   bt_handle* handle() const { return h_; }
@@ -53,6 +58,10 @@ class BTree : public GPU_BTree {
   std::vector<uint64_t> warehouse;  // true values
   std::vector<uint64_t> ans_vals;
   std::vector<uint8_t> ans_status;
+  // range answers: full count per query and its first range_max pairs
+  uint32_t range_max = 16;
+  std::vector<uint32_t> range_counts;
+  std::vector<uint64_t> range_keys, range_vals;
 
  private:
   int mode_;

@@ -131,8 +131,9 @@ int bt_bulk_build(bt_handle *h, const uint64_t *keys, const uint64_t *vals, size
  * BT_ERR_STATIC_LIMIT.  All calls on a device share that array: calls that
  * overlap on the GPU race, so serialise them.  The first call on a device
  * looks up the array's device address; make that first call before any stream
- * capture on the device.  Synchronous.  This entry point has no counterpart in
- * the reference. */
+ * capture on the device.  That address is kept for the process: calls after a
+ * cudaDeviceReset of the device are not supported.  Synchronous.  This entry
+ * point has no counterpart in the reference. */
 #define BT_STATIC_BUILD_MAX_KEYS 65536
 int bt_bulk_build_static(bt_handle *h, const uint64_t *keys, const uint64_t *vals, size_t n, void *stream);
 
@@ -145,10 +146,28 @@ int bt_execute_batch(bt_handle *h, const uint64_t *keys, const uint64_t *vals, c
                      uint64_t *out_vals, uint8_t *out_status, size_t n, int mode, void *stream);
 
 /* Same as bt_execute_batch with HOST buffers: copies in, runs, copies out and
- * synchronises `stream`.  Pinned buffers (bt_host_alloc) give full PCIe speed.
- * Mirrors the reference's transferData -> kernel -> transferAns loop body. */
+ * synchronises `stream`.  Pinned buffers (bt_host_alloc) give full PCIe speed;
+ * with BT_MODE_SORTED and a page-locked `vals`, the value array is not copied:
+ * the kernels read the values of the batch's writes from it over the bus.
+ * Mirrors the reference's transferData -> kernel -> transferAns loop body
+ * (src/gpu-stm-tree-v39/bpt-gpustm.cpp:78-105). */
 int bt_execute_batch_host(bt_handle *h, const uint64_t *keys, const uint64_t *vals, const uint8_t *ops,
                           uint64_t *out_vals, uint8_t *out_status, size_t n, int mode, void *stream);
+/* The same, asynchronous: queues the batch and returns a ticket (> 0; 0 for an
+ * empty batch) that bt_host_wait redeems.  The handle keeps two staging sets,
+ * so a caller that submits batch i + 1 before waiting for batch i gets batch
+ * i + 1's copy-in and batch i's copy-out beside the kernels; a third submit
+ * waits (on the host) until the first batch's answers are out.  Until its
+ * ticket is redeemed, a batch's input buffers must stay unchanged and its
+ * output buffers untouched.  Batches run in submission order, on `stream`.
+ * The reference's loop is synchronous per batch
+ * (src/gpu-stm-tree-v39/bpt-gpustm.cpp:67-132). */
+int bt_execute_batch_host_async(bt_handle *h, const uint64_t *keys, const uint64_t *vals, const uint8_t *ops,
+                                uint64_t *out_vals, uint8_t *out_status, size_t n, int mode, void *stream,
+                                uint64_t *ticket);
+/* Blocks until the batch of `ticket` has its answers in host memory
+ * (its deferred leaf merge may still run; bt_sync orders after that). */
+int bt_host_wait(bt_handle *h, uint64_t ticket);
 
 /* Convenience wrappers: all-GET and all-INSERT batches in BT_MODE_SORTED,
  * the reference's single-mission input (prepareInput(file, mission),
@@ -308,7 +327,10 @@ typedef struct bt_serve_config {
     uint64_t arena_bytes;  /* device memory for batches in flight: 26 B per request (default 1 GiB) */
     uint32_t max_batches;  /* ring slots (default 256) */
     uint32_t idle_us;      /* the persistent kernel exits after this long without work (default 2000) */
-    uint32_t reserved[6];
+    uint32_t policy;       /* which admitted batch a free warp takes work from: 0 the oldest (first in,
+                            * first out), 1 (default) the one with the fewest unclaimed requests among the
+                            * 32 oldest, so that small batches are not held behind a large one */
+    uint32_t reserved[5];
 } bt_serve_config;
 typedef struct bt_serve_stats {
     uint64_t batches;          /* completed since start / last reset */
@@ -317,6 +339,9 @@ typedef struct bt_serve_stats {
     uint64_t in_flight;
     double p50_ms, p99_ms, max_ms, mean_ms;  /* batch latency: submit -> answers in host memory */
     double mops;                             /* completed requests / (last completion - first submit) */
+    double p50_service_ms, p99_service_ms;   /* device time from the batch's first claimed chunk to its
+                                              * last finished one (the rest of the latency is waiting
+                                              * for admission, the copies and the first claim) */
 } bt_serve_stats;
 int bt_serve_config_init(bt_serve_config *cfg);
 int bt_serve_start(bt_handle *h, const bt_serve_config *cfg, bt_server **out);
@@ -373,11 +398,14 @@ int bt_unroute_results(bt_handle *h, const uint32_t *perm, const uint64_t *in_va
 int bt_save(bt_handle *h, const char *path);
 int bt_load(bt_handle *h, const char *path);
 /* Pool image: bt_save_image writes the node pool itself (every allocated
- * node's key and value rows, low fences and the control block);
- * bt_load_image restores it into h, whose pool must hold as many nodes
- * (else BT_ERR_NO_MEMORY), so the loaded tree keeps the saved leaf layout
- * and continues exactly as the saved one would.  Synchronous; BT_ERR_IO for
- * file errors, a bad magic, size or checksum. */
+ * node's key and value rows, low fences, the control block and the handle's
+ * leaf and inner fills); bt_load_image restores it into h, whose pool must
+ * hold as many nodes (else BT_ERR_NO_MEMORY) and whose fills must equal the
+ * saved ones (else BT_ERR_INVALID_ARG: later splits follow the fills), so the
+ * loaded tree keeps the saved leaf layout and continues exactly as the saved
+ * one would.  The loaded handle's counters and sticky error bits start at
+ * zero.  Synchronous; BT_ERR_IO for file errors, a bad magic, size or
+ * checksum. */
 int bt_save_image(bt_handle *h, const char *path);
 int bt_load_image(bt_handle *h, const char *path);
 

@@ -5,11 +5,13 @@
 # src/input-helper.h:10 defines offset_t as a macro that breaks CUB's headers),
 # g++ for every .cpp, link with cudart.  Nothing is copied into this repository.
 set -euo pipefail
+# REF: the reference checkout (the directory holding src/); its default is
+# where this build environment mounts it
 REF=${REF:-/root/reference}
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 OUT="$HERE/_ref"
 NVCC=${NVCC:-/usr/local/cuda/bin/nvcc}
-if [ ! -d "$REF/src" ]; then echo "reference sources not found at $REF" >&2; exit 2; fi
+if [ ! -d "$REF/src" ]; then echo "reference sources not found at $REF (set REF to the reference checkout)" >&2; exit 2; fi
 mkdir -p "$OUT/obj"
 objs=()
 for f in "$REF"/src/gpu-stm-tree-v*/*.cu; do

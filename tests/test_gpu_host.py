@@ -122,3 +122,69 @@ def test_merge_engine_pool_exhaustion(gpu, host):
     k, v = dump(t)
     assert (k == ins_ok).all()
     assert all(int(vv) == vals_now[int(kk)] for kk, vv in zip(k[::97], v[::97]))
+
+
+@pytest.mark.parametrize("pinned", [True, False])
+@pytest.mark.parametrize("mode", [MERGE, E.MODE_SORTED, E.MODE_STM])
+def test_async_host_batches_in_flight(gpu, pinned, mode):
+    # bt_execute_batch_host_async: up to three batches queued before the
+    # first wait (the third submit waits for the first staging set), answers
+    # request by request against the oracle.  With page-locked buffers the
+    # sorted modes read the values of the writes over the bus instead of
+    # copying the value array; pageable buffers are copied.
+    import torch
+
+    keys = O.gen_keys("uniform", 301, 60_000)
+    vals = O.value_of(keys)
+    t = E.BTree(max_keys=1 << 20, max_batch=1 << 16)
+    t.bulk_build(dev(keys), dev(vals))
+    o = O.OracleTree()
+    o.bulk_build(keys, vals)
+    bufs, pinned_bufs, expect = [], [], []
+    for b in range(5):
+        rk, rv, ro = O.gen_requests("uniform", 310 + b, keys, 40_000 + 997 * b, 80)
+        if mode == E.MODE_STM:  # the v39 meaning: compare batches without repeated keys
+            _, at = np.unique(rk, return_index=True)
+            sel = np.sort(at)
+            rk, rv, ro = rk[sel], rv[sel], ro[sel]
+            expect.append(o.execute_serial(rk, rv, ro))
+        else:
+            expect.append(o.execute_merged(rk, rv, ro, engine=O.ENGINE_MERGE))
+        n = rk.size
+        if pinned:
+            hb = [E.HostBuffer(n, d) for d in (torch.int64, torch.int64, torch.uint8, torch.int64, torch.uint8)]
+            pinned_bufs += hb
+            hb[0].tensor.numpy().view(np.uint64)[:] = rk
+            hb[1].tensor.numpy().view(np.uint64)[:] = rv
+            hb[2].tensor.numpy()[:] = ro
+            bufs.append([x.tensor for x in hb])
+        else:
+            bufs.append([torch.from_numpy(rk.view(np.int64).copy()), torch.from_numpy(rv.view(np.int64).copy()),
+                         torch.from_numpy(ro.copy()), torch.zeros(n, dtype=torch.int64),
+                         torch.zeros(n, dtype=torch.uint8)])
+    tickets = []
+    for b in range(3):
+        tickets.append(t.submit_host(*bufs[b], mode=mode))
+    t.wait_host(tickets[1])  # out of order: batches run in submission order anyway
+    t.wait_host(tickets[0])
+    for b in range(3, 5):
+        tickets.append(t.submit_host(*bufs[b], mode=mode))
+    for tk in tickets[2:]:
+        t.wait_host(tk)
+    assert tickets == sorted(tickets) and len(set(tickets)) == 5
+    t.wait_host(tickets[0])  # an old ticket: finished long ago
+    with pytest.raises(E.BTError):
+        t.wait_host(tickets[-1] + 1)  # never issued
+    for b in range(5):
+        ov, os_ = expect[b]
+        gv = bufs[b][3].numpy().view(np.uint64)
+        gs = bufs[b][4].numpy()
+        assert (gs == os_).all(), b
+        assert (gv == ov).all(), b
+    t.sync()
+    gk, gvv = dump(t)
+    ok, ovv = o.dump()
+    assert (gk == ok).all() and (gvv == ovv).all()
+    del bufs
+    for hbuf in pinned_bufs:
+        hbuf.free()

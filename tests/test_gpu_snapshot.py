@@ -79,7 +79,7 @@ def test_pool_image_keeps_layout_and_continues(gpu, tmp_path):
     path = str(tmp_path / "tree.img")
     t.save_image(path)
     n_nodes = t.stats()["n_nodes"]
-    assert os.path.getsize(path) == 32 + 104 + 520 * n_nodes  # header, control block, rows and lows
+    assert os.path.getsize(path) == 40 + 104 + 520 * n_nodes  # header, control block, rows and lows
     t2 = E.BTree(max_keys=1 << 20, max_batch=1 << 17)
     t2.load_image(path)
     ak, av = dump(t)
@@ -106,3 +106,28 @@ def test_pool_image_keeps_layout_and_continues(gpu, tmp_path):
     with pytest.raises(E.BTError) as ei:
         E.BTree(max_keys=0, max_batch=1 << 12).load_image(path)
     assert ei.value.code == -3  # BT_ERR_NO_MEMORY
+    # a handle with other fills would split differently afterwards: refused
+    with pytest.raises(E.BTError) as ei:
+        E.BTree(max_keys=1 << 20, max_batch=1 << 12, leaf_fill=20).load_image(path)
+    assert ei.value.code == -1  # BT_ERR_INVALID_ARG
+
+
+def test_pool_image_starts_with_clean_counters(gpu, tmp_path):
+    # counters of the saving handle do not come back with its tree
+    keys = O.gen_keys("uniform", 71, 20_000)
+    vals = O.value_of(keys)
+    t = E.BTree(max_keys=1 << 18, max_batch=1 << 15)
+    t.bulk_build(dev(keys), dev(vals))
+    rk, rv, ro = O.gen_requests("uniform", 72, keys, 20_000, 0)
+    run_batch(t, rk, rv, ro, E.MODE_SORTED | E.MODE_MERGE_ENGINE)
+    assert t.stats()["leaf_splits"] > 0
+    path = str(tmp_path / "c.img")
+    t.save_image(path)
+    t2 = E.BTree(max_keys=1 << 18, max_batch=1 << 15)
+    t2.bulk_build(dev(keys[:5000]), dev(vals[:5000]))  # rows beyond the image's hold another tree
+    t2.load_image(path)
+    st = t2.stats()
+    assert st["leaf_splits"] == 0 and st["error"] == 0 and st["n_keys"] == t.size()
+    ak, av = dump(t)
+    bk, bv = dump(t2)
+    assert (ak == bk).all() and (av == bv).all()

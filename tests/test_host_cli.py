@@ -29,9 +29,9 @@ def test_unknown_version_rejected(cli):
     assert r.returncode == 2 and "unknown version" in r.stderr
 
 
-def test_range_files_rejected(cli, tmp_path):
+def test_range_file_before_version_rejected(cli, tmp_path):
     r = subprocess.run([cli, "-r", str(tmp_path / "x")], capture_output=True, text=True, timeout=60)
-    assert r.returncode == 2
+    assert r.returncode == 2 and "-v must come first" in r.stderr
 
 
 @pytest.mark.skipif(has_gpu(), reason="checks the no-device path")

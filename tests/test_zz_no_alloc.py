@@ -57,3 +57,49 @@ def test_static_build_rejects_more_than_the_limit(gpu):
     # the handle still works afterwards
     assert static_build(t, kt, kt, 1000) == E.BT_OK
     assert t.size() == 1000
+
+
+def test_static_build_edge_calls(gpu):
+    # an empty build, a build on a non-default stream, and a build straight
+    # after a batch whose deferred leaf/inner merge may still be running:
+    # each gives what the allocating bt_bulk_build gives
+    import torch
+
+    ref = E.BTree(max_keys=1 << 18, max_batch=1 << 15)
+    sta = E.BTree(max_keys=1 << 18, max_batch=1 << 15)
+    keys = O.gen_keys("uniform", 5, 30_000)
+    vals = O.value_of(keys)
+    kt, vt = dev(keys), dev(vals)
+    for t in (ref, sta):
+        t.bulk_build(kt, vt)
+    # empty build
+    ref.bulk_build(kt[:0], vt[:0])
+    assert E.lib().bt_bulk_build_static(sta._h, kt.data_ptr(), vt.data_ptr(), 0, None) == E.BT_OK
+    assert sta.size() == 0 == ref.size()
+    # on a side stream
+    side = torch.cuda.Stream()
+    ref.bulk_build(kt, vt)
+    rc = E.lib().bt_bulk_build_static(sta._h, kt.data_ptr(), vt.data_ptr(), keys.size, side.cuda_stream)
+    side.synchronize()
+    assert rc == E.BT_OK
+    rk, rv = dump(ref)
+    sk, sv = dump(sta)
+    assert (sk == rk).all() and (sv == rv).all()
+    # right after a batch with the deferred write phase on (the default)
+    qk, qv, qo = O.gen_requests("uniform", 6, keys, 20_000, 0)
+    q = (dev(qk), dev(qv), dev(qo))
+    for t in (ref, sta):
+        t.set_option(E.OPT_ASYNC_WRITE, 1)
+        ov = torch.empty(qk.size, dtype=torch.int64, device="cuda")
+        os_ = torch.empty(qk.size, dtype=torch.uint8, device="cuda")
+        t.execute(*q, ov, os_, mode=E.MODE_SORTED | E.MODE_MERGE_ENGINE)
+    k2 = O.gen_keys("uniform", 7, 25_000)
+    v2 = O.value_of(k2)
+    k2t, v2t = dev(k2), dev(v2)
+    ref.bulk_build(k2t, v2t)
+    assert static_build(sta, k2t, v2t, k2.size) == E.BT_OK
+    torch.cuda.synchronize()
+    rk, rv = dump(ref)
+    sk, sv = dump(sta)
+    assert (sk == rk).all() and (sv == rv).all()
+    assert (sta.leaf_sizes() == ref.leaf_sizes()).all()
