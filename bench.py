@@ -163,6 +163,142 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------------------
+# The reference program's own benchmark shape, for a same-box comparison with
+# its GPU build: a tree built from 2^23 - 1 `P` lines, then query files of 95 %
+# `R` / 5 % `P` lines (half the reads hit tree keys), run in batches of
+# 1,310,720 (evalutaion/random_testall_v39.sh:9-28, prof/query23_uniform_95_v39.res,
+# src/gpu-stm-tree-v39/bpt-gpustm.h:25-38).  Keys are 31-bit: the reference
+# is int32 with INT_MAX reserved.  The reference arm runs the reference
+# program on these inputs; this library's arm runs itself on the same ones.
+REF_BATCH = 1_310_720
+
+
+def _mix64(x):
+    import numpy as np
+
+    x = x.astype(np.uint64)
+    with np.errstate(over="ignore"):
+        x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return x ^ (x >> np.uint64(31))
+
+
+def _key31(seed: int, n: int):
+    """n distinct keys in [0, 2^31 - 1), in a seeded random order."""
+    import numpy as np
+
+    out = np.zeros(0, np.uint64)
+    c = 0
+    while out.size < n:
+        i = np.arange(c, c + 2 * n, dtype=np.uint64)
+        with np.errstate(over="ignore"):
+            k = _mix64(i * np.uint64(0x9E3779B97F4A7C15) + np.uint64(seed)) >> np.uint64(33)
+        out = np.unique(np.concatenate([out, k[k < np.uint64(2**31 - 1)]]))
+        c += 2 * n
+    return np.random.default_rng(seed).permutation(out)[:n]
+
+
+def ref31_workload(batches: int = 10, tree: int = (1 << 23) - 1):
+    """(build keys, build values, query keys, query values, query op codes)."""
+    import numpy as np
+
+    pool = _key31(77, tree + batches * REF_BATCH)
+    bk, fresh = pool[:tree], pool[tree:]
+    bv = (bk * np.uint64(7) + np.uint64(3)) & np.uint64(0x7FFFFFFF)
+    rng = np.random.default_rng(5)
+    nq = batches * REF_BATCH
+    is_get = rng.random(nq) < 0.95
+    qk = np.where(rng.random(nq) < 0.5, bk[rng.integers(0, bk.size, nq)], fresh[rng.integers(0, fresh.size, nq)])
+    qk = np.where(is_get, qk, fresh[rng.permutation(nq) % fresh.size])
+    qo = np.where(is_get, 1, 0).astype(np.uint8)
+    qv = (np.arange(nq, dtype=np.uint64) * np.uint64(13) + np.uint64(5)) & np.uint64(0x7FFFFFFF)
+    return bk, bv, qk, qv, qo
+
+
+def reference_gpu(ref_bin: str, batches: int = 10):
+    """The reference program (built from its own sources into oracle/_ref) on
+    the 31-bit workload: its "total gpu exec time" of the build file and of
+    the query file (v39 times its kernel only, v38 all of its phases;
+    src/gpu-stm-tree-v39/bpt-gpustm-kernel.cu:262-282,
+    src/gpu-stm-tree-v38/bpt-gpustm-kernel.cu:289-324)."""
+    import tempfile
+
+    bk, bv, qk, qv, qo = ref31_workload(batches)
+    out = {"tree_keys": int(bk.size), "requests": int(qk.size), "batch": REF_BATCH, "search_frac": 0.95}
+    with tempfile.TemporaryDirectory() as d:
+        b, q = os.path.join(d, "build.txt"), os.path.join(d, "query.txt")
+        with open(b, "w") as f:
+            f.write("".join(f"P {k} {v}\n" for k, v in zip(bk.tolist(), bv.tolist())))
+        with open(q, "w") as f:
+            f.write("".join(f"P {k} {v}\n" if o == 0 else f"R {k}\n"
+                            for k, v, o in zip(qk.tolist(), qv.tolist(), qo.tolist())))
+        for ver in (39, 38):
+            t0 = time.time()
+            try:
+                r = subprocess.run([ref_bin, f"-v{ver}", "-i", b, "-i", q], capture_output=True, text=True,
+                                   timeout=900)
+            except subprocess.TimeoutExpired:
+                out[f"v{ver}"] = {"error": "timeout"}
+                continue
+            times = [float(ln.split(":")[1]) for ln in r.stdout.splitlines() if "total gpu exec time" in ln]
+            if r.returncode != 0 or len(times) < 2:
+                out[f"v{ver}"] = {"error": (r.stdout + r.stderr)[-300:]}
+                continue
+            out[f"v{ver}"] = {"build_s": times[0], "query_s": times[1], "query_mops": qk.size / times[1] / 1e6,
+                              "wall_s": time.time() - t0}
+    return out
+
+
+def same_box_ours(E, torch, batches: int = 10):
+    """This library on the 31-bit workload the reference arm gives the
+    reference program: the tree built by inserting the build file's pairs
+    in batches of 1,310,720 (as the reference builds), then the query file
+    in batches of 1,310,720, device-timed (CUDA events around the batches);
+    the sorted batch meaning (the reference's v38) in both forms, and the
+    STM meaning (v39)."""
+    import numpy as np
+
+    bk, bv, qk, qv, qo = ref31_workload(batches)
+    k = torch.from_numpy(qk.view(np.int64)).cuda()
+    v = torch.from_numpy(qv.view(np.int64)).cuda()
+    o = torch.from_numpy(qo).cuda()
+    bkt = torch.from_numpy(bk.view(np.int64)).cuda()
+    bvt = torch.from_numpy(bv.view(np.int64)).cuda()
+    bot = torch.zeros(bk.size, dtype=torch.uint8, device="cuda")
+    ov = torch.empty(REF_BATCH, dtype=torch.int64, device="cuda")
+    ost = torch.empty(REF_BATCH, dtype=torch.uint8, device="cuda")
+    out = {"tree_keys": int(bk.size), "requests": int(qk.size), "batch": REF_BATCH, "search_frac": 0.95}
+    MERGE = E.MODE_SORTED | E.MODE_MERGE_ENGINE
+    for name, mode, learned in (("sorted_plain", MERGE, False), ("sorted_learned", MERGE, True),
+                                ("stm", E.MODE_STM, False), ("stm_learned", E.MODE_STM, True)):
+        t = E.BTree(max_keys=2 * bk.size + qk.size, max_batch=REF_BATCH)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for i in range(0, bk.size, REF_BATCH):
+            s_ = slice(i, min(bk.size, i + REF_BATCH))
+            t.execute(bkt[s_], bvt[s_], bot[s_], ov[: s_.stop - s_.start], ost[: s_.stop - s_.start], mode=MERGE)
+        t.sync()
+        e1.record()
+        torch.cuda.synchronize()
+        build_ms = e0.elapsed_time(e1)
+        if learned:
+            t.retrain()
+            t.set_descent(True)
+            t.autotune(k[:REF_BATCH])
+        e0.record()
+        for i in range(batches):
+            s_ = slice(i * REF_BATCH, (i + 1) * REF_BATCH)
+            t.execute(k[s_], v[s_], o[s_], ov, ost, mode=mode)
+        t.sync()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out[name] = {"build_s": build_ms / 1e3, "query_s": ms / 1e3, "query_mops": qk.size / (ms / 1e3) / 1e6}
+        t.close()
+    return out
+
+
 def cpu_baseline(args, n_sample: int, threads: int):
     """The oracle (CPU restatement of the reference path; the reference has no
     CPU implementation) on a bounded sample of the same workload."""
@@ -229,12 +365,31 @@ def run_reference(args):
                                    "CPU path; the oracle restatement runs in its place)"},
         "e2e": {"value": val, "unit": "Mops/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    # the reference's GPU build on this box, when it was compiled from the
+    # reference's sources (oracle/_ref): its own benchmark shape, 31-bit keys
+    ref_bin = os.path.join(ROOT, "oracle", "_ref", "stm_test")
+    if not args.no_same_box:
+        try:
+            import torch
+
+            has_gpu = torch.cuda.is_available()
+        except Exception:
+            has_gpu = False
+        if not has_gpu:
+            line["reference_gpu"] = {"unavailable": "no GPU on this machine"}
+        elif os.path.exists(ref_bin):
+            try:
+                line["reference_gpu"] = reference_gpu(ref_bin)
+            except Exception as ex:  # reported, not fatal
+                line["reference_gpu"] = {"error": str(ex)}
+        else:
+            line["reference_gpu"] = {"unavailable": "oracle/_ref/stm_test was not built (no reference sources)"}
     print(json.dumps(line), flush=True)
     return 0
 
 
 # ----------------------------------------------------------------------------
-def serve_bench(E, np, tree, tk_host, n_tree, seconds=1.5, seed=5, load=0.5, policy=1, loads=(0.25, 0.5, 0.75)):
+def serve_bench(E, np, tree, tk_host, n_tree, seconds=1.5, seed=5, load=0.5, policy=0, loads=(0.25, 0.5, 0.75)):
     """Serving loop (continuous batching): batch sizes log-uniform over
     2^10..2^22, per-batch search fraction uniform in [0.5, 1], Poisson arrivals.
     After a warm-up pass, phase 1 submits as fast as admission allows
@@ -277,45 +432,65 @@ def serve_bench(E, np, tree, tk_host, n_tree, seconds=1.5, seed=5, load=0.5, pol
         pending = []
         next_t = t0
         n_sub = 0
+        busy = 0
+        lags = []
+        t_calls = 0.0
         b = draw()
         while True:
             now = time.perf_counter()
             if now - t0 > duration:
                 break
             if rate is None or now >= next_t:
+                c0 = time.perf_counter()
                 tk = srv.submit(*b)
+                t_calls += time.perf_counter() - c0
                 if tk is None:  # admission full: wait for the oldest, then retry the same batch
+                    busy += 1
                     if pending:
                         srv.wait(pending.pop(0))
                     continue
+                if rate is not None:
+                    lags.append(now - next_t)  # how late the host submitted it
                 pending.append(tk)
                 n_sub += 1
                 b = draw()
                 if rate is not None:
                     next_t += rng.exponential(1.0 / rate)
             else:
+                c0 = time.perf_counter()
                 while pending and srv.poll(pending[0]):
                     pending.pop(0)
+                t_calls += time.perf_counter() - c0
                 time.sleep(min(0.0002, max(0.0, next_t - now)))
         for tk in pending:
             srv.wait(tk)
-        return srv.stats(reset=False), n_sub
+        st = srv.stats(reset=False)
+        lags.sort()
+        st["host"] = {"submits": n_sub, "busy_refusals": busy, "call_s": t_calls,
+                      "p50_submit_lag_ms": lags[len(lags) // 2] * 1e3 if lags else 0.0,
+                      "max_submit_lag_ms": lags[-1] * 1e3 if lags else 0.0}
+        return st, n_sub
 
     run(seconds / 2, None)  # warm-up: the first pass inserts the pools' new keys (the tree grows once)
     cap, _ = run(seconds, None)
     mean_batch = (2.0 ** 22 - 2.0 ** 10) / np.log(2.0 ** 12)  # mean of the log-uniform size law
-    out = {"capacity_mops": cap["mops"], "capacity_batches": cap["batches"], "policy": policy}
+    out = {"capacity_mops": cap["mops"], "capacity_device_mops": cap["device_mops"], "capacity_batches": cap["batches"],
+           "policy": policy}
     res = {}
     sustainable = 0.0
     for frac in sorted(set(loads) | {load}):
         rate = frac * cap["mops"] * 1e6 / mean_batch
+        s0 = tree.stats()  # (waits for the persistent kernel's idle exit: counters are flushed then)
         lat, n_sub = run(seconds, rate)
+        s1 = tree.stats()
         offered = rate * mean_batch / 1e6
         res[f"{int(round(frac * 100))}%"] = {
             "offered_batches_per_s": rate, "offered_mops": offered, "mops": lat["mops"], "batches": lat["batches"],
             "p50_batch_ms": lat["p50_ms"], "p99_batch_ms": lat["p99_ms"], "max_batch_ms": lat["max_ms"],
             "p50_service_ms": lat["p50_service_ms"], "p99_service_ms": lat["p99_service_ms"],
-            "kernel_launches": lat["kernel_launches"]}
+            "device_mops": lat["device_mops"], "kernel_launches": lat["kernel_launches"],
+            "stm_commits": s1["commits"] - s0["commits"], "stm_aborts": s1["aborts"] - s0["aborts"],
+            "retry_exhausted": s1["retry_exhausted"] - s0["retry_exhausted"], "host": lat["host"]}
         if lat["mops"] >= 0.95 * offered and lat["p99_ms"] <= 10 * max(lat["p50_ms"], 1e-9):
             sustainable = max(sustainable, offered)
     srv.stop()
@@ -488,9 +663,11 @@ def main():
                     help="sorted batches: hash front end (sort only INSERT-coupled requests) or full sort")
     ap.add_argument("--pool-keys-log2", type=int, default=0,
                     help="size the node pool for 2^x keys (default: 2 x tree + 32 x batch)")
+    ap.add_argument("--no-same-box", action="store_true",
+                    help="skip the comparison with the reference's GPU build on its own 31-bit benchmark shape")
     ap.add_argument("--serve-only", action="store_true",
                     help="run only the serving benchmark (continuous batching) on a 2^tree-log2-key tree")
-    ap.add_argument("--serve-policy", type=int, default=1, choices=[0, 1],
+    ap.add_argument("--serve-policy", type=int, default=0, choices=[0, 1],
                     help="serving: which admitted batch a free warp takes work from (0 oldest, 1 fewest unclaimed)")
     ap.add_argument("--check", action="store_true",
                     help="compare the answers of each form's first timed batch with the CPU oracle, which "
@@ -750,14 +927,12 @@ def main():
             pinned.append(b)
             return b.tensor
 
-        n_writes = []
         for i in range(1 + e2e_steps):
             k = torch.empty(n_b, dtype=torch.int64, device="cuda")
             v = torch.empty(n_b, dtype=torch.int64, device="cuda")
             o = torch.empty(n_b, dtype=torch.uint8, device="cuda")
             E.gen_requests(args.dist, 30_000 + 1000 * rank + i, tk, n_b, args.search_pct, k, v, o, stream)
             torch.cuda.synchronize()
-            n_writes.append(int((o != 1).sum().item()))
             hk, hv, ho = host_buf(n_b, torch.int64), host_buf(n_b, torch.int64), host_buf(n_b, torch.uint8)
             hk.copy_(k)
             hv.copy_(v)
@@ -812,15 +987,11 @@ def main():
         del hb, outs
         for b in pinned:
             b.free()
-        # bytes over the bus per step: keys and op codes copied in; the values
-        # of the writes read by the kernels from page-locked memory (two merge
-        # passes read each); values and status bytes copied out
-        writes = sum(n_writes[1:]) / e2e_steps
-        zc = 0 if sharded is not None else int(16 * writes)
+        # bytes over the bus per step: keys, values and op codes copied in,
+        # values and status bytes copied out
         e2e = {"value": world * n_b * e2e_steps / (e2e_ms / 1e3) / 1e6, "unit": "Mops/s",
-               "h2d_bytes_per_step": (n_b * 17 if sharded is not None else n_b * 9 + zc),
+               "h2d_bytes_per_step": n_b * 17,
                "d2h_bytes_per_step": n_b * 9,
-               "values_read_over_bus_per_step": zc,
                "host_wall_ms_per_step": wall_ms / e2e_steps,
                "pipelined": sharded is None,
                "steps": e2e_steps, "descent": head}
@@ -836,6 +1007,13 @@ def main():
                                             policy=args.serve_policy)
             except Exception as ex:  # reported, not fatal
                 serving[form] = {"error": str(ex)}
+
+    same_box = None
+    if not args.no_same_box and world == 1:
+        try:
+            same_box = same_box_ours(E, torch)
+        except Exception as ex:  # reported, not fatal
+            same_box = {"error": str(ex)}
 
     launches = allsum(R["launches"])
     check = None
@@ -904,6 +1082,8 @@ def main():
             line["learned_error"] = forms["learned_error"]
         if check is not None:
             line["check"] = check
+        if same_box is not None:
+            line["same_box_31bit"] = same_box
         print(json.dumps(line), flush=True)
     tree.close()
     if dist is not None:

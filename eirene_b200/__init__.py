@@ -88,7 +88,8 @@ class ServeStats(ctypes.Structure):
     _fields_ = [("batches", ctypes.c_uint64), ("requests", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint64),
                 ("in_flight", ctypes.c_uint64), ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
                 ("max_ms", ctypes.c_double), ("mean_ms", ctypes.c_double), ("mops", ctypes.c_double),
-                ("p50_service_ms", ctypes.c_double), ("p99_service_ms", ctypes.c_double)]
+                ("p50_service_ms", ctypes.c_double), ("p99_service_ms", ctypes.c_double),
+                ("device_mops", ctypes.c_double)]
 
 
 # every symbol the C header declares (checked by the CPU tests)
@@ -101,12 +102,12 @@ EXPORTS = [
     "bt_set_learned_group", "bt_learned_info", "bt_mlp_grad", "bt_set_option", "bt_autotune",
     "bt_serve_config_init", "bt_serve_start", "bt_submit", "bt_poll", "bt_wait", "bt_serve_get_stats", "bt_serve_stop",
     "bt_route_batch", "bt_unroute_results", "bt_save", "bt_load", "bt_range_batch", "bt_sync", "bt_save_image", "bt_load_image",
-    "bt_refit", "bt_execute_batch_host_async", "bt_host_wait",
+    "bt_refit", "bt_execute_batch_host_async", "bt_host_wait", "bt_serve_batch_times",
 ]
 MAX_SHARDS = 256
 OPT_SORTED_SEARCH, OPT_RETRY_LIMIT, OPT_TRAIN_STEPS, OPT_SORTED_LEAF_VALS, OPT_BATCH_DESCENT = 1, 2, 3, 4, 5
 OPT_FRONT_END, OPT_TOP_CACHE, OPT_SEARCH_PAIRS, OPT_OVERLAP, OPT_ASYNC_WRITE = 6, 7, 8, 9, 10
-OPT_REFIT_STEPS, OPT_LEARNED_MODE = 11, 12
+OPT_REFIT_STEPS, OPT_LEARNED_MODE, OPT_HOST_VALUES_IN_PLACE = 11, 12, 13
 PHASES = ["sort", "merge", "search", "insert", "writeback"]
 
 _lib = None
@@ -155,6 +156,8 @@ def lib():
             "bt_execute_batch_host_async": [_P, _P, _P, _P, _P, _P, _SZ, ctypes.c_int, _P,
                                             ctypes.POINTER(ctypes.c_uint64)],
             "bt_host_wait": [_P, ctypes.c_uint64],
+            "bt_serve_batch_times": [_P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64),
+                                     ctypes.POINTER(ctypes.c_uint64)],
             "bt_set_descent": [_P, ctypes.c_int],
             "bt_set_root_model": [_P, ctypes.c_int],
             "bt_set_search_group": [_P, ctypes.c_uint32],
@@ -489,7 +492,7 @@ class Server:
     """Continuous-batching server over one BTree (host numpy buffers)."""
 
     def __init__(self, tree: "BTree", arena_bytes: int = 1 << 30, max_batches: int = 256, idle_us: int = 2000,
-                 policy: int = 1):
+                 policy: int = 0):
         cfg = ServeConfig()
         _check(lib().bt_serve_config_init(ctypes.byref(cfg)), "bt_serve_config_init")
         cfg.arena_bytes, cfg.max_batches, cfg.idle_us, cfg.policy = arena_bytes, max_batches, idle_us, policy
@@ -520,6 +523,12 @@ class Server:
     def wait(self, ticket, timeout_ms: int = 120000):
         _check(lib().bt_wait(self._s, ticket, timeout_ms), "bt_wait")
         self._keep.pop(ticket, None)
+
+    def batch_times(self, ticket) -> tuple[int, int]:
+        """(first claimed chunk, completion) of a finished batch, device clock in ns."""
+        a, b = ctypes.c_uint64(0), ctypes.c_uint64(0)
+        _check(lib().bt_serve_batch_times(self._s, ticket, ctypes.byref(a), ctypes.byref(b)), "bt_serve_batch_times")
+        return a.value, b.value
 
     def stats(self, reset: bool = False) -> dict:
         st = ServeStats()

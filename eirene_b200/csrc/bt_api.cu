@@ -332,7 +332,10 @@ static int host_submit(bt_handle* H, const uint64_t* keys, const uint64_t* vals,
   if (st.ticket && cudaEventSynchronize(st.done_ev) != cudaSuccess) return BT_ERR_CUDA;
   const auto H2D = cudaMemcpyHostToDevice;
   const auto D2H = cudaMemcpyDeviceToHost;
-  const uint64_t* remote = base == BT_MODE_SORTED ? mapped_alias(vals) : nullptr;
+  // values read in place only when asked for: the merge passes' scattered
+  // 8-byte reads over the bus cost more than copying the whole array, which
+  // the copy-in stream overlaps with the previous batch's kernels
+  const uint64_t* remote = (base == BT_MODE_SORTED && h.host_vals_in_place) ? mapped_alias(vals) : nullptr;
   cudaStream_t in = p.in_stream;
   if (cudaMemcpyAsync(st.ops, ops, n, H2D, in) != cudaSuccess ||
       cudaMemcpyAsync(st.keys, keys, n * 8, H2D, in) != cudaSuccess || cudaEventRecord(st.in_ev, in) != cudaSuccess)
@@ -657,6 +660,9 @@ int bt_set_option(bt_handle* H, int option, int64_t value) {
     case BT_OPT_REFIT_STEPS:
       if (value < 0 || value > 1000000) return BT_ERR_INVALID_ARG;
       H->h.L.refit_steps = (uint32_t)value;
+      return BT_OK;
+    case BT_OPT_HOST_VALUES_IN_PLACE:
+      H->h.host_vals_in_place = value ? 1 : 0;
       return BT_OK;
     case BT_OPT_LEARNED_MODE:
       if (value < 1 || value > 3) return BT_ERR_INVALID_ARG;

@@ -225,6 +225,7 @@ struct Handle {
   int overlap_reserve = 16;  // ... in the overlapped layout (measured: 16 >= 32 > 64 > none)
   // host-buffer entry points: staging sets and copy streams
   HostPipe hp;
+  int host_vals_in_place = 0;  // sorted host batches read page-locked values over the bus instead of copying
   // per-batch hooks of the sorted batch, set by the host-buffer entry points:
   // the stream that first reads `vals` waits for vals_wait; vals_remote says
   // that `vals` is page-locked host memory read over the bus (the merge
@@ -324,6 +325,7 @@ struct ServeDev {
   uint32_t policy;                  // 0 oldest batch first, 1 fewest unclaimed requests first
   unsigned long long idle_ns;
   unsigned long long* last_busy;  // device clock of the latest claim of work by any warp
+  uint32_t* exiting;              // set by the warp that sees the idle timeout: every warp leaves
 };
 cudaError_t launch_serve(Handle* h, const ServeDev& S, cudaStream_t s);
 

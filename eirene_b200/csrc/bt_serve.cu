@@ -66,7 +66,7 @@ struct bt_server {
   uint32_t* h_done = nullptr;  // mapped
   unsigned long long* h_tend = nullptr;
   unsigned long long* h_tclaim = nullptr;  // mapped: device clock of each batch's first claim
-  uint32_t policy = 1;
+  uint32_t policy = 0;
   bt::ServeDesc* st_desc = nullptr;  // pinned staging (outlives the async copies)
   uint32_t* st_tail = nullptr;
   unsigned long long* st_claim = nullptr;
@@ -84,6 +84,7 @@ struct bt_server {
   unsigned long long launches = 0;
   std::vector<double> lat_ms;
   std::vector<double> svc_ms;
+  unsigned long long dev_t0 = ~0ull, dev_t1 = 0;  // earliest first claim, latest completion (device clock)
   unsigned long long completed = 0, requests = 0;
   double t_first = -1, t_last = 0;
   std::mutex mu;
@@ -153,7 +154,12 @@ int pump(bt_server* S) {
       S->lat_ms.push_back(t - sl.t_submit);
       const volatile unsigned long long* te = S->h_tend + (q % S->cap);
       const volatile unsigned long long* tc = S->h_tclaim + (q % S->cap);
-      if (*te >= *tc) S->svc_ms.push_back((double)(*te - *tc) * 1e-6);
+      const unsigned long long tev = *te, tcv = *tc;
+      if (tev >= tcv) {
+        S->svc_ms.push_back((double)(tev - tcv) * 1e-6);
+        S->dev_t0 = std::min(S->dev_t0, tcv);
+        S->dev_t1 = std::max(S->dev_t1, tev);
+      }
       S->completed++;
       S->requests += sl.n;
       S->t_last = t;
@@ -181,7 +187,7 @@ int bt_serve_config_init(bt_serve_config* c) {
   c->arena_bytes = 1ull << 30;
   c->max_batches = 256;
   c->idle_us = 2000;
-  c->policy = 1;
+  c->policy = 0;
   return BT_OK;
 }
 
@@ -254,9 +260,12 @@ int bt_serve_start(bt_handle* H, const bt_serve_config* cfg_in, bt_server** out)
     D.cap = S->cap;
     D.idle_ns = (unsigned long long)(cfg.idle_us ? cfg.idle_us : 2000) * 1000ull;
     D.last_busy = reinterpret_cast<unsigned long long*>(S->d_tail + 48);
-    // the persistent kernel, captured once and relaunched as a graph
+    D.exiting = S->d_tail + 56;
+    // the persistent kernel, captured once and relaunched as a graph; the
+    // graph first clears the exit flag the previous launch left set
     ok = cudaStreamBeginCapture(S->s_k, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
     if (ok) {
+      cudaMemsetAsync(D.exiting, 0, 4, S->s_k);
       bt::launch_serve(&H->h, D, S->s_k);
       ok = cudaStreamEndCapture(S->s_k, &S->graph) == cudaSuccess;
     }
@@ -363,6 +372,18 @@ int bt_wait(bt_server* S, uint64_t ticket, uint32_t timeout_ms) {
   }
 }
 
+int bt_serve_batch_times(bt_server* S, uint64_t ticket, uint64_t* first_claim_ns, uint64_t* done_ns) {
+  if (!S || !first_claim_ns || !done_ns) return BT_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(S->mu);
+  // finished, and its slot not reused since
+  if (ticket >= S->next_seq || ticket + S->cap < S->next_seq) return BT_ERR_INVALID_ARG;
+  const uint32_t q = (uint32_t)ticket;
+  if (q >= S->retire_seq && S->slots[q % S->cap].state != 3) return BT_ERR_INVALID_ARG;
+  *first_claim_ns = *reinterpret_cast<volatile unsigned long long*>(S->h_tclaim + q % S->cap);
+  *done_ns = *reinterpret_cast<volatile unsigned long long*>(S->h_tend + q % S->cap);
+  return BT_OK;
+}
+
 int bt_serve_get_stats(bt_server* S, bt_serve_stats* st, int reset) {
   if (!S || !st) return BT_ERR_INVALID_ARG;
   std::lock_guard<std::mutex> lk(S->mu);
@@ -389,9 +410,12 @@ int bt_serve_get_stats(bt_server* S, bt_serve_stats* st, int reset) {
     st->p99_service_ms = v[std::min(v.size() - 1, (size_t)(0.99 * (v.size() - 1) + 0.5))];
   }
   if (S->t_first >= 0 && S->t_last > S->t_first) st->mops = S->requests / ((S->t_last - S->t_first) * 1e3);
+  if (S->dev_t1 > S->dev_t0) st->device_mops = (double)S->requests / ((double)(S->dev_t1 - S->dev_t0) * 1e-3);
   if (reset) {
     S->lat_ms.clear();
     S->svc_ms.clear();
+    S->dev_t0 = ~0ull;
+    S->dev_t1 = 0;
     S->completed = S->requests = 0;
     S->t_first = -1;
     S->t_last = 0;

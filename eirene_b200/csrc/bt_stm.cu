@@ -367,12 +367,13 @@ __device__ int tx_attempt(const DevTree& t, const uint64_t key, const uint64_t v
 // low <= key < right fence.  A complete leaf image whose fence range holds the
 // key is that key's leaf whatever path led to it, so the answer and an
 // in-leaf update are exact.  Splits and failed checks go to tx_attempt.
-enum : int { FAST_DONE = 0, FAST_SLOW = 1, FAST_RETRY = 2 };
+// FAST_WRONG: the leaf's fences do not cover the key (unlocked unchanged)
+enum : int { FAST_DONE = 0, FAST_SLOW = 1, FAST_RETRY = 2, FAST_WRONG = 3 };
 
 // Insert into a candidate leaf by locking it first: CAS its header, then read
 // the row under the lock (no concurrent writer can change it), check epoch and
 // fences, and apply the update or the shift-insert.  A wrong leaf is unlocked
-// unchanged (retry); a full leaf is unlocked unchanged and goes to the
+// unchanged (FAST_WRONG); a full leaf is unlocked unchanged and goes to the
 // validated split path.
 __device__ int fast_insert_locked(const DevTree& t, const uint32_t epoch, const uint32_t node, const uint64_t key,
                                   const uint64_t val, uint64_t& ans, uint8_t& st) {
@@ -397,7 +398,7 @@ __device__ int fast_insert_locked(const DevTree& t, const uint32_t epoch, const 
   if (!(lo <= key && key < fence_key)) {
     if (lane == 0) st_release(hp, h);
     __syncwarp();
-    return FAST_RETRY;
+    return FAST_WRONG;
   }
   if (lane == 31) k = kKeyMax;
   const uint32_t mm = __ballot_sync(kFull, lane < size && k == key);
@@ -440,7 +441,7 @@ __device__ int fast_insert_locked(const DevTree& t, const uint32_t epoch, const 
 }
 
 // DELETE in a candidate leaf, lock first (as fast_insert_locked): a wrong
-// leaf is unlocked unchanged (retry); an absent key answers ABSENT.
+// leaf is unlocked unchanged (FAST_WRONG); an absent key answers ABSENT.
 __device__ int fast_delete_locked(const DevTree& t, const uint32_t epoch, const uint32_t node, const uint64_t key,
                                   uint64_t& ans, uint8_t& st) {
   const uint32_t lane = lane_id();
@@ -464,7 +465,7 @@ __device__ int fast_delete_locked(const DevTree& t, const uint32_t epoch, const 
   if (!(lo <= key && key < fence_key)) {
     if (lane == 0) st_release(hp, h);
     __syncwarp();
-    return FAST_RETRY;
+    return FAST_WRONG;
   }
   if (lane == 31) k = kKeyMax;
   const uint32_t mm = __ballot_sync(kFull, lane < size && k == key);
@@ -500,8 +501,8 @@ __device__ int tx_fast(const DevTree& t, const uint32_t epoch, const uint64_t ke
                        const bool is_insert, const bool is_del, uint64_t& ans, uint8_t& st, const LearnedDev* M) {
   const uint32_t lane = lane_id();
   Ctrl* C = t.ctrl;
-  uint32_t node = ld_relaxed32(&C->root);
-  if (node == kNil) return FAST_SLOW;
+  const uint32_t root = ld_relaxed32(&C->root);
+  if (root == kNil) return FAST_SLOW;
   // the learned model proposes the leaf; the leaf checks below make any
   // proposal safe, and a miss falls back to the descent
   uint32_t guess = kNil;
@@ -510,79 +511,59 @@ __device__ int tx_fast(const DevTree& t, const uint32_t epoch, const uint64_t ke
     guess = learned_leaf<32>(*M, M->params, key, lane, kFull, dist);
     if (guess >= t.cap) guess = kNil;
   }
-  if (guess != kNil) node = guess;
-  for (int depth = 0; guess == kNil; depth++) {
-    if (depth > 40 || node >= t.cap) return FAST_SLOW;
-    const uint64_t* krow = t.keys + (size_t)node * 32;
-    const uint64_t kr = krow[lane];
-    const uint64_t hdr = __shfl_sync(kFull, kr, 31);
-    if (hdr_level(hdr) == 0) break;
-    const uint64_t v = t.vals[(size_t)node * 32 + lane];
-    const uint32_t c = __popc(__ballot_sync(kFull, lane < 31 && kr <= key));
-    node = (uint32_t)__shfl_sync(kFull, v, c);
-  }
-  const uint64_t* krow = t.keys + (size_t)node * 32;
-  if (is_insert) return fast_insert_locked(t, epoch, node, key, val, ans, st);
-  if (is_del) return fast_delete_locked(t, epoch, node, key, ans, st);
-  // seqlock read of the leaf
-  const uint64_t h = ld_acquire(krow + 31);
-  uint64_t k = ld_relaxed(krow + lane);
-  const uint64_t v = ld_relaxed(t.vals + (size_t)node * 32 + lane);
-  const uint64_t lo = ld_relaxed(t.low + node);
-  fence_acq_rel();
-  const uint64_t h2 = ld_relaxed(krow + 31);
-  const uint64_t h_lane0 = __shfl_sync(kFull, h, 0);
-  const uint64_t fence_key = __shfl_sync(kFull, v, 31);
-  const bool bad = hdr_locked(h) || h2 != h || h != h_lane0 || hdr_level(h) != 0 || hdr_epoch(h) != epoch ||
-                   !(lo <= key && key < fence_key);
-  if (__any_sync(kFull, bad)) return FAST_RETRY;
-  if (lane == 31) k = kKeyMax;
-  const uint32_t size = hdr_size(h);
-  const uint32_t mm = __ballot_sync(kFull, lane < size && k == key);
-  if (!is_insert) {
-    if (mm) {
-      ans = __shfl_sync(kFull, v, __ffs(mm) - 1);
-      st = kFound;
-    } else {
-      ans = 0;
-      st = kAbsent;
+  // Two passes at most: the proposed leaf, then, when its fences show that
+  // it is not the key's leaf (it split after the model was trained), the
+  // descent from the root in the same attempt, without an abort.
+  for (int pass = 0;; pass++) {
+    uint32_t node = guess != kNil ? guess : root;
+    for (int depth = 0; guess == kNil; depth++) {
+      if (depth > 40 || node >= t.cap) return FAST_SLOW;
+      const uint64_t* krow = t.keys + (size_t)node * 32;
+      const uint64_t kr = krow[lane];
+      const uint64_t hdr = __shfl_sync(kFull, kr, 31);
+      if (hdr_level(hdr) == 0) break;
+      const uint64_t v = t.vals[(size_t)node * 32 + lane];
+      const uint32_t c = __popc(__ballot_sync(kFull, lane < 31 && kr <= key));
+      node = (uint32_t)__shfl_sync(kFull, v, c);
     }
-    return FAST_DONE;
+    int r;
+    if (is_insert) {
+      r = fast_insert_locked(t, epoch, node, key, val, ans, st);
+    } else if (is_del) {
+      r = fast_delete_locked(t, epoch, node, key, ans, st);
+    } else {
+      // seqlock read of the leaf
+      const uint64_t* krow = t.keys + (size_t)node * 32;
+      const uint64_t h = ld_acquire(krow + 31);
+      uint64_t k = ld_relaxed(krow + lane);
+      const uint64_t v = ld_relaxed(t.vals + (size_t)node * 32 + lane);
+      const uint64_t lo = ld_relaxed(t.low + node);
+      fence_acq_rel();
+      const uint64_t h2 = ld_relaxed(krow + 31);
+      const uint64_t h_lane0 = __shfl_sync(kFull, h, 0);
+      const uint64_t fence_key = __shfl_sync(kFull, v, 31);
+      const bool bad = hdr_locked(h) || h2 != h || h != h_lane0 || hdr_level(h) != 0 || hdr_epoch(h) != epoch;
+      if (__any_sync(kFull, bad)) return FAST_RETRY;
+      if (__any_sync(kFull, !(lo <= key && key < fence_key))) {
+        r = FAST_WRONG;
+      } else {
+        if (lane == 31) k = kKeyMax;
+        const uint32_t size = hdr_size(h);
+        const uint32_t mm = __ballot_sync(kFull, lane < size && k == key);
+        if (mm) {
+          ans = __shfl_sync(kFull, v, __ffs(mm) - 1);
+          st = kFound;
+        } else {
+          ans = 0;
+          st = kAbsent;
+        }
+        return FAST_DONE;
+      }
+    }
+    if (r != FAST_WRONG) return r;
+    if (guess == kNil || pass > 0) return FAST_RETRY;  // a concurrent split moved the key: retry
+    guess = kNil;
   }
-  if (mm) {
-    const uint32_t at = __ffs(mm) - 1;
-    const uint64_t old = __shfl_sync(kFull, v, at);
-    if (!acquire_locks(t, node, h, kNil, 0, false, 0)) return FAST_RETRY;
-    if (lane == at) t.vals[(size_t)node * 32 + at] = val;
-    __threadfence();
-    __syncwarp();
-    if (lane == 0) st_release(hdr_ptr(t, node), hdr_next(h, size));
-    __syncwarp();
-    ans = old;
-    st = kFound;
-    return FAST_DONE;
-  }
-  if (size >= (uint32_t)kMaxKeys) return FAST_SLOW;  // needs a split: validated path
-  const uint32_t p = __popc(__ballot_sync(kFull, lane < size && k < key));
-  const uint64_t uk = __shfl_up_sync(kFull, k, 1);
-  const uint64_t uv = __shfl_up_sync(kFull, v, 1);
-  const uint64_t nk = lane < p ? k : (lane == p ? key : uk);
-  const uint64_t nv = lane < p ? v : (lane == p ? val : uv);
-  if (!acquire_locks(t, node, h, kNil, 0, false, 0)) return FAST_RETRY;
-  if (lane <= size && lane < 31) {
-    t.keys[(size_t)node * 32 + lane] = nk;
-    t.vals[(size_t)node * 32 + lane] = nv;
-  }
-  __threadfence();
-  __syncwarp();
-  if (lane == 0) {
-    st_release(hdr_ptr(t, node), hdr_next(h, size + 1));
-    atomicAdd(&C->n_keys, 1ull);
-  }
-  __syncwarp();
-  ans = 0;
-  st = kAbsent;
-  return FAST_DONE;
 }
 
 // A GET by an 8-lane group (lane g owns slots 4g..4g+3), so that a warp
@@ -838,20 +819,25 @@ __global__ void __launch_bounds__(256, 4) serve_kernel(DevTree t, ServeDev S, ui
   const LearnedDev* M = use_learned ? &lm : nullptr;
   TxCounters cnt;
   const uint32_t epoch = t.ctrl->epoch;
-  // Idle exit is decided on the whole kernel's activity, not the warp's own:
-  // a warp that slept through a small batch claimed by others must not count
-  // that time as idle, or warps would leave one by one while work keeps
-  // coming and the grid would dwindle (the host relaunches only when the
-  // whole kernel has ended).
+  // Idle exit is decided on the whole kernel's activity, not the warp's own
+  // (a warp that slept through a small batch claimed by others must not count
+  // that time as idle), and it is all or nothing: the warp that sees the
+  // timeout raises `exiting` and every warp leaves at its next turn, even if
+  // work has arrived meanwhile.  Warps that left one by one would leave a
+  // kernel of a few warps that new work keeps alive, so the host (which
+  // relaunches only when the whole kernel has ended) would never restore the
+  // full grid.  The graph clears `exiting` before each launch.
   const unsigned long long t_start = global_ns();
   unsigned long long my_mark = 0;
   for (;;) {
-    uint32_t cur = 0, tail = 0, stop = 0;
+    uint32_t cur = 0, tail = 0, stop = 0, ex = 0;
     if (lane == 0) {
+      ex = ld_relaxed32(S.exiting);
       tail = ld_acquire32(S.tail);
       cur = ld_relaxed32(S.cursor);
       stop = ld_relaxed32(S.stop);
     }
+    if (__shfl_sync(kFull, ex, 0)) break;  // the kernel is ending: later work waits for the relaunch
     cur = __shfl_sync(kFull, cur, 0);
     tail = __shfl_sync(kFull, tail, 0);
     stop = __shfl_sync(kFull, stop, 0);
@@ -863,6 +849,7 @@ __global__ void __launch_bounds__(256, 4) serve_kernel(DevTree t, ServeDev S, ui
         unsigned long long busy = ld_relaxed(reinterpret_cast<const uint64_t*>(S.last_busy));
         if (busy < t_start) busy = t_start;
         leave = now - busy > S.idle_ns;
+        if (leave) atomicExch(S.exiting, 1u);
       }
       if (__shfl_sync(kFull, leave, 0)) break;
       __nanosleep(2000);

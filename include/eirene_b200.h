@@ -147,8 +147,9 @@ int bt_execute_batch(bt_handle *h, const uint64_t *keys, const uint64_t *vals, c
 
 /* Same as bt_execute_batch with HOST buffers: copies in, runs, copies out and
  * synchronises `stream`.  Pinned buffers (bt_host_alloc) give full PCIe speed;
- * with BT_MODE_SORTED and a page-locked `vals`, the value array is not copied:
- * the kernels read the values of the batch's writes from it over the bus.
+ * with BT_OPT_HOST_VALUES_IN_PLACE, BT_MODE_SORTED and a page-locked `vals`,
+ * the value array is not copied: the kernels read the values of the batch's
+ * writes from it over the bus.
  * Mirrors the reference's transferData -> kernel -> transferAns loop body
  * (src/gpu-stm-tree-v39/bpt-gpustm.cpp:78-105). */
 int bt_execute_batch_host(bt_handle *h, const uint64_t *keys, const uint64_t *vals, const uint8_t *ops,
@@ -253,6 +254,10 @@ int bt_set_search_group(bt_handle *h, uint32_t lanes);
                                 * touches the tree (bt_sync waits explicitly); 0 the merge runs on the caller's
                                 * stream.  Same answers and tree. */
 #define BT_OPT_REFIT_STEPS 11  /* warm-started Adam steps of the stage-1 model per bt_refit (default 0) */
+#define BT_OPT_HOST_VALUES_IN_PLACE 13 /* host-buffer entry points, BT_MODE_SORTED: 1 reads the values of the
+                                       * batch's writes from a page-locked value array over the bus instead of
+                                       * copying the array (fewer bytes, but scattered reads; measured slower on
+                                       * a 95/5 batch of 2^22); 0 (default) copies it */
 #define BT_OPT_LEARNED_MODE 12 /* unsorted learned lookups: 1 one request per lane group, 2 two requests per
                                 * group in lock step, 3 (default) software-pipelined: a group carries up to five
                                 * requests, one in each round of loads (list entry, key, leaf-table probe, leaf
@@ -327,9 +332,10 @@ typedef struct bt_serve_config {
     uint64_t arena_bytes;  /* device memory for batches in flight: 26 B per request (default 1 GiB) */
     uint32_t max_batches;  /* ring slots (default 256) */
     uint32_t idle_us;      /* the persistent kernel exits after this long without work (default 2000) */
-    uint32_t policy;       /* which admitted batch a free warp takes work from: 0 the oldest (first in,
-                            * first out), 1 (default) the one with the fewest unclaimed requests among the
-                            * 32 oldest, so that small batches are not held behind a large one */
+    uint32_t policy;       /* which admitted batch a free warp takes work from: 0 (default) the oldest
+                            * (first in, first out), 1 the one with the fewest unclaimed requests among the
+                            * 32 oldest, so that small batches are not held behind a large one (measured:
+                            * lower p50 but a p99 in the hundreds of ms for the large batches it holds back) */
     uint32_t reserved[5];
 } bt_serve_config;
 typedef struct bt_serve_stats {
@@ -342,6 +348,8 @@ typedef struct bt_serve_stats {
     double p50_service_ms, p99_service_ms;   /* device time from the batch's first claimed chunk to its
                                               * last finished one (the rest of the latency is waiting
                                               * for admission, the copies and the first claim) */
+    double device_mops;                      /* completed requests / (latest completion - earliest first
+                                              * claim), both on the device clock */
 } bt_serve_stats;
 int bt_serve_config_init(bt_serve_config *cfg);
 int bt_serve_start(bt_handle *h, const bt_serve_config *cfg, bt_server **out);
@@ -351,6 +359,11 @@ int bt_submit(bt_server *s, const uint64_t *keys_host, const uint64_t *vals_host
 int bt_poll(bt_server *s, uint64_t ticket, int *done);
 int bt_wait(bt_server *s, uint64_t ticket, uint32_t timeout_ms /* 0 = no limit */);
 int bt_serve_get_stats(bt_server *s, bt_serve_stats *st, int reset);
+/* Device clock (ns) of a finished batch's first claimed chunk and of its
+ * completion; BT_ERR_INVALID_ARG for a batch that has not finished or whose
+ * slot has been reused since.  Shows which batches ran on the device at the
+ * same time. */
+int bt_serve_batch_times(bt_server *s, uint64_t ticket, uint64_t *first_claim_ns, uint64_t *done_ns);
 int bt_serve_stop(bt_server *s);
 
 /* ---- benchmark input generators (seeded, counter based; device output) ----

@@ -27,3 +27,5 @@ def test_reference_arm_json_line():
     assert cb["value"] == d["value"] and cb["kind"] in ("port", "reference") and cb["cores"] >= 1
     assert d["e2e"]["value"] == d["value"] and d["e2e"]["unit"] == d["unit"]
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+    # the same-box comparison with the reference's GPU build needs a GPU
+    assert "reference_gpu" in d

@@ -124,20 +124,21 @@ def test_merge_engine_pool_exhaustion(gpu, host):
     assert all(int(vv) == vals_now[int(kk)] for kk, vv in zip(k[::97], v[::97]))
 
 
-@pytest.mark.parametrize("pinned", [True, False])
+@pytest.mark.parametrize("pinned,in_place", [(True, 0), (True, 1), (False, 0), (False, 1)])
 @pytest.mark.parametrize("mode", [MERGE, E.MODE_SORTED, E.MODE_STM])
-def test_async_host_batches_in_flight(gpu, pinned, mode):
+def test_async_host_batches_in_flight(gpu, pinned, in_place, mode):
     # bt_execute_batch_host_async: up to three batches queued before the
     # first wait (the third submit waits for the first staging set), answers
-    # request by request against the oracle.  With page-locked buffers the
-    # sorted modes read the values of the writes over the bus instead of
-    # copying the value array; pageable buffers are copied.
+    # request by request against the oracle.  With page-locked buffers and
+    # OPT_HOST_VALUES_IN_PLACE the sorted modes read the values of the writes
+    # over the bus instead of copying the value array; otherwise it is copied.
     import torch
 
     keys = O.gen_keys("uniform", 301, 60_000)
     vals = O.value_of(keys)
     t = E.BTree(max_keys=1 << 20, max_batch=1 << 16)
     t.bulk_build(dev(keys), dev(vals))
+    t.set_option(E.OPT_HOST_VALUES_IN_PLACE, in_place)  # pageable values are copied either way
     o = O.OracleTree()
     o.bulk_build(keys, vals)
     bufs, pinned_bufs, expect = [], [], []

@@ -51,7 +51,7 @@ def oracle_answers(keys_tree, vals_tree, batches):
     return outs, o
 
 
-def serve_all(server, batches, timeout_s=120):
+def serve_all(server, batches, timeout_s=120, tickets_out=None):
     outs = [(np.zeros(b[0].size, np.uint64), np.zeros(b[0].size, np.uint8)) for b in batches]
     tickets = [None] * len(batches)
     t0 = time.time()
@@ -69,6 +69,8 @@ def serve_all(server, batches, timeout_s=120):
         i += 1
     for tk in tickets:
         server.wait(tk)
+    if tickets_out is not None:
+        tickets_out.extend(tickets)
     return outs
 
 
@@ -76,16 +78,25 @@ def test_alone_equals_in_mix(gpu):
     t1, keys, vals = build()
     parts = [(0, 50_000), (50_000, 100_000), (100_000, 150_000), (150_000, 200_000)]
     A = make_batch(np.sort(keys), parts[0], 20_000, 0.7, seed=1)
-    mix = [make_batch(np.sort(keys), parts[k], 30_000, 0.5 + 0.15 * k, seed=10 + k) for k in (1, 2, 3)]
+    # the first batch of the mix is large, so the others arrive while it runs
+    mix = [make_batch(np.sort(keys), parts[k], 90_000 if k == 1 else 30_000, 0.5 + 0.15 * k, seed=10 + k)
+           for k in (1, 2, 3)]
     s1 = E.Server(t1)
     alone = serve_all(s1, [A])[0]
     s1.stop()
     t2, _, _ = build()
     s2 = E.Server(t2)
     batches = [mix[0], A, mix[1], mix[2]]
-    res = serve_all(s2, batches)
+    tickets = []
+    res = serve_all(s2, batches, tickets_out=tickets)
     st = s2.stats()
+    # the batches were on the device together: A's span (first claimed chunk
+    # to completion, device clock) overlaps another batch's span
+    spans = [s2.batch_times(tk) for tk in tickets]
     s2.stop()
+    a0, a1 = spans[1]
+    assert all(s < e for s, e in spans)
+    assert any(max(a0, s) < min(a1, e) for j, (s, e) in enumerate(spans) if j != 1), spans
     inmix = res[1]
     assert (alone[0] == inmix[0]).all() and (alone[1] == inmix[1]).all()
     ref, o = oracle_answers(keys, vals, batches)
