@@ -249,6 +249,60 @@ def reference_gpu(ref_bin: str, batches: int = 10):
     return out
 
 
+def stm_passes(E, torch, tree, tk, n_b, steps, search_pct, stream):
+    """BT_MODE_STM batches (the reference's v39 meaning: requests are
+    concurrent warp transactions): on the headline tree with its workload, and
+    on a skewed tree (Zipf(0.99) 2^25 keys, 95/5, the inserts drawn from the
+    same Zipf law, so popular keys repeat and transactions collide).  Reports
+    Mops/s and the STM counters: commits, aborts (the reference's
+    ABORT_COUNT roll-backs, src/gpu-stm-tree-v39/bpt-gpustm-kernel.cu:58-63)
+    and requests that exhausted the retry limit."""
+    out = {}
+
+    def run(t, keys_dev, dist, seed0):
+        bs = []
+        for i in range(3 + steps):
+            k = torch.empty(n_b, dtype=torch.int64, device="cuda")
+            v = torch.empty(n_b, dtype=torch.int64, device="cuda")
+            o = torch.empty(n_b, dtype=torch.uint8, device="cuda")
+            E.gen_requests(dist, seed0 + i, keys_dev, n_b, search_pct, k, v, o, stream)
+            bs.append((k, v, o))
+        ov = torch.empty(n_b, dtype=torch.int64, device="cuda")
+        ost = torch.empty(n_b, dtype=torch.uint8, device="cuda")
+        for i in range(3):
+            t.execute(*bs[i], ov, ost, mode=E.MODE_STM, stream=stream)
+        torch.cuda.synchronize()
+        s0 = t.stats()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(3, 3 + steps):
+            t.execute(*bs[i], ov, ost, mode=E.MODE_STM, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        s1 = t.stats()
+        ms = e0.elapsed_time(e1)
+        commits, aborts = s1["commits"] - s0["commits"], s1["aborts"] - s0["aborts"]
+        return {"mops": n_b * steps / (ms / 1e3) / 1e6, "ms_per_batch": ms / steps, "commits": commits,
+                "aborts": aborts, "aborts_per_commit": aborts / max(1, commits),
+                "retry_exhausted": s1["retry_exhausted"] - s0["retry_exhausted"], "batches": steps}
+
+    tree.set_descent(False)
+    out["headline_tree"] = run(tree, tk, "uniform", 60_000)
+    nz = 1 << 25
+    zt = E.BTree(max_keys=2 * nz, max_batch=n_b)
+    zk = torch.empty(nz, dtype=torch.int64, device="cuda")
+    zv = torch.empty(nz, dtype=torch.int64, device="cuda")
+    E.gen_keys("zipf", 2, nz, zk, zv, stream)
+    zt.bulk_build(zk, zv, stream)
+    del zv
+    out["zipf_2e25"] = run(zt, zk, "zipf", 70_000)
+    zt.close()
+    del zk
+    out["workload"] = (f"batches of {n_b} requests, {search_pct}% search, BT_MODE_STM; the headline tree, and a "
+                       "Zipf(0.99) tree of 2^25 keys with Zipf-drawn (duplicate-heavy) inserts")
+    return out
+
+
 def same_box_ours(E, torch, batches: int = 10):
     """This library on the 31-bit workload the reference arm gives the
     reference program: the tree built by inserting the build file's pairs
@@ -663,6 +717,10 @@ def main():
                     help="sorted batches: hash front end (sort only INSERT-coupled requests) or full sort")
     ap.add_argument("--pool-keys-log2", type=int, default=0,
                     help="size the node pool for 2^x keys (default: 2 x tree + 32 x batch)")
+    ap.add_argument("--no-fill-tune", action="store_true",
+                    help="build with the default node fill (24) instead of the fill autotuner's pick")
+    ap.add_argument("--no-stm-pass", action="store_true",
+                    help="skip the BT_MODE_STM passes (headline tree and a skewed Zipf tree) with abort counts")
     ap.add_argument("--no-same-box", action="store_true",
                     help="skip the comparison with the reference's GPU build on its own 31-bit benchmark shape")
     ap.add_argument("--serve-only", action="store_true",
@@ -741,6 +799,11 @@ def main():
     tk = torch.empty(n_tree, dtype=torch.int64, device="cuda")
     tv = torch.empty(n_tree, dtype=torch.int64, device="cuda")
     E.gen_keys(args.dist, 1 + rank, n_tree, tk, tv, stream)
+    # node fill (fanout) from the autotuner, on a sample tree of 2^22 of the
+    # keys, before the tree is built (later splits use it too)
+    fill = None
+    if sharded is None and not args.no_fill_tune:
+        fill = tree.autotune_fill(tk[: min(n_tree, 1 << 22)], stream)
     t0 = time.time()
     if sharded is not None:
         sharded.bulk_build(tk, tv)
@@ -1008,6 +1071,12 @@ def main():
             except Exception as ex:  # reported, not fatal
                 serving[form] = {"error": str(ex)}
 
+    stm = None
+    if world == 1 and not args.no_stm_pass:
+        try:
+            stm = stm_passes(E, torch, tree, tk, n_b, 5, args.search_pct, stream)
+        except Exception as ex:  # reported, not fatal
+            stm = {"error": str(ex)}
     same_box = None
     if not args.no_same_box and world == 1:
         try:
@@ -1065,6 +1134,7 @@ def main():
                                 if sharded is not None else "one tree on one GPU"),
                 "tree_build_s": build_s,
                 "learned_retrain_every": args.retrain_every,
+                "node_fill": fill,
                 "learned_retrain_mode": args.retrain_mode,
             },
             "roofline": roof,
@@ -1084,6 +1154,8 @@ def main():
             line["check"] = check
         if same_box is not None:
             line["same_box_31bit"] = same_box
+        if stm is not None:
+            line["stm"] = stm
         print(json.dumps(line), flush=True)
     tree.close()
     if dist is not None:

@@ -102,12 +102,12 @@ EXPORTS = [
     "bt_set_learned_group", "bt_learned_info", "bt_mlp_grad", "bt_set_option", "bt_autotune",
     "bt_serve_config_init", "bt_serve_start", "bt_submit", "bt_poll", "bt_wait", "bt_serve_get_stats", "bt_serve_stop",
     "bt_route_batch", "bt_unroute_results", "bt_save", "bt_load", "bt_range_batch", "bt_sync", "bt_save_image", "bt_load_image",
-    "bt_refit", "bt_execute_batch_host_async", "bt_host_wait", "bt_serve_batch_times",
+    "bt_refit", "bt_execute_batch_host_async", "bt_host_wait", "bt_serve_batch_times", "bt_autotune_fill",
 ]
 MAX_SHARDS = 256
 OPT_SORTED_SEARCH, OPT_RETRY_LIMIT, OPT_TRAIN_STEPS, OPT_SORTED_LEAF_VALS, OPT_BATCH_DESCENT = 1, 2, 3, 4, 5
 OPT_FRONT_END, OPT_TOP_CACHE, OPT_SEARCH_PAIRS, OPT_OVERLAP, OPT_ASYNC_WRITE = 6, 7, 8, 9, 10
-OPT_REFIT_STEPS, OPT_LEARNED_MODE, OPT_HOST_VALUES_IN_PLACE = 11, 12, 13
+OPT_REFIT_STEPS, OPT_LEARNED_MODE, OPT_HOST_VALUES_IN_PLACE, OPT_SORT_TILE = 11, 12, 13, 14
 PHASES = ["sort", "merge", "search", "insert", "writeback"]
 
 _lib = None
@@ -175,6 +175,7 @@ def lib():
             "bt_mlp_grad": [_P, _P, _P, _P, _SZ, _P, _P, _P],
             "bt_set_option": [_P, ctypes.c_int, ctypes.c_int64],
             "bt_autotune": [_P, _P, _SZ, _P, _P],
+            "bt_autotune_fill": [_P, _P, _SZ, _P, _P],
             "bt_serve_config_init": [ctypes.POINTER(ServeConfig)],
             "bt_serve_start": [_P, ctypes.POINTER(ServeConfig), ctypes.POINTER(_P)],
             "bt_submit": [_P, _P, _P, _P, _SZ, _P, _P, ctypes.POINTER(ctypes.c_uint64)],
@@ -380,7 +381,7 @@ class BTree:
         _check(lib().bt_set_option(self._h, option, value), "bt_set_option")
 
     def autotune(self, sample_keys, stream=None) -> dict:
-        rep = (ctypes.c_double * 16)()
+        rep = (ctypes.c_double * 24)()
         _check(lib().bt_autotune(self._h, _ptr(sample_keys), sample_keys.numel(), _stream_ptr(stream), rep),
                "bt_autotune")
         r = list(rep)
@@ -389,7 +390,19 @@ class BTree:
                 "learned_mode": int(r[15]),
                 "plain_ms": dict(zip([4, 8, 16, 32], r[4:8])),
                 "learned_ms": dict(zip(["4 pipelined", "8 pipelined", "4x1", "4x2"], r[8:12])),
-                "sorted_plain_ms": r[12:14], "sorted_learned_ms": r[14]}
+                "sorted_plain_ms": r[12:14], "sorted_learned_ms": r[14],
+                "sort_threads": int(r[16]), "sort_threads_touched": int(r[17]),
+                "sort_ms": dict(zip([256, 512, 1024], r[18:21])),
+                "sort_touched_ms": dict(zip([256, 512, 1024], r[21:24]))}
+
+    def autotune_fill(self, sample_keys, stream=None) -> dict:
+        """bt_autotune_fill: the node fill for later bulk builds and splits,
+        chosen by timing batches on sample trees."""
+        rep = (ctypes.c_double * 8)()
+        _check(lib().bt_autotune_fill(self._h, _ptr(sample_keys), sample_keys.numel(), _stream_ptr(stream), rep),
+               "bt_autotune_fill")
+        r = list(rep)
+        return {"leaf_fill": int(r[0]), "inner_fill": int(r[1]), "batch_ms": dict(zip([16, 20, 24, 28], r[2:6]))}
 
     def set_learned_group(self, lanes: int):
         _check(lib().bt_set_learned_group(self._h, lanes), "bt_set_learned_group")

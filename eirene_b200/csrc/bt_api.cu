@@ -661,6 +661,10 @@ int bt_set_option(bt_handle* H, int option, int64_t value) {
       if (value < 0 || value > 1000000) return BT_ERR_INVALID_ARG;
       H->h.L.refit_steps = (uint32_t)value;
       return BT_OK;
+    case BT_OPT_SORT_TILE:
+      if (value != 256 && value != 512 && value != 1024) return BT_ERR_INVALID_ARG;
+      H->h.sort_threads = H->h.sort_threads_touch = (int)value;
+      return BT_OK;
     case BT_OPT_HOST_VALUES_IN_PLACE:
       H->h.host_vals_in_place = value ? 1 : 0;
       return BT_OK;
@@ -679,6 +683,78 @@ int bt_autotune(bt_handle* H, const uint64_t* sample_keys, size_t n, void* strea
   if (stream == nullptr) cudaDeviceSynchronize();
   if (bt::tree_join(&H->h, s) != cudaSuccess) return BT_ERR_CUDA;
   return map_internal(bt::autotune(&H->h, sample_keys, n, s, report));
+}
+
+// Node fill: a temporary handle per candidate fill holds a sample tree built
+// from the caller's keys; a sorted 95/5 batch of the same size (half of its
+// searches for sample keys, inserts of fresh keys) is timed on it, and the
+// handle keeps the fill of the fastest for its later bulk builds and splits.
+int bt_autotune_fill(bt_handle* H, const uint64_t* sample_keys, size_t n, void* stream, double* report) {
+  if (!H || !sample_keys || n < 64) return BT_ERR_INVALID_ARG;
+  DeviceGuard g(H->h.device);
+  cudaStream_t s = S(stream);
+  if (cudaStreamSynchronize(s) != cudaSuccess || bt::tree_sync(&H->h) != cudaSuccess) return BT_ERR_CUDA;
+  const uint32_t fills[4] = {16, 20, 24, 28};
+  double out[8] = {};
+  uint64_t *rk = nullptr, *rv = nullptr, *ov = nullptr;
+  uint8_t *ro = nullptr, *os = nullptr;
+  const size_t nb = 2;  // timed batches
+  bool ok = cudaMalloc(&rk, nb * n * 8) == cudaSuccess && cudaMalloc(&rv, nb * n * 8) == cudaSuccess &&
+            cudaMalloc(&ro, nb * n) == cudaSuccess && cudaMalloc(&ov, n * 8) == cudaSuccess &&
+            cudaMalloc(&os, n) == cudaSuccess;
+  for (size_t b = 0; ok && b < nb; b++)
+    ok = bt_gen_requests(0, 0xF111u + b, sample_keys, n, n, 95, rk + b * n, rv + b * n, ro + b * n, s) == BT_OK;
+  double best = 1e30;
+  uint32_t best_fill = H->h.leaf_fill;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  ok = ok && cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess;
+  for (int i = 0; ok && i < 4; i++) {
+    bt_config c;
+    bt_config_init(&c);
+    c.device = H->h.device;
+    c.max_keys = 3 * n;
+    c.max_batch = n;
+    c.leaf_fill = c.inner_fill = fills[i];
+    bt_handle* T = nullptr;
+    if (bt_create(&c, &T) != BT_OK) {
+      ok = false;
+      break;
+    }
+    const int mode = BT_MODE_SORTED | BT_MODE_MERGE_ENGINE;
+    bool run = bt_bulk_build(T, sample_keys, sample_keys, n, s) == BT_OK;
+    // one untimed batch (first touch of the buffers), then the timed ones on a fresh build
+    run = run && bt_execute_batch(T, rk, rv, ro, ov, os, n, mode, s) == BT_OK && bt_sync(T, s) == BT_OK;
+    run = run && bt_bulk_build(T, sample_keys, sample_keys, n, s) == BT_OK;
+    run = run && cudaEventRecord(e0, s) == cudaSuccess;
+    for (size_t b = 0; run && b < nb; b++)
+      run = bt_execute_batch(T, rk + b * n, rv + b * n, ro + b * n, ov, os, n, mode, s) == BT_OK;
+    run = run && bt_sync(T, s) == BT_OK && cudaEventRecord(e1, s) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess;
+    float ms = 0;
+    run = run && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+    bt_destroy(T);
+    if (!run) {
+      ok = false;
+      break;
+    }
+    out[2 + i] = ms / nb;
+    if (ms < best) {
+      best = ms;
+      best_fill = fills[i];
+    }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(rk);
+  cudaFree(rv);
+  cudaFree(ro);
+  cudaFree(ov);
+  cudaFree(os);
+  if (!ok) return BT_ERR_CUDA;
+  H->h.leaf_fill = H->h.inner_fill = best_fill;
+  out[0] = out[1] = best_fill;
+  if (report)
+    for (int i = 0; i < 8; i++) report[i] = out[i];
+  return BT_OK;
 }
 
 int bt_set_learned_group(bt_handle* H, uint32_t lanes) {

@@ -48,7 +48,9 @@ namespace {
 
 constexpr int kThreads = 512;
 constexpr int kItems = 8;
-constexpr int kTile = kThreads * kItems;  // matches the sort tile
+constexpr int kTile = kThreads * kItems;
+
+inline size_t pass_tiles(size_t n) { return (n + kTile - 1) / kTile; }
 constexpr uint32_t kIdxMask = 0x3FFFFFFFu;
 constexpr uint32_t kResolved = 0xFFFFFFFFu;
 
@@ -337,7 +339,7 @@ __global__ void writeback_kernel(const uint32_t* __restrict__ sv, const uint32_t
 int work_alloc(Work* w, size_t cap) {
   work_free(w);
   if (cap == 0) cap = 1;
-  const size_t tiles = sort_tiles(cap);
+  const size_t tiles = pass_tiles(cap);
   bool ok = true;
   auto A = [&](void** p, size_t bytes) {
     if (ok && cudaMalloc(p, bytes) != cudaSuccess) ok = false;
@@ -466,9 +468,9 @@ static int batch_hashed(Handle* h, const uint64_t* keys, const uint64_t* vals, c
   uint64_t* sk = nullptr;
   uint32_t* sv = nullptr;
   if (radix_sort_pairs(w.f_tk, w.f_tv, nullptr, w.k_a, w.v_a, w.k_b, w.v_b, n, 0, 64, w.sort_scratch, s, &sk, &sv,
-                       &h->tree.ctrl->error, n_touch) != cudaSuccess)
+                       &h->tree.ctrl->error, n_touch, h->sort_threads_touch) != cudaSuccess)
     return -2;
-  const uint32_t n_tiles = (uint32_t)sort_tiles(n);
+  const uint32_t n_tiles = (uint32_t)pass_tiles(n);
   prof_mark(h, ov ? kEvSortEnd : 1, s);
   // the locates (side stream) run beside the lookups (`s`); so do the merge
   // passes when the values are still being copied in (vals_wait): the
@@ -561,10 +563,10 @@ int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const ui
   uint64_t* sk = nullptr;
   uint32_t* sv = nullptr;
   prof_mark(h, 0, s);
-  if (radix_sort_pairs(keys, nullptr, ops, w.k_a, w.v_a, w.k_b, w.v_b, n, 0, 64, w.sort_scratch, s, &sk, &sv, &h->tree.ctrl->error) !=
-      cudaSuccess)
+  if (radix_sort_pairs(keys, nullptr, ops, w.k_a, w.v_a, w.k_b, w.v_b, n, 0, 64, w.sort_scratch, s, &sk, &sv,
+                       &h->tree.ctrl->error, nullptr, h->sort_threads) != cudaSuccess)
     return -2;
-  const uint32_t n_tiles = (uint32_t)sort_tiles(n);
+  const uint32_t n_tiles = (uint32_t)pass_tiles(n);
   prof_mark(h, 1, s);
   if (wait_vals(h, s) != 0) return -2;
   merge_pass1<<<n_tiles, kThreads, 0, s>>>(sk, sv, vals, n, nullptr, w.tiles);

@@ -7,7 +7,10 @@
 // of sorting the whole batch, the front end
 //
 //   1. counts the write requests and sizes an open-addressing table for
-//      their keys (a power of two >= 1.5x the count, at least 1024 slots),
+//      their keys (a power of two >= 4x the count, at least 1024 slots:
+//      most lookups ask for a key the table does not hold, and a linear probe
+//      for an absent key runs about (1 + 1/(1-a)^2)/2 slots at load a: 1.4
+//      at a = 1/4, 5 at a = 2/3),
 //   2. records, per written key, the index of its first write,
 //   3. classifies every request: "touched" if its op code is invalid or its
 //      key has a write at or before it; otherwise it is a plain lookup,
@@ -57,7 +60,7 @@ __device__ __forceinline__ uint32_t is_write(uint8_t op) { return (op == kOpInse
 
 __device__ __forceinline__ uint32_t table_cap(uint32_t n_ins, size_t cap_max) {
   uint64_t c = 1024;
-  while (2 * c < 3ull * n_ins) c <<= 1;  // load factor at most 2/3
+  while (c < 4ull * n_ins) c <<= 1;  // load factor at most 1/4 (up to the allocation)
   return (uint32_t)(c < cap_max ? c : cap_max);
 }
 
@@ -121,17 +124,6 @@ __global__ void __launch_bounds__(kThreads) front_insert_kernel(const uint64_t* 
     if (is_write(ops[i])) put(i);
 }
 
-__device__ __forceinline__ uint32_t find_first_from(const Slot* __restrict__ tab, uint32_t mask, uint64_t k,
-                                                    uint32_t h) {
-  for (uint32_t probe = 0; probe <= mask; probe++) {
-    const uint64_t sk = tab[h].key;
-    if (sk == k) return tab[h].first;
-    if (sk == kKeyMax) return kNone;
-    h = (h + 1) & mask;
-  }
-  return kNone;
-}
-
 // Classify, then compact, in three launches over tiles of kTile requests:
 //   front_flag_kernel     one flag byte per request ("touched": invalid op
 //                         code, or its key has a write at or before it) and
@@ -181,18 +173,43 @@ __global__ void __launch_bounds__(kTileThreads) front_flag_kernel(const uint64_t
       sf[j] = (uint32_t)e.y;
     }
   }
+  // the longer probes, all of this thread's unresolved items one slot per
+  // round (their loads in flight together), instead of item after item
+  uint32_t first[kTileItems];
+  uint32_t todo = 0;
+#pragma unroll
+  for (int j = 0; j < kTileItems; j++) {
+    first[j] = kNone;
+    if (sk[j] == k[j] && k[j] != kKeyMax) first[j] = sf[j];
+    else if (sk[j] != kKeyMax) todo |= 1u << j;
+  }
+  for (uint32_t probe = 0; todo && probe < mask; probe++) {
+#pragma unroll
+    for (int j = 0; j < kTileItems; j++) {
+      if (!((todo >> j) & 1u)) continue;
+      sh[j] = (sh[j] + 1) & mask;
+      const ulonglong2 e = __ldg(reinterpret_cast<const ulonglong2*>(tab + sh[j]));
+      sk[j] = e.x;
+      sf[j] = (uint32_t)e.y;
+    }
+#pragma unroll
+    for (int j = 0; j < kTileItems; j++) {
+      if (!((todo >> j) & 1u)) continue;
+      if (sk[j] == k[j]) {
+        first[j] = sf[j];
+        todo &= ~(1u << j);
+      } else if (sk[j] == kKeyMax) {
+        todo &= ~(1u << j);
+      }
+    }
+  }
   uint32_t c = 0;
 #pragma unroll
   for (int j = 0; j < kTileItems; j++) {
     const size_t i = base + (size_t)j * kTileThreads + threadIdx.x;
     if (i < n) {
       bool f = op[j] > 2;  // invalid op codes are rejected on the sorted path
-      if (!f && any && k[j] != kKeyMax) {
-        uint32_t first = kNone;
-        if (sk[j] == k[j]) first = sf[j];
-        else if (sk[j] != kKeyMax) first = find_first_from(tab, mask, k[j], (sh[j] + 1) & mask);
-        f = first != kNone && (uint32_t)i >= first;
-      }
+      if (!f && any && k[j] != kKeyMax) f = first[j] != kNone && (uint32_t)i >= first[j];
       flags[i] = f ? 1 : 0;
       c += f ? 1u : 0u;
     }

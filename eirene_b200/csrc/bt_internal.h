@@ -32,7 +32,7 @@ constexpr int kLayoutEarly = 2;    // answers written back before the leaf merge
 // kSortRadix counters, 64 tile counters, and one look-back table of
 // kSortRadix words per pass and tile of kSortTileKeys keys
 // (sort_scratch_words computes the same; bt_sort.cu checks the constants)
-constexpr size_t kSortTileKeys = 4096;
+constexpr size_t kSortTileKeys = 2048;  // the smallest tile: scratch for every tile size
 constexpr size_t kSortMaxPasses = 8;
 constexpr size_t kSortRadix = 256;
 constexpr size_t sort_scratch_words_for(size_t n) {
@@ -42,13 +42,13 @@ size_t scan_scratch_words(size_t n);
 cudaError_t scan_exclusive_u32(const uint32_t* in, uint32_t* out, size_t n, uint32_t* total_dev, uint32_t* scratch,
                                cudaStream_t s,
                                const uint32_t* n_dev = nullptr);
-size_t sort_tiles(size_t n);
 cudaError_t sort_prepare();
 size_t sort_scratch_words(size_t n);
+// tile_threads: 256, 512 or 1024 threads per onesweep tile of 8 items each
 cudaError_t radix_sort_pairs(const uint64_t* keys_in, const uint32_t* vals_in, const uint8_t* ops, uint64_t* k_a,
                              uint32_t* v_a, uint64_t* k_b, uint32_t* v_b, size_t n, int begin_bit, int end_bit,
                              uint32_t* scratch, cudaStream_t s, uint64_t** k_out, uint32_t** v_out, uint32_t* err,
-                             const uint32_t* n_dev = nullptr);
+                             const uint32_t* n_dev = nullptr, int tile_threads = 512);
 
 // ---- per-batch work buffers, sized for max_batch requests ----
 struct BatchCounts {
@@ -191,6 +191,8 @@ struct Handle {
                           // 3 software-pipelined (up to five requests per group in successive rounds)
   int sorted_search = 1;  // batch GET phase: 1 = path-reusing search over the sorted keys
   int sorted_leaf_vals = 0;  // sorted search: load the leaf's values with its keys (1) or only the match (0)
+  int sort_threads = 512;        // radix sort tile (x 8 items) for whole-batch sorts
+  int sort_threads_touch = 512;  // ... for the hash front end's sort of the touched requests
   int batch_descent = -1;    // autotuned choice for the batch GET phase: -1 = follow `descent`
   int front_end = 1;         // sorted batches: 1 = hash front end (sort only INSERT-coupled requests), 0 = full sort
   int top_cache = 1;         // unsorted searches descend the upper levels from shared memory
@@ -378,6 +380,7 @@ struct LearnedDev;
 int learned_dev(Handle* h, LearnedDev* out);
 
 // ---- autotuner (bt_tune.cu) ----
+constexpr int kTuneReport = 24;  // doubles in bt_autotune's report (BT_AUTOTUNE_REPORT_LEN)
 int autotune(Handle* h, const uint64_t* keys, size_t n, cudaStream_t s, double* rep);
 
 // ---- learned predictor (bt_learned.cu) ----

@@ -636,15 +636,16 @@ __global__ void __launch_bounds__(kPipeThreads) learned_pipe_kernel(DevTree t, L
     if (vE) {
       const uint64_t hdr = __shfl_sync(gmask, rowE[S - 1], G - 1, G);
       if (g == G - 1) rowE[S - 1] = kKeyMax;  // slot 31 holds the header
-      uint32_t c = 0;
-      bool eq = false;
+      // (shuffle sums: a redux.sync or a ballot per group mask, eight
+      // distinct masks per warp, measured 1.5x slower here)
+      uint32_t c = 0, eq = 0;
 #pragma unroll
       for (int i = 0; i < S; i++) {
         c += (rowE[i] <= kE) ? 1u : 0u;
-        eq |= rowE[i] == kE;
+        eq |= (rowE[i] == kE) ? 1u : 0u;
       }
-      c = group_add<G>(c, gmask);
-      const bool found = (__ballot_sync(gmask, eq) & gmask) != 0;
+      c = group_sum<G>(c, gmask);
+      const bool found = group_sum<G>(eq, gmask) != 0;
       okF = okE && hdr_level(hdr) == 0;
       foundF = found;
       needF = !foundF && c >= hdr_size(hdr);
@@ -661,7 +662,7 @@ __global__ void __launch_bounds__(kPipeThreads) learned_pipe_kernel(DevTree t, L
       uint32_t c = 0;
 #pragma unroll
       for (int e = 0; e < E; e++) c += entD[e].x <= kD ? 1u : 0u;
-      c = group_add<G>(c, gmask);
+      c = group_sum<G>(c, gmask);
       okE = okD && c >= 1 && c < (uint32_t)W;
       const uint32_t i = c >= 1 ? c - 1 : 0;
       uint64_t id = entD[0].y;

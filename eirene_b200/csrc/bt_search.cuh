@@ -130,13 +130,6 @@ __device__ __forceinline__ uint32_t group_sum(uint32_t c, uint32_t gmask) {
   return c;
 }
 
-// The same sum in one warp-level reduction instruction (redux.sync, sm_80+)
-// instead of log2(G) shuffle and add steps
-template <int G>
-__device__ __forceinline__ uint32_t group_add(uint32_t c, uint32_t gmask) {
-  return __reduce_add_sync(gmask, c);
-}
-
 // Rank of `key` in an inner row from the prefixes: slots whose prefix is
 // below the key's count, slots with an equal prefix are counted in bits
 // 16.. (the caller then ranks with the full keys); slot 31 is the header.

@@ -6,7 +6,8 @@
 // The sort follows the single-pass-per-digit scheme of Adinets & Merrill,
 // "Onesweep: A Faster Least Significant Digit Radix Sort for GPUs" (2022):
 //   1. one up-front kernel counts all eight 8-bit digits of every key;
-//   2. per digit, one kernel: a tile of 4096 items takes a dynamic tile id,
+//   2. per digit, one kernel: a tile of T x 8 items (T threads: 2048, 4096 or
+//      8192 items; bt_autotune picks T) takes a dynamic tile id,
 //      ranks its items stably with eight bit ballots per item (each warp owns a
 //      contiguous 256-item chunk and walks it in 8 rounds), publishes its
 //      per-digit counts, and finds its global offsets by decoupled look-back
@@ -24,10 +25,9 @@ namespace bt {
 
 namespace {
 
-constexpr int kSortThreads = 512;
-constexpr int kSortItems = 8;
-constexpr int kTile = kSortThreads * kSortItems;  // 4096
-constexpr int kWarps = kSortThreads / 32;           // 16
+constexpr int kSortThreads = 512;                  // the histogram kernel's block
+constexpr int kSortItems = 8;                      // items per thread in a tile
+constexpr int kMinTile = 256 * kSortItems;         // the smallest tile (T = 256)
 constexpr int kRadix = 256;
 
 constexpr int kScanThreads = 1024;
@@ -168,10 +168,11 @@ __global__ void sort_digit_scan_kernel(uint32_t* __restrict__ hist, int passes) 
   }
 }
 
+template <int T>
 struct ScatterSmem {
-  uint64_t k[kTile];
-  uint32_t v[kTile];
-  uint32_t wh[kWarps][kRadix];
+  uint64_t k[T * kSortItems];
+  uint32_t v[T * kSortItems];
+  uint32_t wh[T / 32][kRadix];
   uint32_t tstart[kRadix];
   uint32_t gofs[kRadix];
   uint32_t ws[32];
@@ -182,19 +183,23 @@ struct ScatterSmem {
 // Blocks take tiles in increasing order from tile_counter until the tiles run
 // out; a block only ever waits on lower tiles, which running blocks hold, so
 // any grid size is safe (the launcher uses at most the resident blocks).
-__global__ void __launch_bounds__(kSortThreads) sort_onesweep_kernel(
+template <int T>
+__global__ void __launch_bounds__(T) sort_onesweep_kernel(
     const uint64_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, const uint8_t* __restrict__ ops,
     int payload_mode, uint64_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, size_t n,
     const uint32_t* __restrict__ n_dev, int shift, const uint32_t* __restrict__ gbase,
     uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ status, uint32_t* __restrict__ err) {
+  static_assert(T >= kRadix, "one thread per digit");
+  constexpr int kTile = T * kSortItems;
+  constexpr int kWarps = T / 32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  ScatterSmem& S = *reinterpret_cast<ScatterSmem*>(smem_raw);
+  ScatterSmem<T>& S = *reinterpret_cast<ScatterSmem<T>*>(smem_raw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (n_dev) n = min(n, (size_t)*n_dev);
   const uint32_t lt_mask = (1u << lane) - 1u;
   for (;;) {
     if (threadIdx.x == 0) S.tile = atomicAdd(tile_counter, 1u);
-    for (int i = threadIdx.x; i < kWarps * kRadix; i += kSortThreads) (&S.wh[0][0])[i] = 0;
+    for (int i = threadIdx.x; i < kWarps * kRadix; i += T) (&S.wh[0][0])[i] = 0;
     __syncthreads();
     const uint32_t tile = S.tile;
     const size_t tile_base = (size_t)tile * kTile;
@@ -296,7 +301,7 @@ __global__ void __launch_bounds__(kSortThreads) sort_onesweep_kernel(
     }
     __syncthreads();
     const uint32_t tile_n = (uint32_t)min((size_t)kTile, n - tile_base);
-    for (uint32_t i = threadIdx.x; i < tile_n; i += kSortThreads) {
+    for (uint32_t i = threadIdx.x; i < tile_n; i += T) {
       const uint64_t k = S.k[i];
       const uint32_t d = digit_of(k, shift);
       const uint32_t g = S.gofs[d] + (i - S.tstart[d]);
@@ -346,23 +351,30 @@ cudaError_t scan_exclusive_u32(const uint32_t* in, uint32_t* out, size_t n, uint
   return cudaGetLastError();
 }
 
-size_t sort_tiles(size_t n) { return (n + kTile - 1) / kTile; }
-
-// Opt the onesweep kernel into >48 KB of shared memory on the current device.
+// Opt the onesweep kernels into >48 KB of shared memory on the current device.
 cudaError_t sort_prepare() {
-  return cudaFuncSetAttribute(sort_onesweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)sizeof(ScatterSmem));
+  cudaError_t e = cudaFuncSetAttribute(sort_onesweep_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sizeof(ScatterSmem<256>));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(sort_onesweep_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(ScatterSmem<512>));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(sort_onesweep_kernel<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(ScatterSmem<1024>));
+  return e;
 }
 
-// resident onesweep blocks on the current device (cached per device)
+// resident onesweep blocks on the current device (cached per device and block size)
+template <int T>
 static unsigned onesweep_resident() {
   static unsigned cache[64] = {};
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
   if (!cache[dev]) {
     int per = 0, sms = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sort_onesweep_kernel, kSortThreads,
-                                                      sizeof(ScatterSmem)) != cudaSuccess || per < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sort_onesweep_kernel<T>, T, sizeof(ScatterSmem<T>)) !=
+            cudaSuccess ||
+        per < 1)
       per = 1;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 148;
     cache[dev] = (unsigned)(per * sms);
@@ -370,10 +382,20 @@ static unsigned onesweep_resident() {
   return cache[dev];
 }
 
+// one digit pass with T-thread tiles
+template <int T>
+static void onesweep_pass(const uint64_t* src_k, const uint32_t* src_v, const uint8_t* ops, int mode, uint64_t* dst_k,
+                          uint32_t* dst_v, size_t n, const uint32_t* n_dev, int shift, const uint32_t* gbase,
+                          uint32_t* counter, uint32_t* status, uint32_t* err, uint32_t n_tiles, cudaStream_t s) {
+  const unsigned grid = min(n_tiles, onesweep_resident<T>());
+  sort_onesweep_kernel<T><<<grid, T, sizeof(ScatterSmem<T>), s>>>(src_k, src_v, ops, mode, dst_k, dst_v, n, n_dev,
+                                                                  shift, gbase, counter, status, err);
+}
+
 // scratch: hist[8][256] | tile counters[8] (+pad) | status[8][tiles][256]
-static_assert(kSortTileKeys == (size_t)kTile && kSortMaxPasses == (size_t)kMaxPasses &&
+static_assert(kSortTileKeys == (size_t)kMinTile && kSortMaxPasses == (size_t)kMaxPasses &&
                   kSortRadix == (size_t)kRadix,
-              "the scratch layout in bt_internal.h must match the sort");
+              "the scratch layout in bt_internal.h must match the sort (sized for the smallest tile)");
 
 size_t sort_scratch_words(size_t n) {
   const size_t w = sort_scratch_words_for(n);
@@ -389,7 +411,7 @@ size_t sort_scratch_words(size_t n) {
 cudaError_t radix_sort_pairs(const uint64_t* keys_in, const uint32_t* vals_in, const uint8_t* ops, uint64_t* k_a,
                              uint32_t* v_a, uint64_t* k_b, uint32_t* v_b, size_t n, int begin_bit, int end_bit,
                              uint32_t* scratch, cudaStream_t s, uint64_t** k_out, uint32_t** v_out, uint32_t* err,
-                             const uint32_t* n_dev) {
+                             const uint32_t* n_dev, int tile_threads) {
   *k_out = k_a;
   *v_out = v_a;
   if (n == 0) return cudaSuccess;
@@ -406,28 +428,36 @@ cudaError_t radix_sort_pairs(const uint64_t* keys_in, const uint32_t* vals_in, c
     return cudaGetLastError();
   }
   if (passes > kMaxPasses) return cudaErrorInvalidValue;
-  const uint32_t n_tiles = (uint32_t)sort_tiles(n);
+  const int T = tile_threads == 256 || tile_threads == 1024 ? tile_threads : 512;
+  const size_t tile = (size_t)T * kSortItems;
+  const uint32_t n_tiles = (uint32_t)((n + tile - 1) / tile);
   uint32_t* hist = scratch;
   uint32_t* counters = scratch + kMaxPasses * kRadix;
   uint32_t* status = counters + 64;
   cudaError_t e = cudaMemsetAsync(scratch, 0,
                                   ((size_t)kMaxPasses * kRadix + 64 + (size_t)passes * n_tiles * kRadix) * 4, s);
   if (e != cudaSuccess) return e;
-  unsigned hb = (unsigned)min((size_t)n_tiles, (size_t)1024);
+  unsigned hb = (unsigned)min((n + kSortThreads * kSortItems - 1) / (kSortThreads * kSortItems), (size_t)1024);
   sort_upfront_hist_kernel<<<hb, kSortThreads, 0, s>>>(keys_in, n, n_dev, begin_bit, passes, hist);
   count_launch();
   sort_digit_scan_kernel<<<1, kRadix, 0, s>>>(hist, passes);
   count_launch();
-  const unsigned grid = min(n_tiles, onesweep_resident());
   const uint64_t* src_k = keys_in;
   const uint32_t* src_v = vals_in;
   int mode = vals_in ? 0 : 1;
   uint64_t* dst_k = k_a;
   uint32_t* dst_v = v_a;
   for (int p = 0; p < passes; p++) {
-    sort_onesweep_kernel<<<grid, kSortThreads, sizeof(ScatterSmem), s>>>(
-        src_k, src_v, ops, mode, dst_k, dst_v, n, n_dev, begin_bit + 8 * p, hist + p * kRadix, counters + p,
-        status + (size_t)p * n_tiles * kRadix, err);
+    uint32_t* st = status + (size_t)p * n_tiles * kRadix;
+    if (T == 256)
+      onesweep_pass<256>(src_k, src_v, ops, mode, dst_k, dst_v, n, n_dev, begin_bit + 8 * p, hist + p * kRadix,
+                         counters + p, st, err, n_tiles, s);
+    else if (T == 1024)
+      onesweep_pass<1024>(src_k, src_v, ops, mode, dst_k, dst_v, n, n_dev, begin_bit + 8 * p, hist + p * kRadix,
+                          counters + p, st, err, n_tiles, s);
+    else
+      onesweep_pass<512>(src_k, src_v, ops, mode, dst_k, dst_v, n, n_dev, begin_bit + 8 * p, hist + p * kRadix,
+                         counters + p, st, err, n_tiles, s);
     count_launch();
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;

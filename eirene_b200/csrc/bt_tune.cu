@@ -1,10 +1,11 @@
-// Autotuner: times the candidate lookup configurations on the live tree with
-// a caller-supplied sample of keys and keeps the fastest.  Tuned: lanes per
-// request of the unsorted plain search, lanes per request and requests per
-// group of the unsorted learned lookup, the sorted search's leaf-value load,
-// and which descent serves the batch GET phase.  Lookups
-// only: the tree is not modified.  Node fanout (32, fixed by the node layout)
-// and the sort tile (4096) are compile-time constants.
+// Autotuner: times the candidate configurations on the live tree with a
+// caller-supplied sample of keys and keeps the fastest.  Tuned: lanes per
+// request of the unsorted plain search, lanes per request and the form of
+// the unsorted learned lookup, the sorted search's leaf-value load, which
+// descent serves the batch GET phase, and the radix sort's tile for whole
+// batches and for the hash front end's touched requests.  Lookups and sorts
+// only: the tree is not modified.  The node fill (fanout) is tuned on a
+// sample tree by bt_autotune_fill (bt_api.cu).
 #include <cuda_runtime.h>
 
 #include "bt_common.cuh"
@@ -32,7 +33,7 @@ static float time_ms(cudaStream_t s, F&& f, int reps = 3) {
 int autotune(Handle* h, const uint64_t* keys, size_t n, cudaStream_t s, double* rep) {
   Work& w = h->w;
   if (n == 0 || n > w.cap) return -6;
-  double out[16] = {};
+  double out[kTuneReport] = {};
   // unsorted plain search
   const int gs[4] = {4, 8, 16, 32};
   float best = 1e30f;
@@ -98,9 +99,32 @@ int autotune(Handle* h, const uint64_t* keys, size_t n, cudaStream_t s, double* 
   }
   h->batch_descent = desc;
   out[3] = desc;
+  // radix sort tile (threads x 8 items): on the whole sample (the full-sort
+  // front end sorts whole batches) and on a sixteenth of it (about the
+  // touched requests of a read-mostly batch under the hash front end)
+  const int tt[3] = {256, 512, 1024};
+  for (int pass = 0; pass < 2; pass++) {
+    const size_t m = pass == 0 ? n : (n / 16 ? n / 16 : 1);
+    float bt = 1e30f;
+    int best_t = 512;
+    for (int i = 0; i < 3; i++) {
+      const float ms = time_ms(s, [&] {
+        radix_sort_pairs(keys, nullptr, nullptr, w.k_a, w.v_a, w.k_b, w.v_b, m, 0, 64, w.sort_scratch, s, &sk, &sv,
+                         &h->tree.ctrl->error, nullptr, tt[i]);
+      });
+      out[18 + 3 * pass + i] = ms;
+      if (ms < bt) {
+        bt = ms;
+        best_t = tt[i];
+      }
+    }
+    if (pass == 0) h->sort_threads = best_t;
+    else h->sort_threads_touch = best_t;
+    out[16 + pass] = best_t;
+  }
   if (cudaStreamSynchronize(s) != cudaSuccess) return -2;
   if (rep)
-    for (int i = 0; i < 16; i++) rep[i] = out[i];
+    for (int i = 0; i < kTuneReport; i++) rep[i] = out[i];
   return 0;
 }
 

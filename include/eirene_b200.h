@@ -258,6 +258,9 @@ int bt_set_search_group(bt_handle *h, uint32_t lanes);
                                        * batch's writes from a page-locked value array over the bus instead of
                                        * copying the array (fewer bytes, but scattered reads; measured slower on
                                        * a 95/5 batch of 2^22); 0 (default) copies it */
+#define BT_OPT_SORT_TILE 14     /* radix sort tile of sorted batches: 256, 512 (default) or 1024 threads x 8 keys,
+                                 * for whole batches and for the hash front end's touched requests alike
+                                 * (bt_autotune picks the two separately) */
 #define BT_OPT_LEARNED_MODE 12 /* unsorted learned lookups: 1 one request per lane group, 2 two requests per
                                 * group in lock step, 3 (default) software-pipelined: a group carries up to five
                                 * requests, one in each round of loads (list entry, key, leaf-table probe, leaf
@@ -271,18 +274,34 @@ int bt_set_option(bt_handle *h, int option, int64_t value);
  * reference synchronises after every batch kernel, src/gpu-stm-tree-v38/
  * bpt-gpustm-kernel.cu:289-324). */
 int bt_sync(bt_handle *h, void *stream);
-/* Autotuner: times the lookup configurations on this tree with n sample keys
- * (device pointer, n <= max_batch) and keeps the fastest: lanes per request of
- * the plain search, lanes per request and requests per group of the learned
- * lookup, the sorted search's leaf-value load, and the descent used by the
- * batch GET phase.  Read-only; synchronous.
- * report (nullable, 16 doubles): [0] plain lanes, [1] learned lanes, [2] leaf
- * values mode, [3] batch descent, [4..7] plain ms for 4/8/16/32 lanes,
- * [8..11] learned ms for 4 lanes pipelined, 8 lanes pipelined, 4 lanes one
- * request, 4 lanes two requests, [12..13] sorted plain ms (mode 0/1), [14]
- * sorted learned ms, [15] learned mode (BT_OPT_LEARNED_MODE).  No reference counterpart (the reference's launch
+/* Autotuner: times the lookup and sort configurations on this tree with n
+ * sample keys (device pointer, n <= max_batch) and keeps the fastest: lanes
+ * per request of the plain search, lanes per request and form of the learned
+ * lookup, the sorted search's leaf-value load, the descent used by the batch
+ * GET phase, and the radix sort's tile (256, 512 or 1024 threads x 8 keys) for
+ * whole batches and for the hash front end's touched requests.  Read-only;
+ * synchronous.
+ * report (nullable, BT_AUTOTUNE_REPORT_LEN doubles): [0] plain lanes, [1]
+ * learned lanes, [2] leaf values mode, [3] batch descent, [4..7] plain ms for
+ * 4/8/16/32 lanes, [8..11] learned ms for 4 lanes pipelined, 8 lanes
+ * pipelined, 4 lanes one request, 4 lanes two requests, [12..13] sorted plain
+ * ms (mode 0/1), [14] sorted learned ms, [15] learned mode
+ * (BT_OPT_LEARNED_MODE), [16] sort tile threads (whole batch), [17] sort tile
+ * threads (touched requests), [18..20] whole-sample sort ms for 256/512/1024,
+ * [21..23] sixteenth-sample sort ms for 256/512/1024.  No reference counterpart (the reference's launch
  * shape is compile-time, src/gpu-stm-tree-v39/bpt-gpustm.h:25-38). */
+#define BT_AUTOTUNE_REPORT_LEN 24
 int bt_autotune(bt_handle *h, const uint64_t *sample_keys, size_t n, void *stream, double *report);
+/* Node-fill autotuner (the fanout the merge engine and the bulk loader pack
+ * to): builds a sample tree from the n sample keys (device pointer, n >= 64)
+ * in a temporary handle for each leaf/inner fill of 16, 20, 24 and 28 keys,
+ * times sorted 95/5 batches of n requests on it (merge engine), and keeps the
+ * fastest fill for this handle's later bulk builds and merge splits (the
+ * current leaves are not repacked).  Synchronous; allocates the temporary
+ * trees.  report (nullable, 8 doubles): [0] leaf fill, [1] inner fill, [2..5]
+ * ms per batch for fills 16/20/24/28.  The reference's fanout is the
+ * compile-time ORDER (src/gpu-stm-tree-v39/bpt-gpustm.h:21-31). */
+int bt_autotune_fill(bt_handle *h, const uint64_t *sample_keys, size_t n, void *stream, double *report);
 /* Learned predictor settings and diagnostics (no reference counterpart: the
  * reference has no learned model).
  * Lanes per request in the learned search kernel: 4, 8, 16 or 32 (default 4). */

@@ -141,6 +141,7 @@ def test_autotune_then_batches_stay_exact(gpu):
     rk, rv, ro = O.gen_requests("uniform", 22, keys, 100_000, 95)
     rep = t.autotune(dev(rk))
     assert rep["plain_lanes"] in (4, 8, 16, 32) and rep["learned_lanes"] in (4, 8) and rep["learned_mode"] in (1, 2, 3)
+    assert rep["sort_threads"] in (256, 512, 1024) and rep["sort_threads_touched"] in (256, 512, 1024)
     assert all(v > 0 for v in rep["plain_ms"].values())
     for desc in (0, 1, -1):
         t.set_option(E.OPT_BATCH_DESCENT, desc)

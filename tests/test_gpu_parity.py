@@ -208,3 +208,40 @@ def test_pool_exhaustion_reports_status(gpu):
     assert (np.diff(k.astype(np.float64)) > 0).all()
     ins = rk[st_all == E.ST_ABSENT]
     assert np.isin(k, ins).all() and k.size == ins.size
+
+
+@pytest.mark.parametrize("tile", [256, 512, 1024])
+@pytest.mark.parametrize("front", [1, 0])
+def test_sort_tiles_exact(gpu, tile, front):
+    # every radix sort tile (threads x 8 keys) gives the oracle's answers,
+    # through both front ends; batches large and skewed enough to span many
+    # tiles and repeat keys
+    t, o, keys = make_pair(150_000, dist="zipf", seed=41)
+    t.set_option(E.OPT_FRONT_END, front)
+    t.set_option(E.OPT_SORT_TILE, tile)
+    for b in range(2):
+        rk, rv, ro = O.gen_requests("zipf", 420 + b, keys, 90_000, [50, 80][b])
+        ov, os_ = o.execute_merged(rk, rv, ro)
+        gv, gs = run_batch(t, rk, rv, ro, E.MODE_SORTED)
+        assert (gs == os_).all() and (gv == ov).all(), (tile, front, b)
+    assert_same_contents(t, o)
+
+
+def test_autotune_fill_then_exact(gpu):
+    keys = O.gen_keys("uniform", 51, 200_000)
+    vals = O.value_of(keys)
+    t = E.BTree(max_keys=1 << 21, max_batch=1 << 18)
+    rep = t.autotune_fill(dev(keys[:100_000]))
+    f = rep["leaf_fill"]
+    assert f in (16, 20, 24, 28) and rep["inner_fill"] == f
+    assert all(v > 0 for v in rep["batch_ms"].values())
+    # later builds and splits use the chosen fill: the layout equals the oracle's at that fill
+    t.bulk_build(dev(keys), dev(vals))
+    o = O.OracleTree(f, f)
+    o.bulk_build(keys, vals)
+    assert (t.leaf_sizes() == o.leaf_sizes()).all()
+    rk, rv, ro = O.gen_requests("uniform", 52, keys, 60_000, 50)
+    ov, os_ = o.execute_merged(rk, rv, ro, engine=O.ENGINE_MERGE)
+    gv, gs = run_batch(t, rk, rv, ro, E.MODE_SORTED | E.MODE_MERGE_ENGINE)
+    assert (gs == os_).all() and (gv == ov).all()
+    assert (t.leaf_sizes() == o.leaf_sizes()).all()
