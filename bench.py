@@ -958,6 +958,8 @@ def main():
     # DRAM bytes per unit of the dominant kernel from an ncu capture, kept as a
     # "bytes_per_unit: N" line in profiles/traffic_<phase>.md
     tpath = os.path.join(ROOT, "profiles", f"traffic_{dom}.md")
+    if head == "learned" and dom == "search":  # the learned form's lookup kernel
+        tpath = os.path.join(ROOT, "profiles", "traffic_search_learned.md")
     if os.path.exists(tpath):
         try:
             import re
@@ -970,7 +972,16 @@ def main():
     roof = None
     if dom_bytes:
         ach = dom_bytes / (dom_ms / 1e3) / 1e9
-        roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+        kname = dom
+        if dom == "search":
+            tune = R.get("tune") or {}
+            if head == "learned":
+                m, g = tune.get("learned_mode", 3), tune.get("learned_lanes", 4)
+                kname = (f"search phase: learned_pipe_kernel<{g}> + search2_kernel over its misses" if m == 3 else
+                         f"search phase: learned_lookup_kernel<{g},{m}> + search2_kernel over its misses")
+            else:
+                kname = f"search phase: search2_kernel<{tune.get('plain_lanes', 4)},0,1>"
+        roof = {"kernel": kname, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                 "peak_source": peak_kind, "traffic": traffic, "alg_bytes_per_launch": dom_bytes,
                 "launch_ms": dom_ms}
 

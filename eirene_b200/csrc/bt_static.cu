@@ -9,7 +9,7 @@
 // takes its sort and compaction scratch from cudaMallocAsync; this variant
 // takes it from the file-scope device array below instead.
 //
-// The array is kStaticMaxKeys keys' worth of scratch (about 2.3 MB).  Every
+// The array is kStaticMaxKeys keys' worth of scratch (about 2.6 MB).  Every
 // GPU that loads this library holds it until the process exits.  All calls on
 // one device share it and it keeps whatever the last call left there, so calls
 // that overlap on the GPU (different streams, or different host threads) race

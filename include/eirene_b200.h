@@ -126,7 +126,7 @@ int bt_bulk_build(bt_handle *h, const uint64_t *keys, const uint64_t *vals, size
  * cudaMalloc at request time fails or fragments that pool, and latency-critical
  * threads, since cudaFree synchronises the whole device.  Same result as
  * bt_bulk_build.  Its scratch is a fixed device array inside the library
- * (about 2.3 MB, held on every GPU that loads the library until the process
+ * (about 2.6 MB, held on every GPU that loads the library until the process
  * exits), so n may be at most BT_STATIC_BUILD_MAX_KEYS, else
  * BT_ERR_STATIC_LIMIT.  All calls on a device share that array: calls that
  * overlap on the GPU race, so serialise them.  The first call on a device
