@@ -389,7 +389,7 @@ class BTree:
                 "batch_descent": "learned" if r[3] == 1 else "plain",
                 "learned_mode": int(r[15]),
                 "plain_ms": dict(zip([4, 8, 16, 32], r[4:8])),
-                "learned_ms": dict(zip(["4 pipelined", "8 pipelined", "4x1", "4x2"], r[8:12])),
+                "learned_ms": dict(zip(["4 pipelined", "2 pipelined", "4x1", "2x1"], r[8:12])),
                 "sorted_plain_ms": r[12:14], "sorted_learned_ms": r[14],
                 "sort_threads": int(r[16]), "sort_threads_touched": int(r[17]),
                 "sort_ms": dict(zip([256, 512, 1024], r[18:21])),

@@ -326,9 +326,9 @@ static int host_submit(bt_handle* H, const uint64_t* keys, const uint64_t* vals,
   int rc = hostpipe_init(h);
   if (rc != BT_OK) return rc;
   bt::HostPipe& p = h.hp;
-  bt::Staging& st = p.set[p.issued % 2];
-  // the set was used two batches ago: its answers must be out before its
-  // buffers are written again
+  bt::Staging& st = p.set[p.issued % bt::kStagingSets];
+  // the set was used kStagingSets batches ago: its answers must be out before
+  // its buffers are written again
   if (st.ticket && cudaEventSynchronize(st.done_ev) != cudaSuccess) return BT_ERR_CUDA;
   const auto H2D = cudaMemcpyHostToDevice;
   const auto D2H = cudaMemcpyDeviceToHost;
@@ -759,7 +759,7 @@ int bt_autotune_fill(bt_handle* H, const uint64_t* sample_keys, size_t n, void* 
 
 int bt_set_learned_group(bt_handle* H, uint32_t lanes) {
   if (!H) return BT_ERR_INVALID_ARG;
-  if (lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32) return BT_ERR_INVALID_ARG;
+  if (lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32) return BT_ERR_INVALID_ARG;
   H->h.learned_group = (int)lanes;
   return BT_OK;
 }

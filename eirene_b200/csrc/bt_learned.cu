@@ -1024,6 +1024,7 @@ cudaError_t launch_learned_lookup(Handle* h, const uint64_t* qkeys, const uint32
   (ckeys ? lookup_launch<GG, RR, true>(h, M, qkeys, list, n_dev, n, out_vals, out_st, s, ckeys) \
          : lookup_launch<GG, RR, false>(h, M, qkeys, list, n_dev, n, out_vals, out_st, s, nullptr))
   if (G == 8) e = R == 3 ? BT_LL(8, 0) : R == 2 ? BT_LL(8, 2) : BT_LL(8, 1);
+  else if (G == 2) e = R == 3 ? BT_LL(2, 0) : BT_LL(2, 1);
   else if (G == 16) e = R == 3 ? BT_LL(16, 0) : BT_LL(16, 1);
   else if (G == 32) e = BT_LL(32, 1);
   else e = R == 3 ? BT_LL(4, 0) : R == 2 ? BT_LL(4, 2) : BT_LL(4, 1);

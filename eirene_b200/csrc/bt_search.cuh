@@ -253,9 +253,11 @@ __device__ __forceinline__ void group_descend2(const DevTree& t, uint32_t node, 
       continue;
     }
     if (kChild) {
+      // interleaved 16-byte chunks (load_row_il): the lane counts below do
+      // not depend on which slots a lane holds, only the leaf's key pick does
       const uint64_t pol = level > 0 ? keep : stream;
-      load_slots_hint<S>(t.keys + ra, ka, pol);
-      load_slots_hint<S>(t.keys + rb, kb, pol);
+      load_row_il<G>(t.keys + (size_t)na * 32, g, ka, pol);
+      load_row_il<G>(t.keys + (size_t)nb * 32, g, kb, pol);
     } else {
       load_slots<S>(t.keys + ra, ka);
       load_slots<S>(t.keys + rb, kb);
@@ -289,8 +291,10 @@ __device__ __forceinline__ void group_descend2(const DevTree& t, uint32_t node, 
   }
   // leaf: find both slots, then issue both value loads together
   const uint32_t sa = ca > 0 ? ca - 1 : 0, sb = cb > 0 ? cb - 1 : 0;
-  const uint64_t kka = __shfl_sync(gmask, pick<S>(ka, sa % S), sa / S, G);
-  const uint64_t kkb = __shfl_sync(gmask, pick<S>(kb, sb % S), sb / S, G);
+  const uint64_t kka = kChild ? __shfl_sync(gmask, pick<S>(ka, il_elem<G>(sa)), il_lane<G>(sa), G)
+                              : __shfl_sync(gmask, pick<S>(ka, sa % S), sa / S, G);
+  const uint64_t kkb = kChild ? __shfl_sync(gmask, pick<S>(kb, il_elem<G>(sb)), il_lane<G>(sb), G)
+                              : __shfl_sync(gmask, pick<S>(kb, sb % S), sb / S, G);
   const bool fa = ca > 0 && kka == key_a, fb = cb > 0 && kkb == key_b;
   ans_a = 0;
   ans_b = 0;

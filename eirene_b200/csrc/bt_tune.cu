@@ -52,8 +52,8 @@ int autotune(Handle* h, const uint64_t* keys, size_t n, cudaStream_t s, double* 
   // unsorted learned lookup: lanes per request x requests per group
   float best_learned = 1e30f;
   if (h->L.valid) {
-    // (lanes, mode): pipelined 4 and 8 lanes, one request per 4 lanes, pairs of 4 lanes
-    const int lg[4][2] = {{4, 3}, {8, 3}, {4, 1}, {4, 2}};
+    // (lanes, mode): pipelined 4 and 2 lanes, one request per 4 and per 2 lanes
+    const int lg[4][2] = {{4, 3}, {2, 3}, {4, 1}, {2, 1}};
     int best_i = 0;
     for (int i = 0; i < 4; i++) {
       h->learned_group = lg[i][0];

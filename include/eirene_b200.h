@@ -283,8 +283,8 @@ int bt_sync(bt_handle *h, void *stream);
  * synchronous.
  * report (nullable, BT_AUTOTUNE_REPORT_LEN doubles): [0] plain lanes, [1]
  * learned lanes, [2] leaf values mode, [3] batch descent, [4..7] plain ms for
- * 4/8/16/32 lanes, [8..11] learned ms for 4 lanes pipelined, 8 lanes
- * pipelined, 4 lanes one request, 4 lanes two requests, [12..13] sorted plain
+ * 4/8/16/32 lanes, [8..11] learned ms for 4 lanes pipelined, 2 lanes
+ * pipelined, 4 lanes one request, 2 lanes one request, [12..13] sorted plain
  * ms (mode 0/1), [14] sorted learned ms, [15] learned mode
  * (BT_OPT_LEARNED_MODE), [16] sort tile threads (whole batch), [17] sort tile
  * threads (touched requests), [18..20] whole-sample sort ms for 256/512/1024,
@@ -304,7 +304,7 @@ int bt_autotune(bt_handle *h, const uint64_t *sample_keys, size_t n, void *strea
 int bt_autotune_fill(bt_handle *h, const uint64_t *sample_keys, size_t n, void *stream, double *report);
 /* Learned predictor settings and diagnostics (no reference counterpart: the
  * reference has no learned model).
- * Lanes per request in the learned search kernel: 4, 8, 16 or 32 (default 4). */
+ * Lanes per request in the learned search kernel: 2, 4, 8, 16 or 32 (default 4). */
 int bt_set_learned_group(bt_handle *h, uint32_t lanes);
 /* info[8]: valid, n_leaves, n_segments, segments over the window, window,
  * final training loss, root model (1 MLP, 0 linear), training steps */
