@@ -804,14 +804,30 @@ def main():
     fill = None
     if sharded is None and not args.no_fill_tune:
         fill = tree.autotune_fill(tk[: min(n_tree, 1 << 22)], stream)
+    def build_tree(tv):
+        if sharded is not None:
+            sharded.bulk_build(tk, tv)
+        else:
+            tree.bulk_build(tk, tv, stream)
+
     t0 = time.time()
-    if sharded is not None:
-        sharded.bulk_build(tk, tv)
-    else:
-        tree.bulk_build(tk, tv, stream)
+    build_tree(tv)
     torch.cuda.synchronize()
     build_s = time.time() - t0
     del tv
+    built = [True]  # the tree as bulk-built, no batch applied yet
+
+    def rebuild_tree():
+        # each form starts from the same freshly built tree: the batches of
+        # the form measured first must not grow the other form's tree
+        if built[0]:
+            return
+        tv = torch.empty(n_tree, dtype=torch.int64, device="cuda")
+        E.gen_keys(args.dist, 1 + rank, n_tree, tk, tv, stream)
+        build_tree(tv)
+        torch.cuda.synchronize()
+        del tv
+        built[0] = True
 
     # ---- batches: distinct, device resident (each step reads its own 2^22-request batch)
     def make_batches(seed0):
@@ -842,6 +858,8 @@ def main():
     check_out = {}
 
     def run_form(learned: bool, seed0: int):
+        rebuild_tree()
+        built[0] = False
         batches = make_batches(seed0)
         counts = [unique_op_counts(torch, k, o) for (k, v, o) in batches[args.warmup:]]
         info = None
@@ -924,6 +942,8 @@ def main():
         for form in ("plain", "learned"):
             if form == "learned" and "learned" not in forms:
                 continue
+            if form == "learned":
+                tree.refit(stream)  # the model follows the tree the batches grew
             tree.set_descent(form == "learned")
             for _ in range(3):
                 tree.search(rk, ov, ost, stream)
@@ -1001,6 +1021,7 @@ def main():
             pinned.append(b)
             return b.tensor
 
+        n_ins = []
         for i in range(1 + e2e_steps):
             k = torch.empty(n_b, dtype=torch.int64, device="cuda")
             v = torch.empty(n_b, dtype=torch.int64, device="cuda")
@@ -1011,17 +1032,22 @@ def main():
             hk.copy_(k)
             hv.copy_(v)
             ho.copy_(o)
-            hb.append((hk, hv, ho))
-        # two answer buffers: batch i + 1 is submitted before batch i is waited for
-        outs = [(host_buf(n_b, torch.int64), host_buf(n_b, torch.uint8)) for _ in range(2)]
-        sp = stream.cuda_stream
+            # the same batch with the INSERTs' values only, packed in request order
+            iv = v[o == E.OP_INSERT]
+            hiv = host_buf(max(iv.numel(), 1), torch.int64)[: iv.numel()]
+            hiv.copy_(iv)
+            n_ins.append(iv.numel())
+            hb.append((hk, hv, ho, hiv))
+        # three answer buffers: three batches in flight (the handle's three
+        # staging sets): batch s is submitted once batch s - 3 is answered
+        outs = [(host_buf(n_b, torch.int64), host_buf(n_b, torch.uint8)) for _ in range(3)]
 
         dk = torch.empty(n_b, dtype=torch.int64, device="cuda")
         dv = torch.empty(n_b, dtype=torch.int64, device="cuda")
         do = torch.empty(n_b, dtype=torch.uint8, device="cuda")
 
-        def host_submit(b, out):
-            k, v, o = b
+        def host_submit(b, out, packed):
+            k, v, o, iv = b
             hov, hos = out
             if sharded is not None:
                 # host batch in, host answers out, through the sharded tree
@@ -1032,43 +1058,58 @@ def main():
                 hov.copy_(ov, non_blocking=True)
                 hos.copy_(ost, non_blocking=True)
                 return None
-            # bt_execute_batch_host_async: two batches in flight, the next
-            # batch's copy-in and this batch's copy-out beside the kernels
-            return tree.submit_host(k, v, o, hov, hos, mode=MODE, stream=stream)
+            # three batches in flight: the next batch's copy-in and the
+            # previous batch's copy-out beside this batch's kernels
+            if packed:  # bt_execute_batch_host_packed_async
+                return tree.submit_host_packed(k, o, iv, hov, hos, mode=MODE, stream=stream)
+            return tree.submit_host(k, v, o, hov, hos, mode=MODE, stream=stream)  # bt_execute_batch_host_async
 
         def host_wait(t):
             if t is not None:
                 tree.wait_host(t)
 
-        for _ in range(3):
-            host_wait(host_submit(hb[0], outs[0]))
-        barrier()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        w0 = time.perf_counter()
-        e0.record(stream)
-        prev = None
-        for s in range(e2e_steps):
-            t = host_submit(hb[1 + s], outs[s % 2])
-            host_wait(prev)
-            prev = t
-        host_wait(prev)
-        tree.sync(stream)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        wall_ms = (time.perf_counter() - w0) * 1e3
-        barrier()
-        e2e_ms = allmax(e0.elapsed_time(e1))
+        def timed(packed):
+            for _ in range(3):
+                host_wait(host_submit(hb[0], outs[0], packed))
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            w0 = time.perf_counter()
+            e0.record(stream)
+            tickets = []
+            for s in range(e2e_steps):
+                if s >= 3:
+                    host_wait(tickets[s - 3])
+                tickets.append(host_submit(hb[1 + s], outs[s % 3], packed))
+            for t in tickets[-3:]:
+                host_wait(t)
+            tree.sync(stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            wall_ms = (time.perf_counter() - w0) * 1e3
+            barrier()
+            return allmax(e0.elapsed_time(e1)), wall_ms
+
+        packed = sharded is None
+        full_ms, full_wall = timed(False)
+        e2e_ms, wall_ms = timed(True) if packed else (full_ms, full_wall)
         del hb, outs
         for b in pinned:
             b.free()
-        # bytes over the bus per step: keys, values and op codes copied in,
-        # values and status bytes copied out
+        # bytes over the bus per step: keys and op codes copied in with the
+        # INSERTs' values (packed) or every request's value slot; values and
+        # status bytes copied out
+        ins_per_step = sum(n_ins[1:]) / e2e_steps
         e2e = {"value": world * n_b * e2e_steps / (e2e_ms / 1e3) / 1e6, "unit": "Mops/s",
-               "h2d_bytes_per_step": n_b * 17,
+               "h2d_bytes_per_step": int(n_b * 9 + 8 * ins_per_step) if packed else n_b * 17,
                "d2h_bytes_per_step": n_b * 9,
                "host_wall_ms_per_step": wall_ms / e2e_steps,
                "pipelined": sharded is None,
-               "steps": e2e_steps, "descent": head}
+               "entry_point": "bt_execute_batch_host_packed_async" if packed else "sharded execute",
+               "steps": e2e_steps, "descent": head,
+               "full_values": {"value": world * n_b * e2e_steps / (full_ms / 1e3) / 1e6,
+                               "entry_point": "bt_execute_batch_host_async",
+                               "h2d_bytes_per_step": n_b * 17, "d2h_bytes_per_step": n_b * 9,
+                               "host_wall_ms_per_step": full_wall / e2e_steps}}
 
     serving = {}
     if not args.no_serve and sharded is None:

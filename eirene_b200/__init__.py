@@ -103,6 +103,7 @@ EXPORTS = [
     "bt_serve_config_init", "bt_serve_start", "bt_submit", "bt_poll", "bt_wait", "bt_serve_get_stats", "bt_serve_stop",
     "bt_route_batch", "bt_unroute_results", "bt_save", "bt_load", "bt_range_batch", "bt_sync", "bt_save_image", "bt_load_image",
     "bt_refit", "bt_execute_batch_host_async", "bt_host_wait", "bt_serve_batch_times", "bt_autotune_fill",
+    "bt_execute_batch_host_packed_async",
 ]
 MAX_SHARDS = 256
 OPT_SORTED_SEARCH, OPT_RETRY_LIMIT, OPT_TRAIN_STEPS, OPT_SORTED_LEAF_VALS, OPT_BATCH_DESCENT = 1, 2, 3, 4, 5
@@ -155,6 +156,8 @@ def lib():
             "bt_refit": [_P, _P],
             "bt_execute_batch_host_async": [_P, _P, _P, _P, _P, _P, _SZ, ctypes.c_int, _P,
                                             ctypes.POINTER(ctypes.c_uint64)],
+            "bt_execute_batch_host_packed_async": [_P, _P, _P, _P, _SZ, _P, _P, _SZ, ctypes.c_int, _P,
+                                                   ctypes.POINTER(ctypes.c_uint64)],
             "bt_host_wait": [_P, ctypes.c_uint64],
             "bt_serve_batch_times": [_P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64),
                                      ctypes.POINTER(ctypes.c_uint64)],
@@ -306,6 +309,23 @@ class BTree:
         _check(lib().bt_execute_batch_host_async(self._h, addr(keys), addr(vals), addr(ops), addr(out_vals),
                                                  addr(out_status), n, mode, _stream_ptr(stream), ctypes.byref(t)),
                "bt_execute_batch_host_async")
+        return t.value
+
+    def submit_host_packed(self, keys, ops, insert_vals, out_vals, out_status, mode=MODE_SORTED,
+                           stream=None) -> int:
+        """bt_execute_batch_host_packed_async: like submit_host, with the values
+        of the batch's INSERTs only (insert_vals[j] belongs to the j-th INSERT
+        in request order); returns the ticket."""
+        def addr(a):
+            return a.data_ptr() if hasattr(a, "data_ptr") else a.ctypes.data
+
+        n = keys.numel() if hasattr(keys, "numel") else keys.size
+        m = insert_vals.numel() if hasattr(insert_vals, "numel") else insert_vals.size
+        t = ctypes.c_uint64(0)
+        _check(lib().bt_execute_batch_host_packed_async(self._h, addr(keys), addr(ops), addr(insert_vals) if m else None,
+                                                        m, addr(out_vals), addr(out_status), n, mode,
+                                                        _stream_ptr(stream), ctypes.byref(t)),
+               "bt_execute_batch_host_packed_async")
         return t.value
 
     def wait_host(self, ticket: int):

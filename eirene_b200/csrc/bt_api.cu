@@ -266,8 +266,8 @@ int bt_execute_batch(bt_handle* H, const uint64_t* keys, const uint64_t* vals, c
 // page-locked, not copied at all: the merge passes read the values of the
 // batch's writes over the bus; the batch's kernels on the caller's stream;
 // the answers copied out on the copy-out stream as soon as they are final,
-// while the leaf merge still runs.  Two staging sets let the next batch's
-// copy-in and this batch's copy-out run beside the kernels of the other.
+// while the leaf merge still runs.  Three staging sets let the next batch's
+// copy-in and the previous batch's copy-out run beside this batch's kernels.
 
 static void hostpipe_free(bt::HostPipe& p) {
   for (bt::Staging& st : p.set) {
@@ -276,6 +276,9 @@ static void hostpipe_free(bt::HostPipe& p) {
     cudaFree(st.ops);
     cudaFree(st.out_vals);
     cudaFree(st.out_st);
+    cudaFree(st.packed);
+    cudaFree(st.pack_scratch);
+    if (st.pack_err) cudaFreeHost(st.pack_err);
     for (cudaEvent_t e : {st.in_ev, st.vals_ev, st.ans_ev, st.done_ev})
       if (e) cudaEventDestroy(e);
     st = bt::Staging{};
@@ -289,7 +292,11 @@ static int hostpipe_init(bt::Handle& h) {
   bt::HostPipe& p = h.hp;
   if (p.cap) return BT_OK;
   const size_t cap = h.w.cap;
-  bool ok = cudaStreamCreateWithFlags(&p.in_stream, cudaStreamNonBlocking) == cudaSuccess &&
+  // the copy-in stream at the highest priority: its small kernels (the
+  // packed values' count and placement) go ahead of the running batch's blocks
+  int lo_prio = 0, hi_prio = 0;
+  cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio);
+  bool ok = cudaStreamCreateWithPriority(&p.in_stream, cudaStreamNonBlocking, hi_prio) == cudaSuccess &&
             cudaStreamCreateWithFlags(&p.out_stream, cudaStreamNonBlocking) == cudaSuccess;
   for (bt::Staging& st : p.set) {
     ok = ok && cudaMalloc(&st.keys, cap * 8) == cudaSuccess && cudaMalloc(&st.vals, cap * 8) == cudaSuccess &&
@@ -317,9 +324,15 @@ static const uint64_t* mapped_alias(const uint64_t* p) {
   return a.type == cudaMemoryTypeHost && a.devicePointer ? static_cast<const uint64_t*>(a.devicePointer) : nullptr;
 }
 
-static int host_submit(bt_handle* H, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops,
-                       uint64_t* out_vals, uint8_t* out_status, size_t n, int mode, cudaStream_t s,
-                       uint64_t* ticket) {
+// packed: `vals` holds the values of the batch's INSERTs only, n_packed of
+// them in request order; otherwise one value per request.  The count is
+// checked on the device, between the op codes' copy and the front end: a
+// mismatch turns the batch into one whose every request is rejected, and
+// bt_host_wait reports it (a count on the host cost 0.35 ms of the host
+// thread per 2^22 requests, more than the copy it saved)
+static int host_submit(bt_handle* H, const uint64_t* keys, const uint64_t* vals, size_t n_packed, bool packed,
+                       const uint8_t* ops, uint64_t* out_vals, uint8_t* out_status, size_t n, int mode,
+                       cudaStream_t s, uint64_t* ticket) {
   bt::Handle& h = H->h;
   const int base = mode & 0xF;
   if (base != BT_MODE_SORTED && base != BT_MODE_STM) return BT_ERR_INVALID_ARG;
@@ -330,19 +343,45 @@ static int host_submit(bt_handle* H, const uint64_t* keys, const uint64_t* vals,
   // the set was used kStagingSets batches ago: its answers must be out before
   // its buffers are written again
   if (st.ticket && cudaEventSynchronize(st.done_ev) != cudaSuccess) return BT_ERR_CUDA;
+  if (st.ticket && st.packed_batch && *st.pack_err) {
+    if (p.refused.size() >= 1024) p.refused.erase(p.refused.begin());  // the oldest are forgotten
+    p.refused.push_back(st.ticket);
+  }
+  st.packed_batch = false;
+  if (packed && !st.packed) {
+    if (cudaMalloc(&st.packed, p.cap * 8) != cudaSuccess ||
+        cudaMalloc(&st.pack_scratch, bt::pack_scratch_words(p.cap) * 4) != cudaSuccess ||
+        cudaMallocHost(&st.pack_err, 4) != cudaSuccess) {
+      cudaFree(st.packed);
+      cudaFree(st.pack_scratch);
+      st.packed = nullptr;
+      st.pack_scratch = nullptr;
+      st.pack_err = nullptr;
+      return BT_ERR_NO_MEMORY;
+    }
+  }
   const auto H2D = cudaMemcpyHostToDevice;
   const auto D2H = cudaMemcpyDeviceToHost;
   // values read in place only when asked for: the merge passes' scattered
   // 8-byte reads over the bus cost more than copying the whole array, which
   // the copy-in stream overlaps with the previous batch's kernels
-  const uint64_t* remote = (base == BT_MODE_SORTED && h.host_vals_in_place) ? mapped_alias(vals) : nullptr;
+  const uint64_t* remote =
+      (!packed && base == BT_MODE_SORTED && h.host_vals_in_place) ? mapped_alias(vals) : nullptr;
   cudaStream_t in = p.in_stream;
   if (cudaMemcpyAsync(st.ops, ops, n, H2D, in) != cudaSuccess ||
+      (packed && bt::pack_check(st.ops, n, n_packed, st.pack_scratch, p.cap, h.sm_count, in) != cudaSuccess) ||
       cudaMemcpyAsync(st.keys, keys, n * 8, H2D, in) != cudaSuccess || cudaEventRecord(st.in_ev, in) != cudaSuccess)
     return BT_ERR_CUDA;
-  if (!remote && (cudaMemcpyAsync(st.vals, vals, n * 8, H2D, in) != cudaSuccess ||
-                  cudaEventRecord(st.vals_ev, in) != cudaSuccess))
+  if (packed) {
+    // the INSERTs' values in, then each to its request's slot of st.vals
+    if ((n_packed && cudaMemcpyAsync(st.packed, vals, n_packed * 8, H2D, in) != cudaSuccess) ||
+        bt::pack_expand(st.ops, n, st.packed, n_packed, st.vals, st.pack_scratch, p.cap, in) != cudaSuccess ||
+        cudaEventRecord(st.vals_ev, in) != cudaSuccess)
+      return BT_ERR_CUDA;
+  } else if (!remote && (cudaMemcpyAsync(st.vals, vals, n * 8, H2D, in) != cudaSuccess ||
+                         cudaEventRecord(st.vals_ev, in) != cudaSuccess)) {
     return BT_ERR_CUDA;
+  }
   if (cudaStreamWaitEvent(s, st.in_ev, 0) != cudaSuccess) return BT_ERR_CUDA;
   if (base == BT_MODE_SORTED) {
     h.vals_wait = remote ? nullptr : st.vals_ev;
@@ -368,19 +407,30 @@ static int host_submit(bt_handle* H, const uint64_t* keys, const uint64_t* vals,
   if (cudaStreamWaitEvent(out, st.ans_ev, 0) != cudaSuccess ||
       cudaMemcpyAsync(out_vals, st.out_vals, n * 8, D2H, out) != cudaSuccess ||
       cudaMemcpyAsync(out_status, st.out_st, n, D2H, out) != cudaSuccess ||
+      (packed && cudaMemcpyAsync(st.pack_err, bt::pack_error_word(st.pack_scratch, p.cap), 4, D2H, out) !=
+                     cudaSuccess) ||
       cudaEventRecord(st.done_ev, out) != cudaSuccess)
     return BT_ERR_CUDA;
+  st.packed_batch = packed;
   st.ticket = ++p.issued;
   if (ticket) *ticket = st.ticket;
   return BT_OK;
 }
 
+// BT_ERR_INVALID_ARG for a packed batch whose value count did not match its
+// INSERTs (every request answered kRejected, nothing applied)
 static int host_wait(bt::Handle& h, uint64_t ticket) {
-  const bt::HostPipe& p = h.hp;
+  bt::HostPipe& p = h.hp;
   if (ticket == 0 || ticket > p.issued) return BT_ERR_INVALID_ARG;
-  for (const bt::Staging& st : p.set)
-    if (st.ticket == ticket) return cudaEventSynchronize(st.done_ev) == cudaSuccess ? BT_OK : BT_ERR_CUDA;
-  return BT_OK;  // an older batch: its set has been reused, so it has finished
+  for (bt::Staging& st : p.set)
+    if (st.ticket == ticket) {
+      if (cudaEventSynchronize(st.done_ev) != cudaSuccess) return BT_ERR_CUDA;
+      return st.packed_batch && *st.pack_err ? BT_ERR_INVALID_ARG : BT_OK;
+    }
+  // an older batch: its set has been reused, so it has finished
+  for (uint64_t t : p.refused)
+    if (t == ticket) return BT_ERR_INVALID_ARG;
+  return BT_OK;
 }
 
 int bt_execute_batch_host_async(bt_handle* H, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops,
@@ -392,7 +442,19 @@ int bt_execute_batch_host_async(bt_handle* H, const uint64_t* keys, const uint64
   if (!keys || !ops || !out_vals || !out_status || !vals) return BT_ERR_INVALID_ARG;
   if (n > H->h.w.cap) return BT_ERR_BATCH_TOO_LARGE;
   DeviceGuard g(H->h.device);
-  return host_submit(H, keys, vals, ops, out_vals, out_status, n, mode, S(stream), ticket);
+  return host_submit(H, keys, vals, 0, false, ops, out_vals, out_status, n, mode, S(stream), ticket);
+}
+
+int bt_execute_batch_host_packed_async(bt_handle* H, const uint64_t* keys, const uint8_t* ops,
+                                       const uint64_t* insert_vals, size_t n_inserts, uint64_t* out_vals,
+                                       uint8_t* out_status, size_t n, int mode, void* stream, uint64_t* ticket) {
+  if (!H || !ticket) return BT_ERR_INVALID_ARG;
+  *ticket = 0;
+  if (n == 0) return n_inserts == 0 ? BT_OK : BT_ERR_INVALID_ARG;
+  if (!keys || !ops || !out_vals || !out_status || (n_inserts && !insert_vals)) return BT_ERR_INVALID_ARG;
+  if (n > H->h.w.cap) return BT_ERR_BATCH_TOO_LARGE;
+  DeviceGuard g(H->h.device);
+  return host_submit(H, keys, insert_vals, n_inserts, true, ops, out_vals, out_status, n, mode, S(stream), ticket);
 }
 
 int bt_host_wait(bt_handle* H, uint64_t ticket) {
@@ -410,7 +472,7 @@ int bt_execute_batch_host(bt_handle* H, const uint64_t* keys, const uint64_t* va
   if (n > H->h.w.cap) return BT_ERR_BATCH_TOO_LARGE;
   DeviceGuard g(H->h.device);
   uint64_t t = 0;
-  int rc = host_submit(H, keys, vals, ops, out_vals, out_status, n, mode, S(stream), &t);
+  int rc = host_submit(H, keys, vals, 0, false, ops, out_vals, out_status, n, mode, S(stream), &t);
   if (rc != BT_OK) return rc;
   rc = host_wait(H->h, t);
   if (rc != BT_OK) return rc;

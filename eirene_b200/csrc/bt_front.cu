@@ -319,7 +319,129 @@ __global__ void __launch_bounds__(kTileThreads) front_scatter_kernel(const uint6
   }
 }
 
+// Packed INSERT values (bt_execute_batch_host_packed_async): the caller sends
+// the values of the batch's INSERTs only, in request order.  Value j belongs
+// to the j-th INSERT; two launches around a scan of the per-tile INSERT
+// counts put it at that request's slot, so the batch reads vals[r] as usual.
+// HBM traffic per request: 2 B of op codes (read twice), plus 16 B per INSERT.
+__device__ __forceinline__ uint32_t tile_ballot(const uint8_t* __restrict__ ops, size_t n, size_t i) {
+  return __ballot_sync(0xffffffffu, i < n && ops[i] == kOpInsert);
+}
+
+__global__ void __launch_bounds__(kTileThreads) pack_count_kernel(const uint8_t* __restrict__ ops, size_t n,
+                                                                  uint32_t* __restrict__ tile_cnt) {
+  __shared__ uint32_t wsum[kTileWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const size_t base = (size_t)blockIdx.x * kTile;
+  uint32_t c = 0;
+#pragma unroll
+  for (int j = 0; j < kTileItems; j++) c += __popc(tile_ballot(ops, n, base + (size_t)j * kTileThreads + threadIdx.x));
+  if (lane == 0) wsum[warp] = c;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t v = lane < kTileWarps ? wsum[lane] : 0u;
+    v = __reduce_add_sync(0xffffffffu, v);
+    if (lane == 0) tile_cnt[blockIdx.x] = v;
+  }
+}
+
+__global__ void __launch_bounds__(kTileThreads) pack_expand_kernel(const uint8_t* __restrict__ ops, size_t n,
+                                                                   const uint32_t* __restrict__ tile_off,
+                                                                   const uint64_t* __restrict__ packed,
+                                                                   size_t n_packed, uint64_t* __restrict__ vals) {
+  __shared__ uint32_t cnt[kTileItems][kTileWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t lt = (1u << lane) - 1u;
+  const size_t base = (size_t)blockIdx.x * kTile;
+  uint32_t bal[kTileItems];
+#pragma unroll
+  for (int j = 0; j < kTileItems; j++) {
+    bal[j] = tile_ballot(ops, n, base + (size_t)j * kTileThreads + threadIdx.x);
+    if (lane == 0) cnt[j][warp] = __popc(bal[j]);
+  }
+  __syncthreads();
+  // exclusive prefix over (item, warp) in index order
+  if (warp == 0) {
+    uint32_t carry = 0;
+#pragma unroll
+    for (int j = 0; j < kTileItems; j++) {
+      const uint32_t c = lane < kTileWarps ? cnt[j][lane] : 0u;
+      uint32_t incl = c;
+#pragma unroll
+      for (int o = 1; o < kTileWarps; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      if (lane < kTileWarps) cnt[j][lane] = carry + incl - c;
+      carry += __shfl_sync(0xffffffffu, incl, kTileWarps - 1);
+    }
+  }
+  __syncthreads();
+  const size_t excl = tile_off[blockIdx.x];
+#pragma unroll
+  for (int j = 0; j < kTileItems; j++) {
+    if ((bal[j] >> lane) & 1u) {
+      const size_t p = excl + cnt[j][warp] + __popc(bal[j] & lt);  // INSERTs before this one
+      // the host checked the count; the bound keeps a wrong one inside the buffer
+      vals[base + (size_t)j * kTileThreads + threadIdx.x] = p < n_packed ? packed[p] : 0;
+    }
+  }
+}
+
+// A count of packed values that differs from the batch's INSERTs: every op
+// code becomes invalid, so every request is answered kRejected and nothing
+// is applied (the front end reads the op codes after this kernel)
+__global__ void __launch_bounds__(kThreads) pack_check_kernel(const uint32_t* __restrict__ total, size_t n_packed,
+                                                              uint8_t* __restrict__ ops, size_t n,
+                                                              uint32_t* __restrict__ err) {
+  const bool bad = (size_t)*total != n_packed;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *err = bad ? 1u : 0u;
+  if (!bad) return;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    ops[i] = 0xFF;
+}
+
 }  // namespace
+
+// scratch: tile counts, tile offsets, the INSERT total, the mismatch flag,
+// then the scan's own words
+size_t pack_scratch_words(size_t n) {
+  const size_t tiles = (n + kTile - 1) / kTile;
+  return 2 * (tiles + 1) + 2 + scan_scratch_words(tiles);
+}
+
+uint32_t* pack_error_word(uint32_t* scratch, size_t n_cap) {
+  const size_t tiles = (n_cap + kTile - 1) / kTile;
+  return scratch + 2 * (tiles + 1) + 1;
+}
+
+cudaError_t pack_check(uint8_t* ops, size_t n, size_t n_packed, uint32_t* scratch, size_t n_cap, int sm_count,
+                       cudaStream_t s) {
+  const size_t tiles = (n + kTile - 1) / kTile;
+  const size_t cap_tiles = (n_cap + kTile - 1) / kTile;
+  uint32_t* cnt = scratch;
+  uint32_t* off = cnt + cap_tiles + 1;
+  uint32_t* total = off + cap_tiles + 1;
+  uint32_t* scan = total + 2;
+  pack_count_kernel<<<(unsigned)tiles, kTileThreads, 0, s>>>(ops, n, cnt);
+  count_launch();
+  cudaError_t e = scan_exclusive_u32(cnt, off, tiles, total, scan, s);
+  if (e != cudaSuccess) return e;
+  pack_check_kernel<<<(unsigned)sm_count * 2, kThreads, 0, s>>>(total, n_packed, ops, n, total + 1);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t pack_expand(const uint8_t* ops, size_t n, const uint64_t* packed, size_t n_packed, uint64_t* vals,
+                        const uint32_t* scratch, size_t n_cap, cudaStream_t s) {
+  if (n == 0 || n_packed == 0) return cudaSuccess;
+  const size_t tiles = (n + kTile - 1) / kTile;
+  const size_t cap_tiles = (n_cap + kTile - 1) / kTile;
+  pack_expand_kernel<<<(unsigned)tiles, kTileThreads, 0, s>>>(ops, n, scratch + cap_tiles + 1, packed, n_packed,
+                                                              vals);
+  count_launch();
+  return cudaGetLastError();
+}
 
 // Fills w.f_tk/w.f_tv (touched requests, input order, count counts->n_touch)
 // and w.f_list/w.f_lk (plain lookups and their keys, input order, count

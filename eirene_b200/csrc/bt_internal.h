@@ -124,18 +124,21 @@ struct Work {
 };
 
 // ---- host-buffer entry points (bt_api.cu) ----
-// Two staging sets: while one batch's answers are copied out and the next
-// batch's inputs are copied in, the kernels of the batch between them run.
-// A 2^22-request batch at 95/5 is then bound by its 71 MB copy-in over PCIe
-// (1.40 ms for the copies alone, 1.48 ms per pipelined batch); a third set
-// was measured and changed nothing.
-constexpr int kStagingSets = 2;
+// Three staging sets: batch i + 1's inputs are copied in and batch i - 1's
+// answers copied out while batch i's kernels run.  With two, batch i + 1
+// could be submitted only once batch i - 1's answers were out, so its copy-in
+// started late in batch i's kernels and the GPU waited for it.
+constexpr int kStagingSets = 3;
 struct Staging {
   uint64_t* keys = nullptr;
   uint64_t* vals = nullptr;
   uint8_t* ops = nullptr;
   uint64_t* out_vals = nullptr;
   uint8_t* out_st = nullptr;
+  uint64_t* packed = nullptr;  // packed INSERT values (allocated at the first packed batch)
+  uint32_t* pack_scratch = nullptr;
+  uint32_t* pack_err = nullptr;  // page-locked copy of the batch's count-mismatch flag
+  bool packed_batch = false;     // the set's batch came with packed values
   cudaEvent_t in_ev = nullptr;    // keys and op codes are on the device
   cudaEvent_t vals_ev = nullptr;  // values are on the device
   cudaEvent_t ans_ev = nullptr;   // every answer is final in out_vals / out_st
@@ -147,6 +150,7 @@ struct HostPipe {
   Staging set[kStagingSets];
   cudaStream_t in_stream = nullptr, out_stream = nullptr;
   uint64_t issued = 0;  // tickets handed out so far
+  std::vector<uint64_t> refused;  // packed batches whose value count did not match (answered kRejected)
 };
 
 // ---- learned leaf predictor state (bt_learned.cu) ----
@@ -347,6 +351,19 @@ int delete_apply(Handle* h, size_t n_upper, cudaStream_t s);
 
 // ---- hash front end of the sorted batch (bt_front.cu) ----
 int front_classify(Handle* h, const uint64_t* keys, const uint8_t* ops, size_t n, cudaStream_t s);
+// packed INSERT values (scratch sized by pack_scratch_words(n_cap), n <= n_cap):
+// pack_check counts the INSERTs of ops per tile and, when their total is not
+// n_packed, raises the word at pack_error_word and makes every op code
+// invalid (the batch is then answered kRejected and applies nothing);
+// pack_expand then puts packed[j], the value of the j-th INSERT in request
+// order, at vals[r] of that INSERT's request r (other slots untouched:
+// nothing reads them)
+size_t pack_scratch_words(size_t n_cap);
+uint32_t* pack_error_word(uint32_t* scratch, size_t n_cap);
+cudaError_t pack_check(uint8_t* ops, size_t n, size_t n_packed, uint32_t* scratch, size_t n_cap, int sm_count,
+                       cudaStream_t s);
+cudaError_t pack_expand(const uint8_t* ops, size_t n, const uint64_t* packed, size_t n_packed, uint64_t* vals,
+                        const uint32_t* scratch, size_t n_cap, cudaStream_t s);
 
 // ---- key-range sharding (bt_shard.cu) ----
 int route_batch(Handle* h, const uint64_t* splitters, int n_shards, const uint64_t* keys, const uint64_t* vals,

@@ -851,8 +851,12 @@ cudaError_t launch_range(Handle* h, const uint64_t* lo, const uint64_t* hi, size
   return cudaGetLastError();
 }
 
+// grown with a quarter of headroom: the tree grows a little with every batch,
+// and a reallocation (cudaFree synchronises the device) on every refit or
+// dump stalled the batches queued behind it
 static int ensure_enum(Handle* h, size_t n) {
   if (n <= h->enum_cap) return 0;
+  n += n / 4 + 4096;
   cudaFree(h->enum_a);
   cudaFree(h->enum_b);
   cudaFree(h->enum_cnt);

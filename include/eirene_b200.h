@@ -155,9 +155,10 @@ int bt_execute_batch(bt_handle *h, const uint64_t *keys, const uint64_t *vals, c
 int bt_execute_batch_host(bt_handle *h, const uint64_t *keys, const uint64_t *vals, const uint8_t *ops,
                           uint64_t *out_vals, uint8_t *out_status, size_t n, int mode, void *stream);
 /* The same, asynchronous: queues the batch and returns a ticket (> 0; 0 for an
- * empty batch) that bt_host_wait redeems.  The handle keeps two staging sets,
- * so a caller that submits batch i + 1 before waiting for batch i gets batch
- * i + 1's copy-in and batch i's copy-out beside the kernels; a third submit
+ * empty batch) that bt_host_wait redeems.  The handle keeps three staging
+ * sets: a caller that keeps three batches in flight (submits batch i, then
+ * waits for batch i - 2) gets the next batch's copy-in and the previous
+ * batch's copy-out beside each batch's kernels; a fourth batch in flight
  * waits (on the host) until the first batch's answers are out.  Until its
  * ticket is redeemed, a batch's input buffers must stay unchanged and its
  * output buffers untouched.  Batches run in submission order, on `stream`.
@@ -166,6 +167,21 @@ int bt_execute_batch_host(bt_handle *h, const uint64_t *keys, const uint64_t *va
 int bt_execute_batch_host_async(bt_handle *h, const uint64_t *keys, const uint64_t *vals, const uint8_t *ops,
                                 uint64_t *out_vals, uint8_t *out_status, size_t n, int mode, void *stream,
                                 uint64_t *ticket);
+/* The same with the values of the batch's INSERTs only: insert_vals[j] is the
+ * value of the j-th INSERT request in request order, n_inserts of them (GET
+ * and DELETE requests carry no value).  A read-mostly batch then copies 9 B
+ * per request in (op code and key) plus 8 B per INSERT, instead of 17 B per
+ * request.  n_inserts is checked against the op codes on the device, before
+ * the batch's first kernel: on a mismatch every request of the batch is
+ * answered BT_ST_REJECTED, nothing is applied, and bt_host_wait returns
+ * BT_ERR_INVALID_ARG for its ticket (for the last 1024 such batches).  The
+ * ticket is redeemed by bt_host_wait; the same staging sets, ordering and
+ * buffer rules as bt_execute_batch_host_async.  No reference counterpart: the
+ * reference copies a value slot for every request
+ * (src/gpu-stm-tree-v39/bpt-gpustm.cpp:67-132). */
+int bt_execute_batch_host_packed_async(bt_handle *h, const uint64_t *keys, const uint8_t *ops,
+                                       const uint64_t *insert_vals, size_t n_inserts, uint64_t *out_vals,
+                                       uint8_t *out_status, size_t n, int mode, void *stream, uint64_t *ticket);
 /* Blocks until the batch of `ticket` has its answers in host memory
  * (its deferred leaf merge may still run; bt_sync orders after that). */
 int bt_host_wait(bt_handle *h, uint64_t ticket);

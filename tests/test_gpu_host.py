@@ -127,8 +127,8 @@ def test_merge_engine_pool_exhaustion(gpu, host):
 @pytest.mark.parametrize("pinned,in_place", [(True, 0), (True, 1), (False, 0), (False, 1)])
 @pytest.mark.parametrize("mode", [MERGE, E.MODE_SORTED, E.MODE_STM])
 def test_async_host_batches_in_flight(gpu, pinned, in_place, mode):
-    # bt_execute_batch_host_async: up to three batches queued before the
-    # first wait (the third submit waits for the first staging set), answers
+    # bt_execute_batch_host_async: four batches queued before the first wait
+    # (the fourth submit waits for the first of the three staging sets), answers
     # request by request against the oracle.  With page-locked buffers and
     # OPT_HOST_VALUES_IN_PLACE the sorted modes read the values of the writes
     # over the bus instead of copying the value array; otherwise it is copied.
@@ -164,13 +164,12 @@ def test_async_host_batches_in_flight(gpu, pinned, in_place, mode):
                          torch.from_numpy(ro.copy()), torch.zeros(n, dtype=torch.int64),
                          torch.zeros(n, dtype=torch.uint8)])
     tickets = []
-    for b in range(3):
+    for b in range(4):
         tickets.append(t.submit_host(*bufs[b], mode=mode))
-    t.wait_host(tickets[1])  # out of order: batches run in submission order anyway
-    t.wait_host(tickets[0])
-    for b in range(3, 5):
-        tickets.append(t.submit_host(*bufs[b], mode=mode))
-    for tk in tickets[2:]:
+    t.wait_host(tickets[2])  # out of order: batches run in submission order anyway
+    t.wait_host(tickets[1])
+    tickets.append(t.submit_host(*bufs[4], mode=mode))
+    for tk in tickets[3:]:
         t.wait_host(tk)
     assert tickets == sorted(tickets) and len(set(tickets)) == 5
     t.wait_host(tickets[0])  # an old ticket: finished long ago
@@ -188,4 +187,115 @@ def test_async_host_batches_in_flight(gpu, pinned, in_place, mode):
     assert (gk == ok).all() and (gvv == ovv).all()
     del bufs
     for hbuf in pinned_bufs:
+        hbuf.free()
+
+
+@pytest.mark.parametrize("pinned", [True, False])
+@pytest.mark.parametrize("mode", [MERGE, E.MODE_SORTED, E.MODE_STM])
+def test_packed_insert_values(gpu, pinned, mode):
+    # bt_execute_batch_host_packed_async: only the INSERTs' values cross the
+    # bus, packed in request order.  Batches of 95/5, 50/50, all GETs (no
+    # value at all) and DELETE runs, sizes that are not a multiple of the
+    # eight-byte count step or of a tile, two in flight; answers request by
+    # request and the final contents against the oracle.
+    import torch
+
+    keys = O.gen_keys("uniform", 401, 60_000)
+    vals = O.value_of(keys)
+    t = E.BTree(max_keys=1 << 20, max_batch=1 << 16)
+    t.bulk_build(dev(keys), dev(vals))
+    o = O.OracleTree()
+    o.bulk_build(keys, vals)
+    shapes = [(40_001, 95, 0.0), (33_333, 50, 0.0), (20_007, 100, 0.0), (45_555, 80, 0.1), (7, 50, 0.0)]
+    bufs, keep, expect, n_ins = [], [], [], []
+    for b, (n, pct, dfrac) in enumerate(shapes):
+        rk, rv, ro = O.gen_requests("uniform", 410 + b, keys, n, pct)
+        if dfrac:
+            rk, rv, ro = with_deletes(rk, rv, ro, 420 + b, dfrac)
+        if mode == E.MODE_STM:  # the v39 meaning: compare batches without repeated keys
+            _, at = np.unique(rk, return_index=True)
+            sel = np.sort(at)
+            rk, rv, ro = rk[sel], rv[sel], ro[sel]
+            expect.append(o.execute_serial(rk, rv, ro))
+        else:
+            expect.append(o.execute_merged(rk, rv, ro, engine=O.ENGINE_MERGE))
+        iv = rv[ro == E.OP_INSERT].copy()
+        n_ins.append(iv.size)
+        m = rk.size
+        if pinned:
+            hb = [E.HostBuffer(m, torch.int64), E.HostBuffer(m, torch.uint8), E.HostBuffer(max(iv.size, 1), torch.int64),
+                  E.HostBuffer(m, torch.int64), E.HostBuffer(m, torch.uint8)]
+            keep += hb
+            hb[0].tensor.numpy().view(np.uint64)[:] = rk
+            hb[1].tensor.numpy()[:] = ro
+            hb[2].tensor.numpy().view(np.uint64)[: iv.size] = iv
+            ts = [x.tensor for x in hb]
+            ts[2] = ts[2][: iv.size]
+        else:
+            ts = [torch.from_numpy(rk.view(np.int64).copy()), torch.from_numpy(ro.copy()),
+                  torch.from_numpy(iv.view(np.int64).copy()), torch.zeros(m, dtype=torch.int64),
+                  torch.zeros(m, dtype=torch.uint8)]
+        bufs.append(ts)
+    assert n_ins[2] == 0  # an all-GET batch sends no value
+    tickets = []
+    for b in range(len(shapes)):  # three in flight
+        if b >= 3:
+            t.wait_host(tickets[b - 3])
+        tickets.append(t.submit_host_packed(*bufs[b], mode=mode))
+    for tk in tickets[-3:]:
+        t.wait_host(tk)
+    for b in range(len(shapes)):
+        ov, os_ = expect[b]
+        assert (bufs[b][4].numpy() == os_).all(), b
+        assert (bufs[b][3].numpy().view(np.uint64) == ov).all(), b
+    t.sync()
+    gk, gvv = dump(t)
+    ok, ovv = o.dump()
+    assert (gk == ok).all() and (gvv == ovv).all()
+    # a count that does not match the op codes: every request rejected,
+    # nothing applied, and the batch's wait reports it (also once its
+    # staging set has been reused); the next batch runs normally
+    rk, rv, ro = O.gen_requests("uniform", 430, keys, 1000, 50)
+    iv = rv[ro == E.OP_INSERT]
+    ok_, okv = o.dump()
+    bad = []
+    for wrong in (iv[:-1], np.concatenate([iv, iv[:1]])):
+        st = torch.full((rk.size,), 9, dtype=torch.uint8)
+        tk = t.submit_host_packed(torch.from_numpy(rk.view(np.int64).copy()), torch.from_numpy(ro.copy()),
+                                  torch.from_numpy(wrong.view(np.int64).copy()), torch.zeros(rk.size, dtype=torch.int64),
+                                  st, mode=mode)
+        with pytest.raises(E.BTError) as ei:
+            t.wait_host(tk)
+        assert ei.value.code == -1  # BT_ERR_INVALID_ARG
+        assert (st.numpy() == E.ST_REJECTED).all()
+        bad.append(tk)
+    good = [torch.zeros(rk.size, dtype=torch.int64), torch.zeros(rk.size, dtype=torch.uint8)]
+    if mode == E.MODE_STM:
+        _, at = np.unique(rk, return_index=True)
+        sel = np.sort(at)
+        rk, rv, ro = rk[sel], rv[sel], ro[sel]
+        good = [g[: rk.size] for g in good]
+        ov, os_ = o.execute_serial(rk, rv, ro)
+    else:
+        ov, os_ = o.execute_merged(rk, rv, ro, engine=O.ENGINE_MERGE)
+    gk, gvv = dump(t)
+    assert (gk == ok_).all() and (gvv == okv).all()  # the refused batches changed nothing
+    iv = rv[ro == E.OP_INSERT]
+    t.wait_host(t.submit_host_packed(torch.from_numpy(rk.view(np.int64).copy()), torch.from_numpy(ro.copy()),
+                                     torch.from_numpy(iv.view(np.int64).copy()), *good, mode=mode))
+    assert (good[1].numpy() == os_).all() and (good[0].numpy().view(np.uint64) == ov).all()
+    # an all-GET batch (no values at all), then another: every staging set reused
+    qk = ok_[:: max(1, ok_.size // 500)]
+    qo = np.full(qk.size, E.OP_GET, np.uint8)
+    gv_, gs_ = torch.zeros(qk.size, dtype=torch.int64), torch.zeros(qk.size, dtype=torch.uint8)
+    for _ in range(2):
+        t.wait_host(t.submit_host_packed(torch.from_numpy(qk.view(np.int64).copy()), torch.from_numpy(qo),
+                                         torch.zeros(0, dtype=torch.int64), gv_, gs_, mode=mode))
+    ek, ev = o.dump()
+    assert (gs_.numpy() == 1).all() and (gv_.numpy().view(np.uint64) == ev[np.searchsorted(ek, qk)]).all()
+    for tk in bad:  # both sets reused since: the refusals are still reported
+        with pytest.raises(E.BTError):
+            t.wait_host(tk)
+    del bufs
+    for hbuf in keep:
         hbuf.free()
