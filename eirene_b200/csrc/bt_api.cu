@@ -251,7 +251,15 @@ int bt_execute_batch(bt_handle* H, const uint64_t* keys, const uint64_t* vals, c
   const int base = mode & 0xF;
   if (base == BT_MODE_STM) {
     if (bt::tree_join(&h, S(stream)) != cudaSuccess) return BT_ERR_CUDA;
-    cudaError_t e = bt::launch_stm(&h, keys, vals, ops, 0xFF, nullptr, nullptr, n, out_vals, out_status, S(stream));
+    const uint8_t* run_ops = ops;
+    const uint64_t* run_vals = vals;
+    if (h.stm_combine && bt::stm_combine(&h, keys, vals, ops, n, out_vals, out_status, S(stream), &run_ops,
+                                         &run_vals) != 0)
+      return BT_ERR_CUDA;
+    cudaError_t e =
+        bt::launch_stm(&h, keys, run_vals, run_ops, 0xFF, nullptr, nullptr, n, out_vals, out_status, S(stream));
+    if (e == cudaSuccess && h.stm_combine && bt::stm_combine_fixup(&h, n, out_vals, out_status, S(stream)) != 0)
+      return BT_ERR_CUDA;
     return e == cudaSuccess ? BT_OK : BT_ERR_CUDA;
   }
   if (base != BT_MODE_SORTED) return BT_ERR_INVALID_ARG;
@@ -729,6 +737,9 @@ int bt_set_option(bt_handle* H, int option, int64_t value) {
       return BT_OK;
     case BT_OPT_HOST_VALUES_IN_PLACE:
       H->h.host_vals_in_place = value ? 1 : 0;
+      return BT_OK;
+    case BT_OPT_STM_COMBINE:
+      H->h.stm_combine = value ? 1 : 0;
       return BT_OK;
     case BT_OPT_LEARNED_MODE:
       if (value < 1 || value > 3) return BT_ERR_INVALID_ARG;

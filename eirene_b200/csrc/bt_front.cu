@@ -88,6 +88,7 @@ __global__ void __launch_bounds__(kThreads) front_clear_kernel(Slot* __restrict_
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += (size_t)gridDim.x * blockDim.x) {
     tab[i].key = kKeyMax;
     tab[i].first = kNone;
+    tab[i].pad = 0;
   }
 }
 
@@ -401,7 +402,130 @@ __global__ void __launch_bounds__(kThreads) pack_check_kernel(const uint32_t* __
     ops[i] = 0xFF;
 }
 
+// ---- INSERT combining for BT_MODE_STM batches ----
+// Requests of an STM batch are concurrent transactions (the v39 meaning), so
+// any serial order of them is a valid outcome.  The INSERTs of one key are
+// put in the order in which they reach the key's table slot (an atomic
+// exchange on the slot's tail): the first one (the representative) runs in
+// the STM kernel and stores the value of the last one; every other INSERT is
+// answered at once with the value of the one before it (FOUND), as if the
+// key's INSERTs ran back to back at the representative's commit.  A key that
+// the batch also DELETEs is not combined.  A slot's `first` holds the tail
+// index, and `pad` the representative's index (bit 31: the key has a DELETE).
+constexpr uint32_t kDelBit = 1u << 31;
+
+__global__ void __launch_bounds__(kThreads) combine_arrive_kernel(const uint64_t* __restrict__ keys,
+                                                                  const uint8_t* __restrict__ ops, size_t n,
+                                                                  Slot* __restrict__ tab,
+                                                                  const BatchCounts* __restrict__ counts,
+                                                                  uint32_t* __restrict__ pred,
+                                                                  uint32_t* __restrict__ slot_of) {
+  const uint32_t mask = counts->cap - 1;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const uint8_t op = ops[i];
+    if (op != kOpInsert && op != kOpDelete) continue;
+    const uint64_t k = keys[i];
+    if (k == kKeyMax) continue;
+    uint32_t h = (uint32_t)slot_hash(k) & mask;
+    uint32_t at = kNone;
+    for (uint32_t probe = 0; probe <= mask; probe++) {
+      const unsigned long long prev = atomicCAS(&tab[h].key, (unsigned long long)kKeyMax, (unsigned long long)k);
+      if (prev == kKeyMax || prev == k) {
+        at = h;
+        break;
+      }
+      h = (h + 1) & mask;
+    }
+    if (op == kOpDelete) {
+      if (at != kNone) atomicOr(&tab[at].pad, kDelBit);
+      continue;
+    }
+    slot_of[i] = at;
+    if (at == kNone) continue;  // no slot (cannot happen below load 1): runs uncombined
+    const uint32_t p = atomicExch(&tab[at].first, (uint32_t)i);
+    pred[i] = p;
+    if (p == kNone) atomicOr(&tab[at].pad, (uint32_t)i);
+  }
+}
+
+// op codes and INSERT values for the STM kernel; the combined INSERTs answered
+__global__ void __launch_bounds__(kThreads) combine_mark_kernel(const uint64_t* __restrict__ keys,
+                                                                const uint64_t* __restrict__ vals,
+                                                                const uint8_t* __restrict__ ops, size_t n,
+                                                                const Slot* __restrict__ tab,
+                                                                const uint32_t* __restrict__ pred,
+                                                                const uint32_t* __restrict__ slot_of,
+                                                                uint8_t* __restrict__ cops,
+                                                                uint64_t* __restrict__ cvals,
+                                                                uint64_t* __restrict__ out_vals,
+                                                                uint8_t* __restrict__ out_st) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    uint8_t op = ops[i];
+    if (op == kOpInsert) {
+      const uint32_t at = keys[i] != kKeyMax ? slot_of[i] : kNone;
+      if (at == kNone || (tab[at].pad & kDelBit)) {
+        cvals[i] = vals[i];
+      } else if (pred[i] != kNone) {
+        out_vals[i] = vals[pred[i]];
+        out_st[i] = kFound;
+        op = kOpSkip;
+      } else {
+        cvals[i] = vals[tab[at].first];  // the last INSERT of the key
+      }
+    }
+    cops[i] = op;
+  }
+}
+
+// a representative that did not commit (retry limit, full node pool): the
+// INSERTs combined with it report the same status
+__global__ void __launch_bounds__(kThreads) combine_fixup_kernel(const uint8_t* __restrict__ cops, size_t n,
+                                                                 const Slot* __restrict__ tab,
+                                                                 const uint32_t* __restrict__ slot_of,
+                                                                 uint64_t* __restrict__ out_vals,
+                                                                 uint8_t* __restrict__ out_st) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    if (cops[i] != kOpSkip) continue;
+    const uint32_t rep = tab[slot_of[i]].pad & ~kDelBit;
+    const uint8_t st = out_st[rep];
+    if (st == kRetryExhausted || st == kNoCapacity) {
+      out_st[i] = st;
+      out_vals[i] = 0;
+    }
+  }
+}
+
 }  // namespace
+
+int stm_combine(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, size_t n,
+                uint64_t* out_vals, uint8_t* out_st, cudaStream_t s, const uint8_t** cops, const uint64_t** cvals) {
+  Work& w = h->w;
+  BatchCounts* c = w.counts;
+  Slot* tab = reinterpret_cast<Slot*>(w.f_tab);
+  uint8_t* co = reinterpret_cast<uint8_t*>(w.f_flags);
+  uint64_t* cv = w.f_lk;
+  uint32_t* pred = w.f_list;
+  uint32_t* slot_of = w.f_pos;
+  const unsigned g = (unsigned)min((size_t)h->sm_count * 8, (n + kThreads - 1) / kThreads);
+  if (cudaMemsetAsync(c, 0, sizeof(BatchCounts), s) != cudaSuccess) return -2;
+  front_count_kernel<<<(unsigned)h->sm_count * 2, kThreads, 0, s>>>(ops, n, c);
+  front_clear_kernel<<<(unsigned)h->sm_count * 4, kThreads, 0, s>>>(tab, w.f_tab_cap, c);
+  combine_arrive_kernel<<<g, kThreads, 0, s>>>(keys, ops, n, tab, c, pred, slot_of);
+  combine_mark_kernel<<<g, kThreads, 0, s>>>(keys, vals, ops, n, tab, pred, slot_of, co, cv, out_vals, out_st);
+  count_launch(4);
+  *cops = co;
+  *cvals = cv;
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int stm_combine_fixup(Handle* h, size_t n, uint64_t* out_vals, uint8_t* out_st, cudaStream_t s) {
+  Work& w = h->w;
+  const unsigned g = (unsigned)min((size_t)h->sm_count * 8, (n + kThreads - 1) / kThreads);
+  combine_fixup_kernel<<<g, kThreads, 0, s>>>(reinterpret_cast<const uint8_t*>(w.f_flags), n,
+                                              reinterpret_cast<const Slot*>(w.f_tab), w.f_pos, out_vals, out_st);
+  count_launch();
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
 
 // scratch: tile counts, tile offsets, the INSERT total, the mismatch flag,
 // then the scan's own words

@@ -235,6 +235,7 @@ struct Handle {
   int overlap_reserve = 16;  // ... in the overlapped layout (measured: 16 >= 32 > 64 > none)
   // host-buffer entry points: staging sets and copy streams
   HostPipe hp;
+  int stm_combine = 1;         // BT_MODE_STM batches combine the INSERTs of a key (BT_OPT_STM_COMBINE)
   int host_vals_in_place = 0;  // sorted host batches read page-locked values over the bus instead of copying
   // per-batch hooks of the sorted batch, set by the host-buffer entry points:
   // the stream that first reads `vals` waits for vals_wait; vals_remote says
@@ -351,6 +352,14 @@ int delete_apply(Handle* h, size_t n_upper, cudaStream_t s);
 
 // ---- hash front end of the sorted batch (bt_front.cu) ----
 int front_classify(Handle* h, const uint64_t* keys, const uint8_t* ops, size_t n, cudaStream_t s);
+// INSERT combining of a BT_MODE_STM batch: answers the INSERTs combined with
+// an earlier one of their key and returns the op codes (kOpSkip for those)
+// and INSERT values for the STM kernel (in the front end's buffers);
+// stm_combine_fixup after the kernel gives a chain the status of its
+// representative when that did not commit
+int stm_combine(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, size_t n,
+                uint64_t* out_vals, uint8_t* out_st, cudaStream_t s, const uint8_t** cops, const uint64_t** cvals);
+int stm_combine_fixup(Handle* h, size_t n, uint64_t* out_vals, uint8_t* out_st, cudaStream_t s);
 // packed INSERT values (scratch sized by pack_scratch_words(n_cap), n <= n_cap):
 // pack_check counts the INSERTs of ops per tile and, when their total is not
 // n_packed, raises the word at pack_error_word and makes every op code

@@ -769,6 +769,7 @@ __global__ void __launch_bounds__(256, 4) stm_kernel(DevTree t, const uint64_t* 
       rest &= rest - 1;
       const uint32_t r = list ? list[q] : (uint32_t)q;
       const uint32_t op = op_override <= 1 ? op_override : (uint32_t)ops[r];
+      if (op == kOpSkip) continue;  // a combined INSERT, answered already
       uint64_t ans;
       uint8_t st;
       run_request(t, epoch, keys[r], op, op == kOpInsert ? vals[r] : 0, retry_limit, ans, st, cnt, M);

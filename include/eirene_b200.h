@@ -274,6 +274,12 @@ int bt_set_search_group(bt_handle *h, uint32_t lanes);
                                        * batch's writes from a page-locked value array over the bus instead of
                                        * copying the array (fewer bytes, but scattered reads; measured slower on
                                        * a 95/5 batch of 2^22); 0 (default) copies it */
+#define BT_OPT_STM_COMBINE 15   /* BT_MODE_STM batches: 1 (default) combines the INSERTs of one key into one
+                                 * transaction: the first to arrive stores the last one's value, each other is
+                                 * answered FOUND with the value of the one before it (a serial order of the
+                                 * concurrent requests, which is what the v39 meaning allows; keys the batch
+                                 * also DELETEs are not combined); 0 runs every INSERT as its own transaction,
+                                 * like the reference (src/gpu-stm-tree-v39/bpt-gpustm-kernel.cu:41-56) */
 #define BT_OPT_SORT_TILE 14     /* radix sort tile of sorted batches: 256, 512 (default) or 1024 threads x 8 keys,
                                  * for whole batches and for the hash front end's touched requests alike
                                  * (bt_autotune picks the two separately) */
