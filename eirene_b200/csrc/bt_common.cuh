@@ -27,9 +27,6 @@ constexpr uint32_t kNil = 0xFFFFFFFFu;
 constexpr uint8_t kOpInsert = 0;  // src/input-helper.h:14
 constexpr uint8_t kOpGet = 1;     // src/input-helper.h:15
 constexpr uint8_t kOpDelete = 2;  // src/input-helper.h:16 (declared there, implemented by no reference version)
-// internal: an INSERT answered before the STM kernel (combined with an
-// earlier INSERT of its key); the kernel passes over it
-constexpr uint8_t kOpSkip = 0xFE;
 
 // per-request status byte
 constexpr uint8_t kAbsent = 0;

@@ -414,16 +414,65 @@ __global__ void __launch_bounds__(kThreads) pack_check_kernel(const uint32_t* __
 // index, and `pad` the representative's index (bit 31: the key has a DELETE).
 constexpr uint32_t kDelBit = 1u << 31;
 
+// The write requests (INSERT, DELETE) listed, in no particular order, with
+// one atomic per warp: the later passes then run one thread per write, all
+// of their dependent loads in flight at once, instead of walking every
+// request.  counts->n_ins_req ends as the list's length.
+__global__ void __launch_bounds__(kThreads) combine_list_kernel(const uint8_t* __restrict__ ops, size_t n,
+                                                                uint32_t* __restrict__ list,
+                                                                BatchCounts* __restrict__ counts) {
+  const uint32_t lane = threadIdx.x & 31;
+  // sixteen op codes per load when the array is 16-byte aligned
+  const size_t n16 = ((uintptr_t)ops & 15u) ? 0 : n / 16;
+  const uint4* o16 = reinterpret_cast<const uint4*>(ops);
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  // whole warps iterate together (the appends are warp-aggregated)
+  const size_t warp0 = (size_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u);
+  auto append = [&](uint32_t m, size_t first) {
+    const uint32_t c = __popc(m);
+    uint32_t incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= (uint32_t)o) incl += y;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    uint32_t base = 0;
+    if (lane == 31 && total) base = atomicAdd(&counts->n_ins_req, total);
+    base = __shfl_sync(0xffffffffu, base, 31);
+    uint32_t p = base + incl - c;
+    for (int b = 0; m; b++, m >>= 1)
+      if (m & 1u) list[p++] = (uint32_t)(first + (size_t)b);
+  };
+  for (size_t w = warp0; w < n16; w += stride) {
+    const size_t i = w + lane;
+    uint32_t m = 0;
+    if (i < n16) {
+      const uint4 o = o16[i];
+      const uint32_t words[4] = {o.x, o.y, o.z, o.w};
+#pragma unroll
+      for (int j = 0; j < 16; j++) m |= is_write((uint8_t)(words[j / 4] >> (8 * (j % 4)))) << j;
+    }
+    append(m, 16 * i);
+  }
+  for (size_t w = n16 * 16 + warp0; w < n; w += stride) {
+    const size_t i = w + lane;
+    append(i < n ? is_write(ops[i]) : 0u, i);
+  }
+}
+
 __global__ void __launch_bounds__(kThreads) combine_arrive_kernel(const uint64_t* __restrict__ keys,
-                                                                  const uint8_t* __restrict__ ops, size_t n,
+                                                                  const uint8_t* __restrict__ ops,
+                                                                  const uint32_t* __restrict__ list,
                                                                   Slot* __restrict__ tab,
                                                                   const BatchCounts* __restrict__ counts,
                                                                   uint32_t* __restrict__ pred,
                                                                   uint32_t* __restrict__ slot_of) {
   const uint32_t mask = counts->cap - 1;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+  const size_t m = counts->n_ins_req;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < m; q += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t i = list[q];
     const uint8_t op = ops[i];
-    if (op != kOpInsert && op != kOpDelete) continue;
     const uint64_t k = keys[i];
     if (k == kKeyMax) continue;
     uint32_t h = (uint32_t)slot_hash(k) & mask;
@@ -442,50 +491,59 @@ __global__ void __launch_bounds__(kThreads) combine_arrive_kernel(const uint64_t
     }
     slot_of[i] = at;
     if (at == kNone) continue;  // no slot (cannot happen below load 1): runs uncombined
-    const uint32_t p = atomicExch(&tab[at].first, (uint32_t)i);
+    const uint32_t p = atomicExch(&tab[at].first, i);
     pred[i] = p;
-    if (p == kNone) atomicOr(&tab[at].pad, (uint32_t)i);
+    if (p == kNone) atomicOr(&tab[at].pad, i);
   }
 }
 
-// op codes and INSERT values for the STM kernel; the combined INSERTs answered
+// per INSERT: its value for the STM kernel, or (combined with an earlier one)
+// its answer and a skip mark
 __global__ void __launch_bounds__(kThreads) combine_mark_kernel(const uint64_t* __restrict__ keys,
                                                                 const uint64_t* __restrict__ vals,
-                                                                const uint8_t* __restrict__ ops, size_t n,
+                                                                const uint8_t* __restrict__ ops,
+                                                                const uint32_t* __restrict__ list,
+                                                                const BatchCounts* __restrict__ counts,
                                                                 const Slot* __restrict__ tab,
                                                                 const uint32_t* __restrict__ pred,
                                                                 const uint32_t* __restrict__ slot_of,
-                                                                uint8_t* __restrict__ cops,
+                                                                uint8_t* __restrict__ skip,
                                                                 uint64_t* __restrict__ cvals,
                                                                 uint64_t* __restrict__ out_vals,
                                                                 uint8_t* __restrict__ out_st) {
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    uint8_t op = ops[i];
-    if (op == kOpInsert) {
-      const uint32_t at = keys[i] != kKeyMax ? slot_of[i] : kNone;
-      if (at == kNone || (tab[at].pad & kDelBit)) {
-        cvals[i] = vals[i];
-      } else if (pred[i] != kNone) {
-        out_vals[i] = vals[pred[i]];
-        out_st[i] = kFound;
-        op = kOpSkip;
-      } else {
-        cvals[i] = vals[tab[at].first];  // the last INSERT of the key
-      }
+  const size_t m = counts->n_ins_req;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < m; q += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t i = list[q];
+    if (ops[i] != kOpInsert) continue;
+    const uint32_t at = keys[i] != kKeyMax ? slot_of[i] : kNone;
+    uint8_t sk = 0;
+    if (at == kNone || (tab[at].pad & kDelBit)) {
+      cvals[i] = vals[i];
+    } else if (pred[i] != kNone) {
+      out_vals[i] = vals[pred[i]];
+      out_st[i] = kFound;
+      sk = 1;
+    } else {
+      cvals[i] = vals[tab[at].first];  // the last INSERT of the key
     }
-    cops[i] = op;
+    skip[i] = sk;
   }
 }
 
 // a representative that did not commit (retry limit, full node pool): the
 // INSERTs combined with it report the same status
-__global__ void __launch_bounds__(kThreads) combine_fixup_kernel(const uint8_t* __restrict__ cops, size_t n,
+__global__ void __launch_bounds__(kThreads) combine_fixup_kernel(const uint8_t* __restrict__ ops,
+                                                                 const uint32_t* __restrict__ list,
+                                                                 const BatchCounts* __restrict__ counts,
+                                                                 const uint8_t* __restrict__ skip,
                                                                  const Slot* __restrict__ tab,
                                                                  const uint32_t* __restrict__ slot_of,
                                                                  uint64_t* __restrict__ out_vals,
                                                                  uint8_t* __restrict__ out_st) {
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    if (cops[i] != kOpSkip) continue;
+  const size_t m = counts->n_ins_req;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < m; q += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t i = list[q];
+    if (ops[i] != kOpInsert || !skip[i]) continue;
     const uint32_t rep = tab[slot_of[i]].pad & ~kDelBit;
     const uint8_t st = out_st[rep];
     if (st == kRetryExhausted || st == kNoCapacity) {
@@ -498,30 +556,31 @@ __global__ void __launch_bounds__(kThreads) combine_fixup_kernel(const uint8_t* 
 }  // namespace
 
 int stm_combine(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, size_t n,
-                uint64_t* out_vals, uint8_t* out_st, cudaStream_t s, const uint8_t** cops, const uint64_t** cvals) {
+                uint64_t* out_vals, uint8_t* out_st, cudaStream_t s, const uint8_t** skip, const uint64_t** cvals) {
   Work& w = h->w;
   BatchCounts* c = w.counts;
   Slot* tab = reinterpret_cast<Slot*>(w.f_tab);
-  uint8_t* co = reinterpret_cast<uint8_t*>(w.f_flags);
+  uint8_t* sk = reinterpret_cast<uint8_t*>(w.f_flags);
   uint64_t* cv = w.f_lk;
   uint32_t* pred = w.f_list;
   uint32_t* slot_of = w.f_pos;
-  const unsigned g = (unsigned)min((size_t)h->sm_count * 8, (n + kThreads - 1) / kThreads);
+  uint32_t* list = w.ins_list;
+  const unsigned g = (unsigned)min((size_t)h->sm_count * 8, (n / 4 + kThreads) / kThreads);
   if (cudaMemsetAsync(c, 0, sizeof(BatchCounts), s) != cudaSuccess) return -2;
-  front_count_kernel<<<(unsigned)h->sm_count * 2, kThreads, 0, s>>>(ops, n, c);
+  combine_list_kernel<<<g, kThreads, 0, s>>>(ops, n, list, c);
   front_clear_kernel<<<(unsigned)h->sm_count * 4, kThreads, 0, s>>>(tab, w.f_tab_cap, c);
-  combine_arrive_kernel<<<g, kThreads, 0, s>>>(keys, ops, n, tab, c, pred, slot_of);
-  combine_mark_kernel<<<g, kThreads, 0, s>>>(keys, vals, ops, n, tab, pred, slot_of, co, cv, out_vals, out_st);
+  combine_arrive_kernel<<<g, kThreads, 0, s>>>(keys, ops, list, tab, c, pred, slot_of);
+  combine_mark_kernel<<<g, kThreads, 0, s>>>(keys, vals, ops, list, c, tab, pred, slot_of, sk, cv, out_vals, out_st);
   count_launch(4);
-  *cops = co;
+  *skip = sk;
   *cvals = cv;
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
-int stm_combine_fixup(Handle* h, size_t n, uint64_t* out_vals, uint8_t* out_st, cudaStream_t s) {
+int stm_combine_fixup(Handle* h, const uint8_t* ops, size_t n, uint64_t* out_vals, uint8_t* out_st, cudaStream_t s) {
   Work& w = h->w;
-  const unsigned g = (unsigned)min((size_t)h->sm_count * 8, (n + kThreads - 1) / kThreads);
-  combine_fixup_kernel<<<g, kThreads, 0, s>>>(reinterpret_cast<const uint8_t*>(w.f_flags), n,
+  const unsigned g = (unsigned)min((size_t)h->sm_count * 8, (n / 4 + kThreads) / kThreads);
+  combine_fixup_kernel<<<g, kThreads, 0, s>>>(ops, w.ins_list, w.counts, reinterpret_cast<const uint8_t*>(w.f_flags),
                                               reinterpret_cast<const Slot*>(w.f_tab), w.f_pos, out_vals, out_st);
   count_launch();
   return cudaGetLastError() == cudaSuccess ? 0 : -2;

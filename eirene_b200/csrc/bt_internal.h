@@ -343,7 +343,7 @@ cudaError_t launch_serve(Handle* h, const ServeDev& S, cudaStream_t s);
 // ---- STM kernels (bt_stm.cu) ----
 cudaError_t launch_stm(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, uint8_t op_override,
                        const uint32_t* list, const uint32_t* n_dev, size_t n, uint64_t* out_vals, uint8_t* out_st,
-                       cudaStream_t s);
+                       cudaStream_t s, const uint8_t* skip = nullptr);
 
 // ---- delete phase of the sorted batch (bt_delete.cu) ----
 // locate: reads the tree only (answers the DELETE runs); apply: removes the keys
@@ -353,13 +353,13 @@ int delete_apply(Handle* h, size_t n_upper, cudaStream_t s);
 // ---- hash front end of the sorted batch (bt_front.cu) ----
 int front_classify(Handle* h, const uint64_t* keys, const uint8_t* ops, size_t n, cudaStream_t s);
 // INSERT combining of a BT_MODE_STM batch: answers the INSERTs combined with
-// an earlier one of their key and returns the op codes (kOpSkip for those)
-// and INSERT values for the STM kernel (in the front end's buffers);
+// an earlier one of their key and returns, per INSERT, a skip byte (1: answered
+// already) and the value the STM kernel stores (in the front end's buffers);
 // stm_combine_fixup after the kernel gives a chain the status of its
 // representative when that did not commit
 int stm_combine(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, size_t n,
-                uint64_t* out_vals, uint8_t* out_st, cudaStream_t s, const uint8_t** cops, const uint64_t** cvals);
-int stm_combine_fixup(Handle* h, size_t n, uint64_t* out_vals, uint8_t* out_st, cudaStream_t s);
+                uint64_t* out_vals, uint8_t* out_st, cudaStream_t s, const uint8_t** skip, const uint64_t** cvals);
+int stm_combine_fixup(Handle* h, const uint8_t* ops, size_t n, uint64_t* out_vals, uint8_t* out_st, cudaStream_t s);
 // packed INSERT values (scratch sized by pack_scratch_words(n_cap), n <= n_cap):
 // pack_check counts the INSERTs of ops per tile and, when their total is not
 // n_packed, raises the word at pack_error_word and makes every op code

@@ -743,7 +743,8 @@ __global__ void __launch_bounds__(256, 4) stm_kernel(DevTree t, const uint64_t* 
                                                      uint32_t op_override, const uint32_t* __restrict__ list,
                                                      const uint32_t* __restrict__ n_dev, size_t n_host,
                                                      uint64_t* __restrict__ out_vals, uint8_t* __restrict__ out_st,
-                                                     uint32_t retry_limit, LearnedDev lm, int use_learned) {
+                                                     uint32_t retry_limit, LearnedDev lm, int use_learned,
+                                                     const uint8_t* __restrict__ skip) {
   const uint32_t lane = lane_id();
   const size_t n = n_dev ? (size_t)*n_dev : n_host;
   const LearnedDev* M = use_learned ? &lm : nullptr;
@@ -769,7 +770,7 @@ __global__ void __launch_bounds__(256, 4) stm_kernel(DevTree t, const uint64_t* 
       rest &= rest - 1;
       const uint32_t r = list ? list[q] : (uint32_t)q;
       const uint32_t op = op_override <= 1 ? op_override : (uint32_t)ops[r];
-      if (op == kOpSkip) continue;  // a combined INSERT, answered already
+      if (skip && op == kOpInsert && skip[r]) continue;  // a combined INSERT, answered already
       uint64_t ans;
       uint8_t st;
       run_request(t, epoch, keys[r], op, op == kOpInsert ? vals[r] : 0, retry_limit, ans, st, cnt, M);
@@ -992,7 +993,7 @@ cudaError_t launch_serve(Handle* h, const ServeDev& S, cudaStream_t s) {
 
 cudaError_t launch_stm(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, uint8_t op_override,
                        const uint32_t* list, const uint32_t* n_dev, size_t n, uint64_t* out_vals, uint8_t* out_st,
-                       cudaStream_t s) {
+                       cudaStream_t s, const uint8_t* skip) {
   if (n == 0) return cudaSuccess;
   const int threads = 256;  // 8 warps
   // one resident wave: every warp runs at once, each on a contiguous run
@@ -1009,7 +1010,7 @@ cudaError_t launch_stm(Handle* h, const uint64_t* keys, const uint64_t* vals, co
   const int use = learned_dev(h, &lm);
   h->pfx_valid = false;  // STM writes inner rows without their prefixes
   stm_kernel<<<(unsigned)blocks, threads, 0, s>>>(h->tree, keys, vals, ops, op_override, list, n_dev, n, out_vals,
-                                                   out_st, h->retry_limit, lm, use);
+                                                   out_st, h->retry_limit, lm, use, skip);
   count_launch();
   return cudaGetLastError();
 }
