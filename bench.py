@@ -702,6 +702,8 @@ def main():
     ap.add_argument("--dist", default="uniform", choices=["uniform", "zipf", "normal", "gamma"])
     ap.add_argument("--descent", default="both", choices=["plain", "learned", "both"])
     ap.add_argument("--search-group", type=int, default=4)
+    ap.add_argument("--segments", type=int, default=0,
+                    help="learned predictor segments (0: one per 64 leaves at training, at least 4096)")
     ap.add_argument("--engine", default="merge", choices=["merge", "stm"],
                     help="insert engine of the sorted batch: segmented leaf merge or warp STM")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -791,10 +793,11 @@ def main():
 
         # an owner receives about n_b requests per step; headroom keeps that one local batch
         sharded = ShardedBTree.on_gpu(max_keys=pool_keys, max_batch=n_b + n_b // 8, device=local,
-                                      search_group=args.search_group)
+                                      search_group=args.search_group, n_segments=args.segments)
         tree = sharded.ops.tree
     else:
-        tree = E.BTree(max_keys=pool_keys, max_batch=n_b, device=local, search_group=args.search_group)
+        tree = E.BTree(max_keys=pool_keys, max_batch=n_b, device=local, search_group=args.search_group,
+                       n_segments=args.segments)
     tree.set_option(E.OPT_FRONT_END, 1 if args.front_end == "hash" else 0)
     tk = torch.empty(n_tree, dtype=torch.int64, device="cuda")
     tv = torch.empty(n_tree, dtype=torch.int64, device="cuda")

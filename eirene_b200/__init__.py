@@ -232,7 +232,7 @@ class BTree:
 
     def __init__(self, max_keys: int = 1 << 20, max_batch: int = 1 << 22, leaf_fill: int = 24,
                  inner_fill: int = 24, device: int = 0, search_group: int = 4, retry_limit: int = 0,
-                 n_segments: int = 4096, window: int = 64):
+                 n_segments: int = 0, window: int = 64):
         L = lib()
         cfg = Config()
         _check(L.bt_config_init(ctypes.byref(cfg)), "bt_config_init")

@@ -134,7 +134,7 @@ int bt_config_init(bt_config* c) {
   c->retry_limit = 1u << 16;
   c->device = 0;
   c->search_group = 4;
-  c->n_segments = 4096;
+  c->n_segments = 0;
   c->window = 64;
   return BT_OK;
 }
@@ -165,6 +165,7 @@ int bt_create(const bt_config* cfg_in, bt_handle** out) {
   h.inner_fill = cfg.inner_fill;
   h.retry_limit = cfg.retry_limit ? cfg.retry_limit : (1u << 16);
   h.search_group = (int)cfg.search_group;
+  h.L.seg_config = cfg.n_segments;
   h.L.n_segments = cfg.n_segments ? cfg.n_segments : 4096;
   h.L.window = cfg.window ? cfg.window : 64;
   cudaDeviceGetAttribute(&h.sm_count, cudaDevAttrMultiProcessorCount, cfg.device);

@@ -157,7 +157,8 @@ struct HostPipe {
 struct Learned {
   bool valid = false;
   uint32_t n_leaves = 0;
-  uint32_t n_segments = 0;
+  uint32_t n_segments = 0;  // segments of the current model
+  uint32_t seg_config = 0;  // segments asked for; 0: chosen at each full training (learned_retrain)
   uint32_t window = 64;
   uint64_t* leaf_low = nullptr;  // [n_leaves + 1] (sentinel at the end)
   uint32_t* leaf_id = nullptr;   // [n_leaves]

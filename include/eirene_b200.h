@@ -78,7 +78,8 @@ typedef struct bt_config {
     int32_t device;        /* CUDA device ordinal (default 0) */
     uint32_t search_group; /* lanes per request in the search kernel: 4, 8, 16 or 32 (default 4; bt_autotune
                             * picks the fastest on the live tree) */
-    uint32_t n_segments;   /* learned predictor: leaf segments (default 4096) */
+    uint32_t n_segments;   /* learned predictor: leaf segments (default 0: one per 64 leaves at each full
+                            * training, a power of two, at least 4096; kept by bt_refit) */
     uint32_t window;       /* learned predictor: max error window in leaf slots (default 64) */
     uint32_t reserved[7];
 } bt_config;
