@@ -1015,7 +1015,9 @@ def main():
     tree.set_option(E.OPT_BATCH_DESCENT, 1 if head == "learned" else 0)
     if True:
         hb = []
-        e2e_steps = 10
+        # 30 steps: the first batch's copy-in and the last one's copy-out
+        # overlap nothing (about 1.4 ms per run), spread over the steps
+        e2e_steps = 30
         # page-locked host buffers from the library's own allocator (bt_host_alloc)
         pinned = []
 
@@ -1024,33 +1026,36 @@ def main():
             pinned.append(b)
             return b.tensor
 
-        n_ins = []
+        # pinned host batches, refilled with fresh requests before each timed
+        # loop: a loop that replayed batches the tree had already applied would
+        # time INSERTs that are all updates of existing keys
+        dk = torch.empty(n_b, dtype=torch.int64, device="cuda")
+        dv = torch.empty(n_b, dtype=torch.int64, device="cuda")
+        do = torch.empty(n_b, dtype=torch.uint8, device="cuda")
         for i in range(1 + e2e_steps):
-            k = torch.empty(n_b, dtype=torch.int64, device="cuda")
-            v = torch.empty(n_b, dtype=torch.int64, device="cuda")
-            o = torch.empty(n_b, dtype=torch.uint8, device="cuda")
-            E.gen_requests(args.dist, 30_000 + 1000 * rank + i, tk, n_b, args.search_pct, k, v, o, stream)
-            torch.cuda.synchronize()
-            hk, hv, ho = host_buf(n_b, torch.int64), host_buf(n_b, torch.int64), host_buf(n_b, torch.uint8)
-            hk.copy_(k)
-            hv.copy_(v)
-            ho.copy_(o)
-            # the same batch with the INSERTs' values only, packed in request order
-            iv = v[o == E.OP_INSERT]
-            hiv = host_buf(max(iv.numel(), 1), torch.int64)[: iv.numel()]
-            hiv.copy_(iv)
-            n_ins.append(iv.numel())
-            hb.append((hk, hv, ho, hiv))
+            hb.append((host_buf(n_b, torch.int64), host_buf(n_b, torch.int64), host_buf(n_b, torch.uint8),
+                       host_buf(n_b, torch.int64)))
+        n_ins = [0] * (1 + e2e_steps)
+
+        def fill_host(seed0):
+            for i, (hk, hv, ho, hiv) in enumerate(hb):
+                E.gen_requests(args.dist, seed0 + 1000 * rank + i, tk, n_b, args.search_pct, dk, dv, do, stream)
+                torch.cuda.synchronize()
+                hk.copy_(dk)
+                hv.copy_(dv)
+                ho.copy_(do)
+                # the same batch with the INSERTs' values only, packed in request order
+                iv = dv[do == E.OP_INSERT]
+                hiv[: iv.numel()].copy_(iv)
+                n_ins[i] = iv.numel()
+
         # three answer buffers: three batches in flight (the handle's three
         # staging sets): batch s is submitted once batch s - 3 is answered
         outs = [(host_buf(n_b, torch.int64), host_buf(n_b, torch.uint8)) for _ in range(3)]
 
-        dk = torch.empty(n_b, dtype=torch.int64, device="cuda")
-        dv = torch.empty(n_b, dtype=torch.int64, device="cuda")
-        do = torch.empty(n_b, dtype=torch.uint8, device="cuda")
-
-        def host_submit(b, out, packed):
-            k, v, o, iv = b
+        def host_submit(i, out, packed):
+            k, v, o, iv = hb[i]
+            iv = iv[: n_ins[i]]
             hov, hos = out
             if sharded is not None:
                 # host batch in, host answers out, through the sharded tree
@@ -1071,9 +1076,19 @@ def main():
             if t is not None:
                 tree.wait_host(t)
 
-        def timed(packed):
+        def timed(packed, seed0):
+            # like the device-resident forms: a freshly built tree, the
+            # headline form's model trained on it
+            rebuild_tree()
+            built[0] = False
+            tree.set_descent(False)
+            if head == "learned":
+                tree.retrain(stream)
+            tree.set_descent(head == "learned")
+            tree.set_option(E.OPT_BATCH_DESCENT, 1 if head == "learned" else 0)
+            fill_host(seed0)
             for _ in range(3):
-                host_wait(host_submit(hb[0], outs[0], packed))
+                host_wait(host_submit(0, outs[0], packed))
             barrier()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             w0 = time.perf_counter()
@@ -1082,7 +1097,7 @@ def main():
             for s in range(e2e_steps):
                 if s >= 3:
                     host_wait(tickets[s - 3])
-                tickets.append(host_submit(hb[1 + s], outs[s % 3], packed))
+                tickets.append(host_submit(1 + s, outs[s % 3], packed))
             for t in tickets[-3:]:
                 host_wait(t)
             tree.sync(stream)
@@ -1093,8 +1108,10 @@ def main():
             return allmax(e0.elapsed_time(e1)), wall_ms
 
         packed = sharded is None
-        full_ms, full_wall = timed(False)
-        e2e_ms, wall_ms = timed(True) if packed else (full_ms, full_wall)
+        e2e_ms, wall_ms = timed(True, 50_000) if packed else (None, None)
+        full_ms, full_wall = timed(False, 30_000)
+        if not packed:
+            e2e_ms, wall_ms = full_ms, full_wall
         del hb, outs
         for b in pinned:
             b.free()
