@@ -249,6 +249,36 @@ def reference_gpu(ref_bin: str, batches: int = 10):
     return out
 
 
+def stm_run(E, torch, t, keys_dev, n_b, warmup, steps, dist, search_pct, seed0, stream):
+    """`warmup` then `steps` BT_MODE_STM batches of fresh requests drawn from
+    `dist` over keys_dev; Mops/s over the timed batches and the STM counters."""
+    bs = []
+    for i in range(warmup + steps):
+        k = torch.empty(n_b, dtype=torch.int64, device="cuda")
+        v = torch.empty(n_b, dtype=torch.int64, device="cuda")
+        o = torch.empty(n_b, dtype=torch.uint8, device="cuda")
+        E.gen_requests(dist, seed0 + i, keys_dev, n_b, search_pct, k, v, o, stream)
+        bs.append((k, v, o))
+    ov = torch.empty(n_b, dtype=torch.int64, device="cuda")
+    ost = torch.empty(n_b, dtype=torch.uint8, device="cuda")
+    for i in range(warmup):
+        t.execute(*bs[i], ov, ost, mode=E.MODE_STM, stream=stream)
+    torch.cuda.synchronize()
+    s0 = t.stats()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(warmup, warmup + steps):
+        t.execute(*bs[i], ov, ost, mode=E.MODE_STM, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    s1 = t.stats()
+    ms = e0.elapsed_time(e1)
+    commits, aborts = s1["commits"] - s0["commits"], s1["aborts"] - s0["aborts"]
+    return {"mops": n_b * steps / (ms / 1e3) / 1e6, "ms_per_batch": ms / steps, "commits": commits,
+            "aborts": aborts, "aborts_per_commit": aborts / max(1, commits),
+            "retry_exhausted": s1["retry_exhausted"] - s0["retry_exhausted"], "batches": steps}
+
+
 def stm_passes(E, torch, tree, tk, n_b, steps, search_pct, stream):
     """BT_MODE_STM batches (the reference's v39 meaning: requests are
     concurrent warp transactions): on the headline tree with its workload, and
@@ -260,31 +290,7 @@ def stm_passes(E, torch, tree, tk, n_b, steps, search_pct, stream):
     out = {}
 
     def run(t, keys_dev, dist, seed0):
-        bs = []
-        for i in range(3 + steps):
-            k = torch.empty(n_b, dtype=torch.int64, device="cuda")
-            v = torch.empty(n_b, dtype=torch.int64, device="cuda")
-            o = torch.empty(n_b, dtype=torch.uint8, device="cuda")
-            E.gen_requests(dist, seed0 + i, keys_dev, n_b, search_pct, k, v, o, stream)
-            bs.append((k, v, o))
-        ov = torch.empty(n_b, dtype=torch.int64, device="cuda")
-        ost = torch.empty(n_b, dtype=torch.uint8, device="cuda")
-        for i in range(3):
-            t.execute(*bs[i], ov, ost, mode=E.MODE_STM, stream=stream)
-        torch.cuda.synchronize()
-        s0 = t.stats()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for i in range(3, 3 + steps):
-            t.execute(*bs[i], ov, ost, mode=E.MODE_STM, stream=stream)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        s1 = t.stats()
-        ms = e0.elapsed_time(e1)
-        commits, aborts = s1["commits"] - s0["commits"], s1["aborts"] - s0["aborts"]
-        return {"mops": n_b * steps / (ms / 1e3) / 1e6, "ms_per_batch": ms / steps, "commits": commits,
-                "aborts": aborts, "aborts_per_commit": aborts / max(1, commits),
-                "retry_exhausted": s1["retry_exhausted"] - s0["retry_exhausted"], "batches": steps}
+        return stm_run(E, torch, t, keys_dev, n_b, 3, steps, dist, search_pct, seed0, stream)
 
     tree.set_descent(False)
     out["headline_tree"] = run(tree, tk, "uniform", 60_000)
@@ -559,6 +565,33 @@ def serve_bench(E, np, tree, tk_host, n_tree, seconds=1.5, seed=5, load=0.5, pol
     return out
 
 
+def run_stm_only(args):
+    """BT_MODE_STM batches only (one GPU): a 2^tree-log2-key tree, --warmup
+    then --steps batches of 2^batch-log2 requests (--search-pct GETs), timed
+    with CUDA events; reports Mops/s and the STM counters."""
+    import torch
+
+    import eirene_b200 as E
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+    n_tree, n_b = 1 << args.tree_log2, 1 << args.batch_log2
+    tree = E.BTree(max_keys=2 * n_tree + 32 * n_b, max_batch=n_b, search_group=args.search_group)
+    tree.set_option(E.OPT_STM_COMBINE, 0 if args.no_stm_combine else 1)
+    tk = torch.empty(n_tree, dtype=torch.int64, device="cuda")
+    tv = torch.empty(n_tree, dtype=torch.int64, device="cuda")
+    E.gen_keys(args.dist, 1, n_tree, tk, tv, stream)
+    tree.bulk_build(tk, tv, stream)
+    del tv
+    out = {"workload": f"BT_MODE_STM batches of 2^{args.batch_log2} requests, {args.search_pct}% search, "
+                       f"on a 2^{args.tree_log2}-key {args.dist} tree",
+           "stm_combine": not args.no_stm_combine}
+    out.update(stm_run(E, torch, tree, tk, n_b, args.warmup, args.steps, args.dist, args.search_pct, 80_000, stream))
+    print(json.dumps(out), flush=True)
+    tree.close()
+    return 0
+
+
 def run_serve_only(args):
     """Serving only (one GPU): a 2^tree-log2-key tree, then serve_bench for
     the --descent form(s) with --serve-policy."""
@@ -737,6 +770,12 @@ def main():
                          "with the --descent form(s); a small, bounded workload for kernel profiles")
     ap.add_argument("--no-autotune", action="store_true",
                     help="--lookups-only: keep the default launch shapes (no autotuner launches before timing)")
+    ap.add_argument("--stm-only", action="store_true",
+                    help="time only BT_MODE_STM batches (v39 meaning) of 2^batch-log2 requests on a "
+                         "2^tree-log2-key --dist tree, requests drawn from the same law; a bounded workload for "
+                         "kernel profiles")
+    ap.add_argument("--no-stm-combine", action="store_true",
+                    help="--stm-only: run every INSERT as its own transaction (BT_OPT_STM_COMBINE 0)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -747,6 +786,8 @@ def main():
         return run_lookups(args)
     if args.serve_only:
         return run_serve_only(args)
+    if args.stm_only:
+        return run_stm_only(args)
 
     import numpy as np
     import torch
