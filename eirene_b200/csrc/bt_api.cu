@@ -252,16 +252,7 @@ int bt_execute_batch(bt_handle* H, const uint64_t* keys, const uint64_t* vals, c
   const int base = mode & 0xF;
   if (base == BT_MODE_STM) {
     if (bt::tree_join(&h, S(stream)) != cudaSuccess) return BT_ERR_CUDA;
-    const uint8_t* skip = nullptr;
-    const uint64_t* run_vals = vals;
-    if (h.stm_combine &&
-        bt::stm_combine(&h, keys, vals, ops, n, out_vals, out_status, S(stream), &skip, &run_vals) != 0)
-      return BT_ERR_CUDA;
-    cudaError_t e =
-        bt::launch_stm(&h, keys, run_vals, ops, 0xFF, nullptr, nullptr, n, out_vals, out_status, S(stream), skip);
-    if (e == cudaSuccess && h.stm_combine && bt::stm_combine_fixup(&h, ops, n, out_vals, out_status, S(stream)) != 0)
-      return BT_ERR_CUDA;
-    return e == cudaSuccess ? BT_OK : BT_ERR_CUDA;
+    return map_internal(bt::batch_stm(&h, keys, vals, ops, out_vals, out_status, n, S(stream)));
   }
   if (base != BT_MODE_SORTED) return BT_ERR_INVALID_ARG;
   const int engine = (mode & BT_MODE_MERGE_ENGINE) ? 1 : 0;

@@ -414,50 +414,63 @@ __global__ void __launch_bounds__(kThreads) pack_check_kernel(const uint32_t* __
 // index, and `pad` the representative's index (bit 31: the key has a DELETE).
 constexpr uint32_t kDelBit = 1u << 31;
 
-// The write requests (INSERT, DELETE) listed, in no particular order, with
-// one atomic per warp: the later passes then run one thread per write, all
-// of their dependent loads in flight at once, instead of walking every
-// request.  counts->n_ins_req ends as the list's length.
-__global__ void __launch_bounds__(kThreads) combine_list_kernel(const uint8_t* __restrict__ ops, size_t n,
-                                                                uint32_t* __restrict__ list,
-                                                                BatchCounts* __restrict__ counts) {
+// The requests of an STM batch split in two lists, in no particular order,
+// with one atomic per warp and list: the valid GETs (with their keys, for
+// the lookup kernels) and the rest (INSERT, DELETE, invalid op codes and the
+// reserved key, which the STM kernel answers).  counts->n_lookup and
+// counts->n_ins_req end as the lists' lengths.
+__device__ __forceinline__ uint32_t warp_append(uint32_t m, uint32_t* __restrict__ counter) {
   const uint32_t lane = threadIdx.x & 31;
-  // sixteen op codes per load when the array is 16-byte aligned
-  const size_t n16 = ((uintptr_t)ops & 15u) ? 0 : n / 16;
-  const uint4* o16 = reinterpret_cast<const uint4*>(ops);
-  const size_t stride = (size_t)gridDim.x * blockDim.x;
-  // whole warps iterate together (the appends are warp-aggregated)
-  const size_t warp0 = (size_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u);
-  auto append = [&](uint32_t m, size_t first) {
-    const uint32_t c = __popc(m);
-    uint32_t incl = c;
+  const uint32_t c = __popc(m);
+  uint32_t incl = c;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= (uint32_t)o) incl += y;
-    }
-    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-    uint32_t base = 0;
-    if (lane == 31 && total) base = atomicAdd(&counts->n_ins_req, total);
-    base = __shfl_sync(0xffffffffu, base, 31);
-    uint32_t p = base + incl - c;
-    for (int b = 0; m; b++, m >>= 1)
-      if (m & 1u) list[p++] = (uint32_t)(first + (size_t)b);
-  };
-  for (size_t w = warp0; w < n16; w += stride) {
-    const size_t i = w + lane;
-    uint32_t m = 0;
-    if (i < n16) {
-      const uint4 o = o16[i];
-      const uint32_t words[4] = {o.x, o.y, o.z, o.w};
-#pragma unroll
-      for (int j = 0; j < 16; j++) m |= is_write((uint8_t)(words[j / 4] >> (8 * (j % 4)))) << j;
-    }
-    append(m, 16 * i);
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= (uint32_t)o) incl += y;
   }
-  for (size_t w = n16 * 16 + warp0; w < n; w += stride) {
-    const size_t i = w + lane;
-    append(i < n ? is_write(ops[i]) : 0u, i);
+  const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+  uint32_t base = 0;
+  if (lane == 31 && total) base = atomicAdd(counter, total);
+  base = __shfl_sync(0xffffffffu, base, 31);
+  return base + incl - c;  // this lane's first slot
+}
+
+__global__ void __launch_bounds__(kThreads) stm_split_kernel(const uint64_t* __restrict__ keys,
+                                                             const uint8_t* __restrict__ ops, size_t n,
+                                                             uint32_t* __restrict__ get_list,
+                                                             uint64_t* __restrict__ get_keys,
+                                                             uint32_t* __restrict__ wr_list,
+                                                             BatchCounts* __restrict__ counts) {
+  const uint32_t lane = threadIdx.x & 31;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  // whole warps iterate together (the appends are warp-aggregated); four
+  // requests per lane
+  const size_t warp0 = ((size_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u)) * 4;
+  for (size_t w = warp0; w < n; w += stride * 4) {
+    const size_t i0 = w + 4 * (size_t)lane;
+    uint32_t gm = 0, wm = 0;
+    uint64_t k[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      k[j] = kKeyMax;
+      if (i0 + j < n) {
+        k[j] = keys[i0 + j];
+        const bool get = ops[i0 + j] == kOpGet && k[j] != kKeyMax;
+        gm |= (get ? 1u : 0u) << j;
+        wm |= (get ? 0u : 1u) << j;
+      }
+    }
+    uint32_t pg = warp_append(gm, &counts->n_lookup);
+    uint32_t pw = warp_append(wm, &counts->n_ins_req);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      if ((gm >> j) & 1u) {
+        get_list[pg] = (uint32_t)(i0 + j);
+        get_keys[pg++] = k[j];
+      } else if ((wm >> j) & 1u) {
+        wr_list[pw++] = (uint32_t)(i0 + j);
+      }
+    }
   }
 }
 
@@ -473,6 +486,7 @@ __global__ void __launch_bounds__(kThreads) combine_arrive_kernel(const uint64_t
   for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < m; q += (size_t)gridDim.x * blockDim.x) {
     const uint32_t i = list[q];
     const uint8_t op = ops[i];
+    if (op != kOpInsert && op != kOpDelete) continue;  // an invalid request: the STM kernel rejects it
     const uint64_t k = keys[i];
     if (k == kKeyMax) continue;
     uint32_t h = (uint32_t)slot_hash(k) & mask;
@@ -555,6 +569,15 @@ __global__ void __launch_bounds__(kThreads) combine_fixup_kernel(const uint8_t* 
 
 }  // namespace
 
+int stm_split(Handle* h, const uint64_t* keys, const uint8_t* ops, size_t n, cudaStream_t s) {
+  Work& w = h->w;
+  const unsigned g = (unsigned)min((size_t)h->sm_count * 8, (n / 4 + kThreads) / kThreads);
+  if (cudaMemsetAsync(w.counts, 0, sizeof(BatchCounts), s) != cudaSuccess) return -2;
+  stm_split_kernel<<<g, kThreads, 0, s>>>(keys, ops, n, w.get_list, w.ukeys, w.ins_list, w.counts);
+  count_launch();
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
 int stm_combine(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, size_t n,
                 uint64_t* out_vals, uint8_t* out_st, cudaStream_t s, const uint8_t** skip, const uint64_t** cvals) {
   Work& w = h->w;
@@ -566,12 +589,10 @@ int stm_combine(Handle* h, const uint64_t* keys, const uint64_t* vals, const uin
   uint32_t* slot_of = w.f_pos;
   uint32_t* list = w.ins_list;
   const unsigned g = (unsigned)min((size_t)h->sm_count * 8, (n / 4 + kThreads) / kThreads);
-  if (cudaMemsetAsync(c, 0, sizeof(BatchCounts), s) != cudaSuccess) return -2;
-  combine_list_kernel<<<g, kThreads, 0, s>>>(ops, n, list, c);
   front_clear_kernel<<<(unsigned)h->sm_count * 4, kThreads, 0, s>>>(tab, w.f_tab_cap, c);
   combine_arrive_kernel<<<g, kThreads, 0, s>>>(keys, ops, list, tab, c, pred, slot_of);
   combine_mark_kernel<<<g, kThreads, 0, s>>>(keys, vals, ops, list, c, tab, pred, slot_of, sk, cv, out_vals, out_st);
-  count_launch(4);
+  count_launch(3);
   *skip = sk;
   *cvals = cv;
   return cudaGetLastError() == cudaSuccess ? 0 : -2;

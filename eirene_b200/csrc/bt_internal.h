@@ -353,7 +353,15 @@ int delete_apply(Handle* h, size_t n_upper, cudaStream_t s);
 
 // ---- hash front end of the sorted batch (bt_front.cu) ----
 int front_classify(Handle* h, const uint64_t* keys, const uint8_t* ops, size_t n, cudaStream_t s);
-// INSERT combining of a BT_MODE_STM batch: answers the INSERTs combined with
+// a whole BT_MODE_STM batch: its GETs first, by the lookup kernels, then its
+// writes as STM transactions (bt_stm.cu)
+int batch_stm(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, uint64_t* out_vals,
+              uint8_t* out_st, size_t n, cudaStream_t s);
+// BT_MODE_STM batch, split: the valid GETs to w.get_list (keys compacted in
+// w.ukeys, count counts->n_lookup), every other request to w.ins_list
+// (count counts->n_ins_req)
+int stm_split(Handle* h, const uint64_t* keys, const uint8_t* ops, size_t n, cudaStream_t s);
+// INSERT combining over the write list of stm_split: answers the INSERTs combined with
 // an earlier one of their key and returns, per INSERT, a skip byte (1: answered
 // already) and the value the STM kernel stores (in the front end's buffers);
 // stm_combine_fixup after the kernel gives a chain the status of its

@@ -1015,4 +1015,35 @@ cudaError_t launch_stm(Handle* h, const uint64_t* keys, const uint64_t* vals, co
   return cudaGetLastError();
 }
 
+// A BT_MODE_STM batch.  Its requests are concurrent transactions (the v39
+// meaning), so any serial order of them is a valid outcome; this one puts
+// every valid GET first.  Phase 1 answers the GETs with the batch lookup
+// kernels over the pre-batch tree (learned or plain, as the sorted batches):
+// no writer runs beside them, so they need none of the STM path's seqlock
+// validation.  Phase 2 runs the rest (INSERT, DELETE, invalid requests) as
+// STM transactions over their list, the INSERTs of one key combined
+// (BT_OPT_STM_COMBINE).  The reference interleaves GETs and writes in one
+// kernel (src/gpu-stm-tree-v39/bpt-gpustm-kernel.cu:14-256).
+int batch_stm(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, uint64_t* out_vals,
+              uint8_t* out_st, size_t n, cudaStream_t s) {
+  if (n == 0) return 0;
+  Work& w = h->w;
+  if (n > w.cap) return -6;
+  if (stm_split(h, keys, ops, n, s) != 0) return -2;
+  BatchCounts* c = w.counts;
+  const int desc = h->batch_descent >= 0 ? h->batch_descent : h->descent;
+  const cudaError_t e = (desc == 1 && h->L.valid)
+                            ? launch_learned_lookup(h, keys, w.get_list, &c->n_lookup, n, out_vals, out_st, s, w.ukeys)
+                            : launch_search(h, keys, w.get_list, &c->n_lookup, n, out_vals, out_st, s, w.ukeys);
+  if (e != cudaSuccess) return -2;
+  const uint8_t* skip = nullptr;
+  const uint64_t* run_vals = vals;
+  if (h->stm_combine && stm_combine(h, keys, vals, ops, n, out_vals, out_st, s, &skip, &run_vals) != 0) return -2;
+  if (launch_stm(h, keys, run_vals, ops, 0xFF, w.ins_list, &c->n_ins_req, n, out_vals, out_st, s, skip) !=
+      cudaSuccess)
+    return -2;
+  if (h->stm_combine && stm_combine_fixup(h, ops, n, out_vals, out_st, s) != 0) return -2;
+  return 0;
+}
+
 }  // namespace bt
