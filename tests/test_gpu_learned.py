@@ -262,3 +262,37 @@ def test_refit_follows_splits_and_deletes(gpu):
     t.refit()
     lv, ls = lookups(t, qk)
     assert (ls == os_).all() and (lv == ov).all()
+
+
+def test_segment_count_follows_the_leaves(gpu):
+    # default (n_segments 0): one segment line per 64 leaves at each full
+    # training, a power of two, at least 4096; a refit keeps the count; an
+    # explicit count is used as given.  Lookups stay exact either way.
+    for n_keys in (200_000, 12_000_000):
+        keys = O.gen_keys("uniform", 61, n_keys)
+        vals = O.value_of(keys)
+        t = E.BTree(max_keys=1 << 25, max_batch=1 << 18)
+        t.bulk_build(dev(keys), dev(vals))
+        t.retrain()
+        info = t.learned_info()
+        leaves = int(info["n_leaves"])
+        want = 4096
+        while want < (leaves + 63) // 64:
+            want *= 2
+        assert int(info["n_segments"]) == want, (leaves, info["n_segments"])
+        rk, rv, ro = O.gen_requests("uniform", 62, keys, 100_000, 50)
+        run_batch(t, rk, rv, ro, E.MODE_SORTED | E.MODE_MERGE_ENGINE)
+        t.refit()
+        assert int(t.learned_info()["n_segments"]) == want
+        qk, _, _ = O.gen_requests("uniform", 63, keys, 200_000, 100)
+        t.set_descent(True)
+        lv, ls = lookups(t, qk)
+        t.set_descent(False)
+        pv, ps = lookups(t, qk)
+        assert (lv == pv).all() and (ls == ps).all()
+        t.close()
+    t = E.BTree(max_keys=1 << 21, max_batch=1 << 18, n_segments=512)
+    keys = O.gen_keys("uniform", 64, 300_000)
+    t.bulk_build(dev(keys), dev(O.value_of(keys)))
+    t.retrain()
+    assert int(t.learned_info()["n_segments"]) == 512
