@@ -388,6 +388,10 @@ int work_alloc(Work* w, size_t cap) {
   A((void**)&w->f_lk, cap * 8);
   A((void**)&w->f_tk, cap * 8);
   A((void**)&w->f_tv, cap * 4);
+  A((void**)&w->lb_status, scan_lb_words(cap) * 8);
+  A((void**)&w->lb_ctr, 8);
+  ok = ok && cudaMemset(w->lb_status, 0, scan_lb_words(cap) * 8) == cudaSuccess &&
+       cudaMemset(w->lb_ctr, 0, 8) == cudaSuccess;
   if (!ok) {
     work_free(w);
     return -3;
@@ -402,7 +406,7 @@ void work_free(Work* w) {
                 w->m_path,   w->m_vpos,   w->m_leaf,    w->m_isnew,   w->m_pos,     w->m_newk,       w->m_newv,  w->m_nq,
                 w->m_nleaf,  w->m_seg,     w->d_leaf,    w->d_slot,    w->m_ent_a,   w->m_ent_b,   w->m_counts,     w->m_sync,
                 w->ins_ops,  w->f_tab, w->f_flags,
-                w->f_pos,    w->f_list,    w->f_lk,      w->f_tk,      w->f_tv};
+                w->f_pos,    w->f_list,    w->f_lk,      w->f_tk,      w->f_tv,      w->lb_status, w->lb_ctr};
   for (void* p : ps)
     if (p) cudaFree(p);
   *w = Work{};

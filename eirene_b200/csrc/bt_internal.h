@@ -42,6 +42,13 @@ size_t scan_scratch_words(size_t n);
 cudaError_t scan_exclusive_u32(const uint32_t* in, uint32_t* out, size_t n, uint32_t* total_dev, uint32_t* scratch,
                                cudaStream_t s,
                                const uint32_t* n_dev = nullptr);
+// one-launch scan with decoupled look-back (status: scan_lb_words(n_upper)
+// words; ctr: two words, zero before the first call; *epoch: the caller's
+// call counter)
+size_t scan_lb_words(size_t n_upper);
+cudaError_t scan_exclusive_u32_lb(const uint32_t* in, uint32_t* out, size_t n_upper, const uint32_t* n_dev,
+                                  uint32_t* total_dev, uint64_t* status, uint32_t* ctr, uint32_t* epoch,
+                                  uint32_t* err, cudaStream_t s);
 cudaError_t sort_prepare();
 size_t sort_scratch_words(size_t n);
 // tile_threads: 256, 512 or 1024 threads per onesweep tile of 8 items each
@@ -121,6 +128,10 @@ struct Work {
   uint32_t* f_tv = nullptr;      // [cap] index | op << 30 of the touched requests
   // all-INSERT op codes of bt_insert_batch
   uint8_t* ins_ops = nullptr;
+  // look-back scan of the merge engine (scan_exclusive_u32_lb)
+  uint64_t* lb_status = nullptr;
+  uint32_t* lb_ctr = nullptr;
+  uint32_t lb_epoch = 0;
 };
 
 // ---- host-buffer entry points (bt_api.cu) ----

@@ -847,13 +847,17 @@ int merge_group_phase(Handle* h, size_t n_upper, cudaStream_t s) {
   Work& w = h->w;
   MergeCounts* mc = reinterpret_cast<MergeCounts*>(w.m_counts);
   const uint32_t* n_ins = &w.counts->n_ins;
-  if (scan_exclusive_u32(w.m_isnew, w.m_pos, n_upper, &mc->n_new, w.sort_scratch, s, n_ins) != cudaSuccess) return -2;
+  uint32_t* err = &h->tree.ctrl->error;
+  if (scan_exclusive_u32_lb(w.m_isnew, w.m_pos, n_upper, n_ins, &mc->n_new, w.lb_status, w.lb_ctr, &w.lb_epoch, err,
+                            s) != cudaSuccess)
+    return -2;
   const unsigned gb = (unsigned)min((size_t)h->sm_count * 8, (n_upper + 255) / 256);
   merge_compact_kernel<<<gb, 256, 0, s>>>(w.ins_list, n_ins, w.m_isnew, w.m_pos, w.ukeys, w.uvals, w.m_leaf, w.m_newk,
                                           w.m_newv, w.m_nq, w.m_nleaf);
   merge_seg_flags_kernel<<<gb, 256, 0, s>>>(mc, w.m_nleaf, n_upper, w.m_isnew);
   count_launch(2);
-  if (scan_exclusive_u32(w.m_isnew, w.m_pos, n_upper, &mc->n_segs, w.sort_scratch, s, &mc->n_new) != cudaSuccess)
+  if (scan_exclusive_u32_lb(w.m_isnew, w.m_pos, n_upper, &mc->n_new, &mc->n_segs, w.lb_status, w.lb_ctr, &w.lb_epoch,
+                            err, s) != cudaSuccess)
     return -2;
   merge_seg_start_kernel<<<gb, 256, 0, s>>>(mc, w.m_isnew, w.m_pos, w.m_nleaf, w.m_seg, w.m_leaf);
   count_launch();
@@ -866,7 +870,8 @@ int merge_reserve_phase(Handle* h, size_t n_upper, cudaStream_t s) {
   const unsigned gb = (unsigned)min((size_t)h->sm_count * 8, (n_upper + 255) / 256);
   merge_leaf_count_kernel<<<gb, 256, 0, s>>>(h->tree, h->leaf_fill, mc, w.m_seg, w.m_nleaf, n_upper, w.m_isnew);
   count_launch();
-  if (scan_exclusive_u32(w.m_isnew, w.m_pos, n_upper, &mc->n_leaf_entries, w.sort_scratch, s, &mc->n_segs) !=
+  if (scan_exclusive_u32_lb(w.m_isnew, w.m_pos, n_upper, &mc->n_segs, &mc->n_leaf_entries, w.lb_status, w.lb_ctr,
+                            &w.lb_epoch, &h->tree.ctrl->error, s) !=
       cudaSuccess)
     return -2;
   merge_alloc_kernel<<<1, 1, 0, s>>>(h->tree, mc, (uint32_t)w.cap);

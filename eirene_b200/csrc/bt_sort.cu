@@ -130,6 +130,90 @@ __global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(const uint32_t
   }
 }
 
+// Single-pass exclusive scan with decoupled look-back, for a count on the
+// device far below its bound (the merge engine's scans: about 2^18 live
+// entries under a 2^22 bound): one launch where the reduce / single / apply
+// form takes three.  status[t] = epoch << 34 | state << 32 | value, state 1
+// the tile's own sum, 2 its inclusive prefix; each call's epoch makes the
+// words of earlier calls read as not ready, so the array is never cleared.
+// ctr[0] hands tile ids out in the order blocks take them (a tile waits only
+// on tiles taken before it); the last block to finish resets ctr.  The
+// look-back spin is bounded: past kSpinLimit it sets kErrSpin in *err.
+constexpr uint64_t kLbAgg = 1ull << 32, kLbInc = 2ull << 32;
+constexpr uint32_t kLbSpinLimit = 1u << 22;
+
+__global__ void __launch_bounds__(kScanThreads) scan_lb_kernel(const uint32_t* __restrict__ in,
+                                                               uint32_t* __restrict__ out, size_t n_upper,
+                                                               const uint32_t* __restrict__ n_dev,
+                                                               uint32_t* __restrict__ total_out,
+                                                               uint64_t* __restrict__ status,
+                                                               uint32_t* __restrict__ ctr, uint32_t epoch,
+                                                               uint32_t* __restrict__ err) {
+  __shared__ uint32_t ws[32];
+  __shared__ uint32_t tot, s_tile, s_prefix;
+  const size_t n = n_dev ? min(n_upper, (size_t)*n_dev) : n_upper;
+  const size_t n_tiles = (n + kScanTile - 1) / kScanTile;
+  if (threadIdx.x == 0) s_tile = atomicAdd(&ctr[0], 1u);
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  const uint64_t tag = (uint64_t)epoch << 34;
+  if (tile < n_tiles) {
+    const size_t base = (size_t)tile * kScanTile + (size_t)threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++) {
+      v[i] = base + i < n ? in[base + i] : 0;
+      sum += v[i];
+    }
+    uint32_t ex = block_exclusive_scan(sum, ws, &tot);
+    if (threadIdx.x == 0) {
+      uint32_t prefix = 0;
+      if (tile > 0) {
+        st_release(&status[tile], tag | kLbAgg | tot);
+        int64_t t = (int64_t)tile - 1;
+        uint32_t spins = 0;
+        while (t >= 0) {
+          const uint64_t w = ld_acquire(&status[t]);
+          const uint32_t state = (uint32_t)(w >> 32) & 3u;
+          if ((uint32_t)(w >> 34) != epoch || state == 0) {
+            if (++spins > kLbSpinLimit) {
+              if (err) atomicOr(err, kErrSpin);
+              break;
+            }
+            if (spins > 64) __nanosleep(64);
+            continue;
+          }
+          prefix += (uint32_t)w;
+          if (state == 2) break;
+          t--;
+        }
+      }
+      st_release(&status[tile], tag | kLbInc | (uint64_t)(prefix + tot));
+      s_prefix = prefix;
+      if (tile == n_tiles - 1 && total_out) *total_out = prefix + tot;
+    }
+    __syncthreads();
+    ex += s_prefix;
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++) {
+      if (base + i < n) out[base + i] = ex;
+      ex += v[i];
+    }
+  } else if (tile == 0 && threadIdx.x == 0 && total_out) {
+    *total_out = 0;  // nothing to scan
+  }
+  // the last block to finish makes the tile ids start at 0 again
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&ctr[1], 1u) == gridDim.x - 1) {
+      ctr[0] = 0;
+      ctr[1] = 0;
+      __threadfence();
+    }
+  }
+}
+
 // ---------------------------------------------------------------- sort ----
 constexpr int kMaxPasses = 8;
 constexpr uint32_t kFlagAgg = 1u << 30;
@@ -347,6 +431,20 @@ cudaError_t scan_exclusive_u32(const uint32_t* in, uint32_t* out, size_t n, uint
   scan_single_kernel<<<1, kScanThreads, 0, s>>>(scratch, nb, total_dev);
   count_launch();
   scan_apply_kernel<<<(unsigned)nb, kScanThreads, 0, s>>>(in, out, n, n_dev, scratch);
+  count_launch();
+  return cudaGetLastError();
+}
+
+size_t scan_lb_words(size_t n_upper) { return (n_upper + kScanTile - 1) / kScanTile + 1; }
+
+cudaError_t scan_exclusive_u32_lb(const uint32_t* in, uint32_t* out, size_t n_upper, const uint32_t* n_dev,
+                                  uint32_t* total_dev, uint64_t* status, uint32_t* ctr, uint32_t* epoch,
+                                  uint32_t* err, cudaStream_t s) {
+  *epoch = (*epoch + 1) & ((1u << 30) - 1);
+  if (*epoch == 0) *epoch = 1;  // zeroed status words carry epoch 0
+  const size_t blocks = n_upper ? (n_upper + kScanTile - 1) / kScanTile : 1;
+  scan_lb_kernel<<<(unsigned)blocks, kScanThreads, 0, s>>>(in, out, n_upper, n_dev, total_dev, status, ctr, *epoch,
+                                                           err);
   count_launch();
   return cudaGetLastError();
 }
