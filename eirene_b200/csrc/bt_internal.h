@@ -244,7 +244,7 @@ struct Handle {
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   int overlap = 1;
   int lookup_reserve = 0;    // block slots the overlapped lookups leave free (set per batch)
-  int overlap_reserve = 16;  // ... in the overlapped layout (measured: 16 >= 32 > 64 > none)
+  int overlap_reserve = 4;  // ... in the overlapped layout (measured, per 2^22 batch on 2^26 keys: 4 < 8 < 16 < 32 ms, 1.3 % from 4 to 16)
   // host-buffer entry points: staging sets and copy streams
   HostPipe hp;
   int stm_combine = 1;         // BT_MODE_STM batches combine the INSERTs of a key (BT_OPT_STM_COMBINE)

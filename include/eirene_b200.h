@@ -258,7 +258,7 @@ int bt_set_search_group(bt_handle *h, uint32_t lanes);
                                 * 256 nodes) from a per-launch copy in shared memory; 0 all from global */
 #define BT_OPT_OVERLAP 9       /* 1 (default): with the hash front end, the merge engine's locates and grouping of
                                 * the touched requests run on a high-priority side stream while the lookups run
-                                * (the lookups leave 16 block slots free; a value > 1 sets that to value - 1);
+                                * (the lookups leave 4 block slots free; a value > 1 sets that to value - 1);
                                 * 0 one after the other */
 #define BT_OPT_SEARCH_PAIRS 8  /* unsorted plain searches: 2 (default) two requests per lane group in lock step,
                                 * loading only the chosen child id at inner levels (half the bytes of a full
