@@ -773,8 +773,11 @@ int bt_autotune_fill(bt_handle* H, const uint64_t* sample_keys, size_t n, void* 
   bool ok = cudaMalloc(&rk, nb * n * 8) == cudaSuccess && cudaMalloc(&rv, nb * n * 8) == cudaSuccess &&
             cudaMalloc(&ro, nb * n) == cudaSuccess && cudaMalloc(&ov, n * 8) == cudaSuccess &&
             cudaMalloc(&os, n) == cudaSuccess;
+  // 95/5 batches shaped like the sample (uniform fresh keys would all land
+  // beyond the range of a skewed sample, in its two edge leaves)
   for (size_t b = 0; ok && b < nb; b++)
-    ok = bt_gen_requests(0, 0xF111u + b, sample_keys, n, n, 95, rk + b * n, rv + b * n, ro + b * n, s) == BT_OK;
+    ok = bt::gen_sample_requests(0xF111u + b, sample_keys, n, n, 95, rk + b * n, rv + b * n, ro + b * n, s) ==
+         cudaSuccess;
   double best = 1e30;
   uint32_t best_fill = H->h.leaf_fill;
   cudaEvent_t e0 = nullptr, e1 = nullptr;

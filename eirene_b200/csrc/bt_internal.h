@@ -362,6 +362,11 @@ cudaError_t launch_stm(Handle* h, const uint64_t* keys, const uint64_t* vals, co
 int delete_locate(Handle* h, size_t n_upper, cudaStream_t s);
 int delete_apply(Handle* h, size_t n_upper, cudaStream_t s);
 
+// ---- workload generators (bt_workload.cu) ----
+// requests shaped like a key sample of any law (the node-fill tuner's batches)
+cudaError_t gen_sample_requests(uint64_t seed, const uint64_t* sample, size_t n_sample, size_t n, uint32_t search_pct,
+                                uint64_t* keys, uint64_t* vals, uint8_t* ops, cudaStream_t s);
+
 // ---- hash front end of the sorted batch (bt_front.cu) ----
 int front_classify(Handle* h, const uint64_t* keys, const uint8_t* ops, size_t n, cudaStream_t s);
 // a whole BT_MODE_STM batch: its GETs first, by the lookup kernels, then its

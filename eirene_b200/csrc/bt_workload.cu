@@ -114,7 +114,40 @@ __global__ void gen_requests_kernel(int dist, uint64_t seed, const uint64_t* tre
   }
 }
 
+// Requests shaped like a sample of the caller's keys, whatever law they
+// follow: GETs of sample keys (half) or of a sample key with its low 40 bits
+// redrawn, INSERTs of a sample key with its low 40 bits redrawn (fresh keys
+// where the sample is dense; a 2^22-key sample of 64-bit keys is about 2^42
+// apart on average).  The node-fill tuner times its trial batches on these.
+__global__ void gen_sample_requests_kernel(uint64_t seed, const uint64_t* sample, size_t n_sample, size_t n,
+                                           uint32_t search_pct, uint64_t* keys, uint64_t* vals, uint8_t* ops) {
+  constexpr uint64_t kLow = (1ull << 40) - 1;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint64_t r0 = rnd(seed, i, 0), r1 = rnd(seed, i, 1), r2 = rnd(seed, i, 2);
+    const uint64_t base = sample[(r1 >> 1) % n_sample];
+    uint64_t near = (base & ~kLow) | (r2 & kLow);
+    if (near == kKeyMax) near ^= 1;
+    if (r0 % 100 < search_pct) {
+      ops[i] = kOpGet;
+      vals[i] = 0;
+      keys[i] = (r1 & 1) ? base : near;
+    } else {
+      ops[i] = kOpInsert;
+      keys[i] = near;
+      vals[i] = near ^ 0x9E3779B97F4A7C15ull;
+    }
+  }
+}
+
 }  // namespace
+
+cudaError_t gen_sample_requests(uint64_t seed, const uint64_t* sample, size_t n_sample, size_t n, uint32_t search_pct,
+                                uint64_t* keys, uint64_t* vals, uint8_t* ops, cudaStream_t s) {
+  if (n == 0 || n_sample == 0) return cudaSuccess;
+  gen_sample_requests_kernel<<<1184, 256, 0, s>>>(seed, sample, n_sample, n, search_pct, keys, vals, ops);
+  return cudaGetLastError();
+}
 }  // namespace bt
 
 extern "C" {
