@@ -215,6 +215,7 @@ int bt_destroy(bt_handle* H) {
   cudaFree(h.tree.ctrl);
   bt::work_free(&h.w);
   bt::learned_free(&h.L);
+  bt::learned_policy_free(&h.L);
   cudaFree(h.enum_a);
   cudaFree(h.enum_b);
   cudaFree(h.enum_cnt);
@@ -738,6 +739,11 @@ int bt_set_option(bt_handle* H, int option, int64_t value) {
       return BT_OK;
     case BT_OPT_STM_COMBINE:
       H->h.stm_combine = value ? 1 : 0;
+      return BT_OK;
+    case BT_OPT_LEARNED_POLICY:
+      if (value < 0 || value > 2) return BT_ERR_INVALID_ARG;
+      H->h.L.policy = (int)value;
+      H->h.L.stale = false;
       return BT_OK;
     case BT_OPT_LEARNED_MODE:
       if (value < 1 || value > 3) return BT_ERR_INVALID_ARG;

@@ -464,6 +464,7 @@ static int batch_hashed(Handle* h, const uint64_t* keys, const uint64_t* vals, c
   const bool ov = h->overlap != 0;
   const bool early = merge_usable(h, engine);
   const bool defer = early && h->async_write != 0;
+  const bool learned = batch_learned(h, h->batch_descent >= 0 ? h->batch_descent : h->descent, s);
   prof_mark(h, 0, s);
   prof_set_layout(h, (ov ? kLayoutOverlap : 0) | (early ? kLayoutEarly : 0));
   if (front_classify(h, keys, ops, n, s) != 0) return -2;
@@ -511,16 +512,16 @@ static int batch_hashed(Handle* h, const uint64_t* keys, const uint64_t* vals, c
   if (tree_join(h, s) != cudaSuccess) return -2;
   if (ov) prof_mark(h, 1, s);
   cudaError_t e;
-  const int desc = h->batch_descent >= 0 ? h->batch_descent : h->descent;
   h->lookup_reserve = ov ? h->overlap_reserve : 0;
   // the lookups read their keys compacted (w.f_lk[q], written by the front
   // end) instead of through the list (keys[f_list[q]]): one dependent load less
-  if (desc == 1 && h->L.valid)
-    e = launch_learned_lookup(h, keys, w.f_list, &c->n_lookup, n, out_vals, out_st, s, w.f_lk);
+  if (learned)
+    e = launch_learned_lookup(h, keys, w.f_list, &c->n_lookup, n, out_vals, out_st, s, w.f_lk, true);
   else
     e = launch_search(h, keys, w.f_list, &c->n_lookup, n, out_vals, out_st, s, w.f_lk);
   h->lookup_reserve = 0;
   if (e != cudaSuccess) return -2;
+  if (learned) learned_sample(h, s);
   if (ov) {
     prof_mark(h, kEvLookupEnd, s);
     if (cudaStreamWaitEvent(s, h->join_ev, 0) != cudaSuccess) return -2;
@@ -564,6 +565,7 @@ int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const ui
   if (n > w.cap || n > kIdxMask) return -6;
   if (h->front_end == 1) return batch_hashed(h, keys, vals, ops, out_vals, out_st, n, engine, s);
   if (tree_join(h, s) != cudaSuccess) return -2;
+  const bool learned = batch_learned(h, h->batch_descent >= 0 ? h->batch_descent : h->descent, s);
   uint64_t* sk = nullptr;
   uint32_t* sv = nullptr;
   prof_mark(h, 0, s);
@@ -584,8 +586,7 @@ int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const ui
   // search phase on the pre-batch tree, then the insert phase
   prof_mark(h, 2, s);
   cudaError_t e;
-  const int desc = h->batch_descent >= 0 ? h->batch_descent : h->descent;
-  if (desc == 1 && h->L.valid)
+  if (learned)
     e = launch_learned_search(h, w.ukeys, w.get_list, &w.counts->n_get, n, w.uans, w.uans_st, s,
                               h->sorted_search != 0);
   else if (h->sorted_search)
@@ -593,6 +594,7 @@ int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const ui
   else
     e = launch_search(h, w.ukeys, w.get_list, &w.counts->n_get, n, w.uans, w.uans_st, s);
   if (e != cudaSuccess) return -2;
+  if (learned) learned_sample(h, s);
   prof_mark(h, 3, s);
   if (insert_phase(h, n, engine, s) != 0) return -2;
   prof_mark(h, 4, s);

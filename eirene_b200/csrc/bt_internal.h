@@ -194,7 +194,19 @@ struct Learned {
   // requests the learned lookup leaves to the plain descent, and their count
   uint32_t* miss = nullptr;
   uint32_t* n_miss = nullptr;
+  uint64_t* miss_keys = nullptr;  // their keys, compacted beside them
   size_t miss_cap = 0;
+  // adaptive use (BT_OPT_LEARNED_POLICY): the device gate (LearnedGate,
+  // bt_learned.cuh), and for policy 2 its stale word sampled into
+  // page-locked memory on a side stream, read by a later batch once done
+  int policy = 1;                       // 0 always, 1 plain once stale, 2 and refit
+  struct LearnedGate* gate = nullptr;
+  bool stale = false;                   // the sampled gate was closed
+  uint32_t batches = 0;                 // batches since the last fit
+  uint32_t* sample = nullptr;           // page-locked gate word
+  bool pending = false;
+  cudaEvent_t sample_ev = nullptr, lookups_ev = nullptr;
+  cudaStream_t sample_stream = nullptr;
 };
 
 struct Handle {
@@ -441,13 +453,19 @@ int autotune(Handle* h, const uint64_t* keys, size_t n, cudaStream_t s, double* 
 // ---- learned predictor (bt_learned.cu) ----
 int learned_retrain(Handle* h, cudaStream_t s, bool refit = false);
 void learned_free(Learned* L);
+// whether a batch's lookups use the learned descent (the handle's choice,
+// then the adaptive policy; policy 2 may refit here), and the counter sample
+// to take after them
+bool batch_learned(Handle* h, int desc, cudaStream_t s);
+void learned_sample(Handle* h, cudaStream_t s);
+void learned_policy_free(Learned* L);
 cudaError_t launch_learned_search(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev,
                                   size_t n, uint64_t* out_vals, uint8_t* out_st, cudaStream_t s, bool sorted);
 // unsorted learned lookups (paired groups, misses deferred to a plain descent
 // over a miss list); n <= max_batch when list or n_dev is given
 cudaError_t launch_learned_lookup(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev,
                                   size_t n, uint64_t* out_vals, uint8_t* out_st, cudaStream_t s,
-                                  const uint64_t* ckeys = nullptr);
+                                  const uint64_t* ckeys = nullptr, bool gated = false);
 int learned_mlp_grad(Handle* h, const float* params, const float* x, const float* y, size_t n, float* grad_out,
                      float* loss_out, cudaStream_t s);
 

@@ -420,12 +420,46 @@ __global__ void __launch_bounds__(256, 6) learned_search_kernel(DevTree t, Learn
 // together: with one atomic per miss, a tree whose leaves moved since
 // training (a fifth of the lookups missing) serialised millions of atomics
 // on the list's one counter.
-__device__ __forceinline__ void append_miss(uint32_t* __restrict__ miss, uint32_t* __restrict__ n_miss, uint32_t r) {
+__device__ __forceinline__ void append_miss(uint32_t* __restrict__ miss, uint64_t* __restrict__ miss_keys,
+                                            uint32_t* __restrict__ n_miss, uint32_t r, uint64_t key) {
   const cooperative_groups::coalesced_group c = cooperative_groups::coalesced_threads();
   uint32_t base = 0;
   if (c.thread_rank() == 0) base = atomicAdd(n_miss, (uint32_t)c.size());
   base = c.shfl(base, 0);
   miss[base + c.thread_rank()] = r;
+  miss_keys[base + c.thread_rank()] = key;
+}
+
+// A stale gate: the launch skips the model and lists every request as a miss
+// (request index and key), so the plain descent answers them all.  Returns
+// true when it did (the caller returns).
+__device__ __forceinline__ bool gate_pass_all(const LearnedDev& M, const uint64_t* __restrict__ qkeys,
+                                              const uint32_t* __restrict__ list, const uint64_t* __restrict__ ckeys,
+                                              size_t n, uint32_t* __restrict__ miss, uint32_t* __restrict__ n_miss) {
+  if (!M.gate || !M.gate->stale) return false;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) {
+    const uint32_t r = list ? list[q] : (uint32_t)q;
+    miss[q] = r;
+    M.miss_keys[q] = ckeys ? ckeys[q] : qkeys[r];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *n_miss = (uint32_t)n;
+  return true;
+}
+
+__global__ void learned_judge_kernel(const Ctrl* __restrict__ ctrl, LearnedGate* __restrict__ g) {
+  const unsigned long long hits = ctrl->learned_hits, falls = ctrl->learned_fallbacks;
+  if (!g->have_base || hits < g->base_hits || falls < g->base_falls) {  // first look, or counters reset
+    g->base_hits = hits;
+    g->base_falls = falls;
+    g->have_base = 1;
+    return;
+  }
+  const unsigned long long dh = hits - g->base_hits, df = falls - g->base_falls;
+  if (dh + df < kGateWindow) return;  // the window grows
+  if (df * kGateMissDen > dh + df) g->stale = 1;
+  g->base_hits = hits;
+  g->base_falls = falls;
 }
 
 template <int G, int R>
@@ -448,6 +482,7 @@ __global__ void __launch_bounds__(256) learned_lookup_kernel(DevTree t, LearnedD
   const uint32_t g = lane % G;
   const uint32_t gmask = group_mask<G>(lane);
   const size_t n = n_dev ? (size_t)*n_dev : n_host;
+  if (gate_pass_all(M, qkeys, list, ckeys, n, miss, n_miss)) return;
   const size_t groups = ((size_t)gridDim.x * blockDim.x) / G;
   const int L = (int)M.n_leaves;
   const int p_hi = L + 1 - W > 0 ? L + 1 - W : 0;  // the table holds L + 1 entries (sentinel last)
@@ -554,7 +589,7 @@ __global__ void __launch_bounds__(256) learned_lookup_kernel(DevTree t, LearnedD
         probe += (uint32_t)(pc[j] > (int)pslot[j] ? pc[j] - (int)pslot[j] : (int)pslot[j] - pc[j]);
       } else {
         falls++;
-        append_miss(miss, n_miss, r[j]);
+        append_miss(miss, M.miss_keys, n_miss, r[j], key[j]);
       }
     }
   }
@@ -606,6 +641,7 @@ __global__ void __launch_bounds__(kPipeThreads) learned_pipe_kernel(DevTree t, L
   const uint32_t g = lane % G;
   const uint32_t gmask = group_mask<G>(lane);
   const size_t n = n_dev ? (size_t)*n_dev : n_host;
+  if (gate_pass_all(M, qkeys, list, ckeys, n, miss, n_miss)) return;
   const size_t groups = ((size_t)gridDim.x * blockDim.x) / G;
   const int L = (int)M.n_leaves;
   const int p_hi = L + 1 - W > 0 ? L + 1 - W : 0;
@@ -641,7 +677,7 @@ __global__ void __launch_bounds__(kPipeThreads) learned_pipe_kernel(DevTree t, L
         probe += distF;
       } else {
         falls++;
-        append_miss(miss, n_miss, rF);
+        append_miss(miss, M.miss_keys, n_miss, rF, kF);
       }
     }
     // E -> F: rank the key in its leaf row; load the value or the right fence
@@ -760,6 +796,10 @@ void learned_free(Learned* L) {
   cudaFree(L->seg_of);
   L->seg_of = nullptr;
   cudaFree(L->miss);
+  cudaFree(L->miss_keys);
+  cudaFree(L->gate);
+  L->miss_keys = nullptr;
+  L->gate = nullptr;
   if (L->host_words) cudaFreeHost(L->host_words);
   L->host_words = nullptr;
   L->miss = nullptr;
@@ -774,6 +814,85 @@ void learned_free(Learned* L) {
   L->leaf_cap = 0;
   L->seg_cap = 0;
   L->valid = false;
+}
+
+// ---- adaptive use in the batches (BT_OPT_LEARNED_POLICY) ----
+// The model is trained on the leaves as they are; a batch's inserts split
+// leaves, and a lookup whose predicted leaf has split since the fit falls
+// back to the plain descent (one learned kernel's work wasted).  On a tree
+// that the batches grow fast against its size (2^23 keys and 2^22-request
+// 95/5 batches: 28 % fallbacks over 25 batches; any 50/50 mix) the learned
+// form then loses to the plain one.  So the device judges the miss rate
+// after every learned lookup launch (learned_judge_kernel) and, once it is
+// stale, the learned kernels pass every request to the plain descent until
+// the model is fitted again (LearnedGate): the decision is in stream order,
+// however far the host has queued batches ahead.  Policy 2 also refits on
+// its own: the host reads the gate through a page-locked word copied on a
+// side stream after the lookups (read only once its copy has completed, so
+// no batch waits for it) and refits kRefitAfter batches after the last fit.
+constexpr uint32_t kRefitAfter = 8;
+
+void learned_policy_free(Learned* L) {
+  if (L->sample_stream) cudaStreamSynchronize(L->sample_stream);
+  if (L->sample) cudaFreeHost(L->sample);
+  if (L->sample_ev) cudaEventDestroy(L->sample_ev);
+  if (L->lookups_ev) cudaEventDestroy(L->lookups_ev);
+  if (L->sample_stream) cudaStreamDestroy(L->sample_stream);
+  L->sample = nullptr;
+  L->sample_ev = L->lookups_ev = nullptr;
+  L->sample_stream = nullptr;
+  L->pending = false;
+}
+
+static void learned_fitted(Learned& L) {
+  L.stale = false;
+  L.batches = 0;
+}
+
+bool batch_learned(Handle* h, int desc, cudaStream_t s) {
+  Learned& L = h->L;
+  if (desc != 1 || !L.valid) return false;
+  if (L.policy != 2) return true;
+  L.batches++;
+  if (L.pending && cudaEventQuery(L.sample_ev) == cudaSuccess) {
+    L.pending = false;
+    if (L.sample[0] != 0) L.stale = true;  // the gate closed
+  }
+  cudaGetLastError();  // a copy not done yet (cudaErrorNotReady) is not an error
+  if (L.stale && L.batches >= kRefitAfter) {
+    // the refit reads the leaves: after the previous batch's deferred merge
+    if (tree_join(h, s) != cudaSuccess || learned_retrain(h, s, true) != 0) return false;
+  }
+  return true;
+}
+
+void learned_sample(Handle* h, cudaStream_t s) {
+  Learned& L = h->L;
+  if (L.policy != 2 || L.pending || !L.gate) return;
+  if (!L.sample) {
+    if (cudaHostAlloc(&L.sample, 16, cudaHostAllocDefault) != cudaSuccess) {
+      L.sample = nullptr;
+      cudaGetLastError();
+      return;
+    }
+    L.sample[0] = 0;
+    if (cudaEventCreateWithFlags(&L.sample_ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&L.lookups_ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&L.sample_stream, cudaStreamNonBlocking) != cudaSuccess) {
+      learned_policy_free(&L);
+      cudaGetLastError();
+      return;
+    }
+  }
+  // the gate word, on a side stream behind the lookups: the batch's own stream does not wait
+  L.sample[0] = 0;
+  if (cudaEventRecord(L.lookups_ev, s) != cudaSuccess || cudaStreamWaitEvent(L.sample_stream, L.lookups_ev, 0) != cudaSuccess ||
+      cudaMemcpyAsync(L.sample, &L.gate->stale, 4, cudaMemcpyDeviceToHost, L.sample_stream) != cudaSuccess ||
+      cudaEventRecord(L.sample_ev, L.sample_stream) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  L.pending = true;
 }
 
 // device scratch layout inside Learned:
@@ -828,11 +947,21 @@ static int learned_reserve(Learned* L, size_t n_leaves, uint32_t n_seg) {
 }
 
 static int miss_reserve(Learned* L, size_t cap) {
+  if (!L->gate) {
+    if (cudaMalloc(&L->gate, sizeof(LearnedGate)) != cudaSuccess) {
+      L->gate = nullptr;
+      return -3;
+    }
+    if (cudaMemset(L->gate, 0, sizeof(LearnedGate)) != cudaSuccess) return -3;
+  }
   if (cap <= L->miss_cap) return 0;
   cudaFree(L->miss);
+  cudaFree(L->miss_keys);
   L->miss = nullptr;
+  L->miss_keys = nullptr;
   L->miss_cap = 0;
-  if (cudaMalloc(&L->miss, (cap + 64) * 4) != cudaSuccess) return -3;
+  if (cudaMalloc(&L->miss, (cap + 64) * 4) != cudaSuccess || cudaMalloc(&L->miss_keys, cap * 8) != cudaSuccess)
+    return -3;
   L->n_miss = L->miss + cap;
   L->miss_cap = cap;
   return 0;
@@ -970,6 +1099,9 @@ int learned_retrain(Handle* h, cudaStream_t s, bool refit) {
   }
   L.refits += refit ? 1 : 0;
   L.valid = true;
+  learned_fitted(L);
+  // the gate opens again: the new fit is judged afresh
+  if (cudaMemsetAsync(L.gate, 0, sizeof(LearnedGate), s) != cudaSuccess) return -2;
   return 0;
 }
 
@@ -983,6 +1115,8 @@ static LearnedDev dev_view(const Learned& L) {
   M.n_leaves = L.n_leaves;
   M.n_seg = L.n_segments;
   M.window = L.window;
+  M.gate = L.policy != 0 ? L.gate : nullptr;
+  M.miss_keys = L.miss_keys;
   return M;
 }
 
@@ -1023,9 +1157,11 @@ static cudaError_t lookup_launch(Handle* h, const LearnedDev& M, const uint64_t*
   return cudaGetLastError();
 }
 
+// gated: the batch paths' lookups, which the adaptive gate may hand to the
+// plain descent (bt_search_batch keeps bt_set_descent's choice)
 cudaError_t launch_learned_lookup(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev,
                                   size_t n, uint64_t* out_vals, uint8_t* out_st, cudaStream_t s,
-                                  const uint64_t* ckeys) {
+                                  const uint64_t* ckeys, bool gated) {
   if (!list) ckeys = nullptr;
   if (n == 0) return cudaSuccess;
   Learned& L = h->L;
@@ -1040,7 +1176,8 @@ cudaError_t launch_learned_lookup(Handle* h, const uint64_t* qkeys, const uint32
     }
     return cudaSuccess;
   }
-  const LearnedDev M = dev_view(L);
+  LearnedDev M = dev_view(L);
+  if (!gated) M.gate = nullptr;
   if (cudaMemsetAsync(L.n_miss, 0, 4, s) != cudaSuccess) return cudaGetLastError();
   cudaError_t e;
   const int G = h->learned_group, R = h->learned_mode;
@@ -1054,12 +1191,16 @@ cudaError_t launch_learned_lookup(Handle* h, const uint64_t* qkeys, const uint32
   else e = R == 3 ? BT_LL(4, 0) : R == 2 ? BT_LL(4, 2) : BT_LL(4, 1);
 #undef BT_LL
   if (e != cudaSuccess) return e;
-  // the misses: plain descent over the miss list, one resident wave
+  // the misses: plain descent over the miss list (keys compacted beside it),
+  // one resident wave
   const int saved = h->lookup_reserve;
   h->lookup_reserve = saved > 1 ? saved : 1;
-  e = launch_search(h, qkeys, L.miss, L.n_miss, n, out_vals, out_st, s);
+  e = launch_search(h, qkeys, L.miss, L.n_miss, n, out_vals, out_st, s, L.miss_keys);
   h->lookup_reserve = saved;
-  return e;
+  if (e != cudaSuccess || !M.gate) return e;
+  learned_judge_kernel<<<1, 1, 0, s>>>(h->tree.ctrl, L.gate);
+  count_launch();
+  return cudaGetLastError();
 }
 
 cudaError_t launch_learned_search(Handle* h, const uint64_t* qkeys, const uint32_t* list, const uint32_t* n_dev,

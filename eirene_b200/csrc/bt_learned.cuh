@@ -74,6 +74,19 @@ __device__ __forceinline__ float mlp_group(const float* p, float x, uint32_t g, 
   return y + p[3 * kHidden];
 }
 
+// The adaptive gate (BT_OPT_LEARNED_POLICY 1 and 2): a judge kernel after
+// each learned lookup launch compares the hit and fallback counters with
+// the last judged ones; once a window of at least kGateWindow lookups missed
+// more than 1 in kGateMissDen, `stale` stays set until the model is fitted
+// again, and the learned kernels hand every request to the plain descent.
+constexpr unsigned long long kGateWindow = 65536;
+constexpr unsigned long long kGateMissDen = 20;  // 5 %
+struct LearnedGate {
+  unsigned long long base_hits, base_falls;
+  uint32_t stale;
+  uint32_t have_base;
+};
+
 struct LearnedDev {
   const LeafEnt* tab;
   const SegParam* seg;
@@ -83,6 +96,8 @@ struct LearnedDev {
   uint32_t n_leaves;
   uint32_t n_seg;
   uint32_t window;
+  const LearnedGate* gate;  // nullptr: always use the model (policy 0)
+  uint64_t* miss_keys;      // the misses' keys, beside their request indices
 };
 
 // Predicted leaf for `key`: stage 1 (MLP) -> segment -> line -> one probe of

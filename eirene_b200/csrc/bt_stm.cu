@@ -1029,13 +1029,15 @@ int batch_stm(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8
   if (n == 0) return 0;
   Work& w = h->w;
   if (n > w.cap) return -6;
+  const bool learned = batch_learned(h, h->batch_descent >= 0 ? h->batch_descent : h->descent, s);
   if (stm_split(h, keys, ops, n, s) != 0) return -2;
   BatchCounts* c = w.counts;
-  const int desc = h->batch_descent >= 0 ? h->batch_descent : h->descent;
-  const cudaError_t e = (desc == 1 && h->L.valid)
-                            ? launch_learned_lookup(h, keys, w.get_list, &c->n_lookup, n, out_vals, out_st, s, w.ukeys)
+  const cudaError_t e = learned
+                            ? launch_learned_lookup(h, keys, w.get_list, &c->n_lookup, n, out_vals, out_st, s, w.ukeys,
+                                                    true)
                             : launch_search(h, keys, w.get_list, &c->n_lookup, n, out_vals, out_st, s, w.ukeys);
   if (e != cudaSuccess) return -2;
+  if (learned) learned_sample(h, s);
   const uint8_t* skip = nullptr;
   const uint64_t* run_vals = vals;
   if (h->stm_combine && stm_combine(h, keys, vals, ops, n, out_vals, out_st, s, &skip, &run_vals) != 0) return -2;

@@ -296,3 +296,47 @@ def test_segment_count_follows_the_leaves(gpu):
     t.bulk_build(dev(keys), dev(O.value_of(keys)))
     t.retrain()
     assert int(t.learned_info()["n_segments"]) == 512
+
+
+@pytest.mark.parametrize("policy", [0, 1, 2])
+def test_learned_policy_on_a_fast_growing_tree(gpu, policy):
+    # 50/50 batches of 120 K requests on a 150 K-key tree: leaves split in
+    # every batch and the learned lookups of a batch miss more and more.
+    # Policy 0 keeps the learned descent; policy 1 answers with the plain
+    # descent once the sampled miss rate passes 5 %, until bt_refit; policy 2
+    # refits by itself 8 batches after the last fit.  Every batch is exact.
+    keys = O.gen_keys("uniform", 71, 150_000)
+    vals = O.value_of(keys)
+    t = E.BTree(max_keys=1 << 23, max_batch=1 << 18)
+    t.bulk_build(dev(keys), dev(vals))
+    o = O.OracleTree()
+    o.bulk_build(keys, vals)
+    t.retrain()
+    t.set_descent(True)
+    t.set_option(E.OPT_LEARNED_POLICY, policy)
+    merge = E.MODE_SORTED | E.MODE_MERGE_ENGINE
+    used = []
+    prev = t.stats()["learned_hits"] + t.stats()["learned_fallbacks"]
+    for b in range(14):
+        if policy == 1 and b == 10:
+            t.refit()
+        rk, rv, ro = O.gen_requests("uniform", 80 + b, keys, 120_000, 50)
+        ov, os_ = o.execute_merged(rk, rv, ro, engine=O.ENGINE_MERGE)
+        gv, gs = run_batch(t, rk, rv, ro, merge)
+        assert (gs == os_).all() and (gv == ov).all(), b
+        st = t.stats()
+        now = st["learned_hits"] + st["learned_fallbacks"]
+        used.append(now > prev)  # this batch's lookups went through the model
+        prev = now
+    if policy == 0:
+        assert all(used)
+    elif policy == 1:
+        assert used[0] and not all(used[1:10])  # dropped once stale
+        assert not any(used[6:10])
+        assert used[10]  # back after the refit
+    else:
+        assert used[0] and not all(used[1:8])
+        assert any(used[8:])  # refit by itself, learned again
+    gk, gv = dump(t)
+    ok, ovv = o.dump()
+    assert (gk == ok).all() and (gv == ovv).all()
