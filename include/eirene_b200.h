@@ -281,12 +281,14 @@ int bt_set_search_group(bt_handle *h, uint32_t lanes);
                                  * concurrent requests, which is what the v39 meaning allows; keys the batch
                                  * also DELETEs are not combined); 0 runs every INSERT as its own transaction,
                                  * like the reference (src/gpu-stm-tree-v39/bpt-gpustm-kernel.cu:41-56) */
-#define BT_OPT_LEARNED_POLICY 16 /* batches with the learned descent: 0 use it as chosen; 1 (default) sample its
-                                  * miss rate (no synchronisation) and, once more than 5 % of its lookups fall back
-                                  * to the plain descent because leaves split since the fit, answer the batches with
-                                  * the plain descent until the next bt_retrain / bt_refit; 2 the same, and refit by
-                                  * itself once 8 batches have run since the last fit.  Answers are the same in
-                                  * every case; bt_search_batch keeps bt_set_descent's choice */
+#define BT_OPT_LEARNED_POLICY 16 /* batches with the learned descent: 0 use it as chosen; 1 (default) the device
+                                  * judges the miss rate after each batch's learned lookups and, once more than 5 %
+                                  * of a window of 65536 fall back to the plain descent (leaves split since the fit),
+                                  * the batches hand every lookup to the plain descent until the next bt_retrain /
+                                  * bt_refit (in stream order: batches already queued follow it too); 2 the same,
+                                  * and the library refits by itself once 8 batches have run since the last fit.
+                                  * Answers are the same in every case; bt_search_batch keeps bt_set_descent's
+                                  * choice */
 #define BT_OPT_SORT_TILE 14     /* radix sort tile of sorted batches: 256, 512 (default) or 1024 threads x 8 keys,
                                  * for whole batches and for the hash front end's touched requests alike
                                  * (bt_autotune picks the two separately) */
