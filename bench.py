@@ -625,12 +625,13 @@ def run_serve_only(args):
 
 # ----------------------------------------------------------------------------
 def oracle_check(args, n_b, check_out, tk, draw):
-    """Replays the run's batches through the CPU oracle in the order the GPU
-    ran them (each form: warm-up batches, then the timed ones; the plain form
-    first) and compares each form's first timed batch request by request.
-    The batches are drawn again by the device generator, which is
-    deterministic (`draw(seed)` returns host arrays), and copied to the host
-    one at a time; the tree keys are the device's `tk`."""
+    """Replays batches through the CPU oracle in the order the GPU ran them
+    and compares the first timed batch of each run request by request.  Each
+    run (a form's one-call-per-batch run, and its bt_execute_batches run)
+    starts from the freshly built tree, as on the GPU, and its warm-up
+    batches come first.  The batches are drawn again by the device
+    generator, which is deterministic (`draw(seed)` returns host arrays), and
+    copied to the host one at a time; the tree keys are the device's `tk`."""
     import numpy as np
 
     from oracle import oracle as O
@@ -638,27 +639,22 @@ def oracle_check(args, n_b, check_out, tk, draw):
     threads = os.cpu_count() or 1
     t0 = time.time()
     keys = tk.cpu().numpy().view(np.uint64)
-    tree = O.OracleTree(24, 24)
-    tree.bulk_build(keys, O.value_of(keys))
+    vals = O.value_of(keys)
     engine = O.ENGINE_MERGE if args.engine == "merge" else O.ENGINE_STM
     out = {}
-    for form in ("plain", "learned"):
-        if form not in check_out:
-            continue
-        seed0, gv, gs = check_out[form]
-        n_run = args.warmup + args.steps
+    for run, (seed0, gv, gs) in check_out.items():
+        tree = O.OracleTree(24, 24)
+        tree.bulk_build(keys, vals)
         for i in range(args.warmup + 1):
             rk, rv, ro = draw(seed0 + i)
             ov, os_ = tree.execute_merged(rk, rv, ro, engine, threads)
             if i == args.warmup:
                 bad = int(((ov != gv) | (os_ != gs)).sum())
-                out[form] = {"requests": n_b, "mismatches": bad}
-        # the rest of the form's timed batches, so the next form starts from the same tree
-        for i in range(args.warmup + 1, n_run):
-            tree.execute_merged(*draw(seed0 + i), engine, threads)
+                out[run] = {"requests": n_b, "mismatches": bad}
+        del tree
     out["oracle_s"] = time.time() - t0
-    out["batch"] = "first timed batch of each form, answers (value + status) per request"
-    del tree
+    out["batch"] = ("first timed batch of each run (forms one call per batch; *_pipelined: bt_execute_batches), "
+                    "answers (value + status) per request")
     return out
 
 
@@ -958,8 +954,55 @@ def main():
             check_out["learned" if learned else "plain"] = (seed0, first[0].cpu().numpy().view(np.uint64),
                                                             first[1].cpu().numpy())
         del batches
+        pipe = None
+        if sharded is None:
+            # throughput through bt_execute_batches: fresh batches of the same
+            # kind, each with its own answer arrays, on a freshly built tree
+            # (and model), batch j + 1's front part beside batch j's tree part;
+            # a --retrain-every schedule runs as chunks with the refit between
+            rebuild_tree()
+            built[0] = False
+            tree.set_descent(False)
+            if learned:
+                tree.retrain(stream)
+                tree.set_descent(True)
+            tree.set_option(E.OPT_BATCH_DESCENT, 1 if learned else 0)
+            batches = make_batches(seed0 + 500)
+            outs = [(torch.empty(n_b, dtype=torch.int64, device="cuda"),
+                     torch.empty(n_b, dtype=torch.uint8, device="cuda")) for _ in batches]
+            tree.execute_many(batches[:args.warmup], outs[:args.warmup], mode=MODE, stream=stream)
+            tree.sync(stream)
+            torch.cuda.synchronize()
+            tree.reset_stats()
+            barrier()
+            sampler = ClockSampler(local)
+            sampler.start()
+            l0 = E.launch_count()
+            p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            K = args.retrain_every if (learned and args.retrain_every > 0) else args.steps
+            p0.record(stream)
+            for c0 in range(args.warmup, args.warmup + args.steps, K):
+                c1 = min(c0 + K, args.warmup + args.steps)
+                tree.execute_many(batches[c0:c1], outs[c0:c1], mode=MODE, stream=stream)
+                if K < args.steps and (c1 - args.warmup) % K == 0:
+                    if args.retrain_mode == "refit":
+                        tree.refit(stream)
+                    else:
+                        tree.retrain(stream)
+            tree.sync(stream)
+            p1.record(stream)
+            torch.cuda.synchronize()
+            pipe = {"total_ms": p0.elapsed_time(p1), "launches": E.launch_count() - l0, "clocks": sampler.stop(),
+                    "stats": tree.stats()}
+            if args.check:
+                a, b = outs[args.warmup]
+                check_out[("learned" if learned else "plain") + "_pipelined"] = (
+                    seed0 + 500, a.cpu().numpy().view(np.uint64), b.cpu().numpy())
+            barrier()
+            del batches, outs
         return {"total_ms": total_ms, "step_ms": step_ms, "phases": phases, "counts": counts,
-                "launches": launches, "clocks": clocks, "stats": st, "learned_info": info, "tune": tune}
+                "launches": launches, "clocks": clocks, "stats": st, "learned_info": info, "tune": tune,
+                "pipe": pipe}
 
     forms = {}
     if args.descent in ("plain", "both"):
@@ -971,7 +1014,10 @@ def main():
             forms["learned_error"] = str(e)
     # headline: the faster of the two forms (both are reported under "forms")
     cands = [f for f in ("plain", "learned") if f in forms]
-    head = min(cands, key=lambda f: forms[f]["total_ms"])
+    def form_ms(F):  # the throughput run: bt_execute_batches when it ran, else one call per batch
+        return F["pipe"]["total_ms"] if F.get("pipe") else F["total_ms"]
+
+    head = min(cands, key=lambda f: form_ms(forms[f]))
     R = forms[head]
 
     # unsorted point lookups (bt_search_batch on random keys): plain vs learned
@@ -1001,7 +1047,7 @@ def main():
         del rk, rv, ro
     except E.BTError as ex:
         random_lookup["error"] = str(ex)
-    total_ms = allmax(R["total_ms"])
+    total_ms = allmax(form_ms(R))
     value = world * n_b * args.steps / (total_ms / 1e3) / 1e6
 
     # ---- roofline of the dominant phase
@@ -1197,7 +1243,7 @@ def main():
         except Exception as ex:  # reported, not fatal
             same_box = {"error": str(ex)}
 
-    launches = allsum(R["launches"])
+    launches = allsum((R["pipe"] or R)["launches"])
     check = None
     if args.check and world == 1 and check_out:
         def draw(seed):
@@ -1221,9 +1267,14 @@ def main():
             ms = sorted(F["step_ms"])
             tot = F["total_ms"]
             s = F["stats"]
+            P = F.get("pipe")
+            ptot = form_ms(F)
             return {
-                "value": n_b * steps / (tot / 1e3) / 1e6, "ms_per_step": tot / steps,
+                "value": n_b * steps / (ptot / 1e3) / 1e6, "ms_per_step": ptot / steps,
                 "p50_batch_ms": ms[len(ms) // 2], "p99_batch_ms": ms[min(len(ms) - 1, int(0.99 * len(ms)))],
+                "per_call": {"value": n_b * steps / (tot / 1e3) / 1e6, "ms_per_step": tot / steps},
+                "pipelined": ({"learned_hits": P["stats"]["learned_hits"],
+                               "learned_fallbacks": P["stats"]["learned_fallbacks"]} if P else None),
                 "phases_ms_per_step": {p: F["phases"][p] / max(1, F["phases"]["batches"])
                                        for p in ("sort", "merge", "search", "insert", "writeback")},
                 "stm_aborts": s["aborts"], "stm_commits": s["commits"],
@@ -1249,11 +1300,15 @@ def main():
                 "learned_retrain_every": args.retrain_every,
                 "node_fill": fill,
                 "learned_retrain_mode": args.retrain_mode,
+                "throughput": ("bt_execute_batches over the timed batches (batch j + 1's front part beside batch "
+                               "j's lookups and writes); p50 / p99 batch latency and phases: the same kind of "
+                               "batches, one bt_execute_batch call each (forms.*.per_call)"
+                               if R.get("pipe") else "one bt_execute_batch call per batch"),
             },
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": e2e,
-            "clocks": R["clocks"],
+            "clocks": (R["pipe"] or R)["clocks"],
             "gpu_launches": launches,
             "p50_batch_ms": form_summary(R)["p50_batch_ms"],
             "p99_batch_ms": form_summary(R)["p99_batch_ms"],

@@ -103,7 +103,7 @@ EXPORTS = [
     "bt_serve_config_init", "bt_serve_start", "bt_submit", "bt_poll", "bt_wait", "bt_serve_get_stats", "bt_serve_stop",
     "bt_route_batch", "bt_unroute_results", "bt_save", "bt_load", "bt_range_batch", "bt_sync", "bt_save_image", "bt_load_image",
     "bt_refit", "bt_execute_batch_host_async", "bt_host_wait", "bt_serve_batch_times", "bt_autotune_fill",
-    "bt_execute_batch_host_packed_async",
+    "bt_execute_batch_host_packed_async", "bt_execute_batches",
 ]
 MAX_SHARDS = 256
 OPT_SORTED_SEARCH, OPT_RETRY_LIMIT, OPT_TRAIN_STEPS, OPT_SORTED_LEAF_VALS, OPT_BATCH_DESCENT = 1, 2, 3, 4, 5
@@ -159,6 +159,7 @@ def lib():
                                             ctypes.POINTER(ctypes.c_uint64)],
             "bt_execute_batch_host_packed_async": [_P, _P, _P, _P, _SZ, _P, _P, _SZ, ctypes.c_int, _P,
                                                    ctypes.POINTER(ctypes.c_uint64)],
+            "bt_execute_batches": [_P, _SZ, _P, _P, _P, _P, _P, _P, ctypes.c_int, _P],
             "bt_host_wait": [_P, ctypes.c_uint64],
             "bt_serve_batch_times": [_P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64),
                                      ctypes.POINTER(ctypes.c_uint64)],
@@ -328,6 +329,19 @@ class BTree:
                                                         _stream_ptr(stream), ctypes.byref(t)),
                "bt_execute_batch_host_packed_async")
         return t.value
+
+    def execute_many(self, batches, outs, mode=MODE_SORTED, stream=None):
+        """bt_execute_batches: `batches` a list of (keys, vals, ops) CUDA
+        tensors, `outs` a list of (out_vals, out_status), one per batch."""
+        m = len(batches)
+        if len(outs) != m:
+            raise ValueError("one (out_vals, out_status) per batch")
+        arr = lambda xs: (ctypes.c_void_p * max(m, 1))(*[_ptr(x) for x in xs])
+        ns = (_SZ * max(m, 1))(*[b[0].numel() for b in batches])
+        _check(lib().bt_execute_batches(self._h, m, arr([b[0] for b in batches]), arr([b[1] for b in batches]),
+                                        arr([b[2] for b in batches]), arr([o[0] for o in outs]),
+                                        arr([o[1] for o in outs]), ns, mode, _stream_ptr(stream)),
+               "bt_execute_batches")
 
     def wait_host(self, ticket: int):
         _check(lib().bt_host_wait(self._h, ticket), "bt_host_wait")

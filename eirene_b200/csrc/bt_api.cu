@@ -2,6 +2,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -216,6 +217,9 @@ int bt_destroy(bt_handle* H) {
   bt::work_free(&h.w);
   bt::learned_free(&h.L);
   bt::learned_policy_free(&h.L);
+  if (h.front_stream) cudaStreamDestroy(h.front_stream);
+  for (cudaEvent_t e : {h.front_done[0], h.front_done[1], h.tree_done[0], h.tree_done[1], h.pipe_ev})
+    if (e) cudaEventDestroy(e);
   cudaFree(h.enum_a);
   cudaFree(h.enum_b);
   cudaFree(h.enum_cnt);
@@ -258,6 +262,49 @@ int bt_execute_batch(bt_handle* H, const uint64_t* keys, const uint64_t* vals, c
   if (base != BT_MODE_SORTED) return BT_ERR_INVALID_ARG;
   const int engine = (mode & BT_MODE_MERGE_ENGINE) ? 1 : 0;
   return map_internal(bt::batch_sorted(&h, keys, vals, ops, out_vals, out_status, n, engine, S(stream)));
+}
+
+int bt_execute_batches(bt_handle* H, size_t count, const uint64_t* const* keys, const uint64_t* const* vals,
+                       const uint8_t* const* ops, uint64_t* const* out_vals, uint8_t* const* out_status,
+                       const size_t* n, int mode, void* stream) {
+  if (!H) return BT_ERR_INVALID_ARG;
+  if (count == 0) return BT_OK;
+  if (!keys || !vals || !ops || !out_vals || !out_status || !n) return BT_ERR_INVALID_ARG;
+  bt::Handle& h = H->h;
+  for (size_t j = 0; j < count; j++) {
+    if (n[j] == 0) continue;
+    if (!keys[j] || !vals[j] || !ops[j] || !out_vals[j] || !out_status[j]) return BT_ERR_INVALID_ARG;
+    if (n[j] > h.w.cap) return BT_ERR_BATCH_TOO_LARGE;
+  }
+  const int base = mode & 0xF;
+  if (base != BT_MODE_SORTED && base != BT_MODE_STM) return BT_ERR_INVALID_ARG;
+  DeviceGuard g(h.device);
+  if (base != BT_MODE_SORTED || h.front_end != 1) {
+    // only sorted batches with the hash front end have a front part to run ahead
+    for (size_t j = 0; j < count; j++) {
+      const int rc = bt_execute_batch(H, keys[j], vals[j], ops[j], out_vals[j], out_status[j], n[j], mode, stream);
+      if (rc != BT_OK) return rc;
+    }
+    return BT_OK;
+  }
+  // empty batches do nothing: drop them
+  std::vector<const uint64_t*> k, v;
+  std::vector<const uint8_t*> o;
+  std::vector<uint64_t*> ov;
+  std::vector<uint8_t*> os;
+  std::vector<size_t> m;
+  for (size_t j = 0; j < count; j++)
+    if (n[j]) {
+      k.push_back(keys[j]);
+      v.push_back(vals[j]);
+      o.push_back(ops[j]);
+      ov.push_back(out_vals[j]);
+      os.push_back(out_status[j]);
+      m.push_back(n[j]);
+    }
+  const int engine = (mode & BT_MODE_MERGE_ENGINE) ? 1 : 0;
+  return map_internal(bt::batches_pipelined(&h, m.size(), k.data(), v.data(), o.data(), ov.data(), os.data(), m.data(),
+                                            engine, S(stream)));
 }
 
 // ---- host-buffer entry points ----

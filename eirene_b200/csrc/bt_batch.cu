@@ -18,6 +18,8 @@
 // the latest INSERT before it; the run reaches the tree as one INSERT (last
 // value) or one GET.  The unique count never leaves the device (the reference
 // copies it to the host and synchronises, v38 bpt-gpustm-kernel.cu:303-306).
+#include <utility>
+
 #include <cuda_runtime.h>
 
 #include "bt_block.cuh"
@@ -400,7 +402,49 @@ int work_alloc(Work* w, size_t cap) {
   return 0;
 }
 
+// the fields of Work that make up a BatchSet
+#define BT_SET_FIELDS(X) X(counts) X(f_list) X(f_lk) X(ukeys) X(uvals) X(ins_list) X(get_list) X(del_list) X(pend) \
+  X(k_a) X(k_b) X(v_a) X(v_b)
+
+void work_swap_set(Work* w) {
+#define BT_SWAP(f) std::swap(w->f, w->alt.f);
+  BT_SET_FIELDS(BT_SWAP)
+#undef BT_SWAP
+  w->alt_in = !w->alt_in;
+}
+
+int work_alt_alloc(Work* w) {
+  if (w->alt.counts) return 0;
+  const size_t cap = w->cap;
+  BatchSet& a = w->alt;
+  bool ok = cudaMalloc((void**)&a.counts, sizeof(BatchCounts)) == cudaSuccess &&
+            cudaMalloc((void**)&a.f_list, cap * 4) == cudaSuccess && cudaMalloc((void**)&a.f_lk, cap * 8) == cudaSuccess &&
+            cudaMalloc((void**)&a.ukeys, cap * 8) == cudaSuccess && cudaMalloc((void**)&a.uvals, cap * 8) == cudaSuccess &&
+            cudaMalloc((void**)&a.ins_list, cap * 4) == cudaSuccess &&
+            cudaMalloc((void**)&a.get_list, cap * 4) == cudaSuccess &&
+            cudaMalloc((void**)&a.del_list, cap * 4) == cudaSuccess &&
+            cudaMalloc((void**)&a.pend, cap * 4) == cudaSuccess && cudaMalloc((void**)&a.k_a, cap * 8) == cudaSuccess &&
+            cudaMalloc((void**)&a.k_b, cap * 8) == cudaSuccess && cudaMalloc((void**)&a.v_a, cap * 4) == cudaSuccess &&
+            cudaMalloc((void**)&a.v_b, cap * 4) == cudaSuccess;
+  if (!ok) {
+#define BT_FREE_ALT(f) cudaFree(a.f);
+    BT_SET_FIELDS(BT_FREE_ALT)
+#undef BT_FREE_ALT
+    a = BatchSet{};
+    return -3;
+  }
+  return 0;
+}
+
 void work_free(Work* w) {
+  if (w->alt_in) work_swap_set(w);  // the fields hold the first set again
+  {
+    BatchSet& a = w->alt;
+#define BT_FREE_ALT(f) if (a.f) cudaFree(a.f);
+    BT_SET_FIELDS(BT_FREE_ALT)
+#undef BT_FREE_ALT
+    a = BatchSet{};
+  }
   void* ps[] = {w->k_a,      w->k_b,       w->v_a,       w->v_b,       w->sort_scratch, w->ukeys,   w->uvals,
                 w->uans,     w->uans_st,   w->ins_list,  w->get_list,  w->del_list, w->pend,         w->tiles,   w->counts,
                 w->m_path,   w->m_vpos,   w->m_leaf,    w->m_isnew,   w->m_pos,     w->m_newk,       w->m_newv,  w->m_nq,
@@ -456,8 +500,49 @@ static int answers_ready(Handle* h, cudaStream_t s) {
 // and inner merge run on tree_stream, so the caller's stream goes on to the
 // next batch, whose front end and sort need neither the tree nor the merge
 // scratch; its first tree access waits for tree_ev.
-static int batch_hashed(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops,
-                        uint64_t* out_vals, uint8_t* out_st, size_t n, int engine, cudaStream_t s) {
+//
+// A hash-front-end batch in two parts.  The front part reads no tree: the
+// classification, the touched requests' sort and (unless they wait for the
+// values on the side stream) the merge passes.  The tree part does the
+// rest.  A single batch runs them back to back on `s`; bt_execute_batches
+// runs batch j + 1's front part on its own stream beside batch j's tree
+// part, each batch with its set of the buffers the two parts share
+// (Work::sets).
+struct FrontPart {
+  uint64_t* sk = nullptr;
+  uint32_t* sv = nullptr;
+  uint32_t n_tiles = 0;
+  bool passes_done = false;
+};
+
+static int hashed_front(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, uint64_t* out_vals,
+                        uint8_t* out_st, size_t n, cudaStream_t s, bool passes, FrontPart& fp) {
+  Work& w = h->w;
+  BatchCounts* c = w.counts;
+  const uint32_t* n_touch = &c->n_touch;
+  if (front_classify(h, keys, ops, n, s) != 0) return -2;
+  // the touched requests' sort and merge passes need no tree: they run at
+  // full width (beside the previous batch's deferred merge)
+  if (radix_sort_pairs(w.f_tk, w.f_tv, nullptr, w.k_a, w.v_a, w.k_b, w.v_b, n, 0, 64, w.sort_scratch, s, &fp.sk,
+                       &fp.sv, &h->tree.ctrl->error, n_touch, h->sort_threads_touch) != cudaSuccess)
+    return -2;
+  fp.n_tiles = (uint32_t)pass_tiles(n);
+  prof_mark(h, h->overlap != 0 ? kEvSortEnd : 1, s);
+  if (passes) {
+    merge_pass1<<<fp.n_tiles, kThreads, 0, s>>>(fp.sk, fp.sv, vals, n, n_touch, w.tiles);
+    count_launch();
+    merge_pass2<<<1, 1024, 0, s>>>(w.tiles, fp.n_tiles, n_touch, c);
+    count_launch();
+    merge_pass3<<<fp.n_tiles, kThreads, 0, s>>>(fp.sk, fp.sv, vals, n, n_touch, w.tiles, w.ukeys, w.uvals,
+                                                w.ins_list, w.get_list, w.del_list, w.pend, out_vals, out_st);
+    count_launch();
+    fp.passes_done = true;
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+static int hashed_tree(Handle* h, const uint64_t* keys, const uint64_t* vals, uint64_t* out_vals, uint8_t* out_st,
+                       size_t n, int engine, cudaStream_t s, const FrontPart& fp) {
   Work& w = h->w;
   BatchCounts* c = w.counts;
   const uint32_t* n_touch = &c->n_touch;
@@ -465,41 +550,30 @@ static int batch_hashed(Handle* h, const uint64_t* keys, const uint64_t* vals, c
   const bool early = merge_usable(h, engine);
   const bool defer = early && h->async_write != 0;
   const bool learned = batch_learned(h, h->batch_descent >= 0 ? h->batch_descent : h->descent, s);
-  prof_mark(h, 0, s);
-  prof_set_layout(h, (ov ? kLayoutOverlap : 0) | (early ? kLayoutEarly : 0));
-  if (front_classify(h, keys, ops, n, s) != 0) return -2;
-  // the touched requests' sort and merge passes need no tree: they run on
-  // `s` at full width (beside the previous batch's deferred merge)
-  uint64_t* sk = nullptr;
-  uint32_t* sv = nullptr;
-  if (radix_sort_pairs(w.f_tk, w.f_tv, nullptr, w.k_a, w.v_a, w.k_b, w.v_b, n, 0, 64, w.sort_scratch, s, &sk, &sv,
-                       &h->tree.ctrl->error, n_touch, h->sort_threads_touch) != cudaSuccess)
-    return -2;
-  const uint32_t n_tiles = (uint32_t)pass_tiles(n);
-  prof_mark(h, ov ? kEvSortEnd : 1, s);
   // the locates (side stream) run beside the lookups (`s`); so do the merge
   // passes when the values are still being copied in (vals_wait): the
   // lookups do not need them
   cudaStream_t s2 = ov ? h->hi_stream : s;
-  const bool pass_side = ov && (h->vals_wait != nullptr || h->vals_remote);
   auto fork = [&]() {
     // a stale prefix table is rebuilt before the fork, so that the locates
     // (side stream) and the lookups (`s`) both come after the rebuild
     if (early && h->use_pfx && (tree_join(h, s) != cudaSuccess || ensure_pfx(h, s) != cudaSuccess)) return false;
     return cudaEventRecord(h->fork_ev, s) == cudaSuccess && cudaStreamWaitEvent(s2, h->fork_ev, 0) == cudaSuccess;
   };
-  if (pass_side && !fork()) return -2;
-  cudaStream_t sp = pass_side ? s2 : s;
-  if (wait_vals(h, sp) != 0) return -2;
-  merge_pass1<<<n_tiles, kThreads, 0, sp>>>(sk, sv, vals, n, n_touch, w.tiles);
-  count_launch();
-  merge_pass2<<<1, 1024, 0, sp>>>(w.tiles, n_tiles, n_touch, c);
-  count_launch();
-  merge_pass3<<<n_tiles, kThreads, 0, sp>>>(sk, sv, vals, n, n_touch, w.tiles, w.ukeys, w.uvals, w.ins_list,
-                                            w.get_list, w.del_list, w.pend, out_vals, out_st);
-  count_launch();
-  if (cudaGetLastError() != cudaSuccess) return -2;
-  if (ov && !pass_side && !fork()) return -2;
+  if (!fp.passes_done) {
+    cudaStream_t sp = ov ? s2 : s;
+    if ((ov && !fork()) || wait_vals(h, sp) != 0) return -2;
+    merge_pass1<<<fp.n_tiles, kThreads, 0, sp>>>(fp.sk, fp.sv, vals, n, n_touch, w.tiles);
+    count_launch();
+    merge_pass2<<<1, 1024, 0, sp>>>(w.tiles, fp.n_tiles, n_touch, c);
+    count_launch();
+    merge_pass3<<<fp.n_tiles, kThreads, 0, sp>>>(fp.sk, fp.sv, vals, n, n_touch, w.tiles, w.ukeys, w.uvals,
+                                                 w.ins_list, w.get_list, w.del_list, w.pend, out_vals, out_st);
+    count_launch();
+    if (cudaGetLastError() != cudaSuccess) return -2;
+  } else if (ov && !fork()) {
+    return -2;
+  }
   if (early) {
     if (tree_join(h, s2) != cudaSuccess || delete_locate(h, n, s2) != 0 || merge_locate_phase(h, s2) != 0 ||
         merge_group_phase(h, n, s2) != 0)
@@ -531,7 +605,7 @@ static int batch_hashed(Handle* h, const uint64_t* keys, const uint64_t* vals, c
   if (!early) {
     if (insert_phase(h, n, engine, s) != 0) return -2;
     prof_mark(h, 4, s);
-    writeback_kernel<<<wb_blocks, 256, 0, s>>>(sv, w.pend, n, n_touch, w.uans, w.uans_st, out_vals, out_st);
+    writeback_kernel<<<wb_blocks, 256, 0, s>>>(fp.sv, w.pend, n, n_touch, w.uans, w.uans_st, out_vals, out_st);
     count_launch();
     prof_mark(h, 5, s);
     return answers_ready(h, s) != 0 || cudaGetLastError() != cudaSuccess ? -2 : 0;
@@ -539,7 +613,7 @@ static int batch_hashed(Handle* h, const uint64_t* keys, const uint64_t* vals, c
   if (merge_update_phase(h, n, s) != 0 || delete_apply(h, n, s) != 0 || merge_reserve_phase(h, n, s) != 0)
     return -2;
   prof_mark(h, kEvWbStart, s);
-  writeback_kernel<<<wb_blocks, 256, 0, s>>>(sv, w.pend, n, n_touch, w.uans, w.uans_st, out_vals, out_st);
+  writeback_kernel<<<wb_blocks, 256, 0, s>>>(fp.sv, w.pend, n, n_touch, w.uans, w.uans_st, out_vals, out_st);
   count_launch();
   prof_mark(h, 4, s);
   if (answers_ready(h, s) != 0 || cudaGetLastError() != cudaSuccess) return -2;
@@ -556,6 +630,77 @@ static int batch_hashed(Handle* h, const uint64_t* keys, const uint64_t* vals, c
     h->tree_pending = true;
   }
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+static int batch_hashed(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops,
+                        uint64_t* out_vals, uint8_t* out_st, size_t n, int engine, cudaStream_t s) {
+  const bool ov = h->overlap != 0;
+  const bool pass_side = ov && (h->vals_wait != nullptr || h->vals_remote);
+  prof_mark(h, 0, s);
+  prof_set_layout(h, (ov ? kLayoutOverlap : 0) | (merge_usable(h, engine) ? kLayoutEarly : 0));
+  FrontPart fp;
+  if (hashed_front(h, keys, vals, ops, out_vals, out_st, n, s, !pass_side, fp) != 0) return -2;
+  return hashed_tree(h, keys, vals, out_vals, out_st, n, engine, s, fp);
+}
+
+// Several hash-front-end batches, their inputs all ready on `s`, in order:
+// batch j + 1's front part (classification, sort, merge passes: no tree) on
+// front_stream beside batch j's tree part on `s`, the two with alternate
+// buffer sets.  A front part waits for the tree part that last used its
+// set; a tree part waits for its own front part.  The answers and the tree
+// are the batches' one by one.  Phases are not recorded (they would span
+// two streams).
+int batches_pipelined(Handle* h, size_t count, const uint64_t* const* keys, const uint64_t* const* vals,
+                      const uint8_t* const* ops, uint64_t* const* out_vals, uint8_t* const* out_st, const size_t* n,
+                      int engine, cudaStream_t s) {
+  Work& w = h->w;
+  if (count == 0) return 0;
+  for (size_t j = 0; j < count; j++)
+    if (n[j] == 0 || n[j] > w.cap || n[j] > kIdxMask) return -6;
+  if (work_alt_alloc(&w) != 0) return -3;
+  if (!h->front_stream) {
+    bool ok = cudaStreamCreateWithFlags(&h->front_stream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&h->pipe_ev, cudaEventDisableTiming) == cudaSuccess;
+    for (int p = 0; ok && p < 2; p++)
+      ok = cudaEventCreateWithFlags(&h->front_done[p], cudaEventDisableTiming) == cudaSuccess &&
+           cudaEventCreateWithFlags(&h->tree_done[p], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) return -2;
+  }
+  cudaStream_t F = h->front_stream;
+  const bool prof = h->prof;
+  h->prof = false;
+  auto use = [&](int p) {
+    if ((int)w.alt_in != p) work_swap_set(&w);
+  };
+  int rc = 0;
+  FrontPart fp[2];
+  // the inputs are ready in `s`'s order at this point
+  if (cudaEventRecord(h->pipe_ev, s) != cudaSuccess || cudaStreamWaitEvent(F, h->pipe_ev, 0) != cudaSuccess) rc = -2;
+  for (size_t j = 0; j <= count && rc == 0; j++) {
+    if (j < count) {
+      const int p = (int)(j & 1);
+      use(p);
+      fp[p] = FrontPart{};
+      if ((j >= 2 && cudaStreamWaitEvent(F, h->tree_done[p], 0) != cudaSuccess) ||
+          hashed_front(h, keys[j], vals[j], ops[j], out_vals[j], out_st[j], n[j], F, true, fp[p]) != 0 ||
+          cudaEventRecord(h->front_done[p], F) != cudaSuccess)
+        rc = -2;
+    }
+    if (rc == 0 && j >= 1) {
+      const size_t i = j - 1;
+      const int q = (int)(i & 1);
+      use(q);
+      if (cudaStreamWaitEvent(s, h->front_done[q], 0) != cudaSuccess ||
+          hashed_tree(h, keys[i], vals[i], out_vals[i], out_st[i], n[i], engine, s, fp[q]) != 0 ||
+          cudaEventRecord(h->tree_done[q], s) != cudaSuccess)
+        rc = -2;
+    }
+  }
+  use(0);
+  h->prof = prof;
+  // whatever the front stream did is ordered before `s`'s later work
+  if (cudaEventRecord(h->pipe_ev, F) != cudaSuccess || cudaStreamWaitEvent(s, h->pipe_ev, 0) != cudaSuccess) rc = -2;
+  return rc;
 }
 
 int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, uint64_t* out_vals,

@@ -80,6 +80,26 @@ struct TopInfo {
 
 struct TileSummary;  // bt_batch.cu
 
+// The buffers the front part and the tree part of a hash-front-end batch
+// share (bt_batch.cu): a second set lets bt_execute_batches run one batch's
+// front part beside the previous batch's tree part.  Work's own fields hold
+// the set in use; `alt` the other.
+struct BatchSet {
+  BatchCounts* counts = nullptr;
+  uint32_t* f_list = nullptr;
+  uint64_t* f_lk = nullptr;
+  uint64_t* ukeys = nullptr;
+  uint64_t* uvals = nullptr;
+  uint32_t* ins_list = nullptr;
+  uint32_t* get_list = nullptr;
+  uint32_t* del_list = nullptr;
+  uint32_t* pend = nullptr;
+  uint64_t* k_a = nullptr;
+  uint64_t* k_b = nullptr;
+  uint32_t* v_a = nullptr;
+  uint32_t* v_b = nullptr;
+};
+
 struct Work {
   size_t cap = 0;  // requests
   uint64_t* k_a = nullptr;
@@ -132,7 +152,11 @@ struct Work {
   uint64_t* lb_status = nullptr;
   uint32_t* lb_ctr = nullptr;
   uint32_t lb_epoch = 0;
+  BatchSet alt;        // the second set (allocated by the first bt_execute_batches)
+  bool alt_in = false; // Work's fields hold the second set
 };
+int work_alt_alloc(Work* w);
+void work_swap_set(Work* w);  // exchange the fields' set with `alt`
 
 // ---- host-buffer entry points (bt_api.cu) ----
 // Three staging sets: batch i + 1's inputs are copied in and batch i - 1's
@@ -256,6 +280,10 @@ struct Handle {
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   int overlap = 1;
   int lookup_reserve = 0;    // block slots the overlapped lookups leave free (set per batch)
+  // bt_execute_batches: the front parts' stream and its events
+  cudaStream_t front_stream = nullptr;
+  cudaEvent_t front_done[2] = {nullptr, nullptr}, tree_done[2] = {nullptr, nullptr};
+  cudaEvent_t pipe_ev = nullptr;
   int overlap_reserve = 4;  // ... in the overlapped layout (measured, per 2^22 batch on 2^26 keys: 4 < 8 < 16 < 32 ms, 1.3 % from 4 to 16)
   // host-buffer entry points: staging sets and copy streams
   HostPipe hp;
@@ -423,6 +451,11 @@ int work_alloc(Work* w, size_t cap);
 void work_free(Work* w);
 int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, uint64_t* out_vals,
                  uint8_t* out_st, size_t n, int engine, cudaStream_t s);
+// several hash-front-end batches whose inputs are all ready on `s`: batch
+// j + 1's front part beside batch j's tree part (bt_batch.cu)
+int batches_pipelined(Handle* h, size_t count, const uint64_t* const* keys, const uint64_t* const* vals,
+                      const uint8_t* const* ops, uint64_t* const* out_vals, uint8_t* const* out_st, const size_t* n,
+                      int engine, cudaStream_t s);
 
 // ---- segmented leaf merge (bt_merge.cu) ----
 int merge_engine(Handle* h, size_t n_upper, cudaStream_t s);

@@ -187,6 +187,20 @@ int bt_execute_batch_host_packed_async(bt_handle *h, const uint64_t *keys, const
  * (its deferred leaf merge may still run; bt_sync orders after that). */
 int bt_host_wait(bt_handle *h, uint64_t ticket);
 
+/* `count` batches in order, their inputs all ready on `stream` (device
+ * pointers in host arrays of `count`; batch j has n[j] requests and its own
+ * output arrays).  Same answers and tree as `count` calls of
+ * bt_execute_batch; with BT_MODE_SORTED and the hash front end, batch j + 1's
+ * classification, sort and merge passes (which read no tree) run on an
+ * internal stream beside batch j's lookups and writes, with a second set of
+ * per-batch buffers (allocated at the first call, about 70 B per request of
+ * capacity).  Other modes run the batches one by one.  Phases are not
+ * recorded (bt_profile).  No reference counterpart: the reference runs its
+ * batches one after another (src/gpu-stm-tree-v38/bpt-gpustm.cpp, gpu_work). */
+int bt_execute_batches(bt_handle *h, size_t count, const uint64_t *const *keys, const uint64_t *const *vals,
+                       const uint8_t *const *ops, uint64_t *const *out_vals, uint8_t *const *out_status,
+                       const size_t *n, int mode, void *stream);
+
 /* Convenience wrappers: all-GET and all-INSERT batches in BT_MODE_SORTED,
  * the reference's single-mission input (prepareInput(file, mission),
  * src/tree.h:34). */
