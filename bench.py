@@ -770,6 +770,9 @@ def main():
                     help="time only BT_MODE_STM batches (v39 meaning) of 2^batch-log2 requests on a "
                          "2^tree-log2-key --dist tree, requests drawn from the same law; a bounded workload for "
                          "kernel profiles")
+    ap.add_argument("--no-host-front-overlap", action="store_true",
+                    help="e2e: run each host batch whole on the stream (BT_OPT_HOST_FRONT_OVERLAP 0) instead of "
+                         "its front part beside the previous host batch's tree part")
     ap.add_argument("--no-stm-combine", action="store_true",
                     help="--stm-only: run every INSERT as its own transaction (BT_OPT_STM_COMBINE 0)")
     args = ap.parse_args()
@@ -836,6 +839,7 @@ def main():
         tree = E.BTree(max_keys=pool_keys, max_batch=n_b, device=local, search_group=args.search_group,
                        n_segments=args.segments)
     tree.set_option(E.OPT_FRONT_END, 1 if args.front_end == "hash" else 0)
+    tree.set_option(E.OPT_HOST_FRONT_OVERLAP, 0 if args.no_host_front_overlap else 1)
     tk = torch.empty(n_tree, dtype=torch.int64, device="cuda")
     tv = torch.empty(n_tree, dtype=torch.int64, device="cuda")
     E.gen_keys(args.dist, 1 + rank, n_tree, tk, tv, stream)
@@ -1211,6 +1215,7 @@ def main():
                "d2h_bytes_per_step": n_b * 9,
                "host_wall_ms_per_step": wall_ms / e2e_steps,
                "pipelined": sharded is None,
+               "front_overlap": sharded is None and not args.no_host_front_overlap,
                "entry_point": "bt_execute_batch_host_packed_async" if packed else "sharded execute",
                "steps": e2e_steps, "descent": head,
                "full_values": {"value": world * n_b * e2e_steps / (full_ms / 1e3) / 1e6,

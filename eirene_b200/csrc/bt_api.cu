@@ -27,6 +27,13 @@ struct DeviceGuard {
   }
 };
 
+// DeviceGuard for an entry point that may use the handle's buffers: it also
+// closes the chain of host batches (the next host batch's front part then
+// waits for everything queued before it)
+struct EntryGuard : DeviceGuard {
+  explicit EntryGuard(bt_handle* H) : DeviceGuard(H->h.device) { H->h.chain_open = false; }
+};
+
 inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
 int map_internal(int rc) {
@@ -206,7 +213,7 @@ int bt_create(const bt_config* cfg_in, bt_handle** out) {
 
 int bt_destroy(bt_handle* H) {
   if (!H) return BT_ERR_INVALID_ARG;
-  DeviceGuard g(H->h.device);
+  EntryGuard g(H);
   bt::Handle& h = H->h;
   cudaDeviceSynchronize();
   cudaFree(h.tree.keys);
@@ -218,7 +225,8 @@ int bt_destroy(bt_handle* H) {
   bt::learned_free(&h.L);
   bt::learned_policy_free(&h.L);
   if (h.front_stream) cudaStreamDestroy(h.front_stream);
-  for (cudaEvent_t e : {h.front_done[0], h.front_done[1], h.tree_done[0], h.tree_done[1], h.pipe_ev})
+  for (cudaEvent_t e : {h.front_done[0], h.front_done[1], h.tree_done[0], h.tree_done[1], h.pipe_ev,
+                        h.chain_gate})
     if (e) cudaEventDestroy(e);
   cudaFree(h.enum_a);
   cudaFree(h.enum_b);
@@ -240,7 +248,7 @@ int bt_destroy(bt_handle* H) {
 
 int bt_bulk_build(bt_handle* H, const uint64_t* keys, const uint64_t* vals, size_t n, void* stream) {
   if (!H || (n && (!keys || !vals))) return BT_ERR_INVALID_ARG;
-  DeviceGuard g(H->h.device);
+  EntryGuard g(H);
   H->h.L.valid = false;
   if (bt::tree_join(&H->h, S(stream)) != cudaSuccess) return BT_ERR_CUDA;
   return map_internal(bt::tree_bulk_build(&H->h, keys, vals, n, S(stream)));
@@ -253,7 +261,7 @@ int bt_execute_batch(bt_handle* H, const uint64_t* keys, const uint64_t* vals, c
   if (!keys || !ops || !out_vals || !out_status || !vals) return BT_ERR_INVALID_ARG;
   bt::Handle& h = H->h;
   if (n > h.w.cap) return BT_ERR_BATCH_TOO_LARGE;
-  DeviceGuard g(h.device);
+  EntryGuard g(H);
   const int base = mode & 0xF;
   if (base == BT_MODE_STM) {
     if (bt::tree_join(&h, S(stream)) != cudaSuccess) return BT_ERR_CUDA;
@@ -278,7 +286,7 @@ int bt_execute_batches(bt_handle* H, size_t count, const uint64_t* const* keys, 
   }
   const int base = mode & 0xF;
   if (base != BT_MODE_SORTED && base != BT_MODE_STM) return BT_ERR_INVALID_ARG;
-  DeviceGuard g(h.device);
+  EntryGuard g(H);
   if (base != BT_MODE_SORTED || h.front_end != 1) {
     // only sorted batches with the hash front end have a front part to run ahead
     for (size_t j = 0; j < count; j++) {
@@ -436,18 +444,30 @@ static int host_submit(bt_handle* H, const uint64_t* keys, const uint64_t* vals,
                          cudaEventRecord(st.vals_ev, in) != cudaSuccess)) {
     return BT_ERR_CUDA;
   }
-  if (cudaStreamWaitEvent(s, st.in_ev, 0) != cudaSuccess) return BT_ERR_CUDA;
-  if (base == BT_MODE_SORTED) {
+  const int engine = (mode & BT_MODE_MERGE_ENGINE) ? 1 : 0;
+  // the front part on its own stream once the op codes and keys are in,
+  // beside the previous host batch's tree part; the merge passes once the
+  // values are in (a full value array: beside the lookups instead)
+  const bool chained = base == BT_MODE_SORTED && h.front_end == 1 && h.host_front_overlap && !remote && !h.prof;
+  if (chained) {
+    h.ans_ready = st.ans_ev;
+    rc = map_internal(bt::batch_chained(&h, st.keys, st.vals, st.ops, st.out_vals, st.out_st, n, engine, s,
+                                        st.in_ev, st.vals_ev, !packed));
+    h.ans_ready = nullptr;
+  } else if (cudaStreamWaitEvent(s, st.in_ev, 0) != cudaSuccess) {
+    return BT_ERR_CUDA;
+  } else if (base == BT_MODE_SORTED) {
+    h.chain_open = false;
     h.vals_wait = remote ? nullptr : st.vals_ev;
     h.vals_remote = remote != nullptr;
     h.ans_ready = st.ans_ev;
-    const int engine = (mode & BT_MODE_MERGE_ENGINE) ? 1 : 0;
     rc = map_internal(bt::batch_sorted(&h, st.keys, remote ? remote : st.vals, st.ops, st.out_vals, st.out_st, n,
                                        engine, s));
     h.vals_wait = nullptr;
     h.vals_remote = false;
     h.ans_ready = nullptr;
   } else {
+    h.chain_open = false;
     rc = cudaStreamWaitEvent(s, st.vals_ev, 0) == cudaSuccess
              ? bt_execute_batch(H, st.keys, st.vals, st.ops, st.out_vals, st.out_st, n, mode, s)
              : BT_ERR_CUDA;
@@ -524,7 +544,7 @@ int bt_execute_batch_host(bt_handle* H, const uint64_t* keys, const uint64_t* va
   if (n == 0) return BT_OK;
   if (!keys || !ops || !out_vals || !out_status || !vals) return BT_ERR_INVALID_ARG;
   if (n > H->h.w.cap) return BT_ERR_BATCH_TOO_LARGE;
-  DeviceGuard g(H->h.device);
+  EntryGuard g(H);
   uint64_t t = 0;
   int rc = host_submit(H, keys, vals, 0, false, ops, out_vals, out_status, n, mode, S(stream), &t);
   if (rc != BT_OK) return rc;
@@ -539,7 +559,7 @@ int bt_search_batch(bt_handle* H, const uint64_t* keys, uint64_t* out_vals, uint
   if (n == 0) return BT_OK;
   if (!keys || !out_vals || !out_status) return BT_ERR_INVALID_ARG;
   bt::Handle& h = H->h;
-  DeviceGuard g(h.device);
+  EntryGuard g(H);
   // searches alone never conflict: run the search kernel directly on the batch
   cudaError_t e = bt::tree_join(&h, S(stream));
   if (e != cudaSuccess) return BT_ERR_CUDA;
@@ -555,7 +575,7 @@ int bt_range_batch(bt_handle* H, const uint64_t* lo, const uint64_t* hi, size_t 
   if (!H) return BT_ERR_INVALID_ARG;
   if (n == 0) return BT_OK;
   if (!lo || !hi || !out_counts || (max_per && (!out_keys || !out_vals))) return BT_ERR_INVALID_ARG;
-  DeviceGuard g(H->h.device);
+  EntryGuard g(H);
   if (bt::tree_join(&H->h, S(stream)) != cudaSuccess) return BT_ERR_CUDA;
   return bt::launch_range(&H->h, lo, hi, n, max_per, out_keys, out_vals, out_counts, S(stream)) == cudaSuccess
              ? BT_OK
@@ -569,7 +589,7 @@ int bt_insert_batch(bt_handle* H, const uint64_t* keys, const uint64_t* vals, ui
   if (!keys || !vals || !out_vals || !out_status) return BT_ERR_INVALID_ARG;
   bt::Handle& h = H->h;
   if (n > h.w.cap) return BT_ERR_BATCH_TOO_LARGE;
-  DeviceGuard g(h.device);
+  EntryGuard g(H);
   // an all-insert op array
   if (cudaMemsetAsync(h.w.ins_ops, BT_OP_INSERT, n, S(stream)) != cudaSuccess) return BT_ERR_CUDA;
   return map_internal(bt::batch_sorted(&h, keys, vals, h.w.ins_ops, out_vals, out_status, n, 0, S(stream)));
@@ -577,7 +597,7 @@ int bt_insert_batch(bt_handle* H, const uint64_t* keys, const uint64_t* vals, ui
 
 int bt_size(bt_handle* H, uint64_t* n_keys) {
   if (!H || !n_keys) return BT_ERR_INVALID_ARG;
-  DeviceGuard g(H->h.device);
+  EntryGuard g(H);
   bt::Ctrl c;
   if (bt::tree_sync(&H->h) != cudaSuccess) return BT_ERR_CUDA;
   if (cudaMemcpy(&c, H->h.tree.ctrl, sizeof(c), cudaMemcpyDeviceToHost) != cudaSuccess) return BT_ERR_CUDA;
@@ -587,7 +607,7 @@ int bt_size(bt_handle* H, uint64_t* n_keys) {
 
 int bt_dump_sorted(bt_handle* H, uint64_t* keys, uint64_t* vals, size_t cap, size_t* n_out, void* stream) {
   if (!H || !n_out) return BT_ERR_INVALID_ARG;
-  DeviceGuard g(H->h.device);
+  EntryGuard g(H);
   cudaStream_t s = stream ? S(stream) : H->h.internal_stream;
   if (stream == nullptr) cudaDeviceSynchronize();
   if (bt::tree_join(&H->h, s) != cudaSuccess) return BT_ERR_CUDA;
@@ -596,7 +616,7 @@ int bt_dump_sorted(bt_handle* H, uint64_t* keys, uint64_t* vals, size_t cap, siz
 
 int bt_leaf_sizes(bt_handle* H, uint32_t* sizes_host, size_t cap, size_t* n_leaves) {
   if (!H || !n_leaves) return BT_ERR_INVALID_ARG;
-  DeviceGuard g(H->h.device);
+  EntryGuard g(H);
   cudaDeviceSynchronize();
   bt::Handle& h = H->h;
   uint32_t* leaves = nullptr;
@@ -615,7 +635,7 @@ int bt_leaf_sizes(bt_handle* H, uint32_t* sizes_host, size_t cap, size_t* n_leav
 
 int bt_level_counts(bt_handle* H, uint64_t* counts_host, uint32_t cap, uint32_t* height) {
   if (!H || !height) return BT_ERR_INVALID_ARG;
-  DeviceGuard g(H->h.device);
+  EntryGuard g(H);
   cudaDeviceSynchronize();
   uint32_t* leaves = nullptr;
   size_t nl = 0;
@@ -629,7 +649,7 @@ int bt_level_counts(bt_handle* H, uint64_t* counts_host, uint32_t cap, uint32_t*
 
 int bt_stats_get(bt_handle* H, bt_stats* st, int with_leaves) {
   if (!H || !st) return BT_ERR_INVALID_ARG;
-  DeviceGuard g(H->h.device);
+  EntryGuard g(H);
   cudaDeviceSynchronize();
   bt::Ctrl c;
   if (cudaMemcpy(&c, H->h.tree.ctrl, sizeof(c), cudaMemcpyDeviceToHost) != cudaSuccess) return BT_ERR_CUDA;
@@ -660,7 +680,7 @@ int bt_stats_get(bt_handle* H, bt_stats* st, int with_leaves) {
 
 int bt_stats_reset(bt_handle* H) {
   if (!H) return BT_ERR_INVALID_ARG;
-  DeviceGuard g(H->h.device);
+  EntryGuard g(H);
   cudaDeviceSynchronize();
   bt::Ctrl c;
   if (cudaMemcpy(&c, H->h.tree.ctrl, sizeof(c), cudaMemcpyDeviceToHost) != cudaSuccess) return BT_ERR_CUDA;
@@ -672,7 +692,7 @@ int bt_stats_reset(bt_handle* H) {
 
 int bt_retrain(bt_handle* H, void* stream) {
   if (!H) return BT_ERR_INVALID_ARG;
-  DeviceGuard g(H->h.device);
+  EntryGuard g(H);
   cudaStream_t s = stream ? S(stream) : H->h.internal_stream;
   if (stream == nullptr) cudaDeviceSynchronize();
   if (bt::tree_join(&H->h, s) != cudaSuccess) return BT_ERR_CUDA;
@@ -682,7 +702,7 @@ int bt_retrain(bt_handle* H, void* stream) {
 int bt_refit(bt_handle* H, void* stream) {
   if (!H) return BT_ERR_INVALID_ARG;
   if (!H->h.L.trained) return BT_ERR_NOT_TRAINED;
-  DeviceGuard g(H->h.device);
+  EntryGuard g(H);
   cudaStream_t s = stream ? S(stream) : H->h.internal_stream;
   if (stream == nullptr) cudaDeviceSynchronize();
   if (bt::tree_join(&H->h, s) != cudaSuccess) return BT_ERR_CUDA;
@@ -713,7 +733,7 @@ int bt_set_search_group(bt_handle* H, uint32_t lanes) {
 
 int bt_profile(bt_handle* H, int enable) {
   if (!H) return BT_ERR_INVALID_ARG;
-  DeviceGuard g(H->h.device);
+  EntryGuard g(H);
   int rc = prof_resolve(H->h);
   H->h.prof = enable != 0;
   return rc;
@@ -721,7 +741,7 @@ int bt_profile(bt_handle* H, int enable) {
 
 int bt_profile_read(bt_handle* H, double* phase_ms, uint64_t* batches, int reset) {
   if (!H) return BT_ERR_INVALID_ARG;
-  DeviceGuard g(H->h.device);
+  EntryGuard g(H);
   int rc = prof_resolve(H->h);
   if (rc != BT_OK) return rc;
   if (phase_ms)
@@ -736,7 +756,7 @@ int bt_profile_read(bt_handle* H, double* phase_ms, uint64_t* batches, int reset
 
 int bt_sync(bt_handle* H, void* stream) {
   if (!H) return BT_ERR_INVALID_ARG;
-  DeviceGuard g(H->h.device);
+  EntryGuard g(H);
   const cudaError_t e = stream ? bt::tree_join(&H->h, S(stream)) : bt::tree_sync(&H->h);
   return e == cudaSuccess ? BT_OK : BT_ERR_CUDA;
 }
@@ -787,6 +807,9 @@ int bt_set_option(bt_handle* H, int option, int64_t value) {
     case BT_OPT_STM_COMBINE:
       H->h.stm_combine = value ? 1 : 0;
       return BT_OK;
+    case BT_OPT_HOST_FRONT_OVERLAP:
+      H->h.host_front_overlap = value ? 1 : 0;
+      return BT_OK;
     case BT_OPT_LEARNED_POLICY:
       if (value < 0 || value > 2) return BT_ERR_INVALID_ARG;
       H->h.L.policy = (int)value;
@@ -802,7 +825,7 @@ int bt_set_option(bt_handle* H, int option, int64_t value) {
 
 int bt_autotune(bt_handle* H, const uint64_t* sample_keys, size_t n, void* stream, double* report) {
   if (!H || !sample_keys || n == 0) return BT_ERR_INVALID_ARG;
-  DeviceGuard g(H->h.device);
+  EntryGuard g(H);
   cudaStream_t s = stream ? S(stream) : H->h.internal_stream;
   if (stream == nullptr) cudaDeviceSynchronize();
   if (bt::tree_join(&H->h, s) != cudaSuccess) return BT_ERR_CUDA;
@@ -815,7 +838,7 @@ int bt_autotune(bt_handle* H, const uint64_t* sample_keys, size_t n, void* strea
 // handle keeps the fill of the fastest for its later bulk builds and splits.
 int bt_autotune_fill(bt_handle* H, const uint64_t* sample_keys, size_t n, void* stream, double* report) {
   if (!H || !sample_keys || n < 64) return BT_ERR_INVALID_ARG;
-  DeviceGuard g(H->h.device);
+  EntryGuard g(H);
   cudaStream_t s = S(stream);
   if (cudaStreamSynchronize(s) != cudaSuccess || bt::tree_sync(&H->h) != cudaSuccess) return BT_ERR_CUDA;
   const uint32_t fills[4] = {16, 20, 24, 28};
@@ -893,7 +916,7 @@ int bt_set_learned_group(bt_handle* H, uint32_t lanes) {
 
 int bt_learned_info(bt_handle* H, double* info) {
   if (!H || !info) return BT_ERR_INVALID_ARG;
-  DeviceGuard g(H->h.device);
+  EntryGuard g(H);
   const bt::Learned& L = H->h.L;
   // the last (re)training's loss and segment count arrive in page-locked host words
   if (cudaDeviceSynchronize() != cudaSuccess) return BT_ERR_CUDA;
@@ -917,7 +940,7 @@ int bt_learned_info(bt_handle* H, double* info) {
 int bt_mlp_grad(bt_handle* H, const float* params, const float* x, const float* y, size_t n, float* grad_out,
                 float* loss_out, void* stream) {
   if (!H || !params || !x || !y || !grad_out || !loss_out || n == 0) return BT_ERR_INVALID_ARG;
-  DeviceGuard g(H->h.device);
+  EntryGuard g(H);
   return map_internal(bt::learned_mlp_grad(&H->h, params, x, y, n, grad_out, loss_out, S(stream)));
 }
 
@@ -935,7 +958,7 @@ int bt_route_batch(bt_handle* H, const uint64_t* splitters, int n_shards, const 
   if (n_shards > 1 && !splitters) return BT_ERR_INVALID_ARG;
   if (n && (!keys || !out_keys || !out_perm || (vals && !out_vals) || (ops && !out_ops))) return BT_ERR_INVALID_ARG;
   if (n > 0xFFFFFFFFull) return BT_ERR_BATCH_TOO_LARGE;  // 32-bit permutation
-  DeviceGuard g(H->h.device);
+  EntryGuard g(H);
   return bt::route_batch(&H->h, splitters, n_shards, keys, vals, ops, n, out_keys, out_vals, out_ops, out_perm,
                          out_counts, S(stream));
 }
@@ -945,7 +968,7 @@ int bt_unroute_results(bt_handle* H, const uint32_t* perm, const uint64_t* in_va
   if (!H) return BT_ERR_INVALID_ARG;
   if (n == 0) return BT_OK;
   if (!perm || !in_vals || !in_status || !out_vals || !out_status) return BT_ERR_INVALID_ARG;
-  DeviceGuard g(H->h.device);
+  EntryGuard g(H);
   return bt::unroute_results(&H->h, perm, in_vals, in_status, n, out_vals, out_status, S(stream));
 }
 

@@ -403,7 +403,7 @@ int work_alloc(Work* w, size_t cap) {
 }
 
 // the fields of Work that make up a BatchSet
-#define BT_SET_FIELDS(X) X(counts) X(f_list) X(f_lk) X(ukeys) X(uvals) X(ins_list) X(get_list) X(del_list) X(pend) \
+#define BT_SET_FIELDS(X) X(tiles) X(counts) X(f_list) X(f_lk) X(ukeys) X(uvals) X(ins_list) X(get_list) X(del_list) X(pend) \
   X(k_a) X(k_b) X(v_a) X(v_b)
 
 void work_swap_set(Work* w) {
@@ -417,7 +417,8 @@ int work_alt_alloc(Work* w) {
   if (w->alt.counts) return 0;
   const size_t cap = w->cap;
   BatchSet& a = w->alt;
-  bool ok = cudaMalloc((void**)&a.counts, sizeof(BatchCounts)) == cudaSuccess &&
+  bool ok = cudaMalloc((void**)&a.tiles, pass_tiles(cap) * sizeof(TileSummary)) == cudaSuccess &&
+            cudaMalloc((void**)&a.counts, sizeof(BatchCounts)) == cudaSuccess &&
             cudaMalloc((void**)&a.f_list, cap * 4) == cudaSuccess && cudaMalloc((void**)&a.f_lk, cap * 8) == cudaSuccess &&
             cudaMalloc((void**)&a.ukeys, cap * 8) == cudaSuccess && cudaMalloc((void**)&a.uvals, cap * 8) == cudaSuccess &&
             cudaMalloc((void**)&a.ins_list, cap * 4) == cudaSuccess &&
@@ -516,7 +517,8 @@ struct FrontPart {
 };
 
 static int hashed_front(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, uint64_t* out_vals,
-                        uint8_t* out_st, size_t n, cudaStream_t s, bool passes, FrontPart& fp) {
+                        uint8_t* out_st, size_t n, cudaStream_t s, bool passes, FrontPart& fp,
+                        cudaEvent_t vals_ready = nullptr) {
   Work& w = h->w;
   BatchCounts* c = w.counts;
   const uint32_t* n_touch = &c->n_touch;
@@ -529,6 +531,7 @@ static int hashed_front(Handle* h, const uint64_t* keys, const uint64_t* vals, c
   fp.n_tiles = (uint32_t)pass_tiles(n);
   prof_mark(h, h->overlap != 0 ? kEvSortEnd : 1, s);
   if (passes) {
+    if (vals_ready && cudaStreamWaitEvent(s, vals_ready, 0) != cudaSuccess) return -2;
     merge_pass1<<<fp.n_tiles, kThreads, 0, s>>>(fp.sk, fp.sv, vals, n, n_touch, w.tiles);
     count_launch();
     merge_pass2<<<1, 1024, 0, s>>>(w.tiles, fp.n_tiles, n_touch, c);
@@ -643,6 +646,17 @@ static int batch_hashed(Handle* h, const uint64_t* keys, const uint64_t* vals, c
   return hashed_tree(h, keys, vals, out_vals, out_st, n, engine, s, fp);
 }
 
+static int front_stream_init(Handle* h) {
+  if (h->front_stream) return 0;
+  bool ok = cudaStreamCreateWithFlags(&h->front_stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&h->pipe_ev, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&h->chain_gate, cudaEventDisableTiming) == cudaSuccess;
+  for (int p = 0; ok && p < 2; p++)
+    ok = cudaEventCreateWithFlags(&h->front_done[p], cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&h->tree_done[p], cudaEventDisableTiming) == cudaSuccess;
+  return ok ? 0 : -2;
+}
+
 // Several hash-front-end batches, their inputs all ready on `s`, in order:
 // batch j + 1's front part (classification, sort, merge passes: no tree) on
 // front_stream beside batch j's tree part on `s`, the two with alternate
@@ -658,14 +672,7 @@ int batches_pipelined(Handle* h, size_t count, const uint64_t* const* keys, cons
   for (size_t j = 0; j < count; j++)
     if (n[j] == 0 || n[j] > w.cap || n[j] > kIdxMask) return -6;
   if (work_alt_alloc(&w) != 0) return -3;
-  if (!h->front_stream) {
-    bool ok = cudaStreamCreateWithFlags(&h->front_stream, cudaStreamNonBlocking) == cudaSuccess &&
-              cudaEventCreateWithFlags(&h->pipe_ev, cudaEventDisableTiming) == cudaSuccess;
-    for (int p = 0; ok && p < 2; p++)
-      ok = cudaEventCreateWithFlags(&h->front_done[p], cudaEventDisableTiming) == cudaSuccess &&
-           cudaEventCreateWithFlags(&h->tree_done[p], cudaEventDisableTiming) == cudaSuccess;
-    if (!ok) return -2;
-  }
+  if (front_stream_init(h) != 0) return -2;
   cudaStream_t F = h->front_stream;
   const bool prof = h->prof;
   h->prof = false;
@@ -700,6 +707,52 @@ int batches_pipelined(Handle* h, size_t count, const uint64_t* const* keys, cons
   h->prof = prof;
   // whatever the front stream did is ordered before `s`'s later work
   if (cudaEventRecord(h->pipe_ev, F) != cudaSuccess || cudaStreamWaitEvent(s, h->pipe_ev, 0) != cudaSuccess) rc = -2;
+  return rc;
+}
+
+// The front part of batch j (set j & 1) waits for chain_gate, recorded on
+// `s` just before batch j - 1's tree part was queued: by then `s` holds
+// batch j - 2's tree part, the last user of the set, and nothing else of
+// the handle came after it (chain_open; every other entry point closes the
+// chain).  The other front parts are before it on front_stream.  With
+// `vals_late` (a value slot per request, copied after the keys) the merge
+// passes go to the tree part, beside the lookups as in batch_hashed, so
+// that the lookups need not wait for the values.
+int batch_chained(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, uint64_t* out_vals,
+                  uint8_t* out_st, size_t n, int engine, cudaStream_t s, cudaEvent_t in_ready,
+                  cudaEvent_t vals_ready, bool vals_late) {
+  Work& w = h->w;
+  if (n == 0) return 0;
+  if (n > w.cap || n > kIdxMask) return -6;
+  const bool open = h->chain_open;
+  h->chain_open = false;
+  if (work_alt_alloc(&w) != 0) return -3;
+  if (front_stream_init(h) != 0) return -2;
+  cudaStream_t F = h->front_stream;
+  const int p = h->chain_set ^= 1;
+  const bool prof = h->prof;
+  h->prof = false;
+  auto use = [&](int q) {
+    if ((int)w.alt_in != q) work_swap_set(&w);
+  };
+  int rc = 0;
+  FrontPart fp;
+  const bool pass_tree = vals_late && h->overlap != 0;
+  use(p);
+  if ((!open && cudaEventRecord(h->chain_gate, s) != cudaSuccess) ||
+      cudaStreamWaitEvent(F, h->chain_gate, 0) != cudaSuccess || cudaStreamWaitEvent(F, in_ready, 0) != cudaSuccess ||
+      hashed_front(h, keys, vals, ops, out_vals, out_st, n, F, !pass_tree, fp, vals_ready) != 0 ||
+      cudaEventRecord(h->front_done[p], F) != cudaSuccess || cudaEventRecord(h->chain_gate, s) != cudaSuccess ||
+      cudaStreamWaitEvent(s, h->front_done[p], 0) != cudaSuccess)
+    rc = -2;
+  if (rc == 0) {
+    h->vals_wait = pass_tree ? vals_ready : nullptr;
+    if (hashed_tree(h, keys, vals, out_vals, out_st, n, engine, s, fp) != 0) rc = -2;
+    h->vals_wait = nullptr;
+  }
+  use(0);
+  h->prof = prof;
+  h->chain_open = rc == 0;
   return rc;
 }
 

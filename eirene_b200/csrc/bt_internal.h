@@ -81,10 +81,12 @@ struct TopInfo {
 struct TileSummary;  // bt_batch.cu
 
 // The buffers the front part and the tree part of a hash-front-end batch
-// share (bt_batch.cu): a second set lets bt_execute_batches run one batch's
-// front part beside the previous batch's tree part.  Work's own fields hold
-// the set in use; `alt` the other.
+// share, and the merge passes' tile summaries, which either part may run
+// (bt_batch.cu): a second set lets bt_execute_batches and the host batches
+// run one batch's front part beside the previous batch's tree part.  Work's
+// own fields hold the set in use; `alt` the other.
 struct BatchSet {
+  TileSummary* tiles = nullptr;
   BatchCounts* counts = nullptr;
   uint32_t* f_list = nullptr;
   uint64_t* f_lk = nullptr;
@@ -280,10 +282,18 @@ struct Handle {
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   int overlap = 1;
   int lookup_reserve = 0;    // block slots the overlapped lookups leave free (set per batch)
-  // bt_execute_batches: the front parts' stream and its events
+  // bt_execute_batches and the host-buffer entry points: the front parts'
+  // stream and its events
   cudaStream_t front_stream = nullptr;
   cudaEvent_t front_done[2] = {nullptr, nullptr}, tree_done[2] = {nullptr, nullptr};
   cudaEvent_t pipe_ev = nullptr;
+  // host batches (batch_chained): the point of the caller's stream before
+  // the last such batch's tree part, and whether no other call used the
+  // handle since (the next front part may then start there)
+  cudaEvent_t chain_gate = nullptr;
+  bool chain_open = false;
+  int chain_set = 0;
+  int host_front_overlap = 1;  // BT_OPT_HOST_FRONT_OVERLAP
   int overlap_reserve = 4;  // ... in the overlapped layout (measured, per 2^22 batch on 2^26 keys: 4 < 8 < 16 < 32 ms, 1.3 % from 4 to 16)
   // host-buffer entry points: staging sets and copy streams
   HostPipe hp;
@@ -456,6 +466,17 @@ int batch_sorted(Handle* h, const uint64_t* keys, const uint64_t* vals, const ui
 int batches_pipelined(Handle* h, size_t count, const uint64_t* const* keys, const uint64_t* const* vals,
                       const uint8_t* const* ops, uint64_t* const* out_vals, uint8_t* const* out_st, const size_t* n,
                       int engine, cudaStream_t s);
+// One hash-front-end batch of the host-buffer entry points, its op codes
+// and keys ready at `in_ready` and its values at `vals_ready` (events of the
+// copy-in stream; the merge passes wait for the values, and run in the tree
+// part when `vals_late`): the front part on
+// front_stream, the tree part on `s`, with buffer sets alternating from one
+// such batch to the next.  While chain_open, the front part starts at
+// chain_gate, beside the previous such batch's tree part; otherwise after
+// everything queued on `s`.
+int batch_chained(Handle* h, const uint64_t* keys, const uint64_t* vals, const uint8_t* ops, uint64_t* out_vals,
+                  uint8_t* out_st, size_t n, int engine, cudaStream_t s, cudaEvent_t in_ready,
+                  cudaEvent_t vals_ready, bool vals_late);
 
 // ---- segmented leaf merge (bt_merge.cu) ----
 int merge_engine(Handle* h, size_t n_upper, cudaStream_t s);

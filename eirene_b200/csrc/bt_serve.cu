@@ -202,6 +202,7 @@ int bt_serve_start(bt_handle* H, const bt_serve_config* cfg_in, bt_server** out)
   int prev = -1;
   cudaGetDevice(&prev);
   if (cudaSetDevice(H->h.device) != cudaSuccess) return BT_ERR_CUDA;
+  H->h.chain_open = false;
   bt_server* S = new bt_server();
   S->H = H;
   S->device = H->h.device;

@@ -59,6 +59,7 @@ int bt_save(bt_handle* h, const char* path) {
   int prev = -1;
   cudaGetDevice(&prev);
   cudaSetDevice(h->h.device);
+  h->h.chain_open = false;
   std::vector<uint64_t> keys(n), vals(n);
   if (n) {
     DevBuf dk, dv;  // freed with the handle's device current
@@ -117,6 +118,7 @@ int bt_load(bt_handle* h, const char* path) {
   int prev = -1;
   cudaGetDevice(&prev);
   cudaSetDevice(h->h.device);
+  h->h.chain_open = false;
   int rc = BT_OK;
   {
     DevBuf dk, dv;  // freed with the handle's device current
@@ -154,6 +156,7 @@ int bt_save_image(bt_handle* h, const char* path) {
   int prev = -1;
   cudaGetDevice(&prev);
   cudaSetDevice(H.device);
+  H.chain_open = false;
   int rc = BT_OK;
   bt::Ctrl c{};
   std::vector<uint64_t> keys, vals, low;
@@ -235,6 +238,7 @@ int bt_load_image(bt_handle* h, const char* path) {
   int prev = -1;
   cudaGetDevice(&prev);
   cudaSetDevice(H.device);
+  H.chain_open = false;
   int rc = BT_OK;
   c.root_lock &= ~1u;  // saved at rest: unlocked
   // the loading handle starts with its own record: no sticky error bits or

@@ -303,6 +303,13 @@ int bt_set_search_group(bt_handle *h, uint32_t lanes);
                                   * and the library refits by itself once 8 batches have run since the last fit.
                                   * Answers are the same in every case; bt_search_batch keeps bt_set_descent's
                                   * choice */
+#define BT_OPT_HOST_FRONT_OVERLAP 17 /* host-buffer entry points, BT_MODE_SORTED with the hash front end: 1
+                                      * (default) a batch's classification, sort and merge passes (which read no
+                                      * tree) run on an internal stream once its requests are copied in, beside
+                                      * the previous host batch's lookups and writes, with a second set of
+                                      * per-batch buffers (as bt_execute_batches); any other call on the handle
+                                      * in between makes the next one wait for it.  0 runs each batch whole on
+                                      * `stream`.  Same answers and tree */
 #define BT_OPT_SORT_TILE 14     /* radix sort tile of sorted batches: 256, 512 (default) or 1024 threads x 8 keys,
                                  * for whole batches and for the hash front end's touched requests alike
                                  * (bt_autotune picks the two separately) */

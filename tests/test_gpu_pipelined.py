@@ -102,3 +102,99 @@ def test_pipelined_stm_runs_one_by_one(gpu):
     t.execute_many(batches, outs, mode=E.MODE_STM)
     for b, (ov, os_) in enumerate(expect):
         assert (host_u8(outs[b][1]) == os_).all() and (host_u64(outs[b][0]) == ov).all(), b
+
+
+@pytest.mark.parametrize("learned", [False, True])
+def test_host_batches_chain_beside_other_calls(gpu, learned):
+    # host batches (BT_OPT_HOST_FRONT_OVERLAP on): each front part runs beside
+    # the previous host batch's tree part.  Between them: device batches,
+    # plain searches, bt_execute_batches, STM host batches, packed ones, the
+    # option switched off and on; up to three host batches in flight.  Every
+    # answer and the final tree against the oracle run in call order.
+    import torch
+
+    keys = O.gen_keys("uniform", 681, 100_000)
+    vals = O.value_of(keys)
+    t = E.BTree(max_keys=1 << 21, max_batch=1 << 17)
+    t.bulk_build(dev(keys), dev(vals))
+    o = O.OracleTree()
+    o.bulk_build(keys, vals)
+    if learned:
+        t.retrain()
+        t.set_descent(True)
+    plan = ["host", "host", "host", "dev", "host", "host", "search", "host", "many", "host", "packed", "host",
+            "off", "host", "host", "on", "host", "stm", "host", "host", "packed", "host"]
+    keep, checks, inflight = [], [], []
+
+    def host_tensors(rk, rv, ro):
+        return [torch.from_numpy(rk.view(np.int64).copy()), torch.from_numpy(rv.view(np.int64).copy()),
+                torch.from_numpy(ro.copy()), torch.zeros(rk.size, dtype=torch.int64),
+                torch.zeros(rk.size, dtype=torch.uint8)]
+
+    for i, what in enumerate(plan):
+        if what == "off":
+            t.set_option(E.OPT_HOST_FRONT_OVERLAP, 0)
+            continue
+        if what == "on":
+            t.set_option(E.OPT_HOST_FRONT_OVERLAP, 1)
+            continue
+        n = 20_000 + 3_331 * (i % 5)
+        rk, rv, ro = O.gen_requests("uniform", 690 + i, keys, n, 50 if i % 3 else 90)
+        if what == "stm":
+            _, at = np.unique(rk, return_index=True)
+            sel = np.sort(at)
+            rk, rv, ro = rk[sel], rv[sel], ro[sel]
+            ex = o.execute_serial(rk, rv, ro)
+        elif what == "search":
+            ro = np.full(rk.size, E.OP_GET, dtype=np.uint8)
+            ex = o.execute_merged(rk, rv, ro, engine=O.ENGINE_MERGE)
+        else:
+            ex = o.execute_merged(rk, rv, ro, engine=O.ENGINE_MERGE)
+        if what in ("host", "stm"):
+            hb = host_tensors(rk, rv, ro)
+            tk = t.submit_host(*hb, mode=E.MODE_STM if what == "stm" else MERGE)
+            keep.append(hb)
+            checks.append((ex, hb[3], hb[4], True))
+            inflight.append(tk)
+        elif what == "packed":
+            hb = host_tensors(rk, rv, ro)
+            ins = torch.from_numpy(rv[ro == E.OP_INSERT].view(np.int64).copy())
+            tk = t.submit_host_packed(hb[0], hb[2], ins, hb[3], hb[4], mode=MERGE)
+            keep.append(hb + [ins])
+            checks.append((ex, hb[3], hb[4], True))
+            inflight.append(tk)
+        elif what == "dev":
+            a, s = empty_u64(rk.size), empty_u8(rk.size)
+            d = (dev(rk), dev(rv), dev(ro))
+            t.execute(*d, a, s, mode=MERGE)
+            keep.append(d)
+            checks.append((ex, a, s, False))
+        elif what == "search":
+            a, s = empty_u64(rk.size), empty_u8(rk.size)
+            d = dev(rk)
+            t.search(d, a, s)
+            keep.append(d)
+            checks.append((ex, a, s, False))
+        elif what == "many":
+            # this batch and a second one drawn after it
+            rk2, rv2, ro2 = O.gen_requests("uniform", 790 + i, keys, 17_777, 70)
+            ex2 = o.execute_merged(rk2, rv2, ro2, engine=O.ENGINE_MERGE)
+            bs = [(dev(rk), dev(rv), dev(ro)), (dev(rk2), dev(rv2), dev(ro2))]
+            outs = [(empty_u64(rk.size), empty_u8(rk.size)), (empty_u64(rk2.size), empty_u8(rk2.size))]
+            t.execute_many(bs, outs, mode=MERGE)
+            keep.append((bs, outs))
+            checks.append((ex, outs[0][0], outs[0][1], False))
+            checks.append((ex2, outs[1][0], outs[1][1], False))
+        while len(inflight) > 2:
+            t.wait_host(inflight.pop(0))
+    for tk in inflight:
+        t.wait_host(tk)
+    t.sync()
+    for j, ((ov, os_), a, s, host) in enumerate(checks):
+        ga = a.numpy().view(np.uint64) if host else host_u64(a)
+        gs = s.numpy() if host else host_u8(s)
+        assert (gs == os_).all(), j
+        assert (ga == ov).all(), j
+    gk, gv = dump(t)
+    ok, ovv = o.dump()
+    assert (gk == ok).all() and (gv == ovv).all()
