@@ -109,7 +109,7 @@ MAX_SHARDS = 256
 OPT_SORTED_SEARCH, OPT_RETRY_LIMIT, OPT_TRAIN_STEPS, OPT_SORTED_LEAF_VALS, OPT_BATCH_DESCENT = 1, 2, 3, 4, 5
 OPT_FRONT_END, OPT_TOP_CACHE, OPT_SEARCH_PAIRS, OPT_OVERLAP, OPT_ASYNC_WRITE = 6, 7, 8, 9, 10
 OPT_REFIT_STEPS, OPT_LEARNED_MODE, OPT_HOST_VALUES_IN_PLACE, OPT_SORT_TILE, OPT_STM_COMBINE = 11, 12, 13, 14, 15
-OPT_LEARNED_POLICY, OPT_HOST_FRONT_OVERLAP = 16, 17
+OPT_LEARNED_POLICY, OPT_HOST_FRONT_OVERLAP, OPT_TOUCH_SORT = 16, 17, 18
 PHASES = ["sort", "merge", "search", "insert", "writeback"]
 
 _lib = None

@@ -201,6 +201,11 @@ int bt_create(const bt_config* cfg_in, bt_handle** out) {
          cudaEventCreateWithFlags(&h.tree_ev, cudaEventDisableTiming) == cudaSuccess &&
          cudaEventCreateWithFlags(&h.ans_ev, cudaEventDisableTiming) == cudaSuccess;
   }
+  // the touched-request count of the batches, written by the front end into
+  // page-locked mapped memory: the next batches' sort choice (BT_OPT_TOUCH_SORT 2)
+  ok = ok && cudaHostAlloc((void**)&h.touch_hint, sizeof(uint32_t), cudaHostAllocMapped) == cudaSuccess &&
+       cudaHostGetDevicePointer((void**)&h.touch_hint_dev, h.touch_hint, 0) == cudaSuccess;
+  if (h.touch_hint) *h.touch_hint = UINT32_MAX;  // none seen yet
   ok = ok && bt::tree_reset(&h, h.internal_stream) == cudaSuccess;
   ok = ok && cudaStreamSynchronize(h.internal_stream) == cudaSuccess;
   if (!ok) {
@@ -225,6 +230,7 @@ int bt_destroy(bt_handle* H) {
   bt::learned_free(&h.L);
   bt::learned_policy_free(&h.L);
   if (h.front_stream) cudaStreamDestroy(h.front_stream);
+  if (h.touch_hint) cudaFreeHost(h.touch_hint);
   for (cudaEvent_t e : {h.front_done[0], h.front_done[1], h.tree_done[0], h.tree_done[1], h.pipe_ev,
                         h.chain_gate})
     if (e) cudaEventDestroy(e);
@@ -809,6 +815,10 @@ int bt_set_option(bt_handle* H, int option, int64_t value) {
       return BT_OK;
     case BT_OPT_HOST_FRONT_OVERLAP:
       H->h.host_front_overlap = value ? 1 : 0;
+      return BT_OK;
+    case BT_OPT_TOUCH_SORT:
+      if (value < 0 || value > 2) return BT_ERR_INVALID_ARG;
+      H->h.touch_sort = (int)value;
       return BT_OK;
     case BT_OPT_LEARNED_POLICY:
       if (value < 0 || value > 2) return BT_ERR_INVALID_ARG;

@@ -525,9 +525,17 @@ static int hashed_front(Handle* h, const uint64_t* keys, const uint64_t* vals, c
   if (front_classify(h, keys, ops, n, s) != 0) return -2;
   // the touched requests' sort and merge passes need no tree: they run at
   // full width (beside the previous batch's deferred merge)
-  if (radix_sort_pairs(w.f_tk, w.f_tv, nullptr, w.k_a, w.v_a, w.k_b, w.v_b, n, 0, 64, w.sort_scratch, s, &fp.sk,
-                       &fp.sv, &h->tree.ctrl->error, n_touch, h->sort_threads_touch) != cudaSuccess)
-    return -2;
+  // the merge sort while the touched counts are small (the count of a batch
+  // that ran before: a hint, both sorts give the same order)
+  bool merge = h->touch_sort == 1;
+  if (h->touch_sort == 2 && h->touch_hint)
+    merge = *reinterpret_cast<volatile const uint32_t*>(h->touch_hint) <= kMergeSortMax;
+  const cudaError_t se =
+      merge
+          ? merge_sort_pairs(w.f_tk, w.f_tv, w.k_a, w.v_a, w.k_b, w.v_b, n, n_touch, h->sm_count, s, &fp.sk, &fp.sv)
+          : radix_sort_pairs(w.f_tk, w.f_tv, nullptr, w.k_a, w.v_a, w.k_b, w.v_b, n, 0, 64, w.sort_scratch, s,
+                             &fp.sk, &fp.sv, &h->tree.ctrl->error, n_touch, h->sort_threads_touch);
+  if (se != cudaSuccess) return -2;
   fp.n_tiles = (uint32_t)pass_tiles(n);
   prof_mark(h, h->overlap != 0 ? kEvSortEnd : 1, s);
   if (passes) {

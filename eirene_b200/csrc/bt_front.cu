@@ -228,7 +228,8 @@ __global__ void __launch_bounds__(kTileThreads) front_flag_kernel(const uint64_t
 
 // exclusive offsets of n_tiles counts, in place, with one block
 __global__ void __launch_bounds__(1024) front_tile_scan_kernel(uint32_t* __restrict__ tile, uint32_t n_tiles,
-                                                               size_t n, BatchCounts* __restrict__ counts) {
+                                                               size_t n, BatchCounts* __restrict__ counts,
+                                                               uint32_t* hint) {
   __shared__ uint32_t wtot[32];
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t carry = 0;
@@ -261,6 +262,7 @@ __global__ void __launch_bounds__(1024) front_tile_scan_kernel(uint32_t* __restr
   if (threadIdx.x == 0) {
     counts->n_touch = carry;
     counts->n_lookup = (uint32_t)n - carry;
+    if (hint) *reinterpret_cast<volatile uint32_t*>(hint) = carry;  // host memory: a later batch's sort choice
   }
 }
 
@@ -663,7 +665,7 @@ int front_classify(Handle* h, const uint64_t* keys, const uint8_t* ops, size_t n
   front_clear_kernel<<<(unsigned)h->sm_count * 4, kThreads, 0, s>>>(tab, w.f_tab_cap, c);
   front_insert_kernel<<<g, kThreads, 0, s>>>(keys, ops, n, tab, c);
   front_flag_kernel<<<(unsigned)n_tiles, kTileThreads, 0, s>>>(keys, ops, n, tab, c, flags, tile);
-  front_tile_scan_kernel<<<1, 1024, 0, s>>>(tile, (uint32_t)n_tiles, n, c);
+  front_tile_scan_kernel<<<1, 1024, 0, s>>>(tile, (uint32_t)n_tiles, n, c, h->touch_hint_dev);
   front_scatter_kernel<<<(unsigned)n_tiles, kTileThreads, 0, s>>>(keys, ops, n, flags, tile, w.f_tk, w.f_tv,
                                                                   w.f_list, w.f_lk);
   count_launch(6);

@@ -57,6 +57,18 @@ cudaError_t radix_sort_pairs(const uint64_t* keys_in, const uint32_t* vals_in, c
                              uint32_t* scratch, cudaStream_t s, uint64_t** k_out, uint32_t** v_out, uint32_t* err,
                              const uint32_t* n_dev = nullptr, int tile_threads = 512);
 
+// Stable sort by key of (key, payload) pairs whose payload carries the
+// request index in its low 30 bits, indices increasing in input order (the
+// hash front end's touched requests): tile sort plus merge rounds; the
+// result is always in (k_a, v_a).  n is the capacity, n_dev the count.
+// touched counts up to which BT_OPT_TOUCH_SORT 2 takes the merge sort
+// (2^18 touched requests: 92 against 126 us for the radix sort; the merge
+// rounds grow with the count, the radix passes with its bytes)
+constexpr uint32_t kMergeSortMax = 1u << 19;
+cudaError_t merge_sort_pairs(const uint64_t* keys_in, const uint32_t* vals_in, uint64_t* k_a, uint32_t* v_a,
+                             uint64_t* k_b, uint32_t* v_b, size_t n, const uint32_t* n_dev, int sm_count,
+                             cudaStream_t s, uint64_t** k_out, uint32_t** v_out);
+
 // ---- per-batch work buffers, sized for max_batch requests ----
 struct BatchCounts {
   uint32_t n_unique;
@@ -294,6 +306,12 @@ struct Handle {
   bool chain_open = false;
   int chain_set = 0;
   int host_front_overlap = 1;  // BT_OPT_HOST_FRONT_OVERLAP
+  // BT_OPT_TOUCH_SORT: 0 onesweep radix sort, 1 tile sort + merge rounds, 2 the
+  // second while the touched count last seen (touch_hint, page-locked and
+  // mapped, written by front_tile_scan_kernel) is at most kMergeSortMax
+  int touch_sort = 2;
+  uint32_t* touch_hint = nullptr;
+  uint32_t* touch_hint_dev = nullptr;
   int overlap_reserve = 4;  // ... in the overlapped layout (measured, per 2^22 batch on 2^26 keys: 4 < 8 < 16 < 32 ms, 1.3 % from 4 to 16)
   // host-buffer entry points: staging sets and copy streams
   HostPipe hp;

@@ -570,4 +570,281 @@ cudaError_t radix_sort_pairs(const uint64_t* keys_in, const uint32_t* vals_in, c
   return cudaSuccess;
 }
 
+// ---------------------------------------------------------- merge sort ----
+// Sort of the hash front end's touched requests: at 95/5 a batch of 2^22
+// has about 2^18 of them, too few for the onesweep passes to be bound by
+// bytes: each of the eight is a launch, a one-wave tile pass and a look-back.
+// Here:
+//   1. ms_tile_kernel: each block sorts a tile of kMsTile pairs (bitonic
+//      network in registers, shuffles and shared memory), giving sorted runs;
+//   2. ms_merge_kernel, once per round: pairs of sorted runs merge into runs
+//      of twice the length (merge path: two warps find where the block's
+//      output range splits the two runs with 32-way searches, the block
+//      stages the two pieces in shared memory, each thread merges 4
+//      outputs), until one run remains.
+// The order is by key, then by the request index in the payload's low 30
+// bits.  Those indices are unique and increase in input order, so the order
+// is the stable one (the onesweep passes' order) and every comparison is
+// strict.  The device count n_dev fixes the number of rounds R: the host
+// launches the most rounds the capacity can need, the surplus ones return at
+// once, and the tile kernel writes its runs where R rounds of ping-pong leave
+// the result in (k_a, v_a).
+namespace {
+
+constexpr int kMsThreads = 512;
+constexpr int kMsItems = 4;
+constexpr int kMsTile = kMsThreads * kMsItems;  // 2048 pairs
+constexpr uint32_t kMsIdx = 0x3FFFFFFFu;
+
+// without short-circuit branches: the callers select on the result
+__device__ __forceinline__ bool ms_less(uint64_t ka, uint32_t va, uint64_t kb, uint32_t vb) {
+  return (ka < kb) | ((ka == kb) & ((va & kMsIdx) < (vb & kMsIdx)));
+}
+
+__device__ __forceinline__ size_t ms_count(size_t n_upper, const uint32_t* n_dev) {
+  return n_dev ? min((size_t)*n_dev, n_upper) : n_upper;
+}
+
+// merge rounds that turn ceil(n / kMsTile) sorted runs into one
+__host__ __device__ __forceinline__ int ms_rounds(size_t n) {
+  const size_t runs = (n + kMsTile - 1) / kMsTile;
+  int r = 0;
+  while (((size_t)1 << r) < runs) r++;
+  return r;
+}
+
+// compare-exchange so that (a, b) ends in ascending order when `asc`
+__device__ __forceinline__ void ms_cx(uint64_t& ka, uint32_t& va, uint64_t& kb, uint32_t& vb, bool asc) {
+  const bool sw = ms_less(kb, vb, ka, va) == asc;
+  const uint64_t k0 = sw ? kb : ka, k1 = sw ? ka : kb;
+  const uint32_t v0 = sw ? vb : va, v1 = sw ? va : vb;
+  ka = k0;
+  kb = k1;
+  va = v0;
+  vb = v1;
+}
+
+// a thread's element of index i meets its partner of index i ^ j: the lower
+// index keeps the smaller one where the bitonic sequence ascends
+__device__ __forceinline__ void ms_keep(uint64_t& k, uint32_t& v, uint64_t pk, uint32_t pv, int i, int j, int kk) {
+  const bool asc = (i & kk) == 0, lower = (i & j) == 0;
+  const bool p_lt = ms_less(pk, pv, k, v);
+  const bool m_lt = ms_less(k, v, pk, pv);
+  const bool take = (lower == asc) ? p_lt : m_lt;
+  k = take ? pk : k;
+  v = take ? pv : v;
+}
+
+// the stride-J exchanges inside a thread's registers (J < kMsItems)
+template <int J>
+__device__ __forceinline__ void ms_reg_stage(uint64_t (&K)[kMsItems], uint32_t (&V)[kMsItems], int base, int kk) {
+#pragma unroll
+  for (int e = 0; e < kMsItems; e++)
+    if ((e & J) == 0) ms_cx(K[e], V[e], K[e | J], V[e | J], ((base + e) & kk) == 0);
+}
+
+__device__ __forceinline__ int ms_phys(int i) { return i + (i >> 3); }  // padding: fewer bank conflicts
+
+// Bitonic sort of a tile: element i of the tile is register i % 4 of thread
+// i / 4.  Exchanges at strides 1-2 stay in registers, 4-64 are shuffles
+// within the warp, 128 and up go through shared memory (10 of the 66
+// stages).  Compares and exchanges are selects, not branches: with one tile
+// per SM the kernel is bound by its dependent instructions.
+__global__ void __launch_bounds__(kMsThreads) ms_tile_kernel(const uint64_t* __restrict__ kin,
+                                                             const uint32_t* __restrict__ vin, size_t n_upper,
+                                                             const uint32_t* __restrict__ n_dev, uint64_t* k_a,
+                                                             uint32_t* v_a, uint64_t* k_b, uint32_t* v_b) {
+  __shared__ uint64_t sk[kMsTile + kMsTile / 8];
+  __shared__ uint32_t sv[kMsTile + kMsTile / 8];
+  const size_t n = ms_count(n_upper, n_dev);
+  const bool to_a = (ms_rounds(n) & 1) == 0;
+  uint64_t* ko = to_a ? k_a : k_b;
+  uint32_t* vo = to_a ? v_a : v_b;
+  const int base = threadIdx.x * kMsItems;
+  for (size_t t0 = (size_t)blockIdx.x * kMsTile; t0 < n; t0 += (size_t)gridDim.x * kMsTile) {
+    const int cnt = (int)min((size_t)kMsTile, n - t0);
+    uint64_t K[kMsItems];
+    uint32_t V[kMsItems];
+    // the tail of the last tile sorts after every request (index bits all ones)
+#pragma unroll
+    for (int e = 0; e < kMsItems; e++) {
+      const int i = base + e;
+      K[e] = i < cnt ? kin[t0 + i] : ~0ull;
+      V[e] = i < cnt ? vin[t0 + i] : 0xFFFFFFFFu;
+    }
+    for (int kk = 2; kk <= kMsTile; kk <<= 1) {
+      for (int j = kk >> 1; j >= kMsItems; j >>= 1) {
+        if (j >= 32 * kMsItems) {
+          __syncthreads();  // the previous exchange's reads are done
+#pragma unroll
+          for (int e = 0; e < kMsItems; e++) {
+            sk[ms_phys(base + e)] = K[e];
+            sv[ms_phys(base + e)] = V[e];
+          }
+          __syncthreads();
+#pragma unroll
+          for (int e = 0; e < kMsItems; e++) {
+            const int p = ms_phys((base + e) ^ j);
+            ms_keep(K[e], V[e], sk[p], sv[p], base + e, j, kk);
+          }
+        } else {
+          const int lm = j / kMsItems;
+#pragma unroll
+          for (int e = 0; e < kMsItems; e++) {
+            const uint64_t pk = __shfl_xor_sync(0xffffffffu, K[e], lm);
+            const uint32_t pv = __shfl_xor_sync(0xffffffffu, V[e], lm);
+            ms_keep(K[e], V[e], pk, pv, base + e, j, kk);
+          }
+        }
+      }
+      static_assert(kMsItems == 4, "register stages below are for 4 items per thread");
+      if (kk >= 4) ms_reg_stage<2>(K, V, base, kk);
+      ms_reg_stage<1>(K, V, base, kk);
+    }
+#pragma unroll
+    for (int e = 0; e < kMsItems; e++) {
+      const int i = base + e;
+      if (i < cnt) {
+        ko[t0 + i] = K[e];
+        vo[t0 + i] = V[e];
+      }
+    }
+    __syncthreads();  // shared memory is reused by the next tile
+  }
+}
+
+// a = the number of elements of A among the first d of merge(A, B): the
+// first a in [max(0, d - nb), min(d, na)] with !(A[a] < B[d - 1 - a]); one
+// warp, 32 candidates per step
+__device__ __forceinline__ size_t ms_split(const uint64_t* __restrict__ k, const uint32_t* __restrict__ v,
+                                           size_t a_beg, size_t na, size_t b_beg, size_t nb, size_t d) {
+  const uint32_t lane = threadIdx.x & 31;
+  size_t lo = d > nb ? d - nb : 0, hi = min(d, na);
+  while (lo < hi) {
+    const size_t stride = (hi - lo + 31) / 32;
+    const size_t a = lo + (size_t)lane * stride;
+    bool p = false;
+    if (a < hi) {
+      const size_t b = b_beg + d - 1 - a;
+      p = ms_less(k[a_beg + a], v[a_beg + a], k[b], v[b]);
+    }
+    const int c = __popc(__ballot_sync(0xffffffffu, p));
+    if (c == 0) {
+      hi = lo;
+    } else {
+      const size_t top = lo + (size_t)c * stride;
+      lo += (size_t)(c - 1) * stride + 1;
+      hi = min(hi, top);
+    }
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(kMsThreads) ms_merge_kernel(uint64_t* k_a, uint32_t* v_a, uint64_t* k_b,
+                                                              uint32_t* v_b, size_t n_upper,
+                                                              const uint32_t* __restrict__ n_dev, int round) {
+  __shared__ uint64_t sk[kMsTile];
+  __shared__ uint32_t sv[kMsTile];
+  __shared__ size_t split[2];
+  const size_t n = ms_count(n_upper, n_dev);
+  const int R = ms_rounds(n);
+  if (round >= R) return;
+  const bool from_a = ((R - round) & 1) == 0;
+  const uint64_t* __restrict__ ks = from_a ? k_a : k_b;
+  const uint32_t* __restrict__ vs = from_a ? v_a : v_b;
+  uint64_t* __restrict__ kd = from_a ? k_b : k_a;
+  uint32_t* __restrict__ vd = from_a ? v_b : v_a;
+  const size_t L = (size_t)kMsTile << round;  // input run length
+  const int warp = threadIdx.x >> 5;
+  for (size_t o0 = (size_t)blockIdx.x * kMsTile; o0 < n; o0 += (size_t)gridDim.x * kMsTile) {
+    const int cnt = (int)min((size_t)kMsTile, n - o0);
+    const size_t ps = o0 / (2 * L) * (2 * L);
+    const size_t a_beg = ps, a_end = min(ps + L, n), b_end = min(ps + 2 * L, n);
+    const size_t na = a_end - a_beg, nb = b_end - a_end;
+    if (nb == 0) {  // the last run has no partner this round
+      for (int i = threadIdx.x; i < cnt; i += kMsThreads) {
+        kd[o0 + i] = ks[o0 + i];
+        vd[o0 + i] = vs[o0 + i];
+      }
+      continue;
+    }
+    const size_t d0 = o0 - ps;
+    if (warp < 2) {
+      const size_t a = ms_split(ks, vs, a_beg, na, a_end, nb, warp == 0 ? d0 : d0 + cnt);
+      if ((threadIdx.x & 31) == 0) split[warp] = a;
+    }
+    __syncthreads();
+    const size_t a0 = split[0], a1 = split[1];
+    const int la = (int)(a1 - a0), lb = cnt - la;
+    const size_t b0 = a_end + (d0 - a0);
+    for (int i = threadIdx.x; i < la; i += kMsThreads) {
+      sk[i] = ks[a_beg + a0 + i];
+      sv[i] = vs[a_beg + a0 + i];
+    }
+    for (int i = threadIdx.x; i < lb; i += kMsThreads) {
+      sk[la + i] = ks[b0 + i];
+      sv[la + i] = vs[b0 + i];
+    }
+    __syncthreads();
+    // this thread's outputs: merge path in shared memory, then a serial merge
+    const int d = threadIdx.x * kMsItems;
+    uint64_t ok[kMsItems];
+    uint32_t ov[kMsItems];
+    const int m = d < cnt ? min(kMsItems, cnt - d) : 0;
+    if (m > 0) {
+      int lo = d > lb ? d - lb : 0, hi = min(d, la);
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (ms_less(sk[mid], sv[mid], sk[la + d - 1 - mid], sv[la + d - 1 - mid])) lo = mid + 1;
+        else hi = mid;
+      }
+      int ia = lo, ib = d - lo;
+#pragma unroll
+      for (int j = 0; j < kMsItems; j++) {
+        if (j < m) {
+          const bool take_a = ib >= lb || (ia < la && ms_less(sk[ia], sv[ia], sk[la + ib], sv[la + ib]));
+          const int at = take_a ? ia++ : la + ib++;
+          ok[j] = sk[at];
+          ov[j] = sv[at];
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kMsItems; j++)
+      if (j < m) {
+        sk[d + j] = ok[j];
+        sv[d + j] = ov[j];
+      }
+    __syncthreads();
+    for (int i = threadIdx.x; i < cnt; i += kMsThreads) {
+      kd[o0 + i] = sk[i];
+      vd[o0 + i] = sv[i];
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+cudaError_t merge_sort_pairs(const uint64_t* keys_in, const uint32_t* vals_in, uint64_t* k_a, uint32_t* v_a,
+                             uint64_t* k_b, uint32_t* v_b, size_t n, const uint32_t* n_dev, int sm_count,
+                             cudaStream_t s, uint64_t** k_out, uint32_t** v_out) {
+  *k_out = k_a;
+  *v_out = v_a;
+  if (n == 0) return cudaSuccess;
+  // two blocks per SM (a wave at most): rounds past the count return at once,
+  // and a large count loops over its tiles
+  const size_t tiles = (n + kMsTile - 1) / kMsTile;
+  const unsigned grid = (unsigned)min(tiles, (size_t)(sm_count > 0 ? sm_count : 148) * 2);
+  ms_tile_kernel<<<grid, kMsThreads, 0, s>>>(keys_in, vals_in, n, n_dev, k_a, v_a, k_b, v_b);
+  count_launch();
+  const int r_max = ms_rounds(n);
+  for (int r = 0; r < r_max; r++) {
+    ms_merge_kernel<<<grid, kMsThreads, 0, s>>>(k_a, v_a, k_b, v_b, n, n_dev, r);
+    count_launch();
+  }
+  return cudaGetLastError();
+}
+
 }  // namespace bt

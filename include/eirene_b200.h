@@ -310,6 +310,13 @@ int bt_set_search_group(bt_handle *h, uint32_t lanes);
                                       * per-batch buffers (as bt_execute_batches); any other call on the handle
                                       * in between makes the next one wait for it.  0 runs each batch whole on
                                       * `stream`.  Same answers and tree */
+#define BT_OPT_TOUCH_SORT 18 /* hash front end: the sort of the requests whose key a write touches.  1 sorts
+                              * tiles of 2048 pairs on chip, then merges sorted runs pairwise (merge path)
+                              * until one is left: a few rounds for the few hundred thousand such requests
+                              * of a read-mostly batch; 0 the onesweep radix sort (eight passes of 8 bits,
+                              * BT_OPT_SORT_TILE), better for many; 2 (default) the first while the touched
+                              * count of the batch seen last was at most 2^19, else the second (the first
+                              * batch: the second).  Same order in every case (by key, then request order) */
 #define BT_OPT_SORT_TILE 14     /* radix sort tile of sorted batches: 256, 512 (default) or 1024 threads x 8 keys,
                                  * for whole batches and for the hash front end's touched requests alike
                                  * (bt_autotune picks the two separately) */
