@@ -770,6 +770,9 @@ def main():
                     help="time only BT_MODE_STM batches (v39 meaning) of 2^batch-log2 requests on a "
                          "2^tree-log2-key --dist tree, requests drawn from the same law; a bounded workload for "
                          "kernel profiles")
+    ap.add_argument("--touch-sort", choices=["auto", "merge", "radix"], default="auto",
+                    help="sort of the requests a write touches (BT_OPT_TOUCH_SORT): by the touched count seen "
+                         "last (default), always the tile sort plus merge rounds, always the onesweep radix sort")
     ap.add_argument("--no-host-front-overlap", action="store_true",
                     help="e2e: run each host batch whole on the stream (BT_OPT_HOST_FRONT_OVERLAP 0) instead of "
                          "its front part beside the previous host batch's tree part")
@@ -840,6 +843,7 @@ def main():
                        n_segments=args.segments)
     tree.set_option(E.OPT_FRONT_END, 1 if args.front_end == "hash" else 0)
     tree.set_option(E.OPT_HOST_FRONT_OVERLAP, 0 if args.no_host_front_overlap else 1)
+    tree.set_option(E.OPT_TOUCH_SORT, {"radix": 0, "merge": 1, "auto": 2}[args.touch_sort])
     tk = torch.empty(n_tree, dtype=torch.int64, device="cuda")
     tv = torch.empty(n_tree, dtype=torch.int64, device="cuda")
     E.gen_keys(args.dist, 1 + rank, n_tree, tk, tv, stream)
@@ -1305,6 +1309,7 @@ def main():
                 "learned_retrain_every": args.retrain_every,
                 "node_fill": fill,
                 "learned_retrain_mode": args.retrain_mode,
+                "touch_sort": args.touch_sort,
                 "throughput": ("bt_execute_batches over the timed batches (batch j + 1's front part beside batch "
                                "j's lookups and writes); p50 / p99 batch latency and phases: the same kind of "
                                "batches, one bt_execute_batch call each (forms.*.per_call)"
